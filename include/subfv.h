@@ -1,0 +1,140 @@
+/* subfv_b200: C-ABI of the B200-native subface finite-volume residual path and its
+ * implicit linear solve.
+ *
+ * The entry points mirror the reference's Fortran module procedures so that a thin
+ * iso_c_binding shim can route subfvlagrange / subfvns through them unchanged. All
+ * host arrays use the reference's layouts: sol(5, n_elems) and rhs(5, n_elems) are
+ * column-major (five values per cell, cell after cell), vp(3, n_vert) likewise,
+ * vertex coordinates (3, n_vert). Ids inside descriptors are 1-based like the
+ * reference's.
+ *
+ * Return codes: 0 = OK; > 0 = numerical fault bits (SUBFV_ERR_*); < 0 = API or CUDA
+ * error, text in subfv_last_error(). Handles are not thread-safe; each mesh owns one
+ * CUDA stream and every call is synchronous unless its name ends in _async.
+ */
+#ifndef SUBFV_B200_H
+#define SUBFV_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SUBFV_ERR_MESH_CHECK 1   /* check_mesh failed: mesh_geometry_module.F90:403-408 */
+#define SUBFV_ERR_NONFINITE 2    /* non-finite state, volume or time step */
+#define SUBFV_ERR_NEG_DENSITY 4  /* negative density / specific volume: ns_euler_rs_module.F90:257-266 */
+#define SUBFV_ERR_BAD_OMEGA 8    /* positivity limiter omega <= 1e-6: ns_euler_module.F90:595-598 */
+#define SUBFV_ERR_GMRES 16       /* GMRES did not converge: sparse_bcsr_linear_module.F90:1614,1686 */
+#define SUBFV_ERR_INDEX 32       /* an index outside its array */
+
+const char* subfv_last_error(void);
+int subfv_version(void);
+
+/* ---------------------------------------------------------------------------------
+ * Topology: build_mesh (src/mesh/mesh_connectivity_module.F90:12-59) on the host,
+ * from volume elements as the MSH2 reader produces them
+ * (src/mesh/mesh_reading_module.F90:989-1324). Numbering is identical to the
+ * reference's (BFS vertices, first-touch cells and faces, vertex-ordered subfaces).
+ * Arrays are fetched by name (the mesh_type component they flatten, e.g.
+ * "face_left", "vert_sub_face_off"). */
+typedef struct subfv_topology subfv_topology;
+int subfv_topology_build(int n_vert, const double* coords, int n_elems, const int32_t* elem_kind,
+                         const int32_t* elem_vert_off, const int32_t* elem_vert, int n_bfaces,
+                         const int32_t* bface_off, const int32_t* bface_vert, const int32_t* bface_tag,
+                         int b2d, int periodic, subfv_topology** out);
+int64_t subfv_topology_array_len(const subfv_topology* t, const char* name);
+int subfv_topology_array_get(const subfv_topology* t, const char* name, int32_t* out);
+int subfv_topology_coords(const subfv_topology* t, double* coords_out);
+void subfv_topology_destroy(subfv_topology* t);
+
+/* ---------------------------------------------------------------------------------
+ * Device mesh. subfv_mesh_desc flattens mesh_type (src/mesh/mesh_module.F90:76-89);
+ * the Fortran shim fills it from its mesh after build_mesh. */
+typedef struct subfv_mesh_desc {
+  int32_t n_vert, n_elems, n_faces, n_sub_faces, n_sub_elems;
+  int32_t b2d;
+  const double* vert_coord;             /* (3, n_vert) */
+  const int32_t* elem_kind;             /* (n_elems) */
+  const int32_t* elem_vert_off;         /* (n_elems+1); also offsets of elem%sub_elem */
+  const int32_t* elem_vert;             /* elem%vert */
+  const int32_t* elem_sub_elem;         /* elem%sub_elem */
+  const int32_t* elem_face_off;         /* (n_elems+1) */
+  const int32_t* elem_face;             /* elem%face */
+  const int32_t* face_vert_off;         /* (n_faces+1); also offsets of face%sub_face */
+  const int32_t* face_vert;             /* face%vert */
+  const int32_t* face_sub_face;         /* face%sub_face */
+  const int32_t* face_left;             /* face%left_neigh */
+  const int32_t* face_right;            /* face%right_neigh: >0 cell, 0 wall, <0 -bc tag */
+  const int32_t* sub_face_vert;         /* sub_face%mesh_vert */
+  const int32_t* sub_face_face;         /* sub_face%mesh_face */
+  const int32_t* sub_face_left_sub_elem;  /* sub_face%left_sub_elem_neigh */
+  const int32_t* sub_face_right_sub_elem; /* sub_face%right_sub_elem_neigh (0 none) */
+  const int32_t* sub_face_loc;          /* sub_face%id_loc_around_node */
+  const int32_t* sub_elem_elem;         /* sub_elem%mesh_elem */
+  const int32_t* sub_elem_vert;         /* sub_elem%mesh_vert */
+  const int32_t* sub_elem_loc;          /* sub_elem%id_loc_around_node */
+  const int32_t* sub_elem_sub_face_off; /* (n_sub_elems+1) */
+  const int32_t* sub_elem_sub_face;     /* sub_elem%sub_face */
+  const int32_t* vert_sub_face_off;     /* (n_vert+1) */
+  const int32_t* vert_sub_face;         /* vert%sub_face_neigh */
+  const int32_t* vert_sub_elem_off;     /* (n_vert+1) */
+  const int32_t* vert_sub_elem;         /* vert%sub_elem_neigh */
+  const int32_t* vert_is_bound;         /* vert%is_bound (0/1) */
+} subfv_mesh_desc;
+
+typedef struct subfv_mesh subfv_mesh;
+int subfv_mesh_create(const subfv_mesh_desc* desc, subfv_mesh** out);
+int subfv_mesh_create_from_topology(const subfv_topology* t, int b2d, subfv_mesh** out);
+int subfv_mesh_destroy(subfv_mesh* m);
+int64_t subfv_mesh_device_bytes(const subfv_mesh* m);
+int subfv_mesh_set_coords(subfv_mesh* m, const double* vert_coord);
+int subfv_mesh_get_coords(subfv_mesh* m, double* vert_coord);
+/* name: vert_volume, face_coord, face_norm, face_area, sub_face_norm, sub_face_area,
+ * elem_coord, elem_volume, sub_elem_volume (reference layouts); vert_is_bound as 0/1 doubles */
+int subfv_mesh_get_geometry(subfv_mesh* m, const char* name, double* out);
+
+/* compute_geometry_mesh(mesh, .true., b2d) — src/mesh/mesh_geometry_module.F90:16-57.
+ * Returns SUBFV_ERR_MESH_CHECK where the reference would print and error stop. */
+int subfv_compute_geometry_mesh(subfv_mesh* m);
+
+/* ---------------------------------------------------------------------------------
+ * Lagrangian hydro (subfvlagrange), scheme "classic". */
+
+/* compute_rhs_lagrange(mesh, sol, vp, dt, rhs, n_bc, bc_type, bc_val, b2d, mass) —
+ * src/lagrange/lagrange_module.F90:14-147. sol/rhs (5, n_elems), vp (3, n_vert). */
+int subfv_compute_rhs_lagrange(subfv_mesh* m, const double* sol, double* vp, double* rhs,
+                               int b2d, const double* mass);
+/* compute_dt(mesh, sol, dt, cfl, vp, me, num_procs) — lagrange_module.F90:240-283 */
+int subfv_compute_dt(subfv_mesh* m, const double* sol, double cfl, const double* vp, double* dt);
+/* move_mesh(mesh, vp, dt) — lagrange_module.F90:772-784 */
+int subfv_move_mesh(subfv_mesh* m, const double* vp, double dt);
+
+/* Device-resident time loop of lagrange_main.F90:89-127: state, mass and mesh stay in
+ * HBM; each step = rhs, CFL reduction, mesh motion, geometry, update. The step loop
+ * is replayed from a captured CUDA graph. */
+typedef struct subfv_lag_state subfv_lag_state;
+int subfv_lag_state_create(subfv_mesh* m, const double* sol, const double* mass, double cfl,
+                           double t0, double t_max, int precision, subfv_lag_state** out);
+int subfv_lag_state_destroy(subfv_lag_state* s);
+/* run n_steps (stops early once t >= t_max); returns status bits */
+int subfv_lag_advance(subfv_lag_state* s, int n_steps, int* steps_done, double* t);
+int subfv_lag_advance_async(subfv_lag_state* s, int n_steps);
+int subfv_lag_sync(subfv_lag_state* s, int* steps_done, double* t);
+int subfv_lag_get_sol(subfv_lag_state* s, double* sol);
+int subfv_lag_set_sol(subfv_lag_state* s, const double* sol);
+int subfv_lag_get_vp(subfv_lag_state* s, double* vp);
+int subfv_lag_last_dt(subfv_lag_state* s, double* dt);
+/* one step through host buffers: uploads sol, advances one step, downloads sol */
+int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout);
+/* Runs n_steps steps launched one kernel at a time with CUDA events between kernels on
+ * the mesh's stream; kernel_ms[k] receives the summed milliseconds of kernel k in step
+ * order: node, cell, finalize, move, face geometry, cell geometry + update. */
+int subfv_lag_profile_steps(subfv_lag_state* s, int n_steps, double* kernel_ms);
+
+/* The CUDA stream (cudaStream_t) all work of this mesh is launched on. */
+void* subfv_mesh_stream(subfv_mesh* m);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,172 @@
+"""Test infrastructure only: ctypes binding of the oracle (oracle/_build/liboracle.so).
+
+The oracle is a serial CPU restatement of the reference Fortran (see oracle.h).
+PARITY UNPINNED: no Fortran compiler exists here and the reference's tests hold no
+golden vectors. Only tests/, the smoke check and bench.py's CPU-baseline leg use it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "_build" / "liboracle.so"
+
+PD = C.POINTER(C.c_double)
+PI = C.POINTER(C.c_int32)
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        lib = C.CDLL(str(LIB_PATH))
+        lib.or_mesh_new.restype = C.c_void_p
+        lib.or_mesh_new.argtypes = [C.c_int, PD, C.c_int, PI, PI, PI, C.c_int, PI, PI, PI, C.c_int, C.c_int]
+        lib.or_mesh_free.argtypes = [C.c_void_p]
+        lib.or_topo_len.argtypes = [C.c_void_p, C.c_char_p]
+        lib.or_topo_get.argtypes = [C.c_void_p, C.c_char_p, PI]
+        lib.or_vert_is_bound.argtypes = [C.c_void_p, PI]
+        lib.or_geometry.argtypes = [C.c_void_p, C.c_int]
+        lib.or_geometry_ok.argtypes = [C.c_void_p]
+        lib.or_set_coords.argtypes = [C.c_void_p, PD]
+        lib.or_geom_get.argtypes = [C.c_void_p, C.c_char_p, PD]
+        lib.or_lag_rhs.argtypes = [C.c_void_p, PD, PD, PD, C.c_int, PD]
+        lib.or_lag_dt.restype = C.c_double
+        lib.or_lag_dt.argtypes = [C.c_void_p, PD, C.c_double, PD]
+        lib.or_lag_move.argtypes = [C.c_void_p, PD, C.c_double]
+        lib.or_sedov_init.argtypes = [C.c_void_p, PD, C.c_double, C.c_double, PI]
+        lib.or_lag_run.argtypes = [C.c_void_p, PD, PD, PD, PD, C.c_double, C.c_double, C.c_int, C.c_int, PD, PD]
+        lib.or_inverse_3_by_3.argtypes = [PD, PD]
+        lib.or_fnorm2.restype = C.c_double
+        lib.or_fnorm2.argtypes = [PD, C.c_int]
+        _lib = lib
+    return _lib
+
+
+def _pd(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(PD)
+
+
+def _pi(a):
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(PI)
+
+
+class OracleMesh:
+    """build_mesh + compute_geometry_mesh on the CPU, as the reference does them."""
+
+    def __init__(self, raw):
+        lib = load()
+        self._keep = [np.ascontiguousarray(raw.coords.reshape(-1), np.float64),
+                      np.ascontiguousarray(raw.elem_kind, np.int32),
+                      np.ascontiguousarray(raw.elem_vert_off, np.int32),
+                      np.ascontiguousarray(raw.elem_vert, np.int32),
+                      np.ascontiguousarray(raw.bface_off, np.int32),
+                      np.ascontiguousarray(raw.bface_vert, np.int32),
+                      np.ascontiguousarray(raw.bface_tag, np.int32)]
+        c, k, o, v, bo, bv, bt = self._keep
+        self.b2d = bool(raw.b2d)
+        self._h = lib.or_mesh_new(raw.n_vert, _pd(c), raw.n_elems, _pi(k), _pi(o), _pi(v), int(bo.size - 1),
+                                  _pi(bo), _pi(bv), _pi(bt), int(raw.b2d), int(raw.periodic))
+        if not self._h:
+            raise RuntimeError("oracle build_mesh failed")
+        s = self.topo("sizes")
+        self.n_vert, self.n_elems, self.n_faces, self.n_sub_faces, self.n_sub_elems = map(int, s[:5])
+
+    def topo(self, name):
+        lib = load()
+        n = lib.or_topo_len(self._h, name.encode())
+        if n < 0:
+            raise KeyError(name)
+        out = np.empty(n, np.int32)
+        lib.or_topo_get(self._h, name.encode(), _pi(out))
+        return out
+
+    _N = {"vert_coord": ("n_vert", 3), "vert_volume": ("n_vert", 1), "face_coord": ("n_faces", 3),
+          "face_norm": ("n_faces", 3), "face_area": ("n_faces", 1), "sub_face_norm": ("n_sub_faces", 3),
+          "sub_face_area": ("n_sub_faces", 1), "elem_coord": ("n_elems", 3), "elem_volume": ("n_elems", 1),
+          "sub_elem_volume": ("n_sub_elems", 1)}
+
+    def geom(self, name):
+        cnt, comp = self._N[name]
+        n = getattr(self, cnt)
+        out = np.empty(n * comp)
+        if load().or_geom_get(self._h, name.encode(), _pd(out)) != 0:
+            raise KeyError(name)
+        return out.reshape(n, comp) if comp > 1 else out
+
+    def vert_is_bound(self):
+        out = np.empty(self.n_vert, np.int32)
+        load().or_vert_is_bound(self._h, _pi(out))
+        return out
+
+    def geometry(self):
+        return load().or_geometry(self._h, int(self.b2d))
+
+    def geometry_ok(self):
+        return bool(load().or_geometry_ok(self._h))
+
+    def set_coords(self, c):
+        c = np.ascontiguousarray(np.asarray(c).reshape(-1), np.float64)
+        load().or_set_coords(self._h, _pd(c))
+
+    # --- Lagrange
+    def lag_rhs(self, sol, mass):
+        sol = np.ascontiguousarray(sol, np.float64)
+        mass = np.ascontiguousarray(mass, np.float64)
+        vp = np.zeros((self.n_vert, 3))
+        rhs = np.zeros((self.n_elems, 5))
+        load().or_lag_rhs(self._h, _pd(sol), _pd(vp), _pd(rhs), int(self.b2d), _pd(mass))
+        return vp, rhs
+
+    def lag_dt(self, sol, cfl, vp):
+        sol = np.ascontiguousarray(sol, np.float64)
+        vp = np.ascontiguousarray(vp, np.float64)
+        return load().or_lag_dt(self._h, _pd(sol), float(cfl), _pd(vp))
+
+    def lag_move(self, vp, dt):
+        vp = np.ascontiguousarray(vp, np.float64)
+        load().or_lag_move(self._h, _pd(vp), float(dt))
+
+    def sedov_init(self, r_sedov=0.06, e_total=0.983909, mask=None):
+        sol = np.zeros((self.n_elems, 5))
+        m = None if mask is None else np.ascontiguousarray(mask, np.int32)
+        rc = load().or_sedov_init(self._h, _pd(sol), float(r_sedov), float(e_total), None if m is None else _pi(m))
+        if rc != 0:
+            raise ValueError("r_sedov too small")
+        return sol
+
+    def lag_run(self, sol, mass, cfl, t_max, max_steps, t0=0.0):
+        """Runs the reference time loop in place on sol; returns (steps, t, last dt)."""
+        assert sol.dtype == np.float64 and sol.flags["C_CONTIGUOUS"]
+        mass = np.ascontiguousarray(mass, np.float64)
+        vp = np.zeros((self.n_vert, 3))
+        rhs = np.zeros((self.n_elems, 5))
+        t = C.c_double(t0)
+        dt = C.c_double(0.0)
+        n = load().or_lag_run(self._h, _pd(sol), _pd(vp), _pd(rhs), _pd(mass), float(cfl), float(t_max),
+                              int(max_steps), int(self.b2d), C.byref(t), C.byref(dt))
+        return n, t.value, dt.value, vp
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().or_mesh_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

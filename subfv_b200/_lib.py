@@ -1,0 +1,109 @@
+"""ctypes binding of the native library (include/subfv.h).
+
+The library is built in-tree (subfv_b200/_build/libsubfv_b200.so). There is no
+fallback: if it is missing or was built without the entry points, loading fails with
+an error naming the build command.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "_build" / "libsubfv_b200.so"
+
+c_int = C.c_int
+c_i64 = C.c_int64
+c_dbl = C.c_double
+c_char_p = C.c_char_p
+P = C.c_void_p
+PI32 = C.POINTER(C.c_int32)
+PD = C.POINTER(C.c_double)
+
+# name -> (restype, argtypes); every exported symbol of include/subfv.h
+SIGNATURES = {
+    "subfv_last_error": (c_char_p, []),
+    "subfv_version": (c_int, []),
+    "subfv_topology_build": (c_int, [c_int, PD, c_int, PI32, PI32, PI32, c_int, PI32, PI32, PI32, c_int, c_int,
+                                     C.POINTER(P)]),
+    "subfv_topology_array_len": (c_i64, [P, c_char_p]),
+    "subfv_topology_array_get": (c_int, [P, c_char_p, PI32]),
+    "subfv_topology_coords": (c_int, [P, PD]),
+    "subfv_topology_destroy": (None, [P]),
+    "subfv_mesh_create": (c_int, [P, C.POINTER(P)]),
+    "subfv_mesh_create_from_topology": (c_int, [P, c_int, C.POINTER(P)]),
+    "subfv_mesh_destroy": (c_int, [P]),
+    "subfv_mesh_device_bytes": (c_i64, [P]),
+    "subfv_mesh_set_coords": (c_int, [P, PD]),
+    "subfv_mesh_get_coords": (c_int, [P, PD]),
+    "subfv_mesh_get_geometry": (c_int, [P, c_char_p, PD]),
+    "subfv_compute_geometry_mesh": (c_int, [P]),
+    "subfv_compute_rhs_lagrange": (c_int, [P, PD, PD, PD, c_int, PD]),
+    "subfv_compute_dt": (c_int, [P, PD, c_dbl, PD, PD]),
+    "subfv_move_mesh": (c_int, [P, PD, c_dbl]),
+    "subfv_lag_state_create": (c_int, [P, PD, PD, c_dbl, c_dbl, c_dbl, c_int, C.POINTER(P)]),
+    "subfv_lag_state_destroy": (c_int, [P]),
+    "subfv_lag_advance": (c_int, [P, c_int, C.POINTER(c_int), PD]),
+    "subfv_lag_advance_async": (c_int, [P, c_int]),
+    "subfv_lag_sync": (c_int, [P, C.POINTER(c_int), PD]),
+    "subfv_lag_get_sol": (c_int, [P, PD]),
+    "subfv_lag_set_sol": (c_int, [P, PD]),
+    "subfv_lag_get_vp": (c_int, [P, PD]),
+    "subfv_lag_last_dt": (c_int, [P, PD]),
+    "subfv_lag_step_host": (c_int, [P, PD]),
+    "subfv_lag_profile_steps": (c_int, [P, c_int, PD]),
+    "subfv_mesh_stream": (P, [P]),
+}
+
+_lib = None
+
+
+class SubfvError(RuntimeError):
+    pass
+
+
+def load():
+    """Load the native library once; raise if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise SubfvError(f"native library missing: {LIB_PATH} (run `python -m subfv_b200.build`)")
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    e = load().subfv_last_error()
+    return e.decode() if e else ""
+
+
+def check(rc: int, what: str) -> int:
+    """Raise on API/CUDA errors (rc < 0); return numerical status bits (rc >= 0)."""
+    if rc < 0:
+        raise SubfvError(f"{what} failed ({rc}): {last_error()}")
+    return rc
+
+
+def f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def pd(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(PD)
+
+
+def pi(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(PI32)

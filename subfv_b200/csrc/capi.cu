@@ -1,0 +1,504 @@
+// C-ABI entry points (include/subfv.h): topology, device mesh, Lagrangian hydro.
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/subfv.h"
+#include "common.cuh"
+#include "lagrange.cuh"
+#include "mesh_dev.cuh"
+#include "topology.h"
+
+namespace subfv {
+namespace {
+thread_local std::string g_err;
+}
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+}  // namespace subfv
+
+using namespace subfv;
+
+struct subfv_topology {
+  Topology t;
+};
+
+// A device mesh plus the scratch buffers the stateless reference-shaped calls need.
+struct subfv_mesh {
+  DevMesh d;
+  double* stage = nullptr;  // host-layout staging, max(5*ne, 3*nv) doubles
+  double* sol6 = nullptr;   // [ne][6]
+  double* rhs6 = nullptr;   // [ne][6]
+  double* mass = nullptr;   // [ne]
+  LagScalars* sc = nullptr;
+};
+
+struct subfv_lag_state {
+  subfv_mesh* m = nullptr;
+  double* sol6 = nullptr;
+  double* rhs6 = nullptr;
+  LagScalars* sc = nullptr;
+  double* host_stage = nullptr;  // pinned staging for the host-buffer step
+  double* dev_stage = nullptr;
+  int precision = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_steps = 0;
+};
+
+namespace {
+
+int check_status(DevMesh& d) {
+  unsigned st = 0;
+  SUBFV_CUDA(cudaMemcpyAsync(&st, d.status, sizeof(unsigned), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  return (int)st;
+}
+int clear_status(DevMesh& d) {
+  SUBFV_CUDA(cudaMemsetAsync(d.status, 0, sizeof(unsigned), d.stream));
+  return 0;
+}
+int ensure_scratch(subfv_mesh* m) {
+  if (m->stage) return 0;
+  size_t n = std::max<size_t>(5 * (size_t)m->d.ne, 3 * (size_t)m->d.nv);
+  SUBFV_CUDA(cudaMalloc(&m->stage, n * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&m->sol6, 6 * (size_t)m->d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&m->rhs6, 6 * (size_t)m->d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&m->mass, (size_t)m->d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&m->sc, sizeof(LagScalars)));
+  return 0;
+}
+int load_sol(subfv_mesh* m, const double* sol, const double* mass) {
+  DevMesh& d = m->d;
+  SUBFV_CUDA(cudaMemcpyAsync(m->stage, sol, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  if (mass) SUBFV_CUDA(cudaMemcpyAsync(m->mass, mass, (size_t)d.ne * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  launch_pack6(d, d.ne, m->stage, mass ? m->mass : nullptr, m->sol6);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* subfv_last_error(void) { return subfv::last_error(); }
+int subfv_version(void) { return 1; }
+
+// ------------------------------------------------------------------- topology
+int subfv_topology_build(int n_vert, const double* coords, int n_elems, const int32_t* elem_kind,
+                         const int32_t* elem_vert_off, const int32_t* elem_vert, int n_bfaces,
+                         const int32_t* bface_off, const int32_t* bface_vert, const int32_t* bface_tag,
+                         int b2d, int periodic, subfv_topology** out) {
+  if (!out || !coords || !elem_kind || !elem_vert_off || !elem_vert) {
+    set_error("subfv_topology_build: null argument");
+    return -2;
+  }
+  RawMeshView in{n_vert, coords, n_elems, elem_kind, elem_vert_off, elem_vert,
+                 n_bfaces, bface_off, bface_vert, bface_tag, b2d, periodic};
+  auto* t = new subfv_topology();
+  std::string err;
+  int rc = build_topology(in, t->t, &err);
+  if (rc) {
+    delete t;
+    set_error("subfv_topology_build: " + err);
+    return -3;
+  }
+  *out = t;
+  return 0;
+}
+int64_t subfv_topology_array_len(const subfv_topology* t, const char* name) {
+  auto it = t->t.arr.find(name);
+  return it == t->t.arr.end() ? -1 : (int64_t)it->second.size();
+}
+int subfv_topology_array_get(const subfv_topology* t, const char* name, int32_t* out) {
+  auto it = t->t.arr.find(name);
+  if (it == t->t.arr.end()) {
+    set_error(std::string("unknown topology array ") + name);
+    return -2;
+  }
+  std::memcpy(out, it->second.data(), it->second.size() * sizeof(int32_t));
+  return 0;
+}
+int subfv_topology_coords(const subfv_topology* t, double* out) {
+  std::memcpy(out, t->t.vert_coord.data(), t->t.vert_coord.size() * sizeof(double));
+  return 0;
+}
+void subfv_topology_destroy(subfv_topology* t) { delete t; }
+
+// ------------------------------------------------------------------- mesh
+int subfv_mesh_create(const subfv_mesh_desc* desc, subfv_mesh** out) {
+  if (!desc || !out) {
+    set_error("subfv_mesh_create: null argument");
+    return -2;
+  }
+  auto* m = new subfv_mesh();
+  int rc = devmesh_create(desc, &m->d);
+  if (rc) {
+    devmesh_free(&m->d);
+    delete m;
+    return rc;
+  }
+  *out = m;
+  return 0;
+}
+
+int subfv_mesh_create_from_topology(const subfv_topology* tp, int b2d, subfv_mesh** out) {
+  const Topology& t = tp->t;
+  subfv_mesh_desc d{};
+  d.n_vert = t.n_vert;
+  d.n_elems = t.n_elems;
+  d.n_faces = t.n_faces;
+  d.n_sub_faces = t.n_sub_faces;
+  d.n_sub_elems = t.n_sub_elems;
+  d.b2d = b2d;
+  d.vert_coord = t.vert_coord.data();
+  d.elem_kind = t.a("elem_kind").data();
+  d.elem_vert_off = t.a("elem_vert_off").data();
+  d.elem_vert = t.a("elem_vert").data();
+  d.elem_sub_elem = t.a("elem_sub_elem").data();
+  d.elem_face_off = t.a("elem_face_off").data();
+  d.elem_face = t.a("elem_face").data();
+  d.face_vert_off = t.a("face_vert_off").data();
+  d.face_vert = t.a("face_vert").data();
+  d.face_sub_face = t.a("face_sub_face").data();
+  d.face_left = t.a("face_left").data();
+  d.face_right = t.a("face_right").data();
+  d.sub_face_vert = t.a("sub_face_vert").data();
+  d.sub_face_face = t.a("sub_face_face").data();
+  d.sub_face_left_sub_elem = t.a("sub_face_left_sub_elem").data();
+  d.sub_face_right_sub_elem = t.a("sub_face_right_sub_elem").data();
+  d.sub_face_loc = t.a("sub_face_loc").data();
+  d.sub_elem_elem = t.a("sub_elem_elem").data();
+  d.sub_elem_vert = t.a("sub_elem_vert").data();
+  d.sub_elem_loc = t.a("sub_elem_loc").data();
+  d.sub_elem_sub_face_off = t.a("sub_elem_sub_face_off").data();
+  d.sub_elem_sub_face = t.a("sub_elem_sub_face").data();
+  d.vert_sub_face_off = t.a("vert_sub_face_off").data();
+  d.vert_sub_face = t.a("vert_sub_face").data();
+  d.vert_sub_elem_off = t.a("vert_sub_elem_off").data();
+  d.vert_sub_elem = t.a("vert_sub_elem").data();
+  d.vert_is_bound = t.a("vert_is_bound").data();
+  return subfv_mesh_create(&d, out);
+}
+
+int subfv_mesh_destroy(subfv_mesh* m) {
+  if (!m) return 0;
+  cudaFree(m->stage);
+  cudaFree(m->sol6);
+  cudaFree(m->rhs6);
+  cudaFree(m->mass);
+  cudaFree(m->sc);
+  devmesh_free(&m->d);
+  delete m;
+  return 0;
+}
+
+int64_t subfv_mesh_device_bytes(const subfv_mesh* m) { return (int64_t)m->d.bytes; }
+
+int subfv_mesh_set_coords(subfv_mesh* m, const double* c) {
+  DevMesh& d = m->d;
+  std::vector<double4> x(d.nv);
+  for (int i = 0; i < d.nv; ++i) x[i] = make_double4(c[3 * i], c[3 * i + 1], c[3 * i + 2], 0.0);
+  SUBFV_CUDA(cudaMemcpyAsync(d.x, x.data(), x.size() * sizeof(double4), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  return 0;
+}
+int subfv_mesh_get_coords(subfv_mesh* m, double* c) {
+  DevMesh& d = m->d;
+  std::vector<double4> x(d.nv);
+  SUBFV_CUDA(cudaMemcpyAsync(x.data(), d.x, x.size() * sizeof(double4), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  for (int i = 0; i < d.nv; ++i) {
+    c[3 * i] = x[i].x;
+    c[3 * i + 1] = x[i].y;
+    c[3 * i + 2] = x[i].z;
+  }
+  return 0;
+}
+
+int subfv_mesh_get_geometry(subfv_mesh* m, const char* name, double* out) {
+  DevMesh& d = m->d;
+  std::string n(name);
+  auto get4 = [&](const double4* src, int cnt, int ncomp, int first) -> int {
+    std::vector<double4> h(cnt);
+    SUBFV_CUDA(cudaMemcpyAsync(h.data(), src, cnt * sizeof(double4), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+    for (int i = 0; i < cnt; ++i) {
+      const double v[4] = {h[i].x, h[i].y, h[i].z, h[i].w};
+      for (int k = 0; k < ncomp; ++k) out[(size_t)ncomp * i + k] = v[first + k];
+    }
+    return 0;
+  };
+  auto get1 = [&](const double* src, int cnt) -> int {
+    SUBFV_CUDA(cudaMemcpyAsync(out, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+    return 0;
+  };
+  if (n == "face_coord") return get4(d.fc, d.nf, 3, 0);
+  if (n == "face_norm") return get4(d.fn, d.nf, 3, 0);
+  if (n == "face_area") return get4(d.fn, d.nf, 1, 3);
+  if (n == "sub_face_norm") return get4(d.sfn, d.nsf, 3, 0);
+  if (n == "sub_face_area") return get4(d.sfn, d.nsf, 1, 3);
+  if (n == "elem_coord") return get4(d.cc, d.ne, 3, 0);
+  if (n == "elem_volume") return get1(d.vol, d.ne);
+  if (n == "sub_elem_volume") return get1(d.vol_se, d.nse);
+  if (n == "vert_volume") return get1(d.vol_v, d.nv);
+  if (n == "vert_is_bound") {
+    std::vector<int8_t> h(d.nv);
+    SUBFV_CUDA(cudaMemcpyAsync(h.data(), d.is_bound, d.nv, cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+    for (int i = 0; i < d.nv; ++i) out[i] = h[i];
+    return 0;
+  }
+  set_error("subfv_mesh_get_geometry: unknown array " + n);
+  return -2;
+}
+
+int subfv_compute_geometry_mesh(subfv_mesh* m) {
+  DevMesh& d = m->d;
+  if (clear_status(d)) return -1;
+  launch_face_geometry(d);
+  launch_cell_geometry(d);
+  launch_vert_is_bound(d);
+  launch_vert_volume(d);
+  SUBFV_CUDA(cudaGetLastError());
+  return check_status(d);
+}
+
+// ------------------------------------------------------------------- Lagrange (stateless)
+int subfv_compute_rhs_lagrange(subfv_mesh* m, const double* sol, double* vp, double* rhs, int b2d,
+                               const double* mass) {
+  DevMesh& d = m->d;
+  if (ensure_scratch(m) || clear_status(d)) return -1;
+  d.b2d = b2d;
+  if (load_sol(m, sol, mass)) return -1;
+  launch_lag_node(d, m->sol6, nullptr, 0, 0);
+  launch_lag_cell(d, m->sol6, m->rhs6, nullptr, nullptr, 0, 1);
+  launch_unpack6(d, d.ne, m->rhs6, m->stage);
+  SUBFV_CUDA(cudaMemcpyAsync(rhs, m->stage, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  std::vector<double4> h(d.nv);
+  SUBFV_CUDA(cudaMemcpyAsync(h.data(), d.vp, d.nv * sizeof(double4), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  for (int i = 0; i < d.nv; ++i) {
+    vp[3 * i] = h[i].x;
+    vp[3 * i + 1] = h[i].y;
+    vp[3 * i + 2] = h[i].z;
+  }
+  SUBFV_CUDA(cudaGetLastError());
+  return check_status(d);
+}
+
+int subfv_compute_dt(subfv_mesh* m, const double* sol, double cfl, const double* vp, double* dt) {
+  DevMesh& d = m->d;
+  if (ensure_scratch(m) || clear_status(d)) return -1;
+  if (load_sol(m, sol, nullptr)) return -1;
+  SUBFV_CUDA(cudaMemcpyAsync(m->stage, vp, 3 * (size_t)d.nv * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  launch_vp_in(d, m->stage);
+  double* slot = &m->sc->dtmin;
+  launch_set_scalar(d, slot, 1e6);
+  launch_lag_cell(d, m->sol6, nullptr, nullptr, slot, 0, 2);
+  double h = 0;
+  SUBFV_CUDA(cudaMemcpyAsync(&h, slot, sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  SUBFV_CUDA(cudaGetLastError());
+  *dt = cfl * h;
+  return check_status(d);
+}
+
+int subfv_move_mesh(subfv_mesh* m, const double* vp, double dt) {
+  DevMesh& d = m->d;
+  if (ensure_scratch(m)) return -1;
+  SUBFV_CUDA(cudaMemcpyAsync(m->stage, vp, 3 * (size_t)d.nv * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  launch_vp_in(d, m->stage);
+  launch_lag_move(d, nullptr, dt);
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  SUBFV_CUDA(cudaGetLastError());
+  return 0;
+}
+
+// ------------------------------------------------------------------- Lagrange (device-resident)
+int subfv_lag_state_create(subfv_mesh* m, const double* sol, const double* mass, double cfl, double t0,
+                           double t_max, int precision, subfv_lag_state** out) {
+  if (!m || !sol || !mass || !out || (precision != 0 && precision != 1)) {
+    set_error("subfv_lag_state_create: bad argument");
+    return -2;
+  }
+  DevMesh& d = m->d;
+  if (ensure_scratch(m)) return -1;
+  auto* s = new subfv_lag_state();
+  s->m = m;
+  s->precision = precision;
+  SUBFV_CUDA(cudaMalloc(&s->sol6, 6 * (size_t)d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&s->rhs6, 6 * (size_t)d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&s->sc, sizeof(LagScalars)));
+  SUBFV_CUDA(cudaMallocHost(&s->host_stage, 5 * (size_t)d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&s->dev_stage, 5 * (size_t)d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMemsetAsync(s->rhs6, 0, 6 * (size_t)d.ne * sizeof(double), d.stream));
+  LagScalars h{};
+  h.dtmin = 1e6;
+  h.t = t0;
+  h.t_max = t_max;
+  h.cfl = cfl;
+  h.done = (t0 < t_max) ? 0 : 1;
+  SUBFV_CUDA(cudaMemcpyAsync(s->sc, &h, sizeof(h), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, sol, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(m->mass, mass, (size_t)d.ne * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  launch_pack6(d, d.ne, s->dev_stage, m->mass, s->sol6);
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  SUBFV_CUDA(cudaGetLastError());
+  *out = s;
+  return 0;
+}
+
+int subfv_lag_state_destroy(subfv_lag_state* s) {
+  if (!s) return 0;
+  if (s->graph) cudaGraphExecDestroy(s->graph);
+  cudaFree(s->sol6);
+  cudaFree(s->rhs6);
+  cudaFree(s->sc);
+  cudaFree(s->dev_stage);
+  cudaFreeHost(s->host_stage);
+  delete s;
+  return 0;
+}
+
+namespace {
+// Captures `steps` consecutive steps into one graph (reused while `steps` is unchanged).
+int lag_graph(subfv_lag_state* s, int steps) {
+  if (s->graph && s->graph_steps == steps) return 0;
+  if (s->graph) {
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+  }
+  DevMesh& d = s->m->d;
+  cudaGraph_t g;
+  SUBFV_CUDA(cudaStreamBeginCapture(d.stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < steps; ++i) enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
+  SUBFV_CUDA(cudaStreamEndCapture(d.stream, &g));
+  cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    set_error(std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    return -1;
+  }
+  s->graph_steps = steps;
+  return 0;
+}
+}  // namespace
+
+int subfv_lag_advance_async(subfv_lag_state* s, int n_steps) {
+  DevMesh& d = s->m->d;
+  const int chunk = 16;
+  if (n_steps >= chunk) {
+    if (lag_graph(s, chunk)) return -1;
+    for (int i = 0; i + chunk <= n_steps; i += chunk) SUBFV_CUDA(cudaGraphLaunch(s->graph, d.stream));
+  }
+  for (int i = 0; i < n_steps % chunk; ++i) enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
+  SUBFV_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int subfv_lag_sync(subfv_lag_state* s, int* steps_done, double* t) {
+  DevMesh& d = s->m->d;
+  LagScalars h{};
+  SUBFV_CUDA(cudaMemcpyAsync(&h, s->sc, sizeof(h), cudaMemcpyDeviceToHost, d.stream));
+  int st = check_status(d);
+  if (st < 0) return st;
+  if (steps_done) *steps_done = (int)h.steps;
+  if (t) *t = h.t;
+  return st;
+}
+
+int subfv_lag_advance(subfv_lag_state* s, int n_steps, int* steps_done, double* t) {
+  if (subfv_lag_advance_async(s, n_steps)) return -1;
+  return subfv_lag_sync(s, steps_done, t);
+}
+
+int subfv_lag_get_sol(subfv_lag_state* s, double* sol) {
+  DevMesh& d = s->m->d;
+  launch_unpack6(d, d.ne, s->sol6, s->dev_stage);
+  SUBFV_CUDA(cudaMemcpyAsync(sol, s->dev_stage, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  return 0;
+}
+int subfv_lag_set_sol(subfv_lag_state* s, const double* sol) {
+  DevMesh& d = s->m->d;
+  SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, sol, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  launch_pack6(d, d.ne, s->dev_stage, nullptr, s->sol6);
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  return 0;
+}
+int subfv_lag_get_vp(subfv_lag_state* s, double* vp) {
+  DevMesh& d = s->m->d;
+  std::vector<double4> h(d.nv);
+  SUBFV_CUDA(cudaMemcpyAsync(h.data(), d.vp, d.nv * sizeof(double4), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  for (int i = 0; i < d.nv; ++i) {
+    vp[3 * i] = h[i].x;
+    vp[3 * i + 1] = h[i].y;
+    vp[3 * i + 2] = h[i].z;
+  }
+  return 0;
+}
+int subfv_lag_last_dt(subfv_lag_state* s, double* dt) {
+  DevMesh& d = s->m->d;
+  LagScalars h{};
+  SUBFV_CUDA(cudaMemcpyAsync(&h, s->sc, sizeof(h), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  *dt = h.dt;
+  return 0;
+}
+
+// Host-buffer step: pinned staging, one H2D of the state, one step, one D2H.
+int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout) {
+  DevMesh& d = s->m->d;
+  size_t bytes = 5 * (size_t)d.ne * sizeof(double);
+  std::memcpy(s->host_stage, sol_inout, bytes);
+  SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, s->host_stage, bytes, cudaMemcpyHostToDevice, d.stream));
+  launch_pack6(d, d.ne, s->dev_stage, nullptr, s->sol6);
+  enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
+  launch_unpack6(d, d.ne, s->sol6, s->dev_stage);
+  SUBFV_CUDA(cudaMemcpyAsync(s->host_stage, s->dev_stage, bytes, cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  std::memcpy(sol_inout, s->host_stage, bytes);
+  return check_status(d);
+}
+
+}  // extern "C"
+
+extern "C" {
+
+void* subfv_mesh_stream(subfv_mesh* m) { return (void*)m->d.stream; }
+
+int subfv_lag_profile_steps(subfv_lag_state* s, int n_steps, double* kernel_ms) {
+  DevMesh& d = s->m->d;
+  const int K = 6;
+  cudaEvent_t ev[K + 1];
+  for (int k = 0; k <= K; ++k) SUBFV_CUDA(cudaEventCreate(&ev[k]));
+  for (int k = 0; k < K; ++k) kernel_ms[k] = 0.0;
+  for (int i = 0; i < n_steps; ++i) {
+    SUBFV_CUDA(cudaEventRecord(ev[0], d.stream));
+    launch_lag_node(d, s->sol6, s->sc, s->precision, 1);
+    SUBFV_CUDA(cudaEventRecord(ev[1], d.stream));
+    launch_lag_cell(d, s->sol6, s->rhs6, s->sc, &s->sc->dtmin, s->precision, 3);
+    SUBFV_CUDA(cudaEventRecord(ev[2], d.stream));
+    launch_lag_finalize(d, s->sc);
+    SUBFV_CUDA(cudaEventRecord(ev[3], d.stream));
+    launch_lag_move(d, s->sc, 0.0);
+    SUBFV_CUDA(cudaEventRecord(ev[4], d.stream));
+    launch_face_geometry(d, s->sc);
+    SUBFV_CUDA(cudaEventRecord(ev[5], d.stream));
+    launch_cell_geometry(d, s->sol6, s->rhs6, s->sc);
+    SUBFV_CUDA(cudaEventRecord(ev[6], d.stream));
+    SUBFV_CUDA(cudaEventSynchronize(ev[6]));
+    for (int k = 0; k < K; ++k) {
+      float ms = 0.f;
+      SUBFV_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      kernel_ms[k] += ms;
+    }
+  }
+  for (int k = 0; k <= K; ++k) cudaEventDestroy(ev[k]);
+  SUBFV_CUDA(cudaGetLastError());
+  return check_status(d);
+}
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// Shared device helpers for the subface finite-volume kernels (sm_100a).
+//
+// The plain-FP64 kernels are compiled with --fmad=false and evaluate every
+// expression in the same order as the reference Fortran, so a kernel and the CPU
+// restatement of the same routine produce the same bits.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+namespace subfv {
+
+constexpr double kGamma = 7.0 / 5.0;
+
+// Error bits a kernel records in the step status word (it never traps).
+enum StatusBits : unsigned {
+  kErrMeshCheck = 1u << 0,   // check_mesh failed (mesh_geometry_module.F90:403-408)
+  kErrNonFinite = 1u << 1,   // a non-finite state, volume or time step
+  kErrNegDensity = 1u << 2,  // negative specific volume / density
+  kErrBadOmega = 1u << 3,    // positivity limiter gave omega <= 1e-6 (ns_euler_module.F90:595)
+  kErrGmres = 1u << 4,       // GMRES did not converge (warning)
+  kErrIndex = 1u << 5,       // an index outside its array (checked builds)
+};
+
+// gfortran's inline NORM2 of a 3-vector: scaled sum of squares, scale starting at 1.
+__host__ __device__ inline double fnorm2_3(double a0, double a1, double a2) {
+  double scale = 1.0, res = 0.0;
+  const double a[3] = {a0, a1, a2};
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    if (a[i] != 0.0) {
+      double ax = fabs(a[i]);
+      if (ax > scale) {
+        double v = scale / ax;
+        res = 1.0 + res * v * v;
+        scale = ax;
+      } else {
+        double v = ax / scale;
+        res += v * v;
+      }
+    }
+  }
+  return scale * sqrt(res);
+}
+
+// Lagrangian pressure (lagrange_module.F90:429-436); u = (tau, u, v, w, e).
+__host__ __device__ inline double lag_pressure(double tau, double u1, double u2, double u3, double e) {
+  double n = fnorm2_3(u1, u2, u3);
+  return (kGamma - 1.0) / tau * (e - 0.5 * (n * n));
+}
+
+__host__ __device__ inline double dot3(double a0, double a1, double a2, double b0, double b1, double b2) {
+  double s = 0.0;
+  s = s + a0 * b0;
+  s = s + a1 * b1;
+  s = s + a2 * b2;
+  return s;
+}
+
+// min over non-negative doubles through their bit patterns (order independent, exact)
+__device__ inline void atomic_min_pos(double* addr, double v) {
+  atomicMin(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(v));
+}
+
+void set_error(const std::string& msg);
+
+#define SUBFV_CUDA(call)                                                          \
+  do {                                                                            \
+    cudaError_t e_ = (call);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      ::subfv::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));     \
+      return -1;                                                                  \
+    }                                                                             \
+  } while (0)
+
+// Device-side scalars of a time loop; one struct per in-flight problem.
+struct LagScalars {
+  double dtmin;               // running CFL minimum of the current step
+  double dt;                  // time step of the current step
+  double t, t_max, cfl;
+  unsigned long long steps;   // steps taken
+  int done;                   // t >= t_max: later steps are no-ops
+  int skip;                   // this step was a no-op
+};
+
+inline int grid_for(long long n, int block) { return (int)((n + block - 1) / block); }
+
+}  // namespace subfv

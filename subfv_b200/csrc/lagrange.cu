@@ -1,0 +1,367 @@
+// Lagrangian hydro step, scheme "classic" (src/lagrange/lagrange_module.F90:14-147,
+// 240-283, 772-784; time loop src/lagrange/lagrange_main.F90:89-127) on the GPU.
+//
+// Per step, all in HBM, no host round trip:
+//   k_lag_node     one thread per vertex: nodal 3x3 system (Mp, Rp, Bp) over the
+//                  vertex's subfaces, inverse_3_by_3, vp; also the vertex dual volume
+//   k_lag_cell     one thread per cell: deterministic gather of the subface fluxes in
+//                  the reference's scatter order (no float atomics) -> rhs, and the
+//                  cell's CFL terms -> block min -> one atomicMin on the bit pattern
+//   k_lag_finalize one thread: dt = cfl*min, clip to t_max, t += dt
+//   k_lag_move     x += dt*vp
+//   geometry       k_face_geometry, k_cell_geometry (fused with sol += dt*rhs)
+//
+// precision 0 (plain FP64) evaluates every expression in the reference's order and is
+// compiled without FMA contraction: bit-identical to the CPU restatement.
+// precision 1 (mixed) evaluates the per-subface wave speeds and fluxes in FP32 and
+// keeps the nodal 3x3 solve, positions, volumes and the residual sums in FP64.
+#include <vector>
+
+#include "../../include/subfv.h"
+#include "common.cuh"
+#include "lagrange.cuh"
+#include "mesh_dev.cuh"
+
+namespace subfv {
+
+namespace {
+
+struct U5 {
+  double t, u, v, w, e;
+};
+__device__ inline U5 ld_u(const double* sol6, int c) {
+  const double2* p = reinterpret_cast<const double2*>(sol6 + 6 * (size_t)c);
+  double2 a = p[0], b = p[1], d = p[2];
+  return {a.x, a.y, b.x, b.y, d.x};
+}
+__device__ inline double ld_mass(const double* sol6, int c) { return sol6[6 * (size_t)c + 5]; }
+
+template <int P>
+struct Flt;
+template <>
+struct Flt<0> {
+  using T = double;
+};
+template <>
+struct Flt<1> {
+  using T = float;
+};
+
+// Wave speed of one side (lagrange_module.F90:68-73), in the precision of P.
+template <int P>
+__device__ inline double lam_side(double p_me, double p_ot, double tau_me, double vdiff) {
+  using T = typename Flt<P>::T;
+  T tm = (T)tau_me;
+  T a = sqrt((T)kGamma * (T)p_me * tm) / tm;
+  T mx = (T)p_ot - (T)p_me;
+  T b = sqrt((mx > (T)0 ? mx : (T)0) / tm);
+  T c = -(T)vdiff / tm;
+  T r = a;
+  if (b > r) r = b;
+  if (c > r) r = c;
+  return (double)r;
+}
+template <int P>
+__device__ inline double lam_wall(double p_me, double tau_me) {
+  using T = typename Flt<P>::T;
+  T tm = (T)tau_me;
+  return (double)(sqrt((T)kGamma * (T)p_me * tm) / tm);
+}
+
+template <int P>
+__global__ void k_lag_node(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc, int with_vol) {
+  if (sc && sc->done) return;
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  double M00 = 0, M01 = 0, M02 = 0, M10 = 0, M11 = 0, M12 = 0, M20 = 0, M21 = 0, M22 = 0;
+  double R0 = 0, R1 = 0, R2 = 0, B0 = 0, B1 = 0, B2 = 0;
+  const int p0 = m.vsf_off[v], p1 = m.vsf_off[v + 1];
+  for (int p = p0; p < p1; ++p) {
+    int sf = m.vsf_identity ? p : m.vsf[p];
+    int f = m.sf_face[sf];
+    int2 lr = m.flr[f];
+    double4 fn = m.fn[f];
+    double n0 = fn.x, n1 = fn.y, n2 = fn.z;
+    double area = m.sfn[sf].w;
+    U5 ul = ld_u(sol6, lr.x);
+    double pl = lag_pressure(ul.t, ul.u, ul.v, ul.w, ul.e);
+    double vl = dot3(ul.u, ul.v, ul.w, n0, n1, n2);
+    double w;
+    if (lr.y >= 0) {
+      U5 ur = ld_u(sol6, lr.y);
+      double pr = lag_pressure(ur.t, ur.u, ur.v, ur.w, ur.e);
+      double vr = dot3(ur.u, ur.v, ur.w, n0, n1, n2);
+      double l1 = lam_side<P>(pl, pr, ul.t, vr - vl);
+      double l2 = lam_side<P>(pr, pl, ur.t, vr - vl);
+      double v_bar = (l1 * vl + l2 * vr - (pr - pl)) / (l2 + l1);
+      w = area * (l1 + l2);
+      R0 = R0 + w * n0 * v_bar;
+      R1 = R1 + w * n1 * v_bar;
+      R2 = R2 + w * n2 * v_bar;
+    } else if (m.b2d && fabs(n2) > 1e-8) {
+      double l1 = lam_wall<P>(pl, ul.t);
+      w = area * 2 * l1;
+    } else {
+      double l1 = lam_wall<P>(pl, ul.t);
+      B0 = B0 + area * n0;
+      B1 = B1 + area * n1;
+      B2 = B2 + area * n2;
+      w = area * l1;
+      double q = area * (pl + l1 * vl);
+      R0 = R0 + q * n0;
+      R1 = R1 + q * n1;
+      R2 = R2 + q * n2;
+    }
+    M00 = M00 + w * (n0 * n0); M01 = M01 + w * (n0 * n1); M02 = M02 + w * (n0 * n2);
+    M10 = M10 + w * (n1 * n0); M11 = M11 + w * (n1 * n1); M12 = M12 + w * (n1 * n2);
+    M20 = M20 + w * (n2 * n0); M21 = M21 + w * (n2 * n1); M22 = M22 + w * (n2 * n2);
+  }
+  // inverse_3_by_3 (linear_solver_module.F90:134-172): adjugate of the transpose
+  double A00 = M11 * M22 - M12 * M21;
+  double A01 = -(M01 * M22 - M02 * M21);
+  double A02 = M01 * M12 - M02 * M11;
+  double A10 = -(M10 * M22 - M20 * M12);
+  double A11 = M00 * M22 - M20 * M02;
+  double A12 = -(M00 * M12 - M10 * M02);
+  double A20 = M10 * M21 - M20 * M11;
+  double A21 = -(M00 * M21 - M20 * M01);
+  double A22 = M00 * M11 - M10 * M01;
+  double det = M00 * A00 + M01 * A10 + M02 * A20;
+  double id = 1.0 / det;
+  double I00 = id * A00, I01 = id * A01, I02 = id * A02;
+  double I10 = id * A10, I11 = id * A11, I12 = id * A12;
+  double I20 = id * A20, I21 = id * A21, I22 = id * A22;
+  double b0 = R0, b1 = R1, b2 = R2;
+  double bmax = fmax(fmax(fabs(B0), fabs(B1)), fabs(B2));
+  if (bmax > 1e-8) {
+    double mb0 = 0.0 + I00 * B0 + I01 * B1 + I02 * B2;
+    double mb1 = 0.0 + I10 * B0 + I11 * B1 + I12 * B2;
+    double mb2 = 0.0 + I20 * B0 + I21 * B1 + I22 * B2;
+    double Pp = dot3(R0, R1, R2, mb0, mb1, mb2) / dot3(B0, B1, B2, mb0, mb1, mb2);
+    b0 = R0 - Pp * B0;
+    b1 = R1 - Pp * B1;
+    b2 = R2 - Pp * B2;
+  }
+  double v0 = 0.0 + I00 * b0 + I01 * b1 + I02 * b2;
+  double v1 = 0.0 + I10 * b0 + I11 * b1 + I12 * b2;
+  double v2 = 0.0 + I20 * b0 + I21 * b1 + I22 * b2;
+  m.vp[v] = make_double4(v0, v1, v2, 0.0);
+  if (with_vol) {  // compute_vert_volume of the current geometry (mesh_geometry_module.F90:273-288)
+    double s = 0.0;
+    for (int q = m.vse_off[v]; q < m.vse_off[v + 1]; ++q) s = s + m.vol_se[m.vse[q]];
+    m.vol_v[v] = s;
+  }
+}
+
+__device__ inline double warp_min(double x) {
+  for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+
+// mode bit 1: rhs, bit 2: CFL terms
+template <int P>
+__global__ void k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* __restrict__ rhs6,
+                           LagScalars* sc, double* dt_slot, int mode) {
+  using T = typename Flt<P>::T;
+  if (sc && sc->done) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double dtloc = 1e6;
+  if (c < m.ne) {
+    U5 me = ld_u(sol6, c);
+    double mass = ld_mass(sol6, c);
+    double pme = lag_pressure(me.t, me.u, me.v, me.w, me.e);
+    double csnd = sqrt(kGamma * pme * me.t);
+    double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
+    bool bad = false;
+    for (int q = m.csf_off[c]; q < m.csf_off[c + 1]; ++q) {
+      int e = m.csf[q];
+      int p = e >> 1, side = e & 1;
+      int sf = m.vsf_identity ? p : m.vsf[p];
+      int f = m.sf_face[sf];
+      int2 lr = m.flr[f];
+      double4 fn = m.fn[f];
+      double area = m.sfn[sf].w;
+      int sv = m.sf_vert[sf];
+      int node = m.vsf_identity ? sv : m.p_node[p];
+      if (mode & 1) {
+        double4 vpn = m.vp[node];
+        double v_et = dot3(vpn.x, vpn.y, vpn.z, fn.x, fn.y, fn.z);
+        double vme = dot3(me.u, me.v, me.w, fn.x, fn.y, fn.z);
+        double am = area / mass;
+        if (side == 0) {  // this cell is the face's left neighbour
+          double lam;
+          if (lr.y >= 0) {
+            U5 ot = ld_u(sol6, lr.y);
+            double pot = lag_pressure(ot.t, ot.u, ot.v, ot.w, ot.e);
+            double vot = dot3(ot.u, ot.v, ot.w, fn.x, fn.y, fn.z);
+            lam = lam_side<P>(pme, pot, me.t, vot - vme);
+          } else {
+            lam = lam_wall<P>(pme, me.t);
+          }
+          if (P == 0) {
+            double ps = pme - lam * (v_et - vme);
+            r0 = r0 - am * (-v_et);
+            r1 = r1 - am * (ps * fn.x);
+            r2 = r2 - am * (ps * fn.y);
+            r3 = r3 - am * (ps * fn.z);
+            r4 = r4 - am * (ps * v_et);
+          } else {
+            T ps = (T)pme - (T)lam * ((T)v_et - (T)vme);
+            r0 = r0 - am * (double)(-(T)v_et);
+            r1 = r1 - am * (double)(ps * (T)fn.x);
+            r2 = r2 - am * (double)(ps * (T)fn.y);
+            r3 = r3 - am * (double)(ps * (T)fn.z);
+            r4 = r4 - am * (double)(ps * (T)v_et);
+          }
+        } else {  // right neighbour
+          U5 ot = ld_u(sol6, lr.x);
+          double pot = lag_pressure(ot.t, ot.u, ot.v, ot.w, ot.e);
+          double vot = dot3(ot.u, ot.v, ot.w, fn.x, fn.y, fn.z);
+          double lam = lam_side<P>(pme, pot, me.t, vme - vot);
+          if (P == 0) {
+            double ps = pme + lam * (v_et - vme);
+            r0 = r0 + am * (-v_et);
+            r1 = r1 + am * (ps * fn.x);
+            r2 = r2 + am * (ps * fn.y);
+            r3 = r3 + am * (ps * fn.z);
+            r4 = r4 + am * (ps * v_et);
+          } else {
+            T ps = (T)pme + (T)lam * ((T)v_et - (T)vme);
+            r0 = r0 + am * (double)(-(T)v_et);
+            r1 = r1 + am * (double)(ps * (T)fn.x);
+            r2 = r2 + am * (double)(ps * (T)fn.y);
+            r3 = r3 + am * (double)(ps * (T)fn.z);
+            r4 = r4 + am * (double)(ps * (T)v_et);
+          }
+        }
+      }
+      if (mode & 2) {  // compute_dt terms for (cell, subface)
+        double sg = side == 0 ? 1.0 : -1.0;
+        double4 vps = m.vp[sv];
+        int2 se = m.sf_se[sf];
+        int sub = side == 0 ? se.x : se.y;
+        double t1 = m.vol_se[c] / (area * csnd);  // sub_elem(i) with i the cell (reference quirk)
+        double vn = dot3(vps.x, vps.y, vps.z, sg * fn.x, sg * fn.y, sg * fn.z);
+        double t2 = 0.8 * m.vol_se[sub] / (1e-8 + fabs(vn) * fn.w);
+        if (t1 < dtloc) dtloc = t1;
+        if (t2 < dtloc) dtloc = t2;
+        bad = bad || !(t1 >= 0.0) || !(t2 >= 0.0);
+      }
+    }
+    if (mode & 1) {
+      double2* r = reinterpret_cast<double2*>(rhs6 + 6 * (size_t)c);
+      r[0] = make_double2(r0, r1);
+      r[1] = make_double2(r2, r3);
+      r[2] = make_double2(r4, 0.0);
+    }
+    if (bad) atomicOr(m.status, kErrNonFinite);
+  }
+  if (mode & 2) {
+    __shared__ double wmin[32];
+    double x = warp_min(dtloc);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) wmin[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+      int nw = (blockDim.x + 31) >> 5;
+      x = lane < nw ? wmin[lane] : 1e6;
+      x = warp_min(x);
+      if (lane == 0) atomic_min_pos(dt_slot, x);
+    }
+  }
+}
+
+// dt = cfl*dt; if (t + dt > t_max) dt = t_max - t; t = t + dt (lagrange_main.F90:102-116)
+__global__ void k_lag_finalize(LagScalars* sc) {
+  if (sc->done) {
+    sc->skip = 1;
+    return;
+  }
+  double dt = sc->cfl * sc->dtmin;
+  if (sc->t + dt > sc->t_max) dt = sc->t_max - sc->t;
+  sc->dt = dt;
+  sc->t = sc->t + dt;
+  sc->steps += 1;
+  sc->dtmin = 1e6;  // compute_dt starts from dt = 1e6
+  sc->done = (sc->t < sc->t_max) ? 0 : 1;
+  sc->skip = 0;
+}
+
+__global__ void k_lag_move(DevMesh m, const LagScalars* sc, double dt_host) {
+  if (sc && sc->skip) return;
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  double dt = sc ? sc->dt : dt_host;
+  double4 x = m.x[v], vp = m.vp[v];
+  m.x[v] = make_double4(x.x + dt * vp.x, x.y + dt * vp.y, x.z + dt * vp.z, 0.0);
+}
+
+// (5, n) host layout <-> [n][6] device records; mass goes to slot 5
+__global__ void k_pack6(int n, const double* __restrict__ s5, const double* __restrict__ mass, double* __restrict__ s6) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (int k = 0; k < 5; ++k) s6[6 * (size_t)c + k] = s5[5 * (size_t)c + k];
+  if (mass) s6[6 * (size_t)c + 5] = mass[c];
+}
+__global__ void k_unpack6(int n, const double* __restrict__ s6, double* __restrict__ s5) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (int k = 0; k < 5; ++k) s5[5 * (size_t)c + k] = s6[6 * (size_t)c + k];
+}
+__global__ void k_vp_out(int n, const double4* __restrict__ vp, double* __restrict__ out) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  double4 a = vp[v];
+  out[3 * (size_t)v] = a.x;
+  out[3 * (size_t)v + 1] = a.y;
+  out[3 * (size_t)v + 2] = a.z;
+}
+__global__ void k_vp_in(int n, const double* __restrict__ in, double4* __restrict__ vp) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= n) return;
+  vp[v] = make_double4(in[3 * (size_t)v], in[3 * (size_t)v + 1], in[3 * (size_t)v + 2], 0.0);
+}
+__global__ void k_set_scalar(double* p, double v) { *p = v; }
+
+}  // namespace
+
+constexpr int kBlkNode = 128, kBlkCell = 128, kBlkVert = 256;
+
+void launch_lag_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision, int with_vol) {
+  if (precision == 1)
+    k_lag_node<1><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc, with_vol);
+  else
+    k_lag_node<0><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc, with_vol);
+}
+void launch_lag_cell(const DevMesh& m, const double* sol6, double* rhs6, LagScalars* sc, double* dt_slot,
+                     int precision, int mode) {
+  if (precision == 1)
+    k_lag_cell<1><<<grid_for(m.ne, kBlkCell), kBlkCell, 0, m.stream>>>(m, sol6, rhs6, sc, dt_slot, mode);
+  else
+    k_lag_cell<0><<<grid_for(m.ne, kBlkCell), kBlkCell, 0, m.stream>>>(m, sol6, rhs6, sc, dt_slot, mode);
+}
+void launch_lag_finalize(const DevMesh& m, LagScalars* sc) { k_lag_finalize<<<1, 1, 0, m.stream>>>(sc); }
+void launch_lag_move(const DevMesh& m, const LagScalars* sc, double dt_host) {
+  k_lag_move<<<grid_for(m.nv, kBlkVert), kBlkVert, 0, m.stream>>>(m, sc, dt_host);
+}
+void launch_pack6(const DevMesh& m, int n, const double* s5, const double* mass, double* s6) {
+  k_pack6<<<grid_for(n, 256), 256, 0, m.stream>>>(n, s5, mass, s6);
+}
+void launch_unpack6(const DevMesh& m, int n, const double* s6, double* s5) {
+  k_unpack6<<<grid_for(n, 256), 256, 0, m.stream>>>(n, s6, s5);
+}
+void launch_vp_out(const DevMesh& m, double* out) { k_vp_out<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m.nv, m.vp, out); }
+void launch_vp_in(const DevMesh& m, const double* in) { k_vp_in<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m.nv, in, m.vp); }
+void launch_set_scalar(const DevMesh& m, double* p, double v) { k_set_scalar<<<1, 1, 0, m.stream>>>(p, v); }
+
+// One full time step of lagrange_main.F90:89-127 (graph-capturable: no host sync).
+void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision) {
+  launch_lag_node(m, sol6, sc, precision, 1);
+  launch_lag_cell(m, sol6, rhs6, sc, &sc->dtmin, precision, 3);
+  launch_lag_finalize(m, sc);
+  launch_lag_move(m, sc, 0.0);
+  launch_face_geometry(m, sc);
+  launch_cell_geometry(m, sol6, rhs6, sc);
+}
+
+}  // namespace subfv

@@ -1,0 +1,21 @@
+// Launchers of the Lagrangian step kernels (lagrange.cu).
+#pragma once
+#include "common.cuh"
+#include "mesh_dev.cuh"
+
+namespace subfv {
+
+void launch_lag_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision, int with_vol);
+// mode bit 1: rhs into rhs6; bit 2: CFL terms min-reduced into *dt_slot
+void launch_lag_cell(const DevMesh& m, const double* sol6, double* rhs6, LagScalars* sc, double* dt_slot,
+                     int precision, int mode);
+void launch_lag_finalize(const DevMesh& m, LagScalars* sc);
+void launch_lag_move(const DevMesh& m, const LagScalars* sc, double dt_host);
+void launch_pack6(const DevMesh& m, int n, const double* s5, const double* mass, double* s6);
+void launch_unpack6(const DevMesh& m, int n, const double* s6, double* s5);
+void launch_vp_out(const DevMesh& m, double* out);
+void launch_vp_in(const DevMesh& m, const double* in);
+void launch_set_scalar(const DevMesh& m, double* p, double v);
+void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision);
+
+}  // namespace subfv

@@ -1,0 +1,402 @@
+// Device mesh upload and the geometry kernels of compute_geometry_mesh
+// (src/mesh/mesh_geometry_module.F90:16-57). One thread per face / cell / vertex;
+// each recomputes what it needs from the vertex coordinates in the reference's order.
+#include <algorithm>
+#include <vector>
+
+#include "../../include/subfv.h"
+#include "common.cuh"
+#include "mesh_dev.cuh"
+
+namespace subfv {
+
+namespace {
+
+template <class T>
+int upload(T** dst, const std::vector<T>& h, size_t* bytes, cudaStream_t s) {
+  size_t n = std::max<size_t>(h.size(), 1);
+  SUBFV_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
+  *bytes += n * sizeof(T);
+  if (!h.empty()) SUBFV_CUDA(cudaMemcpyAsync(*dst, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return 0;
+}
+template <class T>
+int alloc(T** dst, size_t n, size_t* bytes) {
+  n = std::max<size_t>(n, 1);
+  SUBFV_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
+  SUBFV_CUDA(cudaMemset(*dst, 0, n * sizeof(T)));
+  *bytes += n * sizeof(T);
+  return 0;
+}
+
+}  // namespace
+
+int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
+  const int nv = d->n_vert, ne = d->n_elems, nf = d->n_faces, nsf = d->n_sub_faces, nse = d->n_sub_elems;
+  if (nv <= 0 || ne <= 0 || nf <= 0 || nsf <= 0 || nse <= 0) {
+    set_error("subfv_mesh_create: empty mesh");
+    return -2;
+  }
+  m->nv = nv;
+  m->ne = ne;
+  m->nf = nf;
+  m->nsf = nsf;
+  m->nse = nse;
+  m->b2d = d->b2d;
+  SUBFV_CUDA(cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking));
+  cudaStream_t s = m->stream;
+  size_t* B = &m->bytes;
+
+  std::vector<double4> x(nv);
+  for (int i = 0; i < nv; ++i) x[i] = make_double4(d->vert_coord[3 * i], d->vert_coord[3 * i + 1], d->vert_coord[3 * i + 2], 0.0);
+  std::vector<int8_t> isb(nv);
+  for (int i = 0; i < nv; ++i) isb[i] = d->vert_is_bound ? (int8_t)(d->vert_is_bound[i] != 0) : 0;
+
+  std::vector<int4> fvert(nf), fsf(nf);
+  std::vector<int2> flr(nf);
+  for (int f = 0; f < nf; ++f) {
+    int b = d->face_vert_off[f], n = d->face_vert_off[f + 1] - b;
+    if (n < 3 || n > 4) {
+      set_error("subfv_mesh_create: faces must have 3 or 4 vertices");
+      return -2;
+    }
+    int v[4] = {-1, -1, -1, -1}, sfi[4] = {-1, -1, -1, -1};
+    for (int k = 0; k < n; ++k) {
+      v[k] = d->face_vert[b + k] - 1;
+      sfi[k] = d->face_sub_face[b + k] - 1;
+    }
+    fvert[f] = make_int4(v[0], v[1], v[2], v[3]);
+    fsf[f] = make_int4(sfi[0], sfi[1], sfi[2], sfi[3]);
+    int r = d->face_right[f];
+    flr[f] = make_int2(d->face_left[f] - 1, r > 0 ? r - 1 : r - 1);  // wall 0 -> -1, -tag -> -tag-1
+  }
+  std::vector<int> sf_face(nsf), sf_vert(nsf), sf_loc(nsf);
+  std::vector<int2> sf_se(nsf);
+  for (int i = 0; i < nsf; ++i) {
+    sf_face[i] = d->sub_face_face[i] - 1;
+    sf_vert[i] = d->sub_face_vert[i] - 1;
+    sf_se[i] = make_int2(d->sub_face_left_sub_elem[i] - 1, d->sub_face_right_sub_elem[i] - 1);
+    sf_loc[i] = d->sub_face_loc ? d->sub_face_loc[i] - 1 : 0;
+  }
+  std::vector<int> se_elem(nse), se_vert(nse), se_loc(nse);
+  std::vector<int4> se_sf(nse);
+  for (int i = 0; i < nse; ++i) {
+    se_elem[i] = d->sub_elem_elem[i] - 1;
+    se_vert[i] = d->sub_elem_vert[i] - 1;
+    se_loc[i] = d->sub_elem_loc ? d->sub_elem_loc[i] - 1 : 0;
+    int b = d->sub_elem_sub_face_off[i], n = d->sub_elem_sub_face_off[i + 1] - b;
+    if (n > 4) {
+      set_error("subfv_mesh_create: a subcell with more than four subfaces");
+      return -2;
+    }
+    int q[4] = {-1, -1, -1, -1};
+    for (int k = 0; k < n; ++k) q[k] = d->sub_elem_sub_face[b + k] - 1;
+    se_sf[i] = make_int4(q[0], q[1], q[2], q[3]);
+  }
+  std::vector<int> ev_off(ne + 1), ev(d->elem_vert_off[ne]), ef8(8 * (size_t)ne, -1), ekind(ne);
+  for (int c = 0; c <= ne; ++c) ev_off[c] = d->elem_vert_off[c];
+  for (int c = 0; c < ne; ++c) {
+    ekind[c] = d->elem_kind ? d->elem_kind[c] : 0;
+    for (int k = ev_off[c]; k < ev_off[c + 1]; ++k) {
+      ev[k] = d->elem_vert[k] - 1;
+      if (d->elem_sub_elem[k] - 1 != k) {
+        set_error("subfv_mesh_create: elem%sub_elem must number subcells cell by cell in vertex order");
+        return -2;
+      }
+    }
+    int b = d->elem_face_off[c], n = d->elem_face_off[c + 1] - b;
+    if (n > 8) {
+      set_error("subfv_mesh_create: a cell with more than eight faces");
+      return -2;
+    }
+    for (int k = 0; k < n; ++k) ef8[8 * (size_t)c + k] = d->elem_face[b + k] - 1;
+  }
+  const int nvsf = d->vert_sub_face_off[nv];
+  std::vector<int> vsf_off(nv + 1), vsf(nvsf), vse_off(nv + 1), vse(d->vert_sub_elem_off[nv]);
+  std::vector<int> p_node(nvsf);
+  bool ident = true;
+  int max_vsf = 0;
+  for (int v = 0; v <= nv; ++v) {
+    vsf_off[v] = d->vert_sub_face_off[v];
+    vse_off[v] = d->vert_sub_elem_off[v];
+  }
+  for (int v = 0; v < nv; ++v) {
+    max_vsf = std::max(max_vsf, vsf_off[v + 1] - vsf_off[v]);
+    for (int p = vsf_off[v]; p < vsf_off[v + 1]; ++p) {
+      vsf[p] = d->vert_sub_face[p] - 1;
+      p_node[p] = v;
+      if (vsf[p] != p) ident = false;
+    }
+  }
+  for (size_t k = 0; k < vse.size(); ++k) vse[k] = d->vert_sub_elem[k] - 1;
+  m->nvsf = nvsf;
+  m->vsf_identity = ident ? 1 : 0;
+  m->max_vsf = max_vsf;
+  // cell CSR over node-ordered subface positions (ascending p = the reference's scatter order)
+  std::vector<int> csf_off(ne + 1, 0);
+  for (int p = 0; p < nvsf; ++p) {
+    int f = sf_face[vsf[p]];
+    csf_off[flr[f].x + 1]++;
+    if (flr[f].y >= 0) csf_off[flr[f].y + 1]++;
+  }
+  for (int c = 0; c < ne; ++c) csf_off[c + 1] += csf_off[c];
+  std::vector<int> csf(csf_off[ne]);
+  {
+    std::vector<int> fill(csf_off.begin(), csf_off.end() - 1);
+    for (int p = 0; p < nvsf; ++p) {
+      int f = sf_face[vsf[p]];
+      csf[fill[flr[f].x]++] = 2 * p;
+      if (flr[f].y >= 0) csf[fill[flr[f].y]++] = 2 * p + 1;
+    }
+  }
+  m->ncsf = csf_off[ne];
+
+  if (upload(&m->x, x, B, s) || alloc(&m->vp, nv, B) || alloc(&m->vol_v, nv, B) || upload(&m->is_bound, isb, B, s) ||
+      upload(&m->fvert, fvert, B, s) || upload(&m->flr, flr, B, s) || upload(&m->fsf, fsf, B, s) ||
+      alloc(&m->fc, nf, B) || alloc(&m->fn, nf, B) || upload(&m->sf_face, sf_face, B, s) ||
+      upload(&m->sf_vert, sf_vert, B, s) || upload(&m->sf_se, sf_se, B, s) || upload(&m->sf_loc, sf_loc, B, s) ||
+      alloc(&m->sfn, nsf, B) || upload(&m->se_elem, se_elem, B, s) || upload(&m->se_vert, se_vert, B, s) ||
+      upload(&m->se_loc, se_loc, B, s) || upload(&m->se_sf, se_sf, B, s) || alloc(&m->vol_se, nse, B) ||
+      upload(&m->ev_off, ev_off, B, s) || upload(&m->ev, ev, B, s) || upload(&m->ef8, ef8, B, s) ||
+      upload(&m->ekind, ekind, B, s) || alloc(&m->cc, ne, B) || alloc(&m->vol, ne, B) ||
+      upload(&m->vsf_off, vsf_off, B, s) || upload(&m->vsf, vsf, B, s) || upload(&m->p_node, p_node, B, s) ||
+      upload(&m->vse_off, vse_off, B, s) || upload(&m->vse, vse, B, s) || upload(&m->csf_off, csf_off, B, s) ||
+      upload(&m->csf, csf, B, s) || alloc(&m->status, 4, B))
+    return -1;
+  SUBFV_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+void devmesh_free(DevMesh* m) {
+  void* ptrs[] = {m->x, m->vp, m->vol_v, m->is_bound, m->fvert, m->flr, m->fsf, m->fc, m->fn,
+                  m->sf_face, m->sf_vert, m->sf_se, m->sf_loc, m->sfn, m->se_elem, m->se_vert, m->se_loc,
+                  m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
+                  m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  if (m->stream) cudaStreamDestroy(m->stream);
+  *m = DevMesh();
+}
+
+// ---------------------------------------------------------------------------------
+// Geometry kernels
+
+namespace {
+
+struct V3 {
+  double x, y, z;
+};
+__device__ inline V3 ld3(const double4* a, int i) {
+  double4 v = a[i];
+  return {v.x, v.y, v.z};
+}
+__device__ inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ inline V3 cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ inline double dot(V3 a, V3 b) { return dot3(a.x, a.y, a.z, b.x, b.y, b.z); }
+__device__ inline V3 half_sum(V3 a, V3 b) { return {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)}; }
+
+// compute_face_centroid + compute_subface_norm + compute_face_norm (:177-271)
+__global__ void k_face_geometry(DevMesh m, const LagScalars* sc) {
+  if (sc && sc->skip) return;
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  int4 fv = m.fvert[f];
+  int vid[4] = {fv.x, fv.y, fv.z, fv.w};
+  int n = fv.w < 0 ? 3 : 4;
+  V3 P[4];
+  for (int k = 0; k < n; ++k) P[k] = ld3(m.x, vid[k]);
+  V3 cg = {0.0, 0.0, 0.0};
+  for (int k = 0; k < n; ++k) cg = {cg.x + P[k].x, cg.y + P[k].y, cg.z + P[k].z};
+  cg = {cg.x / n, cg.y / n, cg.z / n};
+  V3 c = {0.0, 0.0, 0.0};
+  double sum_area = 0.0;
+  for (int j = 0; j < n; ++j) {
+    int jp = (j + 1) % n;
+    V3 x = cross(sub(P[j], cg), sub(P[jp], cg));
+    double area = 0.5 * fnorm2_3(x.x, x.y, x.z);
+    c.x = c.x + area * (P[j].x + P[jp].x + cg.x) / 3.0;
+    c.y = c.y + area * (P[j].y + P[jp].y + cg.y) / 3.0;
+    c.z = c.z + area * (P[j].z + P[jp].z + cg.z) / 3.0;
+    sum_area = sum_area + area;
+  }
+  c = {c.x / sum_area, c.y / sum_area, c.z / sum_area};
+  m.fc[f] = make_double4(c.x, c.y, c.z, 0.0);
+  int4 fs = m.fsf[f];
+  int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
+  V3 fnrm = {0.0, 0.0, 0.0};
+  for (int k = 0; k < n; ++k) {
+    int sf = sfi[k];
+    int vert = m.sf_vert[sf];
+    int j = 0;
+    while (j < n - 1 && vid[j] != vert) ++j;
+    int jp = (j + 1) % n, jm = (j - 1 + n) % n;
+    V3 cp = P[j];
+    V3 cpm = half_sum(P[jm], cp), cpp = half_sum(P[jp], cp);
+    V3 a = cross(sub(cpm, c), sub(cp, c));
+    V3 b = cross(sub(cp, c), sub(cpp, c));
+    V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
+    double area = fnorm2_3(nr.x, nr.y, nr.z);
+    m.sfn[sf] = make_double4(nr.x / area, nr.y / area, nr.z / area, area);
+    fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
+  }
+  double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
+  m.fn[f] = make_double4(fnrm.x / fa, fnrm.y / fa, fnrm.z / fa, fa);
+}
+
+// compute_elem_centroid, compute_subelem_volume, compute_elem_volume, check_mesh
+// (:59-175, :290-396), optionally fused with the explicit update sol += dt*rhs.
+__global__ void k_cell_geometry(DevMesh m, double* sol6, const double* rhs6, const LagScalars* sc) {
+  if (sc && sc->skip) return;
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
+  V3 ce = {0.0, 0.0, 0.0};
+  for (int k = 0; k < nvc; ++k) {
+    V3 p = ld3(m.x, m.ev[vb + k]);
+    ce = {ce.x + p.x, ce.y + p.y, ce.z + p.z};
+  }
+  ce = {ce.x / nvc, ce.y / nvc, ce.z / nvc};
+  int faces[8];
+  int nfc = 0;
+  for (int k = 0; k < 8; ++k) {
+    int f = m.ef8[8 * c + k];
+    if (f < 0) break;
+    faces[nfc++] = f;
+  }
+  V3 cen = {0.0, 0.0, 0.0};
+  double sum_vol = 0.0;
+  for (int j = 0; j < nfc; ++j) {
+    int f = faces[j];
+    int4 fv = m.fvert[f];
+    int vid[4] = {fv.x, fv.y, fv.z, fv.w};
+    int n = fv.w < 0 ? 3 : 4;
+    bool left = m.flr[f].x == c;
+    V3 cf = ld3(m.fc, f);
+    V3 fe = sub(cf, ce);
+    for (int k = 0; k < n; ++k) {
+      V3 cp = ld3(m.x, vid[k]), cpp = ld3(m.x, vid[(k + 1) % n]);
+      V3 x = left ? cross(sub(cp, cf), sub(cpp, cf)) : cross(sub(cpp, cf), sub(cp, cf));
+      double vol = dot(x, fe) / 6.0;
+      cen.x = cen.x + vol * (cp.x + cpp.x + cf.x + ce.x) / 4.0;
+      cen.y = cen.y + vol * (cp.y + cpp.y + cf.y + ce.y) / 4.0;
+      cen.z = cen.z + vol * (cp.z + cpp.z + cf.z + ce.z) / 4.0;
+      sum_vol = sum_vol + vol;
+    }
+  }
+  cen = {cen.x / sum_vol, cen.y / sum_vol, cen.z / sum_vol};
+  m.cc[c] = make_double4(cen.x, cen.y, cen.z, 0.0);
+  bool ok = true;
+  double vcell = 0.0;
+  for (int s = vb; s < vb + nvc; ++s) {
+    int4 q4 = m.se_sf[s];
+    int q[4] = {q4.x, q4.y, q4.z, q4.w};
+    double vol = 0.0;
+    for (int j = 0; j < 4 && q[j] >= 0; ++j) {
+      int sf = q[j];
+      int f = m.sf_face[sf], vert = m.sf_vert[sf];
+      int4 fv = m.fvert[f];
+      int vid[4] = {fv.x, fv.y, fv.z, fv.w};
+      int n = fv.w < 0 ? 3 : 4;
+      int k = 0;
+      while (k < n - 1 && vid[k] != vert) ++k;
+      V3 cp = ld3(m.x, vid[k]);
+      V3 cpm = half_sum(ld3(m.x, vid[(k - 1 + n) % n]), cp);
+      V3 cpp = half_sum(ld3(m.x, vid[(k + 1) % n]), cp);
+      V3 cf = ld3(m.fc, f);
+      V3 fe = sub(cf, cen);
+      V3 a = sub(cpm, cf), b = sub(cp, cf), cc3 = sub(cpp, cf);
+      V3 x1, x2;
+      if (m.flr[f].x == c) {
+        x1 = cross(a, b);
+        x2 = cross(b, cc3);
+      } else {
+        x1 = cross(cc3, b);
+        x2 = cross(b, a);
+      }
+      vol = vol + dot(x1, fe) / 6.0 + dot(x2, fe) / 6.0;
+    }
+    m.vol_se[s] = vol;
+    ok = ok && (vol > 0.0);
+    vcell = vcell + vol;
+  }
+  m.vol[c] = vcell;
+  // check_mesh_elem_volume / _closed / _subface_closed
+  double vdiv = 0.0;
+  V3 nt = {0.0, 0.0, 0.0}, ns = {0.0, 0.0, 0.0};
+  for (int j = 0; j < nfc; ++j) {
+    int f = faces[j];
+    double4 fn = m.fn[f];
+    double sg = m.flr[f].x == c ? 1.0 : -1.0;
+    V3 nn = {sg * fn.x, sg * fn.y, sg * fn.z};
+    V3 an = {fn.w * nn.x, fn.w * nn.y, fn.w * nn.z};
+    vdiv = vdiv + dot(ld3(m.fc, f), an);
+    nt = {nt.x + an.x, nt.y + an.y, nt.z + an.z};
+  }
+  vdiv = vdiv / 3.0;
+  for (int j = 0; j < nfc; ++j) {
+    int f = faces[j];
+    double sg = m.flr[f].x == c ? 1.0 : -1.0;
+    int4 fs = m.fsf[f];
+    int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
+    for (int k = 0; k < 4 && sfi[k] >= 0; ++k) {
+      double4 sn = m.sfn[sfi[k]];
+      ns = {ns.x + sn.w * (sg * sn.x), ns.y + sn.w * (sg * sn.y), ns.z + sn.w * (sg * sn.z)};
+    }
+  }
+  ok = ok && (fabs(vcell - vdiv) < 1e-14);
+  ok = ok && (fnorm2_3(nt.x, nt.y, nt.z) < 1e-14);
+  ok = ok && (fnorm2_3(ns.x, ns.y, ns.z) < 1e-14);
+  if (!ok) atomicOr(m.status, kErrMeshCheck);
+  if (sol6) {  // lagrange_main.F90:110: new_sol = sol + dt*rhs
+    double dt = sc->dt;
+    double* u = sol6 + 6 * (size_t)c;
+    const double* r = rhs6 + 6 * (size_t)c;
+    bool fin = true;
+    for (int k = 0; k < 5; ++k) {
+      u[k] = u[k] + dt * r[k];
+      fin = fin && isfinite(u[k]);
+    }
+    if (!fin) atomicOr(m.status, kErrNonFinite);
+    if (!(u[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
+  }
+}
+
+// compute_vert_volume (:273-288)
+__global__ void k_vert_volume(DevMesh m) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  double s = 0.0;
+  for (int q = m.vse_off[v]; q < m.vse_off[v + 1]; ++q) s = s + m.vol_se[m.vse[q]];
+  m.vol_v[v] = s;
+}
+
+// find_if_vert_is_bound (mesh_connectivity_module.F90:726-750) over the vertex's own
+// subfaces (one per face touching it)
+__global__ void k_vert_is_bound(DevMesh m) {
+  int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  int8_t b = 0;
+  for (int p = m.vsf_off[v]; p < m.vsf_off[v + 1]; ++p) {
+    int sf = m.vsf[p];
+    if (m.sf_vert[sf] != v) continue;
+    int f = m.sf_face[sf];
+    if (m.flr[f].y >= 0) continue;
+    if (!m.b2d || fabs(m.fn[f].z) < 1e-12) b = 1;
+  }
+  m.is_bound[v] = b;
+}
+
+}  // namespace
+
+void launch_face_geometry(const DevMesh& m, const LagScalars* sc) {
+  k_face_geometry<<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, sc);
+}
+void launch_cell_geometry(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc) {
+  k_cell_geometry<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, sol6, rhs6, sc);
+}
+void launch_vert_volume(const DevMesh& m) { k_vert_volume<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }
+void launch_vert_is_bound(const DevMesh& m) { k_vert_is_bound<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }
+
+}  // namespace subfv

@@ -1,0 +1,88 @@
+// Device-resident mesh: the reference's mesh_type (src/mesh/mesh_module.F90:17-89)
+// flattened into 0-based structure-of-arrays and fixed-width records so that
+// per-entity kernels load whole records with vector loads.
+//
+// Layout in HBM (all 0-based):
+//   vertices   x[nv] double4 (x, y, z, -), vp[nv] double4, vol_v[nv]
+//   faces      fvert[nf] int4 (vertex ids, -1 pad), flr[nf] int2 (left cell, right cell
+//              or -(tag+1) for a boundary), fsf[nf] int4 (subface ids in the face's order),
+//              fc[nf] double4 (centroid), fn[nf] double4 (unit normal, area)
+//   subfaces   sf_face, sf_vert [nsf] int, sf_se[nsf] int2 (left/right subcell, -1 none),
+//              sfn[nsf] double4 (unit normal, area)
+//   subcells   se_elem, se_vert [nse], se_sf[nse] int4 (subfaces, -1 pad), vol_se[nse]
+//   cells      ev_off[ne+1] (cell subcells are ev_off[c]..ev_off[c+1]-1, one per vertex),
+//              ev[], ef8[ne] (faces, -1 pad to 8), cc[ne] double4 (centroid), vol[ne]
+//   node CSR   vsf_off[nv+1], vsf[] (subface ids), vse_off[nv+1], vse[] (subcell ids)
+//   cell CSR   csf_off[ne+1], csf[] = 2*p + side over the node-ordered subface
+//              positions p that touch the cell, ascending (the order in which the
+//              reference's node loop scatters into that cell).
+#pragma once
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace subfv {
+
+struct DevMesh {
+  int nv = 0, ne = 0, nf = 0, nsf = 0, nse = 0, nvsf = 0, ncsf = 0;
+  int b2d = 1;
+  int vsf_identity = 0;  // vsf[p] == p for every p (no periodic extension)
+  int max_vsf = 0;
+  // vertices
+  double4* x = nullptr;
+  double4* vp = nullptr;
+  double* vol_v = nullptr;
+  int8_t* is_bound = nullptr;
+  // faces
+  int4* fvert = nullptr;
+  int2* flr = nullptr;
+  int4* fsf = nullptr;
+  double4* fc = nullptr;
+  double4* fn = nullptr;
+  // subfaces
+  int* sf_face = nullptr;
+  int* sf_vert = nullptr;
+  int2* sf_se = nullptr;
+  int* sf_loc = nullptr;
+  double4* sfn = nullptr;
+  // subcells
+  int* se_elem = nullptr;
+  int* se_vert = nullptr;
+  int* se_loc = nullptr;
+  int4* se_sf = nullptr;
+  double* vol_se = nullptr;
+  // cells
+  int* ev_off = nullptr;
+  int* ev = nullptr;
+  int* ef8 = nullptr;
+  int* ekind = nullptr;
+  double4* cc = nullptr;
+  double* vol = nullptr;
+  // node and cell CSR
+  int* vsf_off = nullptr;
+  int* vsf = nullptr;
+  int* p_node = nullptr;  // vertex owning node-ordered position p
+  int* vse_off = nullptr;
+  int* vse = nullptr;
+  int* csf_off = nullptr;
+  int* csf = nullptr;
+  // status word (StatusBits) and the stream the mesh's work runs on
+  unsigned* status = nullptr;
+  cudaStream_t stream = nullptr;
+  size_t bytes = 0;
+};
+
+int devmesh_create(const struct subfv_mesh_desc* d, DevMesh* m);
+void devmesh_free(DevMesh* m);
+
+// Geometry kernels (mesh_geometry_module.F90:16-57), launched on m.stream.
+// sc (optional): a step whose skip flag is set leaves everything untouched; with sol6
+// the cell kernel also applies sol += dt*rhs using sc->dt.
+void launch_face_geometry(const DevMesh& m, const LagScalars* sc = nullptr);
+void launch_cell_geometry(const DevMesh& m, double* sol6 = nullptr, const double* rhs6 = nullptr,
+                          const LagScalars* sc = nullptr);
+void launch_vert_volume(const DevMesh& m);
+void launch_vert_is_bound(const DevMesh& m);
+
+}  // namespace subfv

@@ -1,0 +1,172 @@
+"""Host mirror of the reference's lagrange_module (subfvlagrange, scheme "classic").
+
+Same names, argument meaning and error behaviour as
+src/lagrange/lagrange_module.F90: compute_rhs_lagrange (:14-147), compute_dt
+(:240-283), move_mesh (:772-784), init_sol (:285-427) and the time loop of
+src/lagrange/lagrange_main.F90:81-127. Arrays use the reference's layouts:
+sol and rhs are (5, n_elems) Fortran arrays, i.e. numpy (n_elems, 5); vp is (3, n_vert),
+i.e. numpy (n_vert, 3). The compute runs on the GPU through the C-ABI; there is no CPU
+path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, f64, pd
+from .mesh import Mesh, SUBFV_ERR_MESH_CHECK
+
+GAMMA = 7.0 / 5.0
+PLAIN_FP64, MIXED = 0, 1
+
+
+class MeshCheckError(RuntimeError):
+    """check_mesh failed: the reference prints "MESH GEOMETRY IS NOT OK" and stops."""
+
+
+def compute_rhs_lagrange(mesh: Mesh, sol, vp, dt, rhs, n_bc=0, bc_type=None, bc_val=None, b2d=True, mass=None):
+    """lagrange_module.F90:14-147. Fills vp (n_vert, 3) and rhs (n_elems, 5) in place."""
+    sol = f64(sol)
+    mass = f64(mass)
+    assert vp.dtype == np.float64 and vp.flags["C_CONTIGUOUS"] and vp.shape == (mesh.n_vert, 3)
+    assert rhs.dtype == np.float64 and rhs.flags["C_CONTIGUOUS"] and rhs.shape == (mesh.n_elems, 5)
+    return check(_lib.load().subfv_compute_rhs_lagrange(mesh._h, pd(sol), pd(vp), pd(rhs), int(b2d), pd(mass)),
+                 "subfv_compute_rhs_lagrange")
+
+
+def compute_dt(mesh: Mesh, sol, dt, cfl, vp, me=0, num_procs=1) -> float:
+    """lagrange_module.F90:240-283; returns the new dt (the reference's intent(inout))."""
+    sol, vp = f64(sol), f64(vp)
+    out = C.c_double()
+    check(_lib.load().subfv_compute_dt(mesh._h, pd(sol), float(cfl), pd(vp), C.byref(out)), "subfv_compute_dt")
+    return out.value
+
+
+def move_mesh(mesh: Mesh, vp, dt):
+    """lagrange_module.F90:772-784 (on the device copy of the vertex coordinates)."""
+    vp = f64(vp)
+    check(_lib.load().subfv_move_mesh(mesh._h, pd(vp), float(dt)), "subfv_move_mesh")
+
+
+def compute_geometry_mesh(mesh: Mesh):
+    st = mesh.compute_geometry_mesh()
+    if st & SUBFV_ERR_MESH_CHECK:
+        raise MeshCheckError("MESH GEOMETRY IS NOT OK")
+    return st
+
+
+def init_sol_sedov(mesh: Mesh, e_total=0.983909, r_sedov=0.06, mask=None) -> np.ndarray:
+    """init_sol with init = 1 (lagrange_module.F90:318-356): rho = 1, u = 0, the energy
+    e_total spread over the selected cells, 1e-8/(gamma-1) elsewhere. The reference
+    selects cells whose centroid lies within r_sedov of the z-axis; `mask` overrides the
+    selection (the benchmark deposits 0.244816 in the cells touching the origin)."""
+    vol = mesh.geometry("elem_volume")
+    if mask is None:
+        cc = mesh.geometry("elem_coord")
+        sel = np.sqrt(cc[:, 0] ** 2 + cc[:, 1] ** 2) < r_sedov
+    else:
+        sel = np.asarray(mask).astype(bool)
+    tot_vol = 0.0
+    for v in vol[sel]:  # sequential sum, as the reference's loop
+        tot_vol = tot_vol + float(v)
+    if tot_vol < 1e-10:
+        raise ValueError(f"[-] r_sedov too small, tot_vol_init: {tot_vol}")
+    sol = np.zeros((mesh.n_elems, 5))
+    sol[:, 0] = 1.0
+    sol[:, 4] = np.where(sel, e_total / tot_vol, 1e-8 / (GAMMA - 1.0))
+    return sol
+
+
+class LagrangeState:
+    """The device-resident time loop of lagrange_main.F90:89-127. The state (sol, mass,
+    coordinates, geometry) stays in HBM; `advance` replays graph-captured steps."""
+
+    def __init__(self, mesh: Mesh, sol, mass=None, cfl=0.8, t0=0.0, t_max=1.0, precision=PLAIN_FP64):
+        self.mesh = mesh
+        sol = f64(sol)
+        if mass is None:  # lagrange_main.F90:81-85: mass = volume / tau
+            mass = mesh.geometry("elem_volume") / sol[:, 0]
+        mass = f64(mass)
+        self.mass = mass
+        h = C.c_void_p()
+        check(_lib.load().subfv_lag_state_create(mesh._h, pd(sol), pd(mass), float(cfl), float(t0), float(t_max),
+                                                int(precision), C.byref(h)), "subfv_lag_state_create")
+        self._h = h
+
+    def advance(self, n_steps: int):
+        steps, t = C.c_int(), C.c_double()
+        st = check(_lib.load().subfv_lag_advance(self._h, int(n_steps), C.byref(steps), C.byref(t)),
+                   "subfv_lag_advance")
+        return st, steps.value, t.value
+
+    def advance_async(self, n_steps: int):
+        check(_lib.load().subfv_lag_advance_async(self._h, int(n_steps)), "subfv_lag_advance_async")
+
+    def sync(self):
+        steps, t = C.c_int(), C.c_double()
+        st = check(_lib.load().subfv_lag_sync(self._h, C.byref(steps), C.byref(t)), "subfv_lag_sync")
+        return st, steps.value, t.value
+
+    def run(self, max_steps: int = 10**9, chunk: int = 256):
+        """Steps until t >= t_max (or max_steps); raises on a mesh-check failure.
+        Returns (status bits, steps taken, t)."""
+        st, steps, t = self.sync()
+        start = steps
+        while steps - start < max_steps:
+            n = min(chunk, max_steps - (steps - start))
+            st, new_steps, t = self.advance(n)
+            if st & SUBFV_ERR_MESH_CHECK:
+                raise MeshCheckError("MESH GEOMETRY IS NOT OK")
+            if new_steps < steps + n:  # the loop reached t_max
+                steps = new_steps
+                break
+            steps = new_steps
+        return st, steps, t
+
+    def sol(self) -> np.ndarray:
+        out = np.empty((self.mesh.n_elems, 5))
+        check(_lib.load().subfv_lag_get_sol(self._h, pd(out)), "subfv_lag_get_sol")
+        return out
+
+    def set_sol(self, sol):
+        sol = f64(sol)
+        check(_lib.load().subfv_lag_set_sol(self._h, pd(sol)), "subfv_lag_set_sol")
+
+    def vp(self) -> np.ndarray:
+        out = np.empty((self.mesh.n_vert, 3))
+        check(_lib.load().subfv_lag_get_vp(self._h, pd(out)), "subfv_lag_get_vp")
+        return out
+
+    def last_dt(self) -> float:
+        out = C.c_double()
+        check(_lib.load().subfv_lag_last_dt(self._h, C.byref(out)), "subfv_lag_last_dt")
+        return out.value
+
+    def mesh_stream(self) -> int:
+        """cudaStream_t (as an int) every kernel of this state runs on."""
+        return int(_lib.load().subfv_mesh_stream(self.mesh._h))
+
+    def profile_steps(self, n: int):
+        """Per-kernel device milliseconds summed over n eager steps (node, cell,
+        finalize, move, face geometry, cell geometry)."""
+        out = np.zeros(6)
+        check(_lib.load().subfv_lag_profile_steps(self._h, int(n), pd(out)), "subfv_lag_profile_steps")
+        return out
+
+    def step_host(self, sol: np.ndarray) -> int:
+        """One step through host buffers (upload, step, download), in place."""
+        assert sol.dtype == np.float64 and sol.flags["C_CONTIGUOUS"]
+        return check(_lib.load().subfv_lag_step_host(self._h, pd(sol)), "subfv_lag_step_host")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().subfv_lag_state_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
