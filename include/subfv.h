@@ -106,6 +106,16 @@ int subfv_compute_rhs_lagrange(subfv_mesh* m, const double* sol, double* vp, dou
                                int b2d, const double* mass);
 /* compute_dt(mesh, sol, dt, cfl, vp, me, num_procs) — lagrange_module.F90:240-283 */
 int subfv_compute_dt(subfv_mesh* m, const double* sol, double cfl, const double* vp, double* dt);
+/* No counterpart in the reference. compute_dt for callers that cannot allocate device
+ * memory when they call (all device memory reserved at start-up, or an allocator owned
+ * by a host application): d_sol (5, n_elems), d_vp (3, n_vert) and d_dt (one double)
+ * are device buffers the caller owns; nothing is allocated or freed. Scratch is a
+ * static 128 KiB device array (one minimum per 256 cells), so meshes above 4,194,304
+ * cells are rejected (-4). The first call on a device looks up that array's device
+ * address: make it before any stream capture. Calls share the array: do not let two
+ * calls overlap on the GPU. Runs on the mesh's stream and returns after it finishes;
+ * the result equals subfv_compute_dt's. */
+int subfv_compute_dt_noalloc(subfv_mesh* m, const double* d_sol, const double* d_vp, double cfl, double* d_dt);
 /* move_mesh(mesh, vp, dt) — lagrange_module.F90:772-784 */
 int subfv_move_mesh(subfv_mesh* m, const double* vp, double dt);
 

@@ -41,6 +41,7 @@ SIGNATURES = {
     "subfv_compute_geometry_mesh": (c_int, [P]),
     "subfv_compute_rhs_lagrange": (c_int, [P, PD, PD, PD, c_int, PD]),
     "subfv_compute_dt": (c_int, [P, PD, c_dbl, PD, PD]),
+    "subfv_compute_dt_noalloc": (c_int, [P, P, P, c_dbl, P]),
     "subfv_move_mesh": (c_int, [P, PD, c_dbl]),
     "subfv_lag_state_create": (c_int, [P, PD, PD, c_dbl, c_dbl, c_dbl, c_int, C.POINTER(P)]),
     "subfv_lag_state_destroy": (c_int, [P]),

@@ -46,6 +46,10 @@ struct subfv_lag_state {
   int graph_steps = 0;
 };
 
+namespace subfv {
+const DevMesh& mesh_device_view(const subfv_mesh* m) { return m->d; }
+}  // namespace subfv
+
 namespace {
 
 int check_status(DevMesh& d) {
