@@ -66,7 +66,7 @@ int ensure_scratch(subfv_mesh* m) {
   if (m->stage) return 0;
   size_t n = std::max<size_t>(5 * (size_t)m->d.ne, 3 * (size_t)m->d.nv);
   SUBFV_CUDA(cudaMalloc(&m->stage, n * sizeof(double)));
-  SUBFV_CUDA(cudaMalloc(&m->sol6, 6 * (size_t)m->d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&m->sol6, kRec * (size_t)m->d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->rhs6, 6 * (size_t)m->d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->mass, (size_t)m->d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->sc, sizeof(LagScalars)));
@@ -277,7 +277,7 @@ int subfv_compute_rhs_lagrange(subfv_mesh* m, const double* sol, double* vp, dou
   if (load_sol(m, sol, mass)) return -1;
   launch_lag_node(d, m->sol6, nullptr, 0, 0);
   launch_lag_cell(d, m->sol6, m->rhs6, nullptr, nullptr, 0, 1);
-  launch_unpack6(d, d.ne, m->rhs6, m->stage);
+  launch_unpack6(d, d.ne, kRhs, m->rhs6, m->stage);
   SUBFV_CUDA(cudaMemcpyAsync(rhs, m->stage, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
   std::vector<double4> h(d.nv);
   SUBFV_CUDA(cudaMemcpyAsync(h.data(), d.vp, d.nv * sizeof(double4), cudaMemcpyDeviceToHost, d.stream));
@@ -331,7 +331,7 @@ int subfv_lag_state_create(subfv_mesh* m, const double* sol, const double* mass,
   auto* s = new subfv_lag_state();
   s->m = m;
   s->precision = precision;
-  SUBFV_CUDA(cudaMalloc(&s->sol6, 6 * (size_t)d.ne * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&s->sol6, kRec * (size_t)d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&s->rhs6, 6 * (size_t)d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&s->sc, sizeof(LagScalars)));
   SUBFV_CUDA(cudaMallocHost(&s->host_stage, 5 * (size_t)d.ne * sizeof(double)));
@@ -419,7 +419,7 @@ int subfv_lag_advance(subfv_lag_state* s, int n_steps, int* steps_done, double* 
 
 int subfv_lag_get_sol(subfv_lag_state* s, double* sol) {
   DevMesh& d = s->m->d;
-  launch_unpack6(d, d.ne, s->sol6, s->dev_stage);
+  launch_unpack6(d, d.ne, kRec, s->sol6, s->dev_stage);
   SUBFV_CUDA(cudaMemcpyAsync(sol, s->dev_stage, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
   return 0;
@@ -460,7 +460,7 @@ int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout) {
   SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, s->host_stage, bytes, cudaMemcpyHostToDevice, d.stream));
   launch_pack6(d, d.ne, s->dev_stage, nullptr, s->sol6);
   enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
-  launch_unpack6(d, d.ne, s->sol6, s->dev_stage);
+  launch_unpack6(d, d.ne, kRec, s->sol6, s->dev_stage);
   SUBFV_CUDA(cudaMemcpyAsync(s->host_stage, s->dev_stage, bytes, cudaMemcpyDeviceToHost, d.stream));
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
   std::memcpy(sol_inout, s->host_stage, bytes);

@@ -84,6 +84,12 @@ struct LagScalars {
   int skip;                   // this step was a no-op
 };
 
+// Cell record on the device: tau (or rho), the three velocities / momenta, energy, mass,
+// pressure, pad. The pressure is recomputed whenever the state changes, with the same
+// function the reference calls, so reading it is bit-identical to recomputing it.
+constexpr int kRec = 8;
+constexpr int kRhs = 6;  // rhs record: five residuals and a pad
+
 inline int grid_for(long long n, int block) { return (int)((n + block - 1) / block); }
 
 }  // namespace subfv

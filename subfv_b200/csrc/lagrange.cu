@@ -27,14 +27,15 @@ namespace subfv {
 namespace {
 
 struct U5 {
-  double t, u, v, w, e;
+  double t, u, v, w, e, p;
 };
+// cell record: (tau, u, v, w, e, mass, p, -)
 __device__ inline U5 ld_u(const double* sol6, int c) {
-  const double2* p = reinterpret_cast<const double2*>(sol6 + 6 * (size_t)c);
-  double2 a = p[0], b = p[1], d = p[2];
-  return {a.x, a.y, b.x, b.y, d.x};
+  const double2* q = reinterpret_cast<const double2*>(sol6 + kRec * (size_t)c);
+  double2 a = q[0], b = q[1], d = q[2], g = q[3];
+  return {a.x, a.y, b.x, b.y, d.x, g.x};
 }
-__device__ inline double ld_mass(const double* sol6, int c) { return sol6[6 * (size_t)c + 5]; }
+__device__ inline double ld_mass(const double* sol6, int c) { return sol6[kRec * (size_t)c + 5]; }
 
 template <int P>
 struct Flt;
@@ -69,7 +70,7 @@ __device__ inline double lam_wall(double p_me, double tau_me) {
 }
 
 template <int P>
-__global__ void k_lag_node(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc, int with_vol) {
+__global__ void __launch_bounds__(128, 8) k_lag_node(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc, int with_vol) {
   if (sc && sc->done) return;
   int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= m.nv) return;
@@ -84,12 +85,12 @@ __global__ void k_lag_node(DevMesh m, const double* __restrict__ sol6, const Lag
     double n0 = fn.x, n1 = fn.y, n2 = fn.z;
     double area = m.sfn[sf].w;
     U5 ul = ld_u(sol6, lr.x);
-    double pl = lag_pressure(ul.t, ul.u, ul.v, ul.w, ul.e);
+    double pl = ul.p;
     double vl = dot3(ul.u, ul.v, ul.w, n0, n1, n2);
     double w;
     if (lr.y >= 0) {
       U5 ur = ld_u(sol6, lr.y);
-      double pr = lag_pressure(ur.t, ur.u, ur.v, ur.w, ur.e);
+      double pr = ur.p;
       double vr = dot3(ur.u, ur.v, ur.w, n0, n1, n2);
       double l1 = lam_side<P>(pl, pr, ul.t, vr - vl);
       double l2 = lam_side<P>(pr, pl, ur.t, vr - vl);
@@ -160,7 +161,7 @@ __device__ inline double warp_min(double x) {
 
 // mode bit 1: rhs, bit 2: CFL terms
 template <int P>
-__global__ void k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* __restrict__ rhs6,
+__global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* __restrict__ rhs6,
                            LagScalars* sc, double* dt_slot, int mode) {
   using T = typename Flt<P>::T;
   if (sc && sc->done) return;
@@ -169,7 +170,7 @@ __global__ void k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* _
   if (c < m.ne) {
     U5 me = ld_u(sol6, c);
     double mass = ld_mass(sol6, c);
-    double pme = lag_pressure(me.t, me.u, me.v, me.w, me.e);
+    double pme = me.p;
     double csnd = sqrt(kGamma * pme * me.t);
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
     bool bad = false;
@@ -192,7 +193,7 @@ __global__ void k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* _
           double lam;
           if (lr.y >= 0) {
             U5 ot = ld_u(sol6, lr.y);
-            double pot = lag_pressure(ot.t, ot.u, ot.v, ot.w, ot.e);
+            double pot = ot.p;
             double vot = dot3(ot.u, ot.v, ot.w, fn.x, fn.y, fn.z);
             lam = lam_side<P>(pme, pot, me.t, vot - vme);
           } else {
@@ -215,7 +216,7 @@ __global__ void k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* _
           }
         } else {  // right neighbour
           U5 ot = ld_u(sol6, lr.x);
-          double pot = lag_pressure(ot.t, ot.u, ot.v, ot.w, ot.e);
+          double pot = ot.p;
           double vot = dot3(ot.u, ot.v, ot.w, fn.x, fn.y, fn.z);
           double lam = lam_side<P>(pme, pot, me.t, vme - vot);
           if (P == 0) {
@@ -242,14 +243,14 @@ __global__ void k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* _
         int sub = side == 0 ? se.x : se.y;
         double t1 = m.vol_se[c] / (area * csnd);  // sub_elem(i) with i the cell (reference quirk)
         double vn = dot3(vps.x, vps.y, vps.z, sg * fn.x, sg * fn.y, sg * fn.z);
-        double t2 = 0.8 * m.vol_se[sub] / (1e-8 + fabs(vn) * fn.w);
+        double t2 = sub >= 0 ? 0.8 * m.vol_se[sub] / (1e-8 + fabs(vn) * fn.w) : 1e6;
         if (t1 < dtloc) dtloc = t1;
         if (t2 < dtloc) dtloc = t2;
         bad = bad || !(t1 >= 0.0) || !(t2 >= 0.0);
       }
     }
     if (mode & 1) {
-      double2* r = reinterpret_cast<double2*>(rhs6 + 6 * (size_t)c);
+      double2* r = reinterpret_cast<double2*>(rhs6 + kRhs * (size_t)c);
       r[0] = make_double2(r0, r1);
       r[1] = make_double2(r2, r3);
       r[2] = make_double2(r4, 0.0);
@@ -300,13 +301,17 @@ __global__ void k_lag_move(DevMesh m, const LagScalars* sc, double dt_host) {
 __global__ void k_pack6(int n, const double* __restrict__ s5, const double* __restrict__ mass, double* __restrict__ s6) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  for (int k = 0; k < 5; ++k) s6[6 * (size_t)c + k] = s5[5 * (size_t)c + k];
-  if (mass) s6[6 * (size_t)c + 5] = mass[c];
+  double* r = s6 + kRec * (size_t)c;
+  const double* u = s5 + 5 * (size_t)c;
+  for (int k = 0; k < 5; ++k) r[k] = u[k];
+  if (mass) r[5] = mass[c];
+  r[6] = lag_pressure(u[0], u[1], u[2], u[3], u[4]);
+  r[7] = 0.0;
 }
-__global__ void k_unpack6(int n, const double* __restrict__ s6, double* __restrict__ s5) {
+__global__ void k_unpack6(int n, int stride, const double* __restrict__ s6, double* __restrict__ s5) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  for (int k = 0; k < 5; ++k) s5[5 * (size_t)c + k] = s6[6 * (size_t)c + k];
+  for (int k = 0; k < 5; ++k) s5[5 * (size_t)c + k] = s6[stride * (size_t)c + k];
 }
 __global__ void k_vp_out(int n, const double4* __restrict__ vp, double* __restrict__ out) {
   int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -347,8 +352,8 @@ void launch_lag_move(const DevMesh& m, const LagScalars* sc, double dt_host) {
 void launch_pack6(const DevMesh& m, int n, const double* s5, const double* mass, double* s6) {
   k_pack6<<<grid_for(n, 256), 256, 0, m.stream>>>(n, s5, mass, s6);
 }
-void launch_unpack6(const DevMesh& m, int n, const double* s6, double* s5) {
-  k_unpack6<<<grid_for(n, 256), 256, 0, m.stream>>>(n, s6, s5);
+void launch_unpack6(const DevMesh& m, int n, int stride, const double* s6, double* s5) {
+  k_unpack6<<<grid_for(n, 256), 256, 0, m.stream>>>(n, stride, s6, s5);
 }
 void launch_vp_out(const DevMesh& m, double* out) { k_vp_out<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m.nv, m.vp, out); }
 void launch_vp_in(const DevMesh& m, const double* in) { k_vp_in<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m.nv, in, m.vp); }

@@ -12,7 +12,8 @@ void launch_lag_cell(const DevMesh& m, const double* sol6, double* rhs6, LagScal
 void launch_lag_finalize(const DevMesh& m, LagScalars* sc);
 void launch_lag_move(const DevMesh& m, const LagScalars* sc, double dt_host);
 void launch_pack6(const DevMesh& m, int n, const double* s5, const double* mass, double* s6);
-void launch_unpack6(const DevMesh& m, int n, const double* s6, double* s5);
+// record (stride doubles per cell) -> (5, n) host layout
+void launch_unpack6(const DevMesh& m, int n, int stride, const double* s6, double* s5);
 void launch_vp_out(const DevMesh& m, double* out);
 void launch_vp_in(const DevMesh& m, const double* in);
 void launch_set_scalar(const DevMesh& m, double* p, double v);

@@ -351,13 +351,14 @@ __global__ void k_cell_geometry(DevMesh m, double* sol6, const double* rhs6, con
   if (!ok) atomicOr(m.status, kErrMeshCheck);
   if (sol6) {  // lagrange_main.F90:110: new_sol = sol + dt*rhs
     double dt = sc->dt;
-    double* u = sol6 + 6 * (size_t)c;
-    const double* r = rhs6 + 6 * (size_t)c;
+    double* u = sol6 + kRec * (size_t)c;
+    const double* r = rhs6 + kRhs * (size_t)c;
     bool fin = true;
     for (int k = 0; k < 5; ++k) {
       u[k] = u[k] + dt * r[k];
       fin = fin && isfinite(u[k]);
     }
+    u[6] = lag_pressure(u[0], u[1], u[2], u[3], u[4]);
     if (!fin) atomicOr(m.status, kErrNonFinite);
     if (!(u[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
   }
