@@ -80,6 +80,8 @@ typedef struct subfv_mesh_desc {
   const int32_t* vert_sub_elem_off;     /* (n_vert+1) */
   const int32_t* vert_sub_elem;         /* vert%sub_elem_neigh */
   const int32_t* vert_is_bound;         /* vert%is_bound (0/1) */
+  const int32_t* vert_elem_off;         /* (n_vert+1), or NULL when no second-order NS is run */
+  const int32_t* vert_elem;             /* vert%elem_neigh */
 } subfv_mesh_desc;
 
 typedef struct subfv_mesh subfv_mesh;
@@ -143,6 +145,47 @@ int subfv_lag_profile_steps(subfv_lag_state* s, int n_steps, double* kernel_ms);
 
 /* The CUDA stream (cudaStream_t) all work of this mesh is launched on. */
 void* subfv_mesh_stream(subfv_mesh* m);
+
+/* ---------------------------------------------------------------------------------
+ * Explicit Euler (subfvns): compute_euler_flux with the multi-point nodal solver or the
+ * two-wave subface flux, second-order reconstruction with limiters, flux limiting and
+ * add_timedisc_and_solve, first order or the two-stage scheme of ns_main.F90:83-107.
+ * Conservative state sol(5, n_elems) = (rho, rho u, rho v, rho w, E). */
+typedef struct subfv_ns_cfg {
+  int32_t scheme;             /* 1 multi_point, 4 two_wave (ns_global_data_module.F90:67-70) */
+  int32_t second_order;       /* 0 / 1 */
+  int32_t method;             /* cell gradient: 0 or 1 (none), 4 (ns_euler_recon_module.F90:200-240) */
+  int32_t bc_style;           /* 0, 1, 2 */
+  int32_t boundary_2d;        /* one-cell slab: z-faces are walls */
+  int32_t exclude_bound_vert; /* boundary vertices use two_wave */
+  int32_t local_time_step;    /* must be 0 (global time step) */
+  int32_t n_bc;               /* boundary tags in use (<= 16) */
+  int32_t bc_type[16];        /* per tag: 1 wall, 3 freestream, 4 outflow supersonic */
+  double bc_val[16][5];       /* per tag: primitive (rho, u, v, w, p) */
+  double cfl, tmax;
+  int32_t precision;          /* 0 plain FP64, 1 FP32 flux/reconstruction/limiter arithmetic */
+} subfv_ns_cfg;
+
+/* compute_rhs_ns (ns_main.F90:130-179, no diffusion): one residual evaluation.
+ * rhs (5, n_elems), sum_lambda (n_elems, first-order pass), vp (3, n_vert) of the last
+ * pass, cell_grad (3, 5, n_elems) or NULL. Host arrays. */
+int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs,
+                         double* sum_lambda, double* vp, double* cell_grad);
+
+typedef struct subfv_ns_state subfv_ns_state;
+int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double t0,
+                          subfv_ns_state** out);
+int subfv_ns_state_destroy(subfv_ns_state* s);
+/* n_steps iterations of ns_main.F90:83-107 (stops once t >= tmax); status bits */
+int subfv_ns_advance(subfv_ns_state* s, int n_steps, int* steps_done, double* t);
+int subfv_ns_advance_async(subfv_ns_state* s, int n_steps);
+int subfv_ns_sync(subfv_ns_state* s, int* steps_done, double* t);
+int subfv_ns_get_sol(subfv_ns_state* s, double* sol);
+/* res = sum of |delta|_2 and res_vect(5) of the last add_timedisc_and_solve call */
+int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double* dt);
+/* Gresho vortex of ns_euler_exact_sol_module.F90:7-44 at the cell centroids, as
+ * conservative variables (init_sol with init_gresho, ns_euler_module.F90:49-53). */
+int subfv_ns_init_gresho(subfv_mesh* m, double mach, double* sol);
 
 #ifdef __cplusplus
 }

@@ -50,6 +50,11 @@ def load():
         lib.or_inverse_3_by_3.argtypes = [PD, PD]
         lib.or_fnorm2.restype = C.c_double
         lib.or_fnorm2.argtypes = [PD, C.c_int]
+        lib.or_ns_rhs.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, PD, PD, PD, PD]
+        lib.or_ns_run.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_int, C.c_double, PD, PI, PD, PD, PD]
+        lib.or_ns_gresho.argtypes = [C.c_void_p, C.c_double, PD]
+        lib.or_pinv3.argtypes = [PD]
+        lib.or_lu3.argtypes = [PD, PD, PD]
         _lib = lib
     return _lib
 
@@ -159,6 +164,45 @@ class OracleMesh:
         n = load().or_lag_run(self._h, _pd(sol), _pd(vp), _pd(rhs), _pd(mass), float(cfl), float(t_max),
                               int(max_steps), int(self.b2d), C.byref(t), C.byref(dt))
         return n, t.value, dt.value, vp
+
+    # --- explicit Euler (subfvns)
+    @staticmethod
+    def _ns_args(cfg):
+        ic = np.array([cfg["scheme"], cfg["second_order"], cfg["method"], cfg["bc_style"], cfg["b2d"],
+                       cfg["exclude_bound_vert"], cfg["local_time_step"], cfg.get("n_bc", 0)], np.int32)
+        dc = np.array([cfg["cfl"], cfg["tmax"]], np.float64)
+        bt = np.ascontiguousarray(cfg.get("bc_type", np.zeros(1, np.int32)), np.int32)
+        bv = np.ascontiguousarray(cfg.get("bc_val", np.zeros(5)), np.float64).reshape(-1)
+        return ic, dc, bt, bv
+
+    def ns_gresho(self, mach):
+        sol = np.zeros((self.n_elems, 5))
+        load().or_ns_gresho(self._h, float(mach), _pd(sol))
+        return sol
+
+    def ns_rhs(self, cfg, sol):
+        ic, dc, bt, bv = self._ns_args(cfg)
+        sol = np.ascontiguousarray(sol, np.float64)
+        rhs = np.zeros((self.n_elems, 5))
+        sl = np.zeros(self.n_elems)
+        vp = np.zeros((self.n_vert, 3))
+        grad = np.zeros((self.n_elems, 15))
+        st = load().or_ns_rhs(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), _pd(rhs), _pd(sl), _pd(vp),
+                              _pd(grad))
+        return st, rhs, sl, vp, grad
+
+    def ns_run(self, cfg, sol, n_max_iter, final_res=-1.0, t0=0.0):
+        """The ns_main time loop in place on sol (n_max_iter + 1 steps unless stopped)."""
+        ic, dc, bt, bv = self._ns_args(cfg)
+        assert sol.dtype == np.float64 and sol.flags["C_CONTIGUOUS"]
+        t = C.c_double(t0)
+        it = C.c_int32(0)
+        res = C.c_double(0.0)
+        rv = np.zeros(5)
+        vp = np.zeros((self.n_vert, 3))
+        st = load().or_ns_run(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), int(n_max_iter),
+                              float(final_res), C.byref(t), C.byref(it), C.byref(res), _pd(rv), _pd(vp))
+        return st, it.value, t.value, res.value, rv, vp
 
     def close(self):
         if getattr(self, "_h", None):

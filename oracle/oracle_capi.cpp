@@ -22,6 +22,10 @@ struct OHandle {
   std::map<std::string, std::vector<int32_t>> topo;
 };
 
+namespace oracle {
+Mesh& handle_mesh(void* h) { return ((OHandle*)h)->m; }
+}  // namespace oracle
+
 extern "C" {
 
 void* or_mesh_new(int n_vert, const double* coords, int n_elems, const int* kind, const int* ev_off,

@@ -1,0 +1,781 @@
+// Test infrastructure only (oracle). Restatement of the subfv explicit Euler path
+// (subfvns): src/ns/ns_euler_primitives_module.F90, src/ns/ns_euler_recon_module.F90,
+// src/ns/ns_euler_rs_module.F90 (two_wave, multi_point, the multi-point nodal velocity
+// solver), src/ns/ns_euler_module.F90 (compute_euler_flux, compute_rhs_around_vert,
+// add_timedisc_and_solve), the contained compute_rhs_ns and the time loop of
+// src/ns/ns_main.F90:83-130, and the Gresho initial state of
+// src/ns/ns_euler_exact_sol_module.F90:7-44.
+//
+// LAPACK stand-ins (the reference links an unpinned system LAPACK):
+//  * dgesvd-based pseudo_inverse_inplace_lapack (linear_solver_module.F90:683-715):
+//    one-sided Jacobi SVD, six sweeps, same singular-value cut n*1e-12*max(sigma);
+//  * lu_solve_inplace_lapack (:643-657): LU with partial pivoting in LAPACK's
+//    dgetrf2 / dgetrs operation order, reference-BLAS triangular solves.
+// PARITY UNPINNED (no Fortran compiler or LAPACK build of the reference here).
+#include "oracle.h"
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace oracle {
+
+static const double G = 1.4;  // ns_global_data_module.F90:9
+
+struct NsCfg {
+  int scheme;          // 1 multi_point, 4 two_wave
+  int second_order;    // 0/1
+  int method;          // 0/1 (no gradient) or 4
+  int bc_style;        // 0, 1, 2
+  int b2d;
+  int exclude_bound_vert;
+  double cfl, tmax;
+  int local_time_step;
+  int n_bc;
+  const int* bc_type;     // per tag: 1 wall, 3 freestream, 4 outflow supersonic
+  const double* bc_val;   // per tag: 5 primitive values
+};
+
+// ---------------------------------------------------------------- primitives (:7-111)
+static void p2c(const double* w, double* u) {
+  u[0] = w[0];
+  for (int k = 1; k < 4; ++k) u[k] = w[k] * w[0];
+  u[4] = w[4] / (G - 1) + 0.5 * w[0] * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+}
+static void c2p(const double* u, double* w) {
+  w[0] = u[0];
+  for (int k = 1; k < 4; ++k) w[k] = u[k] / u[0];
+  w[4] = (G - 1) * (u[4] - 0.5 * w[0] * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]));
+}
+static double sound_speed_w(const double* w) { return std::sqrt(G * w[4] / w[0]); }
+static double fmax2(double a, double b) { return b > a ? b : a; }
+static double fmin2(double a, double b) { return b < a ? b : a; }
+static double dot3(const double* a, const double* b) {
+  double s = 0.0;
+  for (int k = 0; k < 3; ++k) s = s + a[k] * b[k];
+  return s;
+}
+
+double max_omega_for_positivity(const double* U, const double* dU) {
+  double omega = 1.0, US[5], WS[5];
+  for (int k = 0; k < 5; ++k) US[k] = U[k] + omega * dU[k];
+  c2p(US, WS);
+  bool pos = WS[0] > 1e-17 && WS[4] > 1e-17;
+  while (!pos && omega > 1e-6) {
+    omega = omega * 0.9;
+    for (int k = 0; k < 5; ++k) US[k] = U[k] + omega * dU[k];
+    c2p(US, WS);
+    pos = WS[0] > 1e-17 && WS[4] > 1e-17;
+  }
+  return omega;
+}
+
+// ---------------------------------------------------------------- LAPACK stand-ins
+// A[r][c] = mat(r+1, c+1). One-sided Jacobi on the columns: A V = U S.
+void pinv3(double A[3][3]) {
+  double U[3][3], V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  std::memcpy(U, A, sizeof(U));
+  const int pr[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int sweep = 0; sweep < 6; ++sweep)
+    for (const auto& pq : pr) {
+      int p = pq[0], q = pq[1];
+      double al = 0.0, be = 0.0, ga = 0.0;
+      for (int i = 0; i < 3; ++i) {
+        al = al + U[i][p] * U[i][p];
+        be = be + U[i][q] * U[i][q];
+        ga = ga + U[i][p] * U[i][q];
+      }
+      if (!(std::fabs(ga) > 1e-15 * std::sqrt(al * be))) continue;
+      double zeta = (be - al) / (2.0 * ga);
+      double t = 1.0 / (std::fabs(zeta) + std::sqrt(1.0 + zeta * zeta));
+      if (zeta < 0.0) t = -t;
+      double c = 1.0 / std::sqrt(1.0 + t * t), s = c * t;
+      for (int i = 0; i < 3; ++i) {
+        double up = U[i][p], uq = U[i][q];
+        U[i][p] = c * up - s * uq;
+        U[i][q] = s * up + c * uq;
+        double vp = V[i][p], vq = V[i][q];
+        V[i][p] = c * vp - s * vq;
+        V[i][q] = s * vp + c * vq;
+      }
+    }
+  double sig[3], smax = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    double s = 0.0;
+    for (int i = 0; i < 3; ++i) s = s + U[i][k] * U[i][k];
+    sig[k] = std::sqrt(s);
+    smax = fmax2(smax, sig[k]);
+  }
+  double tol = 3 * 1e-12 * smax;
+  double SUt[3][3];  // Sigma_plus * U^T, U^T row k = u_k = U[:,k] / sig_k
+  for (int k = 0; k < 3; ++k)
+    for (int j = 0; j < 3; ++j) SUt[k][j] = sig[k] > tol ? (1.0 / sig[k]) * (U[j][k] / sig[k]) : 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = s + V[i][k] * SUt[k][j];
+      A[i][j] = s;
+    }
+}
+
+// dgetrf2 + dgetrs ('N') on a 3x3 system; A is overwritten.
+void lu_solve3(double A[3][3], double* x, const double* b) {
+  const double sfmin = 2.2250738585072014e-308;
+  int ipiv[3];
+  for (int j = 0; j < 3; ++j) {
+    int p = j;
+    double amax = std::fabs(A[j][j]);
+    for (int i = j + 1; i < 3; ++i)
+      if (std::fabs(A[i][j]) > amax) {
+        amax = std::fabs(A[i][j]);
+        p = i;
+      }
+    ipiv[j] = p;
+    if (A[p][j] != 0.0) {
+      if (p != j)
+        for (int k = 0; k < 3; ++k) std::swap(A[j][k], A[p][k]);
+      if (std::fabs(A[j][j]) >= sfmin) {
+        double r = 1.0 / A[j][j];
+        for (int i = j + 1; i < 3; ++i) A[i][j] = r * A[i][j];
+      } else {
+        for (int i = j + 1; i < 3; ++i) A[i][j] = A[i][j] / A[j][j];
+      }
+    }
+    for (int i = j + 1; i < 3; ++i)
+      for (int k = j + 1; k < 3; ++k) A[i][k] = A[i][k] - A[j][k] * A[i][j];
+  }
+  double y[3] = {b[0], b[1], b[2]};
+  for (int j = 0; j < 3; ++j)
+    if (ipiv[j] != j) std::swap(y[j], y[ipiv[j]]);
+  for (int k = 0; k < 3; ++k)
+    if (y[k] != 0.0)
+      for (int i = k + 1; i < 3; ++i) y[i] = y[i] - y[k] * A[i][k];
+  for (int k = 2; k >= 0; --k)
+    if (y[k] != 0.0) {
+      y[k] = y[k] / A[k][k];
+      for (int i = 0; i < k; ++i) y[i] = y[i] - y[k] * A[i][k];
+    }
+  for (int k = 0; k < 3; ++k) x[k] = y[k];
+}
+
+// ---------------------------------------------------------------- fluxes (ns_euler_rs_module.F90)
+// :154-198
+static void two_wave(const double* wl, const double* wr, const double* n, double lr[2][5], double* sl, double* sr) {
+  double rhol = wl[0], vnl = dot3(wl + 1, n), pl = wl[4], al = sound_speed_w(wl), ul[5];
+  p2c(wl, ul);
+  double rhor = wr[0], vnr = dot3(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr), ur[5];
+  p2c(wr, ur);
+  double fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  double lam_l = fmax2(fmax2(al * rhol, std::sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+  double lam_r = fmax2(fmax2(ar * rhor, std::sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+  *sl = vnl - lam_l / rhol;
+  *sr = vnr + lam_r / rhor;
+  for (int k = 0; k < 5; ++k) {
+    double et = (*sr * ur[k] - *sl * ul[k] - (fr[k] - fl[k])) / (*sr - *sl);
+    lr[0][k] = 0.5 * (fl[k] + fr[k]) - 0.5 * (std::fabs(*sl) * (et - ul[k]) + std::fabs(*sr) * (ur[k] - et));
+    lr[1][k] = -lr[0][k];
+  }
+}
+
+// :200-286; returns false on a negative star density (the reference error-stops)
+static bool multi_point(const double* wl, const double* wr, const double* n, double lr[2][5], double vn_nodal,
+                        double lam_l, double lam_r, double* sl, double* sr) {
+  double rhol = wl[0], vnl = dot3(wl + 1, n), pl = wl[4], ul[5];
+  p2c(wl, ul);
+  double el = ul[4] / rhol;
+  double rhor = wr[0], vnr = dot3(wr + 1, n), pr = wr[4], ur[5];
+  p2c(wr, ur);
+  double er = ur[4] / rhor;
+  double fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  double v_et = vn_nodal;
+  double rhol_et = 1.0 / (1.0 / rhol + (v_et - vnl) / lam_l);
+  double pl_bar = pl - lam_l * (v_et - vnl);
+  double sle[5], sre[5];
+  sle[0] = rhol_et;
+  for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (wl[k] + (v_et - vnl) * n[k - 1]);
+  sle[4] = rhol_et * (el + (pl * vnl - pl_bar * v_et) / lam_l);
+  double rhor_et = 1.0 / (1.0 / rhor + (vnr - v_et) / lam_r);
+  double pr_bar = pr + lam_r * (v_et - vnr);
+  sre[0] = rhor_et;
+  for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (wr[k] + (v_et - vnr) * n[k - 1]);
+  sre[4] = rhor_et * (er + (pr_bar * v_et - pr * vnr) / lam_r);
+  bool ok = !(rhol_et < 0.0 || rhor_et < 0.0);
+  *sl = vnl - lam_l / rhol;
+  *sr = vnr + lam_r / rhor;
+  const double e[5] = {0.0, n[0], n[1], n[2], v_et};
+  for (int k = 0; k < 5; ++k) {
+    double base = 0.5 * (fl[k] + fr[k]) -
+                  0.5 * (std::fabs(*sl) * (sle[k] - ul[k]) + std::fabs(v_et) * (sre[k] - sle[k]) +
+                         std::fabs(*sr) * (ur[k] - sre[k]));
+    double jump = 0.5 * (pr_bar - pl_bar) * e[k];
+    lr[0][k] = base - jump;
+    lr[1][k] = -(base + jump);
+  }
+  return ok;
+}
+
+// ---------------------------------------------------------------- reconstruction (ns_euler_recon_module.F90)
+static bool is_wall(const NsCfg& cfg, int re) {
+  if (re > 0) return false;
+  if (re == 0) return true;
+  return cfg.bc_type[-re - 1] == 1;
+}
+
+// :331-409 (wall, freestream, outflow supersonic); sol_l/sol_r conservative
+static void compute_right_state(const Mesh& m, const NsCfg& cfg, int sf, int re, const double* sol_l, double* sol_r) {
+  const double* n = &m.sub_face[sf].norm[1];
+  int kind = re == 0 ? 1 : cfg.bc_type[-re - 1];
+  if (kind == 1) {
+    for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+    double d = dot3(sol_r + 1, n);
+    for (int k = 1; k < 4; ++k) sol_r[k] = sol_r[k] - 2.0 * d * n[k - 1];
+  } else if (kind == 3) {
+    p2c(cfg.bc_val + 5 * (-re - 1), sol_r);
+  } else {
+    for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+  }
+}
+
+// :427-451; grad[c*15 + d*5 + var] = grad(d+1, var+1, c+1)
+static void reconstruct_lr_w(const Mesh& m, const NsCfg& cfg, const double* sol, const double* grad, int v, int sf,
+                             int le, int re, bool so, double* wl, double* wr) {
+  c2p(sol + 5 * (le - 1), wl);
+  if (so) {
+    double dx[3];
+    for (int d = 0; d < 3; ++d) dx[d] = m.vert[v].coord[d + 1] - m.elem[le].coord[d + 1];
+    const double* g = grad + 15 * (le - 1);
+    for (int k = 0; k < 5; ++k) {
+      double s = 0.0;
+      for (int d = 0; d < 3; ++d) s = s + g[5 * d + k] * dx[d];
+      wl[k] = wl[k] + s;
+    }
+  }
+  if (re > 0) {
+    c2p(sol + 5 * (re - 1), wr);
+    if (so) {
+      double dx[3];
+      for (int d = 0; d < 3; ++d) dx[d] = m.vert[v].coord[d + 1] - m.elem[re].coord[d + 1];
+      const double* g = grad + 15 * (re - 1);
+      for (int k = 0; k < 5; ++k) {
+        double s = 0.0;
+        for (int d = 0; d < 3; ++d) s = s + g[5 * d + k] * dx[d];
+        wr[k] = wr[k] + s;
+      }
+    }
+  } else {
+    double ul[5], ghost[5];
+    p2c(wl, ul);
+    compute_right_state(m, cfg, sf, re, ul, ghost);
+    c2p(ghost, wr);
+  }
+}
+
+// :453-490
+static void compute_nodal_grad(const Mesh& m, int v, const double* sol, double* ng) {
+  double g[3][5] = {{0}}, mat[3][3] = {{0}};
+  const Vert& vv = m.vert[v];
+  for (int i = 1; i <= vv.n_sub_faces_neigh; ++i) {
+    int sf = vv.sub_face_neigh[i];
+    const Face& f = m.face[m.sub_face[sf].mesh_face];
+    int le = f.left_neigh, re = f.right_neigh;
+    if (re > 0) {
+      double wl[5], wr[5];
+      c2p(sol + 5 * (le - 1), wl);
+      c2p(sol + 5 * (re - 1), wr);
+      const double* n = &m.sub_face[sf].norm[1];
+      double a = m.sub_face[sf].area;
+      for (int d = 0; d < 3; ++d)
+        for (int k = 0; k < 5; ++k) g[d][k] = g[d][k] + a * (n[d] * (wr[k] - wl[k]));
+      for (int d = 0; d < 3; ++d)
+        for (int e = 0; e < 3; ++e)
+          mat[d][e] = mat[d][e] + a * (n[d] * (m.elem[re].coord[e + 1] - m.elem[le].coord[e + 1]));
+    }
+  }
+  pinv3(mat);
+  for (int d = 0; d < 3; ++d)
+    for (int k = 0; k < 5; ++k) {
+      double s = 0.0;
+      for (int e = 0; e < 3; ++e) s = s + mat[d][e] * g[e][k];
+      ng[5 * d + k] = vv.is_bound ? 0.0 : s;
+    }
+}
+
+static double OI(double a, double b, double c) {
+  const double x[3] = {a, b, c};
+  return fnorm2(x, 3);
+}
+
+// :8-59 (method 4) with physical_slope_limiter (:129-164) and relaxed_maximum_principle (:61-127)
+static void compute_cell_grads(const Mesh& m, const NsCfg& cfg, const double* sol, double* grad, double* ngrad) {
+  for (int v = 1; v <= m.n_vert; ++v) compute_nodal_grad(m, v, sol, ngrad + 15 * (v - 1));
+  if (cfg.method == 0 || cfg.method == 1) {
+    for (int i = 0; i < 15 * m.n_elems; ++i) grad[i] = 0.0;
+    return;
+  }
+  const double eps = 1e-3, tol = 1e-8;
+  for (int c = 1; c <= m.n_elems; ++c) {
+    const Elem& e = m.elem[c];
+    double* g = grad + 15 * (c - 1);
+    double ws[5] = {0, 0, 0, 0, 0};
+    for (int i = 0; i < 15; ++i) g[i] = 0.0;
+    for (int j = 1; j <= e.n_vert; ++j) {
+      int v = e.vert[j];
+      const double* ng = ngrad + 15 * (v - 1);
+      for (int k = 0; k < 5; ++k) {
+        double w = m.vert[v].volume / (eps + OI(ng[k], ng[5 + k], ng[10 + k]));
+        for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] + w * ng[5 * d + k];
+        ws[k] = ws[k] + w;
+      }
+    }
+    for (int k = 0; k < 5; ++k)
+      for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
+    // physical_slope_limiter
+    double w0[5];
+    c2p(sol + 5 * (c - 1), w0);
+    double omega = 1.0;
+    for (int j = 1; j <= e.n_vert; ++j) {
+      int v = e.vert[j];
+      double dx[3], dw[5];
+      for (int d = 0; d < 3; ++d) dx[d] = m.vert[v].coord[d + 1] - e.coord[d + 1];
+      for (int k = 0; k < 5; ++k) {
+        double s = 0.0;
+        for (int d = 0; d < 3; ++d) s = s + g[5 * d + k] * dx[d];
+        dw[k] = s;
+      }
+      if (dw[0] < 0.0) omega = fmin2(omega, fmax2(0.0, w0[0] / (tol - dw[0])));
+      if (dw[4] < 0.0) omega = fmin2(omega, fmax2(0.0, w0[4] / (tol - dw[4])));
+    }
+    for (int i = 0; i < 15; ++i) g[i] = omega * g[i];
+    // relaxed_maximum_principle
+    double rmin = 1e100, rmax = 0.0, pmin = 1e100, pmax = 0.0;
+    for (int j = 1; j <= e.n_vert; ++j) {
+      const Vert& vv = m.vert[e.vert[j]];
+      for (int k = 1; k <= vv.n_elems_neigh; ++k) {
+        double w[5];
+        c2p(sol + 5 * (vv.elem_neigh[k] - 1), w);
+        pmin = fmin2(pmin, w[4]);
+        pmax = fmax2(pmax, w[4]);
+        rmin = fmin2(rmin, w[0]);
+        rmax = fmax2(rmax, w[0]);
+      }
+    }
+    pmin = (1.0 - 1e-2) * pmin;
+    rmin = (1.0 - 1e-2) * rmin;
+    pmax = (1.0 + 1e-2) * pmax;
+    rmax = (1.0 + 1e-2) * rmax;
+    omega = 1.0;
+    for (int j = 1; j <= e.n_vert; ++j) {
+      int v = e.vert[j];
+      double dx[3], dw[5];
+      for (int d = 0; d < 3; ++d) dx[d] = m.vert[v].coord[d + 1] - e.coord[d + 1];
+      for (int k = 0; k < 5; ++k) {
+        double s = 0.0;
+        for (int d = 0; d < 3; ++d) s = s + g[5 * d + k] * dx[d];
+        dw[k] = s;
+      }
+      if (dw[0] < 0.0)
+        omega = fmin2(omega, fmax2(0.0, (w0[0] - rmin) / (tol - dw[0])));
+      else
+        omega = fmin2(omega, fmax2(0.0, -(w0[0] - rmax) / (tol + dw[0])));
+      if (dw[4] < 0.0)
+        omega = fmin2(omega, fmax2(0.0, (w0[4] - pmin) / (tol - dw[4])));
+      else
+        omega = fmin2(omega, fmax2(0.0, -(w0[4] - pmax) / (tol + dw[4])));
+    }
+    for (int i = 0; i < 15; ++i) g[i] = omega * g[i];
+  }
+}
+
+// ns_euler_primitives_module.F90:162-190
+static void wall_normal(const Mesh& m, const NsCfg& cfg, int v, double* B) {
+  B[0] = B[1] = B[2] = 0.0;
+  const Vert& vv = m.vert[v];
+  for (int j = 1; j <= vv.n_sub_faces_neigh; ++j) {
+    int sf = vv.sub_face_neigh[j];
+    int re = m.face[m.sub_face[sf].mesh_face].right_neigh;
+    if (re <= 0) {
+      const double* n = &m.sub_face[sf].norm[1];
+      if (!(cfg.b2d && std::fabs(n[2]) > 1e-12))
+        if (re == 0 || cfg.bc_type[-re - 1] == 1)
+          for (int d = 0; d < 3; ++d) B[d] = B[d] + m.sub_face[sf].area * n[d];
+    }
+  }
+}
+
+// ns_euler_rs_module.F90:288-422
+static void nodal_velocity(const Mesh& m, const NsCfg& cfg, int v, const std::vector<double>& wlr,
+                           std::vector<double>& lam, std::vector<double>& vbar, double* vnode) {
+  const Vert& vv = m.vert[v];
+  int nsfn = vv.n_sub_faces_neigh;
+  double Bp[3];
+  wall_normal(m, cfg, v, Bp);
+  vnode[0] = vnode[1] = vnode[2] = 0.0;
+  for (int iter = 1; iter <= 4; ++iter) {
+    double mat[3][3] = {{0}}, Rp[3] = {0, 0, 0};
+    for (int j = 0; j < nsfn; ++j) {
+      int sf = vv.sub_face_neigh[j + 1];
+      int re = m.face[m.sub_face[sf].mesh_face].right_neigh;
+      const double* n = &m.sub_face[sf].norm[1];
+      double area = m.sub_face[sf].area;
+      const double* wl = &wlr[10 * j];
+      const double* wr = &wlr[10 * j + 5];
+      double rhol = wl[0], vnl = dot3(wl + 1, n), pl = wl[4], al = sound_speed_w(wl);
+      double rhor = wr[0], vnr = dot3(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr);
+      double lam_l = lam[2 * j], lam_r = lam[2 * j + 1];
+      if (iter == 1) {
+        lam_l = fmax2(fmax2(fmax2(lam_l, al * rhol), std::sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+        lam_r = fmax2(fmax2(fmax2(lam_r, ar * rhor), std::sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+        vbar[j] = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(vbar[j] - vnl) / al)));
+        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (vbar[j] - vnr) / ar)));
+      } else if (is_wall(cfg, re) && cfg.bc_style == 1) {
+        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(vbar[j] - vnl) / al)));
+        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (vbar[j] - vnr) / ar)));
+      } else {
+        double v_et = dot3(vnode, n);
+        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(v_et - vnl) / al)));
+        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (v_et - vnr) / ar)));
+      }
+      lam[2 * j] = lam_l;
+      lam[2 * j + 1] = lam_r;
+      vbar[j] = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+      bool wall = is_wall(cfg, re);
+      if (!wall || cfg.bc_style == 0 || cfg.bc_style == 2) {
+        double w = (lam_r + lam_l) * area;
+        for (int d = 0; d < 3; ++d)
+          for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + w * (n[d] * n[e]);
+      }
+      if (!wall || cfg.bc_style == 0) {
+        double q = area * (lam_r + lam_l) * vbar[j];
+        for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
+      } else if (cfg.bc_style == 2) {
+        if (!cfg.b2d || std::fabs(n[2]) < 1e-8) {
+          double q = area * pl;
+          for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
+        }
+      }
+    }
+    auto mv = [&](const double* x, double* y) {
+      for (int d = 0; d < 3; ++d) {
+        double s = 0.0;
+        for (int e = 0; e < 3; ++e) s = s + mat[d][e] * x[e];
+        y[d] = s;
+      }
+    };
+    if (cfg.bc_style == 2) {
+      double bmax = fmax2(fmax2(std::fabs(Bp[0]), std::fabs(Bp[1])), std::fabs(Bp[2]));
+      if (bmax > 1e-8) {
+        pinv3(mat);
+        double mr[3], mb[3], r2[3];
+        mv(Rp, mr);
+        mv(Bp, mb);
+        double p_bound = dot3(mr, Bp) / dot3(mb, Bp);
+        for (int d = 0; d < 3; ++d) r2[d] = Rp[d] - p_bound * Bp[d];
+        mv(r2, vnode);
+        double f = dot3(vnode, Bp) / dot3(Bp, Bp);
+        for (int d = 0; d < 3; ++d) vnode[d] = vnode[d] - f * Bp[d];
+      } else {
+        lu_solve3(mat, vnode, Rp);
+      }
+    } else {
+      pinv3(mat);
+      double r[3] = {Rp[0], Rp[1], Rp[2]};
+      mv(r, vnode);
+    }
+  }
+}
+
+// ns_euler_module.F90:151-339 (scheme_id multi_point or two_wave) + :341-519
+static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol, double* rhs, const double* grad,
+                              double* sum_lambda, bool so, double* vp) {
+  for (int i = 0; i < 5 * m.n_elems; ++i) rhs[i] = 0.0;
+  for (int i = 0; i < m.n_elems; ++i) sum_lambda[i] = 1e-12;
+  int status = 0;
+  std::vector<double> wlr, lam, vbar, fsv, slv;
+  for (int v = 1; v <= m.n_vert; ++v) {
+    const Vert& vv = m.vert[v];
+    int nsfn = vv.n_sub_faces_neigh, nsen = vv.n_sub_elems_neigh;
+    wlr.assign(10 * nsfn, 0.0);
+    lam.assign(2 * nsfn, 0.0);
+    vbar.assign(nsfn, 0.0);
+    fsv.assign(5 * nsen, 0.0);
+    slv.assign(nsen, 0.0);
+    for (int j = 0; j < nsfn; ++j) {
+      int sf = vv.sub_face_neigh[j + 1];
+      const Face& f = m.face[m.sub_face[sf].mesh_face];
+      reconstruct_lr_w(m, cfg, sol, grad, v, sf, f.left_neigh, f.right_neigh, so, &wlr[10 * j], &wlr[10 * j + 5]);
+    }
+    double vv3[3] = {0, 0, 0};
+    bool excl = vv.is_bound && cfg.exclude_bound_vert;
+    if (cfg.scheme == 1) {
+      if (!excl) nodal_velocity(m, cfg, v, wlr, lam, vbar, vv3);
+      for (int d = 0; d < 3; ++d) vp[3 * (v - 1) + d] = vv3[d];
+    }
+    int rse_loc = 0;
+    for (int j = 0; j < nsfn; ++j) {
+      int sf = vv.sub_face_neigh[j + 1];
+      const SubFace& s = m.sub_face[sf];
+      int re = m.face[s.mesh_face].right_neigh;
+      int lse = s.left_sub_elem_neigh, rse = s.right_sub_elem_neigh;
+      int lse_loc = m.sub_elem[lse].id_loc_around_node;
+      if (rse > 0) rse_loc = m.sub_elem[rse].id_loc_around_node;
+      double lr[2][5], sl, sr;
+      const double* n = &s.norm[1];
+      if (cfg.scheme == 1 && !excl) {
+        double vn = is_wall(cfg, re) ? 0.0 : dot3(vv3, n);
+        if (!multi_point(&wlr[10 * j], &wlr[10 * j + 5], n, lr, vn, lam[2 * j], lam[2 * j + 1], &sl, &sr))
+          status |= 4;
+      } else {
+        two_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr, &sl, &sr);
+      }
+      if (m.sub_elem[lse].mesh_vert == v) {
+        slv[lse_loc - 1] = slv[lse_loc - 1] + s.area * fmax2(0.0, -sl);
+        for (int k = 0; k < 5; ++k) fsv[5 * (lse_loc - 1) + k] = fsv[5 * (lse_loc - 1) + k] + s.area * lr[0][k];
+        if (rse > 0 && m.sub_elem[rse].mesh_vert == v) {
+          slv[rse_loc - 1] = slv[rse_loc - 1] + s.area * fmax2(0.0, sr);
+          for (int k = 0; k < 5; ++k) fsv[5 * (rse_loc - 1) + k] = fsv[5 * (rse_loc - 1) + k] + s.area * lr[1][k];
+        }
+      }
+    }
+    for (int j = 0; j < nsen; ++j) {
+      int ide = m.sub_elem[vv.sub_elem_neigh[j + 1]].mesh_elem;
+      for (int k = 0; k < 5; ++k) rhs[5 * (ide - 1) + k] = rhs[5 * (ide - 1) + k] - fsv[5 * j + k];
+      sum_lambda[ide - 1] = sum_lambda[ide - 1] + slv[j];
+    }
+  }
+  return status;
+}
+
+// ns_euler_recon_module.F90:560-601
+static void flux_limiting(const Mesh& m, const double* sol, double* rhs, const double* rhs_o2,
+                          const double* sum_lambda, double cfl) {
+  double dt = 1e10;
+  for (int i = 1; i <= m.n_elems; ++i) dt = fmin2(dt, m.elem[i].volume / sum_lambda[i - 1]);
+  dt = cfl * dt;
+  for (int i = 1; i <= m.n_elems; ++i) {
+    double den = m.elem[i].volume / dt + sum_lambda[i - 1];
+    double U[5], dU[5];
+    for (int k = 0; k < 5; ++k) {
+      U[k] = sol[5 * (i - 1) + k] + rhs[5 * (i - 1) + k] / den;
+      dU[k] = (rhs_o2[5 * (i - 1) + k] - rhs[5 * (i - 1) + k]) / den;
+    }
+    double omega = max_omega_for_positivity(U, dU);
+    double w = fmin2(1.0, omega);
+    for (int k = 0; k < 5; ++k)
+      rhs[5 * (i - 1) + k] = rhs[5 * (i - 1) + k] + w * (rhs_o2[5 * (i - 1) + k] - rhs[5 * (i - 1) + k]);
+  }
+}
+
+struct NsWork {
+  std::vector<double> rhs, rhs_o2, sl, sl_o2, grad, ngrad, vp, delta;
+};
+
+// ns_main.F90:130-179 (no diffusion)
+static int compute_rhs_ns(const Mesh& m, const NsCfg& cfg, const double* sol, NsWork& w) {
+  w.grad.assign(15 * m.n_elems, 0.0);
+  w.ngrad.assign(15 * m.n_vert, 0.0);
+  int st = compute_euler_flux(m, cfg, sol, w.rhs.data(), w.grad.data(), w.sl.data(), false, w.vp.data());
+  if (cfg.second_order) {
+    compute_cell_grads(m, cfg, sol, w.grad.data(), w.ngrad.data());
+    st |= compute_euler_flux(m, cfg, sol, w.rhs_o2.data(), w.grad.data(), w.sl_o2.data(), true, w.vp.data());
+    flux_limiting(m, sol, w.rhs.data(), w.rhs_o2.data(), w.sl.data(), cfg.cfl);
+  }
+  return st;
+}
+
+// ns_euler_module.F90:521-609 (no diffusion blocks: diag = a1*(V/dt + sum_lambda)*I)
+static int add_timedisc_and_solve(const Mesh& m, const NsCfg& cfg, double* sol, double* rhs, double* sum_lambda,
+                                  double* delta, double* res, double* res_vect, double a1, double a2, double t,
+                                  double* dt_io) {
+  double dt = 1e10;
+  for (int i = 1; i <= m.n_elems; ++i) dt = fmin2(dt, m.elem[i].volume / sum_lambda[i - 1]);
+  dt = cfg.cfl * dt;
+  if (!cfg.local_time_step) {
+    dt = fmin2(cfg.tmax - t + 1e-12, dt);
+    for (int i = 0; i < m.n_elems; ++i) sum_lambda[i] = 0.0;
+  }
+  *res = 0.0;
+  for (int k = 0; k < 5; ++k) res_vect[k] = 0.0;
+  double omega = 1.0;
+  for (int i = 1; i <= m.n_elems; ++i) {
+    double* r = rhs + 5 * (i - 1);
+    double* u = sol + 5 * (i - 1);
+    for (int k = 0; k < 5; ++k) res_vect[k] = res_vect[k] + r[k] * r[k];
+    double s = a1 * (m.elem[i].volume / dt + sum_lambda[i - 1]);
+    double nw[5], d5[5], ad[5];
+    for (int k = 0; k < 5; ++k) r[k] = r[k] + s * u[k];
+    for (int k = 0; k < 5; ++k) nw[k] = r[k] / s;
+    for (int k = 0; k < 5; ++k) {
+      d5[k] = nw[k] - u[k];
+      delta[5 * (i - 1) + k] = d5[k];
+      ad[k] = a2 * d5[k];
+    }
+    omega = fmin2(omega, max_omega_for_positivity(u, ad));
+    *res = *res + fnorm2(d5, 5);
+  }
+  for (int k = 0; k < 5; ++k) res_vect[k] = std::sqrt(res_vect[k]);
+  int st = 0;
+  if (omega <= 1e-6) st |= 8;
+  if (!cfg.local_time_step && omega < 1.0) dt = (1.0 - omega) * dt;
+  for (int i = 0; i < 5 * m.n_elems; ++i) sol[i] = sol[i] + a2 * omega * delta[i];
+  *dt_io = dt;
+  return st;
+}
+
+// ns_main.F90:72-107: while (res > final_res .and. iter <= n_max_iter); second order is
+// the two-stage scheme (stage 1 a1 = 2 on sol, stage 2 a1 = 1 on soln), each stage with
+// its own dt. Returns status bits; *iters, *t and *res are updated.
+int ns_run(const Mesh& m, const NsCfg& cfg, double* sol, int n_max_iter, double final_res, double* t_io,
+           int* iters, double* res_out, double* res_vect, double* vp_out) {
+  NsWork w;
+  w.rhs.assign(5 * m.n_elems, 0.0);
+  w.rhs_o2.assign(5 * m.n_elems, 0.0);
+  w.sl.assign(m.n_elems, 0.0);
+  w.sl_o2.assign(m.n_elems, 0.0);
+  w.vp.assign(3 * m.n_vert, 0.0);
+  w.delta.assign(5 * m.n_elems, 0.0);
+  std::vector<double> soln(5 * m.n_elems);
+  double t = *t_io, res = final_res + 1.0, dt = 0.0;
+  int iter = 0, st = 0;
+  while (res > final_res && iter <= n_max_iter) {
+    st |= compute_rhs_ns(m, cfg, sol, w);
+    if (cfg.second_order) {
+      std::memcpy(soln.data(), sol, soln.size() * sizeof(double));
+      st |= add_timedisc_and_solve(m, cfg, sol, w.rhs.data(), w.sl.data(), w.delta.data(), &res, res_vect, 2.0,
+                                   1.0, t, &dt);
+      st |= compute_rhs_ns(m, cfg, sol, w);
+      st |= add_timedisc_and_solve(m, cfg, soln.data(), w.rhs.data(), w.sl.data(), w.delta.data(), &res,
+                                   res_vect, 1.0, 1.0, t, &dt);
+      std::memcpy(sol, soln.data(), soln.size() * sizeof(double));
+    } else {
+      st |= add_timedisc_and_solve(m, cfg, sol, w.rhs.data(), w.sl.data(), w.delta.data(), &res, res_vect, 1.0,
+                                   1.0, t, &dt);
+    }
+    iter = iter + 1;
+    t = t + dt;
+    if (st) break;
+    if (!cfg.local_time_step && t >= cfg.tmax) break;
+  }
+  *t_io = t;
+  *iters = iter;
+  *res_out = res;
+  if (vp_out) std::memcpy(vp_out, w.vp.data(), w.vp.size() * sizeof(double));
+  return st;
+}
+
+// One compute_rhs_ns evaluation (rhs after flux limiting, first-order sum_lambda).
+int ns_rhs(const Mesh& m, const NsCfg& cfg, const double* sol, double* rhs, double* sum_lambda, double* vp,
+           double* cell_grad) {
+  NsWork w;
+  w.rhs.assign(5 * m.n_elems, 0.0);
+  w.rhs_o2.assign(5 * m.n_elems, 0.0);
+  w.sl.assign(m.n_elems, 0.0);
+  w.sl_o2.assign(m.n_elems, 0.0);
+  w.vp.assign(3 * m.n_vert, 0.0);
+  int st = compute_rhs_ns(m, cfg, sol, w);
+  std::memcpy(rhs, w.rhs.data(), w.rhs.size() * sizeof(double));
+  std::memcpy(sum_lambda, w.sl.data(), w.sl.size() * sizeof(double));
+  if (vp) std::memcpy(vp, w.vp.data(), w.vp.size() * sizeof(double));
+  if (cell_grad) std::memcpy(cell_grad, w.grad.data(), w.grad.size() * sizeof(double));
+  return st;
+}
+
+// ns_euler_exact_sol_module.F90:7-44 evaluated at the cell centroids, then
+// primit_to_conserv (ns_euler_module.F90:49-53).
+void init_gresho(const Mesh& m, double mach, double* sol) {
+  for (int i = 1; i <= m.n_elems; ++i) {
+    const double* x = &m.elem[i].coord[1];
+    double w[5];
+    double wg = 0.2, pg = 1.0 / (G * (mach * mach));
+    double r = fnorm2(x, 2);
+    if (r < wg) {
+      w[0] = 1.0;
+      w[1] = -5.0 * x[1];
+      w[2] = 5.0 * x[0];
+      w[3] = 0.0;
+      w[4] = pg + 12.5 * (r * r);
+    } else if (r > 1.0 * wg && r < 2.0 * wg) {
+      w[0] = 1.0;
+      w[1] = (5.0 - 2.0 / r) * x[1];
+      w[2] = (-5.0 + 2.0 / r) * x[0];
+      w[3] = 0.0;
+      w[4] = pg + 12.5 * (r * r) + 4.0 - 20.0 * r + 4.0 * std::log(5.0 * r);
+    } else {
+      w[0] = 1.0;
+      w[1] = w[2] = w[3] = 0.0;
+      w[4] = pg - 2.0 + 4.0 * std::log(2.0);
+    }
+    p2c(w, sol + 5 * (i - 1));
+  }
+}
+
+int oracle_pinv3(double* a9) {
+  double A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A[i][j] = a9[3 * i + j];
+  pinv3(A);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) a9[3 * i + j] = A[i][j];
+  return 0;
+}
+void oracle_lu3(double* a9, double* x, const double* b) {
+  double A[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) A[i][j] = a9[3 * i + j];
+  lu_solve3(A, x, b);
+}
+
+}  // namespace oracle
+
+using namespace oracle;
+struct OHandleNs;  // the mesh handle of oracle_capi.cpp
+namespace oracle {
+Mesh& handle_mesh(void* h);
+}
+
+extern "C" {
+
+static NsCfg make_cfg(const int* ic, const double* dc, const int* bc_type, const double* bc_val) {
+  NsCfg c;
+  c.scheme = ic[0];
+  c.second_order = ic[1];
+  c.method = ic[2];
+  c.bc_style = ic[3];
+  c.b2d = ic[4];
+  c.exclude_bound_vert = ic[5];
+  c.local_time_step = ic[6];
+  c.n_bc = ic[7];
+  c.cfl = dc[0];
+  c.tmax = dc[1];
+  c.bc_type = bc_type;
+  c.bc_val = bc_val;
+  return c;
+}
+
+// ic = {scheme, second_order, method, bc_style, b2d, exclude_bound_vert, local_time_step, n_bc}
+// dc = {cfl, tmax}
+int or_ns_rhs(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val,
+              const double* sol, double* rhs, double* sum_lambda, double* vp, double* grad) {
+  return ns_rhs(handle_mesh(h), make_cfg(ic, dc, bc_type, bc_val), sol, rhs, sum_lambda, vp, grad);
+}
+int or_ns_run(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val, double* sol,
+              int n_max_iter, double final_res, double* t_io, int* iters, double* res, double* res_vect, double* vp) {
+  return ns_run(handle_mesh(h), make_cfg(ic, dc, bc_type, bc_val), sol, n_max_iter, final_res, t_io, iters, res,
+                res_vect, vp);
+}
+void or_ns_gresho(void* h, double mach, double* sol) { init_gresho(handle_mesh(h), mach, sol); }
+void or_pinv3(double* a9) { oracle_pinv3(a9); }
+void or_lu3(double* a9, double* x, const double* b) { oracle_lu3(a9, x, b); }
+
+}  // extern "C"

@@ -54,6 +54,15 @@ SIGNATURES = {
     "subfv_lag_last_dt": (c_int, [P, PD]),
     "subfv_lag_step_host": (c_int, [P, PD]),
     "subfv_lag_profile_steps": (c_int, [P, c_int, PD]),
+    "subfv_compute_rhs_ns": (c_int, [P, P, PD, PD, PD, PD, PD]),
+    "subfv_ns_state_create": (c_int, [P, P, PD, c_dbl, C.POINTER(P)]),
+    "subfv_ns_state_destroy": (c_int, [P]),
+    "subfv_ns_advance": (c_int, [P, c_int, C.POINTER(c_int), PD]),
+    "subfv_ns_advance_async": (c_int, [P, c_int]),
+    "subfv_ns_sync": (c_int, [P, C.POINTER(c_int), PD]),
+    "subfv_ns_get_sol": (c_int, [P, PD]),
+    "subfv_ns_residuals": (c_int, [P, PD, PD, PD]),
+    "subfv_ns_init_gresho": (c_int, [P, c_dbl, PD]),
     "subfv_mesh_stream": (P, [P]),
 }
 

@@ -6,6 +6,7 @@
 
 #include "../../include/subfv.h"
 #include "common.cuh"
+#include "handles.cuh"
 #include "lagrange.cuh"
 #include "mesh_dev.cuh"
 #include "topology.h"
@@ -24,15 +25,6 @@ struct subfv_topology {
   Topology t;
 };
 
-// A device mesh plus the scratch buffers the stateless reference-shaped calls need.
-struct subfv_mesh {
-  DevMesh d;
-  double* stage = nullptr;  // host-layout staging, max(5*ne, 3*nv) doubles
-  double* sol6 = nullptr;   // [ne][6]
-  double* rhs6 = nullptr;   // [ne][6]
-  double* mass = nullptr;   // [ne]
-  LagScalars* sc = nullptr;
-};
 
 struct subfv_lag_state {
   subfv_mesh* m = nullptr;
@@ -48,6 +40,18 @@ struct subfv_lag_state {
 
 namespace subfv {
 const DevMesh& mesh_device_view(const subfv_mesh* m) { return m->d; }
+}  // namespace subfv
+
+namespace {
+int check_status(DevMesh& d);
+int clear_status(DevMesh& d);
+int ensure_scratch(subfv_mesh* m);
+}  // namespace
+
+namespace subfv {
+int handle_check_status(DevMesh& d) { return check_status(d); }
+int handle_clear_status(DevMesh& d) { return clear_status(d); }
+int handle_ensure_scratch(subfv_mesh* m) { return ensure_scratch(m); }
 }  // namespace subfv
 
 namespace {
@@ -181,6 +185,8 @@ int subfv_mesh_create_from_topology(const subfv_topology* tp, int b2d, subfv_mes
   d.vert_sub_elem_off = t.a("vert_sub_elem_off").data();
   d.vert_sub_elem = t.a("vert_sub_elem").data();
   d.vert_is_bound = t.a("vert_is_bound").data();
+  d.vert_elem_off = t.a("vert_elem_off").data();
+  d.vert_elem = t.a("vert_elem").data();
   return subfv_mesh_create(&d, out);
 }
 

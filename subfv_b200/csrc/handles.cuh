@@ -1,0 +1,21 @@
+// Opaque handle types of the C-ABI, shared by the translation units that implement it.
+#pragma once
+#include "../../include/subfv.h"
+#include "common.cuh"
+#include "mesh_dev.cuh"
+
+// A device mesh plus the scratch buffers the stateless reference-shaped calls need.
+struct subfv_mesh {
+  subfv::DevMesh d;
+  double* stage = nullptr;  // host-layout staging, max(5*ne, 3*nv) doubles
+  double* sol6 = nullptr;   // [ne][kRec] cell records
+  double* rhs6 = nullptr;   // [ne][kRhs]
+  double* mass = nullptr;   // [ne]
+  subfv::LagScalars* sc = nullptr;
+};
+
+namespace subfv {
+int handle_check_status(DevMesh& d);
+int handle_clear_status(DevMesh& d);
+int handle_ensure_scratch(subfv_mesh* m);
+}  // namespace subfv

@@ -150,7 +150,22 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
     }
   }
   m->ncsf = csf_off[ne];
+  std::vector<int> vel_off(nv + 1, 0), vel;
+  if (d->vert_elem_off && d->vert_elem) {
+    for (int v = 0; v <= nv; ++v) vel_off[v] = d->vert_elem_off[v];
+    vel.resize(vel_off[nv]);
+    for (int k = 0; k < vel_off[nv]; ++k) vel[k] = d->vert_elem[k] - 1;
+  }
+  std::vector<int> cse_sorted(ev_off[ne]);
+  for (int c = 0; c < ne; ++c) {
+    int b = ev_off[c], n = ev_off[c + 1] - b;
+    for (int k = 0; k < n; ++k) cse_sorted[b + k] = b + k;
+    std::sort(cse_sorted.begin() + b, cse_sorted.begin() + b + n,
+              [&](int a, int q) { return ev[a] < ev[q]; });
+  }
 
+  if (upload(&m->vel_off, vel_off, B, s) || upload(&m->vel, vel, B, s) || upload(&m->cse_sorted, cse_sorted, B, s))
+    return -1;
   if (upload(&m->x, x, B, s) || alloc(&m->vp, nv, B) || alloc(&m->vol_v, nv, B) || upload(&m->is_bound, isb, B, s) ||
       upload(&m->fvert, fvert, B, s) || upload(&m->flr, flr, B, s) || upload(&m->fsf, fsf, B, s) ||
       alloc(&m->fc, nf, B) || alloc(&m->fn, nf, B) || upload(&m->sf_face, sf_face, B, s) ||
@@ -171,7 +186,8 @@ void devmesh_free(DevMesh* m) {
   void* ptrs[] = {m->x, m->vp, m->vol_v, m->is_bound, m->fvert, m->flr, m->fsf, m->fc, m->fn,
                   m->sf_face, m->sf_vert, m->sf_se, m->sf_loc, m->sfn, m->se_elem, m->se_vert, m->se_loc,
                   m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
-                  m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status};
+                  m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
+                  m->vel_off, m->vel, m->cse_sorted};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (m->stream) cudaStreamDestroy(m->stream);

@@ -67,6 +67,11 @@ struct DevMesh {
   int* vse = nullptr;
   int* csf_off = nullptr;
   int* csf = nullptr;
+  // vertex -> cell lists (vert%elem_neigh), and each cell's subcells in ascending
+  // vertex order (the order the reference's node loop scatters into the cell)
+  int* vel_off = nullptr;
+  int* vel = nullptr;
+  int* cse_sorted = nullptr;
   // status word (StatusBits) and the stream the mesh's work runs on
   unsigned* status = nullptr;
   cudaStream_t stream = nullptr;

@@ -1,0 +1,931 @@
+// Explicit Euler residual path of subfvns on the GPU.
+//
+// Reference: src/ns/ns_euler_module.F90:151-609 (compute_euler_flux,
+// compute_rhs_around_vert, add_timedisc_and_solve), src/ns/ns_euler_rs_module.F90:154-422
+// (two_wave, multi_point, compute_lambdas_and_solve_nodal_velocity),
+// src/ns/ns_euler_recon_module.F90:8-601 (nodal and cell gradients, limiters,
+// reconstruction, boundary states, flux_limiting), src/ns/ns_euler_primitives_module.F90.
+//
+// Kernels of one residual evaluation (compute_rhs_ns):
+//   k_ns_node        one thread per vertex: reconstruct the left/right states of its
+//                    subfaces, run the 4-iteration nodal velocity solver (multi_point),
+//                    evaluate the subface fluxes and sum them per corner (subcell)
+//   k_ns_gather      one thread per cell: rhs = -sum of its corners' sums in ascending
+//                    vertex order (the reference's scatter order), no atomics; block min
+//                    of V / sum_lambda for the CFL step
+//   k_ns_nodal_grad  one thread per vertex: least-squares gradient, 3x3 pseudo-inverse
+//   k_ns_cell_grad   one thread per cell: method-4 weighting, physical slope limiter,
+//                    relaxed maximum principle
+// then per stage k_ns_timedisc (flux limiting blend, diagonal solve, positivity limiter,
+// residual partial sums), k_ns_finalize (one thread) and k_ns_apply.
+//
+// Plain FP64 (precision 0) follows the reference's evaluation order and is compiled
+// without FMA contraction, so it reproduces the CPU restatement bit for bit, except the
+// residual norms (res, res_vect), which are summed by a fixed tree of block partials.
+// Precision 1 evaluates reconstruction, limiters and subface fluxes in FP32; the nodal
+// velocity solver, the nodal gradient system and all sums stay FP64.
+#include <cstring>
+
+#include "ns.cuh"
+
+namespace subfv {
+
+NsParams ns_params_from(const subfv_ns_cfg& c) {
+  NsParams p{};
+  p.scheme = c.scheme;
+  p.second_order = c.second_order;
+  p.method = c.method;
+  p.bc_style = c.bc_style;
+  p.b2d = c.boundary_2d;
+  p.excl = c.exclude_bound_vert;
+  p.lts = c.local_time_step;
+  p.n_bc = c.n_bc;
+  for (int i = 0; i < 16; ++i) {
+    p.bc_type[i] = c.bc_type[i];
+    for (int k = 0; k < 5; ++k) p.bc_val[i][k] = c.bc_val[i][k];
+  }
+  p.cfl = c.cfl;
+  p.tmax = c.tmax;
+  p.precision = c.precision;
+  return p;
+}
+
+namespace {
+
+constexpr double G = 1.4;  // ns_global_data_module.F90:9
+
+__device__ inline double fmax2(double a, double b) { return b > a ? b : a; }
+__device__ inline double fmin2(double a, double b) { return b < a ? b : a; }
+template <class T>
+__device__ inline T tmax2(T a, T b) { return b > a ? b : a; }
+template <class T>
+__device__ inline T tmin2(T a, T b) { return b < a ? b : a; }
+
+template <class T>
+__device__ inline void p2c(const T* w, T* u) {
+  u[0] = w[0];
+  for (int k = 1; k < 4; ++k) u[k] = w[k] * w[0];
+  u[4] = w[4] / (T)(G - 1) + (T)0.5 * w[0] * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]);
+}
+template <class T>
+__device__ inline void c2p(const T* u, T* w) {
+  w[0] = u[0];
+  for (int k = 1; k < 4; ++k) w[k] = u[k] / u[0];
+  w[4] = (T)(G - 1) * (u[4] - (T)0.5 * w[0] * (w[1] * w[1] + w[2] * w[2] + w[3] * w[3]));
+}
+template <class T>
+__device__ inline T dotT(const T* a, const T* b) {
+  T s = 0;
+  s = s + a[0] * b[0];
+  s = s + a[1] * b[1];
+  s = s + a[2] * b[2];
+  return s;
+}
+__device__ inline double sound_speed_w(const double* w) { return sqrt(G * w[4] / w[0]); }
+
+__device__ inline void ld5(const double* U, int c, double* u) {
+  const double* r = U + kRec * (size_t)c;
+  for (int k = 0; k < 5; ++k) u[k] = r[k];
+}
+
+// ns_euler_primitives_module.F90:92-111
+__device__ double max_omega_for_positivity(const double* U, const double* dU) {
+  double omega = 1.0, US[5], WS[5];
+  for (int k = 0; k < 5; ++k) US[k] = U[k] + omega * dU[k];
+  c2p(US, WS);
+  bool pos = WS[0] > 1e-17 && WS[4] > 1e-17;
+  while (!pos && omega > 1e-6) {  // at most ~131 halvings by 0.9 before omega <= 1e-6
+    omega = omega * 0.9;
+    for (int k = 0; k < 5; ++k) US[k] = U[k] + omega * dU[k];
+    c2p(US, WS);
+    pos = WS[0] > 1e-17 && WS[4] > 1e-17;
+  }
+  return omega;
+}
+
+// Pseudo-inverse of a 3x3 matrix (A[r][c] = mat(r+1, c+1)) by one-sided Jacobi SVD,
+// six sweeps, singular values below 3e-12 * max discarded (the cut of
+// pseudo_inverse_inplace_lapack, linear_solver_module.F90:683-715).
+__device__ void pinv3(double A[3][3]) {
+  double U[3][3], V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) U[i][j] = A[i][j];
+  const int pr[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int sweep = 0; sweep < 6; ++sweep)
+    for (int r = 0; r < 3; ++r) {
+      const int p = pr[r][0], q = pr[r][1];
+      double al = 0.0, be = 0.0, ga = 0.0;
+      for (int i = 0; i < 3; ++i) {
+        al = al + U[i][p] * U[i][p];
+        be = be + U[i][q] * U[i][q];
+        ga = ga + U[i][p] * U[i][q];
+      }
+      if (!(fabs(ga) > 1e-15 * sqrt(al * be))) continue;
+      double zeta = (be - al) / (2.0 * ga);
+      double t = 1.0 / (fabs(zeta) + sqrt(1.0 + zeta * zeta));
+      if (zeta < 0.0) t = -t;
+      double c = 1.0 / sqrt(1.0 + t * t), s = c * t;
+      for (int i = 0; i < 3; ++i) {
+        double up = U[i][p], uq = U[i][q];
+        U[i][p] = c * up - s * uq;
+        U[i][q] = s * up + c * uq;
+        double vp = V[i][p], vq = V[i][q];
+        V[i][p] = c * vp - s * vq;
+        V[i][q] = s * vp + c * vq;
+      }
+    }
+  double sig[3], smax = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    double s = 0.0;
+    for (int i = 0; i < 3; ++i) s = s + U[i][k] * U[i][k];
+    sig[k] = sqrt(s);
+    smax = fmax2(smax, sig[k]);
+  }
+  const double tol = 3 * 1e-12 * smax;
+  double SUt[3][3];
+  for (int k = 0; k < 3; ++k)
+    for (int j = 0; j < 3; ++j) SUt[k][j] = sig[k] > tol ? (1.0 / sig[k]) * (U[j][k] / sig[k]) : 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = s + V[i][k] * SUt[k][j];
+      A[i][j] = s;
+    }
+}
+
+// LU with partial pivoting and the triangular solves, in the operation order of
+// LAPACK dgetrf2/dgetrs with reference BLAS (lu_solve_inplace_lapack, :643-657).
+__device__ void lu_solve3(double A[3][3], double* x, const double* b) {
+  const double sfmin = 2.2250738585072014e-308;
+  int ipiv[3];
+  for (int j = 0; j < 3; ++j) {
+    int p = j;
+    double amax = fabs(A[j][j]);
+    for (int i = j + 1; i < 3; ++i)
+      if (fabs(A[i][j]) > amax) {
+        amax = fabs(A[i][j]);
+        p = i;
+      }
+    ipiv[j] = p;
+    if (A[p][j] != 0.0) {
+      if (p != j)
+        for (int k = 0; k < 3; ++k) {
+          double t = A[j][k];
+          A[j][k] = A[p][k];
+          A[p][k] = t;
+        }
+      if (fabs(A[j][j]) >= sfmin) {
+        double r = 1.0 / A[j][j];
+        for (int i = j + 1; i < 3; ++i) A[i][j] = r * A[i][j];
+      } else {
+        for (int i = j + 1; i < 3; ++i) A[i][j] = A[i][j] / A[j][j];
+      }
+    }
+    for (int i = j + 1; i < 3; ++i)
+      for (int k = j + 1; k < 3; ++k) A[i][k] = A[i][k] - A[j][k] * A[i][j];
+  }
+  double y[3] = {b[0], b[1], b[2]};
+  for (int j = 0; j < 3; ++j)
+    if (ipiv[j] != j) {
+      double t = y[j];
+      y[j] = y[ipiv[j]];
+      y[ipiv[j]] = t;
+    }
+  for (int k = 0; k < 3; ++k)
+    if (y[k] != 0.0)
+      for (int i = k + 1; i < 3; ++i) y[i] = y[i] - y[k] * A[i][k];
+  for (int k = 2; k >= 0; --k)
+    if (y[k] != 0.0) {
+      y[k] = y[k] / A[k][k];
+      for (int i = 0; i < k; ++i) y[i] = y[i] - y[k] * A[i][k];
+    }
+  for (int k = 0; k < 3; ++k) x[k] = y[k];
+}
+
+// Boundary semantics on the device: flr.y >= 0 is the right cell; otherwise the face's
+// reference right_neigh is flr.y + 1 (0 = default wall, -tag = boundary condition tag).
+__device__ inline bool is_wall(const NsParams& P, int y) {
+  if (y >= 0) return false;
+  if (y == -1) return true;
+  return P.bc_type[-(y + 1) - 1] == 1;
+}
+
+// compute_right_state (:331-409) for walls, freestream and supersonic outflow;
+// sol_l / sol_r conservative, n the subface normal
+template <class T>
+__device__ void right_state(const NsParams& P, int y, const T* n, const T* sol_l, T* sol_r) {
+  int kind = y == -1 ? 1 : P.bc_type[-(y + 1) - 1];
+  if (kind == 1) {
+    for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+    T d = dotT(sol_r + 1, n);
+    for (int k = 1; k < 4; ++k) sol_r[k] = sol_r[k] - (T)2.0 * d * n[k - 1];
+  } else if (kind == 3) {
+    T w[5];
+    for (int k = 0; k < 5; ++k) w[k] = (T)P.bc_val[-(y + 1) - 1][k];
+    p2c(w, sol_r);
+  } else {
+    for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+  }
+}
+
+// reconstruct_lr_w (:427-451); grad records [15] with g[5*d + var] = grad(d+1, var+1)
+template <class T>
+__device__ void reconstruct(const DevMesh& m, const NsParams& P, const double* U, const double* grad, int v, int sf,
+                            int le, int y, bool so, double* wl_out, double* wr_out) {
+  T ul[5], wl[5], wr[5];
+  double u64[5];
+  ld5(U, le, u64);
+  for (int k = 0; k < 5; ++k) ul[k] = (T)u64[k];
+  c2p(ul, wl);
+  const double4 xv = m.x[v];
+  if (so) {
+    const double4 cc = m.cc[le];
+    const T dx[3] = {(T)(xv.x - cc.x), (T)(xv.y - cc.y), (T)(xv.z - cc.z)};
+    const double* g = grad + 15 * (size_t)le;
+    for (int k = 0; k < 5; ++k) {
+      T s = 0;
+      for (int d = 0; d < 3; ++d) s = s + (T)g[5 * d + k] * dx[d];
+      wl[k] = wl[k] + s;
+    }
+  }
+  if (y >= 0) {
+    T ur[5];
+    ld5(U, y, u64);
+    for (int k = 0; k < 5; ++k) ur[k] = (T)u64[k];
+    c2p(ur, wr);
+    if (so) {
+      const double4 cc = m.cc[y];
+      const T dx[3] = {(T)(xv.x - cc.x), (T)(xv.y - cc.y), (T)(xv.z - cc.z)};
+      const double* g = grad + 15 * (size_t)y;
+      for (int k = 0; k < 5; ++k) {
+        T s = 0;
+        for (int d = 0; d < 3; ++d) s = s + (T)g[5 * d + k] * dx[d];
+        wr[k] = wr[k] + s;
+      }
+    }
+  } else {
+    const double4 sn = m.sfn[sf];
+    const T n[3] = {(T)sn.x, (T)sn.y, (T)sn.z};
+    T uc[5], gh[5];
+    p2c(wl, uc);
+    right_state(P, y, n, uc, gh);
+    c2p(gh, wr);
+  }
+  for (int k = 0; k < 5; ++k) {
+    wl_out[k] = (double)wl[k];
+    wr_out[k] = (double)wr[k];
+  }
+}
+
+// two_wave (ns_euler_rs_module.F90:154-198)
+template <class T>
+__device__ void two_wave(const double* wl64, const double* wr64, const double* n64, double lr[2][5], double* sl_o,
+                         double* sr_o) {
+  T wl[5], wr[5], n[3];
+  for (int k = 0; k < 5; ++k) {
+    wl[k] = (T)wl64[k];
+    wr[k] = (T)wr64[k];
+  }
+  for (int d = 0; d < 3; ++d) n[d] = (T)n64[d];
+  T rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], al = sqrt((T)G * wl[4] / wl[0]), ul[5];
+  p2c(wl, ul);
+  T rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ar = sqrt((T)G * wr[4] / wr[0]), ur[5];
+  p2c(wr, ur);
+  T fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  T lam_l = tmax2(tmax2(al * rhol, sqrt(rhol * tmax2((T)0, pr - pl))), -rhol * (vnr - vnl));
+  T lam_r = tmax2(tmax2(ar * rhor, sqrt(rhor * tmax2((T)0, pl - pr))), -rhor * (vnr - vnl));
+  T sl = vnl - lam_l / rhol;
+  T sr = vnr + lam_r / rhor;
+  for (int k = 0; k < 5; ++k) {
+    T et = (sr * ur[k] - sl * ul[k] - (fr[k] - fl[k])) / (sr - sl);
+    T f = (T)0.5 * (fl[k] + fr[k]) - (T)0.5 * (fabs(sl) * (et - ul[k]) + fabs(sr) * (ur[k] - et));
+    lr[0][k] = (double)f;
+    lr[1][k] = (double)(-f);
+  }
+  *sl_o = (double)sl;
+  *sr_o = (double)sr;
+}
+
+// multi_point (ns_euler_rs_module.F90:200-286); false on a negative star density
+template <class T>
+__device__ bool multi_point(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
+                            double vn_nodal, double lam_l64, double lam_r64, double* sl_o, double* sr_o) {
+  T wl[5], wr[5], n[3];
+  for (int k = 0; k < 5; ++k) {
+    wl[k] = (T)wl64[k];
+    wr[k] = (T)wr64[k];
+  }
+  for (int d = 0; d < 3; ++d) n[d] = (T)n64[d];
+  const T lam_l = (T)lam_l64, lam_r = (T)lam_r64;
+  T rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], ul[5];
+  p2c(wl, ul);
+  T el = ul[4] / rhol;
+  T rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ur[5];
+  p2c(wr, ur);
+  T er = ur[4] / rhor;
+  T fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  T v_et = (T)vn_nodal;
+  T rhol_et = (T)1.0 / ((T)1.0 / rhol + (v_et - vnl) / lam_l);
+  T pl_bar = pl - lam_l * (v_et - vnl);
+  T sle[5], sre[5];
+  sle[0] = rhol_et;
+  for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (wl[k] + (v_et - vnl) * n[k - 1]);
+  sle[4] = rhol_et * (el + (pl * vnl - pl_bar * v_et) / lam_l);
+  T rhor_et = (T)1.0 / ((T)1.0 / rhor + (vnr - v_et) / lam_r);
+  T pr_bar = pr + lam_r * (v_et - vnr);
+  sre[0] = rhor_et;
+  for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (wr[k] + (v_et - vnr) * n[k - 1]);
+  sre[4] = rhor_et * (er + (pr_bar * v_et - pr * vnr) / lam_r);
+  bool ok = !(rhol_et < (T)0 || rhor_et < (T)0);
+  T sl = vnl - lam_l / rhol;
+  T sr = vnr + lam_r / rhor;
+  const T e[5] = {(T)0, n[0], n[1], n[2], v_et};
+  for (int k = 0; k < 5; ++k) {
+    T base = (T)0.5 * (fl[k] + fr[k]) -
+             (T)0.5 * (fabs(sl) * (sle[k] - ul[k]) + fabs(v_et) * (sre[k] - sle[k]) + fabs(sr) * (ur[k] - sre[k]));
+    T jump = (T)0.5 * (pr_bar - pl_bar) * e[k];
+    lr[0][k] = (double)(base - jump);
+    lr[1][k] = (double)(-(base + jump));
+  }
+  *sl_o = (double)sl;
+  *sr_o = (double)sr;
+  return ok;
+}
+
+// compute_lambdas_and_solve_nodal_velocity (ns_euler_rs_module.F90:288-422), FP64
+__device__ void nodal_velocity(const DevMesh& m, const NsParams& P, int v, int p0, int nsfn,
+                               const double (*wlr)[10], double (*lam)[2], double* vbar, double* vnode) {
+  double Bp[3] = {0, 0, 0};  // wall_normal (ns_euler_primitives_module.F90:162-190)
+  for (int j = 0; j < nsfn; ++j) {
+    int sf = m.vsf[p0 + j];
+    int y = m.flr[m.sf_face[sf]].y;
+    if (y < 0) {
+      double4 sn = m.sfn[sf];
+      if (!(P.b2d && fabs(sn.z) > 1e-12))
+        if (y == -1 || P.bc_type[-(y + 1) - 1] == 1) {
+          Bp[0] = Bp[0] + sn.w * sn.x;
+          Bp[1] = Bp[1] + sn.w * sn.y;
+          Bp[2] = Bp[2] + sn.w * sn.z;
+        }
+    }
+  }
+  vnode[0] = vnode[1] = vnode[2] = 0.0;
+  for (int iter = 1; iter <= 4; ++iter) {
+    double mat[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Rp[3] = {0, 0, 0};
+    for (int j = 0; j < nsfn; ++j) {
+      int sf = m.vsf[p0 + j];
+      int y = m.flr[m.sf_face[sf]].y;
+      double4 sn = m.sfn[sf];
+      const double n[3] = {sn.x, sn.y, sn.z};
+      double area = sn.w;
+      const double* wl = wlr[j];
+      const double* wr = wlr[j] + 5;
+      double rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], al = sound_speed_w(wl);
+      double rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr);
+      double lam_l = lam[j][0], lam_r = lam[j][1];
+      const bool wall = is_wall(P, y);
+      if (iter == 1) {
+        lam_l = fmax2(fmax2(fmax2(lam_l, al * rhol), sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+        lam_r = fmax2(fmax2(fmax2(lam_r, ar * rhor), sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+        vbar[j] = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(vbar[j] - vnl) / al)));
+        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (vbar[j] - vnr) / ar)));
+      } else if (wall && P.bc_style == 1) {
+        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(vbar[j] - vnl) / al)));
+        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (vbar[j] - vnr) / ar)));
+      } else {
+        double v_et = dotT(vnode, n);
+        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(v_et - vnl) / al)));
+        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (v_et - vnr) / ar)));
+      }
+      lam[j][0] = lam_l;
+      lam[j][1] = lam_r;
+      vbar[j] = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+      if (!wall || P.bc_style == 0 || P.bc_style == 2) {
+        double w = (lam_r + lam_l) * area;
+        for (int d = 0; d < 3; ++d)
+          for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + w * (n[d] * n[e]);
+      }
+      if (!wall || P.bc_style == 0) {
+        double q = area * (lam_r + lam_l) * vbar[j];
+        for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
+      } else if (P.bc_style == 2) {
+        if (!P.b2d || fabs(n[2]) < 1e-8) {
+          double q = area * pl;
+          for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
+        }
+      }
+    }
+    if (P.bc_style == 2) {
+      double bmax = fmax2(fmax2(fabs(Bp[0]), fabs(Bp[1])), fabs(Bp[2]));
+      if (bmax > 1e-8) {
+        pinv3(mat);
+        double mr[3], mb[3], r2[3];
+        for (int d = 0; d < 3; ++d) {
+          double s = 0.0, t = 0.0;
+          for (int e = 0; e < 3; ++e) {
+            s = s + mat[d][e] * Rp[e];
+            t = t + mat[d][e] * Bp[e];
+          }
+          mr[d] = s;
+          mb[d] = t;
+        }
+        double p_bound = dotT(mr, Bp) / dotT(mb, Bp);
+        for (int d = 0; d < 3; ++d) r2[d] = Rp[d] - p_bound * Bp[d];
+        for (int d = 0; d < 3; ++d) {
+          double s = 0.0;
+          for (int e = 0; e < 3; ++e) s = s + mat[d][e] * r2[e];
+          vnode[d] = s;
+        }
+        double f = dotT(vnode, Bp) / dotT(Bp, Bp);
+        for (int d = 0; d < 3; ++d) vnode[d] = vnode[d] - f * Bp[d];
+      } else {
+        lu_solve3(mat, vnode, Rp);
+      }
+    } else {
+      pinv3(mat);
+      for (int d = 0; d < 3; ++d) {
+        double s = 0.0;
+        for (int e = 0; e < 3; ++e) s = s + mat[d][e] * Rp[e];
+        vnode[d] = s;
+      }
+    }
+  }
+}
+
+// compute_rhs_around_vert (ns_euler_module.F90:341-519) for one vertex; writes the
+// corner sums of the vertex's own subcells to fs (kNsFs doubles per subcell).
+template <class T>
+__global__ void __launch_bounds__(128) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
+                                                 const double* __restrict__ grad, double* __restrict__ fs, int so,
+                                                 const NsScalars* sc) {
+  if (sc && sc->done) return;
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  const int p0 = m.vsf_off[v], nsfn = m.vsf_off[v + 1] - p0;
+  const int q0 = m.vse_off[v], nsen = m.vse_off[v + 1] - q0;
+  if (nsfn > kNsMaxSf || nsen > kNsMaxSe) {
+    atomicOr(m.status, kErrIndex);
+    return;
+  }
+  double wlr[kNsMaxSf][10];
+  double lam[kNsMaxSf][2];
+  double vbar[kNsMaxSf];
+  for (int j = 0; j < nsfn; ++j) {
+    const int sf = m.vsf[p0 + j];
+    const int2 lr = m.flr[m.sf_face[sf]];
+    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, wlr[j], wlr[j] + 5);
+    lam[j][0] = lam[j][1] = 0.0;
+    vbar[j] = 0.0;
+  }
+  const bool excl = m.is_bound[v] && P.excl;
+  double vn3[3] = {0.0, 0.0, 0.0};
+  if (P.scheme == 1) {
+    if (!excl) nodal_velocity(m, P, v, p0, nsfn, wlr, lam, vbar, vn3);
+    m.vp[v] = make_double4(vn3[0], vn3[1], vn3[2], 0.0);
+  }
+  double fsv[kNsMaxSe][5], slv[kNsMaxSe];
+  for (int j = 0; j < nsen; ++j) {
+    slv[j] = 0.0;
+    for (int k = 0; k < 5; ++k) fsv[j][k] = 0.0;
+  }
+  bool bad = false;
+  int rse_loc = 0;
+  for (int j = 0; j < nsfn; ++j) {
+    const int sf = m.vsf[p0 + j];
+    const int y = m.flr[m.sf_face[sf]].y;
+    const int2 se = m.sf_se[sf];
+    const int lse_loc = m.se_loc[se.x];
+    if (se.y >= 0) rse_loc = m.se_loc[se.y];
+    const double4 sn = m.sfn[sf];
+    const double n[3] = {sn.x, sn.y, sn.z};
+    double lr[2][5], sl, sr;
+    if (P.scheme == 1 && !excl) {
+      const double vn = is_wall(P, y) ? 0.0 : dotT(vn3, n);
+      if (!multi_point<T>(wlr[j], wlr[j] + 5, n, lr, vn, lam[j][0], lam[j][1], &sl, &sr)) bad = true;
+    } else {
+      two_wave<T>(wlr[j], wlr[j] + 5, n, lr, &sl, &sr);
+    }
+    if (m.se_vert[se.x] == v && lse_loc < nsen) {
+      slv[lse_loc] = slv[lse_loc] + sn.w * fmax2(0.0, -sl);
+      for (int k = 0; k < 5; ++k) fsv[lse_loc][k] = fsv[lse_loc][k] + sn.w * lr[0][k];
+      if (se.y >= 0 && m.se_vert[se.y] == v && rse_loc < nsen) {
+        slv[rse_loc] = slv[rse_loc] + sn.w * fmax2(0.0, sr);
+        for (int k = 0; k < 5; ++k) fsv[rse_loc][k] = fsv[rse_loc][k] + sn.w * lr[1][k];
+      }
+    }
+  }
+  if (bad) atomicOr(m.status, kErrNegDensity);
+  for (int j = 0; j < nsen; ++j) {
+    const int s = m.vse[q0 + j];
+    if (m.se_vert[s] != v) continue;  // a periodic image's subcell: its sums are zero here
+    double* out = fs + kNsFs * (size_t)s;
+    for (int k = 0; k < 5; ++k) out[k] = fsv[j][k];
+    out[5] = slv[j];
+  }
+}
+
+__device__ inline double warp_min(double x) {
+  for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
+  return x;
+}
+__device__ inline double warp_sum_tree(double x) {
+  for (int o = 16; o > 0; o >>= 1) x = x + __shfl_down_sync(0xffffffffu, x, o);
+  return x;
+}
+
+// compute_euler_flux scatter (:320-336) as a gather: rhs = 0 - corners in ascending
+// vertex order; sum_lambda = 1e-12 + corners. Block min of V / sum_lambda into *dtred.
+__global__ void __launch_bounds__(128) k_ns_gather(DevMesh m, const double* __restrict__ fs, double* __restrict__ rhs,
+                                                   NsScalars* sc, int reduce) {
+  if (sc && sc->done) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double dmin = 1e10;
+  if (c < m.ne) {
+    double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, sl = 1e-12;
+    for (int q = m.ev_off[c]; q < m.ev_off[c + 1]; ++q) {
+      const double* f = fs + kNsFs * (size_t)m.cse_sorted[q];
+      for (int k = 0; k < 5; ++k) r[k] = r[k] - f[k];
+      sl = sl + f[5];
+    }
+    double* o = rhs + kRhs * (size_t)c;
+    for (int k = 0; k < 5; ++k) o[k] = r[k];
+    o[5] = sl;
+    dmin = m.vol[c] / sl;
+  }
+  if (reduce) {
+    __shared__ double wm[4];
+    double x = warp_min(dmin);
+    if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      x = fmin(fmin(wm[0], wm[1]), fmin(wm[2], wm[3]));
+      atomic_min_pos(&sc->dtred, x);
+    }
+  }
+}
+
+// compute_nodal_grad (ns_euler_recon_module.F90:453-490); ng[15] = g[5*d + var]
+__global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* __restrict__ U,
+                                                       double* __restrict__ ngrad, const NsScalars* sc) {
+  if (sc && sc->done) return;
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  double g[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
+  double mat[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int p = m.vsf_off[v]; p < m.vsf_off[v + 1]; ++p) {
+    const int sf = m.vsf[p];
+    const int2 lr = m.flr[m.sf_face[sf]];
+    if (lr.y < 0) continue;
+    double ul[5], ur[5], wl[5], wr[5];
+    ld5(U, lr.x, ul);
+    ld5(U, lr.y, ur);
+    c2p(ul, wl);
+    c2p(ur, wr);
+    const double4 sn = m.sfn[sf];
+    const double n[3] = {sn.x, sn.y, sn.z};
+    const double4 cl = m.cc[lr.x], cr = m.cc[lr.y];
+    const double dxc[3] = {cr.x - cl.x, cr.y - cl.y, cr.z - cl.z};
+    for (int d = 0; d < 3; ++d)
+      for (int k = 0; k < 5; ++k) g[d][k] = g[d][k] + sn.w * (n[d] * (wr[k] - wl[k]));
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + sn.w * (n[d] * dxc[e]);
+  }
+  pinv3(mat);
+  const bool bnd = m.is_bound[v] != 0;
+  double* o = ngrad + 15 * (size_t)v;
+  for (int d = 0; d < 3; ++d)
+    for (int k = 0; k < 5; ++k) {
+      double s = 0.0;
+      for (int e = 0; e < 3; ++e) s = s + mat[d][e] * g[e][k];
+      o[5 * d + k] = bnd ? 0.0 : s;
+    }
+}
+
+// compute_cell_grad_method_4 + physical_slope_limiter + relaxed_maximum_principle
+template <class T>
+__global__ void __launch_bounds__(128) k_ns_cell_grad(DevMesh m, NsParams P, const double* __restrict__ U,
+                                                      const double* __restrict__ ngrad, double* __restrict__ grad,
+                                                      const NsScalars* sc) {
+  if (sc && sc->done) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  double* go = grad + 15 * (size_t)c;
+  if (P.method == 0 || P.method == 1) {
+    for (int i = 0; i < 15; ++i) go[i] = 0.0;
+    return;
+  }
+  const T eps = (T)1e-3, tol = (T)1e-8;
+  T g[15];
+  T ws[5] = {0, 0, 0, 0, 0};
+  for (int i = 0; i < 15; ++i) g[i] = 0;
+  const int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
+  for (int j = 0; j < nvc; ++j) {
+    const int v = m.ev[vb + j];
+    const double* ng = ngrad + 15 * (size_t)v;
+    const T vol = (T)m.vol_v[v];
+    for (int k = 0; k < 5; ++k) {
+      T oi;
+      {
+        T a[3] = {(T)ng[k], (T)ng[5 + k], (T)ng[10 + k]};
+        T scale = 1, res = 0;
+        for (int i = 0; i < 3; ++i)
+          if (a[i] != (T)0) {
+            T ax = fabs(a[i]);
+            if (ax > scale) {
+              T q = scale / ax;
+              res = (T)1 + res * q * q;
+              scale = ax;
+            } else {
+              T q = ax / scale;
+              res += q * q;
+            }
+          }
+        oi = scale * sqrt(res);
+      }
+      T w = vol / (eps + oi);
+      for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] + w * (T)ng[5 * d + k];
+      ws[k] = ws[k] + w;
+    }
+  }
+  for (int k = 0; k < 5; ++k)
+    for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
+  double u0[5];
+  ld5(U, c, u0);
+  T uu[5], w0[5];
+  for (int k = 0; k < 5; ++k) uu[k] = (T)u0[k];
+  c2p(uu, w0);
+  const double4 ce = m.cc[c];
+  T omega = 1;
+  for (int j = 0; j < nvc; ++j) {  // physical_slope_limiter
+    const double4 xv = m.x[m.ev[vb + j]];
+    const T dx[3] = {(T)(xv.x - ce.x), (T)(xv.y - ce.y), (T)(xv.z - ce.z)};
+    T dw0 = 0, dw4 = 0;
+    for (int d = 0; d < 3; ++d) dw0 = dw0 + g[5 * d] * dx[d];
+    for (int d = 0; d < 3; ++d) dw4 = dw4 + g[5 * d + 4] * dx[d];
+    if (dw0 < (T)0) omega = tmin2(omega, tmax2((T)0, w0[0] / (tol - dw0)));
+    if (dw4 < (T)0) omega = tmin2(omega, tmax2((T)0, w0[4] / (tol - dw4)));
+  }
+  for (int i = 0; i < 15; ++i) g[i] = omega * g[i];
+  T rmin = (T)1e100, rmax = 0, pmin = (T)1e100, pmax = 0;  // relaxed_maximum_principle
+  if (sizeof(T) == 4) rmin = pmin = (T)3.0e38f;
+  for (int j = 0; j < nvc; ++j) {
+    const int v = m.ev[vb + j];
+    for (int q = m.vel_off[v]; q < m.vel_off[v + 1]; ++q) {
+      double un[5];
+      ld5(U, m.vel[q], un);
+      T ut[5], w[5];
+      for (int k = 0; k < 5; ++k) ut[k] = (T)un[k];
+      c2p(ut, w);
+      pmin = tmin2(pmin, w[4]);
+      pmax = tmax2(pmax, w[4]);
+      rmin = tmin2(rmin, w[0]);
+      rmax = tmax2(rmax, w[0]);
+    }
+  }
+  pmin = ((T)1.0 - (T)1e-2) * pmin;
+  rmin = ((T)1.0 - (T)1e-2) * rmin;
+  pmax = ((T)1.0 + (T)1e-2) * pmax;
+  rmax = ((T)1.0 + (T)1e-2) * rmax;
+  omega = 1;
+  for (int j = 0; j < nvc; ++j) {
+    const double4 xv = m.x[m.ev[vb + j]];
+    const T dx[3] = {(T)(xv.x - ce.x), (T)(xv.y - ce.y), (T)(xv.z - ce.z)};
+    T dw0 = 0, dw4 = 0;
+    for (int d = 0; d < 3; ++d) dw0 = dw0 + g[5 * d] * dx[d];
+    for (int d = 0; d < 3; ++d) dw4 = dw4 + g[5 * d + 4] * dx[d];
+    if (dw0 < (T)0)
+      omega = tmin2(omega, tmax2((T)0, (w0[0] - rmin) / (tol - dw0)));
+    else
+      omega = tmin2(omega, tmax2((T)0, -(w0[0] - rmax) / (tol + dw0)));
+    if (dw4 < (T)0)
+      omega = tmin2(omega, tmax2((T)0, (w0[4] - pmin) / (tol - dw4)));
+    else
+      omega = tmin2(omega, tmax2((T)0, -(w0[4] - pmax) / (tol + dw4)));
+  }
+  for (int i = 0; i < 15; ++i) go[i] = (double)(omega * g[i]);
+}
+
+constexpr int kTdBlock = 128;
+
+// flux_limiting (ns_euler_recon_module.F90:560-601) and the per-cell part of
+// add_timedisc_and_solve (ns_euler_module.F90:546-580). U_rhs: the state the residual
+// was evaluated at; U_td: the state being advanced. Writes delta, per-block omega min
+// (atomic on the bit pattern) and per-block residual partial sums (res, res_vect(5)).
+__global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P, const double* __restrict__ U_rhs,
+                                                          const double* __restrict__ rhs1,
+                                                          const double* __restrict__ rhs2,
+                                                          const double* __restrict__ U_td,
+                                                          double* __restrict__ delta, double* __restrict__ partial,
+                                                          NsScalars* sc, double a1, double a2) {
+  if (sc->done) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const double dt_fl = P.cfl * sc->dtred;
+  double dt = P.cfl * sc->dtred;
+  if (!P.lts) dt = fmin2(P.tmax - sc->t + 1e-12, dt);
+  double om = 1.0, rn = 0.0, rv[5] = {0, 0, 0, 0, 0};
+  if (c < m.ne) {
+    const double V = m.vol[c];
+    const double* r1 = rhs1 + kRhs * (size_t)c;
+    double r[5];
+    for (int k = 0; k < 5; ++k) r[k] = r1[k];
+    if (rhs2) {
+      const double* r2 = rhs2 + kRhs * (size_t)c;
+      const double den = V / dt_fl + r1[5];
+      double us[5], Ub[5], dU[5];
+      ld5(U_rhs, c, us);
+      for (int k = 0; k < 5; ++k) {
+        Ub[k] = us[k] + r[k] / den;
+        dU[k] = (r2[k] - r[k]) / den;
+      }
+      const double w = fmin2(1.0, max_omega_for_positivity(Ub, dU));
+      for (int k = 0; k < 5; ++k) r[k] = r[k] + w * (r2[k] - r[k]);
+    }
+    for (int k = 0; k < 5; ++k) rv[k] = r[k] * r[k];
+    double u[5], d5[5], ad[5];
+    ld5(U_td, c, u);
+    const double s = a1 * (V / dt + 0.0);  // sum_lambda is zeroed once dt is known
+    for (int k = 0; k < 5; ++k) {
+      const double rr = r[k] + s * u[k];
+      d5[k] = rr / s - u[k];
+      ad[k] = a2 * d5[k];
+    }
+    om = max_omega_for_positivity(u, ad);
+    {  // norm2(delta): gfortran's scaled sum of squares
+      double scale = 1.0, res = 0.0;
+      for (int k = 0; k < 5; ++k)
+        if (d5[k] != 0.0) {
+          double ax = fabs(d5[k]);
+          if (ax > scale) {
+            double q = scale / ax;
+            res = 1.0 + res * q * q;
+            scale = ax;
+          } else {
+            double q = ax / scale;
+            res += q * q;
+          }
+        }
+      rn = scale * sqrt(res);
+    }
+    double* dl = delta + 5 * (size_t)c;
+    for (int k = 0; k < 5; ++k) dl[k] = d5[k];
+  }
+  __shared__ double sh[6][kTdBlock / 32];
+  __shared__ double shm[kTdBlock / 32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double x = warp_min(om);
+  if (lane == 0) shm[wid] = x;
+  double vals[6] = {rn, rv[0], rv[1], rv[2], rv[3], rv[4]};
+  for (int i = 0; i < 6; ++i) {
+    double y = warp_sum_tree(vals[i]);
+    if (lane == 0) sh[i][wid] = y;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double mn = shm[0];
+    for (int w = 1; w < kTdBlock / 32; ++w) mn = fmin(mn, shm[w]);
+    atomic_min_pos(&sc->omega, mn);
+    for (int i = 0; i < 6; ++i) {
+      double s = sh[i][0];
+      for (int w = 1; w < kTdBlock / 32; ++w) s = s + sh[i][w];
+      partial[6 * (size_t)blockIdx.x + i] = s;
+    }
+  }
+}
+
+// scalar tail of add_timedisc_and_solve (:582-608); last_stage also advances t
+__global__ void k_ns_finalize(NsScalars* sc, NsParams P, const double* __restrict__ partial, int nblocks,
+                              unsigned* status, int last_stage) {
+  if (sc->done) {
+    sc->skip = 1;
+    return;
+  }
+  double dt = P.cfl * sc->dtred;
+  if (!P.lts) dt = fmin2(P.tmax - sc->t + 1e-12, dt);
+  double res = 0.0, rv[5] = {0, 0, 0, 0, 0};
+  for (int b = 0; b < nblocks; ++b) {
+    res = res + partial[6 * (size_t)b];
+    for (int k = 0; k < 5; ++k) rv[k] = rv[k] + partial[6 * (size_t)b + 1 + k];
+  }
+  const double omega = sc->omega;
+  if (omega <= 1e-6) atomicOr(status, kErrBadOmega);
+  if (!P.lts && omega < 1.0) dt = (1.0 - omega) * dt;
+  sc->res = res;
+  for (int k = 0; k < 5; ++k) sc->resv[k] = sqrt(rv[k]);
+  sc->dt = dt;
+  sc->skip = 0;
+  sc->dtred = 1e10;  // the next stage's reductions start afresh
+  if (last_stage) {
+    sc->t = sc->t + dt;
+    sc->steps += 1;
+    sc->done = ((!P.lts && sc->t >= P.tmax) || !(res > sc->final_res)) ? 1 : 0;
+  }
+}
+
+// sol = sol + a2*omega*delta (:608); U_out may be U_td
+__global__ void k_ns_apply(DevMesh m, const double* __restrict__ U_td, const double* __restrict__ delta,
+                           double* __restrict__ U_out, NsScalars* sc, double a2) {
+  if (sc->skip) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  const double omega = sc->omega;
+  const double* u = U_td + kRec * (size_t)c;
+  double* o = U_out + kRec * (size_t)c;
+  const double* d = delta + 5 * (size_t)c;
+  bool fin = true;
+  for (int k = 0; k < 5; ++k) {
+    o[k] = u[k] + a2 * omega * d[k];
+    fin = fin && isfinite(o[k]);
+  }
+  if (!fin) atomicOr(m.status, kErrNonFinite);
+  if (!(o[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
+}
+
+__global__ void k_ns_reset_omega(NsScalars* sc) { sc->omega = 1.0; }
+
+// flux_limiting alone (ns_euler_recon_module.F90:560-601): rhs1 <- blend(rhs1, rhs2)
+__global__ void k_ns_flux_limiting(DevMesh m, NsParams P, const double* __restrict__ U, double* __restrict__ rhs1,
+                                   const double* __restrict__ rhs2, const NsScalars* sc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  const double dt_fl = P.cfl * sc->dtred;
+  double* r1 = rhs1 + kRhs * (size_t)c;
+  const double* r2 = rhs2 + kRhs * (size_t)c;
+  const double den = m.vol[c] / dt_fl + r1[5];
+  double us[5], Ub[5], dU[5];
+  ld5(U, c, us);
+  for (int k = 0; k < 5; ++k) {
+    Ub[k] = us[k] + r1[k] / den;
+    dU[k] = (r2[k] - r1[k]) / den;
+  }
+  const double w = fmin2(1.0, max_omega_for_positivity(Ub, dU));
+  for (int k = 0; k < 5; ++k) r1[k] = r1[k] + w * (r2[k] - r1[k]);
+}
+
+__global__ void k_ns_pack(int n, const double* __restrict__ s5, double* __restrict__ U) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  double* r = U + kRec * (size_t)c;
+  for (int k = 0; k < 5; ++k) r[k] = s5[5 * (size_t)c + k];
+  r[5] = r[6] = r[7] = 0.0;
+}
+
+}  // namespace
+
+int ns_partial_blocks(const DevMesh& m) { return grid_for(m.ne, kTdBlock); }
+
+void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* U, double* rhs1, const double* rhs2,
+                             const NsScalars* sc) {
+  k_ns_flux_limiting<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, P, U, rhs1, rhs2, sc);
+}
+
+void launch_ns_pack(const DevMesh& m, const double* s5, double* U) {
+  k_ns_pack<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m.ne, s5, U);
+}
+
+void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double* fs, double* rhs1, double* rhs2,
+                   double* ngrad, double* grad, NsScalars* sc) {
+  const int gv = grid_for(m.nv, 128), gc = grid_for(m.ne, 128);
+  if (P.precision == 1)
+    k_ns_node<float><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 0, sc);
+  else
+    k_ns_node<double><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 0, sc);
+  k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs1, sc, sc ? 1 : 0);
+  if (P.second_order) {
+    k_ns_nodal_grad<<<gv, 128, 0, m.stream>>>(m, U, ngrad, sc);
+    if (P.precision == 1)
+      k_ns_cell_grad<float><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+    else
+      k_ns_cell_grad<double><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+    if (P.precision == 1)
+      k_ns_node<float><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 1, sc);
+    else
+      k_ns_node<double><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 1, sc);
+    k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs2, sc, 0);
+  }
+}
+
+void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs, const double* rhs1,
+                        const double* rhs2, const double* U_td, double* U_out, double* delta, double* partial,
+                        NsScalars* sc, double a1, double a2, int last_stage) {
+  const int nb = ns_partial_blocks(m);
+  k_ns_timedisc<<<nb, kTdBlock, 0, m.stream>>>(m, P, U_rhs, rhs1, P.second_order ? rhs2 : nullptr, U_td, delta,
+                                               partial, sc, a1, a2);
+  k_ns_finalize<<<1, 1, 0, m.stream>>>(sc, P, partial, nb, m.status, last_stage);
+  k_ns_apply<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, U_td, delta, U_out, sc, a2);
+  k_ns_reset_omega<<<1, 1, 0, m.stream>>>(sc);
+}
+
+}  // namespace subfv

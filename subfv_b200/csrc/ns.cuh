@@ -1,0 +1,46 @@
+// Explicit Euler (subfvns) on the GPU: launchers and device-side parameter blocks.
+#pragma once
+#include "../../include/subfv.h"
+#include "common.cuh"
+#include "mesh_dev.cuh"
+
+namespace subfv {
+
+constexpr int kNsMaxSf = 32;  // subfaces around a vertex (a 3-D hex vertex has 12)
+constexpr int kNsMaxSe = 16;  // subcells around a vertex (a 3-D hex vertex has 8)
+constexpr int kNsFs = 6;      // per-subcell record: five corner flux sums and the wave-speed sum
+
+struct NsParams {
+  int scheme, second_order, method, bc_style, b2d, excl, lts, n_bc;
+  int bc_type[16];
+  double bc_val[16][5];
+  double cfl, tmax;
+  int precision;
+};
+
+struct NsScalars {
+  double dtred;    // running min of V / sum_lambda of the current stage (starts at 1e10)
+  double omega;    // running min of the positivity limiter (starts at 1)
+  double dt;       // time step of the last stage (after the omega correction)
+  double t, final_res;
+  double res, resv[5];
+  unsigned long long steps;
+  int done, skip;
+};
+
+NsParams ns_params_from(const subfv_ns_cfg& c);
+
+// One residual evaluation at state U (records of kRec doubles): rhs1/sl (first order),
+// and for second order ngrad, grad, rhs2. rhs records: kRhs doubles (5 + sum_lambda).
+void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double* fs, double* rhs1, double* rhs2,
+                   double* ngrad, double* grad, NsScalars* sc);
+// flux limiting + add_timedisc_and_solve + update (stage coefficients a1, a2)
+void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs, const double* rhs1,
+                        const double* rhs2, const double* U_td, double* U_out, double* delta, double* partial,
+                        NsScalars* sc, double a1, double a2, int last_stage);
+void launch_ns_pack(const DevMesh& m, const double* s5, double* U);
+void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* U, double* rhs1, const double* rhs2,
+                             const NsScalars* sc);
+int ns_partial_blocks(const DevMesh& m);
+
+}  // namespace subfv

@@ -1,0 +1,137 @@
+"""Host mirror of the reference's explicit Euler path (subfvns).
+
+compute_rhs_ns mirrors the contained procedure of src/ns/ns_main.F90:130-179 (no
+diffusion); NsState runs the time loop of ns_main.F90:83-107 device-resident, first
+order or the two-stage scheme, with the multi-point nodal solver
+(src/ns/ns_euler_rs_module.F90:200-422) or the two-wave flux (:154-198). Conservative
+state sol(5, n_elems) = (rho, rho u, rho v, rho w, E), numpy (n_elems, 5).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, f64, pd
+from .mesh import Mesh
+
+SCHEME_MULTI_POINT, SCHEME_TWO_WAVE = 1, 4  # ns_global_data_module.F90:67-70
+BC_WALL, BC_FREESTREAM, BC_OUTFLOW_SUPERSONIC = 1, 3, 4
+
+
+class NsCfgC(C.Structure):
+    _fields_ = [("scheme", C.c_int32), ("second_order", C.c_int32), ("method", C.c_int32),
+                ("bc_style", C.c_int32), ("boundary_2d", C.c_int32), ("exclude_bound_vert", C.c_int32),
+                ("local_time_step", C.c_int32), ("n_bc", C.c_int32), ("bc_type", C.c_int32 * 16),
+                ("bc_val", (C.c_double * 5) * 16), ("cfl", C.c_double), ("tmax", C.c_double),
+                ("precision", C.c_int32)]
+
+
+@dataclass
+class NsConfig:
+    """The namelist keys of ns_global_data_module.F90:177-213 that the residual path reads."""
+
+    scheme: int = SCHEME_MULTI_POINT
+    second_order: bool = True
+    method: int = 4
+    bc_style: int = 2
+    boundary_2d: bool = True
+    exclude_bound_vert: bool = False
+    local_time_step: bool = False
+    cfl: float = 0.4
+    tmax: float = 1e30
+    bc_type: list = field(default_factory=list)  # per tag
+    bc_val: list = field(default_factory=list)   # per tag, primitive (rho, u, v, w, p)
+    precision: int = 0  # 0 plain FP64, 1 FP32 flux / reconstruction / limiters
+
+    def to_c(self) -> NsCfgC:
+        c = NsCfgC()
+        c.scheme, c.second_order, c.method = self.scheme, int(self.second_order), self.method
+        c.bc_style, c.boundary_2d = self.bc_style, int(self.boundary_2d)
+        c.exclude_bound_vert, c.local_time_step = int(self.exclude_bound_vert), int(self.local_time_step)
+        c.n_bc = len(self.bc_type)
+        for i, t in enumerate(self.bc_type):
+            c.bc_type[i] = t
+            for k in range(5):
+                c.bc_val[i][k] = float(self.bc_val[i][k]) if i < len(self.bc_val) else 0.0
+        c.cfl, c.tmax, c.precision = float(self.cfl), float(self.tmax), int(self.precision)
+        return c
+
+    def oracle_dict(self) -> dict:
+        d = dict(scheme=self.scheme, second_order=int(self.second_order), method=self.method,
+                 bc_style=self.bc_style, b2d=int(self.boundary_2d), exclude_bound_vert=int(self.exclude_bound_vert),
+                 local_time_step=int(self.local_time_step), cfl=self.cfl, tmax=self.tmax, n_bc=len(self.bc_type))
+        if self.bc_type:
+            d["bc_type"] = np.array(self.bc_type, np.int32)
+            d["bc_val"] = np.array(self.bc_val, np.float64)
+        return d
+
+
+def init_gresho(mesh: Mesh, mach: float) -> np.ndarray:
+    """init_sol with init_gresho (ns_euler_module.F90:49-53) at Mach `mach`."""
+    sol = np.empty((mesh.n_elems, 5))
+    check(_lib.load().subfv_ns_init_gresho(mesh._h, float(mach), pd(sol)), "subfv_ns_init_gresho")
+    return sol
+
+
+def compute_rhs_ns(mesh: Mesh, cfg: NsConfig, sol):
+    """One residual evaluation; returns (status, rhs, sum_lambda, vp, cell_grad (n, 5, 3))."""
+    sol = f64(sol)
+    rhs = np.empty((mesh.n_elems, 5))
+    sl = np.empty(mesh.n_elems)
+    vp = np.empty((mesh.n_vert, 3))
+    grad = np.empty((mesh.n_elems, 5, 3))  # Fortran grad(3, 5, n)
+    c = cfg.to_c()
+    st = check(_lib.load().subfv_compute_rhs_ns(mesh._h, C.byref(c), pd(sol), pd(rhs), pd(sl), pd(vp), pd(grad)),
+               "subfv_compute_rhs_ns")
+    return st, rhs, sl, vp, grad
+
+
+class NsState:
+    """Device-resident time loop of ns_main.F90:83-107 (graph-replayed iterations)."""
+
+    def __init__(self, mesh: Mesh, cfg: NsConfig, sol, t0: float = 0.0):
+        self.mesh, self.cfg = mesh, cfg
+        sol = f64(sol)
+        self._c = cfg.to_c()
+        h = C.c_void_p()
+        check(_lib.load().subfv_ns_state_create(mesh._h, C.byref(self._c), pd(sol), float(t0), C.byref(h)),
+              "subfv_ns_state_create")
+        self._h = h
+
+    def advance(self, n_steps: int):
+        steps, t = C.c_int(), C.c_double()
+        st = check(_lib.load().subfv_ns_advance(self._h, int(n_steps), C.byref(steps), C.byref(t)), "subfv_ns_advance")
+        return st, steps.value, t.value
+
+    def advance_async(self, n_steps: int):
+        check(_lib.load().subfv_ns_advance_async(self._h, int(n_steps)), "subfv_ns_advance_async")
+
+    def sync(self):
+        steps, t = C.c_int(), C.c_double()
+        st = check(_lib.load().subfv_ns_sync(self._h, C.byref(steps), C.byref(t)), "subfv_ns_sync")
+        return st, steps.value, t.value
+
+    def sol(self) -> np.ndarray:
+        out = np.empty((self.mesh.n_elems, 5))
+        check(_lib.load().subfv_ns_get_sol(self._h, pd(out)), "subfv_ns_get_sol")
+        return out
+
+    def residuals(self):
+        res, dt = C.c_double(), C.c_double()
+        rv = np.zeros(5)
+        check(_lib.load().subfv_ns_residuals(self._h, C.byref(res), pd(rv), C.byref(dt)), "subfv_ns_residuals")
+        return res.value, rv, dt.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().subfv_ns_state_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
