@@ -187,6 +187,37 @@ int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double*
  * conservative variables (init_sol with init_gresho, ns_euler_module.F90:49-53). */
 int subfv_ns_init_gresho(subfv_mesh* m, double mach, double* sol);
 
+/* ---------------------------------------------------------------------------------
+ * Block-CSR linear algebra (src/linear_algebra/sparse_bcsr_linear_module.F90).
+ * bcsr_matrix_type layout: m block rows, row(m+1) and col(nnz) 1-based, values
+ * v(bs, bs, nnz) column-major blocks. Vectors have bs*m entries (host arrays). */
+typedef struct subfv_bcsr subfv_bcsr;
+int subfv_bcsr_create(int m, int bs, const int32_t* row, const int32_t* col, const double* v,
+                      subfv_bcsr** out);
+int subfv_bcsr_destroy(subfv_bcsr* A);
+int subfv_bcsr_set_values(subfv_bcsr* A, const double* v);
+/* y = bcsr_matmul(A, x) — :13-29 */
+int subfv_bcsr_matmul(subfv_bcsr* A, const double* x, double* y);
+/* bcsr_diag(A, x, b): x = D^-1 b with a no-pivot LU per diagonal block — :1414-1436 */
+int subfv_bcsr_diag(subfv_bcsr* A, double* x, const double* b);
+/* bcsr_gmres_diag(A, x, b, tol, m, conv, ...) — :1592-1691: restarted GMRES(m),
+ * right block-Jacobi preconditioning, absolute tol, 40 restarts. Returns
+ * SUBFV_ERR_GMRES when not converged (the reference's conv = .false.). */
+int subfv_bcsr_gmres_diag(subfv_bcsr* A, double* x, const double* b, double tol, int m, int* conv,
+                          int* restarts, double* rho);
+/* bcsr_gmres — :194-290: unpreconditioned, 20 restarts */
+int subfv_bcsr_gmres(subfv_bcsr* A, double* x, const double* b, double tol, int m, int* conv,
+                     int* restarts, double* rho);
+/* Either of the above (precond 1/0); H_first (m+1, m) receives the first Arnoldi Hessenberg. */
+int subfv_bcsr_gmres_ex(subfv_bcsr* A, double* x, const double* b, double tol, int m, int precond,
+                        int* conv, int* restarts, double* rho, double* H_first);
+/* No counterpart in the reference: FP64 iterative refinement around block-Jacobi GMRES(m)
+ * whose SpMV reads an FP32 copy of the matrix; stops at |b - A x| < rel_tol |b|. */
+int subfv_bcsr_gmres_refine(subfv_bcsr* A, double* x, const double* b, double rel_tol, int m, int* conv,
+                            int* outer, double* rho);
+/* Device time of one SpMV (FP64 or FP32 matrix), averaged over n_iter launches. */
+int subfv_bcsr_profile_spmv(subfv_bcsr* A, int n_iter, int fp32, double* ms_per_spmv);
+
 #ifdef __cplusplus
 }
 #endif

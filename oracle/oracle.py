@@ -55,6 +55,9 @@ def load():
         lib.or_ns_gresho.argtypes = [C.c_void_p, C.c_double, PD]
         lib.or_pinv3.argtypes = [PD]
         lib.or_lu3.argtypes = [PD, PD, PD]
+        lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
+        lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]
+        lib.or_bcsr_gmres.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD, C.c_double, C.c_int, C.c_int, PI, PD, PD]
         _lib = lib
     return _lib
 
@@ -214,3 +217,36 @@ class OracleMesh:
             self.close()
         except Exception:
             pass
+
+
+class OracleBcsr:
+    """bcsr_matmul / bcsr_diag / bcsr_gmres(_diag) on the CPU (restatement)."""
+
+    def __init__(self, A):
+        self.m, self.bs = A.m, A.blc_size
+        self.row = np.ascontiguousarray(A.row, np.int32)
+        self.col = np.ascontiguousarray(A.col, np.int32)
+        self.v = np.ascontiguousarray(A.v.reshape(-1), np.float64)
+        self.n = self.m * self.bs
+
+    def matmul(self, x):
+        x = np.ascontiguousarray(x, np.float64)
+        y = np.empty(self.n)
+        load().or_bcsr_matmul(self.m, self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), _pd(x), _pd(y))
+        return y
+
+    def diag(self, b):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.n)
+        load().or_bcsr_diag(self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), _pd(x), _pd(b))
+        return x
+
+    def gmres(self, b, tol, m=30, precond=True):
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.empty(self.n)
+        conv = np.zeros(1, np.int32)
+        rho = np.zeros(1)
+        H = np.zeros((m, m + 1))
+        it = load().or_bcsr_gmres(self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), _pd(x), _pd(b),
+                                  float(tol), int(m), int(precond), _pi(conv), _pd(rho), _pd(H))
+        return x, bool(conv[0]), it, float(rho[0]), H

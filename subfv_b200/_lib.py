@@ -63,6 +63,16 @@ SIGNATURES = {
     "subfv_ns_get_sol": (c_int, [P, PD]),
     "subfv_ns_residuals": (c_int, [P, PD, PD, PD]),
     "subfv_ns_init_gresho": (c_int, [P, c_dbl, PD]),
+    "subfv_bcsr_create": (c_int, [c_int, c_int, PI32, PI32, PD, C.POINTER(P)]),
+    "subfv_bcsr_destroy": (c_int, [P]),
+    "subfv_bcsr_set_values": (c_int, [P, PD]),
+    "subfv_bcsr_matmul": (c_int, [P, PD, PD]),
+    "subfv_bcsr_diag": (c_int, [P, PD, PD]),
+    "subfv_bcsr_gmres_diag": (c_int, [P, PD, PD, c_dbl, c_int, C.POINTER(c_int), C.POINTER(c_int), PD]),
+    "subfv_bcsr_gmres": (c_int, [P, PD, PD, c_dbl, c_int, C.POINTER(c_int), C.POINTER(c_int), PD]),
+    "subfv_bcsr_gmres_ex": (c_int, [P, PD, PD, c_dbl, c_int, c_int, C.POINTER(c_int), C.POINTER(c_int), PD, PD]),
+    "subfv_bcsr_gmres_refine": (c_int, [P, PD, PD, c_dbl, c_int, C.POINTER(c_int), C.POINTER(c_int), PD]),
+    "subfv_bcsr_profile_spmv": (c_int, [P, c_int, c_int, PD]),
     "subfv_mesh_stream": (P, [P]),
 }
 

@@ -1,0 +1,481 @@
+// BCSR SpMV, block-Jacobi application and restarted GMRES on the GPU.
+// Reference: src/linear_algebra/sparse_bcsr_linear_module.F90 bcsr_matmul (:13-29),
+// bcsr_diag (:1414-1436) with lu_solve_noswp (linear_solver_module.F90:413-445),
+// modifiedArnoldi(_diag) and bcsr_gmres(_diag) (:194-340, :1568-1691).
+//
+// * SpMV: a group of bs lanes per block row, lane r owns row component r and walks the
+//   row's blocks in order; each block's product is summed over its columns first, then
+//   added, exactly as y(blk) = y(blk) + matmul(v(:,:,j), x(blk(col(j)))). Bit-identical.
+// * block Jacobi: the no-pivot LU of each diagonal block is factored once per matrix
+//   (multipliers and upper factor kept), then applied with the same operations and order
+//   as lu_solve_noswp. Bit-identical.
+// * dot products and norms: a fixed grid of 296 blocks x 256 threads; each thread sums a
+//   fixed strided slice, each block a fixed tree, and the block partials are summed in
+//   block order. Deterministic run to run; not the reference's left-to-right order.
+// * Gram-Schmidt: the axpy of step i is fused with the dot product of step i+1.
+// * Givens rotations and the back substitution run on the host in the reference's order.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "bcsr.cuh"
+
+namespace subfv {
+
+namespace {
+
+constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+constexpr int kRedThreads = 256;
+
+template <int BS, class MT>
+__global__ void __launch_bounds__(128) k_spmv(int m, const int* __restrict__ row, const int* __restrict__ col,
+                                              const MT* __restrict__ v, const double* __restrict__ x,
+                                              double* __restrict__ y) {
+  constexpr int GPW = 32 / BS;
+  const int lane = threadIdx.x & 31;
+  if (lane >= GPW * BS) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int i = warp * GPW + lane / BS;
+  const int r = lane % BS;
+  if (i >= m) return;
+  double acc = 0.0;
+  for (int j = row[i]; j < row[i + 1]; ++j) {
+    const int c0 = col[j];
+    const MT* blk = v + (size_t)BS * BS * j;
+    const double* xc = x + (size_t)BS * c0;
+    double t = 0.0;
+#pragma unroll
+    for (int c = 0; c < BS; ++c) t = t + (double)blk[r + BS * c] * xc[c];
+    acc = acc + t;
+  }
+  y[(size_t)BS * i + r] = acc;
+}
+
+template <int BS>
+__global__ void k_factor_diag(int m, const int* __restrict__ diag, const double* __restrict__ v,
+                              double* __restrict__ lu, double* __restrict__ lo) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double C[BS * BS], L[BS * BS];
+  const int dj = diag[i];
+  for (int q = 0; q < BS * BS; ++q) {
+    C[q] = dj >= 0 ? v[(size_t)BS * BS * dj + q] : (q % (BS + 1) == 0 ? 1.0 : 0.0);
+    L[q] = 0.0;
+  }
+  for (int k = 0; k < BS; ++k) {
+    const double invdiag = 1.0 / C[k + BS * k];
+    for (int ii = k + 1; ii < BS; ++ii) {
+      const double lik = C[ii + BS * k] * invdiag;
+      L[ii + BS * k] = lik;
+      for (int jj = k; jj < BS; ++jj) C[ii + BS * jj] = C[ii + BS * jj] - lik * C[k + BS * jj];
+    }
+  }
+  for (int q = 0; q < BS * BS; ++q) {
+    lu[(size_t)BS * BS * i + q] = C[q];
+    lo[(size_t)BS * BS * i + q] = L[q];
+  }
+}
+
+template <int BS>
+__global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __restrict__ lo,
+                          const double* __restrict__ b, double* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double* C = lu + (size_t)BS * BS * i;
+  const double* L = lo + (size_t)BS * BS * i;
+  double xv[BS];
+  for (int k = 0; k < BS; ++k) xv[k] = b[(size_t)BS * i + k];
+  for (int k = 0; k < BS; ++k)
+    for (int ii = k + 1; ii < BS; ++ii) xv[ii] = xv[ii] - L[ii + BS * k] * xv[k];
+  xv[BS - 1] = xv[BS - 1] / C[(BS - 1) + BS * (BS - 1)];
+  for (int k = BS - 2; k >= 0; --k) {
+    for (int j = k + 1; j < BS; ++j) xv[k] = xv[k] - C[k + BS * j] * xv[j];
+    xv[k] = xv[k] / C[k + BS * k];
+  }
+  for (int k = 0; k < BS; ++k) x[(size_t)BS * i + k] = xv[k];
+}
+
+__device__ inline double block_sum(double v) {
+  __shared__ double sh[kRedThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x == 0)
+    for (int w = 0; w < kRedThreads / 32; ++w) s = s + sh[w];
+  return s;  // valid in thread 0
+}
+
+// partial[b] = sum over the block's fixed slice of a*b
+__global__ void __launch_bounds__(kRedThreads) k_dot(const double* __restrict__ a, const double* __restrict__ b,
+                                                     long n, double* __restrict__ partial) {
+  const long T = (long)gridDim.x * blockDim.x;
+  double s = 0.0;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += T) s = s + a[k] * b[k];
+  s = block_sum(s);
+  if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__device__ inline double sum_partials(const double* p, int nb) {
+  double s = 0.0;
+  for (int q = 0; q < nb; ++q) s = s + p[q];
+  return s;
+}
+
+// h = sum(pin); y -= h*x; then pout = partial dot(y_new, nx), or of y_new with itself
+// when nx is null (the squared norm that closes a Gram-Schmidt column). Block 0 stores h.
+__global__ void __launch_bounds__(kRedThreads) k_axpy_dot(double* __restrict__ y, const double* __restrict__ x,
+                                                          const double* __restrict__ pin, int nb, double* hout,
+                                                          const double* __restrict__ nx, double* __restrict__ pout,
+                                                          long n) {
+  __shared__ double hs;
+  if (threadIdx.x == 0) hs = sum_partials(pin, nb);
+  __syncthreads();
+  const double h = hs;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && hout) *hout = h;
+  const long T = (long)gridDim.x * blockDim.x;
+  double s = 0.0;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += T) {
+    const double yk = y[k] - h * x[k];
+    y[k] = yk;
+    s = s + yk * (nx ? nx[k] : yk);
+  }
+  s = block_sum(s);
+  if (threadIdx.x == 0) pout[blockIdx.x] = s;
+}
+
+// nrm = sqrt(sum(pin)); y = y / nrm; block 0 stores nrm at *hout
+__global__ void __launch_bounds__(kRedThreads) k_normalize(double* __restrict__ y, const double* __restrict__ pin,
+                                                           int nb, double* hout, long n) {
+  __shared__ double hs;
+  if (threadIdx.x == 0) hs = sqrt(sum_partials(pin, nb));
+  __syncthreads();
+  const double h = hs;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *hout = h;
+  const long T = (long)gridDim.x * blockDim.x;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += T) y[k] = y[k] / h;
+}
+
+__global__ void k_scale_div(double* __restrict__ y, double d, long n) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) y[k] = y[k] / d;
+}
+__global__ void k_sub(const double* __restrict__ b, const double* __restrict__ w, double* __restrict__ r, long n) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) r[k] = b[k] - w[k];
+}
+__global__ void k_add(double* __restrict__ x, const double* __restrict__ d, long n) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) x[k] = x[k] + d[k];
+}
+// out = base + sum_i z_i V_i, summed left to right from base (base may alias out)
+__global__ void k_lincomb(const double* __restrict__ V, long n, const double* __restrict__ z, int nr,
+                          const double* base, double* out) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  double acc = base ? base[k] : 0.0;
+  for (int i = 0; i < nr; ++i) acc = acc + z[i] * V[(size_t)i * n + k];
+  out[k] = acc;
+}
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, size_t n) {
+  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) b[k] = (float)a[k];
+}
+
+int egrid(long n) { return (int)((n + 255) / 256); }
+
+}  // namespace
+
+int bcsr_upload(DevBcsr* A, int m, int bs, const int* row1, const int* col1, const double* v, cudaStream_t s) {
+  if (m <= 0 || bs < 1 || bs > kBcsrMaxBs || (bs != 5 && bs != 4 && bs != 1 && bs != 3)) {
+    set_error("subfv_bcsr: supported block sizes are 1, 3, 4 and 5");
+    return -2;
+  }
+  const int nnz = row1[m] - 1;
+  std::vector<int> row(m + 1), col(nnz), diag(m, -1);
+  for (int i = 0; i <= m; ++i) row[i] = row1[i] - 1;
+  for (int j = 0; j < nnz; ++j) {
+    col[j] = col1[j] - 1;
+    if (col[j] < 0 || col[j] >= m) {
+      set_error("subfv_bcsr: column index out of range");
+      return -2;
+    }
+  }
+  for (int i = 0; i < m; ++i)
+    for (int j = row[i]; j < row[i + 1]; ++j)
+      if (col[j] == i) {
+        diag[i] = j;
+        break;
+      }
+  A->m = m;
+  A->bs = bs;
+  A->nnz = nnz;
+  if (s) {
+    A->stream = s;
+  } else {
+    SUBFV_CUDA(cudaStreamCreateWithFlags(&A->stream, cudaStreamNonBlocking));
+    A->own_stream = true;
+  }
+  const size_t vb = (size_t)bs * bs * std::max(nnz, 1);
+  SUBFV_CUDA(cudaMalloc(&A->row, (m + 1) * sizeof(int)));
+  SUBFV_CUDA(cudaMalloc(&A->col, std::max(nnz, 1) * sizeof(int)));
+  SUBFV_CUDA(cudaMalloc(&A->diag, m * sizeof(int)));
+  SUBFV_CUDA(cudaMalloc(&A->v, vb * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&A->v32, vb * sizeof(float)));
+  SUBFV_CUDA(cudaMalloc(&A->lu, (size_t)bs * bs * m * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&A->lo, (size_t)bs * bs * m * sizeof(double)));
+  A->bytes = (m + 1 + nnz + m) * sizeof(int) + vb * 12 + 2 * (size_t)bs * bs * m * 8;
+  SUBFV_CUDA(cudaMemcpyAsync(A->row, row.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice, A->stream));
+  SUBFV_CUDA(cudaMemcpyAsync(A->col, col.data(), nnz * sizeof(int), cudaMemcpyHostToDevice, A->stream));
+  SUBFV_CUDA(cudaMemcpyAsync(A->diag, diag.data(), m * sizeof(int), cudaMemcpyHostToDevice, A->stream));
+  SUBFV_CUDA(cudaStreamSynchronize(A->stream));
+  if (v) return bcsr_set_values(A, v, false);
+  return 0;
+}
+
+int bcsr_set_values(DevBcsr* A, const double* v, bool on_device) {
+  const size_t vb = (size_t)A->bs * A->bs * A->nnz;
+  if (v != A->v)
+    SUBFV_CUDA(cudaMemcpyAsync(A->v, v, vb * sizeof(double), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                               A->stream));
+  k_d2f<<<(int)((vb + 255) / 256), 256, 0, A->stream>>>(A->v, A->v32, vb);
+  launch_bcsr_factor_diag(*A);
+  SUBFV_CUDA(cudaGetLastError());
+  SUBFV_CUDA(cudaStreamSynchronize(A->stream));
+  return 0;
+}
+
+void bcsr_free(DevBcsr* A) {
+  void* p[] = {A->row, A->col, A->v, A->v32, A->diag, A->lu, A->lo};
+  for (void* q : p)
+    if (q) cudaFree(q);
+  if (A->own_stream && A->stream) cudaStreamDestroy(A->stream);
+  *A = DevBcsr();
+}
+
+int gmres_work_alloc(GmresWork* W, long n, int krylov) {
+  W->n = n;
+  W->krylov = krylov;
+  SUBFV_CUDA(cudaMalloc(&W->V, (size_t)n * (krylov + 1) * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->r, n * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->w, n * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->zp, n * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->d, n * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->rr, n * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->z, (krylov + 2) * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->partial, 2 * kRedBlocks * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->H, (size_t)(krylov + 1) * krylov * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->scal, 8 * sizeof(double)));
+  W->bytes = (size_t)n * (krylov + 6) * 8;
+  return 0;
+}
+
+void gmres_work_free(GmresWork* W) {
+  void* p[] = {W->V, W->r, W->w, W->zp, W->z, W->partial, W->H, W->scal, W->d, W->rr};
+  for (void* q : p)
+    if (q) cudaFree(q);
+  *W = GmresWork();
+}
+
+void launch_bcsr_spmv(const DevBcsr& A, const double* x, double* y, bool fp32) {
+  const int gpw = 32 / A.bs;
+  const long warps = (A.m + gpw - 1) / gpw;
+  const int grid = (int)((warps * 32 + 127) / 128);
+  switch (A.bs) {
+    case 5:
+      if (fp32) k_spmv<5, float><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v32, x, y);
+      else k_spmv<5, double><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v, x, y);
+      break;
+    case 4:
+      if (fp32) k_spmv<4, float><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v32, x, y);
+      else k_spmv<4, double><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v, x, y);
+      break;
+    case 3:
+      if (fp32) k_spmv<3, float><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v32, x, y);
+      else k_spmv<3, double><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v, x, y);
+      break;
+    default:
+      if (fp32) k_spmv<1, float><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v32, x, y);
+      else k_spmv<1, double><<<grid, 128, 0, A.stream>>>(A.m, A.row, A.col, A.v, x, y);
+  }
+}
+
+void launch_bcsr_factor_diag(const DevBcsr& A) {
+  const int g = (A.m + 127) / 128;
+  switch (A.bs) {
+    case 5: k_factor_diag<5><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo); break;
+    case 4: k_factor_diag<4><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo); break;
+    case 3: k_factor_diag<3><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo); break;
+    default: k_factor_diag<1><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo);
+  }
+}
+
+void launch_bcsr_bjacobi(const DevBcsr& A, const double* b, double* x) {
+  const int g = (A.m + 127) / 128;
+  switch (A.bs) {
+    case 5: k_bjacobi<5><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x); break;
+    case 4: k_bjacobi<4><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x); break;
+    case 3: k_bjacobi<3><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x); break;
+    default: k_bjacobi<1><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x);
+  }
+}
+
+namespace {
+// host copy of the block partials, summed in block order (the device's order)
+int host_finish(const DevBcsr& A, const double* dpartial, double* out) {
+  double h[kRedBlocks];
+  SUBFV_CUDA(cudaMemcpyAsync(h, dpartial, sizeof(h), cudaMemcpyDeviceToHost, A.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(A.stream));
+  double s = 0.0;
+  for (int q = 0; q < kRedBlocks; ++q) s = s + h[q];
+  *out = s;
+  return 0;
+}
+}  // namespace
+
+double device_norm2(const DevBcsr& A, GmresWork& W, const double* x, long n) {
+  k_dot<<<kRedBlocks, kRedThreads, 0, A.stream>>>(x, x, n, W.partial);
+  double s = 0.0;
+  if (host_finish(A, W.partial, &s)) return -1.0;
+  return std::sqrt(s);
+}
+
+int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, bool precond, bool fp32,
+                 int maxit, GmresStats* st, double* H_first_host) {
+  const int m = W.krylov;
+  const long n = W.n;
+  cudaStream_t s = A.stream;
+  double* pa = W.partial;
+  double* pb = W.partial + kRedBlocks;
+  auto Vc = [&](int j) { return W.V + (size_t)(j - 1) * n; };  // 1-based
+  auto Hd = [&](int i, int j) { return W.H + (i - 1) + (size_t)(m + 1) * (j - 1); };
+  std::vector<double> H((size_t)(m + 1) * m), y(m + 1), c(m + 1), sn(m + 1), z(m + 1);
+  auto h = [&](int i, int j) -> double& { return H[(i - 1) + (size_t)(m + 1) * (j - 1)]; };
+  st->conv = 0;
+  SUBFV_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+  launch_bcsr_spmv(A, x, W.w, fp32);
+  k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.r, n);
+  double rho = device_norm2(A, W, W.r, n);
+  int it = 0;
+  if (rho < tol) {
+    st->conv = 1;
+    st->rho = rho;
+    st->restarts = 0;
+    return 0;
+  }
+  for (int j = 1; j <= maxit; ++j) {
+    it = j;
+    std::fill(y.begin(), y.end(), 0.0);
+    y[0] = rho;
+    k_scale_div<<<egrid(n), 256, 0, s>>>(W.r, y[0], n);
+    SUBFV_CUDA(cudaMemcpyAsync(Vc(1), W.r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    SUBFV_CUDA(cudaMemsetAsync(W.H, 0, H.size() * sizeof(double), s));
+    for (int jj = 2; jj <= m + 1; ++jj) {
+      if (precond) {
+        launch_bcsr_bjacobi(A, Vc(jj - 1), W.zp);
+        launch_bcsr_spmv(A, W.zp, Vc(jj), fp32);
+      } else {
+        launch_bcsr_spmv(A, Vc(jj - 1), Vc(jj), fp32);
+      }
+      k_dot<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(1), Vc(jj), n, pa);
+      for (int i = 1; i <= jj - 1; ++i) {
+        const double* nx = i < jj - 1 ? Vc(i + 1) : nullptr;  // the last one is |V_jj|^2
+        k_axpy_dot<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(jj), Vc(i), pa, kRedBlocks, Hd(i, jj - 1), nx, pb, n);
+        std::swap(pa, pb);
+      }
+      k_normalize<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(jj), pa, kRedBlocks, Hd(jj, jj - 1), n);
+    }
+    SUBFV_CUDA(cudaMemcpyAsync(H.data(), W.H, H.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    SUBFV_CUDA(cudaStreamSynchronize(s));
+    SUBFV_CUDA(cudaGetLastError());
+    if (j == 1 && H_first_host) std::memcpy(H_first_host, H.data(), H.size() * sizeof(double));
+    int nr = m, i;
+    for (i = 1; i <= m; ++i) {  // Givens rotations (:1634-1658)
+      for (int k = 2; k <= i; ++k) {
+        double tmp = h(k - 1, i);
+        h(k - 1, i) = c[k - 2] * h(k - 1, i) + sn[k - 2] * h(k, i);
+        h(k, i) = -sn[k - 2] * tmp + c[k - 2] * h(k, i);
+      }
+      double delta = std::sqrt(h(i, i) * h(i, i) + h(i + 1, i) * h(i + 1, i));
+      c[i - 1] = h(i, i) / delta;
+      sn[i - 1] = h(i + 1, i) / delta;
+      h(i, i) = c[i - 1] * h(i, i) + sn[i - 1] * h(i + 1, i);
+      for (int k = i + 1; k <= m + 1; ++k) h(k, i) = 0.0;
+      y[i] = -sn[i - 1] * y[i - 1];
+      y[i - 1] = c[i - 1] * y[i - 1];
+      rho = std::fabs(y[i]);
+      if (rho < tol) {
+        nr = i + 1;
+        break;
+      }
+    }
+    std::fill(z.begin(), z.end(), 0.0);  // back substitution (:1660-1673)
+    if (i >= m) {
+      nr = m;
+      z[nr - 1] = y[nr - 1] / h(nr, nr);
+    }
+    for (int k = nr - 1; k >= 1; --k) {
+      z[k - 1] = y[k - 1];
+      for (int l = k + 1; l <= nr; ++l) z[k - 1] = z[k - 1] - h(k, l) * z[l - 1];
+      z[k - 1] = z[k - 1] / h(k, k);
+    }
+    SUBFV_CUDA(cudaMemcpyAsync(W.z, z.data(), nr * sizeof(double), cudaMemcpyHostToDevice, s));
+    if (precond) {
+      k_lincomb<<<egrid(n), 256, 0, s>>>(W.V, n, W.z, nr, nullptr, W.r);
+      launch_bcsr_bjacobi(A, W.r, W.zp);
+      k_add<<<egrid(n), 256, 0, s>>>(x, W.zp, n);
+    } else {
+      k_lincomb<<<egrid(n), 256, 0, s>>>(W.V, n, W.z, nr, x, x);
+    }
+    launch_bcsr_spmv(A, x, W.w, fp32);
+    k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.r, n);
+    rho = device_norm2(A, W, W.r, n);
+    if (rho < tol) {
+      if (precond) st->conv = 1;
+      break;
+    }
+  }
+  if (!precond) {
+    launch_bcsr_spmv(A, x, W.w, fp32);
+    k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.r, n);
+    st->conv = !(device_norm2(A, W, W.r, n) > tol);
+  }
+  st->rho = rho;
+  st->restarts = it;
+  SUBFV_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double rel_tol,
+                        double inner_rel_tol, int max_outer, GmresStats* st) {
+  const long n = W.n;
+  cudaStream_t s = A.stream;
+  const double bnorm = device_norm2(A, W, b, n);
+  SUBFV_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
+  SUBFV_CUDA(cudaMemcpyAsync(W.rr, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  st->conv = 0;
+  st->inner_total = 0;
+  double rn = bnorm;
+  int outer = 0;
+  for (outer = 1; outer <= max_outer; ++outer) {
+    if (rn < rel_tol * bnorm) {
+      st->conv = 1;
+      break;
+    }
+    GmresStats in;
+    if (gmres_device(A, W, W.d, W.rr, inner_rel_tol * rn, true, true, 40, &in, nullptr)) return -1;
+    st->inner_total += in.restarts;
+    k_add<<<egrid(n), 256, 0, s>>>(x, W.d, n);
+    launch_bcsr_spmv(A, x, W.w, false);  // FP64 residual
+    k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.rr, n);
+    rn = device_norm2(A, W, W.rr, n);
+  }
+  if (!st->conv && rn < rel_tol * bnorm) st->conv = 1;
+  st->outer = outer - (st->conv ? 1 : 0);
+  st->rho = rn;
+  SUBFV_CUDA(cudaGetLastError());
+  return 0;
+}
+
+}  // namespace subfv

@@ -1,0 +1,64 @@
+// Block-CSR matrices and the restarted, block-Jacobi right-preconditioned GMRES of
+// src/linear_algebra/sparse_bcsr_linear_module.F90 on the GPU.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+namespace subfv {
+
+constexpr int kBcsrMaxBs = 8;
+
+struct DevBcsr {
+  int m = 0, bs = 0, nnz = 0;
+  int* row = nullptr;      // (m+1) 0-based offsets
+  int* col = nullptr;      // (nnz) 0-based block columns
+  double* v = nullptr;     // (bs, bs, nnz) column-major blocks
+  float* v32 = nullptr;    // FP32 copy for the iterative-refinement inner solves
+  int* diag = nullptr;     // (m) index of the diagonal block, -1 if absent
+  double* lu = nullptr;    // (bs, bs, m) no-pivot LU: upper part and diagonal of C
+  double* lo = nullptr;    // (bs, bs, m) the multipliers lik below the diagonal
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  size_t bytes = 0;
+};
+
+struct GmresStats {
+  int restarts = 0;
+  int conv = 0;
+  double rho = 0.0;
+  int inner_total = 0;
+  int outer = 0;
+};
+
+// Workspace for GMRES(m) on n = bs*m unknowns.
+struct GmresWork {
+  int krylov = 0;
+  long n = 0;
+  double *V = nullptr, *r = nullptr, *w = nullptr, *zp = nullptr, *z = nullptr;
+  double *partial = nullptr, *H = nullptr, *scal = nullptr;
+  double *d = nullptr, *rr = nullptr;  // refinement correction and residual
+  size_t bytes = 0;
+};
+
+int bcsr_upload(DevBcsr* A, int m, int bs, const int* row1, const int* col1, const double* v, cudaStream_t s);
+int bcsr_set_values(DevBcsr* A, const double* v_dev_or_host, bool on_device);
+void bcsr_free(DevBcsr* A);
+int gmres_work_alloc(GmresWork* W, long n, int krylov);
+void gmres_work_free(GmresWork* W);
+
+void launch_bcsr_spmv(const DevBcsr& A, const double* x, double* y, bool fp32_matrix);
+void launch_bcsr_factor_diag(const DevBcsr& A);
+void launch_bcsr_bjacobi(const DevBcsr& A, const double* b, double* x);
+
+// bcsr_gmres_diag (precond) or bcsr_gmres; x, b device vectors; tol absolute.
+int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, bool precond,
+                 bool fp32_matrix, int maxit, GmresStats* st, double* H_first_host);
+// FP64 iterative refinement around FP32-matrix GMRES: stops at |b - A x| < rel_tol * |b|.
+int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double rel_tol,
+                        double inner_rel_tol, int max_outer, GmresStats* st);
+double device_norm2(const DevBcsr& A, GmresWork& W, const double* x, long n);
+
+}  // namespace subfv
