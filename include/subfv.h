@@ -183,6 +183,22 @@ int subfv_ns_sync(subfv_ns_state* s, int* steps_done, double* t);
 int subfv_ns_get_sol(subfv_ns_state* s, double* sol);
 /* res = sum of |delta|_2 and res_vect(5) of the last add_timedisc_and_solve call */
 int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double* dt);
+/* No counterpart in the reference (its NS path is point-implicit only). One backward
+ * Euler step U += dU with (V/dt I - d rhs/dU) dU = rhs(U): rhs the first-order two-wave
+ * residual, its Jacobian assembled exactly with the wave speeds frozen, solved by
+ * block-Jacobi GMRES(krylov) to |r| < rel_tol |rhs| (or FP64 iterative refinement around
+ * an FP32-matrix GMRES when refine_fp32); dt = cfl_implicit * min V / sum_lambda. */
+typedef struct subfv_implicit_stats {
+  double dt, b_norm, res_norm;
+  int32_t conv, restarts, outer;
+  double ms_assemble, ms_solve, ms_update;
+  int64_t nnz_blocks;
+} subfv_implicit_stats;
+int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
+                           subfv_implicit_stats* stats);
+/* The assembled matrix at the state's current U for a given dt (bcsr_matrix_type layout,
+ * 1-based row/col, blocks column-major); returns the number of blocks. */
+int subfv_ns_be_jacobian(subfv_ns_state* s, double dt, int32_t* row, int32_t* col, double* v, int64_t cap);
 /* Gresho vortex of ns_euler_exact_sol_module.F90:7-44 at the cell centroids, as
  * conservative variables (init_sol with init_gresho, ns_euler_module.F90:49-53). */
 int subfv_ns_init_gresho(subfv_mesh* m, double mach, double* sol);

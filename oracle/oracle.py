@@ -58,6 +58,8 @@ def load():
         lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_gmres.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD, C.c_double, C.c_int, C.c_int, PI, PD, PD]
+        lib.or_be_jacobian.restype = C.c_long
+        lib.or_be_jacobian.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_double, PI, PI, PD, C.c_long]
         _lib = lib
     return _lib
 
@@ -177,6 +179,20 @@ class OracleMesh:
         bt = np.ascontiguousarray(cfg.get("bc_type", np.zeros(1, np.int32)), np.int32)
         bv = np.ascontiguousarray(cfg.get("bc_val", np.zeros(5)), np.float64).reshape(-1)
         return ic, dc, bt, bv
+
+    def be_jacobian(self, cfg, sol, dt):
+        """Backward-Euler matrix V/dt I - d rhs/dU of the first-order two-wave residual
+        (frozen wave speeds); returns (row, col, v (nnz, 5, 5) with v[j].T the block)."""
+        ic, dc, bt, bv = self._ns_args(cfg)
+        sol = np.ascontiguousarray(sol, np.float64)
+        cap = 64 * self.n_elems
+        row = np.zeros(self.n_elems + 1, np.int32)
+        col = np.zeros(cap, np.int32)
+        v = np.zeros(25 * cap)
+        nnz = load().or_be_jacobian(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), float(dt), _pi(row),
+                                    _pi(col), _pd(v), cap)
+        assert nnz > 0
+        return row, col[:nnz].copy(), v[:25 * nnz].reshape(nnz, 5, 5).copy()
 
     def ns_gresho(self, mach):
         sol = np.zeros((self.n_elems, 5))

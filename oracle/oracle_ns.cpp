@@ -13,6 +13,7 @@
 //    dgetrf2 / dgetrs operation order, reference-BLAS triangular solves.
 // PARITY UNPINNED (no Fortran compiler or LAPACK build of the reference here).
 #include "oracle.h"
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -720,6 +721,136 @@ void init_gresho(const Mesh& m, double mach, double* sol) {
   }
 }
 
+// ------------------------------------------------------------------------------------
+// Backward-Euler Jacobian (no counterpart in the reference, whose NS path is only
+// point-implicit): A = V/dt I - d rhs/dU for the first-order two-wave residual, the
+// wave speeds sl, sr frozen at their current values. The oracle restates the same
+// formulas the product uses; a CPU test also checks them against finite differences.
+
+// dF.n/dU for the Euler flux, conservative variables
+static void euler_jac(const double* U, const double* n, double A[5][5]) {
+  const double rho = U[0];
+  const double u[3] = {U[1] / rho, U[2] / rho, U[3] / rho};
+  const double q2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const double p = (G - 1) * (U[4] - 0.5 * rho * q2);
+  const double vn = dot3(u, n);
+  const double H = (U[4] + p) / rho;
+  const double phi = 0.5 * (G - 1) * q2;
+  A[0][0] = 0.0;
+  for (int m = 0; m < 3; ++m) A[0][m + 1] = n[m];
+  A[0][4] = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    A[k + 1][0] = phi * n[k] - u[k] * vn;
+    for (int m = 0; m < 3; ++m) {
+      double a = u[k] * n[m] - (G - 1) * u[m] * n[k];
+      A[k + 1][m + 1] = k == m ? a + vn : a;
+    }
+    A[k + 1][4] = (G - 1) * n[k];
+  }
+  A[4][0] = vn * (phi - H);
+  for (int m = 0; m < 3; ++m) A[4][m + 1] = H * n[m] - (G - 1) * u[m] * vn;
+  A[4][4] = G * vn;
+}
+
+// d(two_wave flux)/dU_L and /dU_R at frozen sl, sr
+static void two_wave_jac(const double* wl, const double* wr, const double* n, double JL[5][5], double JR[5][5]) {
+  double rhol = wl[0], vnl = dot3(wl + 1, n), pl = wl[4], al = sound_speed_w(wl), ul[5];
+  p2c(wl, ul);
+  double rhor = wr[0], vnr = dot3(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr), ur[5];
+  p2c(wr, ur);
+  double lam_l = fmax2(fmax2(al * rhol, std::sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+  double lam_r = fmax2(fmax2(ar * rhor, std::sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+  double sl = vnl - lam_l / rhol, sr = vnr + lam_r / rhor;
+  double AL[5][5], AR[5][5];
+  euler_jac(ul, n, AL);
+  euler_jac(ur, n, AR);
+  const double den = sr - sl, asl = std::fabs(sl), asr = std::fabs(sr), d = asl - asr;
+  for (int r = 0; r < 5; ++r)
+    for (int c = 0; c < 5; ++c) {
+      const bool I = r == c;
+      double dL = (AL[r][c] - (I ? sl : 0.0)) / den;
+      double dR = ((I ? sr : 0.0) - AR[r][c]) / den;
+      JL[r][c] = 0.5 * AL[r][c] - 0.5 * (d * dL - (I ? asl : 0.0));
+      JR[r][c] = 0.5 * AR[r][c] - 0.5 * (d * dR + (I ? asr : 0.0));
+    }
+}
+
+// Pattern (rows sorted, self included) and values of A = V/dt I - d rhs/dU; blocks are
+// (5, 5) column-major as bcsr_matrix_type stores them. Cells' subfaces in ascending id.
+void be_jacobian(const Mesh& m, const NsCfg& cfg, const double* sol, double dt, std::vector<int>& row,
+                 std::vector<int>& col, std::vector<double>& v) {
+  row.assign(m.n_elems + 1, 1);
+  col.clear();
+  std::vector<std::vector<int>> cols(m.n_elems + 1);
+  for (int i = 1; i <= m.n_elems; ++i) {
+    std::vector<int> cs{i};
+    for (int k = 1; k <= m.elem[i].n_sub_faces; ++k) {
+      const Face& f = m.face[m.sub_face[m.elem[i].sub_face[k]].mesh_face];
+      int o = f.left_neigh == i ? f.right_neigh : f.left_neigh;
+      if (o > 0) cs.push_back(o);
+    }
+    std::sort(cs.begin(), cs.end());
+    cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+    cols[i] = cs;
+    row[i] = row[i - 1] + (int)cs.size();
+    col.insert(col.end(), cs.begin(), cs.end());
+  }
+  v.assign((size_t)25 * col.size(), 0.0);
+  auto blk = [&](int i, int j) -> double* {
+    const auto& cs = cols[i];
+    int q = (int)(std::lower_bound(cs.begin(), cs.end(), j) - cs.begin());
+    return &v[(size_t)25 * (row[i - 1] - 1 + q)];
+  };
+  for (int i = 1; i <= m.n_elems; ++i) {
+    double* D = blk(i, i);
+    const double vdt = m.elem[i].volume / dt;
+    for (int r = 0; r < 5; ++r) D[r + 5 * r] = vdt;
+    for (int k = 1; k <= m.elem[i].n_sub_faces; ++k) {
+      const int sf = m.elem[i].sub_face[k];
+      const SubFace& s = m.sub_face[sf];
+      const Face& f = m.face[s.mesh_face];
+      const double* n = &s.norm[1];
+      const double area = s.area;
+      const int L = f.left_neigh, R = f.right_neigh;
+      double wl[5], wr[5];
+      reconstruct_lr_w(m, cfg, sol, nullptr, s.mesh_vert, sf, L, R, false, wl, wr);
+      double JL[5][5], JR[5][5];
+      two_wave_jac(wl, wr, n, JL, JR);
+      if (i == L) {
+        if (R > 0) {
+          for (int r = 0; r < 5; ++r)
+            for (int c = 0; c < 5; ++c) D[r + 5 * c] = D[r + 5 * c] + area * JL[r][c];
+          double* O = blk(i, R);
+          for (int r = 0; r < 5; ++r)
+            for (int c = 0; c < 5; ++c) O[r + 5 * c] = O[r + 5 * c] + area * JR[r][c];
+        } else {  // ghost state U_R(U_L): wall M = momentum reflection, outflow I, freestream 0
+          const int kind = R == 0 ? 1 : cfg.bc_type[-R - 1];
+          double M[5][5] = {{0}};
+          if (kind == 1) {
+            M[0][0] = M[4][4] = 1.0;
+            for (int a = 0; a < 3; ++a)
+              for (int b = 0; b < 3; ++b) M[a + 1][b + 1] = (a == b ? 1.0 : 0.0) - 2.0 * n[a] * n[b];
+          } else if (kind == 4) {
+            for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
+          }
+          for (int r = 0; r < 5; ++r)
+            for (int c = 0; c < 5; ++c) {
+              double t = 0.0;
+              for (int q = 0; q < 5; ++q) t = t + JR[r][q] * M[q][c];
+              D[r + 5 * c] = D[r + 5 * c] + area * (JL[r][c] + t);
+            }
+        }
+      } else {
+        for (int r = 0; r < 5; ++r)
+          for (int c = 0; c < 5; ++c) D[r + 5 * c] = D[r + 5 * c] - area * JR[r][c];
+        double* O = blk(i, L);
+        for (int r = 0; r < 5; ++r)
+          for (int c = 0; c < 5; ++c) O[r + 5 * c] = O[r + 5 * c] - area * JL[r][c];
+      }
+    }
+  }
+}
+
 int oracle_pinv3(double* a9) {
   double A[3][3];
   for (int i = 0; i < 3; ++i)
@@ -776,6 +907,18 @@ int or_ns_run(void* h, const int* ic, const double* dc, const int* bc_type, cons
 }
 void or_ns_gresho(void* h, double mach, double* sol) { init_gresho(handle_mesh(h), mach, sol); }
 void or_pinv3(double* a9) { oracle_pinv3(a9); }
+// returns nnz blocks; row (n_elems+1), col (nnz) 1-based, v (25 nnz); cap = capacity of col
+long or_be_jacobian(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val,
+                    const double* sol, double dt, int* row, int* col, double* v, long cap) {
+  std::vector<int> r, c;
+  std::vector<double> vv;
+  be_jacobian(handle_mesh(h), make_cfg(ic, dc, bc_type, bc_val), sol, dt, r, c, vv);
+  if ((long)c.size() > cap) return -(long)c.size();
+  std::memcpy(row, r.data(), r.size() * sizeof(int));
+  std::memcpy(col, c.data(), c.size() * sizeof(int));
+  std::memcpy(v, vv.data(), vv.size() * sizeof(double));
+  return (long)c.size();
+}
 void or_lu3(double* a9, double* x, const double* b) { oracle_lu3(a9, x, b); }
 
 }  // extern "C"

@@ -63,6 +63,8 @@ SIGNATURES = {
     "subfv_ns_get_sol": (c_int, [P, PD]),
     "subfv_ns_residuals": (c_int, [P, PD, PD, PD]),
     "subfv_ns_init_gresho": (c_int, [P, c_dbl, PD]),
+    "subfv_ns_implicit_step": (c_int, [P, c_dbl, c_int, c_dbl, c_int, P]),
+    "subfv_ns_be_jacobian": (c_int, [P, c_dbl, PI32, PI32, PD, c_i64]),
     "subfv_bcsr_create": (c_int, [c_int, c_int, PI32, PI32, PD, C.POINTER(P)]),
     "subfv_bcsr_destroy": (c_int, [P]),
     "subfv_bcsr_set_values": (c_int, [P, PD]),

@@ -855,6 +855,137 @@ __global__ void k_ns_apply(DevMesh m, const double* __restrict__ U_td, const dou
 
 __global__ void k_ns_reset_omega(NsScalars* sc) { sc->omega = 1.0; }
 
+// ---------------------------------------------------------------------------------
+// Backward-Euler Jacobian (no counterpart in the reference): A = V/dt I - d rhs/dU of
+// the first-order two-wave residual with sl, sr frozen. One thread per block row, which
+// owns all of its blocks, so the assembly needs no atomics and is deterministic.
+
+// dF.n/dU for the Euler flux, conservative variables
+__device__ void euler_jac(const double* U, const double* n, double A[5][5]) {
+  const double rho = U[0];
+  const double u[3] = {U[1] / rho, U[2] / rho, U[3] / rho};
+  const double q2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+  const double p = (G - 1) * (U[4] - 0.5 * rho * q2);
+  const double vn = dotT(u, n);
+  const double H = (U[4] + p) / rho;
+  const double phi = 0.5 * (G - 1) * q2;
+  A[0][0] = 0.0;
+  for (int mm = 0; mm < 3; ++mm) A[0][mm + 1] = n[mm];
+  A[0][4] = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    A[k + 1][0] = phi * n[k] - u[k] * vn;
+    for (int mm = 0; mm < 3; ++mm) {
+      const double a = u[k] * n[mm] - (G - 1) * u[mm] * n[k];
+      A[k + 1][mm + 1] = k == mm ? a + vn : a;
+    }
+    A[k + 1][4] = (G - 1) * n[k];
+  }
+  A[4][0] = vn * (phi - H);
+  for (int mm = 0; mm < 3; ++mm) A[4][mm + 1] = H * n[mm] - (G - 1) * u[mm] * vn;
+  A[4][4] = G * vn;
+}
+
+__device__ void two_wave_jac(const double* wl, const double* wr, const double* n, double JL[5][5],
+                             double JR[5][5]) {
+  const double rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], al = sound_speed_w(wl);
+  const double rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr);
+  double ul[5], ur[5];
+  p2c(wl, ul);
+  p2c(wr, ur);
+  const double lam_l = fmax2(fmax2(al * rhol, sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+  const double lam_r = fmax2(fmax2(ar * rhor, sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+  const double sl = vnl - lam_l / rhol, sr = vnr + lam_r / rhor;
+  double AL[5][5], AR[5][5];
+  euler_jac(ul, n, AL);
+  euler_jac(ur, n, AR);
+  const double den = sr - sl, asl = fabs(sl), asr = fabs(sr), d = asl - asr;
+  for (int r = 0; r < 5; ++r)
+    for (int c = 0; c < 5; ++c) {
+      const bool I = r == c;
+      const double dL = (AL[r][c] - (I ? sl : 0.0)) / den;
+      const double dR = ((I ? sr : 0.0) - AR[r][c]) / den;
+      JL[r][c] = 0.5 * AL[r][c] - 0.5 * (d * dL - (I ? asl : 0.0));
+      JR[r][c] = 0.5 * AR[r][c] - 0.5 * (d * dR + (I ? asr : 0.0));
+    }
+}
+
+// jq: per cell its subfaces (2*sf + side) in ascending id; jblk: the block of the other
+// cell (-1 for a boundary); row_off/dblk: the row's first block and its diagonal block.
+__global__ void __launch_bounds__(64) k_be_assemble(DevMesh m, NsParams P, const double* __restrict__ U,
+                                                    const int* __restrict__ jq_off, const int* __restrict__ jq,
+                                                    const int* __restrict__ jblk, const int* __restrict__ row_off,
+                                                    const int* __restrict__ dblk, double* __restrict__ v, double dt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  for (size_t q = (size_t)25 * row_off[c]; q < (size_t)25 * row_off[c + 1]; ++q) v[q] = 0.0;
+  double* D = v + (size_t)25 * dblk[c];
+  const double vdt = m.vol[c] / dt;
+  for (int r = 0; r < 5; ++r) D[r + 5 * r] = vdt;
+  for (int q = jq_off[c]; q < jq_off[c + 1]; ++q) {
+    const int e = jq[q];
+    const int sf = e >> 1, side = e & 1;
+    const int2 lr = m.flr[m.sf_face[sf]];
+    const double4 sn = m.sfn[sf];
+    const double n[3] = {sn.x, sn.y, sn.z};
+    const double area = sn.w;
+    double wl[5], wr[5];
+    reconstruct<double>(m, P, U, nullptr, m.sf_vert[sf], sf, lr.x, lr.y, false, wl, wr);
+    double JL[5][5], JR[5][5];
+    two_wave_jac(wl, wr, n, JL, JR);
+    if (side == 0) {
+      if (lr.y >= 0) {
+        for (int r = 0; r < 5; ++r)
+          for (int cc = 0; cc < 5; ++cc) D[r + 5 * cc] = D[r + 5 * cc] + area * JL[r][cc];
+        double* O = v + (size_t)25 * jblk[q];
+        for (int r = 0; r < 5; ++r)
+          for (int cc = 0; cc < 5; ++cc) O[r + 5 * cc] = O[r + 5 * cc] + area * JR[r][cc];
+      } else {  // ghost U_R(U_L): wall M = momentum reflection, outflow I, freestream 0
+        const int kind = lr.y == -1 ? 1 : P.bc_type[-(lr.y + 1) - 1];
+        double M[5][5];
+        for (int a = 0; a < 5; ++a)
+          for (int b = 0; b < 5; ++b) M[a][b] = 0.0;
+        if (kind == 1) {
+          M[0][0] = M[4][4] = 1.0;
+          for (int a = 0; a < 3; ++a)
+            for (int b = 0; b < 3; ++b) M[a + 1][b + 1] = (a == b ? 1.0 : 0.0) - 2.0 * n[a] * n[b];
+        } else if (kind == 4) {
+          for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
+        }
+        for (int r = 0; r < 5; ++r)
+          for (int cc = 0; cc < 5; ++cc) {
+            double t = 0.0;
+            for (int k = 0; k < 5; ++k) t = t + JR[r][k] * M[k][cc];
+            D[r + 5 * cc] = D[r + 5 * cc] + area * (JL[r][cc] + t);
+          }
+      }
+    } else {
+      for (int r = 0; r < 5; ++r)
+        for (int cc = 0; cc < 5; ++cc) D[r + 5 * cc] = D[r + 5 * cc] - area * JR[r][cc];
+      double* O = v + (size_t)25 * jblk[q];
+      for (int r = 0; r < 5; ++r)
+        for (int cc = 0; cc < 5; ++cc) O[r + 5 * cc] = O[r + 5 * cc] - area * JL[r][cc];
+    }
+  }
+}
+
+// b = rhs (the first five entries of each residual record), and U += x after the solve
+__global__ void k_be_pack_rhs(int ne, const double* __restrict__ rhs, double* __restrict__ b) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ne) return;
+  for (int k = 0; k < 5; ++k) b[5 * (size_t)c + k] = rhs[kRhs * (size_t)c + k];
+}
+__global__ void k_be_update(DevMesh m, double* __restrict__ U, const double* __restrict__ x) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  bool fin = true;
+  for (int k = 0; k < 5; ++k) {
+    U[kRec * (size_t)c + k] = U[kRec * (size_t)c + k] + x[5 * (size_t)c + k];
+    fin = fin && isfinite(U[kRec * (size_t)c + k]);
+  }
+  if (!fin) atomicOr(m.status, kErrNonFinite);
+  if (!(U[kRec * (size_t)c] > 0.0)) atomicOr(m.status, kErrNegDensity);
+}
+
 // flux_limiting alone (ns_euler_recon_module.F90:560-601): rhs1 <- blend(rhs1, rhs2)
 __global__ void k_ns_flux_limiting(DevMesh m, NsParams P, const double* __restrict__ U, double* __restrict__ rhs1,
                                    const double* __restrict__ rhs2, const NsScalars* sc) {
@@ -889,6 +1020,17 @@ int ns_partial_blocks(const DevMesh& m) { return grid_for(m.ne, kTdBlock); }
 void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* U, double* rhs1, const double* rhs2,
                              const NsScalars* sc) {
   k_ns_flux_limiting<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, P, U, rhs1, rhs2, sc);
+}
+
+void launch_be_assemble(const DevMesh& m, const NsParams& P, const double* U, const int* jq_off, const int* jq,
+                        const int* jblk, const int* row_off, const int* dblk, double* v, double dt) {
+  k_be_assemble<<<grid_for(m.ne, 64), 64, 0, m.stream>>>(m, P, U, jq_off, jq, jblk, row_off, dblk, v, dt);
+}
+void launch_be_pack_rhs(const DevMesh& m, const double* rhs, double* b) {
+  k_be_pack_rhs<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m.ne, rhs, b);
+}
+void launch_be_update(const DevMesh& m, double* U, const double* x) {
+  k_be_update<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, U, x);
 }
 
 void launch_ns_pack(const DevMesh& m, const double* s5, double* U) {

@@ -41,6 +41,11 @@ void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs
 void launch_ns_pack(const DevMesh& m, const double* s5, double* U);
 void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* U, double* rhs1, const double* rhs2,
                              const NsScalars* sc);
+// Backward-Euler Jacobian of the first-order two-wave residual (frozen wave speeds)
+void launch_be_assemble(const DevMesh& m, const NsParams& P, const double* U, const int* jq_off, const int* jq,
+                        const int* jblk, const int* row_off, const int* dblk, double* v, double dt);
+void launch_be_pack_rhs(const DevMesh& m, const double* rhs, double* b);
+void launch_be_update(const DevMesh& m, double* U, const double* x);
 int ns_partial_blocks(const DevMesh& m);
 
 }  // namespace subfv

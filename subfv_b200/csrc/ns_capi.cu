@@ -3,10 +3,24 @@
 #include <cstring>
 #include <vector>
 
+#include <algorithm>
+
+#include "bcsr.cuh"
 #include "handles.cuh"
 #include "ns.cuh"
 
 using namespace subfv;
+
+// Backward-Euler context: the Jacobian's BCSR pattern on the mesh's cell adjacency and
+// the GMRES workspace.
+struct ImplicitCtx {
+  DevBcsr A;
+  GmresWork W;
+  int *jq_off = nullptr, *jq = nullptr, *jblk = nullptr, *row_off = nullptr, *dblk = nullptr;
+  double *b = nullptr, *x = nullptr;
+  std::vector<int> row1, col1;  // 1-based pattern (bcsr_matrix_type)
+  int krylov = 0;
+};
 
 struct subfv_ns_state {
   subfv_mesh* m = nullptr;
@@ -16,6 +30,7 @@ struct subfv_ns_state {
   NsScalars* sc = nullptr;
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
+  ImplicitCtx* imp = nullptr;
 };
 
 namespace {
@@ -159,6 +174,16 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
 
 int subfv_ns_state_destroy(subfv_ns_state* s) {
   if (!s) return 0;
+  if (s->imp) {
+    ImplicitCtx* c = s->imp;
+    int* ip[] = {c->jq_off, c->jq, c->jblk, c->row_off, c->dblk};
+    for (int* p : ip) cudaFree(p);
+    cudaFree(c->b);
+    cudaFree(c->x);
+    gmres_work_free(&c->W);
+    bcsr_free(&c->A);
+    delete c;
+  }
   if (s->graph) cudaGraphExecDestroy(s->graph);
   double* bufs[] = {s->U0, s->U1, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->delta, s->partial, s->stage};
   for (double* b : bufs) cudaFree(b);
@@ -215,6 +240,197 @@ int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double*
     for (int k = 0; k < 5; ++k) res_vect[k] = h.resv[k];
   if (dt) *dt = h.dt;
   return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+template <class T>
+int up(T** d, const std::vector<T>& h, cudaStream_t s) {
+  SUBFV_CUDA(cudaMalloc((void**)d, std::max<size_t>(h.size(), 1) * sizeof(T)));
+  if (!h.empty()) SUBFV_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return 0;
+}
+
+// Pattern: row i holds i and the other cells of its subfaces, ascending. A cell's
+// subfaces are those of elem%sub_face: every subface it is left of, and those it is right
+// of through its own subcell at the subface's vertex (not a periodic image's).
+int implicit_setup(subfv_ns_state* s, int krylov) {
+  if (s->imp && s->imp->krylov == krylov) return 0;
+  DevMesh& d = s->m->d;
+  if (!s->imp) {
+    auto* c = new ImplicitCtx();
+    s->imp = c;
+    std::vector<int2> flr(d.nf), sse(d.nsf);
+    std::vector<int> sff(d.nsf), sfv(d.nsf), sev(d.nse);
+    SUBFV_CUDA(cudaMemcpyAsync(flr.data(), d.flr, d.nf * sizeof(int2), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaMemcpyAsync(sse.data(), d.sf_se, d.nsf * sizeof(int2), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaMemcpyAsync(sff.data(), d.sf_face, d.nsf * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaMemcpyAsync(sfv.data(), d.sf_vert, d.nsf * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaMemcpyAsync(sev.data(), d.se_vert, d.nse * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+    const int ne = d.ne;
+    std::vector<int> jq_off(ne + 1, 0);
+    auto owns_right = [&](int sf) { return sse[sf].y >= 0 && sev[sse[sf].y] == sfv[sf]; };
+    for (int sf = 0; sf < d.nsf; ++sf) {
+      const int2 lr = flr[sff[sf]];
+      jq_off[lr.x + 1]++;
+      if (lr.y >= 0 && owns_right(sf)) jq_off[lr.y + 1]++;
+    }
+    for (int i = 0; i < ne; ++i) jq_off[i + 1] += jq_off[i];
+    std::vector<int> jq(jq_off[ne]), other(jq_off[ne]);
+    {
+      std::vector<int> fill(jq_off.begin(), jq_off.end() - 1);
+      for (int sf = 0; sf < d.nsf; ++sf) {
+        const int2 lr = flr[sff[sf]];
+        other[fill[lr.x]] = lr.y;
+        jq[fill[lr.x]++] = 2 * sf;
+        if (lr.y >= 0 && owns_right(sf)) {
+          other[fill[lr.y]] = lr.x;
+          jq[fill[lr.y]++] = 2 * sf + 1;
+        }
+      }
+    }
+    std::vector<int> row_off(ne + 1, 0), col, dblk(ne), jblk(jq.size(), -1);
+    for (int i = 0; i < ne; ++i) {
+      std::vector<int> cs{i};
+      for (int q = jq_off[i]; q < jq_off[i + 1]; ++q)
+        if (other[q] >= 0) cs.push_back(other[q]);
+      std::sort(cs.begin(), cs.end());
+      cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+      for (int q = jq_off[i]; q < jq_off[i + 1]; ++q)
+        if (other[q] >= 0) jblk[q] = row_off[i] + (int)(std::lower_bound(cs.begin(), cs.end(), other[q]) - cs.begin());
+      dblk[i] = row_off[i] + (int)(std::lower_bound(cs.begin(), cs.end(), i) - cs.begin());
+      col.insert(col.end(), cs.begin(), cs.end());
+      row_off[i + 1] = (int)col.size();
+    }
+    c->row1.resize(ne + 1);
+    c->col1.resize(col.size());
+    for (int i = 0; i <= ne; ++i) c->row1[i] = row_off[i] + 1;
+    for (size_t j = 0; j < col.size(); ++j) c->col1[j] = col[j] + 1;
+    if (bcsr_upload(&c->A, ne, 5, c->row1.data(), c->col1.data(), nullptr, d.stream)) return -1;
+    if (up(&c->jq_off, jq_off, d.stream) || up(&c->jq, jq, d.stream) || up(&c->jblk, jblk, d.stream) ||
+        up(&c->row_off, row_off, d.stream) || up(&c->dblk, dblk, d.stream))
+      return -1;
+    SUBFV_CUDA(cudaMalloc(&c->b, 5 * (size_t)ne * sizeof(double)));
+    SUBFV_CUDA(cudaMalloc(&c->x, 5 * (size_t)ne * sizeof(double)));
+  }
+  ImplicitCtx* c = s->imp;
+  gmres_work_free(&c->W);
+  if (gmres_work_alloc(&c->W, 5L * d.ne, krylov)) return -1;
+  c->krylov = krylov;
+  return 0;
+}
+
+NsParams implicit_params(const NsParams& P) {
+  NsParams q = P;
+  q.scheme = 4;  // the implicit residual: first-order two-wave
+  q.second_order = 0;
+  q.precision = 0;
+  return q;
+}
+
+// residual at U0, dt = cfl_implicit * min V/sum_lambda (host), Jacobian at U0
+int implicit_assemble(subfv_ns_state* s, double cfl_implicit, double dt_force, double* dt_out) {
+  DevMesh& d = s->m->d;
+  ImplicitCtx* c = s->imp;
+  const NsParams Q = implicit_params(s->P);
+  NsScalars h{};
+  SUBFV_CUDA(cudaMemcpyAsync(&h, s->sc, sizeof(h), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  h.dtred = 1e10;
+  h.omega = 1.0;
+  h.done = 0;
+  SUBFV_CUDA(cudaMemcpyAsync(s->sc, &h, sizeof(h), cudaMemcpyHostToDevice, d.stream));
+  launch_ns_rhs(d, Q, s->U0, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->sc);
+  double dtred = 0.0;
+  SUBFV_CUDA(cudaMemcpyAsync(&dtred, &s->sc->dtred, sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  const double dt = dt_force > 0.0 ? dt_force : cfl_implicit * dtred;
+  launch_be_assemble(d, Q, s->U0, c->jq_off, c->jq, c->jblk, c->row_off, c->dblk, c->A.v, dt);
+  launch_be_pack_rhs(d, s->rhs1, c->b);
+  if (bcsr_set_values(&c->A, c->A.v, true)) return -1;
+  *dt_out = dt;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
+                           subfv_implicit_stats* out) {
+  if (!s || krylov < 1 || krylov > 200 || !(rel_tol > 0.0)) {
+    set_error("subfv_ns_implicit_step: bad argument");
+    return -2;
+  }
+  DevMesh& d = s->m->d;
+  if (handle_clear_status(d) || implicit_setup(s, krylov)) return -1;
+  ImplicitCtx* c = s->imp;
+  cudaEvent_t e[4];
+  for (auto& q : e) SUBFV_CUDA(cudaEventCreate(&q));
+  SUBFV_CUDA(cudaEventRecord(e[0], d.stream));
+  double dt = 0.0;
+  if (implicit_assemble(s, cfl_implicit, 0.0, &dt)) return -1;
+  SUBFV_CUDA(cudaEventRecord(e[1], d.stream));
+  GmresStats st;
+  const double bnorm = device_norm2(c->A, c->W, c->b, 5L * d.ne);
+  if (refine_fp32) {
+    if (gmres_refine_device(c->A, c->W, c->x, c->b, rel_tol, 1e-3, 30, &st)) return -1;
+  } else {
+    if (gmres_device(c->A, c->W, c->x, c->b, rel_tol * bnorm, true, false, 40, &st, nullptr)) return -1;
+  }
+  SUBFV_CUDA(cudaEventRecord(e[2], d.stream));
+  launch_be_update(d, s->U0, c->x);
+  {  // t += dt
+    NsScalars h{};
+    SUBFV_CUDA(cudaMemcpyAsync(&h, s->sc, sizeof(h), cudaMemcpyDeviceToHost, d.stream));
+    SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+    h.t = h.t + dt;
+    h.dt = dt;
+    h.steps += 1;
+    h.dtred = 1e10;
+    h.omega = 1.0;
+    SUBFV_CUDA(cudaMemcpyAsync(s->sc, &h, sizeof(h), cudaMemcpyHostToDevice, d.stream));
+  }
+  SUBFV_CUDA(cudaEventRecord(e[3], d.stream));
+  SUBFV_CUDA(cudaEventSynchronize(e[3]));
+  float ms[3];
+  for (int k = 0; k < 3; ++k) SUBFV_CUDA(cudaEventElapsedTime(&ms[k], e[k], e[k + 1]));
+  for (auto& q : e) cudaEventDestroy(q);
+  if (out) {
+    out->dt = dt;
+    out->conv = st.conv;
+    out->restarts = refine_fp32 ? st.inner_total : st.restarts;
+    out->outer = st.outer;
+    out->b_norm = bnorm;
+    out->res_norm = st.rho;
+    out->ms_assemble = ms[0];
+    out->ms_solve = ms[1];
+    out->ms_update = ms[2];
+    out->nnz_blocks = c->A.nnz;
+  }
+  int stbits = handle_check_status(d);
+  if (stbits < 0) return stbits;
+  return stbits | (st.conv ? 0 : SUBFV_ERR_GMRES);
+}
+
+int subfv_ns_be_jacobian(subfv_ns_state* s, double dt, int32_t* row, int32_t* col, double* v, int64_t cap) {
+  if (implicit_setup(s, 4)) return -1;
+  ImplicitCtx* c = s->imp;
+  if ((int64_t)c->col1.size() > cap) {
+    set_error("subfv_ns_be_jacobian: capacity too small");
+    return -2;
+  }
+  double dto = 0.0;
+  if (implicit_assemble(s, 1.0, dt, &dto)) return -1;
+  DevMesh& d = s->m->d;
+  std::memcpy(row, c->row1.data(), c->row1.size() * sizeof(int32_t));
+  std::memcpy(col, c->col1.data(), c->col1.size() * sizeof(int32_t));
+  SUBFV_CUDA(cudaMemcpyAsync(v, c->A.v, (size_t)25 * c->A.nnz * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  return (int)c->col1.size();
 }
 
 int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs, double* sum_lambda,

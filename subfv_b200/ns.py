@@ -29,6 +29,12 @@ class NsCfgC(C.Structure):
                 ("precision", C.c_int32)]
 
 
+class ImplicitStats(C.Structure):
+    _fields_ = [("dt", C.c_double), ("b_norm", C.c_double), ("res_norm", C.c_double), ("conv", C.c_int32),
+                ("restarts", C.c_int32), ("outer", C.c_int32), ("ms_assemble", C.c_double),
+                ("ms_solve", C.c_double), ("ms_update", C.c_double), ("nnz_blocks", C.c_int64)]
+
+
 @dataclass
 class NsConfig:
     """The namelist keys of ns_global_data_module.F90:177-213 that the residual path reads."""
@@ -74,6 +80,29 @@ def init_gresho(mesh: Mesh, mach: float) -> np.ndarray:
     sol = np.empty((mesh.n_elems, 5))
     check(_lib.load().subfv_ns_init_gresho(mesh._h, float(mach), pd(sol)), "subfv_ns_init_gresho")
     return sol
+
+
+def init_fourier_flow(mesh: Mesh, mach=0.3, n_modes=8, amp=0.05, seed=0, gamma=1.4) -> np.ndarray:
+    """Uniform flow along x at Mach `mach` (rho = 1, |u| = 1) plus `n_modes` seeded
+    divergence-free Fourier modes of velocity with relative amplitude `amp`, periodic on
+    the unit box; conservative variables at the cell centroids."""
+    rng = np.random.default_rng(seed)
+    x = mesh.geometry("elem_coord")
+    u = np.zeros_like(x)
+    u[:, 0] = 1.0
+    for _ in range(n_modes):
+        k = rng.integers(-3, 4, size=3)
+        while not k.any():
+            k = rng.integers(-3, 4, size=3)
+        a = rng.normal(size=3)
+        a -= (a @ k) / (k @ k) * k  # transverse: divergence free
+        a *= amp / np.linalg.norm(a)
+        phase = rng.uniform(0, 2 * np.pi)
+        u += np.sin(2 * np.pi * (x @ k) + phase)[:, None] * a[None, :]
+    rho = np.ones(len(x))
+    p = rho / (gamma * mach ** 2)  # sound speed 1/mach
+    E = p / (gamma - 1) + 0.5 * rho * (u ** 2).sum(1)
+    return np.ascontiguousarray(np.column_stack([rho, rho[:, None] * u, E]))
 
 
 def compute_rhs_ns(mesh: Mesh, cfg: NsConfig, sol):
@@ -124,6 +153,25 @@ class NsState:
         rv = np.zeros(5)
         check(_lib.load().subfv_ns_residuals(self._h, C.byref(res), pd(rv), C.byref(dt)), "subfv_ns_residuals")
         return res.value, rv, dt.value
+
+    def implicit_step(self, cfl_implicit=10.0, krylov=30, rel_tol=1e-8, refine_fp32=False):
+        """One backward-Euler step (first-order two-wave residual, exact frozen-speed
+        Jacobian, block-Jacobi GMRES); returns (status bits, stats dict)."""
+        st = ImplicitStats()
+        rc = check(_lib.load().subfv_ns_implicit_step(self._h, float(cfl_implicit), int(krylov), float(rel_tol),
+                                                      int(refine_fp32), C.byref(st)), "subfv_ns_implicit_step")
+        return rc, {k: getattr(st, k) for k, _ in ImplicitStats._fields_}
+
+    def be_jacobian(self, dt):
+        """(row, col, v (nnz, 5, 5)) of V/dt I - d rhs/dU at the current state."""
+        ne = self.mesh.n_elems
+        cap = 64 * ne
+        row = np.zeros(ne + 1, np.int32)
+        col = np.zeros(cap, np.int32)
+        v = np.zeros(25 * cap)
+        nnz = check(_lib.load().subfv_ns_be_jacobian(self._h, float(dt), row.ctypes.data_as(_lib.PI32),
+                                                     col.ctypes.data_as(_lib.PI32), pd(v), cap), "be_jacobian")
+        return row, col[:nnz].copy(), v[:25 * nnz].reshape(nnz, 5, 5).copy()
 
     def close(self):
         if getattr(self, "_h", None):
