@@ -49,6 +49,10 @@ def _args():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--n", type=int, default=N_SIDE)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="lagrange", choices=["lagrange", "gresho", "implicit", "shocktubes"])
+    p.add_argument("--problems", type=int, default=1024)
+    p.add_argument("--nmax", type=int, default=20000)
+    p.add_argument("--solo-sample", type=int, default=64)
     return p.parse_args()
 
 
@@ -211,9 +215,274 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+def _time_device(stream, fn):
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def run_gresho(args, rank, world, local):
+    """2-D Gresho vortex, explicit Euler (subfvns): 64x64 hex slab on [-0.5,0.5]^2,
+    interior vertices jittered +-10% of h (seed 1), slip walls, peak Mach 0.1, multi_point
+    nodal solver, second order (method 4), two-stage scheme, CFL 0.4, 200 iterations
+    (n_max_iter = 199). One cell-update = one cell advanced one iteration."""
+    import torch
+    from subfv_b200 import meshgen
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsConfig, NsState, init_gresho
+    n = 64 if args.n == N_SIDE else args.n
+    raw = meshgen.hex_slab(n, n, jitter=0.1, seed=SEED)
+    mesh = Mesh.from_raw(raw)
+    sol0 = init_gresho(mesh, 0.1)
+    out = {}
+    for prec_name, prec in (("fp64", 0), ("mixed", 1)):
+        cfg = NsConfig(cfl=0.4, precision=prec)
+        s = NsState(mesh, cfg, sol0)
+        s.advance(args.warmup)
+        s.sync()
+        s2 = NsState(mesh, cfg, sol0)
+        stream = torch.cuda.ExternalStream(int(_libmod().load().subfv_mesh_stream(mesh._h)))
+        torch.cuda.synchronize()
+        ms = _time_device(stream, lambda: s2.advance_async(200))
+        st, steps, t = s2.sync()
+        out[prec_name] = {"ms": ms, "steps": steps, "status": st, "sol": s2.sol()}
+    a, b = out["fp64"]["sol"], out["mixed"]["sol"]
+    scale = np.abs(a).sum(0)
+    l1 = {k: float(np.abs(a[:, i] - b[:, i]).sum() / max(scale[i], 1e-6 * scale[1:4].max()))
+          for i, k in enumerate(["rho", "rho_u", "rho_v", "rho_w", "E"])}
+    cells = mesh.n_elems
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle.oracle import OracleMesh
+        o = OracleMesh(raw)
+        so = o.ns_gresho(0.1)
+        t0 = time.perf_counter()
+        o.ns_run(NsConfig(cfl=0.4).oracle_dict(), so, 19)
+        el = time.perf_counter() - t0
+        cpu = {"value": 20 * cells / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+               "sample": f"20 of the 200 iterations on the same mesh, serial C++ restatement, {el:.1f} s"}
+        parity = float(np.abs(so - out["fp64"]["sol"]).max()) if False else None
+    res = {"metric": "cell-updates/s", "workload": "gresho2d_ns_multipoint_o2_64x64",
+           "value": cells * 200 / (out["fp64"]["ms"] / 1e3), "unit": "cell-updates/s",
+           "mixed_value": cells * 200 / (out["mixed"]["ms"] / 1e3),
+           "ms_per_iteration": out["fp64"]["ms"] / 200, "cells": cells, "iterations": 200,
+           "mixed_l1_rel_vs_fp64": l1, "status": [out["fp64"]["status"], out["mixed"]["status"]],
+           "dtype": "f64", "cpu_baseline": cpu}
+    print(json.dumps(res), flush=True)
+
+
+def run_implicit(args, rank, world, local):
+    """3-D periodic box [-0.5,0.5]^3 (the reference's stitching frame), 96^3 hexahedra
+    (884,736 cells), interior vertices jittered +-5% of h (seed 1); uniform flow at Mach
+    0.3 plus 8 seeded Fourier velocity modes (5%); one backward-Euler step: first-order
+    two-wave residual, its exact frozen-speed Jacobian (5x5 BCSR, 7-point face stencil),
+    block-Jacobi GMRES(30) to 1e-8 relative, CFL 10. FP64 GMRES and FP32-matrix GMRES
+    inside FP64 iterative refinement."""
+    import torch
+    from subfv_b200 import meshgen
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsConfig, NsState, init_fourier_flow
+    n = 96 if args.n == N_SIDE else args.n
+    t0 = time.perf_counter()
+    raw = meshgen.hex_box(n, jitter=0.05, seed=SEED, periodic=True)
+    mesh = Mesh.from_raw(raw)
+    setup_s = time.perf_counter() - t0
+    sol0 = init_fourier_flow(mesh, seed=SEED)
+    cfg = NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5)
+    res = {"metric": "cell-updates/s", "workload": f"periodic_box_{n}^3_backward_euler", "cells": mesh.n_elems,
+           "mesh_setup_s": setup_s}
+    for name, refine in (("fp64", False), ("fp32_refine", True)):
+        s = NsState(mesh, cfg, sol0)
+        s.implicit_step(cfl_implicit=10.0, refine_fp32=refine)  # warm-up (pattern, workspace)
+        s2 = NsState(mesh, cfg, sol0)
+        s2.implicit_step(cfl_implicit=10.0, refine_fp32=refine)
+        s3 = NsState(mesh, cfg, sol0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st, stats = s3.implicit_step(cfl_implicit=10.0, refine_fp32=refine)
+        el = time.perf_counter() - t0
+        stats["wall_ms"] = el * 1e3
+        stats["status"] = st
+        stats["cell_updates_per_s"] = mesh.n_elems / el
+        res[name] = stats
+    from subfv_b200.bcsr import DeviceBcsr
+    res["value"] = res["fp64"]["cell_updates_per_s"]
+    res["unit"] = "cell-updates/s"
+    print(json.dumps(res), flush=True)
+
+
+def _build_meshes(raws, local, threads=None):
+    """Device meshes for a list of raw meshes, built on host threads (the topology build
+    and the upload release the GIL); host topology is dropped once the mesh is on the
+    device."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from subfv_b200.mesh import Mesh
+
+    def one(raw):
+        torch.cuda.set_device(local)
+        m = Mesh.from_raw(raw() if callable(raw) else raw)
+        m.topo.close()
+        m.topo = None
+        return m
+
+    n_thr = threads or max(1, min(32, (os.cpu_count() or 2) - 1))
+    with ThreadPoolExecutor(n_thr) as ex:
+        return list(ex.map(one, raws))
+
+
+def _l1_rel(a, b):
+    """Per-field L1 relative difference; near-zero fields (transverse momenta) are
+    scaled by the largest momentum component's L1 norm."""
+    scale = np.abs(a).sum(0)
+    mom = scale[1:4].max()
+    return [float(np.abs(a[:, i] - b[:, i]).sum() / max(scale[i], 1e-3 * mom, 1e-300)) for i in range(5)]
+
+
+def autotune_batch(batch, steps=2, log=None):
+    """Pick the batched launch shape: coordinate search over the vertex-kernel block
+    (64/128/256 vertices) and the persistent grid sizes (multiples of the 148 SMs),
+    each candidate timed on the device over `steps` steps of the live batch (the steps
+    are real: problems advance). Results do not depend on the shape."""
+    sms = 148
+    best = (128, sms * 8, sms * 8)
+    batch.set_launch(*best)
+    batch.time_steps(1)
+    t_best = batch.time_steps(steps)
+    trials = [(best, t_best)]
+
+    def try_(shape):
+        nonlocal best, t_best
+        batch.set_launch(*shape)
+        batch.time_steps(1)
+        t = batch.time_steps(steps)
+        trials.append((shape, t))
+        if t < t_best:
+            best, t_best = shape, t
+
+    for mult in (2, 4, 16, 32, 64):
+        try_((best[0], best[1], sms * mult))
+    for bv in (64, 256):
+        try_((bv, best[1], best[2]))
+    for mult in (2, 4, 16, 32, 64):
+        try_((best[0], sms * mult, best[2]))
+    batch.set_launch(*best)
+    if log is not None:
+        log.extend({"block_v": s[0], "grid_v": s[1], "grid_c": s[2], "ms_per_step": t / steps} for s, t in trials)
+    return best, t_best / steps
+
+
+def run_shocktubes(args, rank, world, local):
+    """Batched shock tubes: `--problems` (1024) independent Riemann problems on N x 4 quad
+    strips, N uniform in [200, 20000] (seed 1), states as in subfv_b200.shocktube, first
+    order multi_point nodal solver, CFL 0.4, walls all round. Timed: K steps of the whole
+    batch in shared launches (graph-replayed), FP32 flux arithmetic with FP64 nodal
+    solver and accumulation ("mixed"), autotuned and fixed launch shapes, plus the plain
+    FP64 batch; the baseline is the plain FP64 path run one problem at a time
+    (subfv_ns_state, graph-replayed) over a sample of the problems."""
+    import torch
+    from subfv_b200 import shocktube
+    from subfv_b200.ns import NsBatch, NsConfig, NsState
+    rng_tubes = shocktube.sample(args.problems, seed=SEED, n_max=args.nmax)
+    t0 = time.perf_counter()
+    meshes = _build_meshes([(lambda t=t: shocktube.raw_mesh(t)) for t in rng_tubes], local)
+    setup_s = time.perf_counter() - t0
+    sols = [shocktube.initial_state(m, t) for m, t in zip(meshes, rng_tubes)]
+    cells = sum(m.n_elems for m in meshes)
+    base = dict(scheme=1, second_order=False, method=4, bc_style=2, boundary_2d=True, cfl=0.4)
+    budget = int(150e9)
+    res = {"metric": "cell-updates/s", "workload": f"shocktubes_{args.problems}_strips_Nx4",
+           "problems": args.problems, "cells": cells, "mesh_setup_s": setup_s,
+           "mesh_bytes": sum(m.device_bytes for m in meshes)}
+    K = args.steps
+    for name, prec in (("mixed", 1), ("fp64", 0)):
+        b = NsBatch(NsConfig(**base, precision=prec), capacity=args.problems, budget_bytes=budget)
+        slots = [b.add(m, s, t.t_end) for m, s, t in zip(meshes, sols, rng_tubes)]
+        assert None not in slots
+        log = []
+        best, _ = autotune_batch(b, log=log)
+        for _ in range(args.warmup):
+            b.time_steps(1)
+        sampler = ClockSampler(local)
+        sampler.start()
+        ms_tuned = b.time_steps(K)
+        clocks = sampler.stop()
+        b.set_launch(128, 148 * 8, 148 * 8)
+        b.time_steps(1)
+        ms_fixed = b.time_steps(K)
+        b.sync()
+        st = max(b.info(k)[3] for k in slots)
+        res[name] = {"value": cells * K / (ms_tuned / 1e3), "ms_per_step": ms_tuned / K,
+                     "fixed_value": cells * K / (ms_fixed / 1e3), "fixed_ms_per_step": ms_fixed / K,
+                     "tuned_shape": {"block_v": best[0], "grid_v": best[1], "grid_c": best[2]},
+                     "autotune_trials": log, "status": st, "clocks": clocks,
+                     "state_bytes": sum(b.state_bytes(m) for m in meshes)}
+        b.close()
+        torch.cuda.synchronize()
+    # plain FP64, one problem at a time, over a sample of the problems
+    idx = np.random.default_rng(SEED + 1).choice(args.problems, size=min(args.solo_sample, args.problems),
+                                                 replace=False)
+    solo_ms, solo_cells = 0.0, 0
+    for i in idx:
+        m, s, t = meshes[i], sols[i], rng_tubes[i]
+        st_ = NsState(m, NsConfig(**base, precision=0, tmax=t.t_end), s)
+        st_.advance(8)
+        st_.sync()
+        stream = torch.cuda.ExternalStream(int(_libmod().load().subfv_mesh_stream(m._h)))
+        solo_ms += _time_device(stream, lambda: st_.advance_async(K))
+        solo_cells += m.n_elems * K
+        st_.close()
+    res["solo_fp64"] = {"value": solo_cells / (solo_ms / 1e3), "problems": len(idx),
+                        "note": "plain FP64 path, one problem at a time, K steps each"}
+    # accuracy of the mixed path: a sample of small problems run to their end time
+    acc_idx = [i for i in range(args.problems) if rng_tubes[i].n <= 2000][:16]
+    if acc_idx:
+        outs = {}
+        for name, prec in (("fp64", 0), ("mixed", 1)):
+            b = NsBatch(NsConfig(**base, precision=prec), capacity=len(acc_idx), budget_bytes=budget)
+            sl = [b.add(meshes[i], sols[i], rng_tubes[i].t_end) for i in acc_idx]
+            while True:
+                b.advance(64)
+                b.sync()
+                if all(b.info(k)[2] for k in sl):
+                    break
+            outs[name] = [b.sol(k, meshes[i].n_elems) for k, i in zip(sl, acc_idx)]
+            b.close()
+        l1 = np.array([_l1_rel(a, c) for a, c in zip(outs["fp64"], outs["mixed"])])
+        drift = []
+        for i, a, c in zip(acc_idx, outs["fp64"], outs["mixed"]):
+            vol = meshes[i].geometry("elem_volume")
+            t0_ = (sols[i] * vol[:, None]).sum(0)
+            for u in (a, c):
+                t1_ = (u * vol[:, None]).sum(0)
+                drift.append([float(abs(t1_[k] - t0_[k]) / abs(t0_[k])) for k in (0, 4)])
+        res["mixed_accuracy"] = {"problems": len(acc_idx), "l1_rel_max_per_field": l1.max(0).tolist(),
+                                 "l1_rel_mean_per_field": l1.mean(0).tolist(),
+                                 "mass_energy_drift_max": np.array(drift).max(0).tolist(),
+                                 "note": "run to each problem's end time; fields rho, rho u, rho v, rho w, E"}
+    res["value"] = res["mixed"]["value"]
+    res["unit"] = "cell-updates/s"
+    print(json.dumps(res), flush=True)
+
+
+def _libmod():
+    from subfv_b200 import _lib
+    return _lib
+
+
 def main():
     args = _args()
     rank, world, local = _dist()
+    if args.workload != "lagrange":
+        import torch
+        torch.cuda.set_device(local)
+        {"gresho": run_gresho, "implicit": run_implicit,
+         "shocktubes": run_shocktubes}[args.workload](args, rank, world, local)
+        return
     import torch
     import torch.distributed as dist
     from datetime import timedelta

@@ -204,6 +204,53 @@ int subfv_ns_be_jacobian(subfv_ns_state* s, double dt, int32_t* row, int32_t* co
 int subfv_ns_init_gresho(subfv_mesh* m, double mach, double* sol);
 
 /* ---------------------------------------------------------------------------------
+ * Batched and served explicit Euler. No counterpart in the reference, whose
+ * ns_main.F90:83-107 loop advances one mesh per process: here many independent problems
+ * (each its own mesh, initial state and end time, one shared subfv_ns_cfg) are advanced
+ * together in shared persistent launches with the step loop captured in a CUDA graph.
+ * Each problem's result is bit-identical to the same problem run alone through
+ * subfv_ns_state. Problems may join (subfv_ns_batch_add) and leave
+ * (subfv_ns_batch_remove) between calls while earlier steps are still running. */
+#define SUBFV_BATCH_FULL (-3) /* no free slot or the HBM budget is exhausted: retry later */
+typedef struct subfv_ns_batch subfv_ns_batch;
+/* capacity: the most problems in flight; budget_bytes: the device bytes that admitted
+ * problems (their meshes plus their state) may hold. */
+int subfv_ns_batch_create(const subfv_ns_cfg* cfg, int capacity, int64_t budget_bytes, subfv_ns_batch** out);
+int subfv_ns_batch_destroy(subfv_ns_batch* b);
+/* Device bytes of the per-problem state batch b allocates for a problem on mesh m. */
+int64_t subfv_ns_batch_state_bytes(const subfv_ns_batch* b, const subfv_mesh* m);
+int64_t subfv_ns_batch_free_bytes(const subfv_ns_batch* b);
+int subfv_ns_batch_size(const subfv_ns_batch* b, int* n_live, int64_t* used_bytes);
+/* Admit a problem: mesh (with geometry computed), sol (5, n_elems) conservative, start
+ * time t0 and end time tmax. take_mesh != 0 hands the mesh over: the batch destroys it
+ * when the problem is removed. Returns SUBFV_BATCH_FULL when it cannot be admitted now. */
+int subfv_ns_batch_add(subfv_ns_batch* b, subfv_mesh* m, int take_mesh, const double* sol, double t0, double tmax,
+                       int* slot);
+int subfv_ns_batch_remove(subfv_ns_batch* b, int slot);
+/* Enqueue n_steps steps of every problem (finished problems are skipped on the device)
+ * and a snapshot of every problem's time, step count, done flag and status. Returns
+ * without waiting. */
+int subfv_ns_batch_advance(subfv_ns_batch* b, int n_steps);
+/* subfv_ns_batch_advance timed on the device (CUDA events around the enqueued steps,
+ * including the snapshot copy); waits for the end of the steps. */
+int subfv_ns_batch_time_steps(subfv_ns_batch* b, int n_steps, double* ms);
+/* Take the oldest outstanding snapshot: wait != 0 blocks for it; wait == 0 returns 1 if
+ * it is not complete yet. */
+int subfv_ns_batch_poll(subfv_ns_batch* b, int wait);
+/* Wait for everything enqueued and take a snapshot of the state after it. */
+int subfv_ns_batch_sync(subfv_ns_batch* b);
+/* From the latest snapshot taken: returns 1 (and t0, 0 steps) while no snapshot taken
+ * covers the problem yet. */
+int subfv_ns_batch_slot_info(const subfv_ns_batch* b, int slot, double* t, int64_t* steps, int* done,
+                             unsigned* status);
+/* Copy a problem's state to the host (waits for the queued steps unless the latest
+ * snapshot shows the problem finished). */
+int subfv_ns_batch_get_sol(subfv_ns_batch* b, int slot, double* sol);
+/* Launch shape: block_v vertices per block of the vertex kernels (64, 128 or 256), and
+ * the persistent grid sizes of the vertex and cell kernels. Results do not depend on it. */
+int subfv_ns_batch_set_launch(subfv_ns_batch* b, int block_v, int grid_v, int grid_c);
+
+/* ---------------------------------------------------------------------------------
  * Block-CSR linear algebra (src/linear_algebra/sparse_bcsr_linear_module.F90).
  * bcsr_matrix_type layout: m block rows, row(m+1) and col(nnz) 1-based, values
  * v(bs, bs, nnz) column-major blocks. Vectors have bs*m entries (host arrays). */

@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -33,18 +34,32 @@ def _stale() -> bool:
     return any(p.stat().st_mtime > t for p in deps)
 
 
+def _headers():
+    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [PKG.parent / "include" / "subfv.h"]
+
+
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not _stale():
         return LIB
     OUT_DIR.mkdir(exist_ok=True)
-    objs = []
+    newest_header = max(p.stat().st_mtime for p in _headers())
+    jobs = []
     for src in sources():
         obj = OUT_DIR / (src.name + ".o")
+        fresh = obj.exists() and obj.stat().st_mtime > max(src.stat().st_mtime, newest_header)
         cmd = [NVCC, *ARCH, *FLAGS, "-I", str(PKG.parent / "include"), "-c", str(src), "-o", str(obj)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(str(obj))
+        jobs.append((cmd, obj, force or not fresh))
+
+    def run(job):
+        cmd, obj, todo = job
+        if todo:
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+        return str(obj)
+
+    with ThreadPoolExecutor(max_workers=max(1, min(8, os.cpu_count() or 1))) as ex:
+        objs = list(ex.map(run, jobs))
     tmp = LIB.with_suffix(".so.tmp")
     subprocess.run([NVCC, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *objs], check=True)
     os.replace(tmp, LIB)

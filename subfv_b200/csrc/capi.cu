@@ -192,11 +192,11 @@ int subfv_mesh_create_from_topology(const subfv_topology* tp, int b2d, subfv_mes
 
 int subfv_mesh_destroy(subfv_mesh* m) {
   if (!m) return 0;
-  cudaFree(m->stage);
-  cudaFree(m->sol6);
-  cudaFree(m->rhs6);
-  cudaFree(m->mass);
-  cudaFree(m->sc);
+  // scratch of the stateless calls (allocated on first use only); a mesh that never
+  // needed it is released without any device-wide synchronisation
+  void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc};
+  for (void* p : scratch)
+    if (p) cudaFree(p);
   devmesh_free(&m->d);
   delete m;
   return 0;

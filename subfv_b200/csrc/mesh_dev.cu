@@ -15,16 +15,16 @@ namespace {
 template <class T>
 int upload(T** dst, const std::vector<T>& h, size_t* bytes, cudaStream_t s) {
   size_t n = std::max<size_t>(h.size(), 1);
-  SUBFV_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
+  SUBFV_CUDA(cudaMallocAsync((void**)dst, n * sizeof(T), s));
   *bytes += n * sizeof(T);
   if (!h.empty()) SUBFV_CUDA(cudaMemcpyAsync(*dst, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
   return 0;
 }
 template <class T>
-int alloc(T** dst, size_t n, size_t* bytes) {
+int alloc(T** dst, size_t n, size_t* bytes, cudaStream_t s) {
   n = std::max<size_t>(n, 1);
-  SUBFV_CUDA(cudaMalloc((void**)dst, n * sizeof(T)));
-  SUBFV_CUDA(cudaMemset(*dst, 0, n * sizeof(T)));
+  SUBFV_CUDA(cudaMallocAsync((void**)dst, n * sizeof(T), s));
+  SUBFV_CUDA(cudaMemsetAsync(*dst, 0, n * sizeof(T), s));
   *bytes += n * sizeof(T);
   return 0;
 }
@@ -166,17 +166,17 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
 
   if (upload(&m->vel_off, vel_off, B, s) || upload(&m->vel, vel, B, s) || upload(&m->cse_sorted, cse_sorted, B, s))
     return -1;
-  if (upload(&m->x, x, B, s) || alloc(&m->vp, nv, B) || alloc(&m->vol_v, nv, B) || upload(&m->is_bound, isb, B, s) ||
+  if (upload(&m->x, x, B, s) || alloc(&m->vp, nv, B, s) || alloc(&m->vol_v, nv, B, s) || upload(&m->is_bound, isb, B, s) ||
       upload(&m->fvert, fvert, B, s) || upload(&m->flr, flr, B, s) || upload(&m->fsf, fsf, B, s) ||
-      alloc(&m->fc, nf, B) || alloc(&m->fn, nf, B) || upload(&m->sf_face, sf_face, B, s) ||
+      alloc(&m->fc, nf, B, s) || alloc(&m->fn, nf, B, s) || upload(&m->sf_face, sf_face, B, s) ||
       upload(&m->sf_vert, sf_vert, B, s) || upload(&m->sf_se, sf_se, B, s) || upload(&m->sf_loc, sf_loc, B, s) ||
-      alloc(&m->sfn, nsf, B) || upload(&m->se_elem, se_elem, B, s) || upload(&m->se_vert, se_vert, B, s) ||
-      upload(&m->se_loc, se_loc, B, s) || upload(&m->se_sf, se_sf, B, s) || alloc(&m->vol_se, nse, B) ||
+      alloc(&m->sfn, nsf, B, s) || upload(&m->se_elem, se_elem, B, s) || upload(&m->se_vert, se_vert, B, s) ||
+      upload(&m->se_loc, se_loc, B, s) || upload(&m->se_sf, se_sf, B, s) || alloc(&m->vol_se, nse, B, s) ||
       upload(&m->ev_off, ev_off, B, s) || upload(&m->ev, ev, B, s) || upload(&m->ef8, ef8, B, s) ||
-      upload(&m->ekind, ekind, B, s) || alloc(&m->cc, ne, B) || alloc(&m->vol, ne, B) ||
+      upload(&m->ekind, ekind, B, s) || alloc(&m->cc, ne, B, s) || alloc(&m->vol, ne, B, s) ||
       upload(&m->vsf_off, vsf_off, B, s) || upload(&m->vsf, vsf, B, s) || upload(&m->p_node, p_node, B, s) ||
       upload(&m->vse_off, vse_off, B, s) || upload(&m->vse, vse, B, s) || upload(&m->csf_off, csf_off, B, s) ||
-      upload(&m->csf, csf, B, s) || alloc(&m->status, 4, B))
+      upload(&m->csf, csf, B, s) || alloc(&m->status, 4, B, s))
     return -1;
   SUBFV_CUDA(cudaStreamSynchronize(s));
   return 0;
@@ -188,8 +188,13 @@ void devmesh_free(DevMesh* m) {
                   m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
                   m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
                   m->vel_off, m->vel, m->cse_sorted};
+  // stream-ordered frees: they wait for the mesh stream's work but not for other
+  // streams (a caller that used the mesh elsewhere orders that work first)
   for (void* p : ptrs)
-    if (p) cudaFree(p);
+    if (p) {
+      if (m->stream) cudaFreeAsync(p, m->stream);
+      else cudaFree(p);
+    }
   if (m->stream) cudaStreamDestroy(m->stream);
   *m = DevMesh();
 }

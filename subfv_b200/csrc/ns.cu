@@ -468,11 +468,10 @@ __device__ void nodal_velocity(const DevMesh& m, const NsParams& P, int v, int p
 // compute_rhs_around_vert (ns_euler_module.F90:341-519) for one vertex; writes the
 // corner sums of the vertex's own subcells to fs (kNsFs doubles per subcell).
 template <class T>
-__global__ void __launch_bounds__(128) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
-                                                 const double* __restrict__ grad, double* __restrict__ fs, int so,
-                                                 const NsScalars* sc) {
+__device__ void ns_node_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
+                             const double* __restrict__ grad, double* __restrict__ fs, int so, const NsScalars* sc,
+                             const int v) {
   if (sc && sc->done) return;
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= m.nv) return;
   const int p0 = m.vsf_off[v], nsfn = m.vsf_off[v + 1] - p0;
   const int q0 = m.vse_off[v], nsen = m.vse_off[v + 1] - q0;
@@ -537,6 +536,13 @@ __global__ void __launch_bounds__(128) k_ns_node(DevMesh m, NsParams P, const do
   }
 }
 
+template <class T>
+__global__ void __launch_bounds__(128) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
+                                                 const double* __restrict__ grad, double* __restrict__ fs, int so,
+                                                 const NsScalars* sc) {
+  ns_node_body<T>(m, P, U, grad, fs, so, sc, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 __device__ inline double warp_min(double x) {
   for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
   return x;
@@ -548,10 +554,10 @@ __device__ inline double warp_sum_tree(double x) {
 
 // compute_euler_flux scatter (:320-336) as a gather: rhs = 0 - corners in ascending
 // vertex order; sum_lambda = 1e-12 + corners. Block min of V / sum_lambda into *dtred.
-__global__ void __launch_bounds__(128) k_ns_gather(DevMesh m, const double* __restrict__ fs, double* __restrict__ rhs,
-                                                   NsScalars* sc, int reduce) {
+// called by every thread of a 128-thread block (block reduction inside)
+__device__ void ns_gather_body(const DevMesh& m, const double* __restrict__ fs, double* __restrict__ rhs,
+                               NsScalars* sc, int reduce, const int c) {
   if (sc && sc->done) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   double dmin = 1e10;
   if (c < m.ne) {
     double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, sl = 1e-12;
@@ -577,11 +583,15 @@ __global__ void __launch_bounds__(128) k_ns_gather(DevMesh m, const double* __re
   }
 }
 
+__global__ void __launch_bounds__(128) k_ns_gather(DevMesh m, const double* __restrict__ fs, double* __restrict__ rhs,
+                                                   NsScalars* sc, int reduce) {
+  ns_gather_body(m, fs, rhs, sc, reduce, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // compute_nodal_grad (ns_euler_recon_module.F90:453-490); ng[15] = g[5*d + var]
-__global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* __restrict__ U,
-                                                       double* __restrict__ ngrad, const NsScalars* sc) {
+__device__ void ns_nodal_grad_body(const DevMesh& m, const double* __restrict__ U, double* __restrict__ ngrad,
+                                   const NsScalars* sc, const int v) {
   if (sc && sc->done) return;
-  const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= m.nv) return;
   double g[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
   double mat[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -614,13 +624,17 @@ __global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* 
     }
 }
 
+__global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* __restrict__ U,
+                                                       double* __restrict__ ngrad, const NsScalars* sc) {
+  ns_nodal_grad_body(m, U, ngrad, sc, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 // compute_cell_grad_method_4 + physical_slope_limiter + relaxed_maximum_principle
 template <class T>
-__global__ void __launch_bounds__(128) k_ns_cell_grad(DevMesh m, NsParams P, const double* __restrict__ U,
-                                                      const double* __restrict__ ngrad, double* __restrict__ grad,
-                                                      const NsScalars* sc) {
+__device__ void ns_cell_grad_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
+                                  const double* __restrict__ ngrad, double* __restrict__ grad, const NsScalars* sc,
+                                  const int c) {
   if (sc && sc->done) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ne) return;
   double* go = grad + 15 * (size_t)c;
   if (P.method == 0 || P.method == 1) {
@@ -718,23 +732,30 @@ __global__ void __launch_bounds__(128) k_ns_cell_grad(DevMesh m, NsParams P, con
   for (int i = 0; i < 15; ++i) go[i] = (double)(omega * g[i]);
 }
 
+template <class T>
+__global__ void __launch_bounds__(128) k_ns_cell_grad(DevMesh m, NsParams P, const double* __restrict__ U,
+                                                      const double* __restrict__ ngrad, double* __restrict__ grad,
+                                                      const NsScalars* sc) {
+  ns_cell_grad_body<T>(m, P, U, ngrad, grad, sc, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 constexpr int kTdBlock = 128;
 
 // flux_limiting (ns_euler_recon_module.F90:560-601) and the per-cell part of
 // add_timedisc_and_solve (ns_euler_module.F90:546-580). U_rhs: the state the residual
 // was evaluated at; U_td: the state being advanced. Writes delta, per-block omega min
 // (atomic on the bit pattern) and per-block residual partial sums (res, res_vect(5)).
-__global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P, const double* __restrict__ U_rhs,
-                                                          const double* __restrict__ rhs1,
-                                                          const double* __restrict__ rhs2,
-                                                          const double* __restrict__ U_td,
-                                                          double* __restrict__ delta, double* __restrict__ partial,
-                                                          NsScalars* sc, double a1, double a2) {
+// called by every thread of a kTdBlock-thread block; blk is the block's index within
+// its problem (it selects the slot of the residual partial sums)
+__device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U_rhs,
+                                 const double* __restrict__ rhs1, const double* __restrict__ rhs2,
+                                 const double* __restrict__ U_td, double* __restrict__ delta,
+                                 double* __restrict__ partial, NsScalars* sc, double a1, double a2, const int blk) {
   if (sc->done) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = blk * kTdBlock + threadIdx.x;
   const double dt_fl = P.cfl * sc->dtred;
   double dt = P.cfl * sc->dtred;
-  if (!P.lts) dt = fmin2(P.tmax - sc->t + 1e-12, dt);
+  if (!P.lts) dt = fmin2(sc->tmax - sc->t + 1e-12, dt);
   double om = 1.0, rn = 0.0, rv[5] = {0, 0, 0, 0, 0};
   if (c < m.ne) {
     const double V = m.vol[c];
@@ -800,20 +821,29 @@ __global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P,
     for (int i = 0; i < 6; ++i) {
       double s = sh[i][0];
       for (int w = 1; w < kTdBlock / 32; ++w) s = s + sh[i][w];
-      partial[6 * (size_t)blockIdx.x + i] = s;
+      partial[6 * (size_t)blk + i] = s;
     }
   }
 }
 
+__global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P, const double* __restrict__ U_rhs,
+                                                          const double* __restrict__ rhs1,
+                                                          const double* __restrict__ rhs2,
+                                                          const double* __restrict__ U_td,
+                                                          double* __restrict__ delta, double* __restrict__ partial,
+                                                          NsScalars* sc, double a1, double a2) {
+  ns_timedisc_body(m, P, U_rhs, rhs1, rhs2, U_td, delta, partial, sc, a1, a2, blockIdx.x);
+}
+
 // scalar tail of add_timedisc_and_solve (:582-608); last_stage also advances t
-__global__ void k_ns_finalize(NsScalars* sc, NsParams P, const double* __restrict__ partial, int nblocks,
-                              unsigned* status, int last_stage) {
+__device__ void ns_finalize_body(NsScalars* sc, const NsParams& P, const double* __restrict__ partial, int nblocks,
+                                 unsigned* status, int last_stage) {
   if (sc->done) {
     sc->skip = 1;
     return;
   }
   double dt = P.cfl * sc->dtred;
-  if (!P.lts) dt = fmin2(P.tmax - sc->t + 1e-12, dt);
+  if (!P.lts) dt = fmin2(sc->tmax - sc->t + 1e-12, dt);
   double res = 0.0, rv[5] = {0, 0, 0, 0, 0};
   for (int b = 0; b < nblocks; ++b) {
     res = res + partial[6 * (size_t)b];
@@ -830,15 +860,19 @@ __global__ void k_ns_finalize(NsScalars* sc, NsParams P, const double* __restric
   if (last_stage) {
     sc->t = sc->t + dt;
     sc->steps += 1;
-    sc->done = ((!P.lts && sc->t >= P.tmax) || !(res > sc->final_res)) ? 1 : 0;
+    sc->done = ((!P.lts && sc->t >= sc->tmax) || !(res > sc->final_res)) ? 1 : 0;
   }
 }
 
+__global__ void k_ns_finalize(NsScalars* sc, NsParams P, const double* __restrict__ partial, int nblocks,
+                              unsigned* status, int last_stage) {
+  ns_finalize_body(sc, P, partial, nblocks, status, last_stage);
+}
+
 // sol = sol + a2*omega*delta (:608); U_out may be U_td
-__global__ void k_ns_apply(DevMesh m, const double* __restrict__ U_td, const double* __restrict__ delta,
-                           double* __restrict__ U_out, NsScalars* sc, double a2) {
+__device__ void ns_apply_body(const DevMesh& m, const double* __restrict__ U_td, const double* __restrict__ delta,
+                              double* __restrict__ U_out, NsScalars* sc, double a2, const int c) {
   if (sc->skip) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ne) return;
   const double omega = sc->omega;
   const double* u = U_td + kRec * (size_t)c;
@@ -853,7 +887,106 @@ __global__ void k_ns_apply(DevMesh m, const double* __restrict__ U_td, const dou
   if (!(o[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
 }
 
+__global__ void k_ns_apply(DevMesh m, const double* __restrict__ U_td, const double* __restrict__ delta,
+                           double* __restrict__ U_out, NsScalars* sc, double a2) {
+  ns_apply_body(m, U_td, delta, U_out, sc, a2, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 __global__ void k_ns_reset_omega(NsScalars* sc) { sc->omega = 1.0; }
+
+// ---------------------------------------------------------------------------------
+// Batched launches over a table of problems. A persistent grid walks the work blocks of
+// all problems (vertex kernels: blockDim.x vertices per work block, cell kernels: 128
+// cells); each block finds its problem by binary search in the prefix table, so every
+// per-problem reduction sees exactly the blocks of a solo run and the results are the
+// solo results bit for bit. hdr[0] is the number of problems, read on the device so
+// that a captured step loop stays valid while problems join and leave.
+
+__device__ inline int item_of(const int* __restrict__ wofs, int n, int w) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (wofs[mid] <= w) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// which: the state the phase reads (0: U0, 1: U1)
+template <class T>
+__global__ void __launch_bounds__(256) kb_ns_node(const NsItem* __restrict__ it, const int* __restrict__ wv,
+                                                  const int* __restrict__ hdr, NsParams P, int which, int so) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
+    const int p = item_of(wv, n, w);
+    const NsItem& I = it[p];
+    ns_node_body<T>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, I.sc, (w - wv[p]) * blockDim.x + threadIdx.x);
+  }
+}
+__global__ void __launch_bounds__(128) kb_ns_gather(const NsItem* __restrict__ it, const int* __restrict__ wc,
+                                                    const int* __restrict__ hdr, int second) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wc[n]; w += gridDim.x) {
+    const int p = item_of(wc, n, w);
+    const NsItem& I = it[p];
+    ns_gather_body(I.m, I.fs, second ? I.rhs2 : I.rhs1, I.sc, second ? 0 : 1, (w - wc[p]) * 128 + threadIdx.x);
+    __syncthreads();  // the block-reduction scratch is reused by the next work block
+  }
+}
+__global__ void __launch_bounds__(256) kb_ns_nodal_grad(const NsItem* __restrict__ it, const int* __restrict__ wv,
+                                                        const int* __restrict__ hdr, int which) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
+    const int p = item_of(wv, n, w);
+    const NsItem& I = it[p];
+    ns_nodal_grad_body(I.m, which ? I.U1 : I.U0, I.ngrad, I.sc, (w - wv[p]) * blockDim.x + threadIdx.x);
+  }
+}
+template <class T>
+__global__ void __launch_bounds__(128) kb_ns_cell_grad(const NsItem* __restrict__ it, const int* __restrict__ wc,
+                                                       const int* __restrict__ hdr, NsParams P, int which) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wc[n]; w += gridDim.x) {
+    const int p = item_of(wc, n, w);
+    const NsItem& I = it[p];
+    ns_cell_grad_body<T>(I.m, P, which ? I.U1 : I.U0, I.ngrad, I.grad, I.sc, (w - wc[p]) * 128 + threadIdx.x);
+  }
+}
+// stage: 0 first stage of two (rhs at U0, advance U0 -> U1), 1 second stage (rhs at U1,
+// advance U0 in place), 2 the single first-order stage (rhs at U0, U0 in place)
+__global__ void __launch_bounds__(kTdBlock) kb_ns_timedisc(const NsItem* __restrict__ it, const int* __restrict__ wc,
+                                                           const int* __restrict__ hdr, NsParams P, int stage,
+                                                           double a1, double a2) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wc[n]; w += gridDim.x) {
+    const int p = item_of(wc, n, w);
+    const NsItem& I = it[p];
+    const double* Ur = stage == 1 ? I.U1 : I.U0;
+    ns_timedisc_body(I.m, P, Ur, I.rhs1, P.second_order ? I.rhs2 : nullptr, I.U0, I.delta, I.partial, I.sc, a1, a2,
+                     w - wc[p]);
+    __syncthreads();
+  }
+}
+__global__ void kb_ns_finalize(const NsItem* __restrict__ it, const int* __restrict__ hdr, NsParams P,
+                               int last_stage) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= hdr[0]) return;
+  const NsItem& I = it[p];
+  ns_finalize_body(I.sc, P, I.partial, (I.m.ne + kTdBlock - 1) / kTdBlock, I.m.status, last_stage);
+}
+__global__ void __launch_bounds__(128) kb_ns_apply(const NsItem* __restrict__ it, const int* __restrict__ wc,
+                                                   const int* __restrict__ hdr, int stage, double a2) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wc[n]; w += gridDim.x) {
+    const int p = item_of(wc, n, w);
+    const NsItem& I = it[p];
+    ns_apply_body(I.m, I.U0, I.delta, stage == 0 ? I.U1 : I.U0, I.sc, a2, (w - wc[p]) * 128 + threadIdx.x);
+  }
+}
+__global__ void kb_ns_reset_omega(const NsItem* __restrict__ it, const int* __restrict__ hdr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < hdr[0]) it[p].sc->omega = 1.0;
+}
 
 // ---------------------------------------------------------------------------------
 // Backward-Euler Jacobian (no counterpart in the reference): A = V/dt I - d rhs/dU of
@@ -1016,6 +1149,40 @@ __global__ void k_ns_pack(int n, const double* __restrict__ s5, double* __restri
 }  // namespace
 
 int ns_partial_blocks(const DevMesh& m) { return grid_for(m.ne, kTdBlock); }
+
+void launch_ns_batch_step(const NsTable& t, const NsParams& P, cudaStream_t s) {
+  const int gv = t.grid_v, gc = t.grid_c, bv = t.block_v, gp = grid_for(t.cap, 128);
+  auto node = [&](int which, int so) {
+    if (P.precision == 1) kb_ns_node<float><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+    else kb_ns_node<double><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  };
+  auto rhs = [&](int which) {
+    node(which, 0);
+    kb_ns_gather<<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, 0);
+    if (P.second_order) {
+      kb_ns_nodal_grad<<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, which);
+      if (P.precision == 1) kb_ns_cell_grad<float><<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, P, which);
+      else kb_ns_cell_grad<double><<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, P, which);
+      node(which, 1);
+      kb_ns_gather<<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, 1);
+    }
+  };
+  auto stage = [&](int st, double a1, double a2, int last) {
+    kb_ns_timedisc<<<gc, kTdBlock, 0, s>>>(t.items, t.wc, t.hdr, P, st, a1, a2);
+    kb_ns_finalize<<<gp, 128, 0, s>>>(t.items, t.hdr, P, last);
+    kb_ns_apply<<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, st, a2);
+    kb_ns_reset_omega<<<gp, 128, 0, s>>>(t.items, t.hdr);
+  };
+  if (P.second_order) {
+    rhs(0);
+    stage(0, 2.0, 1.0, 0);
+    rhs(1);
+    stage(1, 1.0, 1.0, 1);
+  } else {
+    rhs(0);
+    stage(2, 1.0, 1.0, 1);
+  }
+}
 
 void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* U, double* rhs1, const double* rhs2,
                              const NsScalars* sc) {

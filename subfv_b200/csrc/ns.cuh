@@ -26,7 +26,33 @@ struct NsScalars {
   double res, resv[5];
   unsigned long long steps;
   int done, skip;
+  double tmax;     // end time of this problem (tmax of the namelist)
 };
+
+// One problem of a batch: its mesh and state buffers. Batched launches walk a table of
+// these; work blocks never straddle two problems, so every per-problem reduction is the
+// same as in a solo run.
+struct NsItem {
+  DevMesh m;
+  double *U0, *U1, *fs, *rhs1, *rhs2, *ngrad, *grad, *delta, *partial;
+  NsScalars* sc;
+};
+
+// Table of in-flight problems on the device: items, work-block prefixes over their
+// vertices (wv, block_v vertices per work block) and cells (wc, 128 cells per work
+// block), and hdr[0] = the number of problems. Up to cap problems; the grids are
+// persistent (grid_v, grid_c blocks whatever the table holds).
+struct NsTable {
+  NsItem* items = nullptr;
+  int* wv = nullptr;
+  int* wc = nullptr;
+  int* hdr = nullptr;
+  int cap = 0;
+  int block_v = 128, grid_v = 1, grid_c = 1;
+};
+constexpr int kNsCellBlock = 128;
+// One step of the time loop for every problem of the table, in shared launches.
+void launch_ns_batch_step(const NsTable& t, const NsParams& P, cudaStream_t s);
 
 NsParams ns_params_from(const subfv_ns_cfg& c);
 

@@ -162,6 +162,7 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
   h.omega = 1.0;
   h.t = t0;
   h.final_res = -1.0;
+  h.tmax = s->P.tmax;
   h.done = (t0 < s->P.tmax) ? 0 : 1;
   SUBFV_CUDA(cudaMemcpyAsync(s->sc, &h, sizeof(h), cudaMemcpyHostToDevice, d.stream));
   SUBFV_CUDA(cudaMemcpyAsync(s->stage, sol, 5 * ne * sizeof(double), cudaMemcpyHostToDevice, d.stream));
@@ -450,6 +451,7 @@ int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* s
     h.dtred = 1e10;
     h.omega = 1.0;
     h.t = 0.0;
+    h.tmax = s->P.tmax;
     if (cudaMemcpyAsync(s->sc, &h, sizeof(h), cudaMemcpyHostToDevice, d.stream) != cudaSuccess) {
       st = -1;
       break;

@@ -183,3 +183,97 @@ class NsState:
             self.close()
         except Exception:
             pass
+
+
+SUBFV_BATCH_FULL = -3
+
+
+class NsBatch:
+    """Many independent explicit Euler problems advanced together in shared launches
+    (no counterpart in the reference, which runs one mesh per process). Each problem's
+    result is bit-identical to the same problem run alone through NsState."""
+
+    def __init__(self, cfg: NsConfig, capacity: int, budget_bytes: int):
+        self.cfg = cfg
+        self._c = cfg.to_c()
+        h = C.c_void_p()
+        check(_lib.load().subfv_ns_batch_create(C.byref(self._c), int(capacity), int(budget_bytes), C.byref(h)),
+              "subfv_ns_batch_create")
+        self._h = h
+        self._meshes = {}  # slot -> Mesh kept alive while the batch uses it
+
+    def state_bytes(self, mesh: Mesh) -> int:
+        """Device bytes of the state this batch allocates for a problem on `mesh`."""
+        return int(_lib.load().subfv_ns_batch_state_bytes(self._h, mesh._h))
+
+    def time_steps(self, n_steps: int) -> float:
+        """Advance every problem n_steps; device milliseconds (CUDA events)."""
+        ms = C.c_double()
+        check(_lib.load().subfv_ns_batch_time_steps(self._h, int(n_steps), C.byref(ms)), "subfv_ns_batch_time_steps")
+        return ms.value
+
+    def free_bytes(self) -> int:
+        return int(_lib.load().subfv_ns_batch_free_bytes(self._h))
+
+    def size(self):
+        n, used = C.c_int(), C.c_int64()
+        check(_lib.load().subfv_ns_batch_size(self._h, C.byref(n), C.byref(used)), "subfv_ns_batch_size")
+        return n.value, used.value
+
+    def add(self, mesh: Mesh, sol, tmax: float, t0: float = 0.0, take_mesh: bool = False):
+        """Admit a problem; returns its slot, or None when the batch is full (retry later).
+        take_mesh hands the device mesh over: the batch frees it when the slot is removed."""
+        sol = f64(sol)
+        slot = C.c_int(-1)
+        rc = _lib.load().subfv_ns_batch_add(self._h, mesh._h, int(take_mesh), pd(sol), float(t0), float(tmax),
+                                            C.byref(slot))
+        if rc == SUBFV_BATCH_FULL:
+            return None
+        check(rc, "subfv_ns_batch_add")
+        if take_mesh:
+            mesh._h = None  # owned by the batch now
+        else:
+            self._meshes[slot.value] = mesh
+        return slot.value
+
+    def remove(self, slot: int):
+        check(_lib.load().subfv_ns_batch_remove(self._h, int(slot)), "subfv_ns_batch_remove")
+        self._meshes.pop(slot, None)
+
+    def advance(self, n_steps: int):
+        check(_lib.load().subfv_ns_batch_advance(self._h, int(n_steps)), "subfv_ns_batch_advance")
+
+    def poll(self, wait: bool = True) -> bool:
+        """Take the oldest outstanding snapshot; False if not complete yet (wait=False)."""
+        return check(_lib.load().subfv_ns_batch_poll(self._h, int(wait)), "subfv_ns_batch_poll") == 0
+
+    def sync(self):
+        check(_lib.load().subfv_ns_batch_sync(self._h), "subfv_ns_batch_sync")
+
+    def info(self, slot: int):
+        """(t, steps, done, status bits) from the latest snapshot taken."""
+        t, steps, done, st = C.c_double(), C.c_int64(), C.c_int(), C.c_uint()
+        check(_lib.load().subfv_ns_batch_slot_info(self._h, int(slot), C.byref(t), C.byref(steps), C.byref(done),
+                                                   C.byref(st)), "subfv_ns_batch_slot_info")
+        return t.value, steps.value, bool(done.value), st.value
+
+    def sol(self, slot: int, n_elems: int) -> np.ndarray:
+        out = np.empty((n_elems, 5))
+        check(_lib.load().subfv_ns_batch_get_sol(self._h, int(slot), pd(out)), "subfv_ns_batch_get_sol")
+        return out
+
+    def set_launch(self, block_v: int, grid_v: int, grid_c: int):
+        check(_lib.load().subfv_ns_batch_set_launch(self._h, int(block_v), int(grid_v), int(grid_c)),
+              "subfv_ns_batch_set_launch")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().subfv_ns_batch_destroy(self._h)
+            self._h = None
+            self._meshes.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
