@@ -246,8 +246,9 @@ int subfv_ns_batch_slot_info(const subfv_ns_batch* b, int slot, double* t, int64
 /* Copy a problem's state to the host (waits for the queued steps unless the latest
  * snapshot shows the problem finished). */
 int subfv_ns_batch_get_sol(subfv_ns_batch* b, int slot, double* sol);
-/* Launch shape: block_v vertices per block of the vertex kernels (64, 128 or 256), and
- * the persistent grid sizes of the vertex and cell kernels. Results do not depend on it. */
+/* Launch shape: block_v threads (one per vertex) per block of the vertex kernels (64,
+ * 128 or 256), and the persistent grid sizes of the vertex and cell kernels. Results do
+ * not depend on it. */
 int subfv_ns_batch_set_launch(subfv_ns_batch* b, int block_v, int grid_v, int grid_c);
 
 /* ---------------------------------------------------------------------------------

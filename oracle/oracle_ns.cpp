@@ -71,8 +71,49 @@ double max_omega_for_positivity(const double* U, const double* dU) {
 }
 
 // ---------------------------------------------------------------- LAPACK stand-ins
-// A[r][c] = mat(r+1, c+1). One-sided Jacobi on the columns: A V = U S.
+// When every singular value passes the cut, the pseudo-inverse is the inverse. The cut
+// (3e-12 * sigma_max) is certainly passed when |det A| > 3e-12 ||A||_F^3, because
+// sigma_min >= |det A| / sigma_max^2 and sigma_max <= ||A||_F. Then A^-1 = adj(A) / det,
+// refined by one Newton step X <- X + X (I - A X); otherwise the Jacobi SVD below runs.
+static bool inv3_if_regular(double A[3][3]) {
+  double f2 = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) f2 = f2 + A[i][j] * A[i][j];
+  double C[3][3];  // cofactors
+  C[0][0] = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+  C[0][1] = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+  C[0][2] = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+  C[1][0] = A[0][2] * A[2][1] - A[0][1] * A[2][2];
+  C[1][1] = A[0][0] * A[2][2] - A[0][2] * A[2][0];
+  C[1][2] = A[0][1] * A[2][0] - A[0][0] * A[2][1];
+  C[2][0] = A[0][1] * A[1][2] - A[0][2] * A[1][1];
+  C[2][1] = A[0][2] * A[1][0] - A[0][0] * A[1][2];
+  C[2][2] = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+  const double det = A[0][0] * C[0][0] + A[0][1] * C[0][1] + A[0][2] * C[0][2];
+  if (!(det * det > 9e-24 * (f2 * f2 * f2))) return false;
+  const double r = 1.0 / det;
+  double X[3][3], R[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) X[i][j] = C[j][i] * r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = i == j ? 1.0 : 0.0;
+      for (int k = 0; k < 3; ++k) s = s - A[i][k] * X[k][j];
+      R[i][j] = s;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = s + X[i][k] * R[k][j];
+      A[i][j] = X[i][j] + s;
+    }
+  return true;
+}
+
+// A[r][c] = mat(r+1, c+1). The inverse when the cut cannot bite, else one-sided Jacobi
+// on the columns: A V = U S.
 void pinv3(double A[3][3]) {
+  if (inv3_if_regular(A)) return;
   double U[3][3], V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   std::memcpy(U, A, sizeof(U));
   const int pr[3][2] = {{0, 1}, {0, 2}, {1, 2}};

@@ -129,6 +129,9 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
     }
   }
   for (size_t k = 0; k < vse.size(); ++k) vse[k] = d->vert_sub_elem[k] - 1;
+  int max_vse = 0;
+  for (int v = 0; v < nv; ++v) max_vse = std::max(max_vse, vse_off[v + 1] - vse_off[v]);
+  m->max_vse = max_vse;
   m->nvsf = nvsf;
   m->vsf_identity = ident ? 1 : 0;
   m->max_vsf = max_vsf;

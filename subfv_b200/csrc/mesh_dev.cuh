@@ -28,7 +28,7 @@ struct DevMesh {
   int nv = 0, ne = 0, nf = 0, nsf = 0, nse = 0, nvsf = 0, ncsf = 0;
   int b2d = 1;
   int vsf_identity = 0;  // vsf[p] == p for every p (no periodic extension)
-  int max_vsf = 0;
+  int max_vsf = 0, max_vse = 0;  // the most subfaces / subcells around one vertex
   // vertices
   double4* x = nullptr;
   double4* vp = nullptr;

@@ -24,6 +24,7 @@
 // residual norms (res, res_vect), which are summed by a fixed tree of block partials.
 // Precision 1 evaluates reconstruction, limiters and subface fluxes in FP32; the nodal
 // velocity solver, the nodal gradient system and all sums stay FP64.
+#include <algorithm>
 #include <cstring>
 
 #include "ns.cuh"
@@ -103,10 +104,55 @@ __device__ double max_omega_for_positivity(const double* U, const double* dU) {
   return omega;
 }
 
-// Pseudo-inverse of a 3x3 matrix (A[r][c] = mat(r+1, c+1)) by one-sided Jacobi SVD,
-// six sweeps, singular values below 3e-12 * max discarded (the cut of
-// pseudo_inverse_inplace_lapack, linear_solver_module.F90:683-715).
-__device__ void pinv3(double A[3][3]) {
+// When every singular value passes the cut, the pseudo-inverse is the inverse. The cut
+// (3e-12 * sigma_max) is certainly passed when |det A| > 3e-12 ||A||_F^3, because
+// sigma_min >= |det A| / sigma_max^2 and sigma_max <= ||A||_F. Then A^-1 = adj(A) / det,
+// refined by one Newton step X <- X + X (I - A X); otherwise the Jacobi SVD below runs.
+__device__ bool inv3_if_regular(double A[3][3]) {
+  double f2 = 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) f2 = f2 + A[i][j] * A[i][j];
+  double C[3][3];  // cofactors
+  C[0][0] = A[1][1] * A[2][2] - A[1][2] * A[2][1];
+  C[0][1] = A[1][2] * A[2][0] - A[1][0] * A[2][2];
+  C[0][2] = A[1][0] * A[2][1] - A[1][1] * A[2][0];
+  C[1][0] = A[0][2] * A[2][1] - A[0][1] * A[2][2];
+  C[1][1] = A[0][0] * A[2][2] - A[0][2] * A[2][0];
+  C[1][2] = A[0][1] * A[2][0] - A[0][0] * A[2][1];
+  C[2][0] = A[0][1] * A[1][2] - A[0][2] * A[1][1];
+  C[2][1] = A[0][2] * A[1][0] - A[0][0] * A[1][2];
+  C[2][2] = A[0][0] * A[1][1] - A[0][1] * A[1][0];
+  const double det = A[0][0] * C[0][0] + A[0][1] * C[0][1] + A[0][2] * C[0][2];
+  if (!(det * det > 9e-24 * (f2 * f2 * f2))) return false;
+  const double r = 1.0 / det;
+  double X[3][3], R[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) X[i][j] = C[j][i] * r;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = i == j ? 1.0 : 0.0;
+      for (int k = 0; k < 3; ++k) s = s - A[i][k] * X[k][j];
+      R[i][j] = s;
+    }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = s + X[i][k] * R[k][j];
+      A[i][j] = X[i][j] + s;
+    }
+  return true;
+}
+
+// Pseudo-inverse of a 3x3 matrix (A[r][c] = mat(r+1, c+1)); singular values below
+// 3e-12 * max discarded (the cut of pseudo_inverse_inplace_lapack,
+// linear_solver_module.F90:683-715): the inverse when the cut cannot bite, else a
+// one-sided Jacobi SVD of six sweeps.
+__device__ __noinline__ void pinv3_jacobi(double A[3][3]);
+__device__ inline void pinv3(double A[3][3]) {
+  if (!inv3_if_regular(A)) pinv3_jacobi(A);
+}
+// the rank-deficient case, out of line (rare; keeps the callers' registers low)
+__device__ __noinline__ void pinv3_jacobi(double A[3][3]) {
   double U[3][3], V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   for (int i = 0; i < 3; ++i)
     for (int j = 0; j < 3; ++j) U[i][j] = A[i][j];
@@ -364,165 +410,187 @@ __device__ bool multi_point(const double* wl64, const double* wr64, const double
   return ok;
 }
 
-// compute_lambdas_and_solve_nodal_velocity (ns_euler_rs_module.F90:288-422), FP64
-__device__ void nodal_velocity(const DevMesh& m, const NsParams& P, int v, int p0, int nsfn,
-                               const double (*wlr)[10], double (*lam)[2], double* vbar, double* vnode) {
-  double Bp[3] = {0, 0, 0};  // wall_normal (ns_euler_primitives_module.F90:162-190)
-  for (int j = 0; j < nsfn; ++j) {
-    int sf = m.vsf[p0 + j];
-    int y = m.flr[m.sf_face[sf]].y;
-    if (y < 0) {
-      double4 sn = m.sfn[sf];
-      if (!(P.b2d && fabs(sn.z) > 1e-12))
-        if (y == -1 || P.bc_type[-(y + 1) - 1] == 1) {
-          Bp[0] = Bp[0] + sn.w * sn.x;
-          Bp[1] = Bp[1] + sn.w * sn.y;
-          Bp[2] = Bp[2] + sn.w * sn.z;
-        }
-    }
-  }
-  vnode[0] = vnode[1] = vnode[2] = 0.0;
-  for (int iter = 1; iter <= 4; ++iter) {
-    double mat[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}}, Rp[3] = {0, 0, 0};
-    for (int j = 0; j < nsfn; ++j) {
-      int sf = m.vsf[p0 + j];
-      int y = m.flr[m.sf_face[sf]].y;
-      double4 sn = m.sfn[sf];
-      const double n[3] = {sn.x, sn.y, sn.z};
-      double area = sn.w;
-      const double* wl = wlr[j];
-      const double* wr = wlr[j] + 5;
-      double rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], al = sound_speed_w(wl);
-      double rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr);
-      double lam_l = lam[j][0], lam_r = lam[j][1];
-      const bool wall = is_wall(P, y);
-      if (iter == 1) {
-        lam_l = fmax2(fmax2(fmax2(lam_l, al * rhol), sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
-        lam_r = fmax2(fmax2(fmax2(lam_r, ar * rhor), sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
-        vbar[j] = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
-        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(vbar[j] - vnl) / al)));
-        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (vbar[j] - vnr) / ar)));
-      } else if (wall && P.bc_style == 1) {
-        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(vbar[j] - vnl) / al)));
-        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (vbar[j] - vnr) / ar)));
-      } else {
-        double v_et = dotT(vnode, n);
-        lam_l = fmax2(lam_l, al * rhol * (1.0 + 1.5 * fmax2(0.0, -(v_et - vnl) / al)));
-        lam_r = fmax2(lam_r, ar * rhor * (1.0 + 1.5 * fmax2(0.0, (v_et - vnr) / ar)));
-      }
-      lam[j][0] = lam_l;
-      lam[j][1] = lam_r;
-      vbar[j] = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
-      if (!wall || P.bc_style == 0 || P.bc_style == 2) {
-        double w = (lam_r + lam_l) * area;
-        for (int d = 0; d < 3; ++d)
-          for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + w * (n[d] * n[e]);
-      }
-      if (!wall || P.bc_style == 0) {
-        double q = area * (lam_r + lam_l) * vbar[j];
-        for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
-      } else if (P.bc_style == 2) {
-        if (!P.b2d || fabs(n[2]) < 1e-8) {
-          double q = area * pl;
-          for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
-        }
-      }
-    }
-    if (P.bc_style == 2) {
-      double bmax = fmax2(fmax2(fabs(Bp[0]), fabs(Bp[1])), fabs(Bp[2]));
-      if (bmax > 1e-8) {
-        pinv3(mat);
-        double mr[3], mb[3], r2[3];
-        for (int d = 0; d < 3; ++d) {
-          double s = 0.0, t = 0.0;
-          for (int e = 0; e < 3; ++e) {
-            s = s + mat[d][e] * Rp[e];
-            t = t + mat[d][e] * Bp[e];
-          }
-          mr[d] = s;
-          mb[d] = t;
-        }
-        double p_bound = dotT(mr, Bp) / dotT(mb, Bp);
-        for (int d = 0; d < 3; ++d) r2[d] = Rp[d] - p_bound * Bp[d];
-        for (int d = 0; d < 3; ++d) {
-          double s = 0.0;
-          for (int e = 0; e < 3; ++e) s = s + mat[d][e] * r2[e];
-          vnode[d] = s;
-        }
-        double f = dotT(vnode, Bp) / dotT(Bp, Bp);
-        for (int d = 0; d < 3; ++d) vnode[d] = vnode[d] - f * Bp[d];
-      } else {
-        lu_solve3(mat, vnode, Rp);
-      }
-    } else {
+// The 3x3 solve that ends each iteration of compute_lambdas_and_solve_nodal_velocity
+// (ns_euler_rs_module.F90:404-421): bc_style 2 with a wall at the node imposes the wall
+// pressure through B_p (pseudo-inverse of M); otherwise M v = R by LU (bc_style 2) or
+// the pseudo-inverse (bc_style 0, 1). FP64. mat is overwritten.
+__device__ void nodal_solve(const NsParams& P, double mat[3][3], const double* Rp, const double* Bp, double* vnode) {
+  if (P.bc_style == 2) {
+    double bmax = fmax2(fmax2(fabs(Bp[0]), fabs(Bp[1])), fabs(Bp[2]));
+    if (bmax > 1e-8) {
       pinv3(mat);
+      double mr[3], mb[3], r2[3];
+      for (int d = 0; d < 3; ++d) {
+        double s = 0.0, t = 0.0;
+        for (int e = 0; e < 3; ++e) {
+          s = s + mat[d][e] * Rp[e];
+          t = t + mat[d][e] * Bp[e];
+        }
+        mr[d] = s;
+        mb[d] = t;
+      }
+      double p_bound = dotT(mr, Bp) / dotT(mb, Bp);
+      for (int d = 0; d < 3; ++d) r2[d] = Rp[d] - p_bound * Bp[d];
       for (int d = 0; d < 3; ++d) {
         double s = 0.0;
-        for (int e = 0; e < 3; ++e) s = s + mat[d][e] * Rp[e];
+        for (int e = 0; e < 3; ++e) s = s + mat[d][e] * r2[e];
         vnode[d] = s;
       }
+      double f = dotT(vnode, Bp) / dotT(Bp, Bp);
+      for (int d = 0; d < 3; ++d) vnode[d] = vnode[d] - f * Bp[d];
+    } else {
+      lu_solve3(mat, vnode, Rp);
+    }
+  } else {
+    pinv3(mat);
+    for (int d = 0; d < 3; ++d) {
+      double s = 0.0;
+      for (int e = 0; e < 3; ++e) s = s + mat[d][e] * Rp[e];
+      vnode[d] = s;
     }
   }
 }
 
-// compute_rhs_around_vert (ns_euler_module.F90:341-519) for one vertex; writes the
-// corner sums of the vertex's own subcells to fs (kNsFs doubles per subcell).
-template <class T>
-__device__ void ns_node_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
-                             const double* __restrict__ grad, double* __restrict__ fs, int so, const NsScalars* sc,
-                             const int v) {
-  if (sc && sc->done) return;
+// compute_rhs_around_vert (ns_euler_module.F90:341-519) for one vertex, one thread per
+// vertex; writes the corner sums of the vertex's own subcells to fs (kNsFs doubles per
+// subcell). MS bounds the vertex's subfaces and subcells (8, 16 or 32).
+// Per subface the thread keeps, from the reconstruction on, what the 4-iteration nodal
+// solver reads (left/right density, normal velocity, pressure, sound speed; normal,
+// area, boundary code), so each iteration costs only the wave-speed updates and the 3x3
+// solve; the values are the reference's (the sound speeds of :322-323 are the same
+// expressions of the same states in every iteration).
+constexpr int kNodeThreads = 256;  // the largest block of the node kernel
+
+template <class T, int MS>
+__device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
+                               const double* __restrict__ grad, double* __restrict__ fs, int so, const int v) {
   if (v >= m.nv) return;
   const int p0 = m.vsf_off[v], nsfn = m.vsf_off[v + 1] - p0;
   const int q0 = m.vse_off[v], nsen = m.vse_off[v + 1] - q0;
-  if (nsfn > kNsMaxSf || nsen > kNsMaxSe) {
+  if (nsfn > MS || nsen > MS) {
     atomicOr(m.status, kErrIndex);
     return;
   }
-  double wlr[kNsMaxSf][10];
-  double lam[kNsMaxSf][2];
-  double vbar[kNsMaxSf];
+  // Reconstructed primitive states (left then right) in the compute precision T: the
+  // reconstruction already runs in T, so storing T loses nothing.
+  T wlr[MS][10];
+  double geo[MS][4];  // subface normal and area
+  T lam[MS][3];       // lambda_l, lambda_r, vbar
+  int sfj[MS], yj[MS];
   for (int j = 0; j < nsfn; ++j) {
     const int sf = m.vsf[p0 + j];
     const int2 lr = m.flr[m.sf_face[sf]];
-    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, wlr[j], wlr[j] + 5);
-    lam[j][0] = lam[j][1] = 0.0;
-    vbar[j] = 0.0;
+    sfj[j] = sf;
+    yj[j] = lr.y;
+    double w10[10];
+    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5);
+    for (int k = 0; k < 10; ++k) wlr[j][k] = (T)w10[k];
+    const double4 sn = m.sfn[sf];
+    geo[j][0] = sn.x;
+    geo[j][1] = sn.y;
+    geo[j][2] = sn.z;
+    geo[j][3] = sn.w;
+    lam[j][0] = lam[j][1] = lam[j][2] = (T)0;
   }
   const bool excl = m.is_bound[v] && P.excl;
   double vn3[3] = {0.0, 0.0, 0.0};
   if (P.scheme == 1) {
-    if (!excl) nodal_velocity(m, P, v, p0, nsfn, wlr, lam, vbar, vn3);
+    if (!excl) {  // compute_lambdas_and_solve_nodal_velocity (ns_euler_rs_module.F90:288-422)
+      // wave-speed bounds and vbar in T; M, R and the 3x3 solve in FP64
+      T snd[MS][2];  // left / right sound speeds
+      double Bp[3] = {0.0, 0.0, 0.0};  // wall_normal (ns_euler_primitives_module.F90:162-190)
+      for (int j = 0; j < nsfn; ++j) {
+        const double* n = geo[j];
+        snd[j][0] = sqrt((T)G * wlr[j][4] / wlr[j][0]);
+        snd[j][1] = sqrt((T)G * wlr[j][9] / wlr[j][5]);
+        const int y = yj[j];
+        if (y < 0 && !(P.b2d && fabs(n[2]) > 1e-12) && (y == -1 || P.bc_type[-(y + 1) - 1] == 1))
+          for (int d = 0; d < 3; ++d) Bp[d] = Bp[d] + n[3] * n[d];
+      }
+      for (int iter = 1; iter <= 4; ++iter) {
+        double M6[6] = {0, 0, 0, 0, 0, 0}, Rp[3] = {0, 0, 0};
+        for (int j = 0; j < nsfn; ++j) {
+          const double* n = geo[j];
+          const double area = n[3];
+          const T nt[3] = {(T)n[0], (T)n[1], (T)n[2]};
+          const T* wl = wlr[j];
+          const T* wr = wlr[j] + 5;
+          const T rhol = wl[0], vnl = dotT(wl + 1, nt), pl = wl[4], al = snd[j][0];
+          const T rhor = wr[0], vnr = dotT(wr + 1, nt), pr = wr[4], ar = snd[j][1];
+          T lam_l = lam[j][0], lam_r = lam[j][1], vbar = lam[j][2];
+          const bool wall = is_wall(P, yj[j]);
+          const T c1 = (T)1, c15 = (T)1.5, c0 = (T)0;
+          if (iter == 1) {
+            lam_l = tmax2(tmax2(tmax2(lam_l, al * rhol), sqrt(rhol * tmax2(c0, pr - pl))), -rhol * (vnr - vnl));
+            lam_r = tmax2(tmax2(tmax2(lam_r, ar * rhor), sqrt(rhor * tmax2(c0, pl - pr))), -rhor * (vnr - vnl));
+            vbar = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+            lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -(vbar - vnl) / al)));
+            lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, (vbar - vnr) / ar)));
+          } else if (wall && P.bc_style == 1) {
+            lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -(vbar - vnl) / al)));
+            lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, (vbar - vnr) / ar)));
+          } else {
+            const T v_et = (T)dotT(vn3, n);
+            lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -(v_et - vnl) / al)));
+            lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, (v_et - vnr) / ar)));
+          }
+          vbar = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+          lam[j][0] = lam_l;
+          lam[j][1] = lam_r;
+          lam[j][2] = vbar;
+          const double lsum = (double)lam_r + (double)lam_l;
+          if (!wall || P.bc_style == 0 || P.bc_style == 2) {  // M += (lam_r + lam_l) A n n^T
+            const double w = lsum * area;
+            M6[0] = M6[0] + w * (n[0] * n[0]);
+            M6[1] = M6[1] + w * (n[0] * n[1]);
+            M6[2] = M6[2] + w * (n[0] * n[2]);
+            M6[3] = M6[3] + w * (n[1] * n[1]);
+            M6[4] = M6[4] + w * (n[1] * n[2]);
+            M6[5] = M6[5] + w * (n[2] * n[2]);
+          }
+          if (!wall || P.bc_style == 0) {
+            const double q = area * lsum * (double)vbar;
+            for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
+          } else if (P.bc_style == 2 && (!P.b2d || fabs(n[2]) < 1e-8)) {
+            const double q = area * (double)pl;
+            for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
+          }
+        }
+        // M is symmetric entry by entry: n_d n_e and n_e n_d are the same product
+        double mat[3][3] = {{M6[0], M6[1], M6[2]}, {M6[1], M6[3], M6[4]}, {M6[2], M6[4], M6[5]}};
+        nodal_solve(P, mat, Rp, Bp, vn3);
+      }
+    }
     m.vp[v] = make_double4(vn3[0], vn3[1], vn3[2], 0.0);
   }
-  double fsv[kNsMaxSe][5], slv[kNsMaxSe];
-  for (int j = 0; j < nsen; ++j) {
-    slv[j] = 0.0;
-    for (int k = 0; k < 5; ++k) fsv[j][k] = 0.0;
-  }
+  double fsv[MS][6];  // five flux sums and the wave-speed sum per subcell
+  for (int j = 0; j < nsen; ++j)
+    for (int k = 0; k < 6; ++k) fsv[j][k] = 0.0;
   bool bad = false;
-  int rse_loc = 0;
   for (int j = 0; j < nsfn; ++j) {
-    const int sf = m.vsf[p0 + j];
-    const int y = m.flr[m.sf_face[sf]].y;
+    const int sf = sfj[j];
     const int2 se = m.sf_se[sf];
     const int lse_loc = m.se_loc[se.x];
-    if (se.y >= 0) rse_loc = m.se_loc[se.y];
-    const double4 sn = m.sfn[sf];
-    const double n[3] = {sn.x, sn.y, sn.z};
+    const double* n = geo[j];
+    double w10[10];
+    for (int k = 0; k < 10; ++k) w10[k] = (double)wlr[j][k];
     double lr[2][5], sl, sr;
     if (P.scheme == 1 && !excl) {
-      const double vn = is_wall(P, y) ? 0.0 : dotT(vn3, n);
-      if (!multi_point<T>(wlr[j], wlr[j] + 5, n, lr, vn, lam[j][0], lam[j][1], &sl, &sr)) bad = true;
+      const double vn = is_wall(P, yj[j]) ? 0.0 : dotT(vn3, n);
+      if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam[j][0], (double)lam[j][1], &sl, &sr)) bad = true;
     } else {
-      two_wave<T>(wlr[j], wlr[j] + 5, n, lr, &sl, &sr);
+      two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
     if (m.se_vert[se.x] == v && lse_loc < nsen) {
-      slv[lse_loc] = slv[lse_loc] + sn.w * fmax2(0.0, -sl);
-      for (int k = 0; k < 5; ++k) fsv[lse_loc][k] = fsv[lse_loc][k] + sn.w * lr[0][k];
-      if (se.y >= 0 && m.se_vert[se.y] == v && rse_loc < nsen) {
-        slv[rse_loc] = slv[rse_loc] + sn.w * fmax2(0.0, sr);
-        for (int k = 0; k < 5; ++k) fsv[rse_loc][k] = fsv[rse_loc][k] + sn.w * lr[1][k];
+      const double area = n[3];
+      fsv[lse_loc][5] = fsv[lse_loc][5] + area * fmax2(0.0, -sl);
+      for (int k = 0; k < 5; ++k) fsv[lse_loc][k] = fsv[lse_loc][k] + area * lr[0][k];
+      if (se.y >= 0 && m.se_vert[se.y] == v) {
+        const int rse_loc = m.se_loc[se.y];
+        if (rse_loc < nsen) {
+          fsv[rse_loc][5] = fsv[rse_loc][5] + area * fmax2(0.0, sr);
+          for (int k = 0; k < 5; ++k) fsv[rse_loc][k] = fsv[rse_loc][k] + area * lr[1][k];
+        }
       }
     }
   }
@@ -531,16 +599,16 @@ __device__ void ns_node_body(const DevMesh& m, const NsParams& P, const double* 
     const int s = m.vse[q0 + j];
     if (m.se_vert[s] != v) continue;  // a periodic image's subcell: its sums are zero here
     double* out = fs + kNsFs * (size_t)s;
-    for (int k = 0; k < 5; ++k) out[k] = fsv[j][k];
-    out[5] = slv[j];
+    for (int k = 0; k < 6; ++k) out[k] = fsv[j][k];
   }
 }
 
-template <class T>
-__global__ void __launch_bounds__(128) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
-                                                 const double* __restrict__ grad, double* __restrict__ fs, int so,
-                                                 const NsScalars* sc) {
-  ns_node_body<T>(m, P, U, grad, fs, so, sc, blockIdx.x * blockDim.x + threadIdx.x);
+template <class T, int MS>
+__global__ void __launch_bounds__(kNodeThreads) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
+                                                          const double* __restrict__ grad, double* __restrict__ fs,
+                                                          int so, const NsScalars* sc) {
+  if (sc && sc->done) return;
+  ns_node_vertex<T, MS>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __device__ inline double warp_min(double x) {
@@ -913,14 +981,16 @@ __device__ inline int item_of(const int* __restrict__ wofs, int n, int w) {
 }
 
 // which: the state the phase reads (0: U0, 1: U1)
-template <class T>
-__global__ void __launch_bounds__(256) kb_ns_node(const NsItem* __restrict__ it, const int* __restrict__ wv,
-                                                  const int* __restrict__ hdr, NsParams P, int which, int so) {
+template <class T, int MS>
+__global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restrict__ it, const int* __restrict__ wv,
+                                                           const int* __restrict__ hdr, NsParams P, int which,
+                                                           int so) {
   const int n = hdr[0];
   for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
     const int p = item_of(wv, n, w);
     const NsItem& I = it[p];
-    ns_node_body<T>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, I.sc, (w - wv[p]) * blockDim.x + threadIdx.x);
+    if (I.sc->done) continue;
+    ns_node_vertex<T, MS>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * blockDim.x + threadIdx.x);
   }
 }
 __global__ void __launch_bounds__(128) kb_ns_gather(const NsItem* __restrict__ it, const int* __restrict__ wc,
@@ -1150,17 +1220,25 @@ __global__ void k_ns_pack(int n, const double* __restrict__ s5, double* __restri
 
 int ns_partial_blocks(const DevMesh& m) { return grid_for(m.ne, kTdBlock); }
 
+template <class T>
+void launch_kb_node(const NsTable& t, const NsParams& P, cudaStream_t s, int which, int so) {
+  const int gv = t.grid_v, bv = t.block_v;
+  if (t.group == 8) kb_ns_node<T, 8><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  else if (t.group == 16) kb_ns_node<T, 16><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  else kb_ns_node<T, 32><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+}
+
 void launch_ns_batch_step(const NsTable& t, const NsParams& P, cudaStream_t s) {
-  const int gv = t.grid_v, gc = t.grid_c, bv = t.block_v, gp = grid_for(t.cap, 128);
+  const int gv = t.grid_v, gc = t.grid_c, nb = t.block_v, gp = grid_for(t.cap, 128);
   auto node = [&](int which, int so) {
-    if (P.precision == 1) kb_ns_node<float><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
-    else kb_ns_node<double><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+    if (P.precision == 1) launch_kb_node<float>(t, P, s, which, so);
+    else launch_kb_node<double>(t, P, s, which, so);
   };
   auto rhs = [&](int which) {
     node(which, 0);
     kb_ns_gather<<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, 0);
     if (P.second_order) {
-      kb_ns_nodal_grad<<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, which);
+      kb_ns_nodal_grad<<<gv, nb, 0, s>>>(t.items, t.wv, t.hdr, which);
       if (P.precision == 1) kb_ns_cell_grad<float><<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, P, which);
       else kb_ns_cell_grad<double><<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, P, which);
       node(which, 1);
@@ -1204,13 +1282,26 @@ void launch_ns_pack(const DevMesh& m, const double* s5, double* U) {
   k_ns_pack<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m.ne, s5, U);
 }
 
+int ns_node_lanes(const DevMesh& m) {
+  const int k = std::max(m.max_vsf, m.max_vse);
+  return k <= 8 ? 8 : k <= 16 ? 16 : k <= 32 ? 32 : 0;
+}
+
+template <class T>
+void launch_node(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs, int so,
+                 const NsScalars* sc) {
+  const int ms = std::max(8, ns_node_lanes(m));  // a mesh beyond 32 is flagged by the kernel
+  const int grid = grid_for(m.nv, 128);
+  if (ms == 8) k_ns_node<T, 8><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  else if (ms == 16) k_ns_node<T, 16><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  else k_ns_node<T, 32><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+}
+
 void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double* fs, double* rhs1, double* rhs2,
                    double* ngrad, double* grad, NsScalars* sc) {
   const int gv = grid_for(m.nv, 128), gc = grid_for(m.ne, 128);
-  if (P.precision == 1)
-    k_ns_node<float><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 0, sc);
-  else
-    k_ns_node<double><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 0, sc);
+  if (P.precision == 1) launch_node<float>(m, P, U, grad, fs, 0, sc);
+  else launch_node<double>(m, P, U, grad, fs, 0, sc);
   k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs1, sc, sc ? 1 : 0);
   if (P.second_order) {
     k_ns_nodal_grad<<<gv, 128, 0, m.stream>>>(m, U, ngrad, sc);
@@ -1218,10 +1309,8 @@ void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double*
       k_ns_cell_grad<float><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
     else
       k_ns_cell_grad<double><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
-    if (P.precision == 1)
-      k_ns_node<float><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 1, sc);
-    else
-      k_ns_node<double><<<gv, 128, 0, m.stream>>>(m, P, U, grad, fs, 1, sc);
+    if (P.precision == 1) launch_node<float>(m, P, U, grad, fs, 1, sc);
+    else launch_node<double>(m, P, U, grad, fs, 1, sc);
     k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs2, sc, 0);
   }
 }

@@ -7,7 +7,6 @@
 namespace subfv {
 
 constexpr int kNsMaxSf = 32;  // subfaces around a vertex (a 3-D hex vertex has 12)
-constexpr int kNsMaxSe = 16;  // subcells around a vertex (a 3-D hex vertex has 8)
 constexpr int kNsFs = 6;      // per-subcell record: five corner flux sums and the wave-speed sum
 
 struct NsParams {
@@ -38,17 +37,22 @@ struct NsItem {
   NsScalars* sc;
 };
 
+// Per-vertex array bound of the node kernel for a mesh: the smallest of 8, 16, 32 that
+// holds every vertex's subfaces and subcells (0: a vertex has more than 32).
+int ns_node_lanes(const DevMesh& m);
 // Table of in-flight problems on the device: items, work-block prefixes over their
 // vertices (wv, block_v vertices per work block) and cells (wc, 128 cells per work
 // block), and hdr[0] = the number of problems. Up to cap problems; the grids are
-// persistent (grid_v, grid_c blocks whatever the table holds).
+// persistent (grid_v, grid_c blocks whatever the table holds). block_v: threads (one
+// per vertex) per block of the vertex kernels (64, 128 or 256); group: the node
+// kernel's per-vertex array bound (8, 16, 32), the largest the table needs.
 struct NsTable {
   NsItem* items = nullptr;
   int* wv = nullptr;
   int* wc = nullptr;
   int* hdr = nullptr;
   int cap = 0;
-  int block_v = 128, grid_v = 1, grid_c = 1;
+  int block_v = 128, group = 8, grid_v = 1, grid_c = 1;
 };
 constexpr int kNsCellBlock = 128;
 // One step of the time loop for every problem of the table, in shared launches.

@@ -128,6 +128,17 @@ int table_upload(subfv_ns_batch* b) {
   int* wc = wv + (b->cap + 1);
   int* hdr = wc + (b->cap + 1);
   const int n = (int)b->order.size();
+  int group = 8;
+  for (int i = 0; i < n; ++i) group = std::max(group, ns_node_lanes(b->slots[b->order[i]].mesh->d));
+  if (group != b->tab.group) {  // the captured step loop launches the node kernel for one group size
+    if (b->graph) {
+      SUBFV_CUDA(cudaStreamSynchronize(b->stream));
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+    b->tab.group = group;
+  }
+  const int nbv = b->tab.block_v;  // vertices per work block
   wv[0] = wc[0] = 0;
   for (int i = 0; i < n; ++i) {
     Slot& q = b->slots[b->order[i]];
@@ -144,7 +155,7 @@ int table_upload(subfv_ns_batch* b) {
     I.delta = q.delta;
     I.partial = q.partial;
     I.sc = b->sc + b->order[i];
-    wv[i + 1] = wv[i] + (I.m.nv + b->tab.block_v - 1) / b->tab.block_v;
+    wv[i + 1] = wv[i] + (I.m.nv + nbv - 1) / nbv;
     wc[i + 1] = wc[i] + (I.m.ne + kNsCellBlock - 1) / kNsCellBlock;
   }
   hdr[0] = n;
@@ -232,6 +243,7 @@ int subfv_ns_batch_create(const subfv_ns_cfg* cfg, int capacity, int64_t budget_
   b->tab.hdr = b->tab.wc + (capacity + 1);
   b->tab.cap = capacity;
   b->tab.block_v = 128;
+  b->tab.group = 8;
   b->tab.grid_v = b->tab.grid_c = 148 * 8;
   for (int k = 0; k < 2; ++k) {
     if (cudaHostAlloc((void**)&b->h_items[k], capacity * sizeof(NsItem), cudaHostAllocDefault) != cudaSuccess ||
@@ -293,6 +305,10 @@ int subfv_ns_batch_add(subfv_ns_batch* b, subfv_mesh* m, int take_mesh, const do
     return -2;
   }
   const DevMesh& d = m->d;
+  if (ns_node_lanes(d) == 0) {
+    set_error("subfv_ns_batch_add: a vertex has more than 32 subfaces or subcells");
+    return -2;
+  }
   const int64_t need = state_bytes(d, b->P.second_order) + (int64_t)d.bytes;
   int k = -1;
   for (int i = 0; i < b->cap && k < 0; ++i) {
