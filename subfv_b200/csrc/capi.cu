@@ -46,12 +46,14 @@ namespace {
 int check_status(DevMesh& d);
 int clear_status(DevMesh& d);
 int ensure_scratch(subfv_mesh* m);
+int ensure_full_geometry(DevMesh& d);
 }  // namespace
 
 namespace subfv {
 int handle_check_status(DevMesh& d) { return check_status(d); }
 int handle_clear_status(DevMesh& d) { return clear_status(d); }
 int handle_ensure_scratch(subfv_mesh* m) { return ensure_scratch(m); }
+int handle_ensure_full_geometry(DevMesh& d) { return ensure_full_geometry(d); }
 }  // namespace subfv
 
 namespace {
@@ -74,6 +76,22 @@ int ensure_scratch(subfv_mesh* m) {
   SUBFV_CUDA(cudaMalloc(&m->rhs6, 6 * (size_t)m->d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->mass, (size_t)m->d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->sc, sizeof(LagScalars)));
+  SUBFV_CUDA(cudaMalloc(&m->d.frec, 6 * (size_t)m->d.nf * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&m->d.centry, std::max<size_t>(m->d.ncsf, 1) * sizeof(int4)));
+  launch_build_cell_entries(m->d);
+  return 0;
+}
+// After Lagrangian steps (which refresh only what the next step reads), recompute every
+// geometric array from the current coordinates; check_mesh's verdict on this geometry
+// was already reported by the step that produced it.
+int ensure_full_geometry(DevMesh& d) {
+  if (!d.geom_partial) return 0;
+  launch_geometry(d, 1);
+  launch_vert_is_bound(d);
+  launch_vert_volume(d);
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  SUBFV_CUDA(cudaGetLastError());
+  d.geom_partial = 0;
   return 0;
 }
 int load_sol(subfv_mesh* m, const double* sol, const double* mass) {
@@ -194,7 +212,7 @@ int subfv_mesh_destroy(subfv_mesh* m) {
   if (!m) return 0;
   // scratch of the stateless calls (allocated on first use only); a mesh that never
   // needed it is released without any device-wide synchronisation
-  void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc};
+  void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc, m->d.frec, m->d.centry};
   for (void* p : scratch)
     if (p) cudaFree(p);
   devmesh_free(&m->d);
@@ -227,6 +245,7 @@ int subfv_mesh_get_coords(subfv_mesh* m, double* c) {
 
 int subfv_mesh_get_geometry(subfv_mesh* m, const char* name, double* out) {
   DevMesh& d = m->d;
+  if (ensure_full_geometry(d)) return -1;
   std::string n(name);
   auto get4 = [&](const double4* src, int cnt, int ncomp, int first) -> int {
     std::vector<double4> h(cnt);
@@ -266,11 +285,11 @@ int subfv_mesh_get_geometry(subfv_mesh* m, const char* name, double* out) {
 int subfv_compute_geometry_mesh(subfv_mesh* m) {
   DevMesh& d = m->d;
   if (clear_status(d)) return -1;
-  launch_face_geometry(d);
-  launch_cell_geometry(d);
+  launch_geometry(d, 1);
   launch_vert_is_bound(d);
   launch_vert_volume(d);
   SUBFV_CUDA(cudaGetLastError());
+  d.geom_partial = 0;
   return check_status(d);
 }
 
@@ -281,7 +300,7 @@ int subfv_compute_rhs_lagrange(subfv_mesh* m, const double* sol, double* vp, dou
   if (ensure_scratch(m) || clear_status(d)) return -1;
   d.b2d = b2d;
   if (load_sol(m, sol, mass)) return -1;
-  launch_lag_node(d, m->sol6, nullptr, 0, 0);
+  launch_lag_node(d, m->sol6, nullptr, 0);
   launch_lag_cell(d, m->sol6, m->rhs6, nullptr, nullptr, 0, 1);
   launch_unpack6(d, d.ne, kRhs, m->rhs6, m->stage);
   SUBFV_CUDA(cudaMemcpyAsync(rhs, m->stage, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
@@ -397,6 +416,7 @@ int lag_graph(subfv_lag_state* s, int steps) {
 
 int subfv_lag_advance_async(subfv_lag_state* s, int n_steps) {
   DevMesh& d = s->m->d;
+  if (n_steps > 0) d.geom_partial = 1;
   const int chunk = 16;
   if (n_steps >= chunk) {
     if (lag_graph(s, chunk)) return -1;
@@ -466,6 +486,7 @@ int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout) {
   SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, s->host_stage, bytes, cudaMemcpyHostToDevice, d.stream));
   launch_pack6(d, d.ne, s->dev_stage, nullptr, s->sol6);
   enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
+  d.geom_partial = 1;
   launch_unpack6(d, d.ne, kRec, s->sol6, s->dev_stage);
   SUBFV_CUDA(cudaMemcpyAsync(s->host_stage, s->dev_stage, bytes, cudaMemcpyDeviceToHost, d.stream));
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
@@ -487,17 +508,17 @@ int subfv_lag_profile_steps(subfv_lag_state* s, int n_steps, double* kernel_ms) 
   for (int k = 0; k < K; ++k) kernel_ms[k] = 0.0;
   for (int i = 0; i < n_steps; ++i) {
     SUBFV_CUDA(cudaEventRecord(ev[0], d.stream));
-    launch_lag_node(d, s->sol6, s->sc, s->precision, 1);
+    launch_lag_face_only(d, s->sol6, s->sc, s->precision);
     SUBFV_CUDA(cudaEventRecord(ev[1], d.stream));
-    launch_lag_cell(d, s->sol6, s->rhs6, s->sc, &s->sc->dtmin, s->precision, 3);
+    launch_lag_node_only(d, s->sc, s->precision);
     SUBFV_CUDA(cudaEventRecord(ev[2], d.stream));
-    launch_lag_finalize(d, s->sc);
+    launch_lag_cell(d, s->sol6, s->rhs6, s->sc, &s->sc->dtmin, s->precision, 3);
     SUBFV_CUDA(cudaEventRecord(ev[3], d.stream));
-    launch_lag_move(d, s->sc, 0.0);
+    launch_lag_finalize(d, s->sc);
     SUBFV_CUDA(cudaEventRecord(ev[4], d.stream));
-    launch_face_geometry(d, s->sc);
+    launch_lag_move(d, s->sc, 0.0);
     SUBFV_CUDA(cudaEventRecord(ev[5], d.stream));
-    launch_cell_geometry(d, s->sol6, s->rhs6, s->sc);
+    launch_geometry(d, 0, s->sol6, s->rhs6, s->sc);
     SUBFV_CUDA(cudaEventRecord(ev[6], d.stream));
     SUBFV_CUDA(cudaEventSynchronize(ev[6]));
     for (int k = 0; k < K; ++k) {

@@ -25,6 +25,9 @@ enum StatusBits : unsigned {
 
 // gfortran's inline NORM2 of a 3-vector: scaled sum of squares, scale starting at 1.
 __host__ __device__ inline double fnorm2_3(double a0, double a1, double a2) {
+  // With every |a_i| <= 1 the scale stays 1, each a_i / scale is a_i exactly and a zero
+  // term adds nothing, so the scaled sum below reduces to this one, bit for bit.
+  if (fabs(a0) <= 1.0 && fabs(a1) <= 1.0 && fabs(a2) <= 1.0) return sqrt(a0 * a0 + a1 * a1 + a2 * a2);
   double scale = 1.0, res = 0.0;
   const double a[3] = {a0, a1, a2};
 #pragma unroll

@@ -18,4 +18,6 @@ namespace subfv {
 int handle_check_status(DevMesh& d);
 int handle_clear_status(DevMesh& d);
 int handle_ensure_scratch(subfv_mesh* m);
+// full geometry when Lagrangian steps left only the step's subset current
+int handle_ensure_full_geometry(DevMesh& d);
 }  // namespace subfv

@@ -2,19 +2,23 @@
 // 240-283, 772-784; time loop src/lagrange/lagrange_main.F90:89-127) on the GPU.
 //
 // Per step, all in HBM, no host round trip:
+//   k_lag_face     one thread per face: the wave speeds of the face's two sides
+//                  (:68-73 and the boundary branches) and the normal velocities, once
+//                  per face; the node and cell kernels read them from the face record
 //   k_lag_node     one thread per vertex: nodal 3x3 system (Mp, Rp, Bp) over the
-//                  vertex's subfaces, inverse_3_by_3, vp; also the vertex dual volume
+//                  vertex's subfaces, inverse_3_by_3, vp
 //   k_lag_cell     one thread per cell: deterministic gather of the subface fluxes in
 //                  the reference's scatter order (no float atomics) -> rhs, and the
 //                  cell's CFL terms -> block min -> one atomicMin on the bit pattern
 //   k_lag_finalize one thread: dt = cfl*min, clip to t_max, t += dt
 //   k_lag_move     x += dt*vp
-//   geometry       k_face_geometry, k_cell_geometry (fused with sol += dt*rhs)
+//   k_geom<0>      geometry of the moved mesh, one thread per cell (mesh_dev.cu), fused
+//                  with sol += dt*rhs
 //
 // precision 0 (plain FP64) evaluates every expression in the reference's order and is
 // compiled without FMA contraction: bit-identical to the CPU restatement.
-// precision 1 (mixed) evaluates the per-subface wave speeds and fluxes in FP32 and
-// keeps the nodal 3x3 solve, positions, volumes and the residual sums in FP64.
+// precision 1 (mixed) evaluates the per-face wave speeds and the subface fluxes in
+// FP32 and keeps the nodal 3x3 solve, positions, volumes and the residual sums in FP64.
 #include <vector>
 
 #include "../../include/subfv.h"
@@ -69,8 +73,48 @@ __device__ inline double lam_wall(double p_me, double tau_me) {
   return (double)(sqrt((T)kGamma * (T)p_me * tm) / tm);
 }
 
+// Face record (6 doubles): l1, l2 (the left / right wave speeds lambda of :68-73; l2 = 0
+// on a boundary), vl, vr (the left / right normal velocities), xb, kind. kind 0
+// interior (xb = v_bar of :75), 1 a z-face of a one-layer slab (b2d), 2 a wall
+// (xb = p_l + l1 v_l).
+constexpr int kFrec = 6;
+
 template <int P>
-__global__ void __launch_bounds__(128, 8) k_lag_node(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc, int with_vol) {
+__global__ void __launch_bounds__(128) k_lag_face(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc) {
+  if (sc && sc->done) return;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= m.nf) return;
+  const int2 lr = m.flr[f];
+  const double4 fn = m.fn[f];
+  const double n0 = fn.x, n1 = fn.y, n2 = fn.z;
+  const U5 ul = ld_u(sol6, lr.x);
+  const double pl = ul.p;
+  const double vl = dot3(ul.u, ul.v, ul.w, n0, n1, n2);
+  double l1, l2 = 0.0, vr = 0.0, xb = 0.0, kind;
+  if (lr.y >= 0) {
+    const U5 ur = ld_u(sol6, lr.y);
+    const double pr = ur.p;
+    vr = dot3(ur.u, ur.v, ur.w, n0, n1, n2);
+    l1 = lam_side<P>(pl, pr, ul.t, vr - vl);
+    l2 = lam_side<P>(pr, pl, ur.t, vr - vl);
+    xb = (l1 * vl + l2 * vr - (pr - pl)) / (l2 + l1);
+    kind = 0.0;
+  } else if (m.b2d && fabs(n2) > 1e-8) {
+    l1 = lam_wall<P>(pl, ul.t);
+    kind = 1.0;
+  } else {
+    l1 = lam_wall<P>(pl, ul.t);
+    xb = pl + l1 * vl;
+    kind = 2.0;
+  }
+  double2* r = reinterpret_cast<double2*>(m.frec + kFrec * (size_t)f);
+  r[0] = make_double2(l1, l2);
+  r[1] = make_double2(vl, vr);
+  r[2] = make_double2(xb, kind);
+}
+
+template <int P>
+__global__ void __launch_bounds__(128) k_lag_node(DevMesh m, const LagScalars* sc) {
   if (sc && sc->done) return;
   int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= m.nv) return;
@@ -78,37 +122,28 @@ __global__ void __launch_bounds__(128, 8) k_lag_node(DevMesh m, const double* __
   double R0 = 0, R1 = 0, R2 = 0, B0 = 0, B1 = 0, B2 = 0;
   const int p0 = m.vsf_off[v], p1 = m.vsf_off[v + 1];
   for (int p = p0; p < p1; ++p) {
-    int sf = m.vsf_identity ? p : m.vsf[p];
-    int f = m.sf_face[sf];
-    int2 lr = m.flr[f];
-    double4 fn = m.fn[f];
-    double n0 = fn.x, n1 = fn.y, n2 = fn.z;
-    double area = m.sfn[sf].w;
-    U5 ul = ld_u(sol6, lr.x);
-    double pl = ul.p;
-    double vl = dot3(ul.u, ul.v, ul.w, n0, n1, n2);
+    const int sf = m.vsf_identity ? p : m.vsf[p];
+    const int f = m.sf_face[sf];
+    const double4 fn = m.fn[f];
+    const double n0 = fn.x, n1 = fn.y, n2 = fn.z;
+    const double area = m.sfa[sf];
+    const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)f);
+    const double2 ll = fr[0], xk = fr[2];
     double w;
-    if (lr.y >= 0) {
-      U5 ur = ld_u(sol6, lr.y);
-      double pr = ur.p;
-      double vr = dot3(ur.u, ur.v, ur.w, n0, n1, n2);
-      double l1 = lam_side<P>(pl, pr, ul.t, vr - vl);
-      double l2 = lam_side<P>(pr, pl, ur.t, vr - vl);
-      double v_bar = (l1 * vl + l2 * vr - (pr - pl)) / (l2 + l1);
-      w = area * (l1 + l2);
+    if (xk.y == 0.0) {  // interior face
+      const double v_bar = xk.x;
+      w = area * (ll.x + ll.y);
       R0 = R0 + w * n0 * v_bar;
       R1 = R1 + w * n1 * v_bar;
       R2 = R2 + w * n2 * v_bar;
-    } else if (m.b2d && fabs(n2) > 1e-8) {
-      double l1 = lam_wall<P>(pl, ul.t);
-      w = area * 2 * l1;
+    } else if (xk.y == 1.0) {
+      w = area * 2 * ll.x;
     } else {
-      double l1 = lam_wall<P>(pl, ul.t);
       B0 = B0 + area * n0;
       B1 = B1 + area * n1;
       B2 = B2 + area * n2;
-      w = area * l1;
-      double q = area * (pl + l1 * vl);
+      w = area * ll.x;
+      const double q = area * xk.x;
       R0 = R0 + q * n0;
       R1 = R1 + q * n1;
       R2 = R2 + q * n2;
@@ -147,11 +182,6 @@ __global__ void __launch_bounds__(128, 8) k_lag_node(DevMesh m, const double* __
   double v1 = 0.0 + I10 * b0 + I11 * b1 + I12 * b2;
   double v2 = 0.0 + I20 * b0 + I21 * b1 + I22 * b2;
   m.vp[v] = make_double4(v0, v1, v2, 0.0);
-  if (with_vol) {  // compute_vert_volume of the current geometry (mesh_geometry_module.F90:273-288)
-    double s = 0.0;
-    for (int q = m.vse_off[v]; q < m.vse_off[v + 1]; ++q) s = s + m.vol_se[m.vse[q]];
-    m.vol_v[v] = s;
-  }
 }
 
 __device__ inline double warp_min(double x) {
@@ -175,30 +205,18 @@ __global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __res
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
     bool bad = false;
     for (int q = m.csf_off[c]; q < m.csf_off[c + 1]; ++q) {
-      int e = m.csf[q];
-      int p = e >> 1, side = e & 1;
-      int sf = m.vsf_identity ? p : m.vsf[p];
-      int f = m.sf_face[sf];
-      int2 lr = m.flr[f];
+      const int4 E = m.centry[q];
+      const int sf = E.x, f = E.y, side = (E.z >> 30) & 1, node = E.z & 0x3fffffff;
       double4 fn = m.fn[f];
-      double area = m.sfn[sf].w;
-      int sv = m.sf_vert[sf];
-      int node = m.vsf_identity ? sv : m.p_node[p];
+      double area = m.sfa[sf];
       if (mode & 1) {
         double4 vpn = m.vp[node];
         double v_et = dot3(vpn.x, vpn.y, vpn.z, fn.x, fn.y, fn.z);
-        double vme = dot3(me.u, me.v, me.w, fn.x, fn.y, fn.z);
         double am = area / mass;
-        if (side == 0) {  // this cell is the face's left neighbour
-          double lam;
-          if (lr.y >= 0) {
-            U5 ot = ld_u(sol6, lr.y);
-            double pot = ot.p;
-            double vot = dot3(ot.u, ot.v, ot.w, fn.x, fn.y, fn.z);
-            lam = lam_side<P>(pme, pot, me.t, vot - vme);
-          } else {
-            lam = lam_wall<P>(pme, me.t);
-          }
+        const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)f);
+        const double2 ll = fr[0], vv = fr[1];
+        if (side == 0) {  // this cell is the face's left neighbour: lambda of its side, v.n
+          double lam = ll.x, vme = vv.x;
           if (P == 0) {
             double ps = pme - lam * (v_et - vme);
             r0 = r0 - am * (-v_et);
@@ -215,10 +233,7 @@ __global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __res
             r4 = r4 - am * (double)(ps * (T)v_et);
           }
         } else {  // right neighbour
-          U5 ot = ld_u(sol6, lr.x);
-          double pot = ot.p;
-          double vot = dot3(ot.u, ot.v, ot.w, fn.x, fn.y, fn.z);
-          double lam = lam_side<P>(pme, pot, me.t, vme - vot);
+          double lam = ll.y, vme = vv.y;
           if (P == 0) {
             double ps = pme + lam * (v_et - vme);
             r0 = r0 + am * (-v_et);
@@ -238,9 +253,8 @@ __global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __res
       }
       if (mode & 2) {  // compute_dt terms for (cell, subface)
         double sg = side == 0 ? 1.0 : -1.0;
-        double4 vps = m.vp[sv];
-        int2 se = m.sf_se[sf];
-        int sub = side == 0 ? se.x : se.y;
+        double4 vps = m.vp[m.vsf_identity ? node : m.sf_vert[sf]];  // the subface's own vertex
+        int sub = E.w;
         double t1 = m.vol_se[c] / (area * csnd);  // sub_elem(i) with i the cell (reference quirk)
         double vn = dot3(vps.x, vps.y, vps.z, sg * fn.x, sg * fn.y, sg * fn.z);
         double t2 = sub >= 0 ? 0.8 * m.vol_se[sub] / (1e-8 + fabs(vn) * fn.w) : 1e6;
@@ -328,15 +342,40 @@ __global__ void k_vp_in(int n, const double* __restrict__ in, double4* __restric
 }
 __global__ void k_set_scalar(double* p, double v) { *p = v; }
 
+// Per cell-CSR entry (csf = 2p + side): the subface, its face, the node that owns
+// position p (bit 30: side) and the cell's subcell on the subface; one 16-byte record
+// instead of four dependent lookups in k_lag_cell.
+__global__ void k_build_cell_entries(DevMesh m) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= m.ncsf) return;
+  const int e = m.csf[q];
+  const int p = e >> 1, side = e & 1;
+  const int sf = m.vsf_identity ? p : m.vsf[p];
+  const int node = m.vsf_identity ? m.sf_vert[sf] : m.p_node[p];
+  const int2 se = m.sf_se[sf];
+  m.centry[q] = make_int4(sf, m.sf_face[sf], node | (side << 30), side == 0 ? se.x : se.y);
+}
+
 }  // namespace
 
 constexpr int kBlkNode = 128, kBlkCell = 128, kBlkVert = 256;
 
-void launch_lag_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision, int with_vol) {
-  if (precision == 1)
-    k_lag_node<1><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc, with_vol);
-  else
-    k_lag_node<0><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc, with_vol);
+void launch_lag_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision) {
+  if (precision == 1) {
+    k_lag_face<1><<<grid_for(m.nf, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc);
+    k_lag_node<1><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sc);
+  } else {
+    k_lag_face<0><<<grid_for(m.nf, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc);
+    k_lag_node<0><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sc);
+  }
+}
+void launch_lag_face_only(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision) {
+  if (precision == 1) k_lag_face<1><<<grid_for(m.nf, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc);
+  else k_lag_face<0><<<grid_for(m.nf, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc);
+}
+void launch_lag_node_only(const DevMesh& m, const LagScalars* sc, int precision) {
+  if (precision == 1) k_lag_node<1><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sc);
+  else k_lag_node<0><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sc);
 }
 void launch_lag_cell(const DevMesh& m, const double* sol6, double* rhs6, LagScalars* sc, double* dt_slot,
                      int precision, int mode) {
@@ -358,15 +397,17 @@ void launch_unpack6(const DevMesh& m, int n, int stride, const double* s6, doubl
 void launch_vp_out(const DevMesh& m, double* out) { k_vp_out<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m.nv, m.vp, out); }
 void launch_vp_in(const DevMesh& m, const double* in) { k_vp_in<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m.nv, in, m.vp); }
 void launch_set_scalar(const DevMesh& m, double* p, double v) { k_set_scalar<<<1, 1, 0, m.stream>>>(p, v); }
+void launch_build_cell_entries(const DevMesh& m) {
+  k_build_cell_entries<<<grid_for(m.ncsf, 256), 256, 0, m.stream>>>(m);
+}
 
 // One full time step of lagrange_main.F90:89-127 (graph-capturable: no host sync).
 void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision) {
-  launch_lag_node(m, sol6, sc, precision, 1);
+  launch_lag_node(m, sol6, sc, precision);
   launch_lag_cell(m, sol6, rhs6, sc, &sc->dtmin, precision, 3);
   launch_lag_finalize(m, sc);
   launch_lag_move(m, sc, 0.0);
-  launch_face_geometry(m, sc);
-  launch_cell_geometry(m, sol6, rhs6, sc);
+  launch_geometry(m, 0, sol6, rhs6, sc);
 }
 
 }  // namespace subfv

@@ -5,7 +5,11 @@
 
 namespace subfv {
 
-void launch_lag_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision, int with_vol);
+// the face records (k_lag_face) then the nodal solve (k_lag_node); the mesh's frec must
+// be allocated (devmesh_ensure_lag)
+void launch_lag_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision);
+void launch_lag_face_only(const DevMesh& m, const double* sol6, const LagScalars* sc, int precision);
+void launch_lag_node_only(const DevMesh& m, const LagScalars* sc, int precision);
 // mode bit 1: rhs into rhs6; bit 2: CFL terms min-reduced into *dt_slot
 void launch_lag_cell(const DevMesh& m, const double* sol6, double* rhs6, LagScalars* sc, double* dt_slot,
                      int precision, int mode);
@@ -17,6 +21,8 @@ void launch_unpack6(const DevMesh& m, int n, int stride, const double* s6, doubl
 void launch_vp_out(const DevMesh& m, double* out);
 void launch_vp_in(const DevMesh& m, const double* in);
 void launch_set_scalar(const DevMesh& m, double* p, double v);
+// fills m.centry (allocated by the caller, ncsf records) from the cell CSR
+void launch_build_cell_entries(const DevMesh& m);
 void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision);
 
 }  // namespace subfv

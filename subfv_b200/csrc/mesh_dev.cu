@@ -173,7 +173,7 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
       upload(&m->fvert, fvert, B, s) || upload(&m->flr, flr, B, s) || upload(&m->fsf, fsf, B, s) ||
       alloc(&m->fc, nf, B, s) || alloc(&m->fn, nf, B, s) || upload(&m->sf_face, sf_face, B, s) ||
       upload(&m->sf_vert, sf_vert, B, s) || upload(&m->sf_se, sf_se, B, s) || upload(&m->sf_loc, sf_loc, B, s) ||
-      alloc(&m->sfn, nsf, B, s) || upload(&m->se_elem, se_elem, B, s) || upload(&m->se_vert, se_vert, B, s) ||
+      alloc(&m->sfn, nsf, B, s) || alloc(&m->sfa, nsf, B, s) || upload(&m->se_elem, se_elem, B, s) || upload(&m->se_vert, se_vert, B, s) ||
       upload(&m->se_loc, se_loc, B, s) || upload(&m->se_sf, se_sf, B, s) || alloc(&m->vol_se, nse, B, s) ||
       upload(&m->ev_off, ev_off, B, s) || upload(&m->ev, ev, B, s) || upload(&m->ef8, ef8, B, s) ||
       upload(&m->ekind, ekind, B, s) || alloc(&m->cc, ne, B, s) || alloc(&m->vol, ne, B, s) ||
@@ -187,7 +187,7 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
 
 void devmesh_free(DevMesh* m) {
   void* ptrs[] = {m->x, m->vp, m->vol_v, m->is_bound, m->fvert, m->flr, m->fsf, m->fc, m->fn,
-                  m->sf_face, m->sf_vert, m->sf_se, m->sf_loc, m->sfn, m->se_elem, m->se_vert, m->se_loc,
+                  m->sf_face, m->sf_vert, m->sf_se, m->sf_loc, m->sfn, m->sfa, m->se_elem, m->se_vert, m->se_loc,
                   m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
                   m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
                   m->vel_off, m->vel, m->cse_sorted};
@@ -220,6 +220,8 @@ __device__ inline V3 cross(V3 a, V3 b) {
 }
 __device__ inline double dot(V3 a, V3 b) { return dot3(a.x, a.y, a.z, b.x, b.y, b.z); }
 __device__ inline V3 half_sum(V3 a, V3 b) { return {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)}; }
+
+// ---- full geometry: one thread per face, then one per cell (every array written)
 
 // compute_face_centroid + compute_subface_norm + compute_face_norm (:177-271)
 __global__ void k_face_geometry(DevMesh m, const LagScalars* sc) {
@@ -263,6 +265,7 @@ __global__ void k_face_geometry(DevMesh m, const LagScalars* sc) {
     V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
     double area = fnorm2_3(nr.x, nr.y, nr.z);
     m.sfn[sf] = make_double4(nr.x / area, nr.y / area, nr.z / area, area);
+    m.sfa[sf] = area;
     fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
   }
   double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
@@ -270,9 +273,8 @@ __global__ void k_face_geometry(DevMesh m, const LagScalars* sc) {
 }
 
 // compute_elem_centroid, compute_subelem_volume, compute_elem_volume, check_mesh
-// (:59-175, :290-396), optionally fused with the explicit update sol += dt*rhs.
-__global__ void k_cell_geometry(DevMesh m, double* sol6, const double* rhs6, const LagScalars* sc) {
-  if (sc && sc->skip) return;
+// (:59-175, :290-396) from the stored face geometry; any cell, periodic faces included.
+__global__ void k_cell_geometry(DevMesh m) {
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ne) return;
   int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
@@ -373,8 +375,213 @@ __global__ void k_cell_geometry(DevMesh m, double* sol6, const double* rhs6, con
   ok = ok && (fnorm2_3(nt.x, nt.y, nt.z) < 1e-14);
   ok = ok && (fnorm2_3(ns.x, ns.y, ns.z) < 1e-14);
   if (!ok) atomicOr(m.status, kErrMeshCheck);
+
+}
+
+// compute_geometry_mesh (:16-57) for the Lagrangian step, one cell per thread, each
+// face computed by the cell from its own vertices: compute_face_centroid (:177-208),
+// compute_subface_norm (:210-253), compute_face_norm (:255-271), compute_elem_centroid
+// (:59-110), compute_subelem_volume (:112-160), compute_elem_volume (:162-175) and
+// check_mesh (:374-411), then sol += dt * rhs (lagrange_main.F90:110). A face's
+// quantities are evaluated by both of its cells with the same operations on the same
+// coordinates (the same bits); the face's left cell writes what the next step reads
+// (face normal and area, subface areas). Evaluating each face twice costs less than
+// writing the face records and reading them back. The cell's vertex coordinates, face
+// centroids and face vertex positions are cached in shared memory (one column per
+// thread). Every face vertex must be a vertex of the cell (no periodic faces);
+// otherwise the cell reports SUBFV_ERR_INDEX. Divisions by 4 are written as products
+// by 0.25 (the same value for every operand).
+constexpr int kGeoMaxV = 8, kGeoMaxF = 8, kGeoBlock = 64;
+
+__device__ inline V3 pick4(const V3 (&P)[4], int i) { return i == 0 ? P[0] : i == 1 ? P[1] : i == 2 ? P[2] : P[3]; }
+
+__global__ void __launch_bounds__(kGeoBlock) k_geom_step(DevMesh m, double* sol6, const double* rhs6,
+                                                         const LagScalars* sc) {
+  __shared__ double sX[kGeoMaxV][3][kGeoBlock];
+  __shared__ double sCF[kGeoMaxF][3][kGeoBlock];
+  __shared__ int sV[kGeoMaxV][kGeoBlock];
+  __shared__ int sF[kGeoMaxF][kGeoBlock];
+  __shared__ int8_t sLV[kGeoMaxF][4][kGeoBlock];
+  if (sc && sc->skip) return;
+  const int t = threadIdx.x;
+  const int c = blockIdx.x * kGeoBlock + t;
+  if (c >= m.ne) return;
+  const int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
+  if (nvc > kGeoMaxV) {
+    atomicOr(m.status, kErrIndex);
+    return;
+  }
+  V3 ce = {0.0, 0.0, 0.0};
+  for (int k = 0; k < nvc; ++k) {
+    const int v = m.ev[vb + k];
+    const V3 x = ld3(m.x, v);
+    sV[k][t] = v;
+    sX[k][0][t] = x.x;
+    sX[k][1][t] = x.y;
+    sX[k][2][t] = x.z;
+    ce = {ce.x + x.x, ce.y + x.y, ce.z + x.z};
+  }
+  ce = {ce.x / nvc, ce.y / nvc, ce.z / nvc};
+  int nfc = 0;
+  for (int k = 0; k < kGeoMaxF; ++k) {
+    const int f = m.ef8[8 * (size_t)c + k];
+    if (f < 0) break;
+    sF[nfc++][t] = f;
+  }
+  unsigned leftm = 0, quadm = 0;
+  V3 cen = {0.0, 0.0, 0.0};
+  double sum_vol = 0.0, vdiv = 0.0;
+  V3 nt = {0.0, 0.0, 0.0}, ns = {0.0, 0.0, 0.0};
+  bool ok = true;
+  for (int j = 0; j < nfc; ++j) {
+    const int f = sF[j][t];
+    const int4 fv = m.fvert[f];
+    const int gid[4] = {fv.x, fv.y, fv.z, fv.w};
+    const int n = fv.w < 0 ? 3 : 4;
+    const bool left = m.flr[f].x == c;
+    if (left) leftm |= 1u << j;
+    if (n == 4) quadm |= 1u << j;
+    V3 P[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      P[k] = {0.0, 0.0, 0.0};
+      if (k < n) {
+        int q = 0;
+        while (q < nvc - 1 && sV[q][t] != gid[k]) ++q;
+        if (sV[q][t] != gid[k]) ok = false, q = 0;
+        sLV[j][k][t] = (int8_t)q;
+        P[k] = {sX[q][0][t], sX[q][1][t], sX[q][2][t]};
+      }
+    }
+    if (!ok) {
+      atomicOr(m.status, kErrIndex);
+      return;
+    }
+    // compute_face_centroid
+    V3 cg = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < n) cg = {cg.x + P[k].x, cg.y + P[k].y, cg.z + P[k].z};
+    cg = n == 4 ? V3{cg.x * 0.25, cg.y * 0.25, cg.z * 0.25} : V3{cg.x / 3, cg.y / 3, cg.z / 3};
+    V3 cf = {0.0, 0.0, 0.0};
+    double sum_area = 0.0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < n) {
+        const V3 pk = P[k], pp = pick4(P, k + 1 == n ? 0 : k + 1);
+        const V3 x = cross(sub(pk, cg), sub(pp, cg));
+        const double area = 0.5 * fnorm2_3(x.x, x.y, x.z);
+        cf.x = cf.x + area * (pk.x + pp.x + cg.x) / 3.0;
+        cf.y = cf.y + area * (pk.y + pp.y + cg.y) / 3.0;
+        cf.z = cf.z + area * (pk.z + pp.z + cg.z) / 3.0;
+        sum_area = sum_area + area;
+      }
+    cf = {cf.x / sum_area, cf.y / sum_area, cf.z / sum_area};
+    sCF[j][0][t] = cf.x;
+    sCF[j][1][t] = cf.y;
+    sCF[j][2][t] = cf.z;
+    // compute_subface_norm + compute_face_norm: the face's subfaces in face%sub_face
+    // order, which is ascending vertex id (subfaces are numbered vertex by vertex)
+    int ord = 0x3210;  // four 4-bit positions, sorted by global vertex id below
+#pragma unroll
+    for (int a = 1; a < 4; ++a)
+#pragma unroll
+      for (int b = a; b > 0; --b) {
+        if (b >= n) continue;
+        const int ob = (ord >> (4 * b)) & 15, oa = (ord >> (4 * (b - 1))) & 15;
+        const int gb = ob == 0 ? gid[0] : ob == 1 ? gid[1] : ob == 2 ? gid[2] : gid[3];
+        const int ga = oa == 0 ? gid[0] : oa == 1 ? gid[1] : oa == 2 ? gid[2] : gid[3];
+        if (gb < ga) ord = (ord & ~(0xff << (4 * (b - 1)))) | (oa << (4 * b)) | (ob << (4 * (b - 1)));
+      }
+    int4 fs = make_int4(-1, -1, -1, -1);
+    if (left) fs = m.fsf[f];
+    const int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
+    const double sg = left ? 1.0 : -1.0;
+    V3 fnrm = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int tt = 0; tt < 4; ++tt)
+      if (tt < n) {
+        const int k = (ord >> (4 * tt)) & 15;
+        const V3 cp = pick4(P, k);
+        const V3 cpm = half_sum(pick4(P, k == 0 ? n - 1 : k - 1), cp);
+        const V3 cpp = half_sum(pick4(P, k + 1 == n ? 0 : k + 1), cp);
+        const V3 a = cross(sub(cpm, cf), sub(cp, cf));
+        const V3 b = cross(sub(cp, cf), sub(cpp, cf));
+        const V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
+        const double area = fnorm2_3(nr.x, nr.y, nr.z);
+        const V3 un = {nr.x / area, nr.y / area, nr.z / area};
+        if (left) m.sfa[sfi[tt]] = area;
+        ns = {ns.x + area * (sg * un.x), ns.y + area * (sg * un.y), ns.z + area * (sg * un.z)};
+        fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
+      }
+    const double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
+    const V3 fu = {fnrm.x / fa, fnrm.y / fa, fnrm.z / fa};
+    if (left) m.fn[f] = make_double4(fu.x, fu.y, fu.z, fa);
+    // check_mesh_elem_volume / _closed terms of this face
+    const V3 nn = {sg * fu.x, sg * fu.y, sg * fu.z};
+    const V3 an = {fa * nn.x, fa * nn.y, fa * nn.z};
+    vdiv = vdiv + dot(cf, an);
+    nt = {nt.x + an.x, nt.y + an.y, nt.z + an.z};
+    // compute_elem_centroid: tetrahedra (edge, face centroid, vertex centroid)
+    const V3 fe = sub(cf, ce);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < n) {
+        const V3 cp = P[k], cpp = pick4(P, k + 1 == n ? 0 : k + 1);
+        const V3 x = left ? cross(sub(cp, cf), sub(cpp, cf)) : cross(sub(cpp, cf), sub(cp, cf));
+        const double vol = dot(x, fe) / 6.0;
+        cen.x = cen.x + vol * (cp.x + cpp.x + cf.x + ce.x) * 0.25;
+        cen.y = cen.y + vol * (cp.y + cpp.y + cf.y + ce.y) * 0.25;
+        cen.z = cen.z + vol * (cp.z + cpp.z + cf.z + ce.z) * 0.25;
+        sum_vol = sum_vol + vol;
+      }
+  }
+  cen = {cen.x / sum_vol, cen.y / sum_vol, cen.z / sum_vol};
+  // compute_subelem_volume: subcell k is (cell, vertex k); its subfaces in sub_elem order
+  double vcell = 0.0;
+  for (int k = 0; k < nvc; ++k) {
+    const int s = vb + k;
+    const int4 q4 = m.se_sf[s];
+    const int q[4] = {q4.x, q4.y, q4.z, q4.w};
+    double vol = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      if (q[jj] < 0) break;
+      const int f = m.sf_face[q[jj]], vert = m.sf_vert[q[jj]];
+      int j = 0;
+      while (j < nfc - 1 && sF[j][t] != f) ++j;
+      const int n = 3 + ((quadm >> j) & 1u);
+      int kk = 0;
+      while (kk < n - 1 && sV[sLV[j][kk][t]][t] != vert) ++kk;
+      const int lc = sLV[j][kk][t], lm = sLV[j][kk == 0 ? n - 1 : kk - 1][t], lp = sLV[j][kk + 1 == n ? 0 : kk + 1][t];
+      const V3 cp = {sX[lc][0][t], sX[lc][1][t], sX[lc][2][t]};
+      const V3 cpm = half_sum({sX[lm][0][t], sX[lm][1][t], sX[lm][2][t]}, cp);
+      const V3 cpp = half_sum({sX[lp][0][t], sX[lp][1][t], sX[lp][2][t]}, cp);
+      const V3 cf = {sCF[j][0][t], sCF[j][1][t], sCF[j][2][t]};
+      const V3 fe = sub(cf, cen);
+      const V3 a = sub(cpm, cf), b = sub(cp, cf), cc3 = sub(cpp, cf);
+      V3 x1, x2;
+      if ((leftm >> j) & 1u) {
+        x1 = cross(a, b);
+        x2 = cross(b, cc3);
+      } else {
+        x1 = cross(cc3, b);
+        x2 = cross(b, a);
+      }
+      vol = vol + dot(x1, fe) / 6.0 + dot(x2, fe) / 6.0;
+    }
+    m.vol_se[s] = vol;
+    ok = ok && (vol > 0.0);
+    vcell = vcell + vol;
+  }
+  m.vol[c] = vcell;
+  vdiv = vdiv / 3.0;
+  ok = ok && (fabs(vcell - vdiv) < 1e-14);
+  ok = ok && (fnorm2_3(nt.x, nt.y, nt.z) < 1e-14);
+  ok = ok && (fnorm2_3(ns.x, ns.y, ns.z) < 1e-14);
+  if (!ok) atomicOr(m.status, kErrMeshCheck);
   if (sol6) {  // lagrange_main.F90:110: new_sol = sol + dt*rhs
-    double dt = sc->dt;
+    const double dt = sc->dt;
     double* u = sol6 + kRec * (size_t)c;
     const double* r = rhs6 + kRhs * (size_t)c;
     bool fin = true;
@@ -415,11 +622,13 @@ __global__ void k_vert_is_bound(DevMesh m) {
 
 }  // namespace
 
-void launch_face_geometry(const DevMesh& m, const LagScalars* sc) {
-  k_face_geometry<<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, sc);
-}
-void launch_cell_geometry(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc) {
-  k_cell_geometry<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, sol6, rhs6, sc);
+void launch_geometry(const DevMesh& m, int full, double* sol6, const double* rhs6, const LagScalars* sc) {
+  if (full) {
+    k_face_geometry<<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, nullptr);
+    k_cell_geometry<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m);
+  } else {
+    k_geom_step<<<grid_for(m.ne, kGeoBlock), kGeoBlock, 0, m.stream>>>(m, sol6, rhs6, sc);
+  }
 }
 void launch_vert_volume(const DevMesh& m) { k_vert_volume<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }
 void launch_vert_is_bound(const DevMesh& m) { k_vert_is_bound<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }

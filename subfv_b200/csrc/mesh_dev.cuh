@@ -8,7 +8,7 @@
 //              or -(tag+1) for a boundary), fsf[nf] int4 (subface ids in the face's order),
 //              fc[nf] double4 (centroid), fn[nf] double4 (unit normal, area)
 //   subfaces   sf_face, sf_vert [nsf] int, sf_se[nsf] int2 (left/right subcell, -1 none),
-//              sfn[nsf] double4 (unit normal, area)
+//              sfn[nsf] double4 (unit normal, area), sfa[nsf] (area alone)
 //   subcells   se_elem, se_vert [nse], se_sf[nse] int4 (subfaces, -1 pad), vol_se[nse]
 //   cells      ev_off[ne+1] (cell subcells are ev_off[c]..ev_off[c+1]-1, one per vertex),
 //              ev[], ef8[ne] (faces, -1 pad to 8), cc[ne] double4 (centroid), vol[ne]
@@ -46,6 +46,16 @@ struct DevMesh {
   int2* sf_se = nullptr;
   int* sf_loc = nullptr;
   double4* sfn = nullptr;
+  double* sfa = nullptr;
+  // Lagrangian face records (6 doubles per face, allocated on first Lagrangian use):
+  // wave speeds and normal velocities of the face's two sides for the current state
+  double* frec = nullptr;
+  // per cell-CSR entry: subface, face, owning node | side << 30, subcell (Lagrangian
+  // cell kernel; built on first Lagrangian use)
+  int4* centry = nullptr;
+  // set when a Lagrangian step refreshed only the arrays the next step reads (face
+  // normals and areas, subface areas, volumes); the rest is recomputed on demand
+  int geom_partial = 0;
   // subcells
   int* se_elem = nullptr;
   int* se_vert = nullptr;
@@ -84,9 +94,10 @@ void devmesh_free(DevMesh* m);
 // Geometry kernels (mesh_geometry_module.F90:16-57), launched on m.stream.
 // sc (optional): a step whose skip flag is set leaves everything untouched; with sol6
 // the cell kernel also applies sol += dt*rhs using sc->dt.
-void launch_face_geometry(const DevMesh& m, const LagScalars* sc = nullptr);
-void launch_cell_geometry(const DevMesh& m, double* sol6 = nullptr, const double* rhs6 = nullptr,
-                          const LagScalars* sc = nullptr);
+// full: every geometric array; otherwise the Lagrangian step's subset (with sol6, the
+// update sol += dt*rhs fused in)
+void launch_geometry(const DevMesh& m, int full, double* sol6 = nullptr, const double* rhs6 = nullptr,
+                     const LagScalars* sc = nullptr);
 void launch_vert_volume(const DevMesh& m);
 void launch_vert_is_bound(const DevMesh& m);
 

@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(kNoAllocBlock) k_dt_partial(DevMesh m, const d
       int sf = m.vsf_identity ? p : m.vsf[p];
       int f = m.sf_face[sf];
       double4 fn = m.fn[f];
-      double area = m.sfn[sf].w;
+      double area = m.sfa[sf];
       int sv = m.sf_vert[sf];
       int2 se = m.sf_se[sf];
       int sub = side == 0 ? se.x : se.y;

@@ -304,6 +304,7 @@ int subfv_ns_batch_add(subfv_ns_batch* b, subfv_mesh* m, int take_mesh, const do
     set_error("subfv_ns_batch_add: null argument");
     return -2;
   }
+  if (handle_ensure_full_geometry(m->d)) return -1;
   const DevMesh& d = m->d;
   if (ns_node_lanes(d) == 0) {
     set_error("subfv_ns_batch_add: a vertex has more than 32 subfaces or subcells");

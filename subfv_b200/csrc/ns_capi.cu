@@ -146,6 +146,7 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
                           subfv_ns_state** out) {
   if (!m || !sol || !out || check_cfg(cfg)) return -2;
   DevMesh& d = m->d;
+  if (handle_ensure_full_geometry(d)) return -1;
   auto* s = new subfv_ns_state();
   s->m = m;
   s->P = ns_params_from(*cfg);

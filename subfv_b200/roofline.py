@@ -23,25 +23,21 @@ class MeshSizes:
 def lag_kernel_bytes(s: MeshSizes) -> dict:
     nv, ne, nf, nsf, nse, ncsf = s.nv, s.ne, s.nf, s.nsf, s.nse, s.ncsf
     b = {}
-    # k_lag_node: node CSR offsets, subface->face, face L/R, face normal record,
-    # subface record (area), cell state records, vp write, vertex volume (vse list, vol_se, write)
-    b["node"] = (4 * (nv + 1) + 4 * nsf + 8 * nf + 32 * nf + 32 * nsf + 48 * ne + 32 * nv
-                 + 4 * (nv + 1) + 4 * nse + 8 * nse + 8 * nv)
-    # k_lag_cell: cell CSR, subface->face/vertex, face L/R and normal, subface area,
-    # subcell ids, subcell volumes, vp, cell states, rhs write
-    b["cell"] = (4 * (ne + 1) + 4 * ncsf + 8 * nsf + 8 * nf + 32 * nf + 32 * nsf + 8 * nsf
-                 + 8 * nse + 32 * nv + 48 * ne + 48 * ne)
+    # k_lag_face: face L/R, face normal record, the cell records (each once), face record write
+    b["face"] = 8 * nf + 32 * nf + 64 * ne + 48 * nf
+    # k_lag_node: node CSR offsets, subface->face, face normal, subface area, face record, vp write
+    b["node"] = 4 * (nv + 1) + 4 * nsf + 32 * nf + 8 * nsf + 48 * nf + 32 * nv
+    # k_lag_cell: cell CSR, subface->face/vertex, face normal, subface area, face record, vp,
+    # subface->subcells, subcell volumes, cell records, rhs write
+    b["cell"] = (4 * (ne + 1) + 4 * ncsf + 8 * nsf + 32 * nf + 8 * nsf + 48 * nf + 32 * nv
+                 + 8 * nsf + 8 * nse + 64 * ne + 48 * ne)
     b["finalize"] = 64
     b["move"] = 32 * nv * 3  # x read+write, vp read
-    # k_face_geometry: face vertex ids, vertex records, face subface ids, subface vertex,
-    # writes: face centroid, face normal, subface records
-    b["face_geom"] = 16 * nf + 32 * nv + 16 * nf + 4 * nsf + 32 * nf + 32 * nf + 32 * nsf
-    # k_cell_geometry: cell vertex ids + offsets, cell faces, vertex records, face records
-    # (vertex ids, L/R, centroid, normal, subface ids), subcell subfaces, subface face/vertex,
-    # subface records, writes: centroid, volume, subcell volumes; update: sol and rhs read, sol write
-    b["cell_geom"] = (4 * (ne + 1) + 4 * nse + 32 * ne + 32 * nv + 16 * nf + 8 * nf + 32 * nf + 32 * nf
-                      + 16 * nf + 16 * nse + 8 * nsf + 32 * nsf + 32 * ne + 8 * ne + 8 * nse
-                      + 48 * ne * 3)
+    # k_geom<0>: cell vertex lists, vertex records, cell faces, face vertex ids, L/R, face
+    # subface ids, subcell subface ids, subface->face/vertex; writes: face normal records,
+    # subface areas, subcell and cell volumes; update: cell records read+write, rhs read
+    b["geom"] = (4 * (ne + 1) + 4 * nse + 32 * nv + 32 * ne + 16 * nf + 8 * nf + 16 * nf + 16 * nse
+                 + 8 * nsf + 32 * nf + 8 * nsf + 8 * nse + 8 * ne + 64 * ne * 2 + 48 * ne)
     return b
 
 
