@@ -78,6 +78,7 @@ int ensure_scratch(subfv_mesh* m) {
   SUBFV_CUDA(cudaMalloc(&m->sc, sizeof(LagScalars)));
   SUBFV_CUDA(cudaMalloc(&m->d.frec, 6 * (size_t)m->d.nf * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->d.centry, std::max<size_t>(m->d.ncsf, 1) * sizeof(int4)));
+  SUBFV_CUDA(cudaMalloc(&m->d.fS, (size_t)m->d.nf * sizeof(double4)));
   launch_build_cell_entries(m->d);
   return 0;
 }
@@ -212,7 +213,7 @@ int subfv_mesh_destroy(subfv_mesh* m) {
   if (!m) return 0;
   // scratch of the stateless calls (allocated on first use only); a mesh that never
   // needed it is released without any device-wide synchronisation
-  void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc, m->d.frec, m->d.centry};
+  void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc, m->d.frec, m->d.centry, m->d.fS};
   for (void* p : scratch)
     if (p) cudaFree(p);
   devmesh_free(&m->d);

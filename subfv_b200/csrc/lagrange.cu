@@ -78,6 +78,7 @@ __device__ inline double lam_wall(double p_me, double tau_me) {
 // interior (xb = v_bar of :75), 1 a z-face of a one-layer slab (b2d), 2 a wall
 // (xb = p_l + l1 v_l).
 constexpr int kFrec = 6;
+constexpr int kNodeChunk = 4, kCellChunk = 2;
 
 template <int P>
 __global__ void __launch_bounds__(128) k_lag_face(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc) {
@@ -121,36 +122,57 @@ __global__ void __launch_bounds__(128) k_lag_node(DevMesh m, const LagScalars* s
   double M00 = 0, M01 = 0, M02 = 0, M10 = 0, M11 = 0, M12 = 0, M20 = 0, M21 = 0, M22 = 0;
   double R0 = 0, R1 = 0, R2 = 0, B0 = 0, B1 = 0, B2 = 0;
   const int p0 = m.vsf_off[v], p1 = m.vsf_off[v + 1];
-  for (int p = p0; p < p1; ++p) {
-    const int sf = m.vsf_identity ? p : m.vsf[p];
-    const int f = m.sf_face[sf];
-    const double4 fn = m.fn[f];
-    const double n0 = fn.x, n1 = fn.y, n2 = fn.z;
-    const double area = m.sfa[sf];
-    const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)f);
-    const double2 ll = fr[0], xk = fr[2];
-    double w;
-    if (xk.y == 0.0) {  // interior face
-      const double v_bar = xk.x;
-      w = area * (ll.x + ll.y);
-      R0 = R0 + w * n0 * v_bar;
-      R1 = R1 + w * n1 * v_bar;
-      R2 = R2 + w * n2 * v_bar;
-    } else if (xk.y == 1.0) {
-      w = area * 2 * ll.x;
-    } else {
-      B0 = B0 + area * n0;
-      B1 = B1 + area * n1;
-      B2 = B2 + area * n2;
-      w = area * ll.x;
-      const double q = area * xk.x;
-      R0 = R0 + q * n0;
-      R1 = R1 + q * n1;
-      R2 = R2 + q * n2;
+  // entries in chunks of kNodeChunk: the chunk's loads are issued together, then the
+  // sums run in entry order
+  for (int p = p0; p < p1; p += kNodeChunk) {
+    double4 fnc[kNodeChunk];
+    double2 llc[kNodeChunk], xkc[kNodeChunk];
+    double arc[kNodeChunk];
+    int fc[kNodeChunk];
+#pragma unroll
+    for (int u = 0; u < kNodeChunk; ++u)
+      if (p + u < p1) {
+        const int sf = m.vsf_identity ? p + u : m.vsf[p + u];
+        fc[u] = m.sf_face[sf];
+        arc[u] = m.sfa[sf];
+      }
+#pragma unroll
+    for (int u = 0; u < kNodeChunk; ++u)
+      if (p + u < p1) {
+        fnc[u] = m.fn[fc[u]];
+        const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)fc[u]);
+        llc[u] = fr[0];
+        xkc[u] = fr[2];
+      }
+#pragma unroll
+    for (int u = 0; u < kNodeChunk; ++u) {
+      if (p + u >= p1) break;
+      const double n0 = fnc[u].x, n1 = fnc[u].y, n2 = fnc[u].z;
+      const double area = arc[u];
+      const double2 ll = llc[u], xk = xkc[u];
+      double w;
+      if (xk.y == 0.0) {  // interior face
+        const double v_bar = xk.x;
+        w = area * (ll.x + ll.y);
+        R0 = R0 + w * n0 * v_bar;
+        R1 = R1 + w * n1 * v_bar;
+        R2 = R2 + w * n2 * v_bar;
+      } else if (xk.y == 1.0) {
+        w = area * 2 * ll.x;
+      } else {
+        B0 = B0 + area * n0;
+        B1 = B1 + area * n1;
+        B2 = B2 + area * n2;
+        w = area * ll.x;
+        const double q = area * xk.x;
+        R0 = R0 + q * n0;
+        R1 = R1 + q * n1;
+        R2 = R2 + q * n2;
+      }
+      M00 = M00 + w * (n0 * n0); M01 = M01 + w * (n0 * n1); M02 = M02 + w * (n0 * n2);
+      M10 = M10 + w * (n1 * n0); M11 = M11 + w * (n1 * n1); M12 = M12 + w * (n1 * n2);
+      M20 = M20 + w * (n2 * n0); M21 = M21 + w * (n2 * n1); M22 = M22 + w * (n2 * n2);
     }
-    M00 = M00 + w * (n0 * n0); M01 = M01 + w * (n0 * n1); M02 = M02 + w * (n0 * n2);
-    M10 = M10 + w * (n1 * n0); M11 = M11 + w * (n1 * n1); M12 = M12 + w * (n1 * n2);
-    M20 = M20 + w * (n2 * n0); M21 = M21 + w * (n2 * n1); M22 = M22 + w * (n2 * n2);
   }
   // inverse_3_by_3 (linear_solver_module.F90:134-172): adjugate of the transpose
   double A00 = M11 * M22 - M12 * M21;
@@ -204,63 +226,91 @@ __global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __res
     double csnd = sqrt(kGamma * pme * me.t);
     double r0 = 0, r1 = 0, r2 = 0, r3 = 0, r4 = 0;
     bool bad = false;
-    for (int q = m.csf_off[c]; q < m.csf_off[c + 1]; ++q) {
-      const int4 E = m.centry[q];
-      const int sf = E.x, f = E.y, side = (E.z >> 30) & 1, node = E.z & 0x3fffffff;
-      double4 fn = m.fn[f];
-      double area = m.sfa[sf];
-      if (mode & 1) {
-        double4 vpn = m.vp[node];
-        double v_et = dot3(vpn.x, vpn.y, vpn.z, fn.x, fn.y, fn.z);
-        double am = area / mass;
-        const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)f);
-        const double2 ll = fr[0], vv = fr[1];
-        if (side == 0) {  // this cell is the face's left neighbour: lambda of its side, v.n
-          double lam = ll.x, vme = vv.x;
-          if (P == 0) {
-            double ps = pme - lam * (v_et - vme);
-            r0 = r0 - am * (-v_et);
-            r1 = r1 - am * (ps * fn.x);
-            r2 = r2 - am * (ps * fn.y);
-            r3 = r3 - am * (ps * fn.z);
-            r4 = r4 - am * (ps * v_et);
-          } else {
-            T ps = (T)pme - (T)lam * ((T)v_et - (T)vme);
-            r0 = r0 - am * (double)(-(T)v_et);
-            r1 = r1 - am * (double)(ps * (T)fn.x);
-            r2 = r2 - am * (double)(ps * (T)fn.y);
-            r3 = r3 - am * (double)(ps * (T)fn.z);
-            r4 = r4 - am * (double)(ps * (T)v_et);
+    const double vse_c = m.vol_se[c < m.nse ? c : 0];  // sub_elem(i) with i the cell (reference quirk)
+    const int q1 = m.csf_off[c + 1];
+    // entries in chunks of kCellChunk: the chunk's loads are issued together, then the
+    // sums run in entry order
+    for (int q = m.csf_off[c]; q < q1; q += kCellChunk) {
+      int4 Ec[kCellChunk];
+#pragma unroll
+      for (int u = 0; u < kCellChunk; ++u)
+        if (q + u < q1) Ec[u] = m.centry[q + u];
+      double4 fnc[kCellChunk], vpc[kCellChunk];
+      double2 llc[kCellChunk], vvc[kCellChunk];
+      double arc[kCellChunk], vsub[kCellChunk];
+#pragma unroll
+      for (int u = 0; u < kCellChunk; ++u)
+        if (q + u < q1) {
+          const int4 E = Ec[u];
+          const int node = E.z & 0x3fffffff;
+          fnc[u] = m.fn[E.y];
+          arc[u] = m.sfa[E.x];
+          vpc[u] = m.vp[node];
+          if (mode & 1) {
+            const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)E.y);
+            llc[u] = fr[0];
+            vvc[u] = fr[1];
           }
-        } else {  // right neighbour
-          double lam = ll.y, vme = vv.y;
-          if (P == 0) {
-            double ps = pme + lam * (v_et - vme);
-            r0 = r0 + am * (-v_et);
-            r1 = r1 + am * (ps * fn.x);
-            r2 = r2 + am * (ps * fn.y);
-            r3 = r3 + am * (ps * fn.z);
-            r4 = r4 + am * (ps * v_et);
-          } else {
-            T ps = (T)pme + (T)lam * ((T)v_et - (T)vme);
-            r0 = r0 + am * (double)(-(T)v_et);
-            r1 = r1 + am * (double)(ps * (T)fn.x);
-            r2 = r2 + am * (double)(ps * (T)fn.y);
-            r3 = r3 + am * (double)(ps * (T)fn.z);
-            r4 = r4 + am * (double)(ps * (T)v_et);
+          if (mode & 2) vsub[u] = E.w >= 0 ? m.vol_se[E.w] : 0.0;
+        }
+#pragma unroll
+      for (int u = 0; u < kCellChunk; ++u) {
+        if (q + u >= q1) break;
+        const int side = (Ec[u].z >> 30) & 1;
+        const double4 fn = fnc[u];
+        const double area = arc[u];
+        if (mode & 1) {
+          const double4 vpn = vpc[u];
+          double v_et = dot3(vpn.x, vpn.y, vpn.z, fn.x, fn.y, fn.z);
+          double am = area / mass;
+          const double2 ll = llc[u], vv = vvc[u];
+          if (side == 0) {  // this cell is the face's left neighbour: lambda of its side, v.n
+            double lam = ll.x, vme = vv.x;
+            if (P == 0) {
+              double ps = pme - lam * (v_et - vme);
+              r0 = r0 - am * (-v_et);
+              r1 = r1 - am * (ps * fn.x);
+              r2 = r2 - am * (ps * fn.y);
+              r3 = r3 - am * (ps * fn.z);
+              r4 = r4 - am * (ps * v_et);
+            } else {
+              T ps = (T)pme - (T)lam * ((T)v_et - (T)vme);
+              r0 = r0 - am * (double)(-(T)v_et);
+              r1 = r1 - am * (double)(ps * (T)fn.x);
+              r2 = r2 - am * (double)(ps * (T)fn.y);
+              r3 = r3 - am * (double)(ps * (T)fn.z);
+              r4 = r4 - am * (double)(ps * (T)v_et);
+            }
+          } else {  // right neighbour
+            double lam = ll.y, vme = vv.y;
+            if (P == 0) {
+              double ps = pme + lam * (v_et - vme);
+              r0 = r0 + am * (-v_et);
+              r1 = r1 + am * (ps * fn.x);
+              r2 = r2 + am * (ps * fn.y);
+              r3 = r3 + am * (ps * fn.z);
+              r4 = r4 + am * (ps * v_et);
+            } else {
+              T ps = (T)pme + (T)lam * ((T)v_et - (T)vme);
+              r0 = r0 + am * (double)(-(T)v_et);
+              r1 = r1 + am * (double)(ps * (T)fn.x);
+              r2 = r2 + am * (double)(ps * (T)fn.y);
+              r3 = r3 + am * (double)(ps * (T)fn.z);
+              r4 = r4 + am * (double)(ps * (T)v_et);
+            }
           }
         }
-      }
-      if (mode & 2) {  // compute_dt terms for (cell, subface)
-        double sg = side == 0 ? 1.0 : -1.0;
-        double4 vps = m.vp[m.vsf_identity ? node : m.sf_vert[sf]];  // the subface's own vertex
-        int sub = E.w;
-        double t1 = m.vol_se[c] / (area * csnd);  // sub_elem(i) with i the cell (reference quirk)
-        double vn = dot3(vps.x, vps.y, vps.z, sg * fn.x, sg * fn.y, sg * fn.z);
-        double t2 = sub >= 0 ? 0.8 * m.vol_se[sub] / (1e-8 + fabs(vn) * fn.w) : 1e6;
-        if (t1 < dtloc) dtloc = t1;
-        if (t2 < dtloc) dtloc = t2;
-        bad = bad || !(t1 >= 0.0) || !(t2 >= 0.0);
+        if (mode & 2) {  // compute_dt terms for (cell, subface)
+          double sg = side == 0 ? 1.0 : -1.0;
+          // the subface's own vertex (the owning node unless the node list is a periodic extension)
+          const double4 vps = m.vsf_identity ? vpc[u] : m.vp[m.sf_vert[Ec[u].x]];
+          double t1 = vse_c / (area * csnd);
+          double vn = dot3(vps.x, vps.y, vps.z, sg * fn.x, sg * fn.y, sg * fn.z);
+          double t2 = Ec[u].w >= 0 ? 0.8 * vsub[u] / (1e-8 + fabs(vn) * fn.w) : 1e6;
+          if (t1 < dtloc) dtloc = t1;
+          if (t2 < dtloc) dtloc = t2;
+          bad = bad || !(t1 >= 0.0) || !(t2 >= 0.0);
+        }
       }
     }
     if (mode & 1) {

@@ -223,53 +223,69 @@ __device__ inline V3 half_sum(V3 a, V3 b) { return {0.5 * (a.x + b.x), 0.5 * (a.
 
 // ---- full geometry: one thread per face, then one per cell (every array written)
 
-// compute_face_centroid + compute_subface_norm + compute_face_norm (:177-271)
-__global__ void k_face_geometry(DevMesh m, const LagScalars* sc) {
+__device__ inline V3 pick4(const V3 (&P)[4], int i) { return i == 0 ? P[0] : i == 1 ? P[1] : i == 2 ? P[2] : P[3]; }
+
+// compute_face_centroid + compute_subface_norm + compute_face_norm (:177-271), one thread
+// per face. Also fS[f] = sum over the face's subfaces (in face%sub_face order) of
+// area * unit normal, which the Lagrangian step's cell kernel uses for check_mesh's
+// subface closure. FULL = 0 (the Lagrangian step) skips the subface unit normals, which
+// the step does not read.
+template <int FULL>
+__global__ void k_face_geom(DevMesh m, const LagScalars* sc) {
   if (sc && sc->skip) return;
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= m.nf) return;
-  int4 fv = m.fvert[f];
-  int vid[4] = {fv.x, fv.y, fv.z, fv.w};
-  int n = fv.w < 0 ? 3 : 4;
+  const int4 fv = m.fvert[f];
+  const int vid[4] = {fv.x, fv.y, fv.z, fv.w};
+  const int n = fv.w < 0 ? 3 : 4;
   V3 P[4];
-  for (int k = 0; k < n; ++k) P[k] = ld3(m.x, vid[k]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) P[k] = k < n ? ld3(m.x, vid[k]) : V3{0.0, 0.0, 0.0};
   V3 cg = {0.0, 0.0, 0.0};
-  for (int k = 0; k < n; ++k) cg = {cg.x + P[k].x, cg.y + P[k].y, cg.z + P[k].z};
-  cg = {cg.x / n, cg.y / n, cg.z / n};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < n) cg = {cg.x + P[k].x, cg.y + P[k].y, cg.z + P[k].z};
+  cg = n == 4 ? V3{cg.x * 0.25, cg.y * 0.25, cg.z * 0.25} : V3{cg.x / 3, cg.y / 3, cg.z / 3};
   V3 c = {0.0, 0.0, 0.0};
   double sum_area = 0.0;
-  for (int j = 0; j < n; ++j) {
-    int jp = (j + 1) % n;
-    V3 x = cross(sub(P[j], cg), sub(P[jp], cg));
-    double area = 0.5 * fnorm2_3(x.x, x.y, x.z);
-    c.x = c.x + area * (P[j].x + P[jp].x + cg.x) / 3.0;
-    c.y = c.y + area * (P[j].y + P[jp].y + cg.y) / 3.0;
-    c.z = c.z + area * (P[j].z + P[jp].z + cg.z) / 3.0;
-    sum_area = sum_area + area;
-  }
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (j < n) {
+      const V3 pj = P[j], pp = pick4(P, j + 1 == n ? 0 : j + 1);
+      const V3 x = cross(sub(pj, cg), sub(pp, cg));
+      const double area = 0.5 * fnorm2_3(x.x, x.y, x.z);
+      c.x = c.x + area * (pj.x + pp.x + cg.x) / 3.0;
+      c.y = c.y + area * (pj.y + pp.y + cg.y) / 3.0;
+      c.z = c.z + area * (pj.z + pp.z + cg.z) / 3.0;
+      sum_area = sum_area + area;
+    }
   c = {c.x / sum_area, c.y / sum_area, c.z / sum_area};
   m.fc[f] = make_double4(c.x, c.y, c.z, 0.0);
-  int4 fs = m.fsf[f];
-  int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
-  V3 fnrm = {0.0, 0.0, 0.0};
-  for (int k = 0; k < n; ++k) {
-    int sf = sfi[k];
-    int vert = m.sf_vert[sf];
-    int j = 0;
-    while (j < n - 1 && vid[j] != vert) ++j;
-    int jp = (j + 1) % n, jm = (j - 1 + n) % n;
-    V3 cp = P[j];
-    V3 cpm = half_sum(P[jm], cp), cpp = half_sum(P[jp], cp);
-    V3 a = cross(sub(cpm, c), sub(cp, c));
-    V3 b = cross(sub(cp, c), sub(cpp, c));
-    V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
-    double area = fnorm2_3(nr.x, nr.y, nr.z);
-    m.sfn[sf] = make_double4(nr.x / area, nr.y / area, nr.z / area, area);
-    m.sfa[sf] = area;
-    fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
-  }
-  double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
+  const int4 fs = m.fsf[f];
+  const int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
+  V3 fnrm = {0.0, 0.0, 0.0}, S = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < n) {
+      const int sf = sfi[k];
+      const int vert = m.sf_vert[sf];
+      int j = 0;
+      while (j < n - 1 && vid[j] != vert) ++j;
+      const V3 cp = pick4(P, j);
+      const V3 cpm = half_sum(pick4(P, j == 0 ? n - 1 : j - 1), cp), cpp = half_sum(pick4(P, j + 1 == n ? 0 : j + 1), cp);
+      const V3 a = cross(sub(cpm, c), sub(cp, c));
+      const V3 b = cross(sub(cp, c), sub(cpp, c));
+      const V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
+      const double area = fnorm2_3(nr.x, nr.y, nr.z);
+      const V3 un = {nr.x / area, nr.y / area, nr.z / area};
+      if (FULL) m.sfn[sf] = make_double4(un.x, un.y, un.z, area);
+      m.sfa[sf] = area;
+      S = {S.x + area * un.x, S.y + area * un.y, S.z + area * un.z};
+      fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
+    }
+  const double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
   m.fn[f] = make_double4(fnrm.x / fa, fnrm.y / fa, fnrm.z / fa, fa);
+  if (m.fS) m.fS[f] = make_double4(S.x, S.y, S.z, 0.0);
 }
 
 // compute_elem_centroid, compute_subelem_volume, compute_elem_volume, check_mesh
@@ -378,22 +394,17 @@ __global__ void k_cell_geometry(DevMesh m) {
 
 }
 
-// compute_geometry_mesh (:16-57) for the Lagrangian step, one cell per thread, each
-// face computed by the cell from its own vertices: compute_face_centroid (:177-208),
-// compute_subface_norm (:210-253), compute_face_norm (:255-271), compute_elem_centroid
-// (:59-110), compute_subelem_volume (:112-160), compute_elem_volume (:162-175) and
-// check_mesh (:374-411), then sol += dt * rhs (lagrange_main.F90:110). A face's
-// quantities are evaluated by both of its cells with the same operations on the same
-// coordinates (the same bits); the face's left cell writes what the next step reads
-// (face normal and area, subface areas). Evaluating each face twice costs less than
-// writing the face records and reading them back. The cell's vertex coordinates, face
-// centroids and face vertex positions are cached in shared memory (one column per
-// thread). Every face vertex must be a vertex of the cell (no periodic faces);
-// otherwise the cell reports SUBFV_ERR_INDEX. Divisions by 4 are written as products
-// by 0.25 (the same value for every operand).
+// The cell part of compute_geometry_mesh for the Lagrangian step, one cell per thread,
+// after k_face_geom<0>: compute_elem_centroid (:59-110), compute_subelem_volume
+// (:112-160), compute_elem_volume (:162-175) and check_mesh (:374-411), then
+// sol += dt * rhs (lagrange_main.F90:110). The cell's vertex coordinates, face centroids
+// and face vertex positions are cached in shared memory (one column per thread), so each
+// is loaded once per cell. check_mesh_subface_closed adds each face's subface sum S as a
+// whole: the same total as the subface-by-subface sum up to rounding, and the test is a
+// 1e-14 threshold on its norm. Every face vertex must be a vertex of the cell (no
+// periodic faces); otherwise the cell reports SUBFV_ERR_INDEX.
 constexpr int kGeoMaxV = 8, kGeoMaxF = 8, kGeoBlock = 64;
 
-__device__ inline V3 pick4(const V3 (&P)[4], int i) { return i == 0 ? P[0] : i == 1 ? P[1] : i == 2 ? P[2] : P[3]; }
 
 __global__ void __launch_bounds__(kGeoBlock) k_geom_step(DevMesh m, double* sol6, const double* rhs6,
                                                          const LagScalars* sc) {
@@ -457,71 +468,21 @@ __global__ void __launch_bounds__(kGeoBlock) k_geom_step(DevMesh m, double* sol6
       atomicOr(m.status, kErrIndex);
       return;
     }
-    // compute_face_centroid
-    V3 cg = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (k < n) cg = {cg.x + P[k].x, cg.y + P[k].y, cg.z + P[k].z};
-    cg = n == 4 ? V3{cg.x * 0.25, cg.y * 0.25, cg.z * 0.25} : V3{cg.x / 3, cg.y / 3, cg.z / 3};
-    V3 cf = {0.0, 0.0, 0.0};
-    double sum_area = 0.0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (k < n) {
-        const V3 pk = P[k], pp = pick4(P, k + 1 == n ? 0 : k + 1);
-        const V3 x = cross(sub(pk, cg), sub(pp, cg));
-        const double area = 0.5 * fnorm2_3(x.x, x.y, x.z);
-        cf.x = cf.x + area * (pk.x + pp.x + cg.x) / 3.0;
-        cf.y = cf.y + area * (pk.y + pp.y + cg.y) / 3.0;
-        cf.z = cf.z + area * (pk.z + pp.z + cg.z) / 3.0;
-        sum_area = sum_area + area;
-      }
-    cf = {cf.x / sum_area, cf.y / sum_area, cf.z / sum_area};
+    // the face's geometry from k_face_geom
+    const V3 cf = ld3(m.fc, f);
     sCF[j][0][t] = cf.x;
     sCF[j][1][t] = cf.y;
     sCF[j][2][t] = cf.z;
-    // compute_subface_norm + compute_face_norm: the face's subfaces in face%sub_face
-    // order, which is ascending vertex id (subfaces are numbered vertex by vertex)
-    int ord = 0x3210;  // four 4-bit positions, sorted by global vertex id below
-#pragma unroll
-    for (int a = 1; a < 4; ++a)
-#pragma unroll
-      for (int b = a; b > 0; --b) {
-        if (b >= n) continue;
-        const int ob = (ord >> (4 * b)) & 15, oa = (ord >> (4 * (b - 1))) & 15;
-        const int gb = ob == 0 ? gid[0] : ob == 1 ? gid[1] : ob == 2 ? gid[2] : gid[3];
-        const int ga = oa == 0 ? gid[0] : oa == 1 ? gid[1] : oa == 2 ? gid[2] : gid[3];
-        if (gb < ga) ord = (ord & ~(0xff << (4 * (b - 1)))) | (oa << (4 * b)) | (ob << (4 * (b - 1)));
-      }
-    int4 fs = make_int4(-1, -1, -1, -1);
-    if (left) fs = m.fsf[f];
-    const int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
+    const double4 fn = m.fn[f];
+    const double4 S = m.fS[f];
     const double sg = left ? 1.0 : -1.0;
-    V3 fnrm = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int tt = 0; tt < 4; ++tt)
-      if (tt < n) {
-        const int k = (ord >> (4 * tt)) & 15;
-        const V3 cp = pick4(P, k);
-        const V3 cpm = half_sum(pick4(P, k == 0 ? n - 1 : k - 1), cp);
-        const V3 cpp = half_sum(pick4(P, k + 1 == n ? 0 : k + 1), cp);
-        const V3 a = cross(sub(cpm, cf), sub(cp, cf));
-        const V3 b = cross(sub(cp, cf), sub(cpp, cf));
-        const V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
-        const double area = fnorm2_3(nr.x, nr.y, nr.z);
-        const V3 un = {nr.x / area, nr.y / area, nr.z / area};
-        if (left) m.sfa[sfi[tt]] = area;
-        ns = {ns.x + area * (sg * un.x), ns.y + area * (sg * un.y), ns.z + area * (sg * un.z)};
-        fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
-      }
-    const double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
-    const V3 fu = {fnrm.x / fa, fnrm.y / fa, fnrm.z / fa};
-    if (left) m.fn[f] = make_double4(fu.x, fu.y, fu.z, fa);
-    // check_mesh_elem_volume / _closed terms of this face
-    const V3 nn = {sg * fu.x, sg * fu.y, sg * fu.z};
-    const V3 an = {fa * nn.x, fa * nn.y, fa * nn.z};
+    // check_mesh_elem_volume / _closed / _subface_closed terms of this face (the subface
+    // closure sums the face's own subface sum S, formed in face%sub_face order)
+    const V3 nn = {sg * fn.x, sg * fn.y, sg * fn.z};
+    const V3 an = {fn.w * nn.x, fn.w * nn.y, fn.w * nn.z};
     vdiv = vdiv + dot(cf, an);
     nt = {nt.x + an.x, nt.y + an.y, nt.z + an.z};
+    ns = {ns.x + sg * S.x, ns.y + sg * S.y, ns.z + sg * S.z};
     // compute_elem_centroid: tetrahedra (edge, face centroid, vertex centroid)
     const V3 fe = sub(cf, ce);
 #pragma unroll
@@ -624,9 +585,10 @@ __global__ void k_vert_is_bound(DevMesh m) {
 
 void launch_geometry(const DevMesh& m, int full, double* sol6, const double* rhs6, const LagScalars* sc) {
   if (full) {
-    k_face_geometry<<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, nullptr);
+    k_face_geom<1><<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, nullptr);
     k_cell_geometry<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m);
   } else {
+    k_face_geom<0><<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, sc);
     k_geom_step<<<grid_for(m.ne, kGeoBlock), kGeoBlock, 0, m.stream>>>(m, sol6, rhs6, sc);
   }
 }

@@ -53,6 +53,8 @@ struct DevMesh {
   // per cell-CSR entry: subface, face, owning node | side << 30, subcell (Lagrangian
   // cell kernel; built on first Lagrangian use)
   int4* centry = nullptr;
+  // per face: sum of area * unit normal over its subfaces (Lagrangian step's mesh check)
+  double4* fS = nullptr;
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;
