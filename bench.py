@@ -593,7 +593,7 @@ def main():
             "gpu_launches": 6 * args.steps,
             "clocks": clocks,
             "e2e": e2e,
-            "roofline": {"bound": "hbm", "kernel": ("k_geom<0>" if dom == "geom" else f"k_lag_{dom}"), "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": ("k_face_geom<0>+k_geom_step" if dom == "geom" else f"k_lag_{dom}"), "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": _traffic(dom), "algorithmic_bytes": kb[dom],
                          "kernel_ms": per[dom], "step_achieved_gbs": step_achieved},
