@@ -252,6 +252,33 @@ int subfv_ns_batch_get_sol(subfv_ns_batch* b, int slot, double* sol);
 int subfv_ns_batch_set_launch(subfv_ns_batch* b, int block_v, int grid_v, int grid_c);
 
 /* ---------------------------------------------------------------------------------
+ * Batched and served Lagrangian hydro. No counterpart in the reference (one mesh per
+ * lagrange_main.F90 process): many independent problems, each its own mesh (moved by its
+ * steps), initial state, mass, CFL number and end time, advanced together in shared
+ * launches; each result is bit-identical to the same problem run alone through
+ * subfv_lag_state. Calls and semantics as for subfv_ns_batch_*. */
+typedef struct subfv_lag_batch subfv_lag_batch;
+int subfv_lag_batch_create(int precision, int capacity, int64_t budget_bytes, subfv_lag_batch** out);
+int subfv_lag_batch_destroy(subfv_lag_batch* b);
+int64_t subfv_lag_batch_state_bytes(const subfv_lag_batch* b, const subfv_mesh* m);
+int64_t subfv_lag_batch_free_bytes(const subfv_lag_batch* b);
+int subfv_lag_batch_size(const subfv_lag_batch* b, int* n_live, int64_t* used_bytes);
+/* sol (5, n_elems), mass (n_elems) as for subfv_lag_state_create; returns
+ * SUBFV_BATCH_FULL when the problem cannot be admitted now. */
+int subfv_lag_batch_add(subfv_lag_batch* b, subfv_mesh* m, int take_mesh, const double* sol, const double* mass,
+                        double cfl, double t0, double t_max, int* slot);
+int subfv_lag_batch_remove(subfv_lag_batch* b, int slot);
+int subfv_lag_batch_advance(subfv_lag_batch* b, int n_steps);
+int subfv_lag_batch_time_steps(subfv_lag_batch* b, int n_steps, double* ms);
+int subfv_lag_batch_poll(subfv_lag_batch* b, int wait);
+int subfv_lag_batch_sync(subfv_lag_batch* b);
+int subfv_lag_batch_slot_info(const subfv_lag_batch* b, int slot, double* t, int64_t* steps, int* done,
+                              unsigned* status);
+int subfv_lag_batch_get_sol(subfv_lag_batch* b, int slot, double* sol);
+/* persistent grid size of every batched kernel; results do not depend on it */
+int subfv_lag_batch_set_grid(subfv_lag_batch* b, int grid);
+
+/* ---------------------------------------------------------------------------------
  * Block-CSR linear algebra (src/linear_algebra/sparse_bcsr_linear_module.F90).
  * bcsr_matrix_type layout: m block rows, row(m+1) and col(nnz) 1-based, values
  * v(bs, bs, nnz) column-major blocks. Vectors have bs*m entries (host arrays). */

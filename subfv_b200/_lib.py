@@ -79,6 +79,20 @@ SIGNATURES = {
     "subfv_ns_batch_slot_info": (c_int, [P, c_int, PD, C.POINTER(c_i64), C.POINTER(c_int), C.POINTER(C.c_uint)]),
     "subfv_ns_batch_get_sol": (c_int, [P, c_int, PD]),
     "subfv_ns_batch_set_launch": (c_int, [P, c_int, c_int, c_int]),
+    "subfv_lag_batch_create": (c_int, [c_int, c_int, c_i64, C.POINTER(P)]),
+    "subfv_lag_batch_destroy": (c_int, [P]),
+    "subfv_lag_batch_state_bytes": (c_i64, [P, P]),
+    "subfv_lag_batch_free_bytes": (c_i64, [P]),
+    "subfv_lag_batch_size": (c_int, [P, C.POINTER(c_int), C.POINTER(c_i64)]),
+    "subfv_lag_batch_add": (c_int, [P, P, c_int, PD, PD, c_dbl, c_dbl, c_dbl, C.POINTER(c_int)]),
+    "subfv_lag_batch_remove": (c_int, [P, c_int]),
+    "subfv_lag_batch_advance": (c_int, [P, c_int]),
+    "subfv_lag_batch_time_steps": (c_int, [P, c_int, PD]),
+    "subfv_lag_batch_poll": (c_int, [P, c_int]),
+    "subfv_lag_batch_sync": (c_int, [P]),
+    "subfv_lag_batch_slot_info": (c_int, [P, c_int, PD, C.POINTER(c_i64), C.POINTER(c_int), C.POINTER(C.c_uint)]),
+    "subfv_lag_batch_get_sol": (c_int, [P, c_int, PD]),
+    "subfv_lag_batch_set_grid": (c_int, [P, c_int]),
     "subfv_bcsr_create": (c_int, [c_int, c_int, PI32, PI32, PD, C.POINTER(P)]),
     "subfv_bcsr_destroy": (c_int, [P]),
     "subfv_bcsr_set_values": (c_int, [P, PD]),

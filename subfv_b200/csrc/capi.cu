@@ -47,6 +47,7 @@ int check_status(DevMesh& d);
 int clear_status(DevMesh& d);
 int ensure_scratch(subfv_mesh* m);
 int ensure_full_geometry(DevMesh& d);
+int ensure_lag_arrays(DevMesh& d);
 }  // namespace
 
 namespace subfv {
@@ -54,6 +55,7 @@ int handle_check_status(DevMesh& d) { return check_status(d); }
 int handle_clear_status(DevMesh& d) { return clear_status(d); }
 int handle_ensure_scratch(subfv_mesh* m) { return ensure_scratch(m); }
 int handle_ensure_full_geometry(DevMesh& d) { return ensure_full_geometry(d); }
+int handle_ensure_lag_arrays(DevMesh& d) { return ensure_lag_arrays(d); }
 }  // namespace subfv
 
 namespace {
@@ -76,10 +78,19 @@ int ensure_scratch(subfv_mesh* m) {
   SUBFV_CUDA(cudaMalloc(&m->rhs6, 6 * (size_t)m->d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->mass, (size_t)m->d.ne * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&m->sc, sizeof(LagScalars)));
-  SUBFV_CUDA(cudaMalloc(&m->d.frec, 6 * (size_t)m->d.nf * sizeof(double)));
-  SUBFV_CUDA(cudaMalloc(&m->d.centry, std::max<size_t>(m->d.ncsf, 1) * sizeof(int4)));
-  SUBFV_CUDA(cudaMalloc(&m->d.fS, (size_t)m->d.nf * sizeof(double4)));
-  launch_build_cell_entries(m->d);
+  return ensure_lag_arrays(m->d);
+}
+// The Lagrangian step's per-mesh arrays (face records, cell entries, face subface sums),
+// stream-ordered on the mesh's stream and released with the mesh.
+int ensure_lag_arrays(DevMesh& d) {
+  if (d.frec) return 0;
+  SUBFV_CUDA(cudaMallocAsync((void**)&d.frec, 6 * (size_t)d.nf * sizeof(double), d.stream));
+  SUBFV_CUDA(cudaMallocAsync((void**)&d.centry, std::max<size_t>(d.ncsf, 1) * sizeof(int4), d.stream));
+  SUBFV_CUDA(cudaMallocAsync((void**)&d.fS, (size_t)d.nf * sizeof(double4), d.stream));
+  d.bytes += 6 * (size_t)d.nf * sizeof(double) + std::max<size_t>(d.ncsf, 1) * sizeof(int4) +
+             (size_t)d.nf * sizeof(double4);
+  launch_build_cell_entries(d);
+  SUBFV_CUDA(cudaGetLastError());
   return 0;
 }
 // After Lagrangian steps (which refresh only what the next step reads), recompute every
@@ -213,7 +224,7 @@ int subfv_mesh_destroy(subfv_mesh* m) {
   if (!m) return 0;
   // scratch of the stateless calls (allocated on first use only); a mesh that never
   // needed it is released without any device-wide synchronisation
-  void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc, m->d.frec, m->d.centry, m->d.fS};
+  void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc};
   for (void* p : scratch)
     if (p) cudaFree(p);
   devmesh_free(&m->d);

@@ -1,0 +1,250 @@
+// Geometry of compute_geometry_mesh (src/mesh/mesh_geometry_module.F90) as per-entity
+// device functions, shared by the solo kernels (mesh_dev.cu) and the batched Lagrangian
+// kernels (lagrange.cu).
+#pragma once
+#include "common.cuh"
+#include "mesh_dev.cuh"
+
+namespace subfv {
+namespace geo {
+
+struct V3 {
+  double x, y, z;
+};
+__device__ inline V3 ld3(const double4* a, int i) {
+  double4 v = a[i];
+  return {v.x, v.y, v.z};
+}
+__device__ inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ inline V3 cross(V3 a, V3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ inline double dot(V3 a, V3 b) { return dot3(a.x, a.y, a.z, b.x, b.y, b.z); }
+__device__ inline V3 half_sum(V3 a, V3 b) { return {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)}; }
+
+__device__ inline V3 pick4(const V3 (&P)[4], int i) { return i == 0 ? P[0] : i == 1 ? P[1] : i == 2 ? P[2] : P[3]; }
+
+// compute_face_centroid + compute_subface_norm + compute_face_norm (:177-271), one thread
+// per face. Also fS[f] = sum over the face's subfaces (in face%sub_face order) of
+// area * unit normal, which the Lagrangian step's cell kernel uses for check_mesh's
+// subface closure. FULL = 0 (the Lagrangian step) skips the subface unit normals, which
+// the step does not read.
+template <int FULL>
+__device__ inline void face_geom_body(const DevMesh& m, const int f) {
+  if (f >= m.nf) return;
+  const int4 fv = m.fvert[f];
+  const int vid[4] = {fv.x, fv.y, fv.z, fv.w};
+  const int n = fv.w < 0 ? 3 : 4;
+  V3 P[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) P[k] = k < n ? ld3(m.x, vid[k]) : V3{0.0, 0.0, 0.0};
+  V3 cg = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < n) cg = {cg.x + P[k].x, cg.y + P[k].y, cg.z + P[k].z};
+  cg = n == 4 ? V3{cg.x * 0.25, cg.y * 0.25, cg.z * 0.25} : V3{cg.x / 3, cg.y / 3, cg.z / 3};
+  V3 c = {0.0, 0.0, 0.0};
+  double sum_area = 0.0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (j < n) {
+      const V3 pj = P[j], pp = pick4(P, j + 1 == n ? 0 : j + 1);
+      const V3 x = cross(sub(pj, cg), sub(pp, cg));
+      const double area = 0.5 * fnorm2_3(x.x, x.y, x.z);
+      c.x = c.x + area * (pj.x + pp.x + cg.x) / 3.0;
+      c.y = c.y + area * (pj.y + pp.y + cg.y) / 3.0;
+      c.z = c.z + area * (pj.z + pp.z + cg.z) / 3.0;
+      sum_area = sum_area + area;
+    }
+  c = {c.x / sum_area, c.y / sum_area, c.z / sum_area};
+  m.fc[f] = make_double4(c.x, c.y, c.z, 0.0);
+  const int4 fs = m.fsf[f];
+  const int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
+  V3 fnrm = {0.0, 0.0, 0.0}, S = {0.0, 0.0, 0.0};
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    if (k < n) {
+      const int sf = sfi[k];
+      const int vert = m.sf_vert[sf];
+      int j = 0;
+      while (j < n - 1 && vid[j] != vert) ++j;
+      const V3 cp = pick4(P, j);
+      const V3 cpm = half_sum(pick4(P, j == 0 ? n - 1 : j - 1), cp), cpp = half_sum(pick4(P, j + 1 == n ? 0 : j + 1), cp);
+      const V3 a = cross(sub(cpm, c), sub(cp, c));
+      const V3 b = cross(sub(cp, c), sub(cpp, c));
+      const V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
+      const double area = fnorm2_3(nr.x, nr.y, nr.z);
+      const V3 un = {nr.x / area, nr.y / area, nr.z / area};
+      if (FULL) m.sfn[sf] = make_double4(un.x, un.y, un.z, area);
+      m.sfa[sf] = area;
+      S = {S.x + area * un.x, S.y + area * un.y, S.z + area * un.z};
+      fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
+    }
+  const double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
+  m.fn[f] = make_double4(fnrm.x / fa, fnrm.y / fa, fnrm.z / fa, fa);
+  if (m.fS) m.fS[f] = make_double4(S.x, S.y, S.z, 0.0);
+}
+
+// The cell part of compute_geometry_mesh for the Lagrangian step, one cell per thread,
+// after k_face_geom<0>: compute_elem_centroid (:59-110), compute_subelem_volume
+// (:112-160), compute_elem_volume (:162-175) and check_mesh (:374-411), then
+// sol += dt * rhs (lagrange_main.F90:110). The cell's vertex coordinates, face centroids
+// and face vertex positions are cached in shared memory (one column per thread), so each
+// is loaded once per cell. check_mesh_subface_closed adds each face's subface sum S as a
+// whole: the same total as the subface-by-subface sum up to rounding, and the test is a
+// 1e-14 threshold on its norm. Every face vertex must be a vertex of the cell (no
+// periodic faces); otherwise the cell reports SUBFV_ERR_INDEX.
+constexpr int kGeoMaxV = 8, kGeoMaxF = 8, kGeoBlock = 64;
+
+
+// c: this thread's cell; every thread of a kGeoBlock-thread block calls (the caches are
+// indexed by threadIdx.x); dt: the step's time step for the update (with sol6)
+__device__ inline void geom_step_body(const DevMesh& m, double* sol6, const double* rhs6, const double dt,
+                                      const int c) {
+  __shared__ double sX[kGeoMaxV][3][kGeoBlock];
+  __shared__ double sCF[kGeoMaxF][3][kGeoBlock];
+  __shared__ int sV[kGeoMaxV][kGeoBlock];
+  __shared__ int sF[kGeoMaxF][kGeoBlock];
+  __shared__ int8_t sLV[kGeoMaxF][4][kGeoBlock];
+  const int t = threadIdx.x;
+  if (c >= m.ne) return;
+  const int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
+  if (nvc > kGeoMaxV) {
+    atomicOr(m.status, kErrIndex);
+    return;
+  }
+  V3 ce = {0.0, 0.0, 0.0};
+  for (int k = 0; k < nvc; ++k) {
+    const int v = m.ev[vb + k];
+    const V3 x = ld3(m.x, v);
+    sV[k][t] = v;
+    sX[k][0][t] = x.x;
+    sX[k][1][t] = x.y;
+    sX[k][2][t] = x.z;
+    ce = {ce.x + x.x, ce.y + x.y, ce.z + x.z};
+  }
+  ce = {ce.x / nvc, ce.y / nvc, ce.z / nvc};
+  int nfc = 0;
+  for (int k = 0; k < kGeoMaxF; ++k) {
+    const int f = m.ef8[8 * (size_t)c + k];
+    if (f < 0) break;
+    sF[nfc++][t] = f;
+  }
+  unsigned leftm = 0, quadm = 0;
+  V3 cen = {0.0, 0.0, 0.0};
+  double sum_vol = 0.0, vdiv = 0.0;
+  V3 nt = {0.0, 0.0, 0.0}, ns = {0.0, 0.0, 0.0};
+  bool ok = true;
+  for (int j = 0; j < nfc; ++j) {
+    const int f = sF[j][t];
+    const int4 fv = m.fvert[f];
+    const int gid[4] = {fv.x, fv.y, fv.z, fv.w};
+    const int n = fv.w < 0 ? 3 : 4;
+    const bool left = m.flr[f].x == c;
+    if (left) leftm |= 1u << j;
+    if (n == 4) quadm |= 1u << j;
+    V3 P[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      P[k] = {0.0, 0.0, 0.0};
+      if (k < n) {
+        int q = 0;
+        while (q < nvc - 1 && sV[q][t] != gid[k]) ++q;
+        if (sV[q][t] != gid[k]) ok = false, q = 0;
+        sLV[j][k][t] = (int8_t)q;
+        P[k] = {sX[q][0][t], sX[q][1][t], sX[q][2][t]};
+      }
+    }
+    if (!ok) {
+      atomicOr(m.status, kErrIndex);
+      return;
+    }
+    // the face's geometry from k_face_geom
+    const V3 cf = ld3(m.fc, f);
+    sCF[j][0][t] = cf.x;
+    sCF[j][1][t] = cf.y;
+    sCF[j][2][t] = cf.z;
+    const double4 fn = m.fn[f];
+    const double4 S = m.fS[f];
+    const double sg = left ? 1.0 : -1.0;
+    // check_mesh_elem_volume / _closed / _subface_closed terms of this face (the subface
+    // closure sums the face's own subface sum S, formed in face%sub_face order)
+    const V3 nn = {sg * fn.x, sg * fn.y, sg * fn.z};
+    const V3 an = {fn.w * nn.x, fn.w * nn.y, fn.w * nn.z};
+    vdiv = vdiv + dot(cf, an);
+    nt = {nt.x + an.x, nt.y + an.y, nt.z + an.z};
+    ns = {ns.x + sg * S.x, ns.y + sg * S.y, ns.z + sg * S.z};
+    // compute_elem_centroid: tetrahedra (edge, face centroid, vertex centroid)
+    const V3 fe = sub(cf, ce);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (k < n) {
+        const V3 cp = P[k], cpp = pick4(P, k + 1 == n ? 0 : k + 1);
+        const V3 x = left ? cross(sub(cp, cf), sub(cpp, cf)) : cross(sub(cpp, cf), sub(cp, cf));
+        const double vol = dot(x, fe) / 6.0;
+        cen.x = cen.x + vol * (cp.x + cpp.x + cf.x + ce.x) * 0.25;
+        cen.y = cen.y + vol * (cp.y + cpp.y + cf.y + ce.y) * 0.25;
+        cen.z = cen.z + vol * (cp.z + cpp.z + cf.z + ce.z) * 0.25;
+        sum_vol = sum_vol + vol;
+      }
+  }
+  cen = {cen.x / sum_vol, cen.y / sum_vol, cen.z / sum_vol};
+  // compute_subelem_volume: subcell k is (cell, vertex k); its subfaces in sub_elem order
+  double vcell = 0.0;
+  for (int k = 0; k < nvc; ++k) {
+    const int s = vb + k;
+    const int4 q4 = m.se_sf[s];
+    const int q[4] = {q4.x, q4.y, q4.z, q4.w};
+    double vol = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) {
+      if (q[jj] < 0) break;
+      const int f = m.sf_face[q[jj]], vert = m.sf_vert[q[jj]];
+      int j = 0;
+      while (j < nfc - 1 && sF[j][t] != f) ++j;
+      const int n = 3 + ((quadm >> j) & 1u);
+      int kk = 0;
+      while (kk < n - 1 && sV[sLV[j][kk][t]][t] != vert) ++kk;
+      const int lc = sLV[j][kk][t], lm = sLV[j][kk == 0 ? n - 1 : kk - 1][t], lp = sLV[j][kk + 1 == n ? 0 : kk + 1][t];
+      const V3 cp = {sX[lc][0][t], sX[lc][1][t], sX[lc][2][t]};
+      const V3 cpm = half_sum({sX[lm][0][t], sX[lm][1][t], sX[lm][2][t]}, cp);
+      const V3 cpp = half_sum({sX[lp][0][t], sX[lp][1][t], sX[lp][2][t]}, cp);
+      const V3 cf = {sCF[j][0][t], sCF[j][1][t], sCF[j][2][t]};
+      const V3 fe = sub(cf, cen);
+      const V3 a = sub(cpm, cf), b = sub(cp, cf), cc3 = sub(cpp, cf);
+      V3 x1, x2;
+      if ((leftm >> j) & 1u) {
+        x1 = cross(a, b);
+        x2 = cross(b, cc3);
+      } else {
+        x1 = cross(cc3, b);
+        x2 = cross(b, a);
+      }
+      vol = vol + dot(x1, fe) / 6.0 + dot(x2, fe) / 6.0;
+    }
+    m.vol_se[s] = vol;
+    ok = ok && (vol > 0.0);
+    vcell = vcell + vol;
+  }
+  m.vol[c] = vcell;
+  vdiv = vdiv / 3.0;
+  ok = ok && (fabs(vcell - vdiv) < 1e-14);
+  ok = ok && (fnorm2_3(nt.x, nt.y, nt.z) < 1e-14);
+  ok = ok && (fnorm2_3(ns.x, ns.y, ns.z) < 1e-14);
+  if (!ok) atomicOr(m.status, kErrMeshCheck);
+  if (sol6) {  // lagrange_main.F90:110: new_sol = sol + dt*rhs
+    double* u = sol6 + kRec * (size_t)c;
+    const double* r = rhs6 + kRhs * (size_t)c;
+    bool fin = true;
+    for (int k = 0; k < 5; ++k) {
+      u[k] = u[k] + dt * r[k];
+      fin = fin && isfinite(u[k]);
+    }
+    u[6] = lag_pressure(u[0], u[1], u[2], u[3], u[4]);
+    if (!fin) atomicOr(m.status, kErrNonFinite);
+    if (!(u[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
+  }
+}
+
+}  // namespace geo
+}  // namespace subfv

@@ -20,4 +20,6 @@ int handle_clear_status(DevMesh& d);
 int handle_ensure_scratch(subfv_mesh* m);
 // full geometry when Lagrangian steps left only the step's subset current
 int handle_ensure_full_geometry(DevMesh& d);
+// the Lagrangian step's per-mesh arrays (allocated on the mesh's stream)
+int handle_ensure_lag_arrays(DevMesh& d);
 }  // namespace subfv

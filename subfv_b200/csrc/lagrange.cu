@@ -23,6 +23,7 @@
 
 #include "../../include/subfv.h"
 #include "common.cuh"
+#include "geom_body.cuh"
 #include "lagrange.cuh"
 #include "mesh_dev.cuh"
 
@@ -81,9 +82,7 @@ constexpr int kFrec = 6;
 constexpr int kNodeChunk = 4, kCellChunk = 2;
 
 template <int P>
-__global__ void __launch_bounds__(128) k_lag_face(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc) {
-  if (sc && sc->done) return;
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ inline void lag_face_body(const DevMesh& m, const double* __restrict__ sol6, const int f) {
   if (f >= m.nf) return;
   const int2 lr = m.flr[f];
   const double4 fn = m.fn[f];
@@ -113,11 +112,14 @@ __global__ void __launch_bounds__(128) k_lag_face(DevMesh m, const double* __res
   r[1] = make_double2(vl, vr);
   r[2] = make_double2(xb, kind);
 }
+template <int P>
+__global__ void __launch_bounds__(128) k_lag_face(DevMesh m, const double* __restrict__ sol6, const LagScalars* sc) {
+  if (sc && sc->done) return;
+  lag_face_body<P>(m, sol6, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 template <int P>
-__global__ void __launch_bounds__(128) k_lag_node(DevMesh m, const LagScalars* sc) {
-  if (sc && sc->done) return;
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ inline void lag_node_body(const DevMesh& m, const int v) {
   if (v >= m.nv) return;
   double M00 = 0, M01 = 0, M02 = 0, M10 = 0, M11 = 0, M12 = 0, M20 = 0, M21 = 0, M22 = 0;
   double R0 = 0, R1 = 0, R2 = 0, B0 = 0, B1 = 0, B2 = 0;
@@ -205,19 +207,22 @@ __global__ void __launch_bounds__(128) k_lag_node(DevMesh m, const LagScalars* s
   double v2 = 0.0 + I20 * b0 + I21 * b1 + I22 * b2;
   m.vp[v] = make_double4(v0, v1, v2, 0.0);
 }
+template <int P>
+__global__ void __launch_bounds__(128) k_lag_node(DevMesh m, const LagScalars* sc) {
+  if (sc && sc->done) return;
+  lag_node_body<P>(m, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 __device__ inline double warp_min(double x) {
   for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
   return x;
 }
 
-// mode bit 1: rhs, bit 2: CFL terms
+// mode bit 1: rhs, bit 2: CFL terms; every thread of the block calls (block reduction)
 template <int P>
-__global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* __restrict__ rhs6,
-                           LagScalars* sc, double* dt_slot, int mode) {
+__device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict__ sol6, double* __restrict__ rhs6,
+                                     double* dt_slot, const int mode, const int c) {
   using T = typename Flt<P>::T;
-  if (sc && sc->done) return;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
   double dtloc = 1e6;
   if (c < m.ne) {
     U5 me = ld_u(sol6, c);
@@ -335,9 +340,15 @@ __global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __res
     }
   }
 }
+template <int P>
+__global__ void __launch_bounds__(128) k_lag_cell(DevMesh m, const double* __restrict__ sol6, double* __restrict__ rhs6,
+                                                  LagScalars* sc, double* dt_slot, int mode) {
+  if (sc && sc->done) return;
+  lag_cell_body<P>(m, sol6, rhs6, dt_slot, mode, blockIdx.x * blockDim.x + threadIdx.x);
+}
 
 // dt = cfl*dt; if (t + dt > t_max) dt = t_max - t; t = t + dt (lagrange_main.F90:102-116)
-__global__ void k_lag_finalize(LagScalars* sc) {
+__device__ inline void lag_finalize_body(LagScalars* sc) {
   if (sc->done) {
     sc->skip = 1;
     return;
@@ -351,14 +362,103 @@ __global__ void k_lag_finalize(LagScalars* sc) {
   sc->done = (sc->t < sc->t_max) ? 0 : 1;
   sc->skip = 0;
 }
+__global__ void k_lag_finalize(LagScalars* sc) { lag_finalize_body(sc); }
 
-__global__ void k_lag_move(DevMesh m, const LagScalars* sc, double dt_host) {
-  if (sc && sc->skip) return;
-  int v = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ inline void lag_move_body(const DevMesh& m, const double dt, const int v) {
   if (v >= m.nv) return;
-  double dt = sc ? sc->dt : dt_host;
   double4 x = m.x[v], vp = m.vp[v];
   m.x[v] = make_double4(x.x + dt * vp.x, x.y + dt * vp.y, x.z + dt * vp.z, 0.0);
+}
+__global__ void k_lag_move(DevMesh m, const LagScalars* sc, double dt_host) {
+  if (sc && sc->skip) return;
+  lag_move_body(m, sc ? sc->dt : dt_host, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// ---------------------------------------------------------------------------------
+// Batched step over a table of problems (one mesh, state and scalars each): persistent
+// grids walk the work blocks of all problems, each block finds its problem in the
+// prefix table, so every per-problem result equals the solo run's bit for bit (the only
+// cross-block reduction, the CFL minimum, is exact).
+
+__device__ inline int lag_item_of(const int* __restrict__ wofs, int n, int w) {
+  int lo = 0, hi = n;
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (wofs[mid] <= w) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+template <int P>
+__global__ void __launch_bounds__(kLagFaceBlock) kb_lag_face(const LagItem* __restrict__ it,
+                                                             const int* __restrict__ wf, const int* __restrict__ hdr) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wf[n]; w += gridDim.x) {
+    const int p = lag_item_of(wf, n, w);
+    const LagItem& I = it[p];
+    if (I.sc->done) continue;
+    lag_face_body<P>(I.m, I.sol6, (w - wf[p]) * kLagFaceBlock + threadIdx.x);
+  }
+}
+template <int P>
+__global__ void __launch_bounds__(kLagVertBlock) kb_lag_node(const LagItem* __restrict__ it,
+                                                             const int* __restrict__ wv, const int* __restrict__ hdr) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
+    const int p = lag_item_of(wv, n, w);
+    const LagItem& I = it[p];
+    if (I.sc->done) continue;
+    lag_node_body<P>(I.m, (w - wv[p]) * kLagVertBlock + threadIdx.x);
+  }
+}
+template <int P>
+__global__ void __launch_bounds__(kLagCellBlock) kb_lag_cell(const LagItem* __restrict__ it,
+                                                             const int* __restrict__ wc, const int* __restrict__ hdr) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wc[n]; w += gridDim.x) {
+    const int p = lag_item_of(wc, n, w);
+    const LagItem& I = it[p];
+    if (I.sc->done) continue;
+    lag_cell_body<P>(I.m, I.sol6, I.rhs6, &I.sc->dtmin, 3, (w - wc[p]) * kLagCellBlock + threadIdx.x);
+    __syncthreads();  // the block-reduction scratch is reused by the next work block
+  }
+}
+__global__ void kb_lag_finalize(const LagItem* __restrict__ it, const int* __restrict__ hdr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < hdr[0]) lag_finalize_body(it[p].sc);
+}
+__global__ void __launch_bounds__(kLagVertBlock) kb_lag_move(const LagItem* __restrict__ it,
+                                                             const int* __restrict__ wv, const int* __restrict__ hdr) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
+    const int p = lag_item_of(wv, n, w);
+    const LagItem& I = it[p];
+    if (I.sc->skip) continue;
+    lag_move_body(I.m, I.sc->dt, (w - wv[p]) * kLagVertBlock + threadIdx.x);
+  }
+}
+__global__ void __launch_bounds__(kLagFaceBlock) kb_face_geom(const LagItem* __restrict__ it,
+                                                              const int* __restrict__ wf, const int* __restrict__ hdr) {
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wf[n]; w += gridDim.x) {
+    const int p = lag_item_of(wf, n, w);
+    const LagItem& I = it[p];
+    if (I.sc->skip) continue;
+    geo::face_geom_body<0>(I.m, (w - wf[p]) * kLagFaceBlock + threadIdx.x);
+  }
+}
+__global__ void __launch_bounds__(geo::kGeoBlock) kb_geom_step(const LagItem* __restrict__ it,
+                                                               const int* __restrict__ wc,
+                                                               const int* __restrict__ hdr) {
+  static_assert(geo::kGeoBlock == kLagCellBlock, "cell work blocks");
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wc[n]; w += gridDim.x) {
+    const int p = lag_item_of(wc, n, w);
+    const LagItem& I = it[p];
+    if (I.sc->skip) continue;
+    geo::geom_step_body(I.m, I.sol6, I.rhs6, I.sc->dt, (w - wc[p]) * kLagCellBlock + threadIdx.x);
+  }
 }
 
 // (5, n) host layout <-> [n][6] device records; mass goes to slot 5
@@ -449,6 +549,23 @@ void launch_vp_in(const DevMesh& m, const double* in) { k_vp_in<<<grid_for(m.nv,
 void launch_set_scalar(const DevMesh& m, double* p, double v) { k_set_scalar<<<1, 1, 0, m.stream>>>(p, v); }
 void launch_build_cell_entries(const DevMesh& m) {
   k_build_cell_entries<<<grid_for(m.ncsf, 256), 256, 0, m.stream>>>(m);
+}
+
+void launch_lag_batch_step(const LagTable& t, int precision, cudaStream_t s) {
+  const int g = t.grid, gp = grid_for(t.cap, 128);
+  if (precision == 1) {
+    kb_lag_face<1><<<g, kLagFaceBlock, 0, s>>>(t.items, t.wf, t.hdr);
+    kb_lag_node<1><<<g, kLagVertBlock, 0, s>>>(t.items, t.wv, t.hdr);
+    kb_lag_cell<1><<<g, kLagCellBlock, 0, s>>>(t.items, t.wc, t.hdr);
+  } else {
+    kb_lag_face<0><<<g, kLagFaceBlock, 0, s>>>(t.items, t.wf, t.hdr);
+    kb_lag_node<0><<<g, kLagVertBlock, 0, s>>>(t.items, t.wv, t.hdr);
+    kb_lag_cell<0><<<g, kLagCellBlock, 0, s>>>(t.items, t.wc, t.hdr);
+  }
+  kb_lag_finalize<<<gp, 128, 0, s>>>(t.items, t.hdr);
+  kb_lag_move<<<g, kLagVertBlock, 0, s>>>(t.items, t.wv, t.hdr);
+  kb_face_geom<<<g, kLagFaceBlock, 0, s>>>(t.items, t.wf, t.hdr);
+  kb_geom_step<<<g, geo::kGeoBlock, 0, s>>>(t.items, t.wc, t.hdr);
 }
 
 // One full time step of lagrange_main.F90:89-127 (graph-capturable: no host sync).

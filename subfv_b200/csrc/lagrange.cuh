@@ -25,4 +25,23 @@ void launch_set_scalar(const DevMesh& m, double* p, double v);
 void launch_build_cell_entries(const DevMesh& m);
 void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision);
 
+// One problem of a batch: its mesh (moved by the steps), cell records, residual records
+// and scalars.
+struct LagItem {
+  DevMesh m;
+  double *sol6, *rhs6;
+  LagScalars* sc;
+};
+// Table of in-flight problems: items, work-block prefixes over faces (wf, kLagFaceBlock
+// faces per block), vertices (wv, kLagVertBlock) and cells (wc, kLagCellBlock), and
+// hdr[0] = the number of problems; persistent grids of `grid` blocks.
+constexpr int kLagFaceBlock = 128, kLagVertBlock = 128, kLagCellBlock = 64;
+struct LagTable {
+  LagItem* items = nullptr;
+  int *wf = nullptr, *wv = nullptr, *wc = nullptr, *hdr = nullptr;
+  int cap = 0, grid = 1;
+};
+// One step of lagrange_main.F90:89-127 for every problem of the table, in shared launches.
+void launch_lag_batch_step(const LagTable& t, int precision, cudaStream_t s);
+
 }  // namespace subfv

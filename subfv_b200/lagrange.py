@@ -170,3 +170,95 @@ class LagrangeState:
             self.close()
         except Exception:
             pass
+
+
+SUBFV_BATCH_FULL = -3
+
+
+class LagBatch:
+    """Many independent Lagrangian problems advanced together in shared launches (no
+    counterpart in the reference, which runs one mesh per process). Each problem owns
+    its mesh, which its steps move; each result is bit-identical to the same problem
+    run alone through LagrangeState."""
+
+    def __init__(self, capacity: int, budget_bytes: int, precision: int = PLAIN_FP64):
+        h = C.c_void_p()
+        check(_lib.load().subfv_lag_batch_create(int(precision), int(capacity), int(budget_bytes), C.byref(h)),
+              "subfv_lag_batch_create")
+        self._h = h
+        self._meshes = {}
+
+    def state_bytes(self, mesh: Mesh) -> int:
+        return int(_lib.load().subfv_lag_batch_state_bytes(self._h, mesh._h))
+
+    def free_bytes(self) -> int:
+        return int(_lib.load().subfv_lag_batch_free_bytes(self._h))
+
+    def size(self):
+        n, used = C.c_int(), C.c_int64()
+        check(_lib.load().subfv_lag_batch_size(self._h, C.byref(n), C.byref(used)), "subfv_lag_batch_size")
+        return n.value, used.value
+
+    def add(self, mesh: Mesh, sol, t_max: float, cfl: float = 0.8, mass=None, t0: float = 0.0,
+            take_mesh: bool = False):
+        """Admit a problem; returns its slot, or None when the batch is full."""
+        sol = f64(sol)
+        if mass is None:  # lagrange_main.F90:81-85: mass = volume / tau
+            mass = mesh.geometry("elem_volume") / sol[:, 0]
+        mass = f64(mass)
+        slot = C.c_int(-1)
+        rc = _lib.load().subfv_lag_batch_add(self._h, mesh._h, int(take_mesh), pd(sol), pd(mass), float(cfl),
+                                             float(t0), float(t_max), C.byref(slot))
+        if rc == SUBFV_BATCH_FULL:
+            return None
+        check(rc, "subfv_lag_batch_add")
+        if take_mesh:
+            mesh._h = None
+        else:
+            self._meshes[slot.value] = mesh
+        return slot.value
+
+    def remove(self, slot: int):
+        check(_lib.load().subfv_lag_batch_remove(self._h, int(slot)), "subfv_lag_batch_remove")
+        self._meshes.pop(slot, None)
+
+    def advance(self, n_steps: int):
+        check(_lib.load().subfv_lag_batch_advance(self._h, int(n_steps)), "subfv_lag_batch_advance")
+
+    def time_steps(self, n_steps: int) -> float:
+        ms = C.c_double()
+        check(_lib.load().subfv_lag_batch_time_steps(self._h, int(n_steps), C.byref(ms)), "subfv_lag_batch_time_steps")
+        return ms.value
+
+    def poll(self, wait: bool = True) -> bool:
+        return check(_lib.load().subfv_lag_batch_poll(self._h, int(wait)), "subfv_lag_batch_poll") == 0
+
+    def sync(self):
+        check(_lib.load().subfv_lag_batch_sync(self._h), "subfv_lag_batch_sync")
+
+    def info(self, slot: int):
+        """(t, steps, done, status bits) from the latest snapshot taken."""
+        t, steps, done, st = C.c_double(), C.c_int64(), C.c_int(), C.c_uint()
+        check(_lib.load().subfv_lag_batch_slot_info(self._h, int(slot), C.byref(t), C.byref(steps), C.byref(done),
+                                                    C.byref(st)), "subfv_lag_batch_slot_info")
+        return t.value, steps.value, bool(done.value), st.value
+
+    def sol(self, slot: int, n_elems: int) -> np.ndarray:
+        out = np.empty((n_elems, 5))
+        check(_lib.load().subfv_lag_batch_get_sol(self._h, int(slot), pd(out)), "subfv_lag_batch_get_sol")
+        return out
+
+    def set_grid(self, grid: int):
+        check(_lib.load().subfv_lag_batch_set_grid(self._h, int(grid)), "subfv_lag_batch_set_grid")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().subfv_lag_batch_destroy(self._h)
+            self._h = None
+            self._meshes.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
