@@ -49,10 +49,15 @@ def _args():
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--n", type=int, default=N_SIDE)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", default="lagrange", choices=["lagrange", "gresho", "implicit", "shocktubes"])
+    p.add_argument("--workload", default="lagrange",
+                   choices=["lagrange", "gresho", "implicit", "shocktubes", "serve"])
     p.add_argument("--problems", type=int, default=1024)
     p.add_argument("--nmax", type=int, default=20000)
     p.add_argument("--solo-sample", type=int, default=64)
+    p.add_argument("--requests", type=int, default=200)
+    p.add_argument("--rate", type=float, default=20.0)
+    p.add_argument("--max-cells", type=int, default=1 << 18)
+    p.add_argument("--time-scale", type=float, default=0.05)
     return p.parse_args()
 
 
@@ -249,7 +254,7 @@ def run_gresho(args, rank, world, local):
         torch.cuda.synchronize()
         ms = _time_device(stream, lambda: s2.advance_async(200))
         st, steps, t = s2.sync()
-        out[prec_name] = {"ms": ms, "steps": steps, "status": st, "sol": s2.sol()}
+        out[prec_name] = {"ms": ms, "steps": steps, "status": st, "sol": s2.sol(), "t": t}
     a, b = out["fp64"]["sol"], out["mixed"]["sol"]
     scale = np.abs(a).sum(0)
     l1 = {k: float(np.abs(a[:, i] - b[:, i]).sum() / max(scale[i], 1e-6 * scale[1:4].max()))
@@ -271,6 +276,7 @@ def run_gresho(args, rank, world, local):
            "mixed_value": cells * 200 / (out["mixed"]["ms"] / 1e3),
            "ms_per_iteration": out["fp64"]["ms"] / 200, "cells": cells, "iterations": 200,
            "mixed_l1_rel_vs_fp64": l1, "status": [out["fp64"]["status"], out["mixed"]["status"]],
+           "sim_time_after_200": out["fp64"]["t"],
            "dtype": "f64", "cpu_baseline": cpu}
     print(json.dumps(res), flush=True)
 
@@ -469,6 +475,49 @@ def run_shocktubes(args, rank, world, local):
     print(json.dumps(res), flush=True)
 
 
+def run_serve(args, rank, world, local):
+    """Serving: `--requests` solve requests (Gresho vortex or 2-D Sedov, triangles or
+    quadrilaterals, cells log-uniform in [4096, --max-cells], end time uniform in
+    [0.1, 1] x nominal x --time-scale) on a seeded Poisson stream of `--rate` requests per
+    second, served by subfv_b200.serve.Server under a 150 GB budget, in plain FP64 and in
+    mixed precision. Latency = arrival to result on the host. Baseline: a sample of the
+    same requests solved one at a time on the plain FP64 solo path."""
+    import torch
+    from subfv_b200 import serve
+    reqs = serve.make_requests(args.requests, rate=args.rate, seed=SEED, cells_max=args.max_cells,
+                               time_scale=args.time_scale)
+    res = {"metric": "cell-updates/s", "workload": f"serve_{args.requests}_requests", "requests": args.requests,
+           "rate_per_s": args.rate, "cells_max": args.max_cells, "time_scale": args.time_scale,
+           "budget_bytes": int(150e9)}
+    for name, prec in (("fp64", 0), ("mixed", 1)):
+        srv = serve.Server(budget_bytes=int(150e9), capacity=max(64, args.requests), precision=prec, chunk=8,
+                           build_threads=max(1, min(16, (os.cpu_count() or 2) - 2)), keep_solutions=False)
+        sampler = ClockSampler(local)
+        sampler.start()
+        results, makespan = srv.run(reqs)
+        clocks = sampler.stop()
+        srv.close()
+        torch.cuda.synchronize()
+        cu = sum(r.n_cells * r.steps for r in results)
+        res[name] = {"value": cu / makespan, "makespan_s": makespan, "cell_updates": cu,
+                     "completed": len(results), "failed": sum(1 for r in results if r.status),
+                     "latency": serve.latency_stats(results), "clocks": clocks,
+                     "steps_mean": float(np.mean([r.steps for r in results])) if results else 0.0}
+    # one request at a time on the plain FP64 path, over a sample of the stream
+    idx = np.random.default_rng(SEED + 2).choice(len(reqs), size=min(args.solo_sample, len(reqs)), replace=False)
+    t0 = time.perf_counter()
+    cu = 0
+    for i in idx:
+        steps, t, st, _ = serve.solve_alone(reqs[i], precision=0)
+        cu += reqs[i].n_cells * steps
+    el = time.perf_counter() - t0
+    res["one_by_one_fp64"] = {"value": cu / el, "requests": len(idx), "seconds": el,
+                              "note": "each request built and solved alone on the solo path, sequentially"}
+    res["value"] = res["mixed"]["value"]
+    res["unit"] = "cell-updates/s"
+    print(json.dumps(res), flush=True)
+
+
 def _libmod():
     from subfv_b200 import _lib
     return _lib
@@ -480,8 +529,8 @@ def main():
     if args.workload != "lagrange":
         import torch
         torch.cuda.set_device(local)
-        {"gresho": run_gresho, "implicit": run_implicit,
-         "shocktubes": run_shocktubes}[args.workload](args, rank, world, local)
+        {"gresho": run_gresho, "implicit": run_implicit, "shocktubes": run_shocktubes,
+         "serve": run_serve}[args.workload](args, rank, world, local)
         return
     import torch
     import torch.distributed as dist
