@@ -11,6 +11,8 @@ def test_request_stream_is_seeded():
     assert np.all(gaps > 0)
     cells = np.array([r.n_cells for r in a])
     assert cells.min() >= 4096 * 0.9 and cells.max() <= (1 << 20) * 1.1
+    assert all(r.tri for r in a if r.kind == "sedov")
+    assert {r.tri for r in a if r.kind == "gresho"} == {True, False}
     for r in a:
         nominal = serve.GRESHO_T_NOMINAL if r.kind == "gresho" else serve.SEDOV_T_NOMINAL
         assert 0.1 * nominal <= r.t_end <= nominal
