@@ -163,7 +163,9 @@ typedef struct subfv_ns_cfg {
   int32_t bc_type[16];        /* per tag: 1 wall, 3 freestream, 4 outflow supersonic */
   double bc_val[16][5];       /* per tag: primitive (rho, u, v, w, p) */
   double cfl, tmax;
-  int32_t precision;          /* 0 plain FP64, 1 FP32 flux/reconstruction/limiter arithmetic */
+  int32_t precision;          /* 0 plain FP64; 1 FP32 wave-speed bounds of the nodal solver;
+                                 2 also FP32 flux, reconstruction and limiter arithmetic
+                                 (nodal 3x3 systems and all sums FP64 in both) */
 } subfv_ns_cfg;
 
 /* compute_rhs_ns (ns_main.F90:130-179, no diffusion): one residual evaluation.

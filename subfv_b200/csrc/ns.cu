@@ -22,8 +22,10 @@
 // Plain FP64 (precision 0) follows the reference's evaluation order and is compiled
 // without FMA contraction, so it reproduces the CPU restatement bit for bit, except the
 // residual norms (res, res_vect), which are summed by a fixed tree of block partials.
-// Precision 1 evaluates reconstruction, limiters and subface fluxes in FP32; the nodal
-// velocity solver, the nodal gradient system and all sums stay FP64.
+// Precision 1 evaluates the nodal solver's wave-speed bounds (lambda, vbar) in FP32;
+// precision 2 also the reconstruction, the limiters and the subface fluxes. In both the
+// nodal 3x3 systems (M, R and the solve), the nodal gradient system and all sums stay
+// FP64.
 #include <algorithm>
 #include <cstring>
 
@@ -461,7 +463,16 @@ __device__ void nodal_solve(const NsParams& P, double mat[3][3], const double* R
 // expressions of the same states in every iteration).
 constexpr int kNodeThreads = 256;  // the largest block of the node kernel
 
-template <class T, int MS>
+// vbar = (lambda_l v_l + lambda_r v_r - (p_r - p_l)) / (lambda_r + lambda_l) (:309,316),
+// always in FP64 from the normal velocities and pressures the flux itself uses: with
+// FP32 wave speeds the node's momentum balance sum A (p*_r - p*_l) n =
+// sum A (lambda_l + lambda_r)(v* - vbar) n, which the FP64 solve of M v* = R closes,
+// then holds to FP64 rounding (with an FP64 flux), so the totals stay conserved.
+__device__ inline double vbar_of(double lam_l, double lam_r, double vnl, double vnr, double pl, double pr) {
+  return (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+}
+
+template <class T, class L, int MS>
 __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
                                const double* __restrict__ grad, double* __restrict__ fs, int so, const int v) {
   if (v >= m.nv) return;
@@ -475,7 +486,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
   // reconstruction already runs in T, so storing T loses nothing.
   T wlr[MS][10];
   double geo[MS][4];  // subface normal and area
-  T lam[MS][3];       // lambda_l, lambda_r, vbar
+  double lam[MS][3];  // lambda_l, lambda_r (values of the wave-speed precision L), vbar
   int sfj[MS], yj[MS];
   for (int j = 0; j < nsfn; ++j) {
     const int sf = m.vsf[p0 + j];
@@ -490,19 +501,19 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     geo[j][1] = sn.y;
     geo[j][2] = sn.z;
     geo[j][3] = sn.w;
-    lam[j][0] = lam[j][1] = lam[j][2] = (T)0;
+    lam[j][0] = lam[j][1] = lam[j][2] = 0.0;
   }
   const bool excl = m.is_bound[v] && P.excl;
   double vn3[3] = {0.0, 0.0, 0.0};
   if (P.scheme == 1) {
     if (!excl) {  // compute_lambdas_and_solve_nodal_velocity (ns_euler_rs_module.F90:288-422)
-      // wave-speed bounds and vbar in T; M, R and the 3x3 solve in FP64
-      T snd[MS][2];  // left / right sound speeds
+      // wave-speed bounds and vbar in L; M, R and the 3x3 solve in FP64
+      L snd[MS][2];  // left / right sound speeds
       double Bp[3] = {0.0, 0.0, 0.0};  // wall_normal (ns_euler_primitives_module.F90:162-190)
       for (int j = 0; j < nsfn; ++j) {
         const double* n = geo[j];
-        snd[j][0] = sqrt((T)G * wlr[j][4] / wlr[j][0]);
-        snd[j][1] = sqrt((T)G * wlr[j][9] / wlr[j][5]);
+        snd[j][0] = sqrt((L)G * (L)wlr[j][4] / (L)wlr[j][0]);
+        snd[j][1] = sqrt((L)G * (L)wlr[j][9] / (L)wlr[j][5]);
         const int y = yj[j];
         if (y < 0 && !(P.b2d && fabs(n[2]) > 1e-12) && (y == -1 || P.bc_type[-(y + 1) - 1] == 1))
           for (int d = 0; d < 3; ++d) Bp[d] = Bp[d] + n[3] * n[d];
@@ -512,29 +523,37 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
         for (int j = 0; j < nsfn; ++j) {
           const double* n = geo[j];
           const double area = n[3];
-          const T nt[3] = {(T)n[0], (T)n[1], (T)n[2]};
-          const T* wl = wlr[j];
-          const T* wr = wlr[j] + 5;
-          const T rhol = wl[0], vnl = dotT(wl + 1, nt), pl = wl[4], al = snd[j][0];
-          const T rhor = wr[0], vnr = dotT(wr + 1, nt), pr = wr[4], ar = snd[j][1];
-          T lam_l = lam[j][0], lam_r = lam[j][1], vbar = lam[j][2];
+          const L nt[3] = {(L)n[0], (L)n[1], (L)n[2]};
+          L wl[5], wr[5];
+          for (int k = 0; k < 5; ++k) {
+            wl[k] = (L)wlr[j][k];
+            wr[k] = (L)wlr[j][5 + k];
+          }
+          const L rhol = wl[0], vnl = dotT(wl + 1, nt), pl = wl[4], al = snd[j][0];
+          const L rhor = wr[0], vnr = dotT(wr + 1, nt), pr = wr[4], ar = snd[j][1];
+          L lam_l = (L)lam[j][0], lam_r = (L)lam[j][1];
+          double vbar = lam[j][2];
+          // the flux's own normal velocities and pressures (precision T), for vbar
+          const T ntT[3] = {(T)n[0], (T)n[1], (T)n[2]};
+          const double vnl_f = (double)dotT(wlr[j] + 1, ntT), vnr_f = (double)dotT(wlr[j] + 6, ntT);
+          const double pl_f = (double)wlr[j][4], pr_f = (double)wlr[j][9];
           const bool wall = is_wall(P, yj[j]);
-          const T c1 = (T)1, c15 = (T)1.5, c0 = (T)0;
+          const L c1 = (L)1, c15 = (L)1.5, c0 = (L)0;
           if (iter == 1) {
             lam_l = tmax2(tmax2(tmax2(lam_l, al * rhol), sqrt(rhol * tmax2(c0, pr - pl))), -rhol * (vnr - vnl));
             lam_r = tmax2(tmax2(tmax2(lam_r, ar * rhor), sqrt(rhor * tmax2(c0, pl - pr))), -rhor * (vnr - vnl));
-            vbar = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
-            lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -(vbar - vnl) / al)));
-            lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, (vbar - vnr) / ar)));
+            vbar = vbar_of((double)lam_l, (double)lam_r, vnl_f, vnr_f, pl_f, pr_f);
+            lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -((L)vbar - vnl) / al)));
+            lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, ((L)vbar - vnr) / ar)));
           } else if (wall && P.bc_style == 1) {
-            lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -(vbar - vnl) / al)));
-            lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, (vbar - vnr) / ar)));
+            lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -((L)vbar - vnl) / al)));
+            lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, ((L)vbar - vnr) / ar)));
           } else {
-            const T v_et = (T)dotT(vn3, n);
+            const L v_et = (L)dotT(vn3, n);
             lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -(v_et - vnl) / al)));
             lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, (v_et - vnr) / ar)));
           }
-          vbar = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+          vbar = vbar_of((double)lam_l, (double)lam_r, vnl_f, vnr_f, pl_f, pr_f);
           lam[j][0] = lam_l;
           lam[j][1] = lam_r;
           lam[j][2] = vbar;
@@ -549,7 +568,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
             M6[5] = M6[5] + w * (n[2] * n[2]);
           }
           if (!wall || P.bc_style == 0) {
-            const double q = area * lsum * (double)vbar;
+            const double q = area * lsum * vbar;
             for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
           } else if (P.bc_style == 2 && (!P.b2d || fabs(n[2]) < 1e-8)) {
             const double q = area * (double)pl;
@@ -603,12 +622,12 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
   }
 }
 
-template <class T, int MS>
+template <class T, class L, int MS>
 __global__ void __launch_bounds__(kNodeThreads) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
                                                           const double* __restrict__ grad, double* __restrict__ fs,
                                                           int so, const NsScalars* sc) {
   if (sc && sc->done) return;
-  ns_node_vertex<T, MS>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x);
+  ns_node_vertex<T, L, MS>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __device__ inline double warp_min(double x) {
@@ -981,7 +1000,7 @@ __device__ inline int item_of(const int* __restrict__ wofs, int n, int w) {
 }
 
 // which: the state the phase reads (0: U0, 1: U1)
-template <class T, int MS>
+template <class T, class L, int MS>
 __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restrict__ it, const int* __restrict__ wv,
                                                            const int* __restrict__ hdr, NsParams P, int which,
                                                            int so) {
@@ -990,7 +1009,7 @@ __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restr
     const int p = item_of(wv, n, w);
     const NsItem& I = it[p];
     if (I.sc->done) continue;
-    ns_node_vertex<T, MS>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * blockDim.x + threadIdx.x);
+    ns_node_vertex<T, L, MS>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * blockDim.x + threadIdx.x);
   }
 }
 __global__ void __launch_bounds__(128) kb_ns_gather(const NsItem* __restrict__ it, const int* __restrict__ wc,
@@ -1220,26 +1239,30 @@ __global__ void k_ns_pack(int n, const double* __restrict__ s5, double* __restri
 
 int ns_partial_blocks(const DevMesh& m) { return grid_for(m.ne, kTdBlock); }
 
-template <class T>
-void launch_kb_node(const NsTable& t, const NsParams& P, cudaStream_t s, int which, int so) {
+template <class T, class L>
+void launch_kb_node_tl(const NsTable& t, const NsParams& P, cudaStream_t s, int which, int so) {
   const int gv = t.grid_v, bv = t.block_v;
-  if (t.group == 8) kb_ns_node<T, 8><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
-  else if (t.group == 16) kb_ns_node<T, 16><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
-  else kb_ns_node<T, 32><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  if (t.group == 8) kb_ns_node<T, L, 8><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  else if (t.group == 16) kb_ns_node<T, L, 16><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  else kb_ns_node<T, L, 32><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+}
+// precision 0: FP64 throughout; 1: FP32 wave-speed bounds; 2: FP32 wave speeds, flux and
+// reconstruction
+void launch_kb_node(const NsTable& t, const NsParams& P, cudaStream_t s, int which, int so) {
+  if (P.precision == 2) launch_kb_node_tl<float, float>(t, P, s, which, so);
+  else if (P.precision == 1) launch_kb_node_tl<double, float>(t, P, s, which, so);
+  else launch_kb_node_tl<double, double>(t, P, s, which, so);
 }
 
 void launch_ns_batch_step(const NsTable& t, const NsParams& P, cudaStream_t s) {
   const int gv = t.grid_v, gc = t.grid_c, nb = t.block_v, gp = grid_for(t.cap, 128);
-  auto node = [&](int which, int so) {
-    if (P.precision == 1) launch_kb_node<float>(t, P, s, which, so);
-    else launch_kb_node<double>(t, P, s, which, so);
-  };
+  auto node = [&](int which, int so) { launch_kb_node(t, P, s, which, so); };
   auto rhs = [&](int which) {
     node(which, 0);
     kb_ns_gather<<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, 0);
     if (P.second_order) {
       kb_ns_nodal_grad<<<gv, nb, 0, s>>>(t.items, t.wv, t.hdr, which);
-      if (P.precision == 1) kb_ns_cell_grad<float><<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, P, which);
+      if (P.precision == 2) kb_ns_cell_grad<float><<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, P, which);
       else kb_ns_cell_grad<double><<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, P, which);
       node(which, 1);
       kb_ns_gather<<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, 1);
@@ -1287,30 +1310,34 @@ int ns_node_lanes(const DevMesh& m) {
   return k <= 8 ? 8 : k <= 16 ? 16 : k <= 32 ? 32 : 0;
 }
 
-template <class T>
-void launch_node(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs, int so,
-                 const NsScalars* sc) {
+template <class T, class L>
+void launch_node_tl(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs, int so,
+                    const NsScalars* sc) {
   const int ms = std::max(8, ns_node_lanes(m));  // a mesh beyond 32 is flagged by the kernel
   const int grid = grid_for(m.nv, 128);
-  if (ms == 8) k_ns_node<T, 8><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
-  else if (ms == 16) k_ns_node<T, 16><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
-  else k_ns_node<T, 32><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  if (ms == 8) k_ns_node<T, L, 8><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  else if (ms == 16) k_ns_node<T, L, 16><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  else k_ns_node<T, L, 32><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+}
+void launch_node(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs, int so,
+                 const NsScalars* sc) {
+  if (P.precision == 2) launch_node_tl<float, float>(m, P, U, grad, fs, so, sc);
+  else if (P.precision == 1) launch_node_tl<double, float>(m, P, U, grad, fs, so, sc);
+  else launch_node_tl<double, double>(m, P, U, grad, fs, so, sc);
 }
 
 void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double* fs, double* rhs1, double* rhs2,
                    double* ngrad, double* grad, NsScalars* sc) {
   const int gv = grid_for(m.nv, 128), gc = grid_for(m.ne, 128);
-  if (P.precision == 1) launch_node<float>(m, P, U, grad, fs, 0, sc);
-  else launch_node<double>(m, P, U, grad, fs, 0, sc);
+  launch_node(m, P, U, grad, fs, 0, sc);
   k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs1, sc, sc ? 1 : 0);
   if (P.second_order) {
     k_ns_nodal_grad<<<gv, 128, 0, m.stream>>>(m, U, ngrad, sc);
-    if (P.precision == 1)
+    if (P.precision == 2)
       k_ns_cell_grad<float><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
     else
       k_ns_cell_grad<double><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
-    if (P.precision == 1) launch_node<float>(m, P, U, grad, fs, 1, sc);
-    else launch_node<double>(m, P, U, grad, fs, 1, sc);
+    launch_node(m, P, U, grad, fs, 1, sc);
     k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs2, sc, 0);
   }
 }

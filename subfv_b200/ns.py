@@ -50,7 +50,7 @@ class NsConfig:
     tmax: float = 1e30
     bc_type: list = field(default_factory=list)  # per tag
     bc_val: list = field(default_factory=list)   # per tag, primitive (rho, u, v, w, p)
-    precision: int = 0  # 0 plain FP64, 1 FP32 flux / reconstruction / limiters
+    precision: int = 0  # 0 plain FP64, 1 FP32 wave-speed bounds, 2 also FP32 flux / reconstruction / limiters
 
     def to_c(self) -> NsCfgC:
         c = NsCfgC()
