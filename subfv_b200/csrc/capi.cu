@@ -227,6 +227,7 @@ int subfv_mesh_destroy(subfv_mesh* m) {
   void* scratch[] = {m->stage, m->sol6, m->rhs6, m->mass, m->sc};
   for (void* p : scratch)
     if (p) cudaFree(p);
+  if (m->imp_pattern && m->imp_pattern_free) m->imp_pattern_free(m->imp_pattern);
   devmesh_free(&m->d);
   delete m;
   return 0;

@@ -12,6 +12,9 @@ struct subfv_mesh {
   double* rhs6 = nullptr;   // [ne][kRhs]
   double* mass = nullptr;   // [ne]
   subfv::LagScalars* sc = nullptr;
+  // the backward-Euler Jacobian's host pattern, built on first use and kept with the mesh
+  void* imp_pattern = nullptr;
+  void (*imp_pattern_free)(void*) = nullptr;
 };
 
 namespace subfv {

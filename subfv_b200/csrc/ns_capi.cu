@@ -255,65 +255,99 @@ int up(T** d, const std::vector<T>& h, cudaStream_t s) {
   return 0;
 }
 
+// The Jacobian's pattern on one mesh (host arrays), built once and kept with the mesh.
+struct ImplicitPattern {
+  std::vector<int> jq_off, jq, jblk, row_off, dblk;
+  std::vector<int> row1, col1;  // 1-based (bcsr_matrix_type)
+};
+
+int build_pattern(DevMesh& d, ImplicitPattern& P) {
+  std::vector<int2> flr(d.nf), sse(d.nsf);
+  std::vector<int> sff(d.nsf), sfv(d.nsf), sev(d.nse);
+  SUBFV_CUDA(cudaMemcpyAsync(flr.data(), d.flr, d.nf * sizeof(int2), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(sse.data(), d.sf_se, d.nsf * sizeof(int2), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(sff.data(), d.sf_face, d.nsf * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(sfv.data(), d.sf_vert, d.nsf * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(sev.data(), d.se_vert, d.nse * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  const int ne = d.ne;
+  std::vector<int>& jq_off = P.jq_off;
+  jq_off.assign(ne + 1, 0);
+  auto owns_right = [&](int sf) { return sse[sf].y >= 0 && sev[sse[sf].y] == sfv[sf]; };
+  for (int sf = 0; sf < d.nsf; ++sf) {
+    const int2 lr = flr[sff[sf]];
+    jq_off[lr.x + 1]++;
+    if (lr.y >= 0 && owns_right(sf)) jq_off[lr.y + 1]++;
+  }
+  for (int i = 0; i < ne; ++i) jq_off[i + 1] += jq_off[i];
+  std::vector<int>& jq = P.jq;
+  jq.assign(jq_off[ne], 0);
+  std::vector<int> other(jq_off[ne]);
+  {
+    std::vector<int> fill(jq_off.begin(), jq_off.end() - 1);
+    for (int sf = 0; sf < d.nsf; ++sf) {
+      const int2 lr = flr[sff[sf]];
+      other[fill[lr.x]] = lr.y;
+      jq[fill[lr.x]++] = 2 * sf;
+      if (lr.y >= 0 && owns_right(sf)) {
+        other[fill[lr.y]] = lr.x;
+        jq[fill[lr.y]++] = 2 * sf + 1;
+      }
+    }
+  }
+  std::vector<int>& row_off = P.row_off;
+  std::vector<int> col;
+  row_off.assign(ne + 1, 0);
+  P.dblk.assign(ne, 0);
+  P.jblk.assign(jq.size(), -1);
+  std::vector<int> cs;
+  for (int i = 0; i < ne; ++i) {
+    cs.assign(1, i);
+    for (int q = jq_off[i]; q < jq_off[i + 1]; ++q)
+      if (other[q] >= 0) cs.push_back(other[q]);
+    std::sort(cs.begin(), cs.end());
+    cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
+    for (int q = jq_off[i]; q < jq_off[i + 1]; ++q)
+      if (other[q] >= 0) P.jblk[q] = row_off[i] + (int)(std::lower_bound(cs.begin(), cs.end(), other[q]) - cs.begin());
+    P.dblk[i] = row_off[i] + (int)(std::lower_bound(cs.begin(), cs.end(), i) - cs.begin());
+    col.insert(col.end(), cs.begin(), cs.end());
+    row_off[i + 1] = (int)col.size();
+  }
+  P.row1.resize(ne + 1);
+  P.col1.resize(col.size());
+  for (int i = 0; i <= ne; ++i) P.row1[i] = row_off[i] + 1;
+  for (size_t j = 0; j < col.size(); ++j) P.col1[j] = col[j] + 1;
+  return 0;
+}
+
+void free_pattern(void* p) { delete static_cast<ImplicitPattern*>(p); }
+
 // Pattern: row i holds i and the other cells of its subfaces, ascending. A cell's
 // subfaces are those of elem%sub_face: every subface it is left of, and those it is right
-// of through its own subcell at the subface's vertex (not a periodic image's).
+// of through its own subcell at the subface's vertex (not a periodic image's). The
+// host pattern is cached on the mesh; each state uploads its own copy.
 int implicit_setup(subfv_ns_state* s, int krylov) {
   if (s->imp && s->imp->krylov == krylov) return 0;
   DevMesh& d = s->m->d;
   if (!s->imp) {
+    if (!s->m->imp_pattern) {
+      auto* P = new ImplicitPattern();
+      if (build_pattern(d, *P)) {
+        delete P;
+        return -1;
+      }
+      s->m->imp_pattern = P;
+      s->m->imp_pattern_free = free_pattern;
+    }
+    const ImplicitPattern& P = *static_cast<const ImplicitPattern*>(s->m->imp_pattern);
     auto* c = new ImplicitCtx();
     s->imp = c;
-    std::vector<int2> flr(d.nf), sse(d.nsf);
-    std::vector<int> sff(d.nsf), sfv(d.nsf), sev(d.nse);
-    SUBFV_CUDA(cudaMemcpyAsync(flr.data(), d.flr, d.nf * sizeof(int2), cudaMemcpyDeviceToHost, d.stream));
-    SUBFV_CUDA(cudaMemcpyAsync(sse.data(), d.sf_se, d.nsf * sizeof(int2), cudaMemcpyDeviceToHost, d.stream));
-    SUBFV_CUDA(cudaMemcpyAsync(sff.data(), d.sf_face, d.nsf * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
-    SUBFV_CUDA(cudaMemcpyAsync(sfv.data(), d.sf_vert, d.nsf * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
-    SUBFV_CUDA(cudaMemcpyAsync(sev.data(), d.se_vert, d.nse * sizeof(int), cudaMemcpyDeviceToHost, d.stream));
-    SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+    c->row1 = P.row1;
+    c->col1 = P.col1;
     const int ne = d.ne;
-    std::vector<int> jq_off(ne + 1, 0);
-    auto owns_right = [&](int sf) { return sse[sf].y >= 0 && sev[sse[sf].y] == sfv[sf]; };
-    for (int sf = 0; sf < d.nsf; ++sf) {
-      const int2 lr = flr[sff[sf]];
-      jq_off[lr.x + 1]++;
-      if (lr.y >= 0 && owns_right(sf)) jq_off[lr.y + 1]++;
-    }
-    for (int i = 0; i < ne; ++i) jq_off[i + 1] += jq_off[i];
-    std::vector<int> jq(jq_off[ne]), other(jq_off[ne]);
-    {
-      std::vector<int> fill(jq_off.begin(), jq_off.end() - 1);
-      for (int sf = 0; sf < d.nsf; ++sf) {
-        const int2 lr = flr[sff[sf]];
-        other[fill[lr.x]] = lr.y;
-        jq[fill[lr.x]++] = 2 * sf;
-        if (lr.y >= 0 && owns_right(sf)) {
-          other[fill[lr.y]] = lr.x;
-          jq[fill[lr.y]++] = 2 * sf + 1;
-        }
-      }
-    }
-    std::vector<int> row_off(ne + 1, 0), col, dblk(ne), jblk(jq.size(), -1);
-    for (int i = 0; i < ne; ++i) {
-      std::vector<int> cs{i};
-      for (int q = jq_off[i]; q < jq_off[i + 1]; ++q)
-        if (other[q] >= 0) cs.push_back(other[q]);
-      std::sort(cs.begin(), cs.end());
-      cs.erase(std::unique(cs.begin(), cs.end()), cs.end());
-      for (int q = jq_off[i]; q < jq_off[i + 1]; ++q)
-        if (other[q] >= 0) jblk[q] = row_off[i] + (int)(std::lower_bound(cs.begin(), cs.end(), other[q]) - cs.begin());
-      dblk[i] = row_off[i] + (int)(std::lower_bound(cs.begin(), cs.end(), i) - cs.begin());
-      col.insert(col.end(), cs.begin(), cs.end());
-      row_off[i + 1] = (int)col.size();
-    }
-    c->row1.resize(ne + 1);
-    c->col1.resize(col.size());
-    for (int i = 0; i <= ne; ++i) c->row1[i] = row_off[i] + 1;
-    for (size_t j = 0; j < col.size(); ++j) c->col1[j] = col[j] + 1;
     if (bcsr_upload(&c->A, ne, 5, c->row1.data(), c->col1.data(), nullptr, d.stream)) return -1;
-    if (up(&c->jq_off, jq_off, d.stream) || up(&c->jq, jq, d.stream) || up(&c->jblk, jblk, d.stream) ||
-        up(&c->row_off, row_off, d.stream) || up(&c->dblk, dblk, d.stream))
+    if (up(&c->jq_off, P.jq_off, d.stream) || up(&c->jq, P.jq, d.stream) || up(&c->jblk, P.jblk, d.stream) ||
+        up(&c->row_off, P.row_off, d.stream) || up(&c->dblk, P.dblk, d.stream))
       return -1;
     SUBFV_CUDA(cudaMalloc(&c->b, 5 * (size_t)ne * sizeof(double)));
     SUBFV_CUDA(cudaMalloc(&c->x, 5 * (size_t)ne * sizeof(double)));
