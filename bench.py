@@ -320,14 +320,18 @@ def run_implicit(args, rank, world, local):
         stats["device_ms"] = dev_ms
         stats["wall_ms_first_step"] = el * 1e3
         stats["wall_ms_next_step"] = el2 * 1e3
+        dev2 = stats2["ms_assemble"] + stats2["ms_solve"] + stats2["ms_update"]
         stats["next_step"] = {"status": st2, "restarts": stats2["restarts"], "conv": stats2["conv"],
-                              "device_ms": stats2["ms_assemble"] + stats2["ms_solve"] + stats2["ms_update"]}
+                              "outer": stats2["outer"], "ms_assemble": stats2["ms_assemble"],
+                              "ms_solve": stats2["ms_solve"], "device_ms": dev2}
         stats["status"] = st
-        stats["cell_updates_per_s"] = mesh.n_elems / (dev_ms * 1e-3)
+        stats["cell_updates_per_s_first_step"] = mesh.n_elems / (dev_ms * 1e-3)
+        stats["cell_updates_per_s"] = mesh.n_elems / (dev2 * 1e-3)
         res[name] = stats
     res["value"] = res["fp64"]["cell_updates_per_s"]
     res["unit"] = "cell-updates/s"
-    res["timing"] = "device events around assemble, GMRES and update of one step from the same state"
+    res["timing"] = ("device events around assemble, GMRES and update of the second step on a state "
+                     "(the first step also captures the Arnoldi-cycle graph; both reported)")
     print(json.dumps(res), flush=True)
 
 

@@ -9,10 +9,15 @@
 // * block Jacobi: the no-pivot LU of each diagonal block is factored once per matrix
 //   (multipliers and upper factor kept), then applied with the same operations and order
 //   as lu_solve_noswp. Bit-identical.
-// * dot products and norms: a fixed grid of 296 blocks x 256 threads; each thread sums a
-//   fixed strided slice, each block a fixed tree, and the block partials are summed in
-//   block order. Deterministic run to run; not the reference's left-to-right order.
-// * Gram-Schmidt: the axpy of step i is fused with the dot product of step i+1.
+// * dot products and norms: a fixed grid of 592 blocks x 256 threads (4 per SM); each
+//   thread sums a fixed strided slice, each block a fixed warp-shuffle tree, and the
+//   consumer of the block partials (every block of the next kernel, or one finishing
+//   block) sums them with the same fixed tree. Deterministic run to run; not the
+//   reference's left-to-right order.
+// * Gram-Schmidt (modified, as the reference's): the axpy of step i is fused with the dot
+//   product of step i+1, so one Arnoldi column of step j costs j passes over the vectors.
+// * One restart cycle's Arnoldi process (m columns) has no host decision in it: it is
+//   captured once per matrix and workspace as a CUDA graph and replayed.
 // * Givens rotations and the back substitution run on the host in the reference's order.
 #include <algorithm>
 #include <cmath>
@@ -25,7 +30,7 @@ namespace subfv {
 
 namespace {
 
-constexpr int kRedBlocks = 296;  // 2 x 148 SMs
+constexpr int kRedBlocks = 592;  // 4 x 148 SMs
 constexpr int kRedThreads = 256;
 
 template <int BS, class MT>
@@ -96,9 +101,14 @@ __global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __
   for (int k = 0; k < BS; ++k) x[(size_t)BS * i + k] = xv[k];
 }
 
+__device__ inline double warp_tree(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
 __device__ inline double block_sum(double v) {
   __shared__ double sh[kRedThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, o);
+  v = warp_tree(v);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
   __syncthreads();
   double s = 0.0;
@@ -107,20 +117,52 @@ __device__ inline double block_sum(double v) {
   return s;  // valid in thread 0
 }
 
+// sum of the nb block partials by a fixed tree (thread slices, warp shuffles, warps in
+// order); every block that calls it gets the same value. Returned to all threads.
+__device__ inline double sum_partials(const double* __restrict__ p, int nb) {
+  __shared__ double sh[kRedThreads / 32];
+  __shared__ double tot;
+  double v = 0.0;
+  for (int q = threadIdx.x; q < nb; q += kRedThreads) v = v + p[q];
+  v = warp_tree(v);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kRedThreads / 32; ++w) s = s + sh[w];
+    tot = s;
+  }
+  __syncthreads();
+  return tot;
+}
+
+constexpr int kUnroll = 4;
+
 // partial[b] = sum over the block's fixed slice of a*b
 __global__ void __launch_bounds__(kRedThreads) k_dot(const double* __restrict__ a, const double* __restrict__ b,
                                                      long n, double* __restrict__ partial) {
   const long T = (long)gridDim.x * blockDim.x;
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   double s = 0.0;
-  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += T) s = s + a[k] * b[k];
+  for (; k + (kUnroll - 1) * T < n; k += kUnroll * T) {
+    double av[kUnroll], bv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      av[u] = a[k + u * T];
+      bv[u] = b[k + u * T];
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) s = s + av[u] * bv[u];
+  }
+  for (; k < n; k += T) s = s + a[k] * b[k];
   s = block_sum(s);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
-__device__ inline double sum_partials(const double* p, int nb) {
-  double s = 0.0;
-  for (int q = 0; q < nb; ++q) s = s + p[q];
-  return s;
+// *out = the fixed-tree sum of the partials (one block)
+__global__ void __launch_bounds__(kRedThreads) k_finish(const double* __restrict__ pin, int nb, double* out) {
+  const double s = sum_partials(pin, nb);
+  if (threadIdx.x == 0) *out = s;
 }
 
 // h = sum(pin); y -= h*x; then pout = partial dot(y_new, nx), or of y_new with itself
@@ -129,38 +171,66 @@ __global__ void __launch_bounds__(kRedThreads) k_axpy_dot(double* __restrict__ y
                                                           const double* __restrict__ pin, int nb, double* hout,
                                                           const double* __restrict__ nx, double* __restrict__ pout,
                                                           long n) {
-  __shared__ double hs;
-  if (threadIdx.x == 0) hs = sum_partials(pin, nb);
-  __syncthreads();
-  const double h = hs;
+  const double h = sum_partials(pin, nb);
   if (blockIdx.x == 0 && threadIdx.x == 0 && hout) *hout = h;
   const long T = (long)gridDim.x * blockDim.x;
+  long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   double s = 0.0;
-  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += T) {
-    const double yk = y[k] - h * x[k];
-    y[k] = yk;
-    s = s + yk * (nx ? nx[k] : yk);
+  if (nx) {
+    for (; k + (kUnroll - 1) * T < n; k += kUnroll * T) {
+      double yv[kUnroll], xv[kUnroll], nv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        yv[u] = y[k + u * T];
+        xv[u] = x[k + u * T];
+        nv[u] = nx[k + u * T];
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const double yk = yv[u] - h * xv[u];
+        y[k + u * T] = yk;
+        s = s + yk * nv[u];
+      }
+    }
+    for (; k < n; k += T) {
+      const double yk = y[k] - h * x[k];
+      y[k] = yk;
+      s = s + yk * nx[k];
+    }
+  } else {
+    for (; k + (kUnroll - 1) * T < n; k += kUnroll * T) {
+      double yv[kUnroll], xv[kUnroll];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        yv[u] = y[k + u * T];
+        xv[u] = x[k + u * T];
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const double yk = yv[u] - h * xv[u];
+        y[k + u * T] = yk;
+        s = s + yk * yk;
+      }
+    }
+    for (; k < n; k += T) {
+      const double yk = y[k] - h * x[k];
+      y[k] = yk;
+      s = s + yk * yk;
+    }
   }
   s = block_sum(s);
   if (threadIdx.x == 0) pout[blockIdx.x] = s;
 }
 
-// nrm = sqrt(sum(pin)); y = y / nrm; block 0 stores nrm at *hout
-__global__ void __launch_bounds__(kRedThreads) k_normalize(double* __restrict__ y, const double* __restrict__ pin,
+// nrm = sqrt(sum(pin)); y = src / nrm (src may be y); block 0 stores nrm at *hout
+__global__ void __launch_bounds__(kRedThreads) k_normalize(const double* src, double* y, const double* __restrict__ pin,
                                                            int nb, double* hout, long n) {
-  __shared__ double hs;
-  if (threadIdx.x == 0) hs = sqrt(sum_partials(pin, nb));
-  __syncthreads();
-  const double h = hs;
+  const double h = sqrt(sum_partials(pin, nb));
   if (blockIdx.x == 0 && threadIdx.x == 0) *hout = h;
   const long T = (long)gridDim.x * blockDim.x;
-  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += T) y[k] = y[k] / h;
+  for (long k = (long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += T) y[k] = src[k] / h;
 }
 
-__global__ void k_scale_div(double* __restrict__ y, double d, long n) {
-  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < n) y[k] = y[k] / d;
-}
 __global__ void k_sub(const double* __restrict__ b, const double* __restrict__ w, double* __restrict__ r, long n) {
   const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (k < n) r[k] = b[k] - w[k];
@@ -272,6 +342,7 @@ int gmres_work_alloc(GmresWork* W, long n, int krylov) {
 }
 
 void gmres_work_free(GmresWork* W) {
+  if (W->cycle) cudaGraphExecDestroy(W->cycle);
   void* p[] = {W->V, W->r, W->w, W->zp, W->z, W->partial, W->H, W->scal, W->d, W->rr};
   for (void* q : p)
     if (q) cudaFree(q);
@@ -321,28 +392,23 @@ void launch_bcsr_bjacobi(const DevBcsr& A, const double* b, double* x) {
   }
 }
 
-namespace {
-// host copy of the block partials, summed in block order (the device's order)
-int host_finish(const DevBcsr& A, const double* dpartial, double* out) {
-  double h[kRedBlocks];
-  SUBFV_CUDA(cudaMemcpyAsync(h, dpartial, sizeof(h), cudaMemcpyDeviceToHost, A.stream));
-  SUBFV_CUDA(cudaStreamSynchronize(A.stream));
-  double s = 0.0;
-  for (int q = 0; q < kRedBlocks; ++q) s = s + h[q];
-  *out = s;
-  return 0;
-}
-}  // namespace
-
 double device_norm2(const DevBcsr& A, GmresWork& W, const double* x, long n) {
   k_dot<<<kRedBlocks, kRedThreads, 0, A.stream>>>(x, x, n, W.partial);
+  k_finish<<<1, kRedThreads, 0, A.stream>>>(W.partial, kRedBlocks, W.scal + 1);
   double s = 0.0;
-  if (host_finish(A, W.partial, &s)) return -1.0;
+  if (cudaMemcpyAsync(&s, W.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, A.stream) != cudaSuccess ||
+      cudaStreamSynchronize(A.stream) != cudaSuccess) {
+    set_error("device_norm2: CUDA error");
+    return -1.0;
+  }
   return std::sqrt(s);
 }
 
-int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, bool precond, bool fp32,
-                 int maxit, GmresStats* st, double* H_first_host) {
+namespace {
+// One restart cycle's Arnoldi process: V_1 = r/|r| (|r|^2 from the partials that the
+// preceding device_norm2 left in W.partial), then columns 2..m+1 with modified
+// Gram-Schmidt, H on the device. Launch-only (no host decision), so it can be captured.
+void arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
   const int m = W.krylov;
   const long n = W.n;
   cudaStream_t s = A.stream;
@@ -350,6 +416,58 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
   double* pb = W.partial + kRedBlocks;
   auto Vc = [&](int j) { return W.V + (size_t)(j - 1) * n; };  // 1-based
   auto Hd = [&](int i, int j) { return W.H + (i - 1) + (size_t)(m + 1) * (j - 1); };
+  cudaMemsetAsync(W.H, 0, (size_t)(m + 1) * m * sizeof(double), s);
+  k_normalize<<<kRedBlocks, kRedThreads, 0, s>>>(W.r, Vc(1), pa, kRedBlocks, W.scal, n);
+  for (int jj = 2; jj <= m + 1; ++jj) {
+    if (precond) {
+      launch_bcsr_bjacobi(A, Vc(jj - 1), W.zp);
+      launch_bcsr_spmv(A, W.zp, Vc(jj), fp32);
+    } else {
+      launch_bcsr_spmv(A, Vc(jj - 1), Vc(jj), fp32);
+    }
+    k_dot<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(1), Vc(jj), n, pa);
+    for (int i = 1; i <= jj - 1; ++i) {
+      const double* nx = i < jj - 1 ? Vc(i + 1) : nullptr;  // the last one is |V_jj|^2
+      k_axpy_dot<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(jj), Vc(i), pa, kRedBlocks, Hd(i, jj - 1), nx, pb, n);
+      std::swap(pa, pb);
+    }
+    k_normalize<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(jj), Vc(jj), pa, kRedBlocks, Hd(jj, jj - 1), n);
+  }
+}
+
+// Replays the cycle from a graph captured for this matrix, workspace and mode.
+int run_arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
+  const uintptr_t key[] = {(uintptr_t)A.row, (uintptr_t)A.col, (uintptr_t)A.v, (uintptr_t)A.v32, (uintptr_t)A.lu,
+                           (uintptr_t)A.lo, (uintptr_t)A.m, (uintptr_t)A.bs, (uintptr_t)A.stream,
+                           (uintptr_t)(precond ? 1 : 0) | (fp32 ? 2 : 0)};
+  static_assert(sizeof(key) == sizeof(W.cycle_key), "cycle key size");
+  if (W.cycle && std::memcmp(key, W.cycle_key, sizeof(key)) != 0) {
+    cudaGraphExecDestroy(W.cycle);
+    W.cycle = nullptr;
+  }
+  if (!W.cycle) {
+    cudaGraph_t g = nullptr;
+    SUBFV_CUDA(cudaStreamBeginCapture(A.stream, cudaStreamCaptureModeThreadLocal));
+    arnoldi_cycle(A, W, precond, fp32);
+    const cudaError_t le = cudaGetLastError();
+    const cudaError_t ce = cudaStreamEndCapture(A.stream, &g);
+    SUBFV_CUDA(le);
+    SUBFV_CUDA(ce);
+    const cudaError_t ie = cudaGraphInstantiate(&W.cycle, g, 0);
+    cudaGraphDestroy(g);
+    SUBFV_CUDA(ie);
+    std::memcpy(W.cycle_key, key, sizeof(key));
+  }
+  SUBFV_CUDA(cudaGraphLaunch(W.cycle, A.stream));
+  return 0;
+}
+}  // namespace
+
+int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, bool precond, bool fp32,
+                 int maxit, GmresStats* st, double* H_first_host) {
+  const int m = W.krylov;
+  const long n = W.n;
+  cudaStream_t s = A.stream;
   std::vector<double> H((size_t)(m + 1) * m), y(m + 1), c(m + 1), sn(m + 1), z(m + 1);
   auto h = [&](int i, int j) -> double& { return H[(i - 1) + (size_t)(m + 1) * (j - 1)]; };
   st->conv = 0;
@@ -357,6 +475,7 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
   launch_bcsr_spmv(A, x, W.w, fp32);
   k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.r, n);
   double rho = device_norm2(A, W, W.r, n);
+  if (rho < 0.0) return -1;
   int it = 0;
   if (rho < tol) {
     st->conv = 1;
@@ -368,24 +487,7 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
     it = j;
     std::fill(y.begin(), y.end(), 0.0);
     y[0] = rho;
-    k_scale_div<<<egrid(n), 256, 0, s>>>(W.r, y[0], n);
-    SUBFV_CUDA(cudaMemcpyAsync(Vc(1), W.r, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-    SUBFV_CUDA(cudaMemsetAsync(W.H, 0, H.size() * sizeof(double), s));
-    for (int jj = 2; jj <= m + 1; ++jj) {
-      if (precond) {
-        launch_bcsr_bjacobi(A, Vc(jj - 1), W.zp);
-        launch_bcsr_spmv(A, W.zp, Vc(jj), fp32);
-      } else {
-        launch_bcsr_spmv(A, Vc(jj - 1), Vc(jj), fp32);
-      }
-      k_dot<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(1), Vc(jj), n, pa);
-      for (int i = 1; i <= jj - 1; ++i) {
-        const double* nx = i < jj - 1 ? Vc(i + 1) : nullptr;  // the last one is |V_jj|^2
-        k_axpy_dot<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(jj), Vc(i), pa, kRedBlocks, Hd(i, jj - 1), nx, pb, n);
-        std::swap(pa, pb);
-      }
-      k_normalize<<<kRedBlocks, kRedThreads, 0, s>>>(Vc(jj), pa, kRedBlocks, Hd(jj, jj - 1), n);
-    }
+    if (run_arnoldi_cycle(A, W, precond, fp32)) return -1;
     SUBFV_CUDA(cudaMemcpyAsync(H.data(), W.H, H.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
     SUBFV_CUDA(cudaStreamSynchronize(s));
     SUBFV_CUDA(cudaGetLastError());
@@ -431,6 +533,7 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
     launch_bcsr_spmv(A, x, W.w, fp32);
     k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.r, n);
     rho = device_norm2(A, W, W.r, n);
+    if (rho < 0.0) return -1;
     if (rho < tol) {
       if (precond) st->conv = 1;
       break;
@@ -439,7 +542,9 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
   if (!precond) {
     launch_bcsr_spmv(A, x, W.w, fp32);
     k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.r, n);
-    st->conv = !(device_norm2(A, W, W.r, n) > tol);
+    const double r2 = device_norm2(A, W, W.r, n);
+    if (r2 < 0.0) return -1;
+    st->conv = !(r2 > tol);
   }
   st->rho = rho;
   st->restarts = it;
@@ -452,6 +557,7 @@ int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double*
   const long n = W.n;
   cudaStream_t s = A.stream;
   const double bnorm = device_norm2(A, W, b, n);
+  if (bnorm < 0.0) return -1;
   SUBFV_CUDA(cudaMemsetAsync(x, 0, n * sizeof(double), s));
   SUBFV_CUDA(cudaMemcpyAsync(W.rr, b, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   st->conv = 0;
@@ -470,6 +576,7 @@ int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double*
     launch_bcsr_spmv(A, x, W.w, false);  // FP64 residual
     k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.rr, n);
     rn = device_norm2(A, W, W.rr, n);
+    if (rn < 0.0) return -1;
   }
   if (!st->conv && rn < rel_tol * bnorm) st->conv = 1;
   st->outer = outer - (st->conv ? 1 : 0);

@@ -3,6 +3,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <vector>
 
 #include "common.cuh"
@@ -41,6 +42,8 @@ struct GmresWork {
   double *partial = nullptr, *H = nullptr, *scal = nullptr;
   double *d = nullptr, *rr = nullptr;  // refinement correction and residual
   size_t bytes = 0;
+  cudaGraphExec_t cycle = nullptr;  // the captured Arnoldi cycle and what it was captured for
+  uintptr_t cycle_key[10] = {};
 };
 
 int bcsr_upload(DevBcsr* A, int m, int bs, const int* row1, const int* col1, const double* v, cudaStream_t s);

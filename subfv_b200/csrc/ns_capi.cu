@@ -412,6 +412,7 @@ int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, d
   SUBFV_CUDA(cudaEventRecord(e[1], d.stream));
   GmresStats st;
   const double bnorm = device_norm2(c->A, c->W, c->b, 5L * d.ne);
+  if (bnorm < 0.0) return -1;
   if (refine_fp32) {
     if (gmres_refine_device(c->A, c->W, c->x, c->b, rel_tol, 1e-3, 30, &st)) return -1;
   } else {
