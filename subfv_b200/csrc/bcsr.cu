@@ -33,11 +33,14 @@ namespace {
 constexpr int kRedBlocks = 592;  // 4 x 148 SMs
 constexpr int kRedThreads = 256;
 
+// Four blocks of the row are in flight at once (their column indices, values and x
+// entries are loaded before any product); the arithmetic order is unchanged.
 template <int BS, class MT>
 __global__ void __launch_bounds__(128) k_spmv(int m, const int* __restrict__ row, const int* __restrict__ col,
                                               const MT* __restrict__ v, const double* __restrict__ x,
                                               double* __restrict__ y) {
   constexpr int GPW = 32 / BS;
+  constexpr int U = 4;
   const int lane = threadIdx.x & 31;
   if (lane >= GPW * BS) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -45,59 +48,83 @@ __global__ void __launch_bounds__(128) k_spmv(int m, const int* __restrict__ row
   const int r = lane % BS;
   if (i >= m) return;
   double acc = 0.0;
-  for (int j = row[i]; j < row[i + 1]; ++j) {
-    const int c0 = col[j];
-    const MT* blk = v + (size_t)BS * BS * j;
-    const double* xc = x + (size_t)BS * c0;
-    double t = 0.0;
+  const int je = row[i + 1];
+  for (int j = row[i]; j < je; j += U) {
+    int cc[U];
+    MT bv[U][BS];
+    double xv[U][BS];
 #pragma unroll
-    for (int c = 0; c < BS; ++c) t = t + (double)blk[r + BS * c] * xc[c];
-    acc = acc + t;
+    for (int u = 0; u < U; ++u) cc[u] = j + u < je ? col[j + u] : -1;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const MT* blk = v + (size_t)BS * BS * (j + u);
+#pragma unroll
+      for (int c = 0; c < BS; ++c) bv[u][c] = cc[u] >= 0 ? blk[r + BS * c] : MT(0);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const double* xc = x + (size_t)BS * (cc[u] >= 0 ? cc[u] : 0);
+#pragma unroll
+      for (int c = 0; c < BS; ++c) xv[u][c] = cc[u] >= 0 ? xc[c] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (cc[u] < 0) break;
+      double t = 0.0;
+#pragma unroll
+      for (int c = 0; c < BS; ++c) t = t + (double)bv[u][c] * xv[u][c];
+      acc = acc + t;
+    }
   }
   y[(size_t)BS * i + r] = acc;
 }
 
+// The no-pivot LU of each diagonal block, packed in one block (multipliers below the
+// diagonal, the upper factor on and above it) and stored element-major: entry q of
+// block row i at lu[q * m + i], so that a thread per block row reads coalesced.
 template <int BS>
 __global__ void k_factor_diag(int m, const int* __restrict__ diag, const double* __restrict__ v,
-                              double* __restrict__ lu, double* __restrict__ lo) {
+                              double* __restrict__ lu) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
-  double C[BS * BS], L[BS * BS];
+  double C[BS * BS];
   const int dj = diag[i];
-  for (int q = 0; q < BS * BS; ++q) {
+  for (int q = 0; q < BS * BS; ++q)
     C[q] = dj >= 0 ? v[(size_t)BS * BS * dj + q] : (q % (BS + 1) == 0 ? 1.0 : 0.0);
-    L[q] = 0.0;
-  }
   for (int k = 0; k < BS; ++k) {
     const double invdiag = 1.0 / C[k + BS * k];
     for (int ii = k + 1; ii < BS; ++ii) {
       const double lik = C[ii + BS * k] * invdiag;
-      L[ii + BS * k] = lik;
-      for (int jj = k; jj < BS; ++jj) C[ii + BS * jj] = C[ii + BS * jj] - lik * C[k + BS * jj];
+      for (int jj = k + 1; jj < BS; ++jj) C[ii + BS * jj] = C[ii + BS * jj] - lik * C[k + BS * jj];
+      C[ii + BS * k] = lik;
     }
   }
-  for (int q = 0; q < BS * BS; ++q) {
-    lu[(size_t)BS * BS * i + q] = C[q];
-    lo[(size_t)BS * BS * i + q] = L[q];
-  }
+  for (int q = 0; q < BS * BS; ++q) lu[(size_t)q * m + i] = C[q];
 }
 
 template <int BS>
-__global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __restrict__ lo,
-                          const double* __restrict__ b, double* __restrict__ x) {
+__global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __restrict__ b,
+                          double* __restrict__ x) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
-  const double* C = lu + (size_t)BS * BS * i;
-  const double* L = lo + (size_t)BS * BS * i;
+  double C[BS * BS];
+#pragma unroll
+  for (int q = 0; q < BS * BS; ++q) C[q] = lu[(size_t)q * m + i];
   double xv[BS];
+#pragma unroll
   for (int k = 0; k < BS; ++k) xv[k] = b[(size_t)BS * i + k];
+#pragma unroll
   for (int k = 0; k < BS; ++k)
-    for (int ii = k + 1; ii < BS; ++ii) xv[ii] = xv[ii] - L[ii + BS * k] * xv[k];
+#pragma unroll
+    for (int ii = k + 1; ii < BS; ++ii) xv[ii] = xv[ii] - C[ii + BS * k] * xv[k];
   xv[BS - 1] = xv[BS - 1] / C[(BS - 1) + BS * (BS - 1)];
+#pragma unroll
   for (int k = BS - 2; k >= 0; --k) {
+#pragma unroll
     for (int j = k + 1; j < BS; ++j) xv[k] = xv[k] - C[k + BS * j] * xv[j];
     xv[k] = xv[k] / C[k + BS * k];
   }
+#pragma unroll
   for (int k = 0; k < BS; ++k) x[(size_t)BS * i + k] = xv[k];
 }
 
@@ -294,8 +321,7 @@ int bcsr_upload(DevBcsr* A, int m, int bs, const int* row1, const int* col1, con
   SUBFV_CUDA(cudaMalloc(&A->v, vb * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&A->v32, vb * sizeof(float)));
   SUBFV_CUDA(cudaMalloc(&A->lu, (size_t)bs * bs * m * sizeof(double)));
-  SUBFV_CUDA(cudaMalloc(&A->lo, (size_t)bs * bs * m * sizeof(double)));
-  A->bytes = (m + 1 + nnz + m) * sizeof(int) + vb * 12 + 2 * (size_t)bs * bs * m * 8;
+  A->bytes = (m + 1 + nnz + m) * sizeof(int) + vb * 12 + (size_t)bs * bs * m * 8;
   SUBFV_CUDA(cudaMemcpyAsync(A->row, row.data(), (m + 1) * sizeof(int), cudaMemcpyHostToDevice, A->stream));
   SUBFV_CUDA(cudaMemcpyAsync(A->col, col.data(), nnz * sizeof(int), cudaMemcpyHostToDevice, A->stream));
   SUBFV_CUDA(cudaMemcpyAsync(A->diag, diag.data(), m * sizeof(int), cudaMemcpyHostToDevice, A->stream));
@@ -317,7 +343,7 @@ int bcsr_set_values(DevBcsr* A, const double* v, bool on_device) {
 }
 
 void bcsr_free(DevBcsr* A) {
-  void* p[] = {A->row, A->col, A->v, A->v32, A->diag, A->lu, A->lo};
+  void* p[] = {A->row, A->col, A->v, A->v32, A->diag, A->lu};
   for (void* q : p)
     if (q) cudaFree(q);
   if (A->own_stream && A->stream) cudaStreamDestroy(A->stream);
@@ -375,20 +401,20 @@ void launch_bcsr_spmv(const DevBcsr& A, const double* x, double* y, bool fp32) {
 void launch_bcsr_factor_diag(const DevBcsr& A) {
   const int g = (A.m + 127) / 128;
   switch (A.bs) {
-    case 5: k_factor_diag<5><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo); break;
-    case 4: k_factor_diag<4><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo); break;
-    case 3: k_factor_diag<3><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo); break;
-    default: k_factor_diag<1><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu, A.lo);
+    case 5: k_factor_diag<5><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu); break;
+    case 4: k_factor_diag<4><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu); break;
+    case 3: k_factor_diag<3><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu); break;
+    default: k_factor_diag<1><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, A.lu);
   }
 }
 
 void launch_bcsr_bjacobi(const DevBcsr& A, const double* b, double* x) {
   const int g = (A.m + 127) / 128;
   switch (A.bs) {
-    case 5: k_bjacobi<5><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x); break;
-    case 4: k_bjacobi<4><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x); break;
-    case 3: k_bjacobi<3><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x); break;
-    default: k_bjacobi<1><<<g, 128, 0, A.stream>>>(A.m, A.lu, A.lo, b, x);
+    case 5: k_bjacobi<5><<<g, 128, 0, A.stream>>>(A.m, A.lu, b, x); break;
+    case 4: k_bjacobi<4><<<g, 128, 0, A.stream>>>(A.m, A.lu, b, x); break;
+    case 3: k_bjacobi<3><<<g, 128, 0, A.stream>>>(A.m, A.lu, b, x); break;
+    default: k_bjacobi<1><<<g, 128, 0, A.stream>>>(A.m, A.lu, b, x);
   }
 }
 
@@ -438,7 +464,7 @@ void arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
 // Replays the cycle from a graph captured for this matrix, workspace and mode.
 int run_arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
   const uintptr_t key[] = {(uintptr_t)A.row, (uintptr_t)A.col, (uintptr_t)A.v, (uintptr_t)A.v32, (uintptr_t)A.lu,
-                           (uintptr_t)A.lo, (uintptr_t)A.m, (uintptr_t)A.bs, (uintptr_t)A.stream,
+                           (uintptr_t)A.nnz, (uintptr_t)A.m, (uintptr_t)A.bs, (uintptr_t)A.stream,
                            (uintptr_t)(precond ? 1 : 0) | (fp32 ? 2 : 0)};
   static_assert(sizeof(key) == sizeof(W.cycle_key), "cycle key size");
   if (W.cycle && std::memcmp(key, W.cycle_key, sizeof(key)) != 0) {

@@ -19,8 +19,7 @@ struct DevBcsr {
   double* v = nullptr;     // (bs, bs, nnz) column-major blocks
   float* v32 = nullptr;    // FP32 copy for the iterative-refinement inner solves
   int* diag = nullptr;     // (m) index of the diagonal block, -1 if absent
-  double* lu = nullptr;    // (bs, bs, m) no-pivot LU: upper part and diagonal of C
-  double* lo = nullptr;    // (bs, bs, m) the multipliers lik below the diagonal
+  double* lu = nullptr;    // (bs*bs, m) no-pivot LU, element-major: multipliers below the diagonal, U on and above
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   size_t bytes = 0;
