@@ -363,39 +363,6 @@ def _l1_rel(a, b):
     return [float(np.abs(a[:, i] - b[:, i]).sum() / max(scale[i], 1e-3 * mom, 1e-300)) for i in range(5)]
 
 
-def autotune_batch(batch, steps=2, log=None):
-    """Pick the batched launch shape: coordinate search over the vertex-kernel block
-    (64/128/256 vertices) and the persistent grid sizes (multiples of the 148 SMs),
-    each candidate timed on the device over `steps` steps of the live batch (the steps
-    are real: problems advance). Results do not depend on the shape."""
-    sms = 148
-    best = (128, sms * 8, sms * 8)
-    batch.set_launch(*best)
-    batch.time_steps(1)
-    t_best = batch.time_steps(steps)
-    trials = [(best, t_best)]
-
-    def try_(shape):
-        nonlocal best, t_best
-        batch.set_launch(*shape)
-        batch.time_steps(1)
-        t = batch.time_steps(steps)
-        trials.append((shape, t))
-        if t < t_best:
-            best, t_best = shape, t
-
-    for mult in (2, 4, 16, 32, 64):
-        try_((best[0], best[1], sms * mult))
-    for bv in (64, 256):
-        try_((bv, best[1], best[2]))
-    for mult in (2, 4, 16, 32, 64):
-        try_((best[0], sms * mult, best[2]))
-    batch.set_launch(*best)
-    if log is not None:
-        log.extend({"block_v": s[0], "grid_v": s[1], "grid_c": s[2], "ms_per_step": t / steps} for s, t in trials)
-    return best, t_best / steps
-
-
 def run_shocktubes(args, rank, world, local):
     """Batched shock tubes: `--problems` (1024) independent Riemann problems on N x 4 quad
     strips, N uniform in [200, 20000] (seed 1), states as in subfv_b200.shocktube, first
@@ -405,7 +372,7 @@ def run_shocktubes(args, rank, world, local):
     FP64 batch; the baseline is the plain FP64 path run one problem at a time
     (subfv_ns_state, graph-replayed) over a sample of the problems."""
     import torch
-    from subfv_b200 import shocktube
+    from subfv_b200 import autotune, shocktube
     from subfv_b200.ns import NsBatch, NsConfig, NsState
     rng_tubes = shocktube.sample(args.problems, seed=SEED, n_max=args.nmax)
     t0 = time.perf_counter()
@@ -424,21 +391,22 @@ def run_shocktubes(args, rank, world, local):
         slots = [b.add(m, s, t.t_end) for m, s, t in zip(meshes, sols, rng_tubes)]
         assert None not in slots
         log = []
-        best, _ = autotune_batch(b, log=log)
+        best, _ = autotune.tune_ns_batch(b, log=log)
         for _ in range(args.warmup):
             b.time_steps(1)
         sampler = ClockSampler(local)
         sampler.start()
         ms_tuned = b.time_steps(K)
         clocks = sampler.stop()
-        b.set_launch(128, 148 * 8, 148 * 8)
+        autotune.apply(b, autotune.DEFAULT)
         b.time_steps(1)
         ms_fixed = b.time_steps(K)
         b.sync()
         st = max(b.info(k)[3] for k in slots)
         res[name] = {"value": cells * K / (ms_tuned / 1e3), "ms_per_step": ms_tuned / K,
                      "fixed_value": cells * K / (ms_fixed / 1e3), "fixed_ms_per_step": ms_fixed / K,
-                     "tuned_shape": {"block_v": best[0], "grid_v": best[1], "grid_c": best[2]},
+                     "tuned_shape": {"node_lanes": best[0], "block_v": best[1], "grid_v": best[2],
+                                     "grid_c": best[3]},
                      "autotune_trials": log, "status": st, "clocks": clocks,
                      "state_bytes": sum(b.state_bytes(m) for m in meshes)}
         b.close()

@@ -183,6 +183,11 @@ int subfv_ns_advance(subfv_ns_state* s, int n_steps, int* steps_done, double* t)
 int subfv_ns_advance_async(subfv_ns_state* s, int n_steps);
 int subfv_ns_sync(subfv_ns_state* s, int* steps_done, double* t);
 int subfv_ns_get_sol(subfv_ns_state* s, double* sol);
+/* Node kernel layout: 0 one thread per vertex (default), 1 a group of lanes per vertex
+ * (8, 16 or 32 as the mesh needs, one per subface) with the per-vertex sums formed in
+ * shared memory; 8, 16 or 32: a group of at least that many lanes. Results are
+ * bit-identical in every layout. */
+int subfv_ns_state_set_node_kernel(subfv_ns_state* s, int lanes);
 /* res = sum of |delta|_2 and res_vect(5) of the last add_timedisc_and_solve call */
 int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double* dt);
 /* No counterpart in the reference (its NS path is point-implicit only). One backward
@@ -252,6 +257,8 @@ int subfv_ns_batch_get_sol(subfv_ns_batch* b, int slot, double* sol);
  * 128 or 256), and the persistent grid sizes of the vertex and cell kernels. Results do
  * not depend on it. */
 int subfv_ns_batch_set_launch(subfv_ns_batch* b, int block_v, int grid_v, int grid_c);
+/* Node kernel layout of the batch, as subfv_ns_state_set_node_kernel. */
+int subfv_ns_batch_set_node_kernel(subfv_ns_batch* b, int lanes);
 
 /* ---------------------------------------------------------------------------------
  * Batched and served Lagrangian hydro. No counterpart in the reference (one mesh per

@@ -57,6 +57,7 @@ SIGNATURES = {
     "subfv_compute_rhs_ns": (c_int, [P, P, PD, PD, PD, PD, PD]),
     "subfv_ns_state_create": (c_int, [P, P, PD, c_dbl, C.POINTER(P)]),
     "subfv_ns_state_destroy": (c_int, [P]),
+    "subfv_ns_state_set_node_kernel": (c_int, [P, c_int]),
     "subfv_ns_advance": (c_int, [P, c_int, C.POINTER(c_int), PD]),
     "subfv_ns_advance_async": (c_int, [P, c_int]),
     "subfv_ns_sync": (c_int, [P, C.POINTER(c_int), PD]),
@@ -79,6 +80,7 @@ SIGNATURES = {
     "subfv_ns_batch_slot_info": (c_int, [P, c_int, PD, C.POINTER(c_i64), C.POINTER(c_int), C.POINTER(C.c_uint)]),
     "subfv_ns_batch_get_sol": (c_int, [P, c_int, PD]),
     "subfv_ns_batch_set_launch": (c_int, [P, c_int, c_int, c_int]),
+    "subfv_ns_batch_set_node_kernel": (c_int, [P, c_int]),
     "subfv_lag_batch_create": (c_int, [c_int, c_int, c_i64, C.POINTER(P)]),
     "subfv_lag_batch_destroy": (c_int, [P]),
     "subfv_lag_batch_state_bytes": (c_i64, [P, P]),

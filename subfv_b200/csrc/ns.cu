@@ -50,6 +50,7 @@ NsParams ns_params_from(const subfv_ns_cfg& c) {
   p.cfl = c.cfl;
   p.tmax = c.tmax;
   p.precision = c.precision;
+  p.node_group = 0;
   return p;
 }
 
@@ -622,6 +623,242 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
   }
 }
 
+// The same computation with a group of NG lanes per vertex (warp-per-node segmented
+// reductions over the vertex-to-subface CSR): lane j owns subface j and subcell j of the
+// vertex and keeps its subface's states in registers. The per-vertex sums (B_p, M, R)
+// and the subcell sums are formed in shared memory by one lane per component, adding the
+// subfaces' terms in subface order exactly as the thread-per-vertex kernel does, so the
+// results are bit-identical to it; every lane of the group then runs the same 3x3 solve
+// on the same sums. NG is 8, 16 or 32; a block of kNodeGroupThreads lanes holds
+// kNodeGroupThreads / NG vertices.
+constexpr int kNodeGroupThreads = 256;
+constexpr int kLaneVals = 12;  // per-lane scratch doubles: 9 solver terms or 12 subcell terms
+
+template <int NG>
+__device__ inline unsigned group_mask() {
+  if constexpr (NG == 32) return 0xffffffffu;
+  else return ((1u << NG) - 1u) << ((threadIdx.x & 31) & ~(NG - 1));
+}
+
+// sum over the group's lanes 0..n-1 of lane k's term c at slot `comp` (slots of width
+// kLaneVals), adding in lane order only the terms whose lane set bit `comp` of its flag
+template <int NG>
+__device__ inline double group_ordered_sum(const double* __restrict__ gv, const unsigned* __restrict__ gf, int n,
+                                           int comp) {
+  double s = 0.0;
+  for (int k = 0; k < NG; ++k)
+    if (k < n && ((gf[k] >> comp) & 1u)) s = s + gv[k * kLaneVals + comp];
+  return s;
+}
+
+template <class T, class L, int NG>
+__device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
+                              const double* __restrict__ grad, double* __restrict__ fs, int so, const int v,
+                              const bool live, double* __restrict__ gv, unsigned* __restrict__ gf,
+                              double* __restrict__ gs) {
+  const int j = threadIdx.x & (NG - 1);
+  const unsigned mask = group_mask<NG>();
+  int p0 = 0, nsfn = 0, q0 = 0, nsen = 0;
+  bool act = live && v < m.nv;
+  if (act) {
+    p0 = m.vsf_off[v];
+    nsfn = m.vsf_off[v + 1] - p0;
+    q0 = m.vse_off[v];
+    nsen = m.vse_off[v + 1] - q0;
+    if (nsfn > NG || nsen > NG) {
+      if (j == 0) atomicOr(m.status, kErrIndex);
+      act = false;
+    }
+  }
+  const bool mine = act && j < nsfn;  // this lane owns a subface
+  T w[10];
+  double n[4] = {0.0, 0.0, 0.0, 0.0};
+  int sf = 0, y = 0;
+  for (int k = 0; k < 10; ++k) w[k] = (T)0;
+  if (mine) {
+    sf = m.vsf[p0 + j];
+    const int2 lr = m.flr[m.sf_face[sf]];
+    y = lr.y;
+    double w10[10];
+    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5);
+    for (int k = 0; k < 10; ++k) w[k] = (T)w10[k];
+    const double4 sn = m.sfn[sf];
+    n[0] = sn.x;
+    n[1] = sn.y;
+    n[2] = sn.z;
+    n[3] = sn.w;
+  }
+  const bool excl = act && m.is_bound[v] && P.excl;
+  double vn3[3] = {0.0, 0.0, 0.0};
+  L lam_l = (L)0, lam_r = (L)0;
+  const bool solve = P.scheme == 1 && act && !excl;
+  if (P.scheme == 1) {  // uniform over the launch: every lane takes the same syncs
+    L al = (L)0, ar = (L)0;
+    if (mine) {
+      al = sqrt((L)G * (L)w[4] / (L)w[0]);
+      ar = sqrt((L)G * (L)w[9] / (L)w[5]);
+    }
+    // wall_normal: lane terms area * n
+    {
+      unsigned f = 0u;
+      if (mine && y < 0 && !(P.b2d && fabs(n[2]) > 1e-12) && (y == -1 || P.bc_type[-(y + 1) - 1] == 1)) f = 7u;
+      for (int d = 0; d < 3; ++d) gv[j * kLaneVals + d] = n[3] * n[d];
+      gf[j] = f;
+    }
+    __syncwarp(mask);
+    if (j < 3) gs[j] = group_ordered_sum<NG>(gv, gf, nsfn, j);
+    __syncwarp(mask);
+    const double Bp[3] = {gs[0], gs[1], gs[2]};
+    __syncwarp(mask);
+    const T ntT[3] = {(T)n[0], (T)n[1], (T)n[2]};
+    const double vnl_f = (double)dotT(w + 1, ntT), vnr_f = (double)dotT(w + 6, ntT);
+    const double pl_f = (double)w[4], pr_f = (double)w[9];
+    const bool wall = is_wall(P, y);
+    double vbar = 0.0;
+    for (int iter = 1; iter <= 4; ++iter) {
+      unsigned f = 0u;
+      if (mine && solve) {
+        const double area = n[3];
+        const L nt[3] = {(L)n[0], (L)n[1], (L)n[2]};
+        L wl[5], wr[5];
+        for (int k = 0; k < 5; ++k) {
+          wl[k] = (L)w[k];
+          wr[k] = (L)w[5 + k];
+        }
+        const L rhol = wl[0], vnl = dotT(wl + 1, nt), pl = wl[4];
+        const L rhor = wr[0], vnr = dotT(wr + 1, nt), pr = wr[4];
+        const L c1 = (L)1, c15 = (L)1.5, c0 = (L)0;
+        if (iter == 1) {
+          lam_l = tmax2(tmax2(tmax2(lam_l, al * rhol), sqrt(rhol * tmax2(c0, pr - pl))), -rhol * (vnr - vnl));
+          lam_r = tmax2(tmax2(tmax2(lam_r, ar * rhor), sqrt(rhor * tmax2(c0, pl - pr))), -rhor * (vnr - vnl));
+          vbar = vbar_of((double)lam_l, (double)lam_r, vnl_f, vnr_f, pl_f, pr_f);
+          lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -((L)vbar - vnl) / al)));
+          lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, ((L)vbar - vnr) / ar)));
+        } else if (wall && P.bc_style == 1) {
+          lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -((L)vbar - vnl) / al)));
+          lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, ((L)vbar - vnr) / ar)));
+        } else {
+          const L v_et = (L)dotT(vn3, n);
+          lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -(v_et - vnl) / al)));
+          lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, (v_et - vnr) / ar)));
+        }
+        vbar = vbar_of((double)lam_l, (double)lam_r, vnl_f, vnr_f, pl_f, pr_f);
+        const double lsum = (double)lam_r + (double)lam_l;
+        double* c = gv + j * kLaneVals;
+        if (!wall || P.bc_style == 0 || P.bc_style == 2) {
+          const double wgt = lsum * area;
+          c[0] = wgt * (n[0] * n[0]);
+          c[1] = wgt * (n[0] * n[1]);
+          c[2] = wgt * (n[0] * n[2]);
+          c[3] = wgt * (n[1] * n[1]);
+          c[4] = wgt * (n[1] * n[2]);
+          c[5] = wgt * (n[2] * n[2]);
+          f |= 0x3fu;
+        }
+        if (!wall || P.bc_style == 0) {
+          const double q = area * lsum * vbar;
+          for (int d = 0; d < 3; ++d) c[6 + d] = q * n[d];
+          f |= 0x1c0u;
+        } else if (P.bc_style == 2 && (!P.b2d || fabs(n[2]) < 1e-8)) {
+          const double q = area * (double)pl;
+          for (int d = 0; d < 3; ++d) c[6 + d] = q * n[d];
+          f |= 0x1c0u;
+        }
+      }
+      gf[j] = f;
+      __syncwarp(mask);
+      for (int comp = j; comp < 9; comp += NG) gs[comp] = group_ordered_sum<NG>(gv, gf, nsfn, comp);
+      __syncwarp(mask);
+      if (solve) {
+        double mat[3][3] = {{gs[0], gs[1], gs[2]}, {gs[1], gs[3], gs[4]}, {gs[2], gs[4], gs[5]}};
+        const double Rp[3] = {gs[6], gs[7], gs[8]};
+        nodal_solve(P, mat, Rp, Bp, vn3);
+      }
+      __syncwarp(mask);
+    }
+    if (act && j == 0) m.vp[v] = make_double4(vn3[0], vn3[1], vn3[2], 0.0);
+  }
+  // subface fluxes; lane j's terms to its left / right subcell of this vertex
+  int lse = -1, rse = -1;
+  unsigned f = 0u;
+  if (mine) {
+    const int2 se = m.sf_se[sf];
+    const int lse_loc = m.se_loc[se.x];
+    double w10[10];
+    for (int k = 0; k < 10; ++k) w10[k] = (double)w[k];
+    double lr[2][5], sl, sr;
+    if (solve) {
+      const double vn = is_wall(P, y) ? 0.0 : dotT(vn3, n);
+      if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam_l, (double)lam_r, &sl, &sr))
+        atomicOr(m.status, kErrNegDensity);
+    } else {
+      two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
+    }
+    if (m.se_vert[se.x] == v && lse_loc < nsen) {
+      const double area = n[3];
+      double* c = gv + j * kLaneVals;
+      lse = lse_loc;
+      for (int k = 0; k < 5; ++k) c[k] = area * lr[0][k];
+      c[5] = area * fmax2(0.0, -sl);
+      if (se.y >= 0 && m.se_vert[se.y] == v) {
+        const int rse_loc = m.se_loc[se.y];
+        if (rse_loc < nsen) {
+          rse = rse_loc;
+          for (int k = 0; k < 5; ++k) c[6 + k] = area * lr[1][k];
+          c[11] = area * fmax2(0.0, sr);
+        }
+      }
+    }
+  }
+  // flag word: left subcell + 1 in bits 0-7, right subcell + 1 in bits 8-15
+  f = (unsigned)(lse + 1) | ((unsigned)(rse + 1) << 8);
+  gf[j] = f;
+  __syncwarp(mask);
+  if (act && j < nsen) {
+    double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int k = 0; k < NG; ++k) {
+      if (k >= nsfn) continue;
+      const unsigned fk = gf[k];
+      const double* c = gv + k * kLaneVals;
+      if ((int)(fk & 0xffu) == j + 1) {
+        acc[5] = acc[5] + c[5];
+        for (int q = 0; q < 5; ++q) acc[q] = acc[q] + c[q];
+      }
+      if ((int)((fk >> 8) & 0xffu) == j + 1) {
+        acc[5] = acc[5] + c[11];
+        for (int q = 0; q < 5; ++q) acc[q] = acc[q] + c[6 + q];
+      }
+    }
+    const int s_id = m.vse[q0 + j];
+    if (m.se_vert[s_id] == v) {  // a periodic image's subcell: its sums are zero here
+      double* out = fs + kNsFs * (size_t)s_id;
+      for (int k = 0; k < 6; ++k) out[k] = acc[k];
+    }
+  }
+  __syncwarp(mask);
+}
+
+// shared scratch of the group kernels: kLaneVals doubles and a flag per lane, 12 doubles
+// per group for the sums
+struct NodeGroupSmem {
+  double v[kNodeGroupThreads * kLaneVals];
+  unsigned f[kNodeGroupThreads];
+  double s[kNodeGroupThreads / 8][12];
+};
+
+template <class T, class L, int NG>
+__global__ void __launch_bounds__(kNodeGroupThreads, 2) k_ns_node_group(DevMesh m, NsParams P,
+                                                                     const double* __restrict__ U,
+                                                                     const double* __restrict__ grad,
+                                                                     double* __restrict__ fs, int so,
+                                                                     const NsScalars* sc) {
+  if (sc && sc->done) return;
+  __shared__ NodeGroupSmem sm;
+  const int g = threadIdx.x / NG;
+  const int v = blockIdx.x * (kNodeGroupThreads / NG) + g;
+  ns_node_group<T, L, NG>(m, P, U, grad, fs, so, v, true, sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g]);
+}
+
 template <class T, class L, int MS>
 __global__ void __launch_bounds__(kNodeThreads) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
                                                           const double* __restrict__ grad, double* __restrict__ fs,
@@ -1012,6 +1249,26 @@ __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restr
     ns_node_vertex<T, L, MS>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * blockDim.x + threadIdx.x);
   }
 }
+// the group variant: a work block of block_v vertices is walked kNodeGroupThreads / NG
+// vertices at a time
+template <class T, class L, int NG>
+__global__ void __launch_bounds__(kNodeGroupThreads, 2) kb_ns_node_group(const NsItem* __restrict__ it,
+                                                                      const int* __restrict__ wv,
+                                                                      const int* __restrict__ hdr, NsParams P,
+                                                                      int which, int so, int block_v) {
+  __shared__ NodeGroupSmem sm;
+  constexpr int VPB = kNodeGroupThreads / NG;
+  const int g = threadIdx.x / NG;
+  const int n = hdr[0];
+  for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
+    const int p = item_of(wv, n, w);
+    const NsItem& I = it[p];
+    if (I.sc->done) continue;
+    for (int c = 0; c < block_v; c += VPB)
+      ns_node_group<T, L, NG>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * block_v + c + g, true,
+                             sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g]);
+  }
+}
 __global__ void __launch_bounds__(128) kb_ns_gather(const NsItem* __restrict__ it, const int* __restrict__ wc,
                                                     const int* __restrict__ hdr, int second) {
   const int n = hdr[0];
@@ -1242,6 +1499,13 @@ int ns_partial_blocks(const DevMesh& m) { return grid_for(m.ne, kTdBlock); }
 template <class T, class L>
 void launch_kb_node_tl(const NsTable& t, const NsParams& P, cudaStream_t s, int which, int so) {
   const int gv = t.grid_v, bv = t.block_v;
+  if (P.node_group) {
+    const int nt = kNodeGroupThreads, g = std::max(t.group, P.node_group);
+    if (g == 8) kb_ns_node_group<T, L, 8><<<gv, nt, 0, s>>>(t.items, t.wv, t.hdr, P, which, so, bv);
+    else if (g == 16) kb_ns_node_group<T, L, 16><<<gv, nt, 0, s>>>(t.items, t.wv, t.hdr, P, which, so, bv);
+    else kb_ns_node_group<T, L, 32><<<gv, nt, 0, s>>>(t.items, t.wv, t.hdr, P, which, so, bv);
+    return;
+  }
   if (t.group == 8) kb_ns_node<T, L, 8><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
   else if (t.group == 16) kb_ns_node<T, L, 16><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
   else kb_ns_node<T, L, 32><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
@@ -1313,7 +1577,18 @@ int ns_node_lanes(const DevMesh& m) {
 template <class T, class L>
 void launch_node_tl(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs, int so,
                     const NsScalars* sc) {
-  const int ms = std::max(8, ns_node_lanes(m));  // a mesh beyond 32 is flagged by the kernel
+  int ms = std::max(8, ns_node_lanes(m));  // a mesh beyond 32 is flagged by the kernel
+  if (P.node_group) {
+    ms = std::max(ms, P.node_group);
+    const int nt = kNodeGroupThreads;
+    if (ms == 8)
+      k_ns_node_group<T, L, 8><<<grid_for(m.nv, nt / 8), nt, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+    else if (ms == 16)
+      k_ns_node_group<T, L, 16><<<grid_for(m.nv, nt / 16), nt, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+    else
+      k_ns_node_group<T, L, 32><<<grid_for(m.nv, nt / 32), nt, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+    return;
+  }
   const int grid = grid_for(m.nv, 128);
   if (ms == 8) k_ns_node<T, L, 8><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
   else if (ms == 16) k_ns_node<T, L, 16><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);

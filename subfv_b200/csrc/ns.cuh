@@ -15,6 +15,7 @@ struct NsParams {
   double bc_val[16][5];
   double cfl, tmax;
   int precision;
+  int node_group;  // 0: one thread per vertex; else a group of lanes per vertex, at least node_group
 };
 
 struct NsScalars {

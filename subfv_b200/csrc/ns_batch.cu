@@ -401,6 +401,22 @@ int subfv_ns_batch_set_launch(subfv_ns_batch* b, int block_v, int grid_v, int gr
   return 0;
 }
 
+int subfv_ns_batch_set_node_kernel(subfv_ns_batch* b, int lanes) {
+  if (!b || (lanes != 0 && lanes != 1 && lanes != 8 && lanes != 16 && lanes != 32)) {
+    set_error("subfv_ns_batch_set_node_kernel: lanes must be 0, 1, 8, 16 or 32");
+    return -2;
+  }
+  if (b->P.node_group != lanes) {
+    b->P.node_group = lanes;
+    if (b->graph) {
+      SUBFV_CUDA(cudaStreamSynchronize(b->stream));
+      cudaGraphExecDestroy(b->graph);
+      b->graph = nullptr;
+    }
+  }
+  return 0;
+}
+
 int subfv_ns_batch_advance(subfv_ns_batch* b, int n_steps) {
   if (!b || n_steps < 0) {
     set_error("subfv_ns_batch_advance: bad argument");

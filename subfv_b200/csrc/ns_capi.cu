@@ -174,6 +174,23 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
   return 0;
 }
 
+int subfv_ns_state_set_node_kernel(subfv_ns_state* s, int lanes) {
+  if (!s || (lanes != 0 && lanes != 1 && lanes != 8 && lanes != 16 && lanes != 32)) {
+    set_error("subfv_ns_state_set_node_kernel: lanes must be 0, 1, 8, 16 or 32");
+    return -2;
+  }
+  if (s->P.node_group != lanes) {
+    s->P.node_group = lanes;
+    if (s->graph) {  // the captured step loop holds the old kernel
+      SUBFV_CUDA(cudaStreamSynchronize(s->m->d.stream));
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+      s->graph_steps = 0;
+    }
+  }
+  return 0;
+}
+
 int subfv_ns_state_destroy(subfv_ns_state* s) {
   if (!s) return 0;
   if (s->imp) {

@@ -148,6 +148,11 @@ class NsState:
         check(_lib.load().subfv_ns_get_sol(self._h, pd(out)), "subfv_ns_get_sol")
         return out
 
+    def set_node_kernel(self, lanes: int):
+        """0: one thread per vertex; 1: a group of lanes per vertex (8/16/32 as the mesh
+        needs); 8, 16, 32: a group of at least that many lanes. Same results in all."""
+        check(_lib.load().subfv_ns_state_set_node_kernel(self._h, int(lanes)), "subfv_ns_state_set_node_kernel")
+
     def residuals(self):
         res, dt = C.c_double(), C.c_double()
         rv = np.zeros(5)
@@ -265,6 +270,11 @@ class NsBatch:
     def set_launch(self, block_v: int, grid_v: int, grid_c: int):
         check(_lib.load().subfv_ns_batch_set_launch(self._h, int(block_v), int(grid_v), int(grid_c)),
               "subfv_ns_batch_set_launch")
+
+    def set_node_kernel(self, lanes: int):
+        """0: one thread per vertex; 1: a group of lanes per vertex (8/16/32 as the mesh
+        needs); 8, 16, 32: a group of at least that many lanes. Same results in all."""
+        check(_lib.load().subfv_ns_batch_set_node_kernel(self._h, int(lanes)), "subfv_ns_batch_set_node_kernel")
 
     def close(self):
         if getattr(self, "_h", None):

@@ -173,3 +173,55 @@ def test_batch_budget_and_ownership(native, cuda_ok):
     assert b.info(k2)[1] == 3
     b.remove(k2)
     b.close()
+
+
+NODE_CFGS = dict(CFGS, mp_o1_fp32flux=dict(scheme=1, second_order=False, method=4, bc_style=2, precision=2))
+
+
+@pytest.mark.parametrize("cfg_name", list(NODE_CFGS))
+def test_node_group_kernel_bitwise(native, cuda_ok, cfg_name):
+    """The lane-per-subface node kernel (a group of 8/16/32 lanes per vertex, per-vertex
+    sums in shared memory) gives the thread-per-vertex kernel's results bit for bit, solo
+    and batched, on 2-D slabs and strips (up to 8 subfaces per vertex), prism slabs (16)
+    and a periodic 3-D box (12), in groups of 8, 16 and 32 lanes."""
+    from dataclasses import replace
+    from subfv_b200 import meshgen
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsBatch, NsConfig, NsState, init_fourier_flow
+    cfg = NsConfig(**NODE_CFGS[cfg_name], boundary_2d=True, cfl=0.4)
+    probs = _setup()
+    box = Mesh.from_raw(meshgen.hex_box(5, jitter=0.05, seed=3, periodic=True))
+    box_sol = init_fourier_flow(box, seed=4)
+    for m, sol, tmax in probs[:3]:
+        out = []
+        for lanes in (0, 1, 32):
+            s = NsState(m, replace(cfg, tmax=tmax), sol)
+            s.set_node_kernel(lanes)
+            out.append((s.advance(9), s.sol()))
+            s.close()
+        for o in out[1:]:
+            assert out[0][0] == o[0]
+            np.testing.assert_array_equal(out[0][1], o[1])
+    cfg3 = replace(cfg, boundary_2d=False, tmax=1e30)
+    out = []
+    for lanes in (0, 1):
+        s = NsState(box, cfg3, box_sol)
+        s.set_node_kernel(lanes)
+        out.append((s.advance(5), s.sol()))
+        s.close()
+    assert out[0][0] == out[1][0]
+    np.testing.assert_array_equal(out[0][1], out[1][1])
+    res = []
+    for lanes, shape in ((0, (128, 148 * 8, 148 * 8)), (1, (128, 148 * 8, 148 * 8)), (1, (64, 5, 3)),
+                         (32, (256, 300, 7))):
+        b = NsBatch(cfg, capacity=8, budget_bytes=1 << 34)
+        b.set_launch(*shape)
+        b.set_node_kernel(lanes)
+        slots = [b.add(m, sol, tmax) for m, sol, tmax in probs]
+        b.advance(13)
+        b.sync()
+        res.append([b.sol(k, m.n_elems) for (m, _, _), k in zip(probs, slots)])
+        b.close()
+    for other in res[1:]:
+        for a, c in zip(res[0], other):
+            np.testing.assert_array_equal(a, c)
