@@ -211,9 +211,9 @@ int subfv_lag_batch_create(int precision, int capacity, int64_t budget_bytes, su
       cudaMalloc(&b->tab.items, capacity * sizeof(LagItem)) != cudaSuccess ||
       cudaMalloc(&b->tab.wf, nw * sizeof(int)) != cudaSuccess)
     return fail();
-  cudaMemset(b->sc, 0, capacity * sizeof(LagScalars));
-  cudaMemset(b->status, 0, capacity * sizeof(unsigned));
-  cudaMemset(b->tab.wf, 0, nw * sizeof(int));
+  cudaMemsetAsync(b->sc, 0, capacity * sizeof(LagScalars), b->stream);
+  cudaMemsetAsync(b->status, 0, capacity * sizeof(unsigned), b->stream);
+  cudaMemsetAsync(b->tab.wf, 0, nw * sizeof(int), b->stream);
   b->tab.wv = b->tab.wf + (capacity + 1);
   b->tab.wc = b->tab.wv + (capacity + 1);
   b->tab.hdr = b->tab.wc + (capacity + 1);

@@ -236,9 +236,9 @@ int subfv_ns_batch_create(const subfv_ns_cfg* cfg, int capacity, int64_t budget_
       cudaMalloc(&b->tab.items, capacity * sizeof(NsItem)) != cudaSuccess ||
       cudaMalloc(&b->tab.wv, nw * sizeof(int)) != cudaSuccess)
     return fail();
-  cudaMemset(b->sc, 0, capacity * sizeof(NsScalars));
-  cudaMemset(b->status, 0, capacity * sizeof(unsigned));
-  cudaMemset(b->tab.wv, 0, nw * sizeof(int));
+  cudaMemsetAsync(b->sc, 0, capacity * sizeof(NsScalars), b->stream);
+  cudaMemsetAsync(b->status, 0, capacity * sizeof(unsigned), b->stream);
+  cudaMemsetAsync(b->tab.wv, 0, nw * sizeof(int), b->stream);
   b->tab.wc = b->tab.wv + (capacity + 1);
   b->tab.hdr = b->tab.wc + (capacity + 1);
   b->tab.cap = capacity;

@@ -44,10 +44,12 @@ int check_cfg(const subfv_ns_cfg* c) {
   return 0;
 }
 
+// zeroed on the stream that later fills the buffer (the mesh's non-blocking stream does
+// not order against the legacy default stream)
 template <class T>
-int dalloc(T** p, size_t n) {
+int dalloc(T** p, size_t n, cudaStream_t s) {
   SUBFV_CUDA(cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T)));
-  SUBFV_CUDA(cudaMemset(*p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+  SUBFV_CUDA(cudaMemsetAsync(*p, 0, std::max<size_t>(n, 1) * sizeof(T), s));
   return 0;
 }
 
@@ -151,10 +153,12 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
   s->m = m;
   s->P = ns_params_from(*cfg);
   const size_t ne = d.ne, nv = d.nv, nse = d.nse;
-  if (dalloc(&s->U0, kRec * ne) || dalloc(&s->U1, kRec * ne) || dalloc(&s->fs, kNsFs * nse) ||
-      dalloc(&s->rhs1, kRhs * ne) || dalloc(&s->rhs2, kRhs * ne) || dalloc(&s->ngrad, 15 * nv) ||
-      dalloc(&s->grad, 15 * ne) || dalloc(&s->delta, 5 * ne) || dalloc(&s->partial, 6 * (size_t)ns_partial_blocks(d)) ||
-      dalloc(&s->stage, 5 * ne) || dalloc(&s->sc, 1)) {
+  cudaStream_t q = d.stream;
+  if (dalloc(&s->U0, kRec * ne, q) || dalloc(&s->U1, kRec * ne, q) || dalloc(&s->fs, kNsFs * nse, q) ||
+      dalloc(&s->rhs1, kRhs * ne, q) || dalloc(&s->rhs2, kRhs * ne, q) || dalloc(&s->ngrad, 15 * nv, q) ||
+      dalloc(&s->grad, 15 * ne, q) || dalloc(&s->delta, 5 * ne, q) ||
+      dalloc(&s->partial, 6 * (size_t)ns_partial_blocks(d), q) || dalloc(&s->stage, 5 * ne, q) ||
+      dalloc(&s->sc, 1, q)) {
     subfv_ns_state_destroy(s);
     return -1;
   }
