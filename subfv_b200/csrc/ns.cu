@@ -1378,11 +1378,12 @@ __device__ void two_wave_jac(const double* wl, const double* wr, const double* n
   euler_jac(ul, n, AL);
   euler_jac(ur, n, AR);
   const double den = sr - sl, asl = fabs(sl), asr = fabs(sr), d = asl - asr;
+  const double rden = 1.0 / den;  // one division per subface; both sides multiply by it
   for (int r = 0; r < 5; ++r)
     for (int c = 0; c < 5; ++c) {
       const bool I = r == c;
-      const double dL = (AL[r][c] - (I ? sl : 0.0)) / den;
-      const double dR = ((I ? sr : 0.0) - AR[r][c]) / den;
+      const double dL = (AL[r][c] - (I ? sl : 0.0)) * rden;
+      const double dR = ((I ? sr : 0.0) - AR[r][c]) * rden;
       JL[r][c] = 0.5 * AL[r][c] - 0.5 * (d * dL - (I ? asl : 0.0));
       JR[r][c] = 0.5 * AR[r][c] - 0.5 * (d * dR + (I ? asr : 0.0));
     }
