@@ -1389,63 +1389,175 @@ __device__ void two_wave_jac(const double* wl, const double* wr, const double* n
     }
 }
 
+// The Euler flux Jacobian d(F.n)/dU of euler_jac one entry at a time, from the same
+// intermediate values and with the same operations, so that a caller can consume the
+// 5x5 matrix entry by entry without holding it.
+struct EulerJacScalars {
+  double u[3], vn, H, phi;
+};
+__device__ inline void euler_jac_scalars(const double* U, const double* n, EulerJacScalars& e) {
+  const double rho = U[0];
+  e.u[0] = U[1] / rho;
+  e.u[1] = U[2] / rho;
+  e.u[2] = U[3] / rho;
+  const double q2 = e.u[0] * e.u[0] + e.u[1] * e.u[1] + e.u[2] * e.u[2];
+  const double p = (G - 1) * (U[4] - 0.5 * rho * q2);
+  e.vn = dotT(e.u, n);
+  e.H = (U[4] + p) / rho;
+  e.phi = 0.5 * (G - 1) * q2;
+}
+__device__ inline double euler_jac_entry(const EulerJacScalars& e, const double* n, int r, int c) {
+  if (r == 0) return (c == 0 || c == 4) ? 0.0 : n[c - 1];
+  if (r == 4) {
+    if (c == 0) return e.vn * (e.phi - e.H);
+    if (c == 4) return G * e.vn;
+    return e.H * n[c - 1] - (G - 1) * e.u[c - 1] * e.vn;
+  }
+  const int k = r - 1;
+  if (c == 0) return e.phi * n[k] - e.u[k] * e.vn;
+  if (c == 4) return (G - 1) * n[k];
+  const int mm = c - 1;
+  const double a = e.u[k] * n[mm] - (G - 1) * e.u[mm] * n[k];
+  return k == mm ? a + e.vn : a;
+}
+
+// A boundary subface's term of the diagonal block, area (J_L + J_R M), column-major:
+// the ghost state U_R(U_L) enters through M (wall: momentum reflection, outflow: I,
+// freestream: 0). Out of line: rare, and it holds three full matrices.
+__device__ __noinline__ void ghost_block(const NsParams& P, int y, const double* wl, const double* wr,
+                                         const double* n, double area, double* g) {
+  double JL[5][5], JR[5][5];
+  two_wave_jac(wl, wr, n, JL, JR);
+  const int kind = y == -1 ? 1 : P.bc_type[-(y + 1) - 1];
+  double M[5][5];
+  for (int a = 0; a < 5; ++a)
+    for (int b = 0; b < 5; ++b) M[a][b] = 0.0;
+  if (kind == 1) {
+    M[0][0] = M[4][4] = 1.0;
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) M[a + 1][b + 1] = (a == b ? 1.0 : 0.0) - 2.0 * n[a] * n[b];
+  } else if (kind == 4) {
+    for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
+  }
+  for (int r = 0; r < 5; ++r)
+    for (int cc = 0; cc < 5; ++cc) {
+      double t = 0.0;
+      for (int k = 0; k < 5; ++k) t = t + JR[r][k] * M[k][cc];
+      g[r + 5 * cc] = area * (JL[r][cc] + t);
+    }
+}
+
 // jq: per cell its subfaces (2*sf + side) in ascending id; jblk: the block of the other
 // cell (-1 for a boundary); row_off/dblk: the row's first block and its diagonal block.
-__global__ void __launch_bounds__(64) k_be_assemble(DevMesh m, NsParams P, const double* __restrict__ U,
+// One thread per block row. The diagonal block and the block of the current neighbour
+// are accumulated in registers, entry by entry in subface order (the order of the
+// reference-style accumulation into the stored matrix), and each block is stored once
+// per run of subfaces that share a neighbour; the two-wave Jacobian is formed entry by
+// entry from the scalars of two_wave_jac. Boundary subfaces (the ghost-state chain rule)
+// take the full-matrix path.
+__global__ void __launch_bounds__(64, 6) k_be_assemble(DevMesh m, NsParams P, const double* __restrict__ U,
                                                     const int* __restrict__ jq_off, const int* __restrict__ jq,
                                                     const int* __restrict__ jblk, const int* __restrict__ row_off,
                                                     const int* __restrict__ dblk, double* __restrict__ v, double dt) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ne) return;
-  for (size_t q = (size_t)25 * row_off[c]; q < (size_t)25 * row_off[c + 1]; ++q) v[q] = 0.0;
-  double* D = v + (size_t)25 * dblk[c];
+  const int rb = row_off[c], re = row_off[c + 1], db = dblk[c];
+  const bool small = re - rb <= 64;  // first-touch bits for the row's blocks
+  if (!small)
+    for (size_t q = (size_t)25 * rb; q < (size_t)25 * re; ++q) v[q] = 0.0;
+  unsigned long long touched = 0ull;
+  double D[25], O[25];
   const double vdt = m.vol[c] / dt;
-  for (int r = 0; r < 5; ++r) D[r + 5 * r] = vdt;
+#pragma unroll
+  for (int e = 0; e < 25; ++e) {
+    D[e] = e % 6 == 0 ? vdt : 0.0;
+    O[e] = 0.0;
+  }
+  int ob = -1;  // the block O holds
+  auto flush = [&]() {
+    if (ob >= 0) {
+      double* dst = v + (size_t)25 * ob;
+#pragma unroll
+      for (int e = 0; e < 25; ++e) dst[e] = O[e];
+    }
+  };
   for (int q = jq_off[c]; q < jq_off[c + 1]; ++q) {
-    const int e = jq[q];
-    const int sf = e >> 1, side = e & 1;
+    const int e0 = jq[q];
+    const int sf = e0 >> 1, side = e0 & 1;
     const int2 lr = m.flr[m.sf_face[sf]];
     const double4 sn = m.sfn[sf];
     const double n[3] = {sn.x, sn.y, sn.z};
     const double area = sn.w;
     double wl[5], wr[5];
     reconstruct<double>(m, P, U, nullptr, m.sf_vert[sf], sf, lr.x, lr.y, false, wl, wr);
-    double JL[5][5], JR[5][5];
-    two_wave_jac(wl, wr, n, JL, JR);
-    if (side == 0) {
-      if (lr.y >= 0) {
-        for (int r = 0; r < 5; ++r)
-          for (int cc = 0; cc < 5; ++cc) D[r + 5 * cc] = D[r + 5 * cc] + area * JL[r][cc];
-        double* O = v + (size_t)25 * jblk[q];
-        for (int r = 0; r < 5; ++r)
-          for (int cc = 0; cc < 5; ++cc) O[r + 5 * cc] = O[r + 5 * cc] + area * JR[r][cc];
-      } else {  // ghost U_R(U_L): wall M = momentum reflection, outflow I, freestream 0
-        const int kind = lr.y == -1 ? 1 : P.bc_type[-(lr.y + 1) - 1];
-        double M[5][5];
-        for (int a = 0; a < 5; ++a)
-          for (int b = 0; b < 5; ++b) M[a][b] = 0.0;
-        if (kind == 1) {
-          M[0][0] = M[4][4] = 1.0;
-          for (int a = 0; a < 3; ++a)
-            for (int b = 0; b < 3; ++b) M[a + 1][b + 1] = (a == b ? 1.0 : 0.0) - 2.0 * n[a] * n[b];
-        } else if (kind == 4) {
-          for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
-        }
-        for (int r = 0; r < 5; ++r)
-          for (int cc = 0; cc < 5; ++cc) {
-            double t = 0.0;
-            for (int k = 0; k < 5; ++k) t = t + JR[r][k] * M[k][cc];
-            D[r + 5 * cc] = D[r + 5 * cc] + area * (JL[r][cc] + t);
-          }
-      }
-    } else {
-      for (int r = 0; r < 5; ++r)
-        for (int cc = 0; cc < 5; ++cc) D[r + 5 * cc] = D[r + 5 * cc] - area * JR[r][cc];
-      double* O = v + (size_t)25 * jblk[q];
-      for (int r = 0; r < 5; ++r)
-        for (int cc = 0; cc < 5; ++cc) O[r + 5 * cc] = O[r + 5 * cc] - area * JL[r][cc];
+    if (side == 0 && lr.y < 0) {
+      double g[25];
+      ghost_block(P, lr.y, wl, wr, n, area, g);
+#pragma unroll
+      for (int e = 0; e < 25; ++e) D[e] = D[e] + g[e];
+      continue;
     }
+    // the other cell's block: registers O (a new run loads what earlier runs stored)
+    const int tb = jblk[q];
+    const bool selfb = tb == db;  // a cell that neighbours itself through a periodic face
+    if (!selfb && tb != ob) {
+      flush();
+      const int bit = tb - rb;
+      if (!small || ((touched >> bit) & 1ull)) {
+        const double* src = v + (size_t)25 * tb;
+#pragma unroll
+        for (int e = 0; e < 25; ++e) O[e] = src[e];
+      } else {
+#pragma unroll
+        for (int e = 0; e < 25; ++e) O[e] = 0.0;
+      }
+      if (small) touched |= 1ull << bit;
+      ob = tb;
+    }
+    // two_wave_jac's scalars
+    const double rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], al = sound_speed_w(wl);
+    const double rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr);
+    double ul[5], ur[5];
+    p2c(wl, ul);
+    p2c(wr, ur);
+    const double lam_l = fmax2(fmax2(al * rhol, sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+    const double lam_r = fmax2(fmax2(ar * rhor, sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+    const double sl = vnl - lam_l / rhol, sr = vnr + lam_r / rhor;
+    EulerJacScalars eL, eR;
+    euler_jac_scalars(ul, n, eL);
+    euler_jac_scalars(ur, n, eR);
+    const double den = sr - sl, asl = fabs(sl), asr = fabs(sr), d = asl - asr;
+    const double rden = 1.0 / den;
+#pragma unroll
+    for (int r = 0; r < 5; ++r)
+#pragma unroll
+      for (int cc = 0; cc < 5; ++cc) {
+        const bool I = r == cc;
+        const double AL = euler_jac_entry(eL, n, r, cc), AR = euler_jac_entry(eR, n, r, cc);
+        const double dL = (AL - (I ? sl : 0.0)) * rden;
+        const double dR = ((I ? sr : 0.0) - AR) * rden;
+        const double JL = 0.5 * AL - 0.5 * (d * dL - (I ? asl : 0.0));
+        const double JR = 0.5 * AR - 0.5 * (d * dR + (I ? asr : 0.0));
+        const int e = r + 5 * cc;
+        if (side == 0) {
+          D[e] = D[e] + area * JL;
+          if (selfb) D[e] = D[e] + area * JR;
+          else O[e] = O[e] + area * JR;
+        } else {
+          D[e] = D[e] - area * JR;
+          if (selfb) D[e] = D[e] - area * JL;
+          else O[e] = O[e] - area * JL;
+        }
+      }
   }
+  flush();
+  double* dst = v + (size_t)25 * db;
+#pragma unroll
+  for (int e = 0; e < 25; ++e) dst[e] = D[e];
+  if (small)  // blocks no subface reached (none in a pattern built from the subfaces)
+    for (int b = rb; b < re; ++b)
+      if (b != db && !((touched >> (b - rb)) & 1ull))
+        for (int e = 0; e < 25; ++e) v[(size_t)25 * b + e] = 0.0;
 }
 
 // b = rhs (the first five entries of each residual record), and U += x after the solve
