@@ -1455,7 +1455,7 @@ __device__ __noinline__ void ghost_block(const NsParams& P, int y, const double*
 // per run of subfaces that share a neighbour; the two-wave Jacobian is formed entry by
 // entry from the scalars of two_wave_jac. Boundary subfaces (the ghost-state chain rule)
 // take the full-matrix path.
-__global__ void __launch_bounds__(64, 6) k_be_assemble(DevMesh m, NsParams P, const double* __restrict__ U,
+__global__ void __launch_bounds__(64) k_be_assemble(DevMesh m, NsParams P, const double* __restrict__ U,
                                                     const int* __restrict__ jq_off, const int* __restrict__ jq,
                                                     const int* __restrict__ jblk, const int* __restrict__ row_off,
                                                     const int* __restrict__ dblk, double* __restrict__ v, double dt) {
