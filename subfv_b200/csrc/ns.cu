@@ -457,11 +457,12 @@ __device__ void nodal_solve(const NsParams& P, double mat[3][3], const double* R
 // compute_rhs_around_vert (ns_euler_module.F90:341-519) for one vertex, one thread per
 // vertex; writes the corner sums of the vertex's own subcells to fs (kNsFs doubles per
 // subcell). MS bounds the vertex's subfaces and subcells (8, 16 or 32).
-// Per subface the thread keeps, from the reconstruction on, what the 4-iteration nodal
-// solver reads (left/right density, normal velocity, pressure, sound speed; normal,
-// area, boundary code), so each iteration costs only the wave-speed updates and the 3x3
-// solve; the values are the reference's (the sound speeds of :322-323 are the same
-// expressions of the same states in every iteration).
+// Per subface the thread keeps, in local arrays, only what cannot be re-read: the
+// reconstructed left/right states, the sound speeds, the two wave-speed bounds and the
+// subface and boundary ids; normals and areas are re-read from the mesh (read-only, so
+// no local-memory write-back), and vbar is recomputed from the stored bounds when the
+// next iteration needs it. The values are the reference's (the sound speeds of :322-323
+// are the same expressions of the same states in every iteration).
 constexpr int kNodeThreads = 256;  // the largest block of the node kernel
 
 // vbar = (lambda_l v_l + lambda_r v_r - (p_r - p_l)) / (lambda_r + lambda_l) (:309,316),
@@ -486,8 +487,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
   // Reconstructed primitive states (left then right) in the compute precision T: the
   // reconstruction already runs in T, so storing T loses nothing.
   T wlr[MS][10];
-  double geo[MS][4];  // subface normal and area
-  double lam[MS][3];  // lambda_l, lambda_r (values of the wave-speed precision L), vbar
+  L lam[MS][2];  // lambda_l, lambda_r
   int sfj[MS], yj[MS];
   for (int j = 0; j < nsfn; ++j) {
     const int sf = m.vsf[p0 + j];
@@ -497,12 +497,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     double w10[10];
     reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5);
     for (int k = 0; k < 10; ++k) wlr[j][k] = (T)w10[k];
-    const double4 sn = m.sfn[sf];
-    geo[j][0] = sn.x;
-    geo[j][1] = sn.y;
-    geo[j][2] = sn.z;
-    geo[j][3] = sn.w;
-    lam[j][0] = lam[j][1] = lam[j][2] = 0.0;
+    lam[j][0] = lam[j][1] = (L)0;
   }
   const bool excl = m.is_bound[v] && P.excl;
   double vn3[3] = {0.0, 0.0, 0.0};
@@ -512,7 +507,8 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
       L snd[MS][2];  // left / right sound speeds
       double Bp[3] = {0.0, 0.0, 0.0};  // wall_normal (ns_euler_primitives_module.F90:162-190)
       for (int j = 0; j < nsfn; ++j) {
-        const double* n = geo[j];
+        const double4 sn4 = m.sfn[sfj[j]];
+        const double n[4] = {sn4.x, sn4.y, sn4.z, sn4.w};
         snd[j][0] = sqrt((L)G * (L)wlr[j][4] / (L)wlr[j][0]);
         snd[j][1] = sqrt((L)G * (L)wlr[j][9] / (L)wlr[j][5]);
         const int y = yj[j];
@@ -522,7 +518,8 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
       for (int iter = 1; iter <= 4; ++iter) {
         double M6[6] = {0, 0, 0, 0, 0, 0}, Rp[3] = {0, 0, 0};
         for (int j = 0; j < nsfn; ++j) {
-          const double* n = geo[j];
+          const double4 sn4 = m.sfn[sfj[j]];
+          const double n[4] = {sn4.x, sn4.y, sn4.z, sn4.w};
           const double area = n[3];
           const L nt[3] = {(L)n[0], (L)n[1], (L)n[2]};
           L wl[5], wr[5];
@@ -532,8 +529,8 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
           }
           const L rhol = wl[0], vnl = dotT(wl + 1, nt), pl = wl[4], al = snd[j][0];
           const L rhor = wr[0], vnr = dotT(wr + 1, nt), pr = wr[4], ar = snd[j][1];
-          L lam_l = (L)lam[j][0], lam_r = (L)lam[j][1];
-          double vbar = lam[j][2];
+          L lam_l = lam[j][0], lam_r = lam[j][1];
+          double vbar = 0.0;
           // the flux's own normal velocities and pressures (precision T), for vbar
           const T ntT[3] = {(T)n[0], (T)n[1], (T)n[2]};
           const double vnl_f = (double)dotT(wlr[j] + 1, ntT), vnr_f = (double)dotT(wlr[j] + 6, ntT);
@@ -547,6 +544,8 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
             lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -((L)vbar - vnl) / al)));
             lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, ((L)vbar - vnr) / ar)));
           } else if (wall && P.bc_style == 1) {
+            // the previous iteration's vbar, from the bounds it ended with
+            vbar = vbar_of((double)lam_l, (double)lam_r, vnl_f, vnr_f, pl_f, pr_f);
             lam_l = tmax2(lam_l, al * rhol * (c1 + c15 * tmax2(c0, -((L)vbar - vnl) / al)));
             lam_r = tmax2(lam_r, ar * rhor * (c1 + c15 * tmax2(c0, ((L)vbar - vnr) / ar)));
           } else {
@@ -557,7 +556,6 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
           vbar = vbar_of((double)lam_l, (double)lam_r, vnl_f, vnr_f, pl_f, pr_f);
           lam[j][0] = lam_l;
           lam[j][1] = lam_r;
-          lam[j][2] = vbar;
           const double lsum = (double)lam_r + (double)lam_l;
           if (!wall || P.bc_style == 0 || P.bc_style == 2) {  // M += (lam_r + lam_l) A n n^T
             const double w = lsum * area;
@@ -591,7 +589,8 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     const int sf = sfj[j];
     const int2 se = m.sf_se[sf];
     const int lse_loc = m.se_loc[se.x];
-    const double* n = geo[j];
+    const double4 sn4 = m.sfn[sf];
+    const double n[4] = {sn4.x, sn4.y, sn4.z, sn4.w};
     double w10[10];
     for (int k = 0; k < 10; ++k) w10[k] = (double)wlr[j][k];
     double lr[2][5], sl, sr;
