@@ -142,6 +142,18 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _fp64_peak():
+    """FP64 FMA issue rate of this GPU (subfv_probe_fp64_fma: eight independent FMA chains
+    per thread at full occupancy), measured after the timed region; the denominator of
+    the FP64 fractions in profiles/."""
+    import ctypes as C
+    from subfv_b200 import _lib
+    tf, ms = C.c_double(), C.c_double()
+    if _lib.load().subfv_probe_fp64_fma(4096, C.byref(tf), C.byref(ms)) != 0:
+        return None
+    return {"peak_tflops": tf.value, "probe_ms": ms.value, "how": "fma.rn.f64, 8 chains/thread, 8 blocks x 256 per SM"}
+
+
 def _traffic(kernel):
     """dram read+write bytes per launch from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "lagrange_step_traffic.json"
@@ -635,6 +647,7 @@ def main():
                          "traffic": _traffic(dom), "algorithmic_bytes": kb[dom],
                          "kernel_ms": per[dom], "step_achieved_gbs": step_achieved},
             "kernel_ms": per,
+            "fp64": _fp64_peak(),
             "cpu_baseline": cpu,
         }
         print(json.dumps(out), flush=True)

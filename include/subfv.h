@@ -29,6 +29,11 @@ extern "C" {
 
 const char* subfv_last_error(void);
 int subfv_version(void);
+/* FP64 issue-rate probe (no counterpart in the reference): times fused multiply-adds
+ * in eight independent chains per thread over the whole current device and returns the
+ * achieved TFLOP/s (2 flops per FMA), the denominator of the FP64 fraction reported
+ * for FP64-bound kernels. iters in [1, 2^20]; ~4096 takes a few milliseconds. */
+int subfv_probe_fp64_fma(int iters, double* tflops, double* ms);
 
 /* ---------------------------------------------------------------------------------
  * Topology: build_mesh (src/mesh/mesh_connectivity_module.F90:12-59) on the host,
