@@ -54,6 +54,7 @@ def load():
         lib.or_ns_run.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_int, C.c_double, PD, PI, PD, PD, PD]
         lib.or_ns_gresho.argtypes = [C.c_void_p, C.c_double, PD]
         lib.or_pinv3.argtypes = [PD]
+        lib.or_ns_flux.argtypes = [C.c_int, PD, PD, PD, PD, PD]
         lib.or_lu3.argtypes = [PD, PD, PD]
         lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]

@@ -23,7 +23,7 @@ namespace oracle {
 static const double G = 1.4;  // ns_global_data_module.F90:9
 
 struct NsCfg {
-  int scheme;          // 1 multi_point, 4 two_wave
+  int scheme;          // 1 multi_point, 3 three_wave, 4 two_wave, 5 modified_three_wave
   int second_order;    // 0/1
   int method;          // 0/1 (no gradient) or 4
   int bc_style;        // 0, 1, 2
@@ -220,6 +220,66 @@ static void two_wave(const double* wl, const double* wr, const double* n, double
   for (int k = 0; k < 5; ++k) {
     double et = (*sr * ur[k] - *sl * ul[k] - (fr[k] - fl[k])) / (*sr - *sl);
     lr[0][k] = 0.5 * (fl[k] + fr[k]) - 0.5 * (std::fabs(*sl) * (et - ul[k]) + std::fabs(*sr) * (ur[k] - et));
+    lr[1][k] = -lr[0][k];
+  }
+}
+
+// three_wave (:9-75) and modified_three_wave (:77-152): the two-wave bounds, v* = v_bar,
+// HLLC-type star states (the modified form also averages the tangential velocity and
+// carries its jump energy), no nodal solve.
+static void three_wave(const double* wl, const double* wr, const double* n, double lr[2][5], double* sl, double* sr,
+                       bool modified) {
+  double rhol = wl[0], vnl = dot3(wl + 1, n), pl = wl[4], ul[5];
+  p2c(wl, ul);
+  double el = ul[4] / rhol, al = sound_speed_w(wl);
+  double rhor = wr[0], vnr = dot3(wr + 1, n), pr = wr[4], ur[5];
+  p2c(wr, ur);
+  double er = ur[4] / rhor, ar = sound_speed_w(wr);
+  double fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  double lam_l = fmax2(fmax2(al * rhol, std::sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+  double lam_r = fmax2(fmax2(ar * rhor, std::sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+  double v_et = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+  double vt_et[3] = {0.0, 0.0, 0.0}, tang_energy = 0.0;
+  if (modified) {
+    double vt_l[3], vt_r[3], dvt[3];
+    for (int d = 0; d < 3; ++d) {
+      vt_l[d] = wl[1 + d] - vnl * n[d];
+      vt_r[d] = wr[1 + d] - vnr * n[d];
+    }
+    for (int d = 0; d < 3; ++d) vt_et[d] = (lam_l * vt_l[d] + lam_r * vt_r[d]) / (lam_l + lam_r);
+    for (int d = 0; d < 3; ++d) dvt[d] = vt_r[d] - vt_l[d];
+    double tang_coeff = -(lam_l * lam_r / (lam_l + lam_r));
+    tang_energy = tang_coeff * dot3(dvt, vt_et);
+  }
+  double rhol_et = 1.0 / (1.0 / rhol + (v_et - vnl) / lam_l);
+  double pl_bar = pl - lam_l * (v_et - vnl);
+  double rhor_et = 1.0 / (1.0 / rhor + (vnr - v_et) / lam_r);
+  double pr_bar = pr + lam_r * (v_et - vnr);
+  double sle[5], sre[5];
+  sle[0] = rhol_et;
+  sre[0] = rhor_et;
+  if (modified) {
+    for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (v_et * n[k - 1] + vt_et[k - 1]);
+    sle[4] = rhol_et * (el + (pl * vnl - pl_bar * v_et - tang_energy) / lam_l);
+    for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (v_et * n[k - 1] + vt_et[k - 1]);
+    sre[4] = rhor_et * (er + (pr_bar * v_et - pr * vnr + tang_energy) / lam_r);
+  } else {
+    for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (wl[k] + (v_et - vnl) * n[k - 1]);
+    sle[4] = rhol_et * (el + (pl * vnl - pl_bar * v_et) / lam_l);
+    for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (wr[k] + (v_et - vnr) * n[k - 1]);
+    sre[4] = rhor_et * (er + (pr_bar * v_et - pr * vnr) / lam_r);
+  }
+  *sl = vnl - lam_l / rhol;
+  *sr = vnr + lam_r / rhor;
+  for (int k = 0; k < 5; ++k) {
+    lr[0][k] = 0.5 * (fl[k] + fr[k]) - 0.5 * (std::fabs(*sl) * (sle[k] - ul[k]) + std::fabs(v_et) * (sre[k] - sle[k]) +
+                                              std::fabs(*sr) * (ur[k] - sre[k]));
     lr[1][k] = -lr[0][k];
   }
 }
@@ -538,7 +598,8 @@ static void nodal_velocity(const Mesh& m, const NsCfg& cfg, int v, const std::ve
   }
 }
 
-// ns_euler_module.F90:151-339 (scheme_id multi_point or two_wave) + :341-519
+// ns_euler_module.F90:151-339 (scheme_id multi_point, three_wave, two_wave or
+// modified_three_wave) + :341-519
 static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol, double* rhs, const double* grad,
                               double* sum_lambda, bool so, double* vp) {
   for (int i = 0; i < 5 * m.n_elems; ++i) rhs[i] = 0.0;
@@ -578,6 +639,8 @@ static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol
         double vn = is_wall(cfg, re) ? 0.0 : dot3(vv3, n);
         if (!multi_point(&wlr[10 * j], &wlr[10 * j + 5], n, lr, vn, lam[2 * j], lam[2 * j + 1], &sl, &sr))
           status |= 4;
+      } else if (cfg.scheme == 3 || cfg.scheme == 5) {
+        three_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr, &sl, &sr, cfg.scheme == 5);
       } else {
         two_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr, &sl, &sr);
       }
@@ -949,6 +1012,16 @@ int or_ns_run(void* h, const int* ic, const double* dc, const int* bc_type, cons
 }
 void or_ns_gresho(void* h, double mach, double* sol) { init_gresho(handle_mesh(h), mach, sol); }
 void or_pinv3(double* a9) { oracle_pinv3(a9); }
+// one subface flux: scheme 3 three_wave, 5 modified_three_wave, else two_wave; lr (5, 2)
+void or_ns_flux(int scheme, const double* wl, const double* wr, const double* n, double* lr10, double* slsr) {
+  double lr[2][5];
+  if (scheme == 3 || scheme == 5) three_wave(wl, wr, n, lr, &slsr[0], &slsr[1], scheme == 5);
+  else two_wave(wl, wr, n, lr, &slsr[0], &slsr[1]);
+  for (int k = 0; k < 5; ++k) {
+    lr10[k] = lr[0][k];
+    lr10[5 + k] = lr[1][k];
+  }
+}
 // returns nnz blocks; row (n_elems+1), col (nnz) 1-based, v (25 nnz); cap = capacity of col
 long or_be_jacobian(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val,
                     const double* sol, double dt, int* row, int* col, double* v, long cap) {

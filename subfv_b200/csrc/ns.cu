@@ -361,6 +361,76 @@ __device__ void two_wave(const double* wl64, const double* wr64, const double* n
   *sr_o = (double)sr;
 }
 
+// three_wave (ns_euler_rs_module.F90:9-75) and modified_three_wave (:77-152): two-wave
+// bounds, v* = v_bar, HLLC-type star states (the modified form averages the tangential
+// velocity and carries its jump energy); arithmetic in T, results stored as double.
+template <class T>
+__device__ void three_wave(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
+                           double* sl_o, double* sr_o, bool modified) {
+  T wl[5], wr[5], n[3];
+  for (int k = 0; k < 5; ++k) {
+    wl[k] = (T)wl64[k];
+    wr[k] = (T)wr64[k];
+  }
+  for (int d = 0; d < 3; ++d) n[d] = (T)n64[d];
+  const T c0 = (T)0, c1 = (T)1, ch = (T)0.5;
+  T rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], ul[5];
+  p2c(wl, ul);
+  T el = ul[4] / rhol, al = sqrt((T)G * wl[4] / wl[0]);
+  T rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ur[5];
+  p2c(wr, ur);
+  T er = ur[4] / rhor, ar = sqrt((T)G * wr[4] / wr[0]);
+  T fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  T lam_l = tmax2(tmax2(al * rhol, sqrt(rhol * tmax2(c0, pr - pl))), -rhol * (vnr - vnl));
+  T lam_r = tmax2(tmax2(ar * rhor, sqrt(rhor * tmax2(c0, pl - pr))), -rhor * (vnr - vnl));
+  T v_et = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+  T vt_et[3] = {c0, c0, c0}, tang_energy = c0;
+  if (modified) {
+    T vt_l[3], vt_r[3], dvt[3];
+    for (int d = 0; d < 3; ++d) {
+      vt_l[d] = wl[1 + d] - vnl * n[d];
+      vt_r[d] = wr[1 + d] - vnr * n[d];
+    }
+    for (int d = 0; d < 3; ++d) vt_et[d] = (lam_l * vt_l[d] + lam_r * vt_r[d]) / (lam_l + lam_r);
+    for (int d = 0; d < 3; ++d) dvt[d] = vt_r[d] - vt_l[d];
+    const T tang_coeff = -(lam_l * lam_r / (lam_l + lam_r));
+    tang_energy = tang_coeff * dotT(dvt, vt_et);
+  }
+  T rhol_et = c1 / (c1 / rhol + (v_et - vnl) / lam_l);
+  T pl_bar = pl - lam_l * (v_et - vnl);
+  T rhor_et = c1 / (c1 / rhor + (vnr - v_et) / lam_r);
+  T pr_bar = pr + lam_r * (v_et - vnr);
+  T sle[5], sre[5];
+  sle[0] = rhol_et;
+  sre[0] = rhor_et;
+  if (modified) {
+    for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (v_et * n[k - 1] + vt_et[k - 1]);
+    sle[4] = rhol_et * (el + (pl * vnl - pl_bar * v_et - tang_energy) / lam_l);
+    for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (v_et * n[k - 1] + vt_et[k - 1]);
+    sre[4] = rhor_et * (er + (pr_bar * v_et - pr * vnr + tang_energy) / lam_r);
+  } else {
+    for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (wl[k] + (v_et - vnl) * n[k - 1]);
+    sle[4] = rhol_et * (el + (pl * vnl - pl_bar * v_et) / lam_l);
+    for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (wr[k] + (v_et - vnr) * n[k - 1]);
+    sre[4] = rhor_et * (er + (pr_bar * v_et - pr * vnr) / lam_r);
+  }
+  const T sl = vnl - lam_l / rhol, sr = vnr + lam_r / rhor;
+  for (int k = 0; k < 5; ++k) {
+    const T f = ch * (fl[k] + fr[k]) -
+                ch * (fabs(sl) * (sle[k] - ul[k]) + fabs(v_et) * (sre[k] - sle[k]) + fabs(sr) * (ur[k] - sre[k]));
+    lr[0][k] = (double)f;
+    lr[1][k] = (double)(-f);
+  }
+  *sl_o = (double)sl;
+  *sr_o = (double)sr;
+}
+
 // multi_point (ns_euler_rs_module.F90:200-286); false on a negative star density
 template <class T>
 __device__ bool multi_point(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
@@ -597,6 +667,8 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     if (P.scheme == 1 && !excl) {
       const double vn = is_wall(P, yj[j]) ? 0.0 : dotT(vn3, n);
       if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam[j][0], (double)lam[j][1], &sl, &sr)) bad = true;
+    } else if (P.scheme == 3 || P.scheme == 5) {
+      three_wave<T>(w10, w10 + 5, n, lr, &sl, &sr, P.scheme == 5);
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
@@ -790,6 +862,8 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
       const double vn = is_wall(P, y) ? 0.0 : dotT(vn3, n);
       if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam_l, (double)lam_r, &sl, &sr))
         atomicOr(m.status, kErrNegDensity);
+    } else if (P.scheme == 3 || P.scheme == 5) {
+      three_wave<T>(w10, w10 + 5, n, lr, &sl, &sr, P.scheme == 5);
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }

@@ -22,6 +22,10 @@ CFGS = {
     "mp_o1_bc1": dict(scheme=1, second_order=False, method=4, bc_style=1),
     "mp_o1_bc0": dict(scheme=1, second_order=False, method=4, bc_style=0),
     "tw_o2": dict(scheme=4, second_order=True, method=4, bc_style=2),
+    "3w_o1": dict(scheme=3, second_order=False, method=4, bc_style=2),
+    "3w_o2": dict(scheme=3, second_order=True, method=4, bc_style=2),
+    "m3w_o1": dict(scheme=5, second_order=False, method=4, bc_style=2),
+    "m3w_o2": dict(scheme=5, second_order=True, method=4, bc_style=2),
 }
 
 
@@ -64,7 +68,7 @@ def test_gresho_init_matches_oracle(native, oracle_lib, cuda_ok):
     np.testing.assert_array_equal(init_gresho(m, 0.1), o.ns_gresho(0.1))
 
 
-@pytest.mark.parametrize("cfg_name", ["mp_o2_bc2", "tw_o2", "mp_o1_bc1"])
+@pytest.mark.parametrize("cfg_name", ["mp_o2_bc2", "tw_o2", "mp_o1_bc1", "3w_o2", "m3w_o2"])
 def test_ns_time_loop_bit_exact(native, oracle_lib, cuda_ok, cfg_name):
     from subfv_b200.ns import NsConfig, NsState, init_gresho
     m, o = _pair(_meshes()["hex_slab"])
