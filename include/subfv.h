@@ -157,8 +157,8 @@ void* subfv_mesh_stream(subfv_mesh* m);
  * add_timedisc_and_solve, first order or the two-stage scheme of ns_main.F90:83-107.
  * Conservative state sol(5, n_elems) = (rho, rho u, rho v, rho w, E). */
 typedef struct subfv_ns_cfg {
-  int32_t scheme;             /* 1 multi_point, 3 three_wave, 4 two_wave, 5 modified_three_wave
-                                 (ns_global_data_module.F90:67-71) */
+  int32_t scheme;             /* 1 multi_point, 2 multi_point_iso, 3 three_wave, 4 two_wave,
+                                 5 modified_three_wave (ns_global_data_module.F90:67-71) */
   int32_t second_order;       /* 0 / 1 */
   int32_t method;             /* cell gradient: 0 or 1 (none), 4 (ns_euler_recon_module.F90:200-240) */
   int32_t bc_style;           /* 0, 1, 2 */

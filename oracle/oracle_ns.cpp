@@ -23,7 +23,7 @@ namespace oracle {
 static const double G = 1.4;  // ns_global_data_module.F90:9
 
 struct NsCfg {
-  int scheme;          // 1 multi_point, 3 three_wave, 4 two_wave, 5 modified_three_wave
+  int scheme;          // 1 multi_point, 2 multi_point_iso, 3 three_wave, 4 two_wave, 5 modified_three_wave
   int second_order;    // 0/1
   int method;          // 0/1 (no gradient) or 4
   int bc_style;        // 0, 1, 2
@@ -553,17 +553,20 @@ static void nodal_velocity(const Mesh& m, const NsCfg& cfg, int v, const std::ve
       lam[2 * j + 1] = lam_r;
       vbar[j] = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
       bool wall = is_wall(cfg, re);
+      // multi_point_iso (compute_lambdas_and_solve_nodal_velocity_iso, :424-553) drops
+      // the subface area from M and R
+      const bool iso = cfg.scheme == 2;
       if (!wall || cfg.bc_style == 0 || cfg.bc_style == 2) {
-        double w = (lam_r + lam_l) * area;
+        double w = iso ? (lam_r + lam_l) : (lam_r + lam_l) * area;
         for (int d = 0; d < 3; ++d)
           for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + w * (n[d] * n[e]);
       }
       if (!wall || cfg.bc_style == 0) {
-        double q = area * (lam_r + lam_l) * vbar[j];
+        double q = iso ? (lam_r + lam_l) * vbar[j] : area * (lam_r + lam_l) * vbar[j];
         for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
       } else if (cfg.bc_style == 2) {
         if (!cfg.b2d || std::fabs(n[2]) < 1e-8) {
-          double q = area * pl;
+          double q = iso ? pl : area * pl;
           for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
         }
       }
@@ -614,14 +617,16 @@ static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol
     vbar.assign(nsfn, 0.0);
     fsv.assign(5 * nsen, 0.0);
     slv.assign(nsen, 0.0);
+    double amin = 0.0;  // minval of the subface areas (warea, ns_euler_module.F90:386-397)
     for (int j = 0; j < nsfn; ++j) {
       int sf = vv.sub_face_neigh[j + 1];
       const Face& f = m.face[m.sub_face[sf].mesh_face];
       reconstruct_lr_w(m, cfg, sol, grad, v, sf, f.left_neigh, f.right_neigh, so, &wlr[10 * j], &wlr[10 * j + 5]);
+      amin = j == 0 ? m.sub_face[sf].area : fmin2(amin, m.sub_face[sf].area);
     }
     double vv3[3] = {0, 0, 0};
     bool excl = vv.is_bound && cfg.exclude_bound_vert;
-    if (cfg.scheme == 1) {
+    if (cfg.scheme == 1 || cfg.scheme == 2) {
       if (!excl) nodal_velocity(m, cfg, v, wlr, lam, vbar, vv3);
       for (int d = 0; d < 3; ++d) vp[3 * (v - 1) + d] = vv3[d];
     }
@@ -635,7 +640,7 @@ static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol
       if (rse > 0) rse_loc = m.sub_elem[rse].id_loc_around_node;
       double lr[2][5], sl, sr;
       const double* n = &s.norm[1];
-      if (cfg.scheme == 1 && !excl) {
+      if ((cfg.scheme == 1 || cfg.scheme == 2) && !excl) {
         double vn = is_wall(cfg, re) ? 0.0 : dot3(vv3, n);
         if (!multi_point(&wlr[10 * j], &wlr[10 * j + 5], n, lr, vn, lam[2 * j], lam[2 * j + 1], &sl, &sr))
           status |= 4;
@@ -643,6 +648,13 @@ static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol
         three_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr, &sl, &sr, cfg.scheme == 5);
       } else {
         two_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr, &sl, &sr);
+      }
+      if (cfg.scheme == 2) {  // blend with three_wave by warea = min area / area; sl, sr from three_wave
+        double lr3[2][5];
+        three_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr3, &sl, &sr, false);
+        const double wa = amin / s.area;
+        for (int q = 0; q < 2; ++q)
+          for (int k = 0; k < 5; ++k) lr[q][k] = wa * lr[q][k] + (1.0 - wa) * lr3[q][k];
       }
       if (m.sub_elem[lse].mesh_vert == v) {
         slv[lse_loc - 1] = slv[lse_loc - 1] + s.area * fmax2(0.0, -sl);

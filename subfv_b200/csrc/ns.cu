@@ -431,6 +431,19 @@ __device__ void three_wave(const double* wl64, const double* wr64, const double*
   *sr_o = (double)sr;
 }
 
+// multi_point_iso's flux (ns_euler_module.F90:464-483): the multi-point (or, at an
+// excluded boundary vertex, two-wave) flux blended with three_wave by
+// warea = min area / area; the wave speeds sl, sr are three_wave's.
+template <class T>
+__device__ void blend_three_wave(const double* w10, const double* n, double amin, double lr[2][5], double* sl,
+                                 double* sr) {
+  double lr3[2][5];
+  three_wave<T>(w10, w10 + 5, n, lr3, sl, sr, false);
+  const double wa = amin / n[3];
+  for (int q = 0; q < 2; ++q)
+    for (int k = 0; k < 5; ++k) lr[q][k] = wa * lr[q][k] + (1.0 - wa) * lr3[q][k];
+}
+
 // multi_point (ns_euler_rs_module.F90:200-286); false on a negative star density
 template <class T>
 __device__ bool multi_point(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
@@ -559,19 +572,22 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
   T wlr[MS][10];
   L lam[MS][2];  // lambda_l, lambda_r
   int sfj[MS], yj[MS];
+  double amin = 0.0;  // minval of the subface areas (warea of multi_point_iso, ns_euler_module.F90:386-397)
   for (int j = 0; j < nsfn; ++j) {
     const int sf = m.vsf[p0 + j];
     const int2 lr = m.flr[m.sf_face[sf]];
     sfj[j] = sf;
     yj[j] = lr.y;
+    if (P.scheme == 2) amin = j == 0 ? m.sfn[sf].w : fmin2(amin, m.sfn[sf].w);
     double w10[10];
     reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5);
     for (int k = 0; k < 10; ++k) wlr[j][k] = (T)w10[k];
     lam[j][0] = lam[j][1] = (L)0;
   }
   const bool excl = m.is_bound[v] && P.excl;
+  const bool iso = P.scheme == 2;  // multi_point_iso: M and R without the subface areas (:424-553)
   double vn3[3] = {0.0, 0.0, 0.0};
-  if (P.scheme == 1) {
+  if (P.scheme == 1 || iso) {
     if (!excl) {  // compute_lambdas_and_solve_nodal_velocity (ns_euler_rs_module.F90:288-422)
       // wave-speed bounds and vbar in L; M, R and the 3x3 solve in FP64
       L snd[MS][2];  // left / right sound speeds
@@ -628,7 +644,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
           lam[j][1] = lam_r;
           const double lsum = (double)lam_r + (double)lam_l;
           if (!wall || P.bc_style == 0 || P.bc_style == 2) {  // M += (lam_r + lam_l) A n n^T
-            const double w = lsum * area;
+            const double w = iso ? lsum : lsum * area;
             M6[0] = M6[0] + w * (n[0] * n[0]);
             M6[1] = M6[1] + w * (n[0] * n[1]);
             M6[2] = M6[2] + w * (n[0] * n[2]);
@@ -637,10 +653,10 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
             M6[5] = M6[5] + w * (n[2] * n[2]);
           }
           if (!wall || P.bc_style == 0) {
-            const double q = area * lsum * vbar;
+            const double q = iso ? lsum * vbar : area * lsum * vbar;
             for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
           } else if (P.bc_style == 2 && (!P.b2d || fabs(n[2]) < 1e-8)) {
-            const double q = area * (double)pl;
+            const double q = iso ? (double)pl : area * (double)pl;
             for (int d = 0; d < 3; ++d) Rp[d] = Rp[d] + q * n[d];
           }
         }
@@ -664,7 +680,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     double w10[10];
     for (int k = 0; k < 10; ++k) w10[k] = (double)wlr[j][k];
     double lr[2][5], sl, sr;
-    if (P.scheme == 1 && !excl) {
+    if ((P.scheme == 1 || iso) && !excl) {
       const double vn = is_wall(P, yj[j]) ? 0.0 : dotT(vn3, n);
       if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam[j][0], (double)lam[j][1], &sl, &sr)) bad = true;
     } else if (P.scheme == 3 || P.scheme == 5) {
@@ -672,6 +688,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
+    if (iso) blend_three_wave<T>(w10, n, amin, lr, &sl, &sr);
     if (m.se_vert[se.x] == v && lse_loc < nsen) {
       const double area = n[3];
       fsv[lse_loc][5] = fsv[lse_loc][5] + area * fmax2(0.0, -sl);
@@ -762,8 +779,14 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
   const bool excl = act && m.is_bound[v] && P.excl;
   double vn3[3] = {0.0, 0.0, 0.0};
   L lam_l = (L)0, lam_r = (L)0;
-  const bool solve = P.scheme == 1 && act && !excl;
-  if (P.scheme == 1) {  // uniform over the launch: every lane takes the same syncs
+  const bool iso = P.scheme == 2;
+  const bool solve = (P.scheme == 1 || iso) && act && !excl;
+  double amin = 0.0;  // minval of the group's subface areas (exact in any order)
+  if (iso) {
+    amin = mine ? n[3] : (double)INFINITY;
+    for (int o = NG / 2; o > 0; o >>= 1) amin = fmin2(amin, __shfl_xor_sync(mask, amin, o, NG));
+  }
+  if (P.scheme == 1 || iso) {  // uniform over the launch: every lane takes the same syncs
     L al = (L)0, ar = (L)0;
     if (mine) {
       al = sqrt((L)G * (L)w[4] / (L)w[0]);
@@ -817,7 +840,7 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
         const double lsum = (double)lam_r + (double)lam_l;
         double* c = gv + j * kLaneVals;
         if (!wall || P.bc_style == 0 || P.bc_style == 2) {
-          const double wgt = lsum * area;
+          const double wgt = iso ? lsum : lsum * area;
           c[0] = wgt * (n[0] * n[0]);
           c[1] = wgt * (n[0] * n[1]);
           c[2] = wgt * (n[0] * n[2]);
@@ -827,11 +850,11 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
           f |= 0x3fu;
         }
         if (!wall || P.bc_style == 0) {
-          const double q = area * lsum * vbar;
+          const double q = iso ? lsum * vbar : area * lsum * vbar;
           for (int d = 0; d < 3; ++d) c[6 + d] = q * n[d];
           f |= 0x1c0u;
         } else if (P.bc_style == 2 && (!P.b2d || fabs(n[2]) < 1e-8)) {
-          const double q = area * (double)pl;
+          const double q = iso ? (double)pl : area * (double)pl;
           for (int d = 0; d < 3; ++d) c[6 + d] = q * n[d];
           f |= 0x1c0u;
         }
@@ -867,6 +890,7 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
+    if (iso) blend_three_wave<T>(w10, n, amin, lr, &sl, &sr);
     if (m.se_vert[se.x] == v && lse_loc < nsen) {
       const double area = n[3];
       double* c = gv + j * kLaneVals;

@@ -26,6 +26,9 @@ CFGS = {
     "3w_o2": dict(scheme=3, second_order=True, method=4, bc_style=2),
     "m3w_o1": dict(scheme=5, second_order=False, method=4, bc_style=2),
     "m3w_o2": dict(scheme=5, second_order=True, method=4, bc_style=2),
+    "iso_o1_bc2": dict(scheme=2, second_order=False, method=4, bc_style=2),
+    "iso_o2_bc2": dict(scheme=2, second_order=True, method=4, bc_style=2),
+    "iso_o1_bc0": dict(scheme=2, second_order=False, method=4, bc_style=0),
 }
 
 
@@ -56,7 +59,7 @@ def test_compute_rhs_ns_bit_exact(native, oracle_lib, cuda_ok, mesh_name, cfg_na
     assert st == st_o == 0
     np.testing.assert_array_equal(sl, sl_o)
     np.testing.assert_array_equal(rhs, rhs_o)
-    if cfg.scheme == 1:
+    if cfg.scheme in (1, 2):
         np.testing.assert_array_equal(vp, vp_o)
     # oracle grad rows are [d*5 + var]; product (5, 3) per cell is grad(d, var) at [var, d]
     np.testing.assert_array_equal(grad.transpose(0, 2, 1).reshape(-1, 15), grad_o)
@@ -68,7 +71,7 @@ def test_gresho_init_matches_oracle(native, oracle_lib, cuda_ok):
     np.testing.assert_array_equal(init_gresho(m, 0.1), o.ns_gresho(0.1))
 
 
-@pytest.mark.parametrize("cfg_name", ["mp_o2_bc2", "tw_o2", "mp_o1_bc1", "3w_o2", "m3w_o2"])
+@pytest.mark.parametrize("cfg_name", ["mp_o2_bc2", "tw_o2", "mp_o1_bc1", "3w_o2", "m3w_o2", "iso_o2_bc2"])
 def test_ns_time_loop_bit_exact(native, oracle_lib, cuda_ok, cfg_name):
     from subfv_b200.ns import NsConfig, NsState, init_gresho
     m, o = _pair(_meshes()["hex_slab"])
