@@ -158,7 +158,8 @@ void* subfv_mesh_stream(subfv_mesh* m);
  * Conservative state sol(5, n_elems) = (rho, rho u, rho v, rho w, E). */
 typedef struct subfv_ns_cfg {
   int32_t scheme;             /* 1 multi_point, 2 multi_point_iso, 3 three_wave, 4 two_wave,
-                                 5 modified_three_wave (ns_global_data_module.F90:67-71) */
+                                 5 modified_three_wave, 6 multi_point_pressure,
+                                 8 multi_point_pressure_ph (ns_global_data_module.F90:67-73) */
   int32_t second_order;       /* 0 / 1 */
   int32_t method;             /* cell gradient: 0 or 1 (none), 4 (ns_euler_recon_module.F90:200-240) */
   int32_t bc_style;           /* 0, 1, 2 */

@@ -23,7 +23,7 @@ namespace oracle {
 static const double G = 1.4;  // ns_global_data_module.F90:9
 
 struct NsCfg {
-  int scheme;          // 1 multi_point, 2 multi_point_iso, 3 three_wave, 4 two_wave, 5 modified_three_wave
+  int scheme;  // 1 multi_point, 2 _iso, 3 three_wave, 4 two_wave, 5 modified_three_wave, 6/8 multi_point_pressure(_ph)
   int second_order;    // 0/1
   int method;          // 0/1 (no gradient) or 4
   int bc_style;        // 0, 1, 2
@@ -279,6 +279,46 @@ static void three_wave(const double* wl, const double* wr, const double* n, doub
   *sr = vnr + lam_r / rhor;
   for (int k = 0; k < 5; ++k) {
     lr[0][k] = 0.5 * (fl[k] + fr[k]) - 0.5 * (std::fabs(*sl) * (sle[k] - ul[k]) + std::fabs(v_et) * (sre[k] - sle[k]) +
+                                              std::fabs(*sr) * (ur[k] - sre[k]));
+    lr[1][k] = -lr[0][k];
+  }
+}
+
+// multi_point_pressure (:555-616) and multi_point_pressure_ph (:618-679): star states from
+// the nodal pressure p_nodal and the bounds of the nodal pressure solver
+static void multi_point_pressure(const double* wl, const double* wr, const double* n, double lr[2][5],
+                                 double p_nodal, double lam_l, double lam_r, double* sl, double* sr, bool ph) {
+  double rhol = wl[0], vnl = dot3(wl + 1, n), pl = wl[4], ul[5], vt_l[3];
+  for (int d = 0; d < 3; ++d) vt_l[d] = wl[1 + d] - vnl * n[d];
+  p2c(wl, ul);
+  double el = ul[4] / rhol;
+  double rhor = wr[0], vnr = dot3(wr + 1, n), pr = wr[4], ur[5], vt_r[3];
+  for (int d = 0; d < 3; ++d) vt_r[d] = wr[1 + d] - vnr * n[d];
+  p2c(wr, ur);
+  double er = ur[4] / rhor;
+  double fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  double vn_bar = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+  double vn_l_et = vnl - (p_nodal - pl) / lam_l;
+  double rhol_et = 1.0 / (1.0 / rhol + (vn_bar - vnl) / lam_l);
+  double sle[5], sre[5];
+  sle[0] = rhol_et;
+  for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (vt_l[k - 1] + vn_l_et * n[k - 1]);
+  sle[4] = rhol_et * (el + (pl * vnl - p_nodal * (ph ? vn_l_et : vn_bar)) / lam_l);
+  double vn_r_et = vnr + (p_nodal - pr) / lam_r;
+  double rhor_et = 1.0 / (1.0 / rhor + (vnr - vn_bar) / lam_r);
+  sre[0] = rhor_et;
+  for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (vt_r[k - 1] + vn_r_et * n[k - 1]);
+  sre[4] = rhor_et * (er + (p_nodal * (ph ? vn_r_et : vn_bar) - pr * vnr) / lam_r);
+  *sl = vnl - lam_l / rhol;
+  *sr = vnr + lam_r / rhor;
+  for (int k = 0; k < 5; ++k) {
+    lr[0][k] = 0.5 * (fl[k] + fr[k]) - 0.5 * (std::fabs(*sl) * (sle[k] - ul[k]) + std::fabs(vn_bar) * (sre[k] - sle[k]) +
                                               std::fabs(*sr) * (ur[k] - sre[k]));
     lr[1][k] = -lr[0][k];
   }
@@ -601,8 +641,56 @@ static void nodal_velocity(const Mesh& m, const NsCfg& cfg, int v, const std::ve
   }
 }
 
-// ns_euler_module.F90:151-339 (scheme_id multi_point, three_wave, two_wave or
-// modified_three_wave) + :341-519
+// compute_lambdas_and_solve_nodal_pressure (ns_euler_rs_module.F90:681-758): ten
+// fixed-point iterations of p_node = s1 / s2 over the vertex's subfaces
+static double nodal_pressure(const Mesh& m, const NsCfg& cfg, int v, const std::vector<double>& wlr,
+                             std::vector<double>& lam) {
+  const Vert& vv = m.vert[v];
+  int nsfn = vv.n_sub_faces_neigh;
+  std::vector<double> pbar(nsfn, 0.0);
+  double p_node = 0.0;
+  for (int iter = 1; iter <= 10; ++iter) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < nsfn; ++j) {
+      int sf = vv.sub_face_neigh[j + 1];
+      int re = m.face[m.sub_face[sf].mesh_face].right_neigh;
+      const double* n = &m.sub_face[sf].norm[1];
+      double area = m.sub_face[sf].area;
+      const double* wl = &wlr[10 * j];
+      const double* wr = &wlr[10 * j + 5];
+      double rhol = wl[0], vnl = dot3(wl + 1, n), pl = wl[4], al = sound_speed_w(wl);
+      double rhor = wr[0], vnr = dot3(wr + 1, n), pr = wr[4], ar = sound_speed_w(wr);
+      double lam_l = lam[2 * j], lam_r = lam[2 * j + 1];
+      const bool wall1 = cfg.bc_style == 1 && is_wall(cfg, re);
+      if (iter == 1) {
+        lam_l = fmax2(fmax2(fmax2(lam_l, al * rhol), std::sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+        lam_r = fmax2(fmax2(fmax2(lam_r, ar * rhor), std::sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+        pbar[j] = (lam_r * pl + lam_l * pr - lam_r * lam_l * (vnr - vnl)) / (lam_r + lam_l);
+        lam_l = fmax2(lam_l, al * rhol + 1.5 * std::sqrt(fmax2(0.0, (pbar[j] - pl) * rhol)));
+        lam_r = fmax2(lam_r, ar * rhor + 1.5 * std::sqrt(fmax2(0.0, (pbar[j] - pr) * rhor)));
+      } else {
+        const double pq = wall1 ? pbar[j] : p_node;
+        lam_l = fmax2(lam_l, al * rhol + 1.5 * std::sqrt(fmax2(0.0, (pq - pl) * rhol)));
+        lam_r = fmax2(lam_r, ar * rhor + 1.5 * std::sqrt(fmax2(0.0, (pq - pr) * rhor)));
+      }
+      pbar[j] = (lam_r * pl + lam_l * pr - lam_r * lam_l * (vnr - vnl)) / (lam_r + lam_l);
+      if (wall1) {
+        s1 = s1 + (1.0 / lam_r + 1.0 / lam_l) * area * (lam_r * pl + lam_r * lam_l * vnl) / (lam_r + lam_l);
+        s2 = s2 + (1.0 / lam_l) * area;
+      } else {
+        s1 = s1 + (1.0 / lam_r + 1.0 / lam_l) * area * pbar[j];
+        s2 = s2 + (1.0 / lam_r + 1.0 / lam_l) * area;
+      }
+      lam[2 * j] = lam_l;
+      lam[2 * j + 1] = lam_r;
+    }
+    p_node = s1 / s2;
+  }
+  return p_node;
+}
+
+// ns_euler_module.F90:151-339 (scheme_id multi_point, multi_point_iso, three_wave,
+// two_wave, modified_three_wave, multi_point_pressure(_ph)) + :341-519
 static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol, double* rhs, const double* grad,
                               double* sum_lambda, bool so, double* vp) {
   for (int i = 0; i < 5 * m.n_elems; ++i) rhs[i] = 0.0;
@@ -626,6 +714,9 @@ static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol
     }
     double vv3[3] = {0, 0, 0};
     bool excl = vv.is_bound && cfg.exclude_bound_vert;
+    double p_nodal = 0.0;
+    const bool pres = cfg.scheme == 6 || cfg.scheme == 8;
+    if (pres) p_nodal = nodal_pressure(m, cfg, v, wlr, lam);
     if (cfg.scheme == 1 || cfg.scheme == 2) {
       if (!excl) nodal_velocity(m, cfg, v, wlr, lam, vbar, vv3);
       for (int d = 0; d < 3; ++d) vp[3 * (v - 1) + d] = vv3[d];
@@ -646,6 +737,9 @@ static int compute_euler_flux(const Mesh& m, const NsCfg& cfg, const double* sol
           status |= 4;
       } else if (cfg.scheme == 3 || cfg.scheme == 5) {
         three_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr, &sl, &sr, cfg.scheme == 5);
+      } else if (pres) {
+        multi_point_pressure(&wlr[10 * j], &wlr[10 * j + 5], n, lr, p_nodal, lam[2 * j], lam[2 * j + 1], &sl, &sr,
+                             cfg.scheme == 8);
       } else {
         two_wave(&wlr[10 * j], &wlr[10 * j + 5], n, lr, &sl, &sr);
       }

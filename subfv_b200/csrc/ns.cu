@@ -363,9 +363,11 @@ __device__ void two_wave(const double* wl64, const double* wr64, const double* n
 
 // three_wave (ns_euler_rs_module.F90:9-75) and modified_three_wave (:77-152): two-wave
 // bounds, v* = v_bar, HLLC-type star states (the modified form averages the tangential
-// velocity and carries its jump energy); arithmetic in T, results stored as double.
+// velocity and carries its jump energy); arithmetic in T, results stored as double. The
+// fluxes of the schemes beyond multi_point and two_wave are out of line, so the node
+// kernel's register allocation for those two does not grow with them.
 template <class T>
-__device__ void three_wave(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
+__device__ __noinline__ void three_wave(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
                            double* sl_o, double* sr_o, bool modified) {
   T wl[5], wr[5], n[3];
   for (int k = 0; k < 5; ++k) {
@@ -431,11 +433,93 @@ __device__ void three_wave(const double* wl64, const double* wr64, const double*
   *sr_o = (double)sr;
 }
 
+// multi_point_pressure (ns_euler_rs_module.F90:555-616) and multi_point_pressure_ph
+// (:618-679): star states from the nodal pressure and the nodal pressure solver's bounds.
+template <class T>
+__device__ __noinline__ void multi_point_pressure(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
+                                     double p_nodal64, double lam_l64, double lam_r64, double* sl_o, double* sr_o,
+                                     bool ph) {
+  T wl[5], wr[5], n[3];
+  for (int k = 0; k < 5; ++k) {
+    wl[k] = (T)wl64[k];
+    wr[k] = (T)wr64[k];
+  }
+  for (int d = 0; d < 3; ++d) n[d] = (T)n64[d];
+  const T lam_l = (T)lam_l64, lam_r = (T)lam_r64, p_nodal = (T)p_nodal64, c1 = (T)1, ch = (T)0.5;
+  T rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], ul[5], vt_l[3];
+  for (int d = 0; d < 3; ++d) vt_l[d] = wl[1 + d] - vnl * n[d];
+  p2c(wl, ul);
+  T el = ul[4] / rhol;
+  T rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ur[5], vt_r[3];
+  for (int d = 0; d < 3; ++d) vt_r[d] = wr[1 + d] - vnr * n[d];
+  p2c(wr, ur);
+  T er = ur[4] / rhor;
+  T fl[5], fr[5];
+  fl[0] = vnl * ul[0];
+  for (int k = 1; k < 4; ++k) fl[k] = vnl * ul[k] + pl * n[k - 1];
+  fl[4] = (ul[4] + pl) * vnl;
+  fr[0] = vnr * ur[0];
+  for (int k = 1; k < 4; ++k) fr[k] = vnr * ur[k] + pr * n[k - 1];
+  fr[4] = (ur[4] + pr) * vnr;
+  T vn_bar = (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
+  T vn_l_et = vnl - (p_nodal - pl) / lam_l;
+  T rhol_et = c1 / (c1 / rhol + (vn_bar - vnl) / lam_l);
+  T sle[5], sre[5];
+  sle[0] = rhol_et;
+  for (int k = 1; k < 4; ++k) sle[k] = rhol_et * (vt_l[k - 1] + vn_l_et * n[k - 1]);
+  sle[4] = rhol_et * (el + (pl * vnl - p_nodal * (ph ? vn_l_et : vn_bar)) / lam_l);
+  T vn_r_et = vnr + (p_nodal - pr) / lam_r;
+  T rhor_et = c1 / (c1 / rhor + (vnr - vn_bar) / lam_r);
+  sre[0] = rhor_et;
+  for (int k = 1; k < 4; ++k) sre[k] = rhor_et * (vt_r[k - 1] + vn_r_et * n[k - 1]);
+  sre[4] = rhor_et * (er + (p_nodal * (ph ? vn_r_et : vn_bar) - pr * vnr) / lam_r);
+  const T sl = vnl - lam_l / rhol, sr = vnr + lam_r / rhor;
+  for (int k = 0; k < 5; ++k) {
+    const T f = ch * (fl[k] + fr[k]) -
+                ch * (fabs(sl) * (sle[k] - ul[k]) + fabs(vn_bar) * (sre[k] - sle[k]) + fabs(sr) * (ur[k] - sre[k]));
+    lr[0][k] = (double)f;
+    lr[1][k] = (double)(-f);
+  }
+  *sl_o = (double)sl;
+  *sr_o = (double)sr;
+}
+
+// One subface's share of iteration `iter` of compute_lambdas_and_solve_nodal_pressure
+// (ns_euler_rs_module.F90:681-758), FP64: the bounds lam_l, lam_r (updated in place),
+// and the terms t1, t2 of s1 and s2 (p_node = s1 / s2). The previous iteration's p_bar
+// (read at bc_style 1 walls) is recomputed from the bounds it ended with.
+__device__ inline void nodal_pressure_terms(int iter, bool wall1, const double* wl, const double* wr,
+                                            const double* n, double area, double p_node, double& lam_l,
+                                            double& lam_r, double& t1, double& t2) {
+  const double rhol = wl[0], vnl = dotT(wl + 1, n), pl = wl[4], al = sqrt(G * wl[4] / wl[0]);
+  const double rhor = wr[0], vnr = dotT(wr + 1, n), pr = wr[4], ar = sqrt(G * wr[4] / wr[0]);
+  auto pbar_of = [&](double ll, double lr) { return (lr * pl + ll * pr - lr * ll * (vnr - vnl)) / (lr + ll); };
+  if (iter == 1) {
+    lam_l = fmax2(fmax2(fmax2(lam_l, al * rhol), sqrt(rhol * fmax2(0.0, pr - pl))), -rhol * (vnr - vnl));
+    lam_r = fmax2(fmax2(fmax2(lam_r, ar * rhor), sqrt(rhor * fmax2(0.0, pl - pr))), -rhor * (vnr - vnl));
+    const double pb = pbar_of(lam_l, lam_r);
+    lam_l = fmax2(lam_l, al * rhol + 1.5 * sqrt(fmax2(0.0, (pb - pl) * rhol)));
+    lam_r = fmax2(lam_r, ar * rhor + 1.5 * sqrt(fmax2(0.0, (pb - pr) * rhor)));
+  } else {
+    const double pq = wall1 ? pbar_of(lam_l, lam_r) : p_node;
+    lam_l = fmax2(lam_l, al * rhol + 1.5 * sqrt(fmax2(0.0, (pq - pl) * rhol)));
+    lam_r = fmax2(lam_r, ar * rhor + 1.5 * sqrt(fmax2(0.0, (pq - pr) * rhor)));
+  }
+  const double pb = pbar_of(lam_l, lam_r);
+  if (wall1) {
+    t1 = (1.0 / lam_r + 1.0 / lam_l) * area * (lam_r * pl + lam_r * lam_l * vnl) / (lam_r + lam_l);
+    t2 = (1.0 / lam_l) * area;
+  } else {
+    t1 = (1.0 / lam_r + 1.0 / lam_l) * area * pb;
+    t2 = (1.0 / lam_r + 1.0 / lam_l) * area;
+  }
+}
+
 // multi_point_iso's flux (ns_euler_module.F90:464-483): the multi-point (or, at an
 // excluded boundary vertex, two-wave) flux blended with three_wave by
 // warea = min area / area; the wave speeds sl, sr are three_wave's.
 template <class T>
-__device__ void blend_three_wave(const double* w10, const double* n, double amin, double lr[2][5], double* sl,
+__device__ __noinline__ void blend_three_wave(const double* w10, const double* n, double amin, double lr[2][5], double* sl,
                                  double* sr) {
   double lr3[2][5];
   three_wave<T>(w10, w10 + 5, n, lr3, sl, sr, false);
@@ -557,7 +641,36 @@ __device__ inline double vbar_of(double lam_l, double lam_r, double vnl, double 
   return (lam_l * vnl + lam_r * vnr - (pr - pl)) / (lam_r + lam_l);
 }
 
+// compute_lambdas_and_solve_nodal_pressure for one vertex (thread-per-vertex layout):
+// ten iterations of p_node = s1 / s2, the bounds kept in L between iterations. Out of
+// line, so the other schemes' register allocation does not carry it.
 template <class T, class L, int MS>
+__device__ __noinline__ double nodal_pressure_vertex(const DevMesh& m, const NsParams& P, int nsfn, const int* sfj,
+                                                     const int* yj, const T (*wlr)[10], L (*lam)[2]) {
+  double p_node = 0.0;
+  for (int iter = 1; iter <= 10; ++iter) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < nsfn; ++j) {
+      const double4 sn4 = m.sfn[sfj[j]];
+      const double n[3] = {sn4.x, sn4.y, sn4.z};
+      double w10[10];
+      for (int k = 0; k < 10; ++k) w10[k] = (double)wlr[j][k];
+      double ll = (double)lam[j][0], lr = (double)lam[j][1], t1, t2;
+      nodal_pressure_terms(iter, P.bc_style == 1 && is_wall(P, yj[j]), w10, w10 + 5, n, sn4.w, p_node, ll, lr, t1,
+                           t2);
+      s1 = s1 + t1;
+      s2 = s2 + t2;
+      lam[j][0] = (L)ll;
+      lam[j][1] = (L)lr;
+    }
+    p_node = s1 / s2;
+  }
+  return p_node;
+}
+
+// EXT: compiled with the schemes beyond multi_point and two_wave (2, 3, 5, 6, 8); the
+// instantiation without them keeps the common path's register allocation.
+template <class T, class L, int MS, bool EXT>
 __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
                                const double* __restrict__ grad, double* __restrict__ fs, int so, const int v) {
   if (v >= m.nv) return;
@@ -578,14 +691,14 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     const int2 lr = m.flr[m.sf_face[sf]];
     sfj[j] = sf;
     yj[j] = lr.y;
-    if (P.scheme == 2) amin = j == 0 ? m.sfn[sf].w : fmin2(amin, m.sfn[sf].w);
+    if (EXT && P.scheme == 2) amin = j == 0 ? m.sfn[sf].w : fmin2(amin, m.sfn[sf].w);
     double w10[10];
     reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5);
     for (int k = 0; k < 10; ++k) wlr[j][k] = (T)w10[k];
     lam[j][0] = lam[j][1] = (L)0;
   }
   const bool excl = m.is_bound[v] && P.excl;
-  const bool iso = P.scheme == 2;  // multi_point_iso: M and R without the subface areas (:424-553)
+  const bool iso = EXT && P.scheme == 2;  // multi_point_iso: M and R without the subface areas (:424-553)
   double vn3[3] = {0.0, 0.0, 0.0};
   if (P.scheme == 1 || iso) {
     if (!excl) {  // compute_lambdas_and_solve_nodal_velocity (ns_euler_rs_module.F90:288-422)
@@ -667,6 +780,8 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     }
     m.vp[v] = make_double4(vn3[0], vn3[1], vn3[2], 0.0);
   }
+  const double p_node =
+      (EXT && (P.scheme == 6 || P.scheme == 8)) ? nodal_pressure_vertex<T, L, MS>(m, P, nsfn, sfj, yj, wlr, lam) : 0.0;
   double fsv[MS][6];  // five flux sums and the wave-speed sum per subcell
   for (int j = 0; j < nsen; ++j)
     for (int k = 0; k < 6; ++k) fsv[j][k] = 0.0;
@@ -683,8 +798,11 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     if ((P.scheme == 1 || iso) && !excl) {
       const double vn = is_wall(P, yj[j]) ? 0.0 : dotT(vn3, n);
       if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam[j][0], (double)lam[j][1], &sl, &sr)) bad = true;
-    } else if (P.scheme == 3 || P.scheme == 5) {
+    } else if (EXT && (P.scheme == 3 || P.scheme == 5)) {
       three_wave<T>(w10, w10 + 5, n, lr, &sl, &sr, P.scheme == 5);
+    } else if (EXT && (P.scheme == 6 || P.scheme == 8)) {
+      multi_point_pressure<T>(w10, w10 + 5, n, lr, p_node, (double)lam[j][0], (double)lam[j][1], &sl, &sr,
+                              P.scheme == 8);
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
@@ -872,6 +990,29 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
     }
     if (act && j == 0) m.vp[v] = make_double4(vn3[0], vn3[1], vn3[2], 0.0);
   }
+  const bool pres = P.scheme == 6 || P.scheme == 8;
+  double p_node = 0.0;
+  if (pres) {  // nodal pressure: s1 and s2 summed in subface order by lanes 0 and 1
+    for (int iter = 1; iter <= 10; ++iter) {
+      unsigned f = 0u;
+      if (mine) {
+        double w10[10];
+        for (int k = 0; k < 10; ++k) w10[k] = (double)w[k];
+        double ll = (double)lam_l, lr = (double)lam_r;
+        nodal_pressure_terms(iter, P.bc_style == 1 && is_wall(P, y), w10, w10 + 5, n, n[3], p_node, ll, lr,
+                             gv[j * kLaneVals], gv[j * kLaneVals + 1]);
+        lam_l = (L)ll;
+        lam_r = (L)lr;
+        f = 3u;
+      }
+      gf[j] = f;
+      __syncwarp(mask);
+      if (j < 2) gs[j] = group_ordered_sum<NG>(gv, gf, nsfn, j);
+      __syncwarp(mask);
+      p_node = gs[0] / gs[1];
+      __syncwarp(mask);
+    }
+  }
   // subface fluxes; lane j's terms to its left / right subcell of this vertex
   int lse = -1, rse = -1;
   unsigned f = 0u;
@@ -887,6 +1028,9 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
         atomicOr(m.status, kErrNegDensity);
     } else if (P.scheme == 3 || P.scheme == 5) {
       three_wave<T>(w10, w10 + 5, n, lr, &sl, &sr, P.scheme == 5);
+    } else if (P.scheme == 6 || P.scheme == 8) {
+      multi_point_pressure<T>(w10, w10 + 5, n, lr, p_node, (double)lam_l, (double)lam_r, &sl, &sr,
+                              P.scheme == 8);
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
@@ -956,12 +1100,12 @@ __global__ void __launch_bounds__(kNodeGroupThreads, 2) k_ns_node_group(DevMesh 
   ns_node_group<T, L, NG>(m, P, U, grad, fs, so, v, true, sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g]);
 }
 
-template <class T, class L, int MS>
+template <class T, class L, int MS, bool EXT>
 __global__ void __launch_bounds__(kNodeThreads) k_ns_node(DevMesh m, NsParams P, const double* __restrict__ U,
                                                           const double* __restrict__ grad, double* __restrict__ fs,
                                                           int so, const NsScalars* sc) {
   if (sc && sc->done) return;
-  ns_node_vertex<T, L, MS>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x);
+  ns_node_vertex<T, L, MS, EXT>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 __device__ inline double warp_min(double x) {
@@ -1334,7 +1478,7 @@ __device__ inline int item_of(const int* __restrict__ wofs, int n, int w) {
 }
 
 // which: the state the phase reads (0: U0, 1: U1)
-template <class T, class L, int MS>
+template <class T, class L, int MS, bool EXT>
 __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restrict__ it, const int* __restrict__ wv,
                                                            const int* __restrict__ hdr, NsParams P, int which,
                                                            int so) {
@@ -1343,7 +1487,8 @@ __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restr
     const int p = item_of(wv, n, w);
     const NsItem& I = it[p];
     if (I.sc->done) continue;
-    ns_node_vertex<T, L, MS>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * blockDim.x + threadIdx.x);
+    ns_node_vertex<T, L, MS, EXT>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so,
+                                  (w - wv[p]) * blockDim.x + threadIdx.x);
   }
 }
 // the group variant: a work block of block_v vertices is walked kNodeGroupThreads / NG
@@ -1706,6 +1851,9 @@ __global__ void k_ns_pack(int n, const double* __restrict__ s5, double* __restri
 
 int ns_partial_blocks(const DevMesh& m) { return grid_for(m.ne, kTdBlock); }
 
+// the schemes compiled only into the extended node kernels
+bool ns_scheme_ext(const NsParams& P) { return !(P.scheme == 1 || P.scheme == 4); }
+
 template <class T, class L>
 void launch_kb_node_tl(const NsTable& t, const NsParams& P, cudaStream_t s, int which, int so) {
   const int gv = t.grid_v, bv = t.block_v;
@@ -1716,9 +1864,15 @@ void launch_kb_node_tl(const NsTable& t, const NsParams& P, cudaStream_t s, int 
     else kb_ns_node_group<T, L, 32><<<gv, nt, 0, s>>>(t.items, t.wv, t.hdr, P, which, so, bv);
     return;
   }
-  if (t.group == 8) kb_ns_node<T, L, 8><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
-  else if (t.group == 16) kb_ns_node<T, L, 16><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
-  else kb_ns_node<T, L, 32><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  if (ns_scheme_ext(P)) {
+    if (t.group == 8) kb_ns_node<T, L, 8, true><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+    else if (t.group == 16) kb_ns_node<T, L, 16, true><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+    else kb_ns_node<T, L, 32, true><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+    return;
+  }
+  if (t.group == 8) kb_ns_node<T, L, 8, false><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  else if (t.group == 16) kb_ns_node<T, L, 16, false><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
+  else kb_ns_node<T, L, 32, false><<<gv, bv, 0, s>>>(t.items, t.wv, t.hdr, P, which, so);
 }
 // precision 0: FP64 throughout; 1: FP32 wave-speed bounds; 2: FP32 wave speeds, flux and
 // reconstruction
@@ -1800,9 +1954,15 @@ void launch_node_tl(const DevMesh& m, const NsParams& P, const double* U, const 
     return;
   }
   const int grid = grid_for(m.nv, 128);
-  if (ms == 8) k_ns_node<T, L, 8><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
-  else if (ms == 16) k_ns_node<T, L, 16><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
-  else k_ns_node<T, L, 32><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  if (ns_scheme_ext(P)) {
+    if (ms == 8) k_ns_node<T, L, 8, true><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+    else if (ms == 16) k_ns_node<T, L, 16, true><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+    else k_ns_node<T, L, 32, true><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+    return;
+  }
+  if (ms == 8) k_ns_node<T, L, 8, false><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  else if (ms == 16) k_ns_node<T, L, 16, false><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
+  else k_ns_node<T, L, 32, false><<<grid, 128, 0, m.stream>>>(m, P, U, grad, fs, so, sc);
 }
 void launch_node(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs, int so,
                  const NsScalars* sc) {

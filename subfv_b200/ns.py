@@ -18,6 +18,7 @@ from ._lib import check, f64, pd
 from .mesh import Mesh
 
 SCHEME_MULTI_POINT, SCHEME_MULTI_POINT_ISO, SCHEME_THREE_WAVE, SCHEME_TWO_WAVE, SCHEME_MODIFIED_THREE_WAVE = 1, 2, 3, 4, 5
+SCHEME_MULTI_POINT_PRESSURE, SCHEME_MULTI_POINT_PRESSURE_PH = 6, 8
 # (the scheme ids of ns_global_data_module.F90:67-71)
 BC_WALL, BC_FREESTREAM, BC_OUTFLOW_SUPERSONIC = 1, 3, 4
 

@@ -58,6 +58,7 @@ CFGS = {
     "tw_o2_fp32": dict(scheme=4, second_order=True, method=4, bc_style=2, precision=1),
     "m3w_o2": dict(scheme=5, second_order=True, method=4, bc_style=2, precision=0),
     "iso_o1_fp32": dict(scheme=2, second_order=False, method=4, bc_style=2, precision=1),
+    "mpph_o2": dict(scheme=8, second_order=True, method=4, bc_style=1, precision=0),
 }
 
 

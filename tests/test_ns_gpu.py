@@ -29,6 +29,10 @@ CFGS = {
     "iso_o1_bc2": dict(scheme=2, second_order=False, method=4, bc_style=2),
     "iso_o2_bc2": dict(scheme=2, second_order=True, method=4, bc_style=2),
     "iso_o1_bc0": dict(scheme=2, second_order=False, method=4, bc_style=0),
+    "mpp_o1_bc2": dict(scheme=6, second_order=False, method=4, bc_style=2),
+    "mpp_o2_bc1": dict(scheme=6, second_order=True, method=4, bc_style=1),
+    "mpph_o1_bc1": dict(scheme=8, second_order=False, method=4, bc_style=1),
+    "mpph_o2_bc2": dict(scheme=8, second_order=True, method=4, bc_style=2),
 }
 
 
@@ -71,7 +75,8 @@ def test_gresho_init_matches_oracle(native, oracle_lib, cuda_ok):
     np.testing.assert_array_equal(init_gresho(m, 0.1), o.ns_gresho(0.1))
 
 
-@pytest.mark.parametrize("cfg_name", ["mp_o2_bc2", "tw_o2", "mp_o1_bc1", "3w_o2", "m3w_o2", "iso_o2_bc2"])
+@pytest.mark.parametrize("cfg_name", ["mp_o2_bc2", "tw_o2", "mp_o1_bc1", "3w_o2", "m3w_o2", "iso_o2_bc2", "mpp_o2_bc1",
+                                      "mpph_o2_bc2"])
 def test_ns_time_loop_bit_exact(native, oracle_lib, cuda_ok, cfg_name):
     from subfv_b200.ns import NsConfig, NsState, init_gresho
     m, o = _pair(_meshes()["hex_slab"])
