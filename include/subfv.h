@@ -111,6 +111,13 @@ int subfv_compute_geometry_mesh(subfv_mesh* m);
  * src/lagrange/lagrange_module.F90:14-147. sol/rhs (5, n_elems), vp (3, n_vert). */
 int subfv_compute_rhs_lagrange(subfv_mesh* m, const double* sol, double* vp, double* rhs,
                                int b2d, const double* mass);
+/* compute_rhs_lagrange_sidil(mesh, sol, vp, dt, rhs, n_bc, bc_type, bc_val, b2d, mass,
+ * method, b2d_h) — lagrange_module.F90:149-223 with compute_nodal_velocity_sidil,
+ * compute_nodal_pressure_sidil and compute_length (:538-711): scheme "sidil", FP64.
+ * method_length 0..4; b2d_h is unused by the reference. A negative nodal pressure (the
+ * reference's error stop) sets SUBFV_ERR_NEG_DENSITY in the returned status. */
+int subfv_compute_rhs_lagrange_sidil(subfv_mesh* m, const double* sol, double* vp, double* rhs, int b2d,
+                                     const double* mass, int method_length);
 /* compute_dt(mesh, sol, dt, cfl, vp, me, num_procs) — lagrange_module.F90:240-283 */
 int subfv_compute_dt(subfv_mesh* m, const double* sol, double cfl, const double* vp, double* dt);
 /* No counterpart in the reference. compute_dt for callers that cannot allocate device
@@ -133,6 +140,9 @@ typedef struct subfv_lag_state subfv_lag_state;
 int subfv_lag_state_create(subfv_mesh* m, const double* sol, const double* mass, double cfl,
                            double t0, double t_max, int precision, subfv_lag_state** out);
 int subfv_lag_state_destroy(subfv_lag_state* s);
+/* The state's scheme (lagrange_main.F90:91-100): 0 "classic" (default), 1 "sidil" with
+ * method_length 0..4 (FP64 whatever the state's precision). */
+int subfv_lag_state_set_scheme(subfv_lag_state* s, int scheme, int method_length);
 /* run n_steps (stops early once t >= t_max); returns status bits */
 int subfv_lag_advance(subfv_lag_state* s, int n_steps, int* steps_done, double* t);
 int subfv_lag_advance_async(subfv_lag_state* s, int n_steps);

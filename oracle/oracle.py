@@ -47,6 +47,9 @@ def load():
         lib.or_lag_move.argtypes = [C.c_void_p, PD, C.c_double]
         lib.or_sedov_init.argtypes = [C.c_void_p, PD, C.c_double, C.c_double, PI]
         lib.or_lag_run.argtypes = [C.c_void_p, PD, PD, PD, PD, C.c_double, C.c_double, C.c_int, C.c_int, PD, PD]
+        lib.or_lag_run_scheme.argtypes = [C.c_void_p, PD, PD, PD, PD, C.c_double, C.c_double, C.c_int, C.c_int, PD,
+                                          PD, C.c_int, C.c_int]
+        lib.or_lag_rhs_sidil.argtypes = [C.c_void_p, PD, PD, PD, C.c_int, PD, C.c_int]
         lib.or_inverse_3_by_3.argtypes = [PD, PD]
         lib.or_fnorm2.restype = C.c_double
         lib.or_fnorm2.argtypes = [PD, C.c_int]
@@ -142,6 +145,15 @@ class OracleMesh:
         load().or_lag_rhs(self._h, _pd(sol), _pd(vp), _pd(rhs), int(self.b2d), _pd(mass))
         return vp, rhs
 
+    def lag_rhs_sidil(self, sol, mass, method):
+        """compute_rhs_lagrange_sidil: (status, vp, rhs)."""
+        sol = np.ascontiguousarray(sol, np.float64)
+        mass = np.ascontiguousarray(mass, np.float64)
+        vp = np.zeros((self.n_vert, 3))
+        rhs = np.zeros((self.n_elems, 5))
+        st = load().or_lag_rhs_sidil(self._h, _pd(sol), _pd(vp), _pd(rhs), int(self.b2d), _pd(mass), int(method))
+        return st, vp, rhs
+
     def lag_dt(self, sol, cfl, vp):
         sol = np.ascontiguousarray(sol, np.float64)
         vp = np.ascontiguousarray(vp, np.float64)
@@ -159,16 +171,18 @@ class OracleMesh:
             raise ValueError("r_sedov too small")
         return sol
 
-    def lag_run(self, sol, mass, cfl, t_max, max_steps, t0=0.0):
-        """Runs the reference time loop in place on sol; returns (steps, t, last dt)."""
+    def lag_run(self, sol, mass, cfl, t_max, max_steps, t0=0.0, scheme=0, method=0):
+        """Runs the reference time loop in place on sol (scheme 0 classic, 1 sidil with
+        method_length `method`); returns (steps, t, last dt, vp)."""
         assert sol.dtype == np.float64 and sol.flags["C_CONTIGUOUS"]
         mass = np.ascontiguousarray(mass, np.float64)
         vp = np.zeros((self.n_vert, 3))
         rhs = np.zeros((self.n_elems, 5))
         t = C.c_double(t0)
         dt = C.c_double(0.0)
-        n = load().or_lag_run(self._h, _pd(sol), _pd(vp), _pd(rhs), _pd(mass), float(cfl), float(t_max),
-                              int(max_steps), int(self.b2d), C.byref(t), C.byref(dt))
+        n = load().or_lag_run_scheme(self._h, _pd(sol), _pd(vp), _pd(rhs), _pd(mass), float(cfl), float(t_max),
+                                     int(max_steps), int(self.b2d), C.byref(t), C.byref(dt), int(scheme),
+                                     int(method))
         return n, t.value, dt.value, vp
 
     # --- explicit Euler (subfvns)

@@ -11,7 +11,9 @@ double compute_dt(const Mesh& m, const double* sol, double cfl, const double* vp
 void move_mesh(Mesh& m, const double* vp, double dt);
 int init_sedov(const Mesh& m, double* sol, double r_sedov, double e_total, const int* mask);
 int lagrange_run(Mesh& m, double* sol, double* vp, double* rhs, const double* mass, double cfl,
-                 double t_max, int max_steps, bool b2d, double* t_io, double* last_dt);
+                 double t_max, int max_steps, bool b2d, double* t_io, double* last_dt, int scheme, int method);
+int compute_rhs_lagrange_sidil(const Mesh& m, const double* sol, double* vp, double* rhs, bool b2d,
+                               const double* mass, int method);
 void inverse_3_by_3(const double M[3][3], double Inv[3][3]);
 }  // namespace oracle
 
@@ -121,7 +123,16 @@ int or_sedov_init(void* p, double* sol, double r_sedov, double e_total, const in
 int or_lag_run(void* p, double* sol, double* vp, double* rhs, const double* mass, double cfl,
                double t_max, int max_steps, int b2d, double* t_io, double* last_dt) {
   return lagrange_run(((OHandle*)p)->m, sol, vp, rhs, mass, cfl, t_max, max_steps, b2d != 0, t_io,
-                      last_dt);
+                      last_dt, 0, 0);
+}
+int or_lag_run_scheme(void* p, double* sol, double* vp, double* rhs, const double* mass, double cfl,
+                      double t_max, int max_steps, int b2d, double* t_io, double* last_dt, int scheme, int method) {
+  return lagrange_run(((OHandle*)p)->m, sol, vp, rhs, mass, cfl, t_max, max_steps, b2d != 0, t_io,
+                      last_dt, scheme, method);
+}
+int or_lag_rhs_sidil(void* p, const double* sol, double* vp, double* rhs, int b2d, const double* mass,
+                     int method) {
+  return compute_rhs_lagrange_sidil(((OHandle*)p)->m, sol, vp, rhs, b2d != 0, mass, method);
 }
 void or_inverse_3_by_3(const double* m9, double* inv9) {
   double M[3][3], I[3][3];

@@ -1,6 +1,8 @@
 // Test infrastructure only (oracle). Restatement of the subfv Lagrangian hydro step:
 // src/lagrange/lagrange_module.F90 (compute_rhs_lagrange, compute_dt, init_sol,
-// pressure, move_mesh), src/linear_algebra/linear_solver_module.F90 (inverse_3_by_3)
+// pressure, move_mesh; the "sidil" scheme's compute_rhs_lagrange_sidil, nodal velocity,
+// nodal pressure, compute_length, boundary_normal, corner_normal, lag_to_primit),
+// src/linear_algebra/linear_solver_module.F90 (inverse_3_by_3)
 // and the time loop of src/lagrange/lagrange_main.F90:81-127.
 // PARITY UNPINNED (no Fortran compiler here; the reference tests hold no golden data).
 #include "oracle.h"
@@ -146,6 +148,136 @@ void compute_rhs_lagrange(const Mesh& m, const double* sol, double* vp, double* 
   }
 }
 
+// ---------------------------------------------------------------- scheme "sidil"
+// lagrange_module.F90:802-809 (lag_to_primit): (1/tau, u, v, w, p)
+static void lag_to_primit(const double* u, double* w) {
+  w[0] = 1.0 / u[0];
+  for (int d = 1; d < 4; ++d) w[d] = u[d];
+  w[4] = pressure(u);
+}
+
+// the primitive states either side of face f: the neighbour's, or at a boundary the
+// left state with its velocity mirrored in the face normal (:568-576, :643-651)
+static void sidil_lr(const Mesh& m, const double* sol, const Face& f, double* wl, double* wr) {
+  const double* ul = sol + 5 * (f.left_neigh - 1);
+  double ur[5];
+  if (f.right_neigh > 0) {
+    for (int k = 0; k < 5; ++k) ur[k] = sol[5 * (f.right_neigh - 1) + k];
+  } else {
+    for (int k = 0; k < 5; ++k) ur[k] = ul[k];
+    const double d = dot3(ur + 1, &f.norm[1]);
+    for (int k = 1; k < 4; ++k) ur[k] = ur[k] - 2.0 * d * f.norm[k];
+  }
+  lag_to_primit(ul, wl);
+  lag_to_primit(ur, wr);
+}
+
+// compute_length (:680-711) with corner_normal (:730-757): method scales V_p / sum |n_c|
+static double sidil_length(const Mesh& m, int v, int method, bool b2d) {
+  const Vert& vv = m.vert[v];
+  double area_sum = 0.0;
+  for (int j = 1; j <= vv.n_sub_elems_neigh; ++j) {
+    const SubElem& se = m.sub_elem[vv.sub_elem_neigh[j]];
+    double nc[3] = {0.0, 0.0, 0.0};
+    for (int k = 1; k <= se.n_sub_faces; ++k) {
+      const SubFace& s = m.sub_face[se.sub_face[k]];
+      const Face& f = m.face[s.mesh_face];
+      if (!b2d || std::fabs(f.norm[3]) < 1e-12) {
+        if (f.left_neigh == se.mesh_elem)
+          for (int d = 0; d < 3; ++d) nc[d] = nc[d] + s.area * f.norm[d + 1];
+        else
+          for (int d = 0; d < 3; ++d) nc[d] = nc[d] - s.area * f.norm[d + 1];
+      }
+    }
+    area_sum = area_sum + fnorm2(nc, 3);
+  }
+  const double c = method == 0 ? 0.0 : method == 1 ? 1.0 : method == 2 ? 2.0 : method == 3 ? 4.0 : 8.0;
+  return c * vv.volume / area_sum;
+}
+
+// compute_nodal_velocity_sidil (:538-612) and compute_nodal_pressure_sidil (:614-678)
+// for vertex v; returns false on a negative nodal pressure (the reference stops)
+static bool sidil_node(const Mesh& m, const double* sol, int v, int method, bool b2d, double* vp, double* pp_out) {
+  const Vert& vv = m.vert[v];
+  double w[5], wl[5], wr[5];
+  double rho_p = 0.0, a_p = 0.0, pp = 0.0;
+  vp[0] = vp[1] = vp[2] = 0.0;
+  for (int j = 1; j <= vv.n_sub_elems_neigh; ++j) {
+    const SubElem& se = m.sub_elem[vv.sub_elem_neigh[j]];
+    lag_to_primit(sol + 5 * (se.mesh_elem - 1), w);
+    for (int d = 0; d < 3; ++d) vp[d] = vp[d] + se.volume * w[1 + d];
+    rho_p = rho_p + se.volume * w[0];
+    a_p = a_p + se.volume * std::sqrt(kGamma * w[4] / w[0]);
+    pp = pp + se.volume * w[4];
+  }
+  rho_p = rho_p / vv.volume;
+  a_p = a_p / vv.volume;
+  for (int d = 0; d < 3; ++d) vp[d] = vp[d] / vv.volume;
+  pp = pp / vv.volume;
+  double grad_p[3] = {0.0, 0.0, 0.0}, div_v = 0.0;
+  for (int j = 1; j <= vv.n_sub_faces_neigh; ++j) {
+    const SubFace& s = m.sub_face[vv.sub_face_neigh[j]];
+    const Face& f = m.face[s.mesh_face];
+    sidil_lr(m, sol, f, wl, wr);
+    for (int d = 0; d < 3; ++d) grad_p[d] = grad_p[d] + (wr[4] - wl[4]) * s.area * f.norm[d + 1];
+    double dv[3], an[3];
+    for (int d = 0; d < 3; ++d) {
+      dv[d] = wr[1 + d] - wl[1 + d];
+      an[d] = s.area * f.norm[d + 1];
+    }
+    div_v = div_v + dot3(dv, an);
+  }
+  for (int d = 0; d < 3; ++d) grad_p[d] = grad_p[d] / vv.volume;
+  div_v = div_v / vv.volume;
+  if (vv.is_bound) {  // boundary_normal (:713-728), normalised
+    double Bp[3] = {0.0, 0.0, 0.0};
+    for (int j = 1; j <= vv.n_sub_faces_neigh; ++j) {
+      const SubFace& s = m.sub_face[vv.sub_face_neigh[j]];
+      const Face& f = m.face[s.mesh_face];
+      if (f.right_neigh <= 0)
+        for (int d = 0; d < 3; ++d) Bp[d] = Bp[d] + s.area * f.norm[d + 1];
+    }
+    const double nb = fnorm2(Bp, 3);
+    for (int d = 0; d < 3; ++d) Bp[d] = Bp[d] / nb;
+    const double gb = dot3(grad_p, Bp);
+    for (int d = 0; d < 3; ++d) grad_p[d] = grad_p[d] - gb * Bp[d];
+  }
+  const double h_p = sidil_length(m, v, method, b2d);
+  for (int d = 0; d < 3; ++d) vp[d] = vp[d] - 0.5 * h_p / (rho_p * a_p) * grad_p[d];
+  pp = pp - 0.5 * h_p * rho_p * a_p * div_v;
+  *pp_out = pp;
+  return !(pp < 0.0);
+}
+
+// compute_rhs_lagrange_sidil (:149-223); returns 4 (negative nodal pressure) or 0
+int compute_rhs_lagrange_sidil(const Mesh& m, const double* sol, double* vp, double* rhs, bool b2d,
+                               const double* mass, int method) {
+  for (int i = 0; i < 5 * m.n_elems; ++i) rhs[i] = 0.0;
+  for (int i = 0; i < 3 * m.n_vert; ++i) vp[i] = 0.0;
+  int status = 0;
+  for (int v = 1; v <= m.n_vert; ++v) {
+    double* vpv = vp + 3 * (v - 1);
+    double pp = 0.0;
+    if (!sidil_node(m, sol, v, method, b2d, vpv, &pp)) status |= 4;
+    const Vert& vv = m.vert[v];
+    for (int j = 1; j <= vv.n_sub_faces_neigh; ++j) {
+      const SubFace& s = m.sub_face[vv.sub_face_neigh[j]];
+      const Face& f = m.face[s.mesh_face];
+      const double* n = &f.norm[1];
+      const double v_et = dot3(vpv, n);
+      const double fl[5] = {-v_et, pp * n[0], pp * n[1], pp * n[2], pp * v_et};
+      const int idl = f.left_neigh, idr = f.right_neigh;
+      const double al = s.area / mass[idl - 1];
+      for (int k = 0; k < 5; ++k) rhs[5 * (idl - 1) + k] = rhs[5 * (idl - 1) + k] - al * fl[k];
+      if (idr > 0) {
+        const double ar = s.area / mass[idr - 1];
+        for (int k = 0; k < 5; ++k) rhs[5 * (idr - 1) + k] = rhs[5 * (idr - 1) + k] + ar * fl[k];
+      }
+    }
+  }
+  return status;
+}
+
 // lagrange_module.F90:240-283 (keeps the reference's sub_elem(i) with i a cell index)
 double compute_dt(const Mesh& m, const double* sol, double cfl, const double* vp) {
   const double CV = 0.8;
@@ -198,15 +330,23 @@ int init_sedov(const Mesh& m, double* sol, double r_sedov, double e_total, const
   return 0;
 }
 
-// lagrange_main.F90:81-127, scheme = "classic". Runs until t >= t_max or max_steps.
-// Returns the number of steps taken; *t_io is updated.
+// lagrange_main.F90:81-127, scheme "classic" (scheme 0) or "sidil" (scheme 1, with
+// method_length). Runs until t >= t_max or max_steps. Returns the number of steps taken
+// (negated on a negative sidil nodal pressure); *t_io is updated.
 int lagrange_run(Mesh& m, double* sol, double* vp, double* rhs, const double* mass, double cfl,
-                 double t_max, int max_steps, bool b2d, double* t_io, double* last_dt) {
+                 double t_max, int max_steps, bool b2d, double* t_io, double* last_dt, int scheme, int method) {
   double t = *t_io;
   int iter = 0;
   std::vector<double> new_sol(5 * m.n_elems);
   while (t < t_max && iter < max_steps) {
-    compute_rhs_lagrange(m, sol, vp, rhs, b2d, mass);
+    if (scheme == 1) {
+      if (compute_rhs_lagrange_sidil(m, sol, vp, rhs, b2d, mass, method)) {
+        *t_io = t;
+        return -iter - 1;
+      }
+    } else {
+      compute_rhs_lagrange(m, sol, vp, rhs, b2d, mass);
+    }
     double dt = compute_dt(m, sol, cfl, vp);
     if (t + dt > t_max) dt = t_max - t;
     move_mesh(m, vp, dt);

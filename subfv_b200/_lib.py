@@ -41,6 +41,8 @@ SIGNATURES = {
     "subfv_mesh_get_geometry": (c_int, [P, c_char_p, PD]),
     "subfv_compute_geometry_mesh": (c_int, [P]),
     "subfv_compute_rhs_lagrange": (c_int, [P, PD, PD, PD, c_int, PD]),
+    "subfv_compute_rhs_lagrange_sidil": (c_int, [P, PD, PD, PD, c_int, PD, c_int]),
+    "subfv_lag_state_set_scheme": (c_int, [P, c_int, c_int]),
     "subfv_compute_dt": (c_int, [P, PD, c_dbl, PD, PD]),
     "subfv_compute_dt_noalloc": (c_int, [P, P, P, c_dbl, P]),
     "subfv_move_mesh": (c_int, [P, PD, c_dbl]),

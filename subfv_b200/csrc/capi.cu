@@ -34,6 +34,7 @@ struct subfv_lag_state {
   double* host_stage = nullptr;  // pinned staging for the host-buffer step
   double* dev_stage = nullptr;
   int precision = 0;
+  int scheme = 0, method = 0;  // 0 "classic"; 1 "sidil" with method_length
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
 };
@@ -329,6 +330,50 @@ int subfv_compute_rhs_lagrange(subfv_mesh* m, const double* sol, double* vp, dou
   return check_status(d);
 }
 
+int subfv_compute_rhs_lagrange_sidil(subfv_mesh* m, const double* sol, double* vp, double* rhs, int b2d,
+                                     const double* mass, int method_length) {
+  if (!m || !sol || !vp || !rhs || !mass || method_length < 0 || method_length > 4) {
+    set_error("subfv_compute_rhs_lagrange_sidil: null argument or method_length outside 0..4");
+    return -2;
+  }
+  DevMesh& d = m->d;
+  if (ensure_scratch(m) || ensure_full_geometry(d) || clear_status(d)) return -1;
+  d.b2d = b2d;
+  if (load_sol(m, sol, mass)) return -1;
+  launch_lag_sidil_node(d, m->sol6, nullptr, method_length);
+  launch_lag_cell(d, m->sol6, m->rhs6, nullptr, nullptr, 0, 5);
+  launch_unpack6(d, d.ne, kRhs, m->rhs6, m->stage);
+  SUBFV_CUDA(cudaMemcpyAsync(rhs, m->stage, 5 * (size_t)d.ne * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  std::vector<double4> h(d.nv);
+  SUBFV_CUDA(cudaMemcpyAsync(h.data(), d.vp, d.nv * sizeof(double4), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  for (int i = 0; i < d.nv; ++i) {
+    vp[3 * i] = h[i].x;
+    vp[3 * i + 1] = h[i].y;
+    vp[3 * i + 2] = h[i].z;
+  }
+  SUBFV_CUDA(cudaGetLastError());
+  return check_status(d);
+}
+
+int subfv_lag_state_set_scheme(subfv_lag_state* s, int scheme, int method_length) {
+  if (!s || scheme < 0 || scheme > 1 || method_length < 0 || method_length > 4) {
+    set_error("subfv_lag_state_set_scheme: scheme 0 (classic) or 1 (sidil), method_length 0..4");
+    return -2;
+  }
+  if (s->scheme != scheme || s->method != method_length) {
+    s->scheme = scheme;
+    s->method = method_length;
+    if (s->graph) {  // the captured step loop holds the old scheme
+      SUBFV_CUDA(cudaStreamSynchronize(s->m->d.stream));
+      cudaGraphExecDestroy(s->graph);
+      s->graph = nullptr;
+      s->graph_steps = 0;
+    }
+  }
+  return 0;
+}
+
 int subfv_compute_dt(subfv_mesh* m, const double* sol, double cfl, const double* vp, double* dt) {
   DevMesh& d = m->d;
   if (ensure_scratch(m) || clear_status(d)) return -1;
@@ -414,7 +459,7 @@ int lag_graph(subfv_lag_state* s, int steps) {
   DevMesh& d = s->m->d;
   cudaGraph_t g;
   SUBFV_CUDA(cudaStreamBeginCapture(d.stream, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < steps; ++i) enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
+  for (int i = 0; i < steps; ++i) enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision, s->scheme, s->method);
   SUBFV_CUDA(cudaStreamEndCapture(d.stream, &g));
   cudaError_t e = cudaGraphInstantiate(&s->graph, g, 0);
   cudaGraphDestroy(g);
@@ -435,7 +480,8 @@ int subfv_lag_advance_async(subfv_lag_state* s, int n_steps) {
     if (lag_graph(s, chunk)) return -1;
     for (int i = 0; i + chunk <= n_steps; i += chunk) SUBFV_CUDA(cudaGraphLaunch(s->graph, d.stream));
   }
-  for (int i = 0; i < n_steps % chunk; ++i) enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
+  for (int i = 0; i < n_steps % chunk; ++i)
+    enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision, s->scheme, s->method);
   SUBFV_CUDA(cudaGetLastError());
   return 0;
 }
@@ -498,7 +544,7 @@ int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout) {
   std::memcpy(s->host_stage, sol_inout, bytes);
   SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, s->host_stage, bytes, cudaMemcpyHostToDevice, d.stream));
   launch_pack6(d, d.ne, s->dev_stage, nullptr, s->sol6);
-  enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision);
+  enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision, s->scheme, s->method);
   d.geom_partial = 1;
   launch_unpack6(d, d.ne, kRec, s->sol6, s->dev_stage);
   SUBFV_CUDA(cudaMemcpyAsync(s->host_stage, s->dev_stage, bytes, cudaMemcpyDeviceToHost, d.stream));

@@ -213,12 +213,126 @@ __global__ void __launch_bounds__(128) k_lag_node(DevMesh m, const LagScalars* s
   lag_node_body<P>(m, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
+// Scheme "sidil" (lagrange_module.F90:149-223, 538-809), one thread per vertex, FP64:
+// nodal velocity and pressure from the volume-weighted averages of the vertex's subcells
+// (lag_to_primit: 1/tau, u, p), corrected by the subface jumps of p (velocity) and of
+// u.n (pressure) over the vertex's subfaces, the pressure gradient projected off the
+// boundary normal at boundary vertices, with h_p = c V_p / sum |corner normal| of
+// compute_length (c = 0, 1, 2, 4, 8 for method 0..4). vp[v] = (velocity, nodal p).
+// Across a boundary face the right state is the left one with its velocity mirrored.
+__device__ inline void lag_sidil_node_body(const DevMesh& m, const double* __restrict__ sol6, int method,
+                                           const int v) {
+  if (v >= m.nv) return;
+  double vx = 0.0, vy = 0.0, vz = 0.0, rho_p = 0.0, a_p = 0.0, pp = 0.0;
+  for (int q = m.vse_off[v]; q < m.vse_off[v + 1]; ++q) {
+    const int se = m.vse[q];
+    const U5 u = ld_u(sol6, m.se_elem[se]);
+    const double vol = m.vol_se[se], w0 = 1.0 / u.t;
+    vx = vx + vol * u.u;
+    vy = vy + vol * u.v;
+    vz = vz + vol * u.w;
+    rho_p = rho_p + vol * w0;
+    a_p = a_p + vol * sqrt(kGamma * u.p / w0);
+    pp = pp + vol * u.p;
+  }
+  const double V = m.vol_v[v];
+  rho_p = rho_p / V;
+  a_p = a_p / V;
+  vx = vx / V;
+  vy = vy / V;
+  vz = vz / V;
+  pp = pp / V;
+  double g0 = 0.0, g1 = 0.0, g2 = 0.0, div_v = 0.0, b0 = 0.0, b1 = 0.0, b2 = 0.0;
+  for (int q = m.vsf_off[v]; q < m.vsf_off[v + 1]; ++q) {
+    const int sf = m.vsf[q], f = m.sf_face[sf];
+    const int2 lr = m.flr[f];
+    const double4 fn = m.fn[f];
+    const double area = m.sfa[sf];
+    const U5 ul = ld_u(sol6, lr.x);
+    double r1, r2, r3, rp;
+    if (lr.y >= 0) {
+      const U5 ur = ld_u(sol6, lr.y);
+      r1 = ur.u;
+      r2 = ur.v;
+      r3 = ur.w;
+      rp = ur.p;
+    } else {
+      const double d = dot3(ul.u, ul.v, ul.w, fn.x, fn.y, fn.z);
+      r1 = ul.u - 2.0 * d * fn.x;
+      r2 = ul.v - 2.0 * d * fn.y;
+      r3 = ul.w - 2.0 * d * fn.z;
+      rp = lag_pressure(ul.t, r1, r2, r3, ul.e);
+      b0 = b0 + area * fn.x;  // boundary_normal: the faces with right_neigh <= 0
+      b1 = b1 + area * fn.y;
+      b2 = b2 + area * fn.z;
+    }
+    g0 = g0 + (rp - ul.p) * area * fn.x;
+    g1 = g1 + (rp - ul.p) * area * fn.y;
+    g2 = g2 + (rp - ul.p) * area * fn.z;
+    div_v = div_v + dot3(r1 - ul.u, r2 - ul.v, r3 - ul.w, area * fn.x, area * fn.y, area * fn.z);
+  }
+  g0 = g0 / V;
+  g1 = g1 / V;
+  g2 = g2 / V;
+  div_v = div_v / V;
+  if (m.is_bound[v]) {
+    const double nb = fnorm2_3(b0, b1, b2);
+    b0 = b0 / nb;
+    b1 = b1 / nb;
+    b2 = b2 / nb;
+    const double gb = dot3(g0, g1, g2, b0, b1, b2);
+    g0 = g0 - gb * b0;
+    g1 = g1 - gb * b1;
+    g2 = g2 - gb * b2;
+  }
+  double area_sum = 0.0;  // compute_length over corner_normal of each subcell
+  for (int q = m.vse_off[v]; q < m.vse_off[v + 1]; ++q) {
+    const int se = m.vse[q], c = m.se_elem[se];
+    const int4 ss = m.se_sf[se];
+    const int sfs[4] = {ss.x, ss.y, ss.z, ss.w};
+    double n0 = 0.0, n1 = 0.0, n2 = 0.0;
+    for (int k = 0; k < 4; ++k) {
+      if (sfs[k] < 0) break;
+      const int f = m.sf_face[sfs[k]];
+      const double4 fn = m.fn[f];
+      const double a = m.sfa[sfs[k]];
+      if (!m.b2d || fabs(fn.z) < 1e-12) {
+        if (m.flr[f].x == c) {
+          n0 = n0 + a * fn.x;
+          n1 = n1 + a * fn.y;
+          n2 = n2 + a * fn.z;
+        } else {
+          n0 = n0 - a * fn.x;
+          n1 = n1 - a * fn.y;
+          n2 = n2 - a * fn.z;
+        }
+      }
+    }
+    area_sum = area_sum + fnorm2_3(n0, n1, n2);
+  }
+  const double cm = method == 0 ? 0.0 : method == 1 ? 1.0 : method == 2 ? 2.0 : method == 3 ? 4.0 : 8.0;
+  const double h_p = cm * V / area_sum;
+  vx = vx - 0.5 * h_p / (rho_p * a_p) * g0;
+  vy = vy - 0.5 * h_p / (rho_p * a_p) * g1;
+  vz = vz - 0.5 * h_p / (rho_p * a_p) * g2;
+  pp = pp - 0.5 * h_p * rho_p * a_p * div_v;
+  if (pp < 0.0) atomicOr(m.status, kErrNegDensity);  // "Neg prex in sidil nodal" (:674-676)
+  m.vp[v] = make_double4(vx, vy, vz, pp);
+}
+__global__ void __launch_bounds__(128) k_lag_sidil_node(DevMesh m, const double* __restrict__ sol6,
+                                                        const LagScalars* sc, int method) {
+  if (sc && sc->done) return;
+  lag_sidil_node_body(m, sol6, method, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
 __device__ inline double warp_min(double x) {
   for (int o = 16; o > 0; o >>= 1) x = fmin(x, __shfl_xor_sync(0xffffffffu, x, o));
   return x;
 }
 
-// mode bit 1: rhs, bit 2: CFL terms; every thread of the block calls (block reduction)
+// mode bit 1: rhs, bit 2: CFL terms, bit 4: the rhs of scheme "sidil" (the nodal
+// pressure vp.w in place of the face's star pressures); every thread of the block calls
+// (block reduction)
 template <int P>
 __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict__ sol6, double* __restrict__ rhs6,
                                      double* dt_slot, const int mode, const int c) {
@@ -251,7 +365,7 @@ __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict_
           fnc[u] = m.fn[E.y];
           arc[u] = m.sfa[E.x];
           vpc[u] = m.vp[node];
-          if (mode & 1) {
+          if ((mode & 1) && !(mode & 4)) {
             const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)E.y);
             llc[u] = fr[0];
             vvc[u] = fr[1];
@@ -264,7 +378,24 @@ __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict_
         const int side = (Ec[u].z >> 30) & 1;
         const double4 fn = fnc[u];
         const double area = arc[u];
-        if (mode & 1) {
+        if ((mode & 5) == 5) {  // sidil: flux (-v.n, pp n, pp v.n) of the vertex
+          const double4 vpn = vpc[u];
+          const double v_et = dot3(vpn.x, vpn.y, vpn.z, fn.x, fn.y, fn.z);
+          const double am = area / mass, ps = vpn.w;
+          if (side == 0) {
+            r0 = r0 - am * (-v_et);
+            r1 = r1 - am * (ps * fn.x);
+            r2 = r2 - am * (ps * fn.y);
+            r3 = r3 - am * (ps * fn.z);
+            r4 = r4 - am * (ps * v_et);
+          } else {
+            r0 = r0 + am * (-v_et);
+            r1 = r1 + am * (ps * fn.x);
+            r2 = r2 + am * (ps * fn.y);
+            r3 = r3 + am * (ps * fn.z);
+            r4 = r4 + am * (ps * v_et);
+          }
+        } else if (mode & 1) {
           const double4 vpn = vpc[u];
           double v_et = dot3(vpn.x, vpn.y, vpn.z, fn.x, fn.y, fn.z);
           double am = area / mass;
@@ -527,6 +658,10 @@ void launch_lag_node_only(const DevMesh& m, const LagScalars* sc, int precision)
   if (precision == 1) k_lag_node<1><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sc);
   else k_lag_node<0><<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sc);
 }
+void launch_lag_sidil_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int method) {
+  launch_vert_volume(m);  // V_p of the current (moved) mesh
+  k_lag_sidil_node<<<grid_for(m.nv, kBlkNode), kBlkNode, 0, m.stream>>>(m, sol6, sc, method);
+}
 void launch_lag_cell(const DevMesh& m, const double* sol6, double* rhs6, LagScalars* sc, double* dt_slot,
                      int precision, int mode) {
   if (precision == 1)
@@ -568,10 +703,17 @@ void launch_lag_batch_step(const LagTable& t, int precision, cudaStream_t s) {
   kb_geom_step<<<g, geo::kGeoBlock, 0, s>>>(t.items, t.wc, t.hdr);
 }
 
-// One full time step of lagrange_main.F90:89-127 (graph-capturable: no host sync).
-void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision) {
-  launch_lag_node(m, sol6, sc, precision);
-  launch_lag_cell(m, sol6, rhs6, sc, &sc->dtmin, precision, 3);
+// One full time step of lagrange_main.F90:89-127 (graph-capturable: no host sync);
+// scheme 0 "classic", 1 "sidil" (FP64, method_length `method`).
+void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision, int scheme,
+                      int method) {
+  if (scheme == 1) {
+    launch_lag_sidil_node(m, sol6, sc, method);
+    launch_lag_cell(m, sol6, rhs6, sc, &sc->dtmin, 0, 7);
+  } else {
+    launch_lag_node(m, sol6, sc, precision);
+    launch_lag_cell(m, sol6, rhs6, sc, &sc->dtmin, precision, 3);
+  }
   launch_lag_finalize(m, sc);
   launch_lag_move(m, sc, 0.0);
   launch_geometry(m, 0, sol6, rhs6, sc);

@@ -23,7 +23,11 @@ void launch_vp_in(const DevMesh& m, const double* in);
 void launch_set_scalar(const DevMesh& m, double* p, double v);
 // fills m.centry (allocated by the caller, ncsf records) from the cell CSR
 void launch_build_cell_entries(const DevMesh& m);
-void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision);
+// scheme 0 "classic", 1 "sidil" (method_length `method`, FP64)
+void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision, int scheme = 0,
+                      int method = 0);
+// scheme "sidil": vertex volumes of the current mesh, then vp = (velocity, nodal pressure)
+void launch_lag_sidil_node(const DevMesh& m, const double* sol6, const LagScalars* sc, int method);
 
 // One problem of a batch: its mesh (moved by the steps), cell records, residual records
 // and scalars.

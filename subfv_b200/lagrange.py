@@ -36,6 +36,18 @@ def compute_rhs_lagrange(mesh: Mesh, sol, vp, dt, rhs, n_bc=0, bc_type=None, bc_
                  "subfv_compute_rhs_lagrange")
 
 
+def compute_rhs_lagrange_sidil(mesh: Mesh, sol, vp, dt, rhs, n_bc=0, bc_type=None, bc_val=None, b2d=True,
+                               mass=None, method=0, b2d_h=0.0):
+    """lagrange_module.F90:149-223 (scheme "sidil"). Fills vp (n_vert, 3) and rhs
+    (n_elems, 5) in place; returns the status bits (4: a negative nodal pressure)."""
+    sol = f64(sol)
+    mass = f64(mass)
+    assert vp.dtype == np.float64 and vp.flags["C_CONTIGUOUS"] and vp.shape == (mesh.n_vert, 3)
+    assert rhs.dtype == np.float64 and rhs.flags["C_CONTIGUOUS"] and rhs.shape == (mesh.n_elems, 5)
+    return check(_lib.load().subfv_compute_rhs_lagrange_sidil(mesh._h, pd(sol), pd(vp), pd(rhs), int(b2d), pd(mass),
+                                                              int(method)), "subfv_compute_rhs_lagrange_sidil")
+
+
 def compute_dt(mesh: Mesh, sol, dt, cfl, vp, me=0, num_procs=1) -> float:
     """lagrange_module.F90:240-283; returns the new dt (the reference's intent(inout))."""
     sol, vp = f64(sol), f64(vp)
@@ -94,6 +106,10 @@ class LagrangeState:
         check(_lib.load().subfv_lag_state_create(mesh._h, pd(sol), pd(mass), float(cfl), float(t0), float(t_max),
                                                 int(precision), C.byref(h)), "subfv_lag_state_create")
         self._h = h
+
+    def set_scheme(self, scheme: int, method: int = 0):
+        """0: "classic" (default); 1: "sidil" with method_length `method` (0..4)."""
+        check(_lib.load().subfv_lag_state_set_scheme(self._h, int(scheme), int(method)), "subfv_lag_state_set_scheme")
 
     def advance(self, n_steps: int):
         steps, t = C.c_int(), C.c_double()

@@ -161,3 +161,42 @@ def test_mesh_check_failure_is_reported(native, cuda_ok):
     m.set_coords(c)
     with pytest.raises(MeshCheckError):
         compute_geometry_mesh(m)
+
+
+@pytest.mark.parametrize("case", list(lagrange_cases()))
+@pytest.mark.parametrize("method", [0, 2, 4])
+def test_sidil_rhs_bit_exact(native, oracle_lib, cuda_ok, case, method):
+    """Scheme "sidil" (compute_rhs_lagrange_sidil with its nodal velocity and pressure,
+    lagrange_module.F90:149-223, 538-711): vp and rhs bit-identical to the oracle."""
+    from subfv_b200 import lagrange as L
+    m, o = _pair(lagrange_cases()[case])
+    sol = _random_state(m.n_elems, 5)
+    mass = m.geometry("elem_volume") / sol[:, 0]
+    vp = np.zeros((m.n_vert, 3))
+    rhs = np.zeros((m.n_elems, 5))
+    st = L.compute_rhs_lagrange_sidil(m, sol, vp, 0.0, rhs, b2d=m.b2d, mass=mass, method=method)
+    st_o, vp_o, rhs_o = o.lag_rhs_sidil(sol, mass, method)
+    assert st == st_o == 0
+    np.testing.assert_array_equal(vp, vp_o)
+    np.testing.assert_array_equal(rhs, rhs_o)
+
+
+@pytest.mark.parametrize("case", ["prism_jit", "hex_jit"])
+def test_sidil_run_bit_exact(native, oracle_lib, cuda_ok, case):
+    """The device time loop with scheme "sidil": state, moved mesh, vp, t and dt after 25
+    steps equal the oracle's lagrange_main loop with the same scheme."""
+    from subfv_b200.lagrange import LagrangeState
+    m, o = _pair(lagrange_cases()[case])
+    sol = _random_state(m.n_elems, 6)
+    mass = m.geometry("elem_volume") / sol[:, 0]
+    steps = 25
+    s = LagrangeState(m, sol, mass, cfl=0.5, t_max=1.0)
+    s.set_scheme(1, 2)
+    st, n, t = s.run(max_steps=steps)
+    assert st == 0 and n == steps
+    sol_o = sol.copy()
+    n_o, t_o, dt_o, vp_o = o.lag_run(sol_o, mass, 0.5, 1.0, steps, scheme=1, method=2)
+    assert n_o == steps and t == t_o and s.last_dt() == dt_o
+    np.testing.assert_array_equal(s.sol(), sol_o)
+    np.testing.assert_array_equal(m.coords(), o.geom("vert_coord"))
+    np.testing.assert_array_equal(s.vp(), vp_o)
