@@ -176,7 +176,8 @@ def test_sidil_rhs_bit_exact(native, oracle_lib, cuda_ok, case, method):
     rhs = np.zeros((m.n_elems, 5))
     st = L.compute_rhs_lagrange_sidil(m, sol, vp, 0.0, rhs, b2d=m.b2d, mass=mass, method=method)
     st_o, vp_o, rhs_o = o.lag_rhs_sidil(sol, mass, method)
-    assert st == st_o == 0
+    assert st == st_o  # the largest length scale gives negative nodal pressures (flagged) on this state
+    assert st == 0 or method == 4
     np.testing.assert_array_equal(vp, vp_o)
     np.testing.assert_array_equal(rhs, rhs_o)
 
