@@ -322,10 +322,23 @@ int subfv_bcsr_diag(subfv_bcsr* A, double* x, const double* b);
  * SUBFV_ERR_GMRES when not converged (the reference's conv = .false.). */
 int subfv_bcsr_gmres_diag(subfv_bcsr* A, double* x, const double* b, double tol, int m, int* conv,
                           int* restarts, double* rho);
+/* Colouring for the parallel LU-SGS preconditioner: colour (1..n_color_sets) of each
+ * block row, as bcsr_parallel_lusgs takes it (color, with color_set the rows of each
+ * colour; the order of rows inside a set does not change the result). */
+int subfv_bcsr_set_colors(subfv_bcsr* A, int n_color_sets, const int32_t* color);
+/* bcsr_parallel_lusgs(A, x, b, n_color_sets, color_set, color) — :1438-1502:
+ * x = (U+D)^-1 D (L+D)^-1 b, the sweeps ordered by colour set */
+int subfv_bcsr_parallel_lusgs(subfv_bcsr* A, double* x, const double* b);
+/* bcsr_gmres_parallel_lusgs — :885-993 with modifiedArnoldi_parallel_lusgs (:583-611):
+ * restarted GMRES(m) right-preconditioned by the coloured LU-SGS, 20 restarts,
+ * absolute tol; conv from the final true residual as the reference sets it */
+int subfv_bcsr_gmres_parallel_lusgs(subfv_bcsr* A, double* x, const double* b, double tol, int m, int* conv,
+                                    int* restarts, double* rho);
 /* bcsr_gmres — :194-290: unpreconditioned, 20 restarts */
 int subfv_bcsr_gmres(subfv_bcsr* A, double* x, const double* b, double tol, int m, int* conv,
                      int* restarts, double* rho);
-/* Either of the above (precond 1/0); H_first (m+1, m) receives the first Arnoldi Hessenberg. */
+/* Any of the above (precond 1 block Jacobi, 2 coloured LU-SGS, 0 none); H_first (m+1, m)
+ * receives the first Arnoldi Hessenberg. */
 int subfv_bcsr_gmres_ex(subfv_bcsr* A, double* x, const double* b, double tol, int m, int precond,
                         int* conv, int* restarts, double* rho, double* H_first);
 /* No counterpart in the reference: FP64 iterative refinement around block-Jacobi GMRES(m)

@@ -61,6 +61,9 @@ def load():
         lib.or_lu3.argtypes = [PD, PD, PD]
         lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]
+        lib.or_bcsr_parallel_lusgs.argtypes = [C.c_int, C.c_int, PI, PI, PD, C.c_int, PI, PD, PD]
+        lib.or_bcsr_gmres_lusgs.argtypes = [C.c_int, C.c_int, PI, PI, PD, C.c_int, PI, PD, PD, C.c_double, C.c_int,
+                                            PI, PD]
         lib.or_bcsr_gmres.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD, C.c_double, C.c_int, C.c_int, PI, PD, PD]
         lib.or_be_jacobian.restype = C.c_long
         lib.or_be_jacobian.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_double, PI, PI, PD, C.c_long]
@@ -271,6 +274,24 @@ class OracleBcsr:
         x = np.zeros(self.n)
         load().or_bcsr_diag(self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), _pd(x), _pd(b))
         return x
+
+    def parallel_lusgs(self, b, ncs, color):
+        b = np.ascontiguousarray(b, np.float64)
+        c = np.ascontiguousarray(color, np.int32)
+        x = np.zeros(self.n)
+        load().or_bcsr_parallel_lusgs(self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), int(ncs), _pi(c),
+                                      _pd(x), _pd(b))
+        return x
+
+    def gmres_lusgs(self, b, tol, m, ncs, color):
+        b = np.ascontiguousarray(b, np.float64)
+        c = np.ascontiguousarray(color, np.int32)
+        x = np.empty(self.n)
+        conv = np.zeros(1, np.int32)
+        rho = np.zeros(1)
+        it = load().or_bcsr_gmres_lusgs(self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), int(ncs),
+                                        _pi(c), _pd(x), _pd(b), float(tol), int(m), _pi(conv), _pd(rho))
+        return x, bool(conv[0]), it, float(rho[0])
 
     def gmres(self, b, tol, m=30, precond=True):
         b = np.ascontiguousarray(b, np.float64)

@@ -1,8 +1,9 @@
 // Test infrastructure only (oracle). Restatement of the BCSR linear algebra of
 // src/linear_algebra/sparse_bcsr_linear_module.F90: bcsr_matmul (:13-29), bcsr_diag
 // (:1414-1436) with lu_solve_noswp (linear_solver_module.F90:413-445),
-// modifiedArnoldi_diag + bcsr_gmres_diag (:1568-1691) and the unpreconditioned
-// bcsr_gmres (:194-290). norm2 is gfortran's scaled sum of squares and dot_product a
+// modifiedArnoldi_diag + bcsr_gmres_diag (:1568-1691), the unpreconditioned
+// bcsr_gmres (:194-290), and bcsr_parallel_lusgs with bcsr_gmres_parallel_lusgs and
+// modifiedArnoldi_parallel_lusgs (:1438-1502, :885-993, :583-611). norm2 is gfortran's scaled sum of squares and dot_product a
 // left-to-right sum, as the serial reference evaluates them.
 // PARITY UNPINNED (no Fortran compiler here).
 #include "oracle.h"
@@ -67,18 +68,70 @@ static void bcsr_diag(const Bcsr& A, double* x, const double* b) {
       }
 }
 
+// bcsr_parallel_lusgs (:1438-1502): colour sets ascending for (L+D) y = b (only blocks of
+// lower colours), descending for (U+D) x = D y (higher colours, then the diagonal LU);
+// color (m) 1..ncs, the rows of a set in ascending order
+static void bcsr_parallel_lusgs(const Bcsr& A, double* x, const double* b, int ncs, const int* color) {
+  const int bs = A.bs;
+  std::vector<double> y((size_t)bs * A.m), t(bs), tmp(bs);
+  std::vector<int> d(A.m);
+  for (int i = 1; i <= A.m; ++i)
+    for (int j = A.row[i - 1]; j <= A.row[i] - 1; ++j)
+      if (A.col[j - 1] == i) {
+        d[i - 1] = j;
+        break;
+      }
+  auto sub_blocks = [&](int i, int cs, bool lower, double* v, const double* u) {
+    for (int j = A.row[i - 1]; j <= A.row[i] - 1; ++j) {
+      const int c = A.col[j - 1];
+      if (lower ? !(color[c - 1] < cs) : !(color[c - 1] > cs)) continue;
+      const double* blk = A.v + (size_t)bs * bs * (j - 1);
+      const double* uc = u + (size_t)bs * (c - 1);
+      for (int r = 0; r < bs; ++r) {
+        double s = 0.0;
+        for (int k = 0; k < bs; ++k) s = s + blk[r + bs * k] * uc[k];
+        t[r] = s;
+      }
+      for (int r = 0; r < bs; ++r) v[r] = v[r] - t[r];
+    }
+  };
+  for (int cs = 1; cs <= ncs; ++cs)
+    for (int i = 1; i <= A.m; ++i) {
+      if (color[i - 1] != cs) continue;
+      double* yi = y.data() + (size_t)bs * (i - 1);
+      for (int r = 0; r < bs; ++r) yi[r] = b[(size_t)bs * (i - 1) + r];
+      sub_blocks(i, cs, true, yi, y.data());
+    }
+  for (int cs = ncs; cs >= 1; --cs)
+    for (int i = 1; i <= A.m; ++i) {
+      if (color[i - 1] != cs) continue;
+      double* xi = x + (size_t)bs * (i - 1);
+      double* yi = y.data() + (size_t)bs * (i - 1);
+      for (int r = 0; r < bs; ++r) xi[r] = yi[r];
+      sub_blocks(i, cs, false, xi, x);
+      for (int r = 0; r < bs; ++r) yi[r] = xi[r];
+      lu_solve_noswp(bs, A.v + (size_t)bs * bs * (d[i - 1] - 1), xi, yi);
+    }
+}
+
 static double dotp(const double* a, const double* b, long n) {
   double s = 0.0;
   for (long i = 0; i < n; ++i) s = s + a[i] * b[i];
   return s;
 }
 
-// GMRES(m) with restarts; precond = bcsr_gmres_diag (maxit 40), else bcsr_gmres (maxit 20).
-// H is (m+1, m) column-major; returns restarts used; *conv as the reference sets it.
-static int gmres(const Bcsr& A, double* x, const double* b, double tol, int m, bool precond, bool* conv,
-                 double* rho_out, double* H_first) {
+// GMRES(m) with restarts; precond 1 = bcsr_gmres_diag (maxit 40), 2 =
+// bcsr_gmres_parallel_lusgs (:885-993, maxit 20, colours ncs/color), 0 = bcsr_gmres
+// (maxit 20). H is (m+1, m) column-major; returns restarts used; *conv as the reference
+// sets it.
+static int gmres(const Bcsr& A, double* x, const double* b, double tol, int m, int precond, bool* conv,
+                 double* rho_out, double* H_first, int ncs = 0, const int* color = nullptr) {
   const long n = (long)A.bs * A.m;
-  const int maxit = precond ? 40 : 20;
+  const int maxit = precond == 1 ? 40 : 20;
+  auto apply_precond = [&](double* out, const double* in) {
+    if (precond == 2) bcsr_parallel_lusgs(A, out, in, ncs, color);
+    else bcsr_diag(A, out, in);
+  };
   std::vector<double> H((m + 1) * m, 0.0), V(n * (m + 1)), r(n), y(m + 1), c(m + 1), s(m + 1), z(m + 1), zp(n), w(n);
   auto h = [&](int i, int j) -> double& { return H[(i - 1) + (m + 1) * (j - 1)]; };  // 1-based
   auto Vc = [&](int j) { return V.data() + n * (j - 1); };
@@ -102,7 +155,7 @@ static int gmres(const Bcsr& A, double* x, const double* b, double tol, int m, b
     for (long i = 0; i < n; ++i) Vc(1)[i] = r[i];
     for (int jj = 2; jj <= m + 1; ++jj) {
       if (precond) {
-        bcsr_diag(A, Vc(jj), Vc(jj - 1));
+        apply_precond(Vc(jj), Vc(jj - 1));
         bcsr_matmul(A, Vc(jj), w.data());
       } else {
         bcsr_matmul(A, Vc(jj - 1), w.data());
@@ -153,7 +206,7 @@ static int gmres(const Bcsr& A, double* x, const double* b, double tol, int m, b
       for (long k = 0; k < n; ++k) r[k] = 0.0;
       for (int q = 1; q <= nr; ++q)
         for (long k = 0; k < n; ++k) r[k] = r[k] + z[q - 1] * Vc(q)[k];
-      bcsr_diag(A, zp.data(), r.data());
+      apply_precond(zp.data(), r.data());
       for (long k = 0; k < n; ++k) x[k] = x[k] + zp[k];
     } else {
       for (int q = 1; q <= nr; ++q)
@@ -163,11 +216,11 @@ static int gmres(const Bcsr& A, double* x, const double* b, double tol, int m, b
     for (long k = 0; k < n; ++k) r[k] = b[k] - w[k];
     rho = fnorm2(r.data(), (int)n);
     if (rho < tol) {
-      if (precond) *conv = true;
+      if (precond == 1) *conv = true;
       break;
     }
   }
-  if (!precond) {  // :284-289
+  if (precond != 1) {  // :284-289 and :987-992
     bcsr_matmul(A, x, w.data());
     for (long k = 0; k < n; ++k) r[k] = b[k] - w[k];
     *conv = !(fnorm2(r.data(), (int)n) > tol);
@@ -194,7 +247,20 @@ int or_bcsr_gmres(int m, int bs, const int* row, const int* col, const double* v
                   double tol, int krylov, int precond, int* conv, double* rho, double* H_first) {
   Bcsr A{m, m, bs, row, col, v};
   bool cv = false;
-  int it = gmres(A, x, b, tol, krylov, precond != 0, &cv, rho, H_first);
+  int it = gmres(A, x, b, tol, krylov, precond != 0 ? 1 : 0, &cv, rho, H_first);
+  *conv = cv ? 1 : 0;
+  return it;
+}
+void or_bcsr_parallel_lusgs(int m, int bs, const int* row, const int* col, const double* v, int ncs,
+                            const int* color, double* x, const double* b) {
+  Bcsr A{m, m, bs, row, col, v};
+  bcsr_parallel_lusgs(A, x, b, ncs, color);
+}
+int or_bcsr_gmres_lusgs(int m, int bs, const int* row, const int* col, const double* v, int ncs, const int* color,
+                        double* x, const double* b, double tol, int krylov, int* conv, double* rho) {
+  Bcsr A{m, m, bs, row, col, v};
+  bool cv = false;
+  int it = gmres(A, x, b, tol, krylov, 2, &cv, rho, nullptr, ncs, color);
   *conv = cv ? 1 : 0;
   return it;
 }

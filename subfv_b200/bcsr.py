@@ -1,6 +1,7 @@
 """Host mirror of the reference's sparse_bcsr_linear_module
 (src/linear_algebra/sparse_bcsr_linear_module.F90): bcsr_matrix_type, bcsr_matmul,
-bcsr_diag, bcsr_gmres_diag, bcsr_gmres; all compute on the GPU through the C-ABI.
+bcsr_diag, bcsr_gmres_diag, bcsr_gmres, bcsr_parallel_lusgs, bcsr_gmres_parallel_lusgs;
+all compute on the GPU through the C-ABI.
 """
 from __future__ import annotations
 
@@ -61,6 +62,27 @@ class DeviceBcsr:
         x = np.empty(self.n)
         check(_lib.load().subfv_bcsr_diag(self._h, pd(x), pd(b)), "subfv_bcsr_diag")
         return x
+
+    def set_colors(self, n_color_sets: int, color):
+        """Colour (1..n_color_sets) of each block row for the parallel LU-SGS."""
+        self._color = i32(color)
+        check(_lib.load().subfv_bcsr_set_colors(self._h, int(n_color_sets), pi(self._color)), "subfv_bcsr_set_colors")
+
+    def parallel_lusgs(self, b) -> np.ndarray:
+        """bcsr_parallel_lusgs (:1438-1502): x = (U+D)^-1 D (L+D)^-1 b by colour sets."""
+        b = f64(b)
+        x = np.empty(self.n)
+        check(_lib.load().subfv_bcsr_parallel_lusgs(self._h, pd(x), pd(b)), "subfv_bcsr_parallel_lusgs")
+        return x
+
+    def gmres_lusgs(self, b, tol, m=30):
+        """bcsr_gmres_parallel_lusgs (:885-993); returns (x, conv, restarts, rho)."""
+        b = f64(b)
+        x = np.empty(self.n)
+        conv, it, rho = C.c_int(), C.c_int(), C.c_double()
+        check(_lib.load().subfv_bcsr_gmres_ex(self._h, pd(x), pd(b), float(tol), int(m), 2, C.byref(conv),
+                                              C.byref(it), C.byref(rho), None), "subfv_bcsr_gmres_parallel_lusgs")
+        return x, bool(conv.value), it.value, rho.value
 
     def gmres(self, b, tol, m=30, precond=True, want_h=False):
         """bcsr_gmres_diag (precond) / bcsr_gmres; returns (x, conv, restarts, rho[, H_first])."""
@@ -144,3 +166,18 @@ def grid_matrix(nx, ny, nz, bs=5, stencil=27, seed=0, diag_shift=None, periodic=
     dmask = col == rr
     v[dmask] += shift * np.eye(bs)[None]
     return BcsrMatrix(m, bs, row + 1, col + 1, v)
+
+
+def greedy_colors(A: BcsrMatrix) -> tuple[int, np.ndarray]:
+    """A colouring of the block rows for the parallel LU-SGS (the reference takes it from
+    its caller): rows in order, each the smallest colour (1-based) not used by a coupled
+    row of lower index. Returns (n_color_sets, color)."""
+    row, col = np.asarray(A.row) - 1, np.asarray(A.col) - 1
+    color = np.zeros(A.m, np.int32)
+    for i in range(A.m):
+        used = {int(color[c]) for c in col[row[i]:row[i + 1]] if c < i}
+        k = 1
+        while k in used:
+            k += 1
+        color[i] = k
+    return int(color.max()), color

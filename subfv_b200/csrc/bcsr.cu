@@ -102,17 +102,12 @@ __global__ void k_factor_diag(int m, const int* __restrict__ diag, const double*
   for (int q = 0; q < BS * BS; ++q) lu[(size_t)q * m + i] = C[q];
 }
 
+// xv = D_i^-1 xv with the packed no-pivot LU of block row i (lu_solve_noswp's operations)
 template <int BS>
-__global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __restrict__ b,
-                          double* __restrict__ x) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= m) return;
+__device__ inline void lu_apply(const double* __restrict__ lu, int m, int i, double* xv) {
   double C[BS * BS];
 #pragma unroll
   for (int q = 0; q < BS * BS; ++q) C[q] = lu[(size_t)q * m + i];
-  double xv[BS];
-#pragma unroll
-  for (int k = 0; k < BS; ++k) xv[k] = b[(size_t)BS * i + k];
 #pragma unroll
   for (int k = 0; k < BS; ++k)
 #pragma unroll
@@ -124,8 +119,77 @@ __global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __
     for (int j = k + 1; j < BS; ++j) xv[k] = xv[k] - C[k + BS * j] * xv[j];
     xv[k] = xv[k] / C[k + BS * k];
   }
+}
+
+template <int BS>
+__global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __restrict__ b,
+                          double* __restrict__ x) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  double xv[BS];
+#pragma unroll
+  for (int k = 0; k < BS; ++k) xv[k] = b[(size_t)BS * i + k];
+  lu_apply<BS>(lu, m, i, xv);
 #pragma unroll
   for (int k = 0; k < BS; ++k) x[(size_t)BS * i + k] = xv[k];
+}
+
+// v_i = v_i - matmul(A_ij, u_col) over the row's blocks whose colour passes `pick`
+// (below the set's for the forward sweep, above it for the backward one), in row order
+template <int BS, bool FWD>
+__device__ inline void lusgs_row(const int* __restrict__ row, const int* __restrict__ col,
+                                 const double* __restrict__ v, const int* __restrict__ color, int cs, int i,
+                                 const double* u, double* vi) {
+  for (int j = row[i]; j < row[i + 1]; ++j) {
+    const int c = col[j];
+    const int cc = color[c];
+    if (FWD ? !(cc < cs) : !(cc > cs)) continue;
+    const double* blk = v + (size_t)BS * BS * j;
+    const double* uc = u + (size_t)BS * c;
+    double t[BS];
+#pragma unroll
+    for (int r = 0; r < BS; ++r) {
+      double a = 0.0;
+#pragma unroll
+      for (int k = 0; k < BS; ++k) a = a + blk[r + BS * k] * uc[k];
+      t[r] = a;
+    }
+#pragma unroll
+    for (int r = 0; r < BS; ++r) vi[r] = vi[r] - t[r];
+  }
+}
+
+// forward sweep of colour set cs: y_i = b_i - sum over lower colours of A_ij y_j
+template <int BS>
+__global__ void k_lusgs_fwd(int nrows, const int* __restrict__ rows, const int* __restrict__ row,
+                            const int* __restrict__ col, const double* __restrict__ v,
+                            const int* __restrict__ color, int cs, const double* __restrict__ b, double* y) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  const int i = rows[t];
+  double yi[BS];
+#pragma unroll
+  for (int r = 0; r < BS; ++r) yi[r] = b[(size_t)BS * i + r];
+  lusgs_row<BS, true>(row, col, v, color, cs, i, y, yi);
+#pragma unroll
+  for (int r = 0; r < BS; ++r) y[(size_t)BS * i + r] = yi[r];
+}
+// backward sweep of colour set cs: x_i = D_i^-1 (y_i - sum over higher colours of A_ij x_j)
+template <int BS>
+__global__ void k_lusgs_bwd(int nrows, const int* __restrict__ rows, const int* __restrict__ row,
+                            const int* __restrict__ col, const double* __restrict__ v,
+                            const int* __restrict__ color, int cs, const double* __restrict__ lu, int m,
+                            const double* __restrict__ y, double* x) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nrows) return;
+  const int i = rows[t];
+  double xi[BS];
+#pragma unroll
+  for (int r = 0; r < BS; ++r) xi[r] = y[(size_t)BS * i + r];
+  lusgs_row<BS, false>(row, col, v, color, cs, i, x, xi);
+  lu_apply<BS>(lu, m, i, xi);
+#pragma unroll
+  for (int r = 0; r < BS; ++r) x[(size_t)BS * i + r] = xi[r];
 }
 
 __device__ inline double warp_tree(double v) {
@@ -343,7 +407,7 @@ int bcsr_set_values(DevBcsr* A, const double* v, bool on_device) {
 }
 
 void bcsr_free(DevBcsr* A) {
-  void* p[] = {A->row, A->col, A->v, A->v32, A->diag, A->lu};
+  void* p[] = {A->row, A->col, A->v, A->v32, A->diag, A->lu, A->color, A->set_rows};
   for (void* q : p)
     if (q) cudaFree(q);
   if (A->own_stream && A->stream) cudaStreamDestroy(A->stream);
@@ -359,17 +423,18 @@ int gmres_work_alloc(GmresWork* W, long n, int krylov) {
   SUBFV_CUDA(cudaMalloc(&W->zp, n * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&W->d, n * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&W->rr, n * sizeof(double)));
+  SUBFV_CUDA(cudaMalloc(&W->ty, n * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&W->z, (krylov + 2) * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&W->partial, 2 * kRedBlocks * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&W->H, (size_t)(krylov + 1) * krylov * sizeof(double)));
   SUBFV_CUDA(cudaMalloc(&W->scal, 8 * sizeof(double)));
-  W->bytes = (size_t)n * (krylov + 6) * 8;
+  W->bytes = (size_t)n * (krylov + 7) * 8;
   return 0;
 }
 
 void gmres_work_free(GmresWork* W) {
   if (W->cycle) cudaGraphExecDestroy(W->cycle);
-  void* p[] = {W->V, W->r, W->w, W->zp, W->z, W->partial, W->H, W->scal, W->d, W->rr};
+  void* p[] = {W->V, W->r, W->w, W->zp, W->z, W->partial, W->H, W->scal, W->d, W->rr, W->ty};
   for (void* q : p)
     if (q) cudaFree(q);
   *W = GmresWork();
@@ -430,11 +495,73 @@ double device_norm2(const DevBcsr& A, GmresWork& W, const double* x, long n) {
   return std::sqrt(s);
 }
 
+void launch_bcsr_lusgs(const DevBcsr& A, const double* b, double* x, double* ty) {
+  for (int cs = 1; cs <= A.ncs; ++cs) {
+    const int o = A.set_off[cs - 1], n = A.set_off[cs] - o;
+    if (n == 0) continue;
+    const int g = (n + 127) / 128;
+    switch (A.bs) {
+      case 5: k_lusgs_fwd<5><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, b, ty); break;
+      case 4: k_lusgs_fwd<4><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, b, ty); break;
+      case 3: k_lusgs_fwd<3><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, b, ty); break;
+      default: k_lusgs_fwd<1><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, b, ty);
+    }
+  }
+  for (int cs = A.ncs; cs >= 1; --cs) {
+    const int o = A.set_off[cs - 1], n = A.set_off[cs] - o;
+    if (n == 0) continue;
+    const int g = (n + 127) / 128;
+    switch (A.bs) {
+      case 5:
+        k_lusgs_bwd<5><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, A.lu, A.m, ty, x);
+        break;
+      case 4:
+        k_lusgs_bwd<4><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, A.lu, A.m, ty, x);
+        break;
+      case 3:
+        k_lusgs_bwd<3><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, A.lu, A.m, ty, x);
+        break;
+      default:
+        k_lusgs_bwd<1><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, A.lu, A.m, ty, x);
+    }
+  }
+}
+
+int bcsr_set_colors(DevBcsr* A, int ncs, const int* color) {
+  if (ncs < 1 || ncs > A->m) {
+    set_error("subfv_bcsr_set_colors: the number of colour sets must be in [1, m]");
+    return -2;
+  }
+  std::vector<int> cnt(ncs + 1, 0);
+  for (int i = 0; i < A->m; ++i) {
+    if (color[i] < 1 || color[i] > ncs) {
+      set_error("subfv_bcsr_set_colors: colour out of [1, n_color_sets]");
+      return -2;
+    }
+    cnt[color[i]]++;
+  }
+  std::vector<int> off(ncs + 1, 0), rows(A->m);
+  for (int c = 1; c <= ncs; ++c) off[c] = off[c - 1] + cnt[c];
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (int i = 0; i < A->m; ++i) rows[fill[color[i] - 1]++] = i;  // ascending rows within a set
+  if (A->color) cudaFree(A->color);
+  if (A->set_rows) cudaFree(A->set_rows);
+  A->color = A->set_rows = nullptr;
+  SUBFV_CUDA(cudaMalloc(&A->color, A->m * sizeof(int)));
+  SUBFV_CUDA(cudaMalloc(&A->set_rows, A->m * sizeof(int)));
+  SUBFV_CUDA(cudaMemcpyAsync(A->color, color, A->m * sizeof(int), cudaMemcpyHostToDevice, A->stream));
+  SUBFV_CUDA(cudaMemcpyAsync(A->set_rows, rows.data(), A->m * sizeof(int), cudaMemcpyHostToDevice, A->stream));
+  SUBFV_CUDA(cudaStreamSynchronize(A->stream));
+  A->ncs = ncs;
+  A->set_off = off;
+  return 0;
+}
+
 namespace {
 // One restart cycle's Arnoldi process: V_1 = r/|r| (|r|^2 from the partials that the
 // preceding device_norm2 left in W.partial), then columns 2..m+1 with modified
 // Gram-Schmidt, H on the device. Launch-only (no host decision), so it can be captured.
-void arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
+void arnoldi_cycle(const DevBcsr& A, GmresWork& W, int precond, bool fp32) {
   const int m = W.krylov;
   const long n = W.n;
   cudaStream_t s = A.stream;
@@ -446,7 +573,8 @@ void arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
   k_normalize<<<kRedBlocks, kRedThreads, 0, s>>>(W.r, Vc(1), pa, kRedBlocks, W.scal, n);
   for (int jj = 2; jj <= m + 1; ++jj) {
     if (precond) {
-      launch_bcsr_bjacobi(A, Vc(jj - 1), W.zp);
+      if (precond == kPrecondLusgs) launch_bcsr_lusgs(A, Vc(jj - 1), W.zp, W.ty);
+      else launch_bcsr_bjacobi(A, Vc(jj - 1), W.zp);
       launch_bcsr_spmv(A, W.zp, Vc(jj), fp32);
     } else {
       launch_bcsr_spmv(A, Vc(jj - 1), Vc(jj), fp32);
@@ -462,10 +590,10 @@ void arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
 }
 
 // Replays the cycle from a graph captured for this matrix, workspace and mode.
-int run_arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
+int run_arnoldi_cycle(const DevBcsr& A, GmresWork& W, int precond, bool fp32) {
   const uintptr_t key[] = {(uintptr_t)A.row, (uintptr_t)A.col, (uintptr_t)A.v, (uintptr_t)A.v32, (uintptr_t)A.lu,
-                           (uintptr_t)A.nnz, (uintptr_t)A.m, (uintptr_t)A.bs, (uintptr_t)A.stream,
-                           (uintptr_t)(precond ? 1 : 0) | (fp32 ? 2 : 0)};
+                           (uintptr_t)A.nnz, (uintptr_t)A.m, (uintptr_t)A.set_rows, (uintptr_t)A.stream,
+                           (uintptr_t)precond | (fp32 ? 4 : 0) | ((uintptr_t)A.bs << 3) | ((uintptr_t)A.ncs << 8)};
   static_assert(sizeof(key) == sizeof(W.cycle_key), "cycle key size");
   if (W.cycle && std::memcmp(key, W.cycle_key, sizeof(key)) != 0) {
     cudaGraphExecDestroy(W.cycle);
@@ -489,7 +617,7 @@ int run_arnoldi_cycle(const DevBcsr& A, GmresWork& W, bool precond, bool fp32) {
 }
 }  // namespace
 
-int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, bool precond, bool fp32,
+int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, int precond, bool fp32,
                  int maxit, GmresStats* st, double* H_first_host) {
   const int m = W.krylov;
   const long n = W.n;
@@ -551,7 +679,8 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
     SUBFV_CUDA(cudaMemcpyAsync(W.z, z.data(), nr * sizeof(double), cudaMemcpyHostToDevice, s));
     if (precond) {
       k_lincomb<<<egrid(n), 256, 0, s>>>(W.V, n, W.z, nr, nullptr, W.r);
-      launch_bcsr_bjacobi(A, W.r, W.zp);
+      if (precond == kPrecondLusgs) launch_bcsr_lusgs(A, W.r, W.zp, W.ty);
+      else launch_bcsr_bjacobi(A, W.r, W.zp);
       k_add<<<egrid(n), 256, 0, s>>>(x, W.zp, n);
     } else {
       k_lincomb<<<egrid(n), 256, 0, s>>>(W.V, n, W.z, nr, x, x);
@@ -561,11 +690,11 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
     rho = device_norm2(A, W, W.r, n);
     if (rho < 0.0) return -1;
     if (rho < tol) {
-      if (precond) st->conv = 1;
+      if (precond == kPrecondDiag) st->conv = 1;
       break;
     }
   }
-  if (!precond) {
+  if (precond != kPrecondDiag) {  // bcsr_gmres (:284-289) and bcsr_gmres_parallel_lusgs (:987-992)
     launch_bcsr_spmv(A, x, W.w, fp32);
     k_sub<<<egrid(n), 256, 0, s>>>(b, W.w, W.r, n);
     const double r2 = device_norm2(A, W, W.r, n);

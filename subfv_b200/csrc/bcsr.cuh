@@ -20,6 +20,12 @@ struct DevBcsr {
   float* v32 = nullptr;    // FP32 copy for the iterative-refinement inner solves
   int* diag = nullptr;     // (m) index of the diagonal block, -1 if absent
   double* lu = nullptr;    // (bs*bs, m) no-pivot LU, element-major: multipliers below the diagonal, U on and above
+  // colouring for the parallel LU-SGS preconditioner (bcsr_parallel_lusgs): colour per
+  // block row (1..ncs), the rows grouped by colour, and the groups' offsets (host)
+  int ncs = 0;
+  int* color = nullptr;
+  int* set_rows = nullptr;
+  std::vector<int> set_off;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   size_t bytes = 0;
@@ -40,6 +46,7 @@ struct GmresWork {
   double *V = nullptr, *r = nullptr, *w = nullptr, *zp = nullptr, *z = nullptr;
   double *partial = nullptr, *H = nullptr, *scal = nullptr;
   double *d = nullptr, *rr = nullptr;  // refinement correction and residual
+  double* ty = nullptr;                 // the LU-SGS forward sweep
   size_t bytes = 0;
   cudaGraphExec_t cycle = nullptr;  // the captured Arnoldi cycle and what it was captured for
   uintptr_t cycle_key[10] = {};
@@ -54,9 +61,18 @@ void gmres_work_free(GmresWork* W);
 void launch_bcsr_spmv(const DevBcsr& A, const double* x, double* y, bool fp32_matrix);
 void launch_bcsr_factor_diag(const DevBcsr& A);
 void launch_bcsr_bjacobi(const DevBcsr& A, const double* b, double* x);
+// bcsr_parallel_lusgs (:1438-1502): x = (U+D)^-1 D (L+D)^-1 b by colour sets; ty is an
+// n-vector of scratch (the forward sweep)
+void launch_bcsr_lusgs(const DevBcsr& A, const double* b, double* x, double* ty);
+// colours (1..ncs) per block row, host array; rejects colours out of range
+int bcsr_set_colors(DevBcsr* A, int ncs, const int* color);
 
-// bcsr_gmres_diag (precond) or bcsr_gmres; x, b device vectors; tol absolute.
-int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, bool precond,
+// preconditioners of gmres_device
+enum GmresPrecond { kPrecondNone = 0, kPrecondDiag = 1, kPrecondLusgs = 2 };
+
+// bcsr_gmres_diag (precond 1), bcsr_gmres_parallel_lusgs (2) or bcsr_gmres (0); x, b
+// device vectors; tol absolute.
+int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, int precond,
                  bool fp32_matrix, int maxit, GmresStats* st, double* H_first_host);
 // FP64 iterative refinement around FP32-matrix GMRES: stops at |b - A x| < rel_tol * |b|.
 int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double rel_tol,

@@ -88,17 +88,51 @@ int subfv_bcsr_gmres_ex(subfv_bcsr* h, double* x, const double* b, double tol, i
     set_error("subfv_bcsr_gmres: Krylov dimension must be in [1, 200]");
     return -2;
   }
+  if (precond < 0 || precond > 2 || (precond == kPrecondLusgs && h->A.ncs < 1)) {
+    set_error("subfv_bcsr_gmres: precond 0, 1 or 2 (2 needs subfv_bcsr_set_colors first)");
+    return -2;
+  }
   if (ensure_vecs(h) || ensure_work(h, m)) return -1;
   const size_t n = (size_t)h->A.m * h->A.bs;
   SUBFV_CUDA(cudaMemcpyAsync(h->b, b, n * sizeof(double), cudaMemcpyHostToDevice, h->A.stream));
   GmresStats st;
-  if (gmres_device(h->A, h->W, h->x, h->b, tol, precond != 0, false, precond ? 40 : 20, &st, H_first)) return -1;
+  // maxit: 40 restarts for bcsr_gmres_diag (:1603), 20 for bcsr_gmres and the LU-SGS variant (:205, :898)
+  if (gmres_device(h->A, h->W, h->x, h->b, tol, precond, false, precond == kPrecondDiag ? 40 : 20, &st, H_first))
+    return -1;
   SUBFV_CUDA(cudaMemcpyAsync(x, h->x, n * sizeof(double), cudaMemcpyDeviceToHost, h->A.stream));
   SUBFV_CUDA(cudaStreamSynchronize(h->A.stream));
   if (conv) *conv = st.conv;
   if (restarts) *restarts = st.restarts;
   if (rho) *rho = st.rho;
   return st.conv ? 0 : SUBFV_ERR_GMRES;
+}
+
+int subfv_bcsr_set_colors(subfv_bcsr* h, int n_color_sets, const int32_t* color) {
+  if (!h || !color) {
+    set_error("subfv_bcsr_set_colors: null argument");
+    return -2;
+  }
+  return bcsr_set_colors(&h->A, n_color_sets, color);
+}
+
+int subfv_bcsr_parallel_lusgs(subfv_bcsr* h, double* x, const double* b) {
+  if (h->A.ncs < 1) {
+    set_error("subfv_bcsr_parallel_lusgs: no colouring (subfv_bcsr_set_colors)");
+    return -2;
+  }
+  if (ensure_vecs(h) || ensure_work(h, h->W.krylov > 0 ? h->W.krylov : 1)) return -1;
+  const size_t n = (size_t)h->A.m * h->A.bs;
+  SUBFV_CUDA(cudaMemcpyAsync(h->b, b, n * sizeof(double), cudaMemcpyHostToDevice, h->A.stream));
+  launch_bcsr_lusgs(h->A, h->b, h->x, h->W.ty);
+  SUBFV_CUDA(cudaMemcpyAsync(x, h->x, n * sizeof(double), cudaMemcpyDeviceToHost, h->A.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(h->A.stream));
+  SUBFV_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int subfv_bcsr_gmres_parallel_lusgs(subfv_bcsr* h, double* x, const double* b, double tol, int m, int* conv,
+                                    int* restarts, double* rho) {
+  return subfv_bcsr_gmres_ex(h, x, b, tol, m, kPrecondLusgs, conv, restarts, rho, nullptr);
 }
 
 int subfv_bcsr_gmres_diag(subfv_bcsr* h, double* x, const double* b, double tol, int m, int* conv, int* restarts,

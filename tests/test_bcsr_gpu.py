@@ -92,3 +92,37 @@ def test_iterative_refinement_fp32_matrix(native, cuda_ok):
     assert np.linalg.norm(b - _dense(A) @ x) < 1e-8 * np.linalg.norm(b)
     x64, conv64, _, _ = d.gmres(b, 1e-8 * np.linalg.norm(b), 30)
     assert np.abs(x - x64).max() <= 1e-6 * np.abs(x64).max()
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_parallel_lusgs_bit_exact(native, oracle_lib, cuda_ok, case):
+    """bcsr_parallel_lusgs (:1438-1502) with a greedy colouring: bit-identical."""
+    from oracle.oracle import OracleBcsr
+    from subfv_b200.bcsr import DeviceBcsr, greedy_colors
+    A = _mat(case)
+    ncs, color = greedy_colors(A)
+    d, o = DeviceBcsr(A), OracleBcsr(A)
+    d.set_colors(ncs, color)
+    b = np.random.default_rng(9).normal(size=d.n)
+    np.testing.assert_array_equal(d.parallel_lusgs(b), o.parallel_lusgs(b, ncs, color))
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_gmres_parallel_lusgs_matches_oracle(native, oracle_lib, cuda_ok, case):
+    """bcsr_gmres_parallel_lusgs (:885-993): same restarts and convergence flag, solution
+    within 1e-9 of the oracle's (dot products by a fixed tree), true residual below tol."""
+    from oracle.oracle import OracleBcsr
+    from subfv_b200.bcsr import DeviceBcsr, greedy_colors
+    A = _mat(case)
+    ncs, color = greedy_colors(A)
+    d, o = DeviceBcsr(A), OracleBcsr(A)
+    d.set_colors(ncs, color)
+    b = np.random.default_rng(10).normal(size=d.n)
+    tol = 1e-8 * np.linalg.norm(b)
+    m = 30 if d.n > 40 else 8
+    x, conv, it, rho = d.gmres_lusgs(b, tol, m)
+    xo, convo, ito, rhoo = o.gmres_lusgs(b, tol, m, ncs, color)
+    assert conv == convo and it == ito
+    assert np.abs(x - xo).max() <= 1e-9 * np.abs(xo).max()
+    if conv:
+        assert np.linalg.norm(b - _dense(A) @ x) < 1.5 * tol
