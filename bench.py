@@ -300,7 +300,8 @@ def run_implicit(args, rank, world, local):
     0.3 plus 8 seeded Fourier velocity modes (5%); one backward-Euler step: first-order
     two-wave residual, its exact frozen-speed Jacobian (5x5 BCSR, 7-point face stencil),
     block-Jacobi GMRES(30) to 1e-8 relative, CFL 10. FP64 GMRES and FP32-matrix GMRES
-    inside FP64 iterative refinement."""
+    inside FP64 iterative refinement; FP64 GMRES with the coloured LU-SGS preconditioner
+    beside them."""
     import torch
     from subfv_b200 import meshgen
     from subfv_b200.mesh import Mesh
@@ -314,19 +315,19 @@ def run_implicit(args, rank, world, local):
     cfg = NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5)
     res = {"metric": "cell-updates/s", "workload": f"periodic_box_{n}^3_backward_euler", "cells": mesh.n_elems,
            "mesh_setup_s": setup_s}
-    for name, refine in (("fp64", False), ("fp32_refine", True)):
+    for name, refine, pc in (("fp64", False, 1), ("fp32_refine", True, 1), ("fp64_lusgs", False, 2)):
         s = NsState(mesh, cfg, sol0)
-        s.implicit_step(cfl_implicit=10.0, refine_fp32=refine)  # warm-up (pattern, workspace)
+        s.implicit_step(cfl_implicit=10.0, refine_fp32=refine, precond=pc)  # warm-up (pattern, workspace)
         s2 = NsState(mesh, cfg, sol0)
-        s2.implicit_step(cfl_implicit=10.0, refine_fp32=refine)
+        s2.implicit_step(cfl_implicit=10.0, refine_fp32=refine, precond=pc)
         s3 = NsState(mesh, cfg, sol0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        st, stats = s3.implicit_step(cfl_implicit=10.0, refine_fp32=refine)
+        st, stats = s3.implicit_step(cfl_implicit=10.0, refine_fp32=refine, precond=pc)
         el = time.perf_counter() - t0
         # a second step on the same state: no per-state uploads or workspace allocation
         t1 = time.perf_counter()
-        st2, stats2 = s3.implicit_step(cfl_implicit=10.0, refine_fp32=refine)
+        st2, stats2 = s3.implicit_step(cfl_implicit=10.0, refine_fp32=refine, precond=pc)
         el2 = time.perf_counter() - t1
         dev_ms = stats["ms_assemble"] + stats["ms_solve"] + stats["ms_update"]
         stats["device_ms"] = dev_ms

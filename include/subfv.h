@@ -220,6 +220,11 @@ typedef struct subfv_implicit_stats {
 } subfv_implicit_stats;
 int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
                            subfv_implicit_stats* stats);
+/* The same with the preconditioner chosen: 1 block Jacobi (bcsr_gmres_diag, 40
+ * restarts), 2 the coloured LU-SGS (bcsr_gmres_parallel_lusgs, 20 restarts; the cells
+ * are coloured greedily in order, once per mesh). */
+int subfv_ns_implicit_step_ex(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
+                              int precond, subfv_implicit_stats* out);
 /* The assembled matrix at the state's current U for a given dt (bcsr_matrix_type layout,
  * 1-based row/col, blocks column-major); returns the number of blocks. */
 int subfv_ns_be_jacobian(subfv_ns_state* s, double dt, int32_t* row, int32_t* col, double* v, int64_t cap);

@@ -68,6 +68,7 @@ SIGNATURES = {
     "subfv_ns_residuals": (c_int, [P, PD, PD, PD]),
     "subfv_ns_init_gresho": (c_int, [P, c_dbl, PD]),
     "subfv_ns_implicit_step": (c_int, [P, c_dbl, c_int, c_dbl, c_int, P]),
+    "subfv_ns_implicit_step_ex": (c_int, [P, c_dbl, c_int, c_dbl, c_int, c_int, P]),
     "subfv_ns_be_jacobian": (c_int, [P, c_dbl, PI32, PI32, PD, c_i64]),
     "subfv_ns_batch_create": (c_int, [P, c_int, c_i64, C.POINTER(P)]),
     "subfv_ns_batch_destroy": (c_int, [P]),

@@ -708,7 +708,7 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
 }
 
 int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double rel_tol,
-                        double inner_rel_tol, int max_outer, GmresStats* st) {
+                        double inner_rel_tol, int max_outer, GmresStats* st, int precond) {
   const long n = W.n;
   cudaStream_t s = A.stream;
   const double bnorm = device_norm2(A, W, b, n);
@@ -725,7 +725,7 @@ int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double*
       break;
     }
     GmresStats in;
-    if (gmres_device(A, W, W.d, W.rr, inner_rel_tol * rn, true, true, 40, &in, nullptr)) return -1;
+    if (gmres_device(A, W, W.d, W.rr, inner_rel_tol * rn, precond, true, 40, &in, nullptr)) return -1;
     st->inner_total += in.restarts;
     k_add<<<egrid(n), 256, 0, s>>>(x, W.d, n);
     launch_bcsr_spmv(A, x, W.w, false);  // FP64 residual

@@ -76,7 +76,7 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
                  bool fp32_matrix, int maxit, GmresStats* st, double* H_first_host);
 // FP64 iterative refinement around FP32-matrix GMRES: stops at |b - A x| < rel_tol * |b|.
 int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double rel_tol,
-                        double inner_rel_tol, int max_outer, GmresStats* st);
+                        double inner_rel_tol, int max_outer, GmresStats* st, int precond = kPrecondDiag);
 double device_norm2(const DevBcsr& A, GmresWork& W, const double* x, long n);
 
 }  // namespace subfv

@@ -280,6 +280,8 @@ int up(T** d, const std::vector<T>& h, cudaStream_t s) {
 struct ImplicitPattern {
   std::vector<int> jq_off, jq, jblk, row_off, dblk;
   std::vector<int> row1, col1;  // 1-based (bcsr_matrix_type)
+  int ncs = 0;                  // greedy colouring of the rows for the LU-SGS preconditioner
+  std::vector<int> color;
 };
 
 int build_pattern(DevMesh& d, ImplicitPattern& P) {
@@ -338,6 +340,20 @@ int build_pattern(DevMesh& d, ImplicitPattern& P) {
   P.col1.resize(col.size());
   for (int i = 0; i <= ne; ++i) P.row1[i] = row_off[i] + 1;
   for (size_t j = 0; j < col.size(); ++j) P.col1[j] = col[j] + 1;
+  // rows in order, each the smallest colour not taken by a coupled row of lower index
+  // (the pattern is symmetric: cell adjacency)
+  P.color.assign(ne, 0);
+  P.ncs = 0;
+  std::vector<int> seen;
+  for (int i = 0; i < ne; ++i) {
+    seen.assign(P.ncs + 2, 0);
+    for (int j = row_off[i]; j < row_off[i + 1]; ++j)
+      if (col[j] < i) seen[P.color[col[j]]] = 1;
+    int k = 1;
+    while (seen[k]) ++k;
+    P.color[i] = k;
+    P.ncs = std::max(P.ncs, k);
+  }
   return 0;
 }
 
@@ -366,7 +382,9 @@ int implicit_setup(subfv_ns_state* s, int krylov) {
     c->row1 = P.row1;
     c->col1 = P.col1;
     const int ne = d.ne;
-    if (bcsr_upload(&c->A, ne, 5, c->row1.data(), c->col1.data(), nullptr, d.stream)) return -1;
+    if (bcsr_upload(&c->A, ne, 5, c->row1.data(), c->col1.data(), nullptr, d.stream) ||
+        bcsr_set_colors(&c->A, P.ncs, P.color.data()))
+      return -1;
     if (up(&c->jq_off, P.jq_off, d.stream) || up(&c->jq, P.jq, d.stream) || up(&c->jblk, P.jblk, d.stream) ||
         up(&c->row_off, P.row_off, d.stream) || up(&c->dblk, P.dblk, d.stream))
       return -1;
@@ -418,7 +436,12 @@ extern "C" {
 
 int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
                            subfv_implicit_stats* out) {
-  if (!s || krylov < 1 || krylov > 200 || !(rel_tol > 0.0)) {
+  return subfv_ns_implicit_step_ex(s, cfl_implicit, krylov, rel_tol, refine_fp32, 1, out);
+}
+
+int subfv_ns_implicit_step_ex(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
+                              int precond, subfv_implicit_stats* out) {
+  if (!s || krylov < 1 || krylov > 200 || !(rel_tol > 0.0) || (precond != 1 && precond != 2)) {
     set_error("subfv_ns_implicit_step: bad argument");
     return -2;
   }
@@ -435,9 +458,11 @@ int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, d
   const double bnorm = device_norm2(c->A, c->W, c->b, 5L * d.ne);
   if (bnorm < 0.0) return -1;
   if (refine_fp32) {
-    if (gmres_refine_device(c->A, c->W, c->x, c->b, rel_tol, 1e-3, 30, &st)) return -1;
+    if (gmres_refine_device(c->A, c->W, c->x, c->b, rel_tol, 1e-3, 30, &st, precond)) return -1;
   } else {
-    if (gmres_device(c->A, c->W, c->x, c->b, rel_tol * bnorm, true, false, 40, &st, nullptr)) return -1;
+    if (gmres_device(c->A, c->W, c->x, c->b, rel_tol * bnorm, precond, false, precond == kPrecondDiag ? 40 : 20,
+                     &st, nullptr))
+      return -1;
   }
   SUBFV_CUDA(cudaEventRecord(e[2], d.stream));
   launch_be_update(d, s->U0, c->x);

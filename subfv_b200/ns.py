@@ -161,12 +161,14 @@ class NsState:
         check(_lib.load().subfv_ns_residuals(self._h, C.byref(res), pd(rv), C.byref(dt)), "subfv_ns_residuals")
         return res.value, rv, dt.value
 
-    def implicit_step(self, cfl_implicit=10.0, krylov=30, rel_tol=1e-8, refine_fp32=False):
+    def implicit_step(self, cfl_implicit=10.0, krylov=30, rel_tol=1e-8, refine_fp32=False, precond=1):
         """One backward-Euler step (first-order two-wave residual, exact frozen-speed
-        Jacobian, block-Jacobi GMRES); returns (status bits, stats dict)."""
+        Jacobian, GMRES preconditioned by block Jacobi (precond 1) or the coloured LU-SGS
+        (2)); returns (status bits, stats dict)."""
         st = ImplicitStats()
-        rc = check(_lib.load().subfv_ns_implicit_step(self._h, float(cfl_implicit), int(krylov), float(rel_tol),
-                                                      int(refine_fp32), C.byref(st)), "subfv_ns_implicit_step")
+        rc = check(_lib.load().subfv_ns_implicit_step_ex(self._h, float(cfl_implicit), int(krylov), float(rel_tol),
+                                                         int(refine_fp32), int(precond), C.byref(st)),
+                   "subfv_ns_implicit_step")
         return rc, {k: getattr(st, k) for k, _ in ImplicitStats._fields_}
 
     def be_jacobian(self, dt):
