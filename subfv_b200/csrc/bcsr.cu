@@ -134,62 +134,63 @@ __global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __
   for (int k = 0; k < BS; ++k) x[(size_t)BS * i + k] = xv[k];
 }
 
-// v_i = v_i - matmul(A_ij, u_col) over the row's blocks whose colour passes `pick`
-// (below the set's for the forward sweep, above it for the backward one), in row order
+// The sweeps use BS lanes per block row, as the SpMV does (lane r owns component r, and
+// the row's blocks are walked in order, each product summed over its columns first);
+// the backward sweep then gathers the row's components by shuffles and every lane of
+// the group applies the diagonal LU to the whole block, keeping its own component.
 template <int BS, bool FWD>
-__device__ inline void lusgs_row(const int* __restrict__ row, const int* __restrict__ col,
-                                 const double* __restrict__ v, const int* __restrict__ color, int cs, int i,
-                                 const double* u, double* vi) {
+__device__ inline double lusgs_lane(const int* __restrict__ row, const int* __restrict__ col,
+                                    const double* __restrict__ v, const int* __restrict__ color, int cs, int i, int r,
+                                    const double* u, double acc) {
   for (int j = row[i]; j < row[i + 1]; ++j) {
     const int c = col[j];
     const int cc = color[c];
     if (FWD ? !(cc < cs) : !(cc > cs)) continue;
     const double* blk = v + (size_t)BS * BS * j;
     const double* uc = u + (size_t)BS * c;
-    double t[BS];
+    double t = 0.0;
 #pragma unroll
-    for (int r = 0; r < BS; ++r) {
-      double a = 0.0;
-#pragma unroll
-      for (int k = 0; k < BS; ++k) a = a + blk[r + BS * k] * uc[k];
-      t[r] = a;
-    }
-#pragma unroll
-    for (int r = 0; r < BS; ++r) vi[r] = vi[r] - t[r];
+    for (int k = 0; k < BS; ++k) t = t + blk[r + BS * k] * uc[k];
+    acc = acc - t;
   }
+  return acc;
 }
 
 // forward sweep of colour set cs: y_i = b_i - sum over lower colours of A_ij y_j
 template <int BS>
-__global__ void k_lusgs_fwd(int nrows, const int* __restrict__ rows, const int* __restrict__ row,
-                            const int* __restrict__ col, const double* __restrict__ v,
-                            const int* __restrict__ color, int cs, const double* __restrict__ b, double* y) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_lusgs_fwd(int nrows, const int* __restrict__ rows,
+                                                   const int* __restrict__ row, const int* __restrict__ col,
+                                                   const double* __restrict__ v, const int* __restrict__ color,
+                                                   int cs, const double* __restrict__ b, double* y) {
+  constexpr int GPW = 32 / BS;
+  const int lane = threadIdx.x & 31;
+  if (lane >= GPW * BS) return;
+  const int t = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * GPW + lane / BS;
   if (t >= nrows) return;
-  const int i = rows[t];
-  double yi[BS];
-#pragma unroll
-  for (int r = 0; r < BS; ++r) yi[r] = b[(size_t)BS * i + r];
-  lusgs_row<BS, true>(row, col, v, color, cs, i, y, yi);
-#pragma unroll
-  for (int r = 0; r < BS; ++r) y[(size_t)BS * i + r] = yi[r];
+  const int i = rows[t], r = lane % BS;
+  y[(size_t)BS * i + r] = lusgs_lane<BS, true>(row, col, v, color, cs, i, r, y, b[(size_t)BS * i + r]);
 }
 // backward sweep of colour set cs: x_i = D_i^-1 (y_i - sum over higher colours of A_ij x_j)
 template <int BS>
-__global__ void k_lusgs_bwd(int nrows, const int* __restrict__ rows, const int* __restrict__ row,
-                            const int* __restrict__ col, const double* __restrict__ v,
-                            const int* __restrict__ color, int cs, const double* __restrict__ lu, int m,
-                            const double* __restrict__ y, double* x) {
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= nrows) return;
-  const int i = rows[t];
-  double xi[BS];
+__global__ void __launch_bounds__(128) k_lusgs_bwd(int nrows, const int* __restrict__ rows,
+                                                   const int* __restrict__ row, const int* __restrict__ col,
+                                                   const double* __restrict__ v, const int* __restrict__ color,
+                                                   int cs, const double* __restrict__ lu, int m,
+                                                   const double* __restrict__ y, double* x) {
+  constexpr int GPW = 32 / BS;
+  const int lane = threadIdx.x & 31;
+  const int g = lane / BS, r = lane % BS;
+  const int t = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * GPW + g;
+  const bool live = lane < GPW * BS && t < nrows;  // every lane joins the shuffles
+  const int i = live ? rows[t] : 0;
+  double xr = 0.0;
+  if (live) xr = lusgs_lane<BS, false>(row, col, v, color, cs, i, r, x, y[(size_t)BS * i + r]);
+  double xv[BS];
 #pragma unroll
-  for (int r = 0; r < BS; ++r) xi[r] = y[(size_t)BS * i + r];
-  lusgs_row<BS, false>(row, col, v, color, cs, i, x, xi);
-  lu_apply<BS>(lu, m, i, xi);
-#pragma unroll
-  for (int r = 0; r < BS; ++r) x[(size_t)BS * i + r] = xi[r];
+  for (int k = 0; k < BS; ++k) xv[k] = __shfl_sync(0xffffffffu, xr, (lane < GPW * BS ? g * BS : 0) + k);
+  if (!live) return;
+  lu_apply<BS>(lu, m, i, xv);
+  x[(size_t)BS * i + r] = xv[r];
 }
 
 __device__ inline double warp_tree(double v) {
@@ -495,11 +496,20 @@ double device_norm2(const DevBcsr& A, GmresWork& W, const double* x, long n) {
   return std::sqrt(s);
 }
 
+namespace {
+// blocks of 128 threads (4 warps of 32 / bs row groups) covering n rows
+int lusgs_grid(int bs, int n) {
+  const int gpw = 32 / bs;
+  const long warps = (n + gpw - 1) / gpw;
+  return (int)((warps * 32 + 127) / 128);
+}
+}  // namespace
+
 void launch_bcsr_lusgs(const DevBcsr& A, const double* b, double* x, double* ty) {
   for (int cs = 1; cs <= A.ncs; ++cs) {
     const int o = A.set_off[cs - 1], n = A.set_off[cs] - o;
     if (n == 0) continue;
-    const int g = (n + 127) / 128;
+    const int g = lusgs_grid(A.bs, n);
     switch (A.bs) {
       case 5: k_lusgs_fwd<5><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, b, ty); break;
       case 4: k_lusgs_fwd<4><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, b, ty); break;
@@ -510,7 +520,7 @@ void launch_bcsr_lusgs(const DevBcsr& A, const double* b, double* x, double* ty)
   for (int cs = A.ncs; cs >= 1; --cs) {
     const int o = A.set_off[cs - 1], n = A.set_off[cs] - o;
     if (n == 0) continue;
-    const int g = (n + 127) / 128;
+    const int g = lusgs_grid(A.bs, n);
     switch (A.bs) {
       case 5:
         k_lusgs_bwd<5><<<g, 128, 0, A.stream>>>(n, A.set_rows + o, A.row, A.col, A.v, A.color, cs, A.lu, A.m, ty, x);
