@@ -154,6 +154,18 @@ def _fp64_peak():
     return {"peak_tflops": tf.value, "probe_ms": ms.value, "how": "fma.rn.f64, 8 chains/thread, 8 blocks x 256 per SM"}
 
 
+def _ns_roofline(sz, stages, ms_per_update):
+    """HBM roofline of the explicit Euler update from the compulsory bytes of
+    roofline.algorithmic_bytes("ns_update"); sz = dict(ne, nv, nsf, nse) summed over meshes."""
+    from subfv_b200.roofline import algorithmic_bytes
+    peak, kind = _peaks()
+    b = algorithmic_bytes("ns_update", stages=stages, **sz)
+    gbs = b / (ms_per_update * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "explicit update (all kernels)", "achieved": gbs, "peak": peak, "unit": "GB/s",
+            "frac": gbs / peak, "peak_kind": kind, "traffic": None, "algorithmic_bytes": b,
+            "note": "step-level compulsory bytes; the node kernel is FP64-latency-bound (profiles/)"}
+
+
 def _traffic(kernel):
     """dram read+write bytes per launch from the committed ncu summary, if any."""
     p = ROOT / "profiles" / "lagrange_step_traffic.json"
@@ -254,6 +266,7 @@ def run_gresho(args, rank, world, local):
     n = 64 if args.n == N_SIDE else args.n
     raw = meshgen.hex_slab(n, n, jitter=0.1, seed=SEED)
     mesh = Mesh.from_raw(raw)
+    mesh_sizes = dict(ne=mesh.n_elems, nv=mesh.n_vert, nsf=mesh.n_sub_faces, nse=mesh.n_sub_elems)
     sol0 = init_gresho(mesh, 0.1)
     out = {}
     for prec_name, prec in (("fp64", 0), ("mixed", 1), ("mixed_flux", 2)):
@@ -282,7 +295,6 @@ def run_gresho(args, rank, world, local):
         el = time.perf_counter() - t0
         cpu = {"value": 20 * cells / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
                "sample": f"20 of the 200 iterations on the same mesh, serial C++ restatement, {el:.1f} s"}
-        parity = float(np.abs(so - out["fp64"]["sol"]).max()) if False else None
     res = {"metric": "cell-updates/s", "workload": "gresho2d_ns_multipoint_o2_64x64",
            "value": cells * 200 / (out["fp64"]["ms"] / 1e3), "unit": "cell-updates/s",
            "mixed_value": cells * 200 / (out["mixed"]["ms"] / 1e3),
@@ -290,6 +302,7 @@ def run_gresho(args, rank, world, local):
            "ms_per_iteration": out["fp64"]["ms"] / 200, "cells": cells, "iterations": 200,
            "mixed_l1_rel_vs_fp64": l1, "status": [out[k]["status"] for k in ("fp64", "mixed", "mixed_flux")],
            "sim_time_after_200": out["fp64"]["t"],
+           "roofline": _ns_roofline(mesh_sizes, 2, out["fp64"]["ms"] / 200),
            "dtype": "f64", "cpu_baseline": cpu}
     print(json.dumps(res), flush=True)
 
@@ -343,6 +356,15 @@ def run_implicit(args, rank, world, local):
         res[name] = stats
     res["value"] = res["fp64"]["cell_updates_per_s"]
     res["unit"] = "cell-updates/s"
+    from subfv_b200.roofline import algorithmic_bytes
+    peak, kind = _peaks()
+    nx = res["fp64"]["next_step"]
+    cyc = algorithmic_bytes("gmres_cycle", m=mesh.n_elems, bs=5, nnzb=res["fp64"]["nnz_blocks"], krylov=30)
+    solve_b = nx["restarts"] * cyc
+    gbs = solve_b / (nx["ms_solve"] * 1e-3) / 1e9
+    res["roofline"] = {"bound": "hbm", "kernel": "GMRES(30) solve (SpMV, block Jacobi, MGS)", "achieved": gbs,
+                       "peak": peak, "unit": "GB/s", "frac": gbs / peak, "peak_kind": kind, "traffic": None,
+                       "algorithmic_bytes": solve_b}
     res["timing"] = ("device events around assemble, GMRES and update of the second step on a state "
                      "(the first step also captures the Arnoldi-cycle graph; both reported)")
     print(json.dumps(res), flush=True)
@@ -393,6 +415,8 @@ def run_shocktubes(args, rank, world, local):
     setup_s = time.perf_counter() - t0
     sols = [shocktube.initial_state(m, t) for m, t in zip(meshes, rng_tubes)]
     cells = sum(m.n_elems for m in meshes)
+    tube_sizes = dict(ne=cells, nv=sum(m.n_vert for m in meshes), nsf=sum(m.n_sub_faces for m in meshes),
+                      nse=sum(m.n_sub_elems for m in meshes))
     base = dict(scheme=1, second_order=False, method=4, bc_style=2, boundary_2d=True, cfl=0.4)
     budget = int(150e9)
     res = {"metric": "cell-updates/s", "workload": f"shocktubes_{args.problems}_strips_Nx4",
@@ -417,6 +441,7 @@ def run_shocktubes(args, rank, world, local):
         b.sync()
         st = max(b.info(k)[3] for k in slots)
         res[name] = {"value": cells * K / (ms_tuned / 1e3), "ms_per_step": ms_tuned / K,
+                     "roofline": _ns_roofline(tube_sizes, 1, ms_tuned / K),
                      "fixed_value": cells * K / (ms_fixed / 1e3), "fixed_ms_per_step": ms_fixed / K,
                      "tuned_shape": {"node_lanes": best[0], "block_v": best[1], "grid_v": best[2],
                                      "grid_c": best[3]},

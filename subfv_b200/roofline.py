@@ -43,3 +43,38 @@ def lag_kernel_bytes(s: MeshSizes) -> dict:
 
 def step_bytes(s: MeshSizes) -> int:
     return sum(lag_kernel_bytes(s).values())
+
+
+def algorithmic_bytes(path: str, *, ne: int = 0, nv: int = 0, nsf: int = 0, nse: int = 0, stages: int = 1,
+                      m: int = 0, bs: int = 5, nnzb: int = 0, w: int = 8, krylov: int = 30,
+                      precond: str = "diag", sizes: MeshSizes | None = None) -> int:
+    """Compulsory HBM bytes of one unit of work on a path (each array touched once):
+
+    - "lagrange_step": one Lagrangian step, the sum of lag_kernel_bytes(sizes);
+    - "ns_stage": one explicit Euler stage, state read and write (2 x 40 B), volume (8),
+      subface normal + area (32) and left/right cell ids (8), node CSR offsets (4) and
+      the corner -> cell map (4): 80 C + 8 C + 32 SF + 8 SF + 4 (V + 1) + 4 SE;
+    - "ns_update": `stages` stages plus the re-read of U^n (40 C) in the two-stage scheme;
+    - "spmv": nnzb (bs^2 w + 4) + (m + 1) 4 + 2 m bs 8 (values of w bytes);
+    - "gmres_cycle": one restart cycle of GMRES(krylov): krylov SpMVs and preconditioner
+      applications (block Jacobi: the packed LU, bs^2 8 per row, and two vectors), the
+      modified Gram-Schmidt projections (column j: j projections of 3 vectors, fused
+      axpy + next dot) and the normalisations (2 vectors).
+    """
+    if path == "lagrange_step":
+        return step_bytes(sizes)
+    if path == "ns_stage":
+        return 80 * ne + 8 * ne + 32 * nsf + 8 * nsf + 4 * (nv + 1) + 4 * nse
+    if path == "ns_update":
+        b = stages * algorithmic_bytes("ns_stage", ne=ne, nv=nv, nsf=nsf, nse=nse)
+        return b + (40 * ne if stages == 2 else 0)
+    if path == "spmv":
+        return nnzb * (bs * bs * w + 4) + (m + 1) * 4 + 2 * m * bs * 8
+    if path == "gmres_cycle":
+        n = m * bs
+        vec = 8 * n
+        pc = (bs * bs * 8 * m + 2 * vec) if precond == "diag" else 0
+        spmv = algorithmic_bytes("spmv", m=m, bs=bs, nnzb=nnzb, w=w)
+        mgs = sum(3 * j * vec + 2 * vec for j in range(1, krylov + 1))
+        return krylov * (spmv + pc) + mgs
+    raise ValueError(f"unknown path {path}")
