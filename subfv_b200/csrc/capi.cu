@@ -541,15 +541,21 @@ int subfv_lag_last_dt(subfv_lag_state* s, double* dt) {
 int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout) {
   DevMesh& d = s->m->d;
   size_t bytes = 5 * (size_t)d.ne * sizeof(double);
-  std::memcpy(s->host_stage, sol_inout, bytes);
-  SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, s->host_stage, bytes, cudaMemcpyHostToDevice, d.stream));
+  // a page-locked caller buffer is copied to and from directly; a pageable one goes
+  // through the state's pinned staging buffer
+  cudaPointerAttributes attr{};
+  const bool pinned = cudaPointerGetAttributes(&attr, sol_inout) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  cudaGetLastError();  // a pageable pointer is not an error here
+  double* hbuf = pinned ? sol_inout : s->host_stage;
+  if (!pinned) std::memcpy(s->host_stage, sol_inout, bytes);
+  SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, hbuf, bytes, cudaMemcpyHostToDevice, d.stream));
   launch_pack6(d, d.ne, s->dev_stage, nullptr, s->sol6);
   enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision, s->scheme, s->method);
   d.geom_partial = 1;
   launch_unpack6(d, d.ne, kRec, s->sol6, s->dev_stage);
-  SUBFV_CUDA(cudaMemcpyAsync(s->host_stage, s->dev_stage, bytes, cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(hbuf, s->dev_stage, bytes, cudaMemcpyDeviceToHost, d.stream));
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
-  std::memcpy(sol_inout, s->host_stage, bytes);
+  if (!pinned) std::memcpy(sol_inout, s->host_stage, bytes);
   return check_status(d);
 }
 

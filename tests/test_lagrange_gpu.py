@@ -201,3 +201,33 @@ def test_sidil_run_bit_exact(native, oracle_lib, cuda_ok, case):
     np.testing.assert_array_equal(s.sol(), sol_o)
     np.testing.assert_array_equal(m.coords(), o.geom("vert_coord"))
     np.testing.assert_array_equal(s.vp(), vp_o)
+
+
+def test_step_host_pinned_and_pageable_agree(native, cuda_ok):
+    """subfv_lag_step_host copies a page-locked caller buffer directly and a pageable one
+    through its staging buffer: both give the device loop's state, bit for bit."""
+    import torch
+    from subfv_b200.lagrange import LagrangeState
+    from subfv_b200.mesh import Mesh
+    raw = lagrange_cases()["prism_jit"]
+    outs = []
+    for kind in ("pageable", "pinned", "device"):
+        m = Mesh.from_raw(raw)
+        sol = _random_state(m.n_elems, 7)
+        mass = m.geometry("elem_volume") / sol[:, 0]
+        s = LagrangeState(m, sol, mass, cfl=0.5, t_max=1.0)
+        if kind == "device":
+            s.advance(4)
+            outs.append(s.sol())
+            continue
+        if kind == "pinned":
+            t = torch.empty(sol.shape, dtype=torch.float64, pin_memory=True)
+            buf = t.numpy()
+            buf[:] = sol
+        else:
+            buf = sol.copy()
+        for _ in range(4):
+            assert s.step_host(buf) == 0
+        outs.append(buf.copy())
+    np.testing.assert_array_equal(outs[0], outs[2])
+    np.testing.assert_array_equal(outs[1], outs[2])
