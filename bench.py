@@ -573,7 +573,7 @@ def main():
         return
 
     torch.cuda.set_device(local)
-    from subfv_b200 import meshgen
+    from subfv_b200 import meshgen, replicas
     from subfv_b200.lagrange import MIXED, PLAIN_FP64, LagrangeState, init_sol_sedov
     from subfv_b200.mesh import Mesh
     from subfv_b200.roofline import lag_kernel_bytes
@@ -607,10 +607,7 @@ def main():
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
     st, steps_done, t_now = state.sync()
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = replicas.max_over_ranks(ms)  # the slowest replica's device time
     cells = mesh.n_elems
     value = world * cells * args.steps / (ms / 1e3)
 
@@ -643,11 +640,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(k_e2e):
         st_e2e.step_host(host)
-    e2e_s = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0)
     e2e = {"value": world * cells * k_e2e / e2e_s, "unit": "cell-updates/s",
            "h2d_bytes_per_step": 5 * 8 * cells, "d2h_bytes_per_step": 5 * 8 * cells,
            "steps": k_e2e, "api": "subfv_lag_step_host", "host_buffer": "page-locked"}
