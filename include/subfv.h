@@ -24,7 +24,7 @@ extern "C" {
 #define SUBFV_ERR_NONFINITE 2    /* non-finite state, volume or time step */
 #define SUBFV_ERR_NEG_DENSITY 4  /* negative density / specific volume: ns_euler_rs_module.F90:257-266 */
 #define SUBFV_ERR_BAD_OMEGA 8    /* positivity limiter omega <= 1e-6: ns_euler_module.F90:595-598 */
-#define SUBFV_ERR_GMRES 16       /* GMRES did not converge: sparse_bcsr_linear_module.F90:1614,1686 */
+#define SUBFV_ERR_GMRES 16       /* a Krylov solve did not converge: sparse_bcsr_linear_module.F90:1614,1686,1164 */
 #define SUBFV_ERR_INDEX 32       /* an index outside its array */
 
 const char* subfv_last_error(void);
@@ -339,6 +339,12 @@ int subfv_bcsr_parallel_lusgs(subfv_bcsr* A, double* x, const double* b);
  * absolute tol; conv from the final true residual as the reference sets it */
 int subfv_bcsr_gmres_parallel_lusgs(subfv_bcsr* A, double* x, const double* b, double tol, int m, int* conv,
                                     int* restarts, double* rho);
+/* bcsr_pcgm(A, x, b, tol) — :1110-1169: conjugate gradients from the initial guess in
+ * x, preconditioned by lu_solve (partial pivoting) on each diagonal block (the
+ * reference hard-codes 3x3 blocks; any supported block size works here). Returns
+ * SUBFV_ERR_GMRES where the reference stops on non-convergence, SUBFV_ERR_NONFINITE on
+ * a singular diagonal block. */
+int subfv_bcsr_pcgm(subfv_bcsr* A, double* x, const double* b, double tol, int* iters, double* res);
 /* bcsr_gmres — :194-290: unpreconditioned, 20 restarts */
 int subfv_bcsr_gmres(subfv_bcsr* A, double* x, const double* b, double tol, int m, int* conv,
                      int* restarts, double* rho);

@@ -61,6 +61,7 @@ def load():
         lib.or_lu3.argtypes = [PD, PD, PD]
         lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]
+        lib.or_bcsr_pcgm.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD, C.c_double, PI, PD]
         lib.or_bcsr_parallel_lusgs.argtypes = [C.c_int, C.c_int, PI, PI, PD, C.c_int, PI, PD, PD]
         lib.or_bcsr_gmres_lusgs.argtypes = [C.c_int, C.c_int, PI, PI, PD, C.c_int, PI, PD, PD, C.c_double, C.c_int,
                                             PI, PD]
@@ -274,6 +275,16 @@ class OracleBcsr:
         x = np.zeros(self.n)
         load().or_bcsr_diag(self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), _pd(x), _pd(b))
         return x
+
+    def pcgm(self, b, tol, x0=None):
+        """bcsr_pcgm from x0 (zeros if None): (x, iterations, status, res)."""
+        b = np.ascontiguousarray(b, np.float64)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, np.float64)
+        st = np.zeros(1, np.int32)
+        res = np.zeros(1)
+        it = load().or_bcsr_pcgm(self.m, self.bs, _pi(self.row), _pi(self.col), _pd(self.v), _pd(x), _pd(b),
+                                 float(tol), _pi(st), _pd(res))
+        return x, it, int(st[0]), float(res[0])
 
     def parallel_lusgs(self, b, ncs, color):
         b = np.ascontiguousarray(b, np.float64)

@@ -3,7 +3,8 @@
 // (:1414-1436) with lu_solve_noswp (linear_solver_module.F90:413-445),
 // modifiedArnoldi_diag + bcsr_gmres_diag (:1568-1691), the unpreconditioned
 // bcsr_gmres (:194-290), and bcsr_parallel_lusgs with bcsr_gmres_parallel_lusgs and
-// modifiedArnoldi_parallel_lusgs (:1438-1502, :885-993, :583-611). norm2 is gfortran's scaled sum of squares and dot_product a
+// modifiedArnoldi_parallel_lusgs (:1438-1502, :885-993, :583-611), and bcsr_pcgm
+// (:1110-1169) with lu_solve (linear_solver_module.F90:447-484). norm2 is gfortran's scaled sum of squares and dot_product a
 // left-to-right sum, as the serial reference evaluates them.
 // PARITY UNPINNED (no Fortran compiler here).
 #include "oracle.h"
@@ -118,6 +119,84 @@ static double dotp(const double* a, const double* b, long n) {
   double s = 0.0;
   for (long i = 0; i < n; ++i) s = s + a[i] * b[i];
   return s;
+}
+
+// linear_solver_module.F90:447-484 (lu_solve): partial pivoting on the first largest
+// |C(k:n, k)|, whole rows swapped; returns false where the reference stops on
+// |C(n,n)| < 1e-12
+static bool lu_solve_pivot(int n, const double* A, double* x, const double* b) {
+  std::vector<double> C(A, A + n * n);
+  auto c = [&](int i, int j) -> double& { return C[i + n * j]; };
+  for (int i = 0; i < n; ++i) x[i] = b[i];
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    for (int i = k + 1; i < n; ++i)
+      if (std::fabs(c(i, k)) > std::fabs(c(p, k))) p = i;
+    for (int j = 0; j < n; ++j) std::swap(c(k, j), c(p, j));
+    std::swap(x[k], x[p]);
+    const double invdiag = 1.0 / c(k, k);
+    for (int i = k + 1; i < n; ++i) {
+      const double lik = c(i, k) * invdiag;
+      for (int j = k; j < n; ++j) c(i, j) = c(i, j) - lik * c(k, j);
+      x[i] = x[i] - lik * x[k];
+    }
+  }
+  if (std::fabs(c(n - 1, n - 1)) < 1e-12) return false;
+  x[n - 1] = x[n - 1] / c(n - 1, n - 1);
+  for (int k = n - 2; k >= 0; --k) {
+    for (int j = k + 1; j < n; ++j) x[k] = x[k] - c(k, j) * x[j];
+    x[k] = x[k] / c(k, k);
+  }
+  return true;
+}
+
+// bcsr_pcgm (:1110-1169): conjugate gradients from the caller's x, preconditioned by
+// lu_solve on each diagonal block (the reference passes n = 3: blocks of size 3).
+// Returns the iterations; *status 0, 1 not converged (the reference stops), 2 a
+// singular diagonal block.
+static int bcsr_pcgm(const Bcsr& A, double* x, const double* b, double tol, int* status, double* res) {
+  const long n = (long)A.bs * A.m;
+  const int bs = A.bs;
+  std::vector<double> r(n), p(n), Ap(n), mr(n), w(n);
+  std::vector<int> d(A.m);
+  for (int i = 1; i <= A.m; ++i)
+    for (int j = A.row[i - 1]; j <= A.row[i] - 1; ++j)
+      if (A.col[j - 1] == i) {
+        d[i - 1] = j;
+        break;
+      }
+  *status = 0;
+  auto precond = [&]() {
+    for (int i = 0; i < A.m; ++i)
+      if (!lu_solve_pivot(bs, A.v + (size_t)bs * bs * (d[i] - 1), mr.data() + (size_t)bs * i,
+                          r.data() + (size_t)bs * i))
+        *status = 2;
+  };
+  double rpdrp = 0.0;
+  bcsr_matmul(A, x, w.data());
+  for (long k = 0; k < n; ++k) r[k] = b[k] - w[k];
+  precond();
+  double rdr = dotp(mr.data(), r.data(), n);
+  *res = std::sqrt(rdr);
+  if (std::sqrt(rdr) < tol) return 0;
+  p = mr;
+  long it = 0;
+  for (long k = 1; k <= n; ++k) {
+    it = k;
+    bcsr_matmul(A, p.data(), Ap.data());
+    const double alpha = rdr / dotp(p.data(), Ap.data(), n);
+    for (long q = 0; q < n; ++q) x[q] = x[q] + alpha * p[q];
+    for (long q = 0; q < n; ++q) r[q] = r[q] - alpha * Ap[q];
+    precond();
+    rpdrp = dotp(mr.data(), r.data(), n);
+    if (std::sqrt(rpdrp) <= tol)
+      if (fnorm2(r.data(), (int)n) <= tol) break;
+    for (long q = 0; q < n; ++q) p[q] = mr[q] + (rpdrp / rdr) * p[q];
+    rdr = rpdrp;
+  }
+  *res = std::sqrt(rpdrp);
+  if (std::sqrt(rpdrp) > tol && *status == 0) *status = 1;
+  return (int)it;
 }
 
 // GMRES(m) with restarts; precond 1 = bcsr_gmres_diag (maxit 40), 2 =
@@ -250,6 +329,11 @@ int or_bcsr_gmres(int m, int bs, const int* row, const int* col, const double* v
   int it = gmres(A, x, b, tol, krylov, precond != 0 ? 1 : 0, &cv, rho, H_first);
   *conv = cv ? 1 : 0;
   return it;
+}
+int or_bcsr_pcgm(int m, int bs, const int* row, const int* col, const double* v, double* x, const double* b,
+                 double tol, int* status, double* res) {
+  Bcsr A{m, m, bs, row, col, v};
+  return bcsr_pcgm(A, x, b, tol, status, res);
 }
 void or_bcsr_parallel_lusgs(int m, int bs, const int* row, const int* col, const double* v, int ncs,
                             const int* color, double* x, const double* b) {

@@ -102,6 +102,7 @@ SIGNATURES = {
     "subfv_bcsr_create": (c_int, [c_int, c_int, PI32, PI32, PD, C.POINTER(P)]),
     "subfv_bcsr_destroy": (c_int, [P]),
     "subfv_bcsr_set_colors": (c_int, [P, c_int, PI32]),
+    "subfv_bcsr_pcgm": (c_int, [P, PD, PD, c_dbl, C.POINTER(c_int), PD]),
     "subfv_bcsr_parallel_lusgs": (c_int, [P, PD, PD]),
     "subfv_bcsr_gmres_parallel_lusgs": (c_int, [P, PD, PD, c_dbl, c_int, C.POINTER(c_int), C.POINTER(c_int), PD]),
     "subfv_bcsr_set_values": (c_int, [P, PD]),

@@ -84,6 +84,17 @@ class DeviceBcsr:
                                               C.byref(it), C.byref(rho), None), "subfv_bcsr_gmres_parallel_lusgs")
         return x, bool(conv.value), it.value, rho.value
 
+    def pcgm(self, b, tol, x0=None):
+        """bcsr_pcgm (:1110-1169) from x0 (zeros if None); returns (x, iterations, status
+        bits, sqrt(r.M^-1 r)). Status SUBFV_ERR_GMRES: not converged (the reference stops)."""
+        b = f64(b)
+        x = np.zeros(self.n) if x0 is None else np.array(x0, np.float64)
+        it, res = C.c_int(), C.c_double()
+        st = _lib.load().subfv_bcsr_pcgm(self._h, pd(x), pd(b), float(tol), C.byref(it), C.byref(res))
+        if st < 0:
+            check(st, "subfv_bcsr_pcgm")
+        return x, it.value, st, res.value
+
     def gmres(self, b, tol, m=30, precond=True, want_h=False):
         """bcsr_gmres_diag (precond) / bcsr_gmres; returns (x, conv, restarts, rho[, H_first])."""
         b = f64(b)

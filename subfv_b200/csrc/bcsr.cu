@@ -134,6 +134,63 @@ __global__ void k_bjacobi(int m, const double* __restrict__ lu, const double* __
   for (int k = 0; k < BS; ++k) x[(size_t)BS * i + k] = xv[k];
 }
 
+// lu_solve (linear_solver_module.F90:447-484) on block row i's diagonal block: partial
+// pivoting on the first largest |C(k:n, k)|, whole rows swapped; a pivot below 1e-12 at
+// the last step (where the reference stops) sets bit 2 of *flag and skips the back
+// substitution
+template <int BS>
+__global__ void k_pivot_diag(int m, const int* __restrict__ diag, const double* __restrict__ v,
+                             const double* __restrict__ r, double* __restrict__ mr, unsigned* flag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int dj = diag[i];
+  double C[BS * BS], x[BS];
+  for (int q = 0; q < BS * BS; ++q) C[q] = dj >= 0 ? v[(size_t)BS * BS * dj + q] : (q % (BS + 1) == 0 ? 1.0 : 0.0);
+  for (int k = 0; k < BS; ++k) x[k] = r[(size_t)BS * i + k];
+  for (int k = 0; k < BS; ++k) {
+    int p = k;
+    for (int ii = k + 1; ii < BS; ++ii)
+      if (fabs(C[ii + BS * k]) > fabs(C[p + BS * k])) p = ii;
+    for (int j = 0; j < BS; ++j) {
+      const double t = C[k + BS * j];
+      C[k + BS * j] = C[p + BS * j];
+      C[p + BS * j] = t;
+    }
+    const double tx = x[k];
+    x[k] = x[p];
+    x[p] = tx;
+    const double invdiag = 1.0 / C[k + BS * k];
+    for (int ii = k + 1; ii < BS; ++ii) {
+      const double lik = C[ii + BS * k] * invdiag;
+      for (int j = k; j < BS; ++j) C[ii + BS * j] = C[ii + BS * j] - lik * C[k + BS * j];
+      x[ii] = x[ii] - lik * x[k];
+    }
+  }
+  if (fabs(C[BS * BS - 1]) < 1e-12) {
+    atomicOr(flag, 2u);
+  } else {
+    x[BS - 1] = x[BS - 1] / C[BS * BS - 1];
+    for (int k = BS - 2; k >= 0; --k) {
+      for (int j = k + 1; j < BS; ++j) x[k] = x[k] - C[k + BS * j] * x[j];
+      x[k] = x[k] / C[k + BS * k];
+    }
+  }
+  for (int k = 0; k < BS; ++k) mr[(size_t)BS * i + k] = x[k];
+}
+
+// x += a p; r -= a q; p = z + b p (conjugate gradients, bcsr_pcgm's vector updates)
+__global__ void k_cg_update(double* __restrict__ x, double* __restrict__ r, const double* __restrict__ p,
+                            const double* __restrict__ q, double a, long n) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  x[k] = x[k] + a * p[k];
+  r[k] = r[k] - a * q[k];
+}
+__global__ void k_cg_dir(double* __restrict__ p, const double* __restrict__ z, double beta, long n) {
+  const long k = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) p[k] = z[k] + beta * p[k];
+}
+
 // The sweeps use BS lanes per block row, as the SpMV does (lane r owns component r, and
 // the row's blocks are walked in order, each product summed over its columns first);
 // the backward sweep then gathers the row's components by shuffles and every lane of
@@ -747,6 +804,67 @@ int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double*
   st->outer = outer - (st->conv ? 1 : 0);
   st->rho = rn;
   SUBFV_CUDA(cudaGetLastError());
+  return 0;
+}
+
+namespace {
+double device_dot(const DevBcsr& A, GmresWork& W, const double* a, const double* b, long n) {
+  k_dot<<<kRedBlocks, kRedThreads, 0, A.stream>>>(a, b, n, W.partial);
+  k_finish<<<1, kRedThreads, 0, A.stream>>>(W.partial, kRedBlocks, W.scal + 1);
+  double s = 0.0;
+  if (cudaMemcpyAsync(&s, W.scal + 1, sizeof(double), cudaMemcpyDeviceToHost, A.stream) != cudaSuccess ||
+      cudaStreamSynchronize(A.stream) != cudaSuccess)
+    return std::nan("");
+  return s;
+}
+void launch_pivot_diag(const DevBcsr& A, const double* r, double* mr, unsigned* flag) {
+  const int g = (A.m + 127) / 128;
+  switch (A.bs) {
+    case 5: k_pivot_diag<5><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, r, mr, flag); break;
+    case 4: k_pivot_diag<4><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, r, mr, flag); break;
+    case 3: k_pivot_diag<3><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, r, mr, flag); break;
+    default: k_pivot_diag<1><<<g, 128, 0, A.stream>>>(A.m, A.diag, A.v, r, mr, flag);
+  }
+}
+}  // namespace
+
+// bcsr_pcgm (:1110-1169): CG from the caller's x (device), preconditioned by lu_solve on
+// each diagonal block. Dot products by the fixed tree (not left to right). status 0, 1
+// not converged (the reference stops), 2 a singular diagonal block.
+int pcg_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, PcgStats* st) {
+  const long n = (long)A.m * A.bs;
+  cudaStream_t s = A.stream;
+  double *r = W.r, *p = W.zp, *Ap = W.w, *mr = W.ty;
+  unsigned* flag = reinterpret_cast<unsigned*>(W.scal + 4);
+  SUBFV_CUDA(cudaMemsetAsync(flag, 0, sizeof(unsigned), s));
+  st->status = 0;
+  st->iters = 0;
+  double rpdrp = 0.0;
+  launch_bcsr_spmv(A, x, Ap, false);
+  k_sub<<<egrid(n), 256, 0, s>>>(b, Ap, r, n);
+  launch_pivot_diag(A, r, mr, flag);
+  double rdr = device_dot(A, W, mr, r, n);
+  st->res = std::sqrt(rdr);
+  const bool done0 = std::sqrt(rdr) < tol;
+  if (!done0) SUBFV_CUDA(cudaMemcpyAsync(p, mr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  for (long k = 1; k <= n && !done0; ++k) {
+    st->iters = (int)k;
+    launch_bcsr_spmv(A, p, Ap, false);
+    const double alpha = rdr / device_dot(A, W, p, Ap, n);
+    k_cg_update<<<egrid(n), 256, 0, s>>>(x, r, p, Ap, alpha, n);
+    launch_pivot_diag(A, r, mr, flag);
+    rpdrp = device_dot(A, W, mr, r, n);
+    if (!(rpdrp == rpdrp)) return -1;  // a CUDA error inside device_dot
+    if (std::sqrt(rpdrp) <= tol && device_norm2(A, W, r, n) <= tol) break;
+    k_cg_dir<<<egrid(n), 256, 0, s>>>(p, mr, rpdrp / rdr, n);
+    rdr = rpdrp;
+  }
+  if (!done0) st->res = std::sqrt(rpdrp);
+  unsigned f = 0;
+  SUBFV_CUDA(cudaMemcpyAsync(&f, flag, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+  SUBFV_CUDA(cudaStreamSynchronize(s));
+  SUBFV_CUDA(cudaGetLastError());
+  st->status = (f & 2u) ? 2 : (!done0 && std::sqrt(rpdrp) > tol ? 1 : 0);
   return 0;
 }
 

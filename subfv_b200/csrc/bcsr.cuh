@@ -79,4 +79,12 @@ int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double*
                         double inner_rel_tol, int max_outer, GmresStats* st, int precond = kPrecondDiag);
 double device_norm2(const DevBcsr& A, GmresWork& W, const double* x, long n);
 
+struct PcgStats {
+  int iters = 0;
+  int status = 0;  // 0 converged, 1 not converged, 2 singular diagonal block
+  double res = 0.0;
+};
+// bcsr_pcgm (:1110-1169) from the initial guess in x (device vectors)
+int pcg_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, double tol, PcgStats* st);
+
 }  // namespace subfv

@@ -135,6 +135,25 @@ int subfv_bcsr_gmres_parallel_lusgs(subfv_bcsr* h, double* x, const double* b, d
   return subfv_bcsr_gmres_ex(h, x, b, tol, m, kPrecondLusgs, conv, restarts, rho, nullptr);
 }
 
+int subfv_bcsr_pcgm(subfv_bcsr* h, double* x, const double* b, double tol, int* iters, double* res) {
+  if (!h || !x || !b) {
+    set_error("subfv_bcsr_pcgm: null argument");
+    return -2;
+  }
+  if (ensure_vecs(h) || ensure_work(h, h->W.krylov > 0 ? h->W.krylov : 1)) return -1;
+  const size_t n = (size_t)h->A.m * h->A.bs;
+  SUBFV_CUDA(cudaMemcpyAsync(h->b, b, n * sizeof(double), cudaMemcpyHostToDevice, h->A.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(h->x, x, n * sizeof(double), cudaMemcpyHostToDevice, h->A.stream));
+  PcgStats st;
+  if (pcg_device(h->A, h->W, h->x, h->b, tol, &st)) return -1;
+  SUBFV_CUDA(cudaMemcpyAsync(x, h->x, n * sizeof(double), cudaMemcpyDeviceToHost, h->A.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(h->A.stream));
+  if (iters) *iters = st.iters;
+  if (res) *res = st.res;
+  if (st.status == 2) return SUBFV_ERR_NONFINITE;
+  return st.status ? SUBFV_ERR_GMRES : 0;
+}
+
 int subfv_bcsr_gmres_diag(subfv_bcsr* h, double* x, const double* b, double tol, int m, int* conv, int* restarts,
                           double* rho) {
   return subfv_bcsr_gmres_ex(h, x, b, tol, m, 1, conv, restarts, rho, nullptr);

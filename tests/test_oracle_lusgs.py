@@ -42,3 +42,17 @@ def test_lusgs_inverts_the_colour_splitting(oracle_lib):
     b = np.random.default_rng(2).normal(size=o.n)
     x = o.parallel_lusgs(b, ncs, color)
     np.testing.assert_allclose(P @ x, b, rtol=1e-10, atol=1e-10 * np.abs(b).max())
+
+
+def test_oracle_pcgm_solves_spd(oracle_lib):
+    """The oracle's bcsr_pcgm restatement reaches the exact solution of an SPD system."""
+    import sys
+    sys.path.insert(0, __file__.rsplit("/", 1)[0])
+    from test_bcsr_gpu import _spd
+    from oracle.oracle import OracleBcsr
+    A = _spd(4, 3, 3, 3, 11)
+    o = OracleBcsr(A)
+    b = np.random.default_rng(3).normal(size=o.n)
+    x, it, st, res = o.pcgm(b, 1e-11 * np.linalg.norm(b))
+    assert st == 0 and 0 < it < o.n
+    np.testing.assert_allclose(_dense(A) @ x, b, rtol=0, atol=1e-9 * np.abs(b).max())
