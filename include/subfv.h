@@ -171,7 +171,8 @@ typedef struct subfv_ns_cfg {
                                  5 modified_three_wave, 6 multi_point_pressure,
                                  8 multi_point_pressure_ph (ns_global_data_module.F90:67-73) */
   int32_t second_order;       /* 0 / 1 */
-  int32_t method;             /* cell gradient: 0 or 1 (none), 4 (ns_euler_recon_module.F90:200-240) */
+  int32_t method;             /* cell gradient: 0 or 1 (none), 2-6 (compute_cell_grad_method_2..6,
+                                 ns_euler_recon_module.F90:166-320) */
   int32_t bc_style;           /* 0, 1, 2 */
   int32_t boundary_2d;        /* one-cell slab: z-faces are walls */
   int32_t exclude_bound_vert; /* boundary vertices use two_wave */

@@ -25,7 +25,7 @@ static const double G = 1.4;  // ns_global_data_module.F90:9
 struct NsCfg {
   int scheme;  // 1 multi_point, 2 _iso, 3 three_wave, 4 two_wave, 5 modified_three_wave, 6/8 multi_point_pressure(_ph)
   int second_order;    // 0/1
-  int method;          // 0/1 (no gradient) or 4
+  int method;          // 0/1 (no gradient), 2-6 (compute_cell_grad_method_2..6)
   int bc_style;        // 0, 1, 2
   int b2d;
   int exclude_bound_vert;
@@ -458,7 +458,8 @@ static double OI(double a, double b, double c) {
   return fnorm2(x, 3);
 }
 
-// :8-59 (method 4) with physical_slope_limiter (:129-164) and relaxed_maximum_principle (:61-127)
+// :8-59 (methods 2-6, :166-320) with physical_slope_limiter (:129-164) and
+// relaxed_maximum_principle (:61-127)
 static void compute_cell_grads(const Mesh& m, const NsCfg& cfg, const double* sol, double* grad, double* ngrad) {
   for (int v = 1; v <= m.n_vert; ++v) compute_nodal_grad(m, v, sol, ngrad + 15 * (v - 1));
   if (cfg.method == 0 || cfg.method == 1) {
@@ -471,17 +472,52 @@ static void compute_cell_grads(const Mesh& m, const NsCfg& cfg, const double* so
     double* g = grad + 15 * (c - 1);
     double ws[5] = {0, 0, 0, 0, 0};
     for (int i = 0; i < 15; ++i) g[i] = 0.0;
-    for (int j = 1; j <= e.n_vert; ++j) {
-      int v = e.vert[j];
-      const double* ng = ngrad + 15 * (v - 1);
-      for (int k = 0; k < 5; ++k) {
-        double w = m.vert[v].volume / (eps + OI(ng[k], ng[5 + k], ng[10 + k]));
-        for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] + w * ng[5 * d + k];
-        ws[k] = ws[k] + w;
+    if (cfg.method == 2) {  // :166-187 dual-volume average
+      double dvs = 0.0;
+      for (int j = 1; j <= e.n_vert; ++j) {
+        int v = e.vert[j];
+        const double* ng = ngrad + 15 * (v - 1);
+        for (int i = 0; i < 15; ++i) g[i] = g[i] + m.vert[v].volume * ng[i];
+        dvs = dvs + m.vert[v].volume;
       }
+      for (int i = 0; i < 15; ++i) g[i] = g[i] / dvs;
+    } else if (cfg.method == 3) {  // :189-209 the vertex gradient of smallest norm, per variable
+      const double* ng1 = ngrad + 15 * (e.vert[1] - 1);
+      for (int i = 0; i < 15; ++i) g[i] = ng1[i];
+      for (int j = 2; j <= e.n_vert; ++j) {
+        const double* ng = ngrad + 15 * (e.vert[j] - 1);
+        for (int k = 0; k < 5; ++k)
+          if (OI(ng[k], ng[5 + k], ng[10 + k]) < OI(g[k], g[5 + k], g[10 + k]))
+            for (int d = 0; d < 3; ++d) g[5 * d + k] = ng[5 * d + k];
+      }
+    } else {  // 4 (:211-241): weights V/(eps+|g|); 5, 6 (:243-320): V/(eps+|g|)^2
+      double cg[15] = {0}, cws = 0.0;
+      for (int j = 1; j <= e.n_vert; ++j) {
+        int v = e.vert[j];
+        const double* ng = ngrad + 15 * (v - 1);
+        for (int k = 0; k < 5; ++k) {
+          const double q = eps + OI(ng[k], ng[5 + k], ng[10 + k]);
+          double w = cfg.method == 4 ? m.vert[v].volume / q : m.vert[v].volume / (q * q);
+          for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] + w * ng[5 * d + k];
+          ws[k] = ws[k] + w;
+        }
+        if (cfg.method == 6) {
+          for (int i = 0; i < 15; ++i) cg[i] = cg[i] + m.vert[v].volume * ng[i];
+          cws = cws + m.vert[v].volume;
+        }
+      }
+      if (cfg.method == 6) {
+        // the central gradient's weight: OI of the whole (3, 5) array is, by sequence
+        // association with OI's dimension(3) argument, the norm of its first column
+        for (int i = 0; i < 15; ++i) cg[i] = cg[i] / cws;
+        const double q = eps + OI(cg[0], cg[5], cg[10]);
+        const double wc = cws / (q * q);
+        for (int i = 0; i < 15; ++i) g[i] = g[i] + wc * cg[i];
+        for (int k = 0; k < 5; ++k) ws[k] = ws[k] + wc;
+      }
+      for (int k = 0; k < 5; ++k)
+        for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
     }
-    for (int k = 0; k < 5; ++k)
-      for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
     // physical_slope_limiter
     double w0[5];
     c2p(sol + 5 * (c - 1), w0);

@@ -1194,7 +1194,27 @@ __global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* 
   ns_nodal_grad_body(m, U, ngrad, sc, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// compute_cell_grad_method_4 + physical_slope_limiter + relaxed_maximum_principle
+// OI (ns_euler_recon_module.F90:322-329): gfortran's scaled NORM2 of a 3-vector, in T
+template <class T>
+__device__ inline T oi3(T a0, T a1, T a2) {
+  const T a[3] = {a0, a1, a2};
+  T scale = 1, res = 0;
+  for (int i = 0; i < 3; ++i)
+    if (a[i] != (T)0) {
+      T ax = fabs(a[i]);
+      if (ax > scale) {
+        T q = scale / ax;
+        res = (T)1 + res * q * q;
+        scale = ax;
+      } else {
+        T q = ax / scale;
+        res += q * q;
+      }
+    }
+  return scale * sqrt(res);
+}
+
+// compute_cell_grad_method_2..6 (:166-320) + physical_slope_limiter + relaxed_maximum_principle
 template <class T>
 __device__ void ns_cell_grad_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
                                   const double* __restrict__ ngrad, double* __restrict__ grad, const NsScalars* sc,
@@ -1211,36 +1231,53 @@ __device__ void ns_cell_grad_body(const DevMesh& m, const NsParams& P, const dou
   T ws[5] = {0, 0, 0, 0, 0};
   for (int i = 0; i < 15; ++i) g[i] = 0;
   const int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
-  for (int j = 0; j < nvc; ++j) {
-    const int v = m.ev[vb + j];
-    const double* ng = ngrad + 15 * (size_t)v;
-    const T vol = (T)m.vol_v[v];
-    for (int k = 0; k < 5; ++k) {
-      T oi;
-      {
-        T a[3] = {(T)ng[k], (T)ng[5 + k], (T)ng[10 + k]};
-        T scale = 1, res = 0;
-        for (int i = 0; i < 3; ++i)
-          if (a[i] != (T)0) {
-            T ax = fabs(a[i]);
-            if (ax > scale) {
-              T q = scale / ax;
-              res = (T)1 + res * q * q;
-              scale = ax;
-            } else {
-              T q = ax / scale;
-              res += q * q;
-            }
-          }
-        oi = scale * sqrt(res);
-      }
-      T w = vol / (eps + oi);
-      for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] + w * (T)ng[5 * d + k];
-      ws[k] = ws[k] + w;
+  if (P.method == 2) {  // dual-volume average
+    T dvs = 0;
+    for (int j = 0; j < nvc; ++j) {
+      const int v = m.ev[vb + j];
+      const double* ng = ngrad + 15 * (size_t)v;
+      const T vol = (T)m.vol_v[v];
+      for (int i = 0; i < 15; ++i) g[i] = g[i] + vol * (T)ng[i];
+      dvs = dvs + vol;
     }
+    for (int i = 0; i < 15; ++i) g[i] = g[i] / dvs;
+  } else if (P.method == 3) {  // the vertex gradient of smallest norm, per variable
+    const double* ng1 = ngrad + 15 * (size_t)m.ev[vb];
+    for (int i = 0; i < 15; ++i) g[i] = (T)ng1[i];
+    for (int j = 1; j < nvc; ++j) {
+      const double* ng = ngrad + 15 * (size_t)m.ev[vb + j];
+      for (int k = 0; k < 5; ++k)
+        if (oi3<T>((T)ng[k], (T)ng[5 + k], (T)ng[10 + k]) < oi3<T>(g[k], g[5 + k], g[10 + k]))
+          for (int d = 0; d < 3; ++d) g[5 * d + k] = (T)ng[5 * d + k];
+    }
+  } else {  // 4: V / (eps + |g|); 5, 6: V / (eps + |g|)^2 (6 adds the central average)
+    T cg[15], cws = 0;
+    for (int i = 0; i < 15; ++i) cg[i] = 0;
+    for (int j = 0; j < nvc; ++j) {
+      const int v = m.ev[vb + j];
+      const double* ng = ngrad + 15 * (size_t)v;
+      const T vol = (T)m.vol_v[v];
+      for (int k = 0; k < 5; ++k) {
+        const T q = eps + oi3<T>((T)ng[k], (T)ng[5 + k], (T)ng[10 + k]);
+        const T w = P.method == 4 ? vol / q : vol / (q * q);
+        for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] + w * (T)ng[5 * d + k];
+        ws[k] = ws[k] + w;
+      }
+      if (P.method == 6) {
+        for (int i = 0; i < 15; ++i) cg[i] = cg[i] + vol * (T)ng[i];
+        cws = cws + vol;
+      }
+    }
+    if (P.method == 6) {  // OI of the (3, 5) central gradient: the norm of its first column
+      for (int i = 0; i < 15; ++i) cg[i] = cg[i] / cws;
+      const T q = eps + oi3<T>(cg[0], cg[5], cg[10]);
+      const T wc = cws / (q * q);
+      for (int i = 0; i < 15; ++i) g[i] = g[i] + wc * cg[i];
+      for (int k = 0; k < 5; ++k) ws[k] = ws[k] + wc;
+    }
+    for (int k = 0; k < 5; ++k)
+      for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
   }
-  for (int k = 0; k < 5; ++k)
-    for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
   double u0[5];
   ld5(U, c, u0);
   T uu[5], w0[5];

@@ -213,7 +213,7 @@ extern "C" {
 
 int subfv_ns_batch_create(const subfv_ns_cfg* cfg, int capacity, int64_t budget_bytes, subfv_ns_batch** out) {
   if (!cfg || !out || capacity < 1 || capacity > (1 << 20) || budget_bytes <= 0 ||
-      (cfg->scheme < 1 || cfg->scheme > 8 || cfg->scheme == 7) || (cfg->method != 0 && cfg->method != 1 && cfg->method != 4) ||
+      (cfg->scheme < 1 || cfg->scheme > 8 || cfg->scheme == 7) || (cfg->method < 0 || cfg->method > 6) ||
       cfg->local_time_step != 0 || cfg->n_bc < 0 || cfg->n_bc > 16 || (cfg->precision < 0 || cfg->precision > 2)) {
     set_error("subfv_ns_batch_create: bad argument or unsupported configuration");
     return -2;

@@ -36,9 +36,9 @@ struct subfv_ns_state {
 namespace {
 
 int check_cfg(const subfv_ns_cfg* c) {
-  if (!c || (c->scheme < 1 || c->scheme > 8 || c->scheme == 7) || (c->method != 0 && c->method != 1 && c->method != 4) ||
+  if (!c || (c->scheme < 1 || c->scheme > 8 || c->scheme == 7) || (c->method < 0 || c->method > 6) ||
       c->local_time_step != 0 || c->n_bc < 0 || c->n_bc > 16 || (c->precision < 0 || c->precision > 2)) {
-    set_error("subfv_ns: unsupported configuration (scheme 1-6 or 8, method 0/1/4, global time step, n_bc <= 16)");
+    set_error("subfv_ns: unsupported configuration (scheme 1-6 or 8, method 0-6, global time step, n_bc <= 16)");
     return -2;
   }
   return 0;

@@ -33,6 +33,10 @@ CFGS = {
     "mpp_o2_bc1": dict(scheme=6, second_order=True, method=4, bc_style=1),
     "mpph_o1_bc1": dict(scheme=8, second_order=False, method=4, bc_style=1),
     "mpph_o2_bc2": dict(scheme=8, second_order=True, method=4, bc_style=2),
+    "mp_o2_m2": dict(scheme=1, second_order=True, method=2, bc_style=2),
+    "mp_o2_m3": dict(scheme=1, second_order=True, method=3, bc_style=2),
+    "mp_o2_m5": dict(scheme=1, second_order=True, method=5, bc_style=2),
+    "tw_o2_m6": dict(scheme=4, second_order=True, method=6, bc_style=2),
 }
 
 
@@ -76,7 +80,7 @@ def test_gresho_init_matches_oracle(native, oracle_lib, cuda_ok):
 
 
 @pytest.mark.parametrize("cfg_name", ["mp_o2_bc2", "tw_o2", "mp_o1_bc1", "3w_o2", "m3w_o2", "iso_o2_bc2", "mpp_o2_bc1",
-                                      "mpph_o2_bc2"])
+                                      "mpph_o2_bc2", "mp_o2_m3", "tw_o2_m6"])
 def test_ns_time_loop_bit_exact(native, oracle_lib, cuda_ok, cfg_name):
     from subfv_b200.ns import NsConfig, NsState, init_gresho
     m, o = _pair(_meshes()["hex_slab"])
