@@ -178,7 +178,10 @@ typedef struct subfv_ns_cfg {
   int32_t exclude_bound_vert; /* boundary vertices use two_wave */
   int32_t local_time_step;    /* must be 0 (global time step) */
   int32_t n_bc;               /* boundary tags in use (<= 16) */
-  int32_t bc_type[16];        /* per tag: 1 wall, 3 freestream, 4 outflow supersonic */
+  int32_t bc_type[16];        /* per tag (ns_global_data_module.F90:53-61): 1 wall, 2 adherence
+                                 wall, 3 freestream, 4 outflow supersonic, 5 pondered inflow,
+                                 6 double-Mach inflow/outflow, 7 double-Mach bottom, 8 / 9
+                                 potential flow 2-D / 3-D; others are rejected */
   double bc_val[16][5];       /* per tag: primitive (rho, u, v, w, p) */
   double cfl, tmax;
   int32_t precision;          /* 0 plain FP64; 1 FP32 wave-speed bounds of the nodal solver;

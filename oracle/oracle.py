@@ -59,6 +59,7 @@ def load():
         lib.or_pinv3.argtypes = [PD]
         lib.or_ns_flux.argtypes = [C.c_int, PD, PD, PD, PD, PD]
         lib.or_lu3.argtypes = [PD, PD, PD]
+        lib.or_potential_flow.argtypes = [PD, C.c_int, PD]
         lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_pcgm.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD, C.c_double, PI, PD]

@@ -375,15 +375,83 @@ static bool is_wall(const NsCfg& cfg, int re) {
 }
 
 // :331-409 (wall, freestream, outflow supersonic); sol_l/sol_r conservative
+// the time of the step being evaluated (ns_global_data_module's t, read by the
+// time-dependent boundary states); set by the time loop
+static double g_ns_time = 0.0;
+
+// :413-419 (sol_potential_flow_2d / _3d, ns_euler_exact_sol_module.F90:105-170)
+static void potential_flow(const double* x, bool three_d, double* w) {
+  // the 2-D routine declares its Mach number with a default-kind (single precision)
+  // literal, 1e-4, so its value is the float nearest 1e-4; the 3-D one uses 1e-4_DOUBLE
+  const double r0 = 0.5, r1 = 5.5, rhoinf = 1.4, pinf = 1.0;
+  const double mach = three_d ? 1e-4 : (double)1e-4f;
+  const double vinf = mach * std::sqrt(G * pinf / rhoinf);
+  double ux, uy, uz;
+  if (!three_d) {
+    const double r = std::sqrt(x[0] * x[0] + x[1] * x[1]);
+    const double th = std::atan2(x[1], x[0]);
+    const double c = r1 * r1 / (r1 * r1 - r0 * r0), q = (r0 / r) * (r0 / r);
+    const double vr = c * (1.0 - q) * std::cos(th);
+    const double vt = -c * (1.0 + q) * std::sin(th);
+    ux = vinf * (std::cos(th) * vr - std::sin(th) * vt);
+    uy = vinf * (std::sin(th) * vr + std::cos(th) * vt);
+    uz = 0.0;
+  } else {
+    const double r = std::sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    const double f = r0 * r0 * r0 / (2.0 * (r * r * r * r * r));
+    ux = vinf * (1.0 + f * (r * r - 3.0 * (x[0] * x[0])));
+    uy = -3.0 * vinf * f * x[0] * x[1];
+    uz = -3.0 * vinf * f * x[0] * x[2];
+  }
+  const double vmag2 = ux * ux + uy * uy + uz * uz;
+  w[0] = rhoinf;
+  w[1] = ux;
+  w[2] = uy;
+  w[3] = uz;
+  w[4] = pinf + 0.5 * rhoinf * (vinf * vinf - vmag2);
+}
+
+// :331-409: the ghost state by boundary kind (1 wall, 2 adherence wall, 3 freestream,
+// 4 supersonic outflow, 5 pondered inflow, 6 and 7 the double-Mach inflow/outflow and
+// bottom, 8 and 9 the potential flows), sol_l / sol_r conservative
 static void compute_right_state(const Mesh& m, const NsCfg& cfg, int sf, int re, const double* sol_l, double* sol_r) {
   const double* n = &m.sub_face[sf].norm[1];
+  const double* fx = &m.face[m.sub_face[sf].mesh_face].coord[1];
   int kind = re == 0 ? 1 : cfg.bc_type[-re - 1];
-  if (kind == 1) {
+  const double* bv = re < 0 ? cfg.bc_val + 5 * (-re - 1) : nullptr;
+  auto mirror = [&]() {
     for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
     double d = dot3(sol_r + 1, n);
     for (int k = 1; k < 4; ++k) sol_r[k] = sol_r[k] - 2.0 * d * n[k - 1];
+  };
+  const double post[5] = {8.0, 7.145, -4.125, 0.0, 116.5}, pre[5] = {1.4, 0.0, 0.0, 0.0, 1.0};
+  if (kind == 1) {
+    mirror();
+  } else if (kind == 2) {
+    for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+    for (int k = 1; k < 4; ++k) sol_r[k] = 2.0 * sol_l[0] * bv[k] - sol_l[k];
+    double ul[3], ur[3];
+    for (int d = 0; d < 3; ++d) {
+      ul[d] = sol_l[1 + d] / sol_l[0];
+      ur[d] = sol_r[1 + d] / sol_r[0];
+    }
+    const double nl = fnorm2(ul, 3), nr = fnorm2(ur, 3);
+    sol_r[4] = sol_l[4] - 0.5 * sol_l[0] * (nl * nl) + 0.5 * sol_l[0] * (nr * nr);
   } else if (kind == 3) {
-    p2c(cfg.bc_val + 5 * (-re - 1), sol_r);
+    p2c(bv, sol_r);
+  } else if (kind == 5) {
+    p2c(bv, sol_r);
+    if (dot3(sol_r + 1, n) > 0.0)
+      for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+  } else if (kind == 6) {
+    p2c(fx[1] > 1.732 * (fx[0] - 0.1667 - 10.0 * g_ns_time) ? post : pre, sol_r);
+  } else if (kind == 7) {
+    if (fx[0] < 0.1667) p2c(post, sol_r);
+    else mirror();
+  } else if (kind == 8 || kind == 9) {
+    double w[5];
+    potential_flow(fx, kind == 9, w);
+    p2c(w, sol_r);
   } else {
     for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
   }
@@ -896,6 +964,7 @@ int ns_run(const Mesh& m, const NsCfg& cfg, double* sol, int n_max_iter, double 
   double t = *t_io, res = final_res + 1.0, dt = 0.0;
   int iter = 0, st = 0;
   while (res > final_res && iter <= n_max_iter) {
+    g_ns_time = t;
     st |= compute_rhs_ns(m, cfg, sol, w);
     if (cfg.second_order) {
       std::memcpy(soln.data(), sol, soln.size() * sizeof(double));
@@ -930,6 +999,7 @@ int ns_rhs(const Mesh& m, const NsCfg& cfg, const double* sol, double* rhs, doub
   w.sl.assign(m.n_elems, 0.0);
   w.sl_o2.assign(m.n_elems, 0.0);
   w.vp.assign(3 * m.n_vert, 0.0);
+  g_ns_time = 0.0;
   int st = compute_rhs_ns(m, cfg, sol, w);
   std::memcpy(rhs, w.rhs.data(), w.rhs.size() * sizeof(double));
   std::memcpy(sum_lambda, w.sl.data(), w.sl.size() * sizeof(double));
@@ -1070,15 +1140,38 @@ void be_jacobian(const Mesh& m, const NsCfg& cfg, const double* sol, double dt, 
           double* O = blk(i, R);
           for (int r = 0; r < 5; ++r)
             for (int c = 0; c < 5; ++c) O[r + 5 * c] = O[r + 5 * c] + area * JR[r][c];
-        } else {  // ghost state U_R(U_L): wall M = momentum reflection, outflow I, freestream 0
+        } else {  // ghost state U_R(U_L) through M = dU_R/dU_L: reflections, I or 0
           const int kind = R == 0 ? 1 : cfg.bc_type[-R - 1];
+          const double* bv = R < 0 ? cfg.bc_val + 5 * (-R - 1) : nullptr;
+          const double fx0 = m.face[s.mesh_face].coord[1];
           double M[5][5] = {{0}};
-          if (kind == 1) {
+          if (kind == 1 || (kind == 7 && !(fx0 < 0.1667))) {
             M[0][0] = M[4][4] = 1.0;
             for (int a = 0; a < 3; ++a)
               for (int b = 0; b < 3; ++b) M[a + 1][b + 1] = (a == b ? 1.0 : 0.0) - 2.0 * n[a] * n[b];
           } else if (kind == 4) {
             for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
+          } else if (kind == 5) {
+            double ub[5];
+            p2c(bv, ub);
+            if (dot3(ub + 1, n) > 0.0)
+              for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
+          } else if (kind == 2) {  // rho_r = rho, m_r = 2 rho b - m, E_r = E - |m|^2/2rho + |m_r|^2/2rho
+            double uu = 0.0, rb = 0.0, rr = 0.0;
+            for (int a = 0; a < 3; ++a) {
+              const double r = 2.0 * bv[a + 1] - wl[a + 1];
+              uu = uu + wl[a + 1] * wl[a + 1];
+              rb = rb + r * bv[a + 1];
+              rr = rr + r * r;
+            }
+            M[0][0] = 1.0;
+            for (int a = 0; a < 3; ++a) {
+              M[a + 1][0] = 2.0 * bv[a + 1];
+              M[a + 1][a + 1] = -1.0;
+              M[4][a + 1] = -2.0 * bv[a + 1];
+            }
+            M[4][0] = 0.5 * uu + 2.0 * rb - 0.5 * rr;
+            M[4][4] = 1.0;
           }
           for (int r = 0; r < 5; ++r)
             for (int c = 0; c < 5; ++c) {
@@ -1169,6 +1262,7 @@ long or_be_jacobian(void* h, const int* ic, const double* dc, const int* bc_type
                     const double* sol, double dt, int* row, int* col, double* v, long cap) {
   std::vector<int> r, c;
   std::vector<double> vv;
+  g_ns_time = 0.0;
   be_jacobian(handle_mesh(h), make_cfg(ic, dc, bc_type, bc_val), sol, dt, r, c, vv);
   if ((long)c.size() > cap) return -(long)c.size();
   std::memcpy(row, r.data(), r.size() * sizeof(int));
@@ -1177,5 +1271,7 @@ long or_be_jacobian(void* h, const int* ic, const double* dc, const int* bc_type
   return (long)c.size();
 }
 void or_lu3(double* a9, double* x, const double* b) { oracle_lu3(a9, x, b); }
+// sol_potential_flow_2d / _3d at x (primitive w)
+void or_potential_flow(const double* x, int three_d, double* w) { potential_flow(x, three_d != 0, w); }
 
 }  // extern "C"

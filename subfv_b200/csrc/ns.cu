@@ -259,10 +259,108 @@ __device__ inline bool is_wall(const NsParams& P, int y) {
   return P.bc_type[-(y + 1) - 1] == 1;
 }
 
-// compute_right_state (:331-409) for walls, freestream and supersonic outflow;
-// sol_l / sol_r conservative, n the subface normal
+// OI (ns_euler_recon_module.F90:322-329): gfortran's scaled NORM2 of a 3-vector, in T
 template <class T>
-__device__ void right_state(const NsParams& P, int y, const T* n, const T* sol_l, T* sol_r) {
+__device__ inline T oi3(T a0, T a1, T a2) {
+  const T a[3] = {a0, a1, a2};
+  T scale = 1, res = 0;
+  for (int i = 0; i < 3; ++i)
+    if (a[i] != (T)0) {
+      T ax = fabs(a[i]);
+      if (ax > scale) {
+        T q = scale / ax;
+        res = (T)1 + res * q * q;
+        scale = ax;
+      } else {
+        T q = ax / scale;
+        res += q * q;
+      }
+    }
+  return scale * sqrt(res);
+}
+
+// sol_potential_flow_2d / _3d (ns_euler_exact_sol_module.F90:105-170) at x, primitive.
+// The 2-D routine's Mach number is a default-kind (single precision) literal, so its
+// value is the float nearest 1e-4; the 3-D one is 1e-4 in double.
+template <class T>
+__device__ __noinline__ void potential_flow(const double4 x4, bool three_d, T* w) {
+  const T x[3] = {(T)x4.x, (T)x4.y, (T)x4.z};
+  const T r0 = (T)0.5, r1 = (T)5.5, rhoinf = (T)1.4, pinf = (T)1.0;
+  const T mach = three_d ? (T)1e-4 : (T)1e-4f;
+  const T vinf = mach * sqrt((T)G * pinf / rhoinf);
+  T ux, uy, uz;
+  if (!three_d) {
+    const T r = sqrt(x[0] * x[0] + x[1] * x[1]);
+    const T th = atan2(x[1], x[0]);
+    const T c = r1 * r1 / (r1 * r1 - r0 * r0), q = (r0 / r) * (r0 / r);
+    const T vr = c * ((T)1 - q) * cos(th);
+    const T vt = -c * ((T)1 + q) * sin(th);
+    ux = vinf * (cos(th) * vr - sin(th) * vt);
+    uy = vinf * (sin(th) * vr + cos(th) * vt);
+    uz = (T)0;
+  } else {
+    const T r = sqrt(x[0] * x[0] + x[1] * x[1] + x[2] * x[2]);
+    const T f = r0 * r0 * r0 / ((T)2 * (r * r * r * r * r));
+    ux = vinf * ((T)1 + f * (r * r - (T)3 * (x[0] * x[0])));
+    uy = (T)-3 * vinf * f * x[0] * x[1];
+    uz = (T)-3 * vinf * f * x[0] * x[2];
+  }
+  const T vmag2 = ux * ux + uy * uy + uz * uz;
+  w[0] = rhoinf;
+  w[1] = ux;
+  w[2] = uy;
+  w[3] = uz;
+  w[4] = pinf + (T)0.5 * rhoinf * (vinf * vinf - vmag2);
+}
+
+// compute_right_state (:331-409): the ghost state by boundary kind (1 wall, 2 adherence
+// wall, 3 freestream, 4 supersonic outflow, 5 pondered inflow, 6 double-Mach inflow /
+// outflow, 7 double-Mach bottom, 8 and 9 the potential flows in 2-D and 3-D); sol_l /
+// sol_r conservative, n the subface normal. The kinds that read the face centroid or the
+// time do so out of line; sc->t is the time of the step being evaluated (null: 0).
+template <class T>
+__device__ __noinline__ void right_state_ext(const DevMesh& m, const NsParams& P, int kind, int y, int sf,
+                                             const T* n, const T* sol_l, T* sol_r, const NsScalars* sc) {
+  const double* bv = P.bc_val[-(y + 1) - 1];
+  if (kind == 2) {
+    for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+    for (int k = 1; k < 4; ++k) sol_r[k] = (T)2.0 * sol_l[0] * (T)bv[k] - sol_l[k];
+    const T nl = oi3<T>(sol_l[1] / sol_l[0], sol_l[2] / sol_l[0], sol_l[3] / sol_l[0]);
+    const T nr = oi3<T>(sol_r[1] / sol_r[0], sol_r[2] / sol_r[0], sol_r[3] / sol_r[0]);
+    sol_r[4] = sol_l[4] - (T)0.5 * sol_l[0] * (nl * nl) + (T)0.5 * sol_l[0] * (nr * nr);
+    return;
+  }
+  if (kind == 5) {
+    T w[5];
+    for (int k = 0; k < 5; ++k) w[k] = (T)bv[k];
+    p2c(w, sol_r);
+    if (dotT(sol_r + 1, n) > (T)0)
+      for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+    return;
+  }
+  const double4 fx = m.fc[m.sf_face[sf]];
+  if (kind == 8 || kind == 9) {
+    T w[5];
+    potential_flow<T>(fx, kind == 9, w);
+    p2c(w, sol_r);
+    return;
+  }
+  const T post[5] = {(T)8.0, (T)7.145, (T)-4.125, (T)0.0, (T)116.5}, pre[5] = {(T)1.4, 0, 0, 0, (T)1.0};
+  if (kind == 6) {
+    const T t = sc ? (T)sc->t : (T)0;
+    p2c((T)fx.y > (T)1.732 * ((T)fx.x - (T)0.1667 - (T)10.0 * t) ? post : pre, sol_r);
+  } else if ((T)fx.x < (T)0.1667) {  // kind 7
+    p2c(post, sol_r);
+  } else {
+    for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+    T d = dotT(sol_r + 1, n);
+    for (int k = 1; k < 4; ++k) sol_r[k] = sol_r[k] - (T)2.0 * d * n[k - 1];
+  }
+}
+
+template <class T>
+__device__ void right_state(const DevMesh& m, const NsParams& P, int y, int sf, const T* n, const T* sol_l, T* sol_r,
+                            const NsScalars* sc) {
   int kind = y == -1 ? 1 : P.bc_type[-(y + 1) - 1];
   if (kind == 1) {
     for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
@@ -272,15 +370,17 @@ __device__ void right_state(const NsParams& P, int y, const T* n, const T* sol_l
     T w[5];
     for (int k = 0; k < 5; ++k) w[k] = (T)P.bc_val[-(y + 1) - 1][k];
     p2c(w, sol_r);
-  } else {
+  } else if (kind == 4) {
     for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
+  } else {
+    right_state_ext<T>(m, P, kind, y, sf, n, sol_l, sol_r, sc);
   }
 }
 
 // reconstruct_lr_w (:427-451); grad records [15] with g[5*d + var] = grad(d+1, var+1)
 template <class T>
 __device__ void reconstruct(const DevMesh& m, const NsParams& P, const double* U, const double* grad, int v, int sf,
-                            int le, int y, bool so, double* wl_out, double* wr_out) {
+                            int le, int y, bool so, double* wl_out, double* wr_out, const NsScalars* sc) {
   T ul[5], wl[5], wr[5];
   double u64[5];
   ld5(U, le, u64);
@@ -317,7 +417,7 @@ __device__ void reconstruct(const DevMesh& m, const NsParams& P, const double* U
     const T n[3] = {(T)sn.x, (T)sn.y, (T)sn.z};
     T uc[5], gh[5];
     p2c(wl, uc);
-    right_state(P, y, n, uc, gh);
+    right_state(m, P, y, sf, n, uc, gh, sc);
     c2p(gh, wr);
   }
   for (int k = 0; k < 5; ++k) {
@@ -672,7 +772,8 @@ __device__ __noinline__ double nodal_pressure_vertex(const DevMesh& m, const NsP
 // instantiation without them keeps the common path's register allocation.
 template <class T, class L, int MS, bool EXT>
 __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
-                               const double* __restrict__ grad, double* __restrict__ fs, int so, const int v) {
+                               const double* __restrict__ grad, double* __restrict__ fs, int so, const int v,
+                               const NsScalars* sc) {
   if (v >= m.nv) return;
   const int p0 = m.vsf_off[v], nsfn = m.vsf_off[v + 1] - p0;
   const int q0 = m.vse_off[v], nsen = m.vse_off[v + 1] - q0;
@@ -693,7 +794,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     yj[j] = lr.y;
     if (EXT && P.scheme == 2) amin = j == 0 ? m.sfn[sf].w : fmin2(amin, m.sfn[sf].w);
     double w10[10];
-    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5);
+    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5, sc);
     for (int k = 0; k < 10; ++k) wlr[j][k] = (T)w10[k];
     lam[j][0] = lam[j][1] = (L)0;
   }
@@ -861,7 +962,7 @@ template <class T, class L, int NG>
 __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
                               const double* __restrict__ grad, double* __restrict__ fs, int so, const int v,
                               const bool live, double* __restrict__ gv, unsigned* __restrict__ gf,
-                              double* __restrict__ gs) {
+                              double* __restrict__ gs, const NsScalars* sc) {
   const int j = threadIdx.x & (NG - 1);
   const unsigned mask = group_mask<NG>();
   int p0 = 0, nsfn = 0, q0 = 0, nsen = 0;
@@ -886,7 +987,7 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
     const int2 lr = m.flr[m.sf_face[sf]];
     y = lr.y;
     double w10[10];
-    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5);
+    reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5, sc);
     for (int k = 0; k < 10; ++k) w[k] = (T)w10[k];
     const double4 sn = m.sfn[sf];
     n[0] = sn.x;
@@ -1097,7 +1198,7 @@ __global__ void __launch_bounds__(kNodeGroupThreads, 2) k_ns_node_group(DevMesh 
   __shared__ NodeGroupSmem sm;
   const int g = threadIdx.x / NG;
   const int v = blockIdx.x * (kNodeGroupThreads / NG) + g;
-  ns_node_group<T, L, NG>(m, P, U, grad, fs, so, v, true, sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g]);
+  ns_node_group<T, L, NG>(m, P, U, grad, fs, so, v, true, sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g], sc);
 }
 
 template <class T, class L, int MS, bool EXT>
@@ -1105,7 +1206,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_ns_node(DevMesh m, NsParams P,
                                                           const double* __restrict__ grad, double* __restrict__ fs,
                                                           int so, const NsScalars* sc) {
   if (sc && sc->done) return;
-  ns_node_vertex<T, L, MS, EXT>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x);
+  ns_node_vertex<T, L, MS, EXT>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x, sc);
 }
 
 __device__ inline double warp_min(double x) {
@@ -1192,26 +1293,6 @@ __device__ void ns_nodal_grad_body(const DevMesh& m, const double* __restrict__ 
 __global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* __restrict__ U,
                                                        double* __restrict__ ngrad, const NsScalars* sc) {
   ns_nodal_grad_body(m, U, ngrad, sc, blockIdx.x * blockDim.x + threadIdx.x);
-}
-
-// OI (ns_euler_recon_module.F90:322-329): gfortran's scaled NORM2 of a 3-vector, in T
-template <class T>
-__device__ inline T oi3(T a0, T a1, T a2) {
-  const T a[3] = {a0, a1, a2};
-  T scale = 1, res = 0;
-  for (int i = 0; i < 3; ++i)
-    if (a[i] != (T)0) {
-      T ax = fabs(a[i]);
-      if (ax > scale) {
-        T q = scale / ax;
-        res = (T)1 + res * q * q;
-        scale = ax;
-      } else {
-        T q = ax / scale;
-        res += q * q;
-      }
-    }
-  return scale * sqrt(res);
 }
 
 // compute_cell_grad_method_2..6 (:166-320) + physical_slope_limiter + relaxed_maximum_principle
@@ -1525,7 +1606,7 @@ __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restr
     const NsItem& I = it[p];
     if (I.sc->done) continue;
     ns_node_vertex<T, L, MS, EXT>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so,
-                                  (w - wv[p]) * blockDim.x + threadIdx.x);
+                                  (w - wv[p]) * blockDim.x + threadIdx.x, I.sc);
   }
 }
 // the group variant: a work block of block_v vertices is walked kNodeGroupThreads / NG
@@ -1545,7 +1626,7 @@ __global__ void __launch_bounds__(kNodeGroupThreads, 2) kb_ns_node_group(const N
     if (I.sc->done) continue;
     for (int c = 0; c < block_v; c += VPB)
       ns_node_group<T, L, NG>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * block_v + c + g, true,
-                             sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g]);
+                             sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g], I.sc);
   }
 }
 __global__ void __launch_bounds__(128) kb_ns_gather(const NsItem* __restrict__ it, const int* __restrict__ wc,
@@ -1701,22 +1782,49 @@ __device__ inline double euler_jac_entry(const EulerJacScalars& e, const double*
 }
 
 // A boundary subface's term of the diagonal block, area (J_L + J_R M), column-major:
-// the ghost state U_R(U_L) enters through M (wall: momentum reflection, outflow: I,
-// freestream: 0). Out of line: rare, and it holds three full matrices.
+// the ghost state U_R(U_L) enters through M = dU_R/dU_L (wall, and the double-Mach
+// bottom past x = 0.1667: momentum reflection; outflow, and pondered inflow leaving the
+// domain: I; adherence wall: the derivative of its reflection about the wall velocity;
+// imposed states: 0). fx0 is the face centroid's x. Out of line: rare, and it holds
+// three full matrices.
 __device__ __noinline__ void ghost_block(const NsParams& P, int y, const double* wl, const double* wr,
-                                         const double* n, double area, double* g) {
+                                         const double* n, double area, double fx0, double* g) {
   double JL[5][5], JR[5][5];
   two_wave_jac(wl, wr, n, JL, JR);
   const int kind = y == -1 ? 1 : P.bc_type[-(y + 1) - 1];
   double M[5][5];
   for (int a = 0; a < 5; ++a)
     for (int b = 0; b < 5; ++b) M[a][b] = 0.0;
-  if (kind == 1) {
+  const double* bv = y == -1 ? nullptr : P.bc_val[-(y + 1) - 1];
+  if (kind == 1 || (kind == 7 && !(fx0 < 0.1667))) {
     M[0][0] = M[4][4] = 1.0;
     for (int a = 0; a < 3; ++a)
       for (int b = 0; b < 3; ++b) M[a + 1][b + 1] = (a == b ? 1.0 : 0.0) - 2.0 * n[a] * n[b];
   } else if (kind == 4) {
     for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
+  } else if (kind == 5) {
+    double ub[5];
+    p2c(bv, ub);
+    if (dotT(ub + 1, n) > 0.0)
+      for (int a = 0; a < 5; ++a) M[a][a] = 1.0;
+  } else if (kind == 2) {
+    // rho_r = rho, m_r = 2 rho b - m, E_r = E - |m|^2/(2 rho) + |m_r|^2/(2 rho); with
+    // u = m / rho and r = 2 b - u: dE_r/drho = |u|^2/2 + 2 r.b - |r|^2/2, dE_r/dm = -2 b
+    double uu = 0.0, rb = 0.0, rr = 0.0;
+    for (int a = 0; a < 3; ++a) {
+      const double r = 2.0 * bv[a + 1] - wl[a + 1];
+      uu = uu + wl[a + 1] * wl[a + 1];
+      rb = rb + r * bv[a + 1];
+      rr = rr + r * r;
+    }
+    M[0][0] = 1.0;
+    for (int a = 0; a < 3; ++a) {
+      M[a + 1][0] = 2.0 * bv[a + 1];
+      M[a + 1][a + 1] = -1.0;
+      M[4][a + 1] = -2.0 * bv[a + 1];
+    }
+    M[4][0] = 0.5 * uu + 2.0 * rb - 0.5 * rr;
+    M[4][4] = 1.0;
   }
   for (int r = 0; r < 5; ++r)
     for (int cc = 0; cc < 5; ++cc) {
@@ -1737,7 +1845,8 @@ __device__ __noinline__ void ghost_block(const NsParams& P, int y, const double*
 __global__ void __launch_bounds__(64) k_be_assemble(DevMesh m, NsParams P, const double* __restrict__ U,
                                                     const int* __restrict__ jq_off, const int* __restrict__ jq,
                                                     const int* __restrict__ jblk, const int* __restrict__ row_off,
-                                                    const int* __restrict__ dblk, double* __restrict__ v, double dt) {
+                                                    const int* __restrict__ dblk, double* __restrict__ v, double dt,
+                                                    const NsScalars* sc) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= m.ne) return;
   const int rb = row_off[c], re = row_off[c + 1], db = dblk[c];
@@ -1768,10 +1877,10 @@ __global__ void __launch_bounds__(64) k_be_assemble(DevMesh m, NsParams P, const
     const double n[3] = {sn.x, sn.y, sn.z};
     const double area = sn.w;
     double wl[5], wr[5];
-    reconstruct<double>(m, P, U, nullptr, m.sf_vert[sf], sf, lr.x, lr.y, false, wl, wr);
+    reconstruct<double>(m, P, U, nullptr, m.sf_vert[sf], sf, lr.x, lr.y, false, wl, wr, sc);
     if (side == 0 && lr.y < 0) {
       double g[25];
-      ghost_block(P, lr.y, wl, wr, n, area, g);
+      ghost_block(P, lr.y, wl, wr, n, area, m.fc[m.sf_face[sf]].x, g);
 #pragma unroll
       for (int e = 0; e < 25; ++e) D[e] = D[e] + g[e];
       continue;
@@ -1956,8 +2065,9 @@ void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* 
 }
 
 void launch_be_assemble(const DevMesh& m, const NsParams& P, const double* U, const int* jq_off, const int* jq,
-                        const int* jblk, const int* row_off, const int* dblk, double* v, double dt) {
-  k_be_assemble<<<grid_for(m.ne, 64), 64, 0, m.stream>>>(m, P, U, jq_off, jq, jblk, row_off, dblk, v, dt);
+                        const int* jblk, const int* row_off, const int* dblk, double* v, double dt,
+                        const NsScalars* sc) {
+  k_be_assemble<<<grid_for(m.ne, 64), 64, 0, m.stream>>>(m, P, U, jq_off, jq, jblk, row_off, dblk, v, dt, sc);
 }
 void launch_be_pack_rhs(const DevMesh& m, const double* rhs, double* b) {
   k_be_pack_rhs<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m.ne, rhs, b);

@@ -74,7 +74,8 @@ void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* 
                              const NsScalars* sc);
 // Backward-Euler Jacobian of the first-order two-wave residual (frozen wave speeds)
 void launch_be_assemble(const DevMesh& m, const NsParams& P, const double* U, const int* jq_off, const int* jq,
-                        const int* jblk, const int* row_off, const int* dblk, double* v, double dt);
+                        const int* jblk, const int* row_off, const int* dblk, double* v, double dt,
+                        const NsScalars* sc);
 void launch_be_pack_rhs(const DevMesh& m, const double* rhs, double* b);
 void launch_be_update(const DevMesh& m, double* U, const double* x);
 int ns_partial_blocks(const DevMesh& m);

@@ -41,6 +41,12 @@ int check_cfg(const subfv_ns_cfg* c) {
     set_error("subfv_ns: unsupported configuration (scheme 1-6 or 8, method 0-6, global time step, n_bc <= 16)");
     return -2;
   }
+  // compute_right_state's select case stops on a kind it does not know
+  for (int i = 0; i < c->n_bc; ++i)
+    if (c->bc_type[i] < 1 || c->bc_type[i] > 9) {
+      set_error("subfv_ns: boundary kind not recognized (1-9)");
+      return -2;
+    }
   return 0;
 }
 
@@ -423,7 +429,7 @@ int implicit_assemble(subfv_ns_state* s, double cfl_implicit, double dt_force, d
   SUBFV_CUDA(cudaMemcpyAsync(&dtred, &s->sc->dtred, sizeof(double), cudaMemcpyDeviceToHost, d.stream));
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
   const double dt = dt_force > 0.0 ? dt_force : cfl_implicit * dtred;
-  launch_be_assemble(d, Q, s->U0, c->jq_off, c->jq, c->jblk, c->row_off, c->dblk, c->A.v, dt);
+  launch_be_assemble(d, Q, s->U0, c->jq_off, c->jq, c->jblk, c->row_off, c->dblk, c->A.v, dt, s->sc);
   launch_be_pack_rhs(d, s->rhs1, c->b);
   if (bcsr_set_values(&c->A, c->A.v, true)) return -1;
   *dt_out = dt;

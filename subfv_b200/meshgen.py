@@ -87,6 +87,27 @@ def hex_slab(nx, ny, x0=-0.5, x1=0.5, y0=-0.5, y1=0.5, z0=-0.5, z1=0.5, jitter=0
                    ev.astype(np.int32).ravel(), b2d=True)
 
 
+def tag_slab_sides(raw: RawMesh, nx: int, ny: int, tags: dict) -> RawMesh:
+    """A copy of a hex_slab / prism_slab mesh of nx*ny columns with its side boundaries
+    tagged (the MSH2 boundary elements the reference reads): tags maps "xlo", "xhi",
+    "ylo", "yhi" to a physical tag (1-based; a side left out stays a default wall)."""
+    nl = (nx + 1) * (ny + 1)
+    vid = lambda i, j: j * (nx + 1) + i
+    edges = {"ylo": [(vid(i, 0), vid(i + 1, 0)) for i in range(nx)],
+             "yhi": [(vid(i, ny), vid(i + 1, ny)) for i in range(nx)],
+             "xlo": [(vid(0, j), vid(0, j + 1)) for j in range(ny)],
+             "xhi": [(vid(nx, j), vid(nx, j + 1)) for j in range(ny)]}
+    fv, ft = [], []
+    for side, tag in tags.items():
+        for p, q in edges[side]:
+            fv.append([p + 1, q + 1, q + nl + 1, p + nl + 1])
+            ft.append(int(tag))
+    off = (np.arange(len(fv) + 1) * 4).astype(np.int32)
+    return RawMesh(raw.coords, raw.elem_kind, raw.elem_vert_off, raw.elem_vert, off,
+                   np.asarray(fv, np.int32).reshape(-1), np.asarray(ft, np.int32), b2d=raw.b2d,
+                   periodic=raw.periodic)
+
+
 def prism_slab(nx, ny, x0=0.0, x1=1.2, y0=0.0, y1=1.2, z0=0.0, z1=1.0, jitter=0.0, seed=0):
     """Each square split into two triangles along alternating diagonals, extruded
     one layer: 2*nx*ny prisms (a triangle mesh in the reference's 2-D mode)."""

@@ -20,7 +20,10 @@ from .mesh import Mesh
 SCHEME_MULTI_POINT, SCHEME_MULTI_POINT_ISO, SCHEME_THREE_WAVE, SCHEME_TWO_WAVE, SCHEME_MODIFIED_THREE_WAVE = 1, 2, 3, 4, 5
 SCHEME_MULTI_POINT_PRESSURE, SCHEME_MULTI_POINT_PRESSURE_PH = 6, 8
 # (the scheme ids of ns_global_data_module.F90:67-71)
-BC_WALL, BC_FREESTREAM, BC_OUTFLOW_SUPERSONIC = 1, 3, 4
+# the Euler boundary kinds of ns_global_data_module.F90:53-61 (bc_type per tag; bc_val
+# the primitive state a kind reads: freestream, pondered inflow, the adherence wall's velocity)
+BC_WALL, BC_ADHERENCE_WALL, BC_FREESTREAM, BC_OUTFLOW_SUPERSONIC, BC_INFLOW_POND = 1, 2, 3, 4, 5
+BC_INOUT_DOUBLE_MACH, BC_DOUBLE_MACH_BOTTOM, BC_POTENTIAL_FLOW_2D, BC_POTENTIAL_FLOW_3D = 6, 7, 8, 9
 
 
 class NsCfgC(C.Structure):
