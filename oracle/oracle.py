@@ -60,6 +60,7 @@ def load():
         lib.or_ns_flux.argtypes = [C.c_int, PD, PD, PD, PD, PD]
         lib.or_lu3.argtypes = [PD, PD, PD]
         lib.or_potential_flow.argtypes = [PD, C.c_int, PD]
+        lib.or_ns_set_diffusion.argtypes = [C.c_int, C.c_int, PD, C.c_int, PI, PD, PI, PD]
         lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_pcgm.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD, C.c_double, PI, PD]
@@ -193,6 +194,15 @@ class OracleMesh:
     # --- explicit Euler (subfvns)
     @staticmethod
     def _ns_args(cfg):
+        nb = max(1, int(cfg.get("n_bc", 0)))
+        dif = [np.ascontiguousarray(cfg.get("diff_dc", [1.329e-5, 1.716e-5, 273.15, 720.19471]), np.float64),
+               np.ascontiguousarray(cfg.get("bc_type_V", np.zeros(nb)), np.int32),
+               np.ascontiguousarray(cfg.get("bc_val_V", np.zeros((nb, 3))), np.float64).reshape(-1),
+               np.ascontiguousarray(cfg.get("bc_type_T", np.zeros(nb)), np.int32),
+               np.ascontiguousarray(cfg.get("bc_val_T", np.zeros(nb)), np.float64)]
+        load().or_ns_set_diffusion(int(cfg.get("activate_diffusion", 0)), int(cfg.get("use_sutherland", 0)),
+                                   _pd(dif[0]), int(cfg.get("n_bc", 0)), _pi(dif[1]), _pd(dif[2]), _pi(dif[3]),
+                                   _pd(dif[4]))
         ic = np.array([cfg["scheme"], cfg["second_order"], cfg["method"], cfg["bc_style"], cfg["b2d"],
                        cfg["exclude_bound_vert"], cfg["local_time_step"], cfg.get("n_bc", 0)], np.int32)
         dc = np.array([cfg["cfl"], cfg["tmax"]], np.float64)

@@ -893,18 +893,389 @@ static void flux_limiting(const Mesh& m, const double* sol, double* rhs, const d
 }
 
 struct NsWork {
-  std::vector<double> rhs, rhs_o2, sl, sl_o2, grad, ngrad, vp, delta;
+  std::vector<double> rhs, rhs_o2, sl, sl_o2, grad, ngrad, vp, delta, diag;
 };
 
-// ns_main.F90:130-179 (no diffusion)
+// ------------------------------------------------------------------------------------
+// Diffusion (activate_diffusion): ns_vectorial_diffusion_module.F90 (momentum) and
+// ns_diffusion_module.F90 (heat), point-implicit blocks in mat_diag and terms in rhs.
+// The LAPACK / BLAS calls are restated in the reference (netlib) implementations'
+// operation order: dgetrf for n < 64 is dgetrf2, which for these sizes performs the
+// right-looking elimination with partial pivoting (first largest |pivot|, the column
+// scaled by the pivot's reciprocal); dgetri (the workspace of n the reference passes
+// selects the unblocked code) is dtrti2 then the column sweep with dgemv; dgemm / dgemv
+// accumulate each output from zero over the inner index in ascending order.
+
+struct DiffCfg {
+  int active = 0, use_sutherland = 0;
+  double mu_p = 1.329e-5, mu0 = 1.716e-5, T0 = 273.15, Cv_p = 720.19471;
+  int bcV[16] = {0}, bcT[16] = {0};  // 1 neumann, 2 dirichlet
+  double valV[16][3] = {{0}}, valT[16] = {0};
+};
+static DiffCfg g_diff;
+static const double kPrandtl = 0.71, kC0 = 110.4;  // ns_global_data_module.F90:10,20
+
+// column-major n x n, A(i,j) = a[i + n*j]
+static void lapack_getrf(int n, double* a, int* ipiv) {
+  const double sfmin = 2.2250738585072014e-308;  // dlamch('S')
+  for (int j = 0; j < n; ++j) {
+    int p = j;
+    double big = std::fabs(a[j + n * j]);
+    for (int i = j + 1; i < n; ++i)
+      if (std::fabs(a[i + n * j]) > big) {
+        big = std::fabs(a[i + n * j]);
+        p = i;
+      }
+    ipiv[j] = p;
+    if (a[p + n * j] != 0.0) {
+      if (p != j)
+        for (int k = 0; k < n; ++k) std::swap(a[j + n * k], a[p + n * k]);
+      if (std::fabs(a[j + n * j]) >= sfmin) {
+        const double r = 1.0 / a[j + n * j];
+        for (int i = j + 1; i < n; ++i) a[i + n * j] = r * a[i + n * j];
+      } else {
+        for (int i = j + 1; i < n; ++i) a[i + n * j] = a[i + n * j] / a[j + n * j];
+      }
+    }
+    for (int k = j + 1; k < n; ++k)
+      for (int i = j + 1; i < n; ++i) a[i + n * k] = a[i + n * k] - a[i + n * j] * a[j + n * k];
+  }
+}
+// dgetrs('N') for one right-hand side
+static void lapack_getrs(int n, const double* a, const int* ipiv, double* b) {
+  for (int j = 0; j < n; ++j)
+    if (ipiv[j] != j) std::swap(b[j], b[ipiv[j]]);
+  for (int k = 0; k < n; ++k)
+    if (b[k] != 0.0)
+      for (int i = k + 1; i < n; ++i) b[i] = b[i] - b[k] * a[i + n * k];
+  for (int k = n - 1; k >= 0; --k)
+    if (b[k] != 0.0) {
+      b[k] = b[k] / a[k + n * k];
+      for (int i = 0; i < k; ++i) b[i] = b[i] - b[k] * a[i + n * k];
+    }
+}
+// inv_lapack (linear_solver_module.F90:629-641): dgetrf + dgetri
+static void lapack_inverse(int n, double* a) {
+  std::vector<int> ipiv(n);
+  std::vector<double> work(n);
+  lapack_getrf(n, a, ipiv.data());
+  for (int j = 0; j < n; ++j) {  // dtrti2 ('Upper', 'Non-unit')
+    a[j + n * j] = 1.0 / a[j + n * j];
+    const double ajj = -a[j + n * j];
+    double* x = a + n * j;  // dtrmv on x(0:j-1) with the inverted leading block
+    for (int jj = 0; jj < j; ++jj)
+      if (x[jj] != 0.0) {
+        const double temp = x[jj];
+        for (int i = 0; i < jj; ++i) x[i] = x[i] + temp * a[i + n * jj];
+        x[jj] = x[jj] * a[jj + n * jj];
+      }
+    for (int i = 0; i < j; ++i) x[i] = ajj * x[i];
+  }
+  for (int j = n - 1; j >= 0; --j) {
+    for (int i = j + 1; i < n; ++i) {
+      work[i] = a[i + n * j];
+      a[i + n * j] = 0.0;
+    }
+    for (int jj = j + 1; jj < n; ++jj) {  // dgemv: A(:,j) += -work(jj) * A(:,jj)
+      const double temp = -work[jj];
+      for (int i = 0; i < n; ++i) a[i + n * j] = a[i + n * j] + temp * a[i + n * jj];
+    }
+  }
+  for (int j = n - 2; j >= 0; --j)
+    if (ipiv[j] != j)
+      for (int i = 0; i < n; ++i) std::swap(a[i + n * j], a[i + n * ipiv[j]]);
+}
+// C(m x p) = A(m x k) * B(k x p), netlib dgemm order
+static void blas_gemm(int m, int p, int k, const double* A, const double* B, double* C) {
+  for (int j = 0; j < p; ++j)
+    for (int i = 0; i < m; ++i) {
+      double s = 0.0;
+      for (int l = 0; l < k; ++l) s = s + B[l + k * j] * A[i + m * l];
+      C[i + m * j] = s;
+    }
+}
+// y(m) = A(m x n) x, netlib dgemv order
+static void blas_gemv(int m, int n, const double* A, const double* x, double* y) {
+  for (int i = 0; i < m; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s = s + x[j] * A[i + m * j];
+    y[i] = s;
+  }
+}
+
+// temp_u (ns_euler_primitives_module.F90:52-63)
+static double temp_u(const double* u) {
+  const double tau = 1.0 / u[0];
+  const double uu = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+  return (u[4] * tau - 0.5 * uu * (tau * tau)) / g_diff.Cv_p;
+}
+// mu_sutherland / compute_mu (ns_vectorial_diffusion_module.F90:320-357)
+static double mu_of(const double* u) {
+  if (!g_diff.use_sutherland) return g_diff.mu_p;
+  const double T = temp_u(u);
+  return g_diff.mu0 * std::pow(T / g_diff.T0, 1.5) * (g_diff.T0 + kC0) / (T + kC0);
+}
+
+// the sub_elem / sub_face relations of one vertex in the reference's local numbering
+static double se_sign_norm(const Mesh& m, int isfp, int se, double* np) {
+  const SubFace& s = m.sub_face[isfp];
+  for (int d = 0; d < 3; ++d) np[d] = s.left_sub_elem_neigh == se ? s.norm[1 + d] : -s.norm[1 + d];
+  return s.area;
+}
+
+// the momentum blc_3 (:85-91): s * (mu (nl.np) I + (mu - mu0corr) np (x) nl + (mu0corr - 2/3 mu) nl (x) np)
+static void mom_block(double al, double ap, double vol, double mu, double mu0c, const double* nl, const double* np,
+                      double blc[3][3]) {
+  const double s = al * ap * (1.0 / vol);
+  const double d = nl[0] * np[0] + nl[1] * np[1] + nl[2] * np[2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double e = i == j ? 1.0 : 0.0;
+      const double tp = np[i] * nl[j], tpt = np[j] * nl[i];
+      blc[i][j] = s * ((mu * d * e + (mu - mu0c) * tp) + (mu0c - (2.0 / 3.0) * mu) * tpt);
+    }
+}
+// the Neumann face's N and S block (:149-152): s * ((nl.np) I + (np (x) nl)^T / 3)
+static void neumann_block(double al, double ap, double vol, const double* nl, const double* np, double blc[3][3]) {
+  const double s = al * ap * (1.0 / vol);
+  const double d = nl[0] * np[0] + nl[1] * np[1] + nl[2] * np[2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double e = i == j ? 1.0 : 0.0;
+      blc[i][j] = s * (d * e + (np[j] * nl[i]) / 3.0);
+    }
+}
+
+// build_momentum_diff_mat_into_global_mat_diag (:195-318), all vertices
+static void momentum_diffusion(const Mesh& m, const double* sol, const double* mu, double mu0c, double* diag,
+                               double* rhs) {
+  for (int v = 1; v <= m.n_vert; ++v) {
+    const Vert& V = m.vert[v];
+    const int nf = V.n_sub_faces_neigh, ne = V.n_sub_elems_neigh, F = 3 * nf, E = 3 * ne;
+    std::vector<double> N(F * F, 0.0), S(F * E, 0.0), St(E * F, 0.0), B(F, 0.0);
+    // build_momentum_diff_nodal_system (:7-193)
+    for (int l = 0; l < nf; ++l) {
+      const int isfl = V.sub_face_neigh[l + 1];
+      const SubFace& sl = m.sub_face[isfl];
+      const int ifl0 = 3 * (sl.id_loc_around_node - 1);
+      const int re = sl.right_elem_neigh;
+      bool neu = false, dir = false;
+      if (re < 0) {
+        dir = g_diff.bcV[-re - 1] == 2;
+        neu = g_diff.bcV[-re - 1] == 1;
+      } else if (re == 0) {
+        neu = true;
+      }
+      auto side = [&](int se, int elem, const double* nl, int mode) {
+        // mode 0: N, S, St with the full block; 1: Neumann (N, S the plain block, St the
+        // full one); 2: Dirichlet (St only)
+        const SubElem& E0 = m.sub_elem[se];
+        const int ise0 = 3 * (E0.id_loc_around_node - 1);
+        const double mue = mu[elem - 1];
+        for (int p = 0; p < E0.n_sub_faces; ++p) {
+          const int isfp = E0.sub_face[p + 1];
+          const int ifp0 = 3 * (m.sub_face[isfp].id_loc_around_node - 1);
+          double np[3];
+          const double ap = se_sign_norm(m, isfp, se, np);
+          double blc[3][3], bn[3][3];
+          mom_block(sl.area, ap, E0.volume, mue, mu0c, nl, np, blc);
+          if (mode == 1) neumann_block(sl.area, ap, E0.volume, nl, np, bn);
+          const double (*bNS)[3] = mode == 1 ? bn : blc;
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+              St[(ise0 + i) + E * (ifl0 + j)] += blc[j][i];
+              if (mode != 2) {
+                N[(ifl0 + i) + F * (ifp0 + j)] += bNS[i][j];
+                S[(ifl0 + i) + F * (ise0 + j)] += bNS[i][j];
+              }
+            }
+        }
+      };
+      const double nl[3] = {sl.norm[1], sl.norm[2], sl.norm[3]};
+      const double nr[3] = {-sl.norm[1], -sl.norm[2], -sl.norm[3]};
+      if (!neu && !dir) {
+        side(sl.left_sub_elem_neigh, sl.left_elem_neigh, nl, 0);
+        side(sl.right_sub_elem_neigh, sl.right_elem_neigh, nr, 0);
+      } else if (neu) {
+        side(sl.left_sub_elem_neigh, sl.left_elem_neigh, nl, 1);
+      } else {
+        side(sl.left_sub_elem_neigh, sl.left_elem_neigh, nl, 2);
+        for (int k = 0; k < 3; ++k) B[ifl0 + k] = sl.area * g_diff.valV[-re - 1][k];
+        for (int i = 0; i < 3; ++i) {
+          for (int c = 0; c < E; ++c) S[(ifl0 + i) + F * c] = 0.0;
+          for (int c = 0; c < F; ++c) N[(ifl0 + i) + F * c] = 0.0;
+          for (int j = 0; j < 3; ++j) N[(ifl0 + i) + F * (ifl0 + j)] = sl.area * (i == j ? 1.0 : 0.0);
+        }
+      }
+    }
+    std::vector<double> Ve(E), Vf(F), SB(E), SNS(E * E), T1(E * F), tmp(F), SNSVe(E), blc3(9 * ne);
+    for (int l = 0; l < ne; ++l) {
+      const double* u = sol + 5 * (m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem - 1);
+      for (int k = 0; k < 3; ++k) Ve[3 * l + k] = u[1 + k] / u[0];
+    }
+    for (int p = 0; p < ne; ++p) {
+      const double* u = sol + 5 * (m.sub_elem[V.sub_elem_neigh[p + 1]].mesh_elem - 1);
+      double Spc[3][3] = {{0}};
+      for (int l = 0; l < nf; ++l)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) Spc[i][j] = Spc[i][j] + St[(3 * p + i) + E * (3 * l + j)];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) blc3[9 * p + i + 3 * j] = Spc[j][i] / u[0];
+    }
+    blas_gemv(F, E, S.data(), Ve.data(), Vf.data());
+    for (int i = 0; i < F; ++i) Vf[i] = Vf[i] + B[i];
+    lapack_inverse(F, N.data());
+    blas_gemm(E, F, F, St.data(), N.data(), T1.data());
+    blas_gemm(E, E, F, T1.data(), S.data(), SNS.data());
+    blas_gemv(F, F, N.data(), B.data(), tmp.data());
+    blas_gemv(E, F, St.data(), tmp.data(), SB.data());
+    blas_gemv(F, F, N.data(), Vf.data(), B.data());
+    Vf = B;
+    blas_gemv(E, E, SNS.data(), Ve.data(), SNSVe.data());
+    for (int l = 0; l < ne; ++l) {
+      const int iel = m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem;
+      const double* u = sol + 5 * (iel - 1);
+      double* D = diag + 25 * (iel - 1);
+      double* r = rhs + 5 * (iel - 1);
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+          D[(1 + i) + 5 * (1 + j)] =
+              (D[(1 + i) + 5 * (1 + j)] - SNS[(3 * l + i) + E * (3 * l + j)] / u[0]) + blc3[9 * l + i + 3 * j];
+      for (int i = 0; i < 3; ++i) {
+        double mv = 0.0;
+        for (int k = 0; k < 3; ++k) mv = mv + SNS[(3 * l + i) + E * (3 * l + k)] * Ve[3 * l + k];
+        r[1 + i] = ((r[1 + i] + SNSVe[3 * l + i]) - mv) + SB[3 * l + i];
+      }
+    }
+    for (int p = 0; p < ne; ++p) {  // viscous work
+      const int isep = V.sub_elem_neigh[p + 1];
+      const SubElem& Ep = m.sub_elem[isep];
+      const int iep = Ep.mesh_elem;
+      double Spc[3][3] = {{0}};
+      for (int l = 0; l < Ep.n_sub_faces; ++l) {
+        const int isfl = Ep.sub_face[l + 1];
+        double nl[3];
+        const double a = se_sign_norm(m, isfl, isep, nl);
+        const int q = 3 * (m.sub_face[isfl].id_loc_around_node - 1);
+        double vm[3];
+        for (int k = 0; k < 3; ++k) vm[k] = Vf[q + k] - Ve[3 * p + k];
+        const double dd = vm[0] * nl[0] + vm[1] * nl[1] + vm[2] * nl[2];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            const double e = i == j ? 1.0 : 0.0;
+            Spc[i][j] = Spc[i][j] + a * ((vm[i] * nl[j] + vm[j] * nl[i]) - (2.0 / 3.0) * dd * e);
+          }
+      }
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Spc[i][j] = Spc[i][j] * mu[iep - 1] / Ep.volume;
+      for (int l = 0; l < Ep.n_sub_faces; ++l) {
+        const int isfl = Ep.sub_face[l + 1];
+        double nl[3];
+        const double a = se_sign_norm(m, isfl, isep, nl);
+        const int q = 3 * (m.sub_face[isfl].id_loc_around_node - 1);
+        double sv[3];
+        for (int i = 0; i < 3; ++i) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s = s + Spc[i][k] * Vf[q + k];
+          sv[i] = s;
+        }
+        rhs[5 * (iep - 1) + 4] = rhs[5 * (iep - 1) + 4] + a * (sv[0] * nl[0] + sv[1] * nl[1] + sv[2] * nl[2]);
+      }
+    }
+  }
+}
+
+// build_diff_mat_into_global_mat_diag (ns_diffusion_module.F90:112-184), all vertices
+static void heat_diffusion(const Mesh& m, const double* sol, const double* mu, double* diag, double* rhs) {
+  for (int v = 1; v <= m.n_vert; ++v) {
+    const Vert& V = m.vert[v];
+    const int nf = V.n_sub_faces_neigh, ne = V.n_sub_elems_neigh;
+    std::vector<double> N(nf * nf, 0.0), S(nf * ne, 0.0), St(ne * nf, 0.0), B(nf, 0.0);
+    for (int l = 0; l < nf; ++l) {  // build_diff_nodal_system (:7-110)
+      const int isfl = V.sub_face_neigh[l + 1];
+      const SubFace& sl = m.sub_face[isfl];
+      const int il = sl.id_loc_around_node - 1;
+      const Face& fl = m.face[sl.mesh_face];
+      auto side = [&](int se, int elem, const double* nl) {
+        const SubElem& E0 = m.sub_elem[se];
+        const int ie = E0.id_loc_around_node - 1;
+        const double kap = mu[elem - 1] * g_diff.Cv_p * G / kPrandtl;
+        for (int p = 0; p < E0.n_sub_faces; ++p) {
+          const int isfp = E0.sub_face[p + 1];
+          const int ip = m.sub_face[isfp].id_loc_around_node - 1;
+          double np[3];
+          const double ap = se_sign_norm(m, isfp, se, np);
+          const double b = kap * sl.area * ap * (1.0 / E0.volume) * (np[0] * nl[0] + np[1] * nl[1] + np[2] * nl[2]);
+          N[il + nf * ip] += b;
+          S[il + nf * ie] += b;
+          St[ie + ne * il] += b;
+        }
+      };
+      const double nl[3] = {sl.norm[1], sl.norm[2], sl.norm[3]};
+      const double nr[3] = {-sl.norm[1], -sl.norm[2], -sl.norm[3]};
+      side(sl.left_sub_elem_neigh, fl.left_neigh, nl);
+      if (sl.right_sub_elem_neigh > 0) {
+        side(sl.right_sub_elem_neigh, fl.right_neigh, nr);
+      } else if (fl.right_neigh < 0 && g_diff.bcT[-fl.right_neigh - 1] == 2) {
+        B[il] = sl.area * g_diff.valT[-fl.right_neigh - 1];
+        for (int c = 0; c < ne; ++c) S[il + nf * c] = 0.0;
+        for (int c = 0; c < nf; ++c) N[il + nf * c] = 0.0;
+        N[il + nf * il] = sl.area;
+      }
+    }
+    std::vector<double> SNS(ne * ne), T1(ne * nf), tmp(nf), SB(ne), theta(ne), P(5 * ne), b1(ne);
+    lapack_inverse(nf, N.data());
+    blas_gemm(ne, nf, nf, St.data(), N.data(), T1.data());
+    blas_gemm(ne, ne, nf, T1.data(), S.data(), SNS.data());
+    blas_gemv(nf, nf, N.data(), B.data(), tmp.data());
+    blas_gemv(ne, nf, St.data(), tmp.data(), SB.data());
+    for (int l = 0; l < ne; ++l) {
+      const double* u = sol + 5 * (m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem - 1);
+      theta[l] = temp_u(u);
+      const double uv[3] = {u[1] / u[0], u[2] / u[0], u[3] / u[0]};
+      const double nn = fnorm2(uv, 3);
+      P[5 * l] = (nn * nn - u[4] / u[0]) / (u[0] * g_diff.Cv_p);
+      for (int k = 1; k < 4; ++k) P[5 * l + k] = -u[k] / ((u[0] * u[0]) * g_diff.Cv_p);
+      P[5 * l + 4] = 1.0 / (u[0] * g_diff.Cv_p);
+      double s = 0.0;
+      for (int c = 0; c < nf; ++c) s = s + St[l + ne * c];
+      b1[l] = s;
+    }
+    for (int l = 0; l < ne; ++l) {
+      const int iel = m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem;
+      const double* u = sol + 5 * (iel - 1);
+      double* D = diag + 25 * (iel - 1);
+      double& r5 = rhs[5 * (iel - 1) + 4];
+      for (int p = 0; p < ne; ++p) r5 = r5 + SNS[l + ne * p] * theta[p];
+      const double snl = SNS[l + ne * l], cc = b1[l] - snl;
+      for (int k = 0; k < 5; ++k) D[4 + 5 * k] = D[4 + 5 * k] + cc * P[5 * l + k];
+      double pu = 0.0;
+      for (int k = 0; k < 5; ++k) pu = pu + P[5 * l + k] * u[k];
+      r5 = (((r5 - snl * pu) + cc * pu) - b1[l] * theta[l]) + SB[l];
+    }
+  }
+}
+
+// ns_main.F90:130-179
 static int compute_rhs_ns(const Mesh& m, const NsCfg& cfg, const double* sol, NsWork& w) {
   w.grad.assign(15 * m.n_elems, 0.0);
   w.ngrad.assign(15 * m.n_vert, 0.0);
+  w.diag.assign(25 * m.n_elems, 0.0);
   int st = compute_euler_flux(m, cfg, sol, w.rhs.data(), w.grad.data(), w.sl.data(), false, w.vp.data());
   if (cfg.second_order) {
     compute_cell_grads(m, cfg, sol, w.grad.data(), w.ngrad.data());
     st |= compute_euler_flux(m, cfg, sol, w.rhs_o2.data(), w.grad.data(), w.sl_o2.data(), true, w.vp.data());
     flux_limiting(m, sol, w.rhs.data(), w.rhs_o2.data(), w.sl.data(), cfg.cfl);
+  }
+  if (g_diff.active) {
+    std::vector<double> mu(m.n_elems);
+    double mu0c = g_diff.use_sutherland ? 1e12 : g_diff.mu_p;
+    for (int i = 0; i < m.n_elems; ++i) {
+      mu[i] = mu_of(sol + 5 * i);
+      if (g_diff.use_sutherland) mu0c = fmin2(mu0c, mu[i]);
+    }
+    momentum_diffusion(m, sol, mu.data(), mu0c, w.diag.data(), w.rhs.data());
+    heat_diffusion(m, sol, mu.data(), w.diag.data(), w.rhs.data());
   }
   return st;
 }
@@ -912,7 +1283,7 @@ static int compute_rhs_ns(const Mesh& m, const NsCfg& cfg, const double* sol, Ns
 // ns_euler_module.F90:521-609 (no diffusion blocks: diag = a1*(V/dt + sum_lambda)*I)
 static int add_timedisc_and_solve(const Mesh& m, const NsCfg& cfg, double* sol, double* rhs, double* sum_lambda,
                                   double* delta, double* res, double* res_vect, double a1, double a2, double t,
-                                  double* dt_io) {
+                                  double* dt_io, double* diag) {
   double dt = 1e10;
   for (int i = 1; i <= m.n_elems; ++i) dt = fmin2(dt, m.elem[i].volume / sum_lambda[i - 1]);
   dt = cfg.cfl * dt;
@@ -930,7 +1301,17 @@ static int add_timedisc_and_solve(const Mesh& m, const NsCfg& cfg, double* sol, 
     double s = a1 * (m.elem[i].volume / dt + sum_lambda[i - 1]);
     double nw[5], d5[5], ad[5];
     for (int k = 0; k < 5; ++k) r[k] = r[k] + s * u[k];
-    for (int k = 0; k < 5; ++k) nw[k] = r[k] / s;
+    if (g_diff.active) {  // diag + s I, then lu_solve_inplace_lapack (dgetrf + dgetrs)
+      double* D = diag + 25 * (i - 1);
+      for (int a = 0; a < 5; ++a)
+        for (int b = 0; b < 5; ++b) D[a + 5 * b] = D[a + 5 * b] + s * (a == b ? 1.0 : 0.0);
+      int ipiv[5];
+      lapack_getrf(5, D, ipiv);
+      for (int k = 0; k < 5; ++k) nw[k] = r[k];
+      lapack_getrs(5, D, ipiv, nw);
+    } else {
+      for (int k = 0; k < 5; ++k) nw[k] = r[k] / s;
+    }
     for (int k = 0; k < 5; ++k) {
       d5[k] = nw[k] - u[k];
       delta[5 * (i - 1) + k] = d5[k];
@@ -969,14 +1350,14 @@ int ns_run(const Mesh& m, const NsCfg& cfg, double* sol, int n_max_iter, double 
     if (cfg.second_order) {
       std::memcpy(soln.data(), sol, soln.size() * sizeof(double));
       st |= add_timedisc_and_solve(m, cfg, sol, w.rhs.data(), w.sl.data(), w.delta.data(), &res, res_vect, 2.0,
-                                   1.0, t, &dt);
+                                   1.0, t, &dt, w.diag.data());
       st |= compute_rhs_ns(m, cfg, sol, w);
       st |= add_timedisc_and_solve(m, cfg, soln.data(), w.rhs.data(), w.sl.data(), w.delta.data(), &res,
-                                   res_vect, 1.0, 1.0, t, &dt);
+                                   res_vect, 1.0, 1.0, t, &dt, w.diag.data());
       std::memcpy(sol, soln.data(), soln.size() * sizeof(double));
     } else {
       st |= add_timedisc_and_solve(m, cfg, sol, w.rhs.data(), w.sl.data(), w.delta.data(), &res, res_vect, 1.0,
-                                   1.0, t, &dt);
+                                   1.0, t, &dt, w.diag.data());
     }
     iter = iter + 1;
     t = t + dt;
@@ -1271,6 +1652,24 @@ long or_be_jacobian(void* h, const int* ic, const double* dc, const int* bc_type
   return (long)c.size();
 }
 void or_lu3(double* a9, double* x, const double* b) { oracle_lu3(a9, x, b); }
+// the diffusion namelist entries (activate_diffusion, use_sutherland, mu_p, mu0, T0, Cv_p
+// and per tag bc_type_V / bc_val_V(3) / bc_type_T / bc_val_T, kinds 1 neumann, 2 dirichlet)
+void or_ns_set_diffusion(int active, int use_sutherland, const double* dc4, int n_bc, const int* bcV,
+                         const double* valV, const int* bcT, const double* valT) {
+  g_diff = DiffCfg();
+  g_diff.active = active;
+  g_diff.use_sutherland = use_sutherland;
+  g_diff.mu_p = dc4[0];
+  g_diff.mu0 = dc4[1];
+  g_diff.T0 = dc4[2];
+  g_diff.Cv_p = dc4[3];
+  for (int i = 0; i < n_bc && i < 16; ++i) {
+    g_diff.bcV[i] = bcV[i];
+    g_diff.bcT[i] = bcT[i];
+    g_diff.valT[i] = valT[i];
+    for (int k = 0; k < 3; ++k) g_diff.valV[i][k] = valV[3 * i + k];
+  }
+}
 // sol_potential_flow_2d / _3d at x (primitive w)
 void or_potential_flow(const double* x, int three_d, double* w) { potential_flow(x, three_d != 0, w); }
 

@@ -1,0 +1,91 @@
+"""The oracle's restatement of the Navier-Stokes diffusion terms (activate_diffusion:
+src/ns/ns_vectorial_diffusion_module.F90 for momentum and viscous work,
+src/ns/ns_diffusion_module.F90 for heat, assembled point-implicitly into mat_diag and
+solved per cell by add_timedisc_and_solve, src/ns/ns_euler_module.F90:521-609) has no
+golden vectors; these tests check its physics: a fluid at rest at uniform temperature
+stays at rest (Neumann walls, and Dirichlet walls at the fluid's velocity and
+temperature), a moving Dirichlet wall drags the fluid along it, heat flows from a hot
+Dirichlet wall into the fluid, and diffusion changes the result of the inviscid run."""
+import numpy as np
+import pytest
+
+NX, NY = 8, 6
+
+
+def _mesh():
+    from oracle.oracle import OracleMesh
+    from subfv_b200 import meshgen
+    raw = meshgen.tag_slab_sides(meshgen.hex_slab(NX, NY, jitter=0.1, seed=3), NX, NY,
+                                 {"xlo": 1, "xhi": 2, "ylo": 3, "yhi": 4})
+    return OracleMesh(raw)
+
+
+def _cons(w):
+    return np.ascontiguousarray(np.column_stack([w[:, 0], w[:, 1:4] * w[:, :1],
+                                                 w[:, 4] / 0.4 + 0.5 * w[:, 0] * (w[:, 1:4] ** 2).sum(1)]))
+
+
+def _cfg(**kw):
+    d = dict(scheme=1, second_order=1, method=4, bc_style=2, b2d=1, exclude_bound_vert=0, local_time_step=0,
+             cfl=0.3, tmax=1e30, n_bc=4, bc_type=np.ones(4, np.int32), bc_val=np.zeros((4, 5)),
+             activate_diffusion=1, diff_dc=[0.05, 1.716e-5, 273.15, 2.5])
+    d.update(kw)
+    return d
+
+
+CV = 2.5
+
+
+@pytest.mark.parametrize("walls", ["neumann", "dirichlet"])
+def test_rest_state_is_preserved(oracle_lib, walls):
+    o = _mesh()
+    sol = _cons(np.tile([1.2, 0.0, 0.0, 0.0, 1.0], (o.n_elems, 1)))
+    T = sol[0, 4] / sol[0, 0] / CV
+    kw = {}
+    if walls == "dirichlet":
+        kw = dict(bc_type_V=np.full(4, 2, np.int32), bc_val_V=np.zeros((4, 3)),
+                  bc_type_T=np.full(4, 2, np.int32), bc_val_T=np.full(4, T))
+    s = sol.copy()
+    st, it, _, _, _, _ = o.ns_run(_cfg(**kw), s, 4)
+    assert st == 0 and it == 5
+    np.testing.assert_allclose(s, sol, rtol=0, atol=1e-14)
+
+
+def test_moving_wall_drags_fluid(oracle_lib):
+    o = _mesh()
+    sol = _cons(np.tile([1.2, 0.0, 0.0, 0.0, 1.0], (o.n_elems, 1)))
+    kw = dict(bc_type_V=np.array([1, 1, 2, 2], np.int32), bc_val_V=np.array([[0, 0, 0]] * 3 + [[0.1, 0, 0]], float))
+    s = sol.copy()
+    st, _, _, _, _, _ = o.ns_run(_cfg(**kw), s, 20)
+    assert st == 0
+    y = o.geom("elem_coord")[:, 1]
+    top, bottom = s[y > 0.3, 1].mean(), s[y < -0.3, 1].mean()
+    assert top > 10 * abs(bottom) and top > 1e-3
+
+
+def test_hot_wall_heats_fluid(oracle_lib):
+    o = _mesh()
+    sol = _cons(np.tile([1.2, 0.0, 0.0, 0.0, 1.0], (o.n_elems, 1)))
+    T = sol[0, 4] / sol[0, 0] / CV
+    kw = dict(bc_type_T=np.array([2, 1, 1, 1], np.int32), bc_val_T=np.array([1.5 * T, 0, 0, 0]))
+    s = sol.copy()
+    st, _, _, _, _, _ = o.ns_run(_cfg(**kw), s, 10)
+    assert st == 0
+    vol = o.geom("elem_volume")
+    assert np.sum(s[:, 4] * vol) > np.sum(sol[:, 4] * vol) * (1 + 1e-6)
+    x = o.geom("elem_coord")[:, 0]
+    assert s[x < -0.3, 4].mean() > s[x > 0.3, 4].mean()
+
+
+def test_diffusion_changes_the_inviscid_result(oracle_lib):
+    o = _mesh()
+    rng = np.random.default_rng(2)
+    w = np.column_stack([rng.uniform(1.1, 1.3, o.n_elems), rng.uniform(-0.1, 0.1, (o.n_elems, 2)),
+                         np.zeros(o.n_elems), rng.uniform(0.9, 1.1, o.n_elems)])
+    sol = _cons(w)
+    a, b, c = sol.copy(), sol.copy(), sol.copy()
+    assert o.ns_run(_cfg(), a, 3)[0] == 0
+    assert o.ns_run(_cfg(activate_diffusion=0), b, 3)[0] == 0
+    assert o.ns_run(_cfg(use_sutherland=1, diff_dc=[0.05, 0.05, 0.4, CV]), c, 3)[0] == 0
+    assert np.isfinite(a).all() and np.isfinite(c).all()
+    assert np.abs(a - b).max() > 1e-4 and np.abs(c - a).max() > 1e-6
