@@ -187,6 +187,16 @@ typedef struct subfv_ns_cfg {
   int32_t precision;          /* 0 plain FP64; 1 FP32 wave-speed bounds of the nodal solver;
                                  2 also FP32 flux, reconstruction and limiter arithmetic
                                  (nodal 3x3 systems and all sums FP64 in both) */
+  /* Navier-Stokes diffusion (namelist entries of ns_global_data_module.F90:10-46, 111):
+     momentum and heat assembled point-implicitly into the cells' 5x5 blocks, always FP64.
+     Explicit time loop and residual entry point only, on meshes without periodic faces. */
+  int32_t activate_diffusion;
+  int32_t use_sutherland;     /* mu from Sutherland's law (mu0, T0, C0 = 110.4), else mu_p */
+  double mu_p, mu0, T0, Cv_p; /* reference defaults 1.329e-5, 1.716e-5, 273.15, 720.19471 */
+  int32_t bc_type_V[16];      /* per tag: 0 or 1 neumann, 2 dirichlet (velocity bc_val_V) */
+  double bc_val_V[16][3];
+  int32_t bc_type_T[16];      /* per tag: 0 or 1 neumann, 2 dirichlet (temperature bc_val_T) */
+  double bc_val_T[16];
 } subfv_ns_cfg;
 
 /* compute_rhs_ns (ns_main.F90:130-179, no diffusion): one residual evaluation.
@@ -196,6 +206,10 @@ int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* s
                          double* sum_lambda, double* vp, double* cell_grad);
 
 typedef struct subfv_ns_state subfv_ns_state;
+/* compute_rhs_ns with the diffusion blocks: mat_diag (5, 5, n_elems), column-major per
+   cell, as ns_main.F90:130-179 leaves it for add_timedisc_and_solve (may be NULL) */
+int subfv_compute_rhs_ns_ex(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs,
+                            double* sum_lambda, double* vp, double* cell_grad, double* mat_diag);
 int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double t0,
                           subfv_ns_state** out);
 int subfv_ns_state_destroy(subfv_ns_state* s);

@@ -54,6 +54,7 @@ def load():
         lib.or_fnorm2.restype = C.c_double
         lib.or_fnorm2.argtypes = [PD, C.c_int]
         lib.or_ns_rhs.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, PD, PD, PD, PD]
+        lib.or_ns_rhs_diag.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, PD, PD, PD]
         lib.or_ns_run.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_int, C.c_double, PD, PI, PD, PD, PD]
         lib.or_ns_gresho.argtypes = [C.c_void_p, C.c_double, PD]
         lib.or_pinv3.argtypes = [PD]
@@ -239,6 +240,17 @@ class OracleMesh:
         st = load().or_ns_rhs(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), _pd(rhs), _pd(sl), _pd(vp),
                               _pd(grad))
         return st, rhs, sl, vp, grad
+
+    def ns_rhs_diag(self, cfg, sol):
+        """compute_rhs_ns with the diffusion blocks: (status, rhs, sum_lambda, mat_diag (n, 5, 5))."""
+        ic, dc, bt, bv = self._ns_args(cfg)
+        sol = np.ascontiguousarray(sol, np.float64)
+        rhs = np.zeros((self.n_elems, 5))
+        sl = np.zeros(self.n_elems)
+        diag = np.zeros((self.n_elems, 5, 5))
+        st = load().or_ns_rhs_diag(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), _pd(rhs), _pd(sl),
+                                   _pd(diag))
+        return st, rhs, sl, diag
 
     def ns_run(self, cfg, sol, n_max_iter, final_res=-1.0, t0=0.0):
         """The ns_main time loop in place on sol (n_max_iter + 1 steps unless stopped)."""

@@ -909,7 +909,7 @@ struct NsWork {
 struct DiffCfg {
   int active = 0, use_sutherland = 0;
   double mu_p = 1.329e-5, mu0 = 1.716e-5, T0 = 273.15, Cv_p = 720.19471;
-  int bcV[16] = {0}, bcT[16] = {0};  // 1 neumann, 2 dirichlet
+  int bcV[16] = {0}, bcT[16] = {0};  // 0 or 1 neumann, 2 dirichlet
   double valV[16][3] = {{0}}, valT[16] = {0};
 };
 static DiffCfg g_diff;
@@ -1060,9 +1060,9 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
       const int ifl0 = 3 * (sl.id_loc_around_node - 1);
       const int re = sl.right_elem_neigh;
       bool neu = false, dir = false;
-      if (re < 0) {
+      if (re < 0) {  // bc_V_id: "" and "neumann" are Neumann (ns_global_data_module.F90:229-236)
         dir = g_diff.bcV[-re - 1] == 2;
-        neu = g_diff.bcV[-re - 1] == 1;
+        neu = !dir;
       } else if (re == 0) {
         neu = true;
       }
@@ -1373,7 +1373,7 @@ int ns_run(const Mesh& m, const NsCfg& cfg, double* sol, int n_max_iter, double 
 
 // One compute_rhs_ns evaluation (rhs after flux limiting, first-order sum_lambda).
 int ns_rhs(const Mesh& m, const NsCfg& cfg, const double* sol, double* rhs, double* sum_lambda, double* vp,
-           double* cell_grad) {
+           double* cell_grad, double* mat_diag = nullptr) {
   NsWork w;
   w.rhs.assign(5 * m.n_elems, 0.0);
   w.rhs_o2.assign(5 * m.n_elems, 0.0);
@@ -1386,6 +1386,7 @@ int ns_rhs(const Mesh& m, const NsCfg& cfg, const double* sol, double* rhs, doub
   std::memcpy(sum_lambda, w.sl.data(), w.sl.size() * sizeof(double));
   if (vp) std::memcpy(vp, w.vp.data(), w.vp.size() * sizeof(double));
   if (cell_grad) std::memcpy(cell_grad, w.grad.data(), w.grad.size() * sizeof(double));
+  if (mat_diag) std::memcpy(mat_diag, w.diag.data(), w.diag.size() * sizeof(double));
   return st;
 }
 
@@ -1620,6 +1621,11 @@ static NsCfg make_cfg(const int* ic, const double* dc, const int* bc_type, const
 int or_ns_rhs(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val,
               const double* sol, double* rhs, double* sum_lambda, double* vp, double* grad) {
   return ns_rhs(handle_mesh(h), make_cfg(ic, dc, bc_type, bc_val), sol, rhs, sum_lambda, vp, grad);
+}
+// compute_rhs_ns with mat_diag (5, 5, n) column-major per cell
+int or_ns_rhs_diag(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val,
+                   const double* sol, double* rhs, double* sum_lambda, double* mat_diag) {
+  return ns_rhs(handle_mesh(h), make_cfg(ic, dc, bc_type, bc_val), sol, rhs, sum_lambda, nullptr, nullptr, mat_diag);
 }
 int or_ns_run(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val, double* sol,
               int n_max_iter, double final_res, double* t_io, int* iters, double* res, double* res_vect, double* vp) {

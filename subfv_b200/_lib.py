@@ -58,6 +58,7 @@ SIGNATURES = {
     "subfv_lag_step_host": (c_int, [P, PD]),
     "subfv_lag_profile_steps": (c_int, [P, c_int, PD]),
     "subfv_compute_rhs_ns": (c_int, [P, P, PD, PD, PD, PD, PD]),
+    "subfv_compute_rhs_ns_ex": (c_int, [P, P, PD, PD, PD, PD, PD, PD]),
     "subfv_ns_state_create": (c_int, [P, P, PD, c_dbl, C.POINTER(P)]),
     "subfv_ns_state_destroy": (c_int, [P]),
     "subfv_ns_state_set_node_kernel": (c_int, [P, c_int]),

@@ -30,6 +30,7 @@
 #include <cstring>
 
 #include "ns.cuh"
+#include "ns_diffusion.cuh"
 
 namespace subfv {
 
@@ -51,6 +52,8 @@ NsParams ns_params_from(const subfv_ns_cfg& c) {
   p.tmax = c.tmax;
   p.precision = c.precision;
   p.node_group = 0;
+  p.diff = c.activate_diffusion;
+  p.diff_kd = 0;
   return p;
 }
 
@@ -1430,10 +1433,27 @@ constexpr int kTdBlock = 128;
 // (atomic on the bit pattern) and per-block residual partial sums (res, res_vect(5)).
 // called by every thread of a kTdBlock-thread block; blk is the block's index within
 // its problem (it selects the slot of the residual partial sums)
+// With diffusion the cell's terms go onto the limited residual and into its 5x5 block,
+// and the cell solves (block + s I) x = rhs + s U by LU (out of line: rare).
+__device__ __noinline__ void diffusion_cell_solve(const DevMesh& m, int c, const double* __restrict__ dterm, int kd,
+                                                  double* r, double* rv, const double* u, double s, double* d5) {
+  double D[25];
+  for (int k = 0; k < 25; ++k) D[k] = 0.0;
+  apply_diffusion_terms(m, c, dterm, kd, r, D);
+  for (int k = 0; k < 5; ++k) rv[k] = r[k] * r[k];
+  for (int a = 0; a < 5; ++a)
+    for (int b = 0; b < 5; ++b) D[a + 5 * b] = D[a + 5 * b] + s * (a == b ? 1.0 : 0.0);
+  double x[5];
+  for (int k = 0; k < 5; ++k) x[k] = r[k] + s * u[k];
+  lu_solve5(D, x);
+  for (int k = 0; k < 5; ++k) d5[k] = x[k] - u[k];
+}
+
 __device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U_rhs,
                                  const double* __restrict__ rhs1, const double* __restrict__ rhs2,
                                  const double* __restrict__ U_td, double* __restrict__ delta,
-                                 double* __restrict__ partial, NsScalars* sc, double a1, double a2, const int blk) {
+                                 double* __restrict__ partial, NsScalars* sc, double a1, double a2, const int blk,
+                                 const double* __restrict__ dterm = nullptr) {
   if (sc->done) return;
   const int c = blk * kTdBlock + threadIdx.x;
   const double dt_fl = P.cfl * sc->dtred;
@@ -1457,14 +1477,19 @@ __device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const doub
       const double w = fmin2(1.0, max_omega_for_positivity(Ub, dU));
       for (int k = 0; k < 5; ++k) r[k] = r[k] + w * (r2[k] - r[k]);
     }
-    for (int k = 0; k < 5; ++k) rv[k] = r[k] * r[k];
     double u[5], d5[5], ad[5];
     ld5(U_td, c, u);
     const double s = a1 * (V / dt + 0.0);  // sum_lambda is zeroed once dt is known
-    for (int k = 0; k < 5; ++k) {
-      const double rr = r[k] + s * u[k];
-      d5[k] = rr / s - u[k];
-      ad[k] = a2 * d5[k];
+    if (dterm) {
+      diffusion_cell_solve(m, c, dterm, P.diff_kd, r, rv, u, s, d5);
+      for (int k = 0; k < 5; ++k) ad[k] = a2 * d5[k];
+    } else {
+      for (int k = 0; k < 5; ++k) rv[k] = r[k] * r[k];
+      for (int k = 0; k < 5; ++k) {
+        const double rr = r[k] + s * u[k];
+        d5[k] = rr / s - u[k];
+        ad[k] = a2 * d5[k];
+      }
     }
     om = max_omega_for_positivity(u, ad);
     {  // norm2(delta): gfortran's scaled sum of squares
@@ -1514,8 +1539,9 @@ __global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P,
                                                           const double* __restrict__ rhs2,
                                                           const double* __restrict__ U_td,
                                                           double* __restrict__ delta, double* __restrict__ partial,
-                                                          NsScalars* sc, double a1, double a2) {
-  ns_timedisc_body(m, P, U_rhs, rhs1, rhs2, U_td, delta, partial, sc, a1, a2, blockIdx.x);
+                                                          NsScalars* sc, double a1, double a2,
+                                                          const double* __restrict__ dterm) {
+  ns_timedisc_body(m, P, U_rhs, rhs1, rhs2, U_td, delta, partial, sc, a1, a2, blockIdx.x, dterm);
 }
 
 // scalar tail of add_timedisc_and_solve (:582-608); last_stage also advances t
@@ -2136,10 +2162,10 @@ void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double*
 
 void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs, const double* rhs1,
                         const double* rhs2, const double* U_td, double* U_out, double* delta, double* partial,
-                        NsScalars* sc, double a1, double a2, int last_stage) {
+                        NsScalars* sc, double a1, double a2, int last_stage, const double* dterm) {
   const int nb = ns_partial_blocks(m);
   k_ns_timedisc<<<nb, kTdBlock, 0, m.stream>>>(m, P, U_rhs, rhs1, P.second_order ? rhs2 : nullptr, U_td, delta,
-                                               partial, sc, a1, a2);
+                                               partial, sc, a1, a2, P.diff ? dterm : nullptr);
   k_ns_finalize<<<1, 1, 0, m.stream>>>(sc, P, partial, nb, m.status, last_stage);
   k_ns_apply<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, U_td, delta, U_out, sc, a2);
   k_ns_reset_omega<<<1, 1, 0, m.stream>>>(sc);

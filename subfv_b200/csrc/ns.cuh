@@ -16,6 +16,7 @@ struct NsParams {
   double cfl, tmax;
   int precision;
   int node_group;  // 0: one thread per vertex; else a group of lanes per vertex, at least node_group
+  int diff, diff_kd;  // diffusion terms to apply in the time discretisation, doubles per corner record
 };
 
 struct NsScalars {
@@ -66,9 +67,10 @@ NsParams ns_params_from(const subfv_ns_cfg& c);
 void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double* fs, double* rhs1, double* rhs2,
                    double* ngrad, double* grad, NsScalars* sc);
 // flux limiting + add_timedisc_and_solve + update (stage coefficients a1, a2)
+// (dterm: the diffusion corner records when P.diff, else null)
 void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs, const double* rhs1,
                         const double* rhs2, const double* U_td, double* U_out, double* delta, double* partial,
-                        NsScalars* sc, double a1, double a2, int last_stage);
+                        NsScalars* sc, double a1, double a2, int last_stage, const double* dterm = nullptr);
 void launch_ns_pack(const DevMesh& m, const double* s5, double* U);
 void launch_ns_flux_limiting(const DevMesh& m, const NsParams& P, const double* U, double* rhs1, const double* rhs2,
                              const NsScalars* sc);

@@ -214,10 +214,16 @@ extern "C" {
 int subfv_ns_batch_create(const subfv_ns_cfg* cfg, int capacity, int64_t budget_bytes, subfv_ns_batch** out) {
   if (!cfg || !out || capacity < 1 || capacity > (1 << 20) || budget_bytes <= 0 ||
       (cfg->scheme < 1 || cfg->scheme > 8 || cfg->scheme == 7) || (cfg->method < 0 || cfg->method > 6) ||
-      cfg->local_time_step != 0 || cfg->n_bc < 0 || cfg->n_bc > 16 || (cfg->precision < 0 || cfg->precision > 2)) {
-    set_error("subfv_ns_batch_create: bad argument or unsupported configuration");
+      cfg->local_time_step != 0 || cfg->n_bc < 0 || cfg->n_bc > 16 || (cfg->precision < 0 || cfg->precision > 2) ||
+      cfg->activate_diffusion) {
+    set_error("subfv_ns_batch_create: bad argument or unsupported configuration (diffusion is not batched)");
     return -2;
   }
+  for (int i = 0; i < cfg->n_bc; ++i)
+    if (cfg->bc_type[i] < 1 || cfg->bc_type[i] > 9) {
+      set_error("subfv_ns_batch_create: boundary kind not recognized (1-9)");
+      return -2;
+    }
   auto* b = new subfv_ns_batch();
   b->P = ns_params_from(*cfg);
   b->cap = capacity;

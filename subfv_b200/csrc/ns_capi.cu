@@ -8,6 +8,7 @@
 #include "bcsr.cuh"
 #include "handles.cuh"
 #include "ns.cuh"
+#include "ns_diffusion.cuh"
 
 using namespace subfv;
 
@@ -31,6 +32,8 @@ struct subfv_ns_state {
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   ImplicitCtx* imp = nullptr;
+  DiffParams D{};                                // diffusion parameters (P.diff)
+  double *dterm = nullptr, *mu0c = nullptr;      // corner records, mu0corr
 };
 
 namespace {
@@ -47,6 +50,17 @@ int check_cfg(const subfv_ns_cfg* c) {
       set_error("subfv_ns: boundary kind not recognized (1-9)");
       return -2;
     }
+  if (c->activate_diffusion) {  // bc_type_V / bc_type_T: "" or neumann, dirichlet
+    for (int i = 0; i < c->n_bc; ++i)
+      if (c->bc_type_V[i] < 0 || c->bc_type_V[i] > 2 || c->bc_type_T[i] < 0 || c->bc_type_T[i] > 2) {
+        set_error("subfv_ns: diffusion boundary kind not recognized (0/1 neumann, 2 dirichlet)");
+        return -2;
+      }
+    if (!(c->Cv_p > 0.0) || !(c->mu_p >= 0.0) || (c->use_sutherland && !(c->mu0 > 0.0 && c->T0 > 0.0))) {
+      set_error("subfv_ns: diffusion parameters out of range");
+      return -2;
+    }
+  }
   return 0;
 }
 
@@ -63,14 +77,21 @@ int dalloc(T** p, size_t n, cudaStream_t s) {
 void enqueue_ns_step(subfv_ns_state* s) {
   const DevMesh& d = s->m->d;
   const NsParams& P = s->P;
+  auto rhs = [&](const double* U) {
+    launch_ns_rhs(d, P, U, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->sc);
+    if (P.diff) launch_ns_diffusion(d, s->D, U, s->dterm, s->mu0c);
+  };
   if (P.second_order) {
-    launch_ns_rhs(d, P, s->U0, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->sc);
-    launch_ns_timedisc(d, P, s->U0, s->rhs1, s->rhs2, s->U0, s->U1, s->delta, s->partial, s->sc, 2.0, 1.0, 0);
-    launch_ns_rhs(d, P, s->U1, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->sc);
-    launch_ns_timedisc(d, P, s->U1, s->rhs1, s->rhs2, s->U0, s->U0, s->delta, s->partial, s->sc, 1.0, 1.0, 1);
+    rhs(s->U0);
+    launch_ns_timedisc(d, P, s->U0, s->rhs1, s->rhs2, s->U0, s->U1, s->delta, s->partial, s->sc, 2.0, 1.0, 0,
+                       s->dterm);
+    rhs(s->U1);
+    launch_ns_timedisc(d, P, s->U1, s->rhs1, s->rhs2, s->U0, s->U0, s->delta, s->partial, s->sc, 1.0, 1.0, 1,
+                       s->dterm);
   } else {
-    launch_ns_rhs(d, P, s->U0, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->sc);
-    launch_ns_timedisc(d, P, s->U0, s->rhs1, nullptr, s->U0, s->U0, s->delta, s->partial, s->sc, 1.0, 1.0, 1);
+    rhs(s->U0);
+    launch_ns_timedisc(d, P, s->U0, s->rhs1, nullptr, s->U0, s->U0, s->delta, s->partial, s->sc, 1.0, 1.0, 1,
+                       s->dterm);
   }
 }
 
@@ -168,6 +189,23 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
     subfv_ns_state_destroy(s);
     return -1;
   }
+  if (s->P.diff) {
+    // the reference's diffusion indexes the periodic extension of a vertex's lists by the
+    // subfaces' original local ids, which collide; only meshes without periodic faces
+    const size_t smem = diffusion_smem_bytes(d);
+    if (!d.vsf_identity || smem > 200 * 1024) {
+      set_error(!d.vsf_identity ? "subfv_ns: diffusion on a mesh with periodic faces is not supported"
+                                : "subfv_ns: a vertex's diffusion system exceeds shared memory");
+      subfv_ns_state_destroy(s);
+      return -2;
+    }
+    s->D = diff_params_from(*cfg, d);
+    s->P.diff_kd = s->D.kd;
+    if (diffusion_prepare(smem) || dalloc(&s->dterm, (size_t)s->D.kd * nse, q) || dalloc(&s->mu0c, 1, q)) {
+      subfv_ns_state_destroy(s);
+      return -1;
+    }
+  }
   NsScalars h{};
   h.dtred = 1e10;
   h.omega = 1.0;
@@ -217,6 +255,8 @@ int subfv_ns_state_destroy(subfv_ns_state* s) {
   double* bufs[] = {s->U0, s->U1, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->delta, s->partial, s->stage};
   for (double* b : bufs) cudaFree(b);
   cudaFree(s->sc);
+  cudaFree(s->dterm);
+  cudaFree(s->mu0c);
   delete s;
   return 0;
 }
@@ -447,8 +487,8 @@ int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, d
 
 int subfv_ns_implicit_step_ex(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
                               int precond, subfv_implicit_stats* out) {
-  if (!s || krylov < 1 || krylov > 200 || !(rel_tol > 0.0) || (precond != 1 && precond != 2)) {
-    set_error("subfv_ns_implicit_step: bad argument");
+  if (!s || krylov < 1 || krylov > 200 || !(rel_tol > 0.0) || (precond != 1 && precond != 2) || s->P.diff) {
+    set_error("subfv_ns_implicit_step: bad argument (the backward-Euler step has no diffusion blocks)");
     return -2;
   }
   DevMesh& d = s->m->d;
@@ -506,6 +546,10 @@ int subfv_ns_implicit_step_ex(subfv_ns_state* s, double cfl_implicit, int krylov
 }
 
 int subfv_ns_be_jacobian(subfv_ns_state* s, double dt, int32_t* row, int32_t* col, double* v, int64_t cap) {
+  if (s && s->P.diff) {
+    set_error("subfv_ns_be_jacobian: the backward-Euler Jacobian has no diffusion blocks");
+    return -2;
+  }
   if (implicit_setup(s, 4)) return -1;
   ImplicitCtx* c = s->imp;
   if ((int64_t)c->col1.size() > cap) {
@@ -524,6 +568,11 @@ int subfv_ns_be_jacobian(subfv_ns_state* s, double dt, int32_t* row, int32_t* co
 
 int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs, double* sum_lambda,
                          double* vp, double* cell_grad) {
+  return subfv_compute_rhs_ns_ex(m, cfg, sol, rhs, sum_lambda, vp, cell_grad, nullptr);
+}
+
+int subfv_compute_rhs_ns_ex(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs,
+                            double* sum_lambda, double* vp, double* cell_grad, double* mat_diag) {
   if (!m || !sol || !rhs || !sum_lambda || check_cfg(cfg)) return -2;
   subfv_ns_state* s = nullptr;
   int rc = subfv_ns_state_create(m, cfg, sol, 0.0, &s);
@@ -546,6 +595,15 @@ int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* s
     }
     launch_ns_rhs(d, s->P, s->U0, s->fs, s->rhs1, s->rhs2, s->ngrad, s->grad, s->sc);
     if (s->P.second_order) launch_ns_flux_limiting(d, s->P, s->U0, s->rhs1, s->rhs2, s->sc);
+    double* ddiag = nullptr;
+    if (s->P.diff) {
+      launch_ns_diffusion(d, s->D, s->U0, s->dterm, s->mu0c);
+      if (mat_diag && cudaMallocAsync(&ddiag, 25 * sizeof(double) * d.ne, d.stream) != cudaSuccess) {
+        st = -1;
+        break;
+      }
+      launch_ns_diffusion_apply(d, s->dterm, s->D.kd, s->rhs1, ddiag);
+    }
     std::vector<double> r(kRhs * (size_t)d.ne);
     if (cudaMemcpyAsync(r.data(), s->rhs1, r.size() * sizeof(double), cudaMemcpyDeviceToHost, d.stream) !=
         cudaSuccess) {
@@ -556,6 +614,11 @@ int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* s
     if (cell_grad) cudaMemcpyAsync(g.data(), s->grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, d.stream);
     std::vector<double4> vph(vp ? d.nv : 0);
     if (vp) cudaMemcpyAsync(vph.data(), d.vp, vph.size() * sizeof(double4), cudaMemcpyDeviceToHost, d.stream);
+    if (mat_diag) {  // mat_diag(5, 5, n): the diffusion blocks (zero without diffusion)
+      if (ddiag) cudaMemcpyAsync(mat_diag, ddiag, 25 * sizeof(double) * d.ne, cudaMemcpyDeviceToHost, d.stream);
+      else std::memset(mat_diag, 0, 25 * sizeof(double) * d.ne);
+    }
+    if (ddiag) cudaFreeAsync(ddiag, d.stream);
     st = handle_check_status(d);
     for (int c = 0; c < d.ne; ++c) {
       for (int k = 0; k < 5; ++k) rhs[5 * (size_t)c + k] = r[kRhs * (size_t)c + k];

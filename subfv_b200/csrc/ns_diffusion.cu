@@ -1,0 +1,527 @@
+// Navier-Stokes diffusion kernels: the per-vertex momentum and heat systems of
+// src/ns/ns_vectorial_diffusion_module.F90:7-318 and src/ns/ns_diffusion_module.F90:7-184,
+// a warp per vertex with the vertex's matrices in shared memory. Every output element of
+// a matrix product, solve or inverse is produced by one lane in the order the reference
+// (netlib LAPACK / BLAS) accumulates it, so the results are those of the serial code.
+#include <algorithm>
+
+#include "ns.cuh"
+#include "ns_diffusion.cuh"
+
+namespace subfv {
+
+namespace {
+
+constexpr double kGamma = 1.4, kPrandtl = 0.71, kC0 = 110.4;  // ns_global_data_module.F90:9,10,20
+
+__device__ inline double temp_u(const double* u, double cv) {  // ns_euler_primitives_module.F90:52-63
+  const double tau = 1.0 / u[0];
+  const double uu = u[1] * u[1] + u[2] * u[2] + u[3] * u[3];
+  return (u[4] * tau - 0.5 * uu * (tau * tau)) / cv;
+}
+__device__ inline double mu_of(const DiffParams& D, const double* u) {  // compute_mu / mu_sutherland
+  if (!D.sutherland) return D.mu_p;
+  const double T = temp_u(u, D.Cv_p);
+  return D.mu0 * pow(T / D.T0, 1.5) * (D.T0 + kC0) / (T + kC0);
+}
+__device__ inline void load_u(const double* U, int c, double* u) {
+  const double* p = U + kRec * (size_t)c;
+  for (int k = 0; k < 5; ++k) u[k] = p[k];
+}
+__device__ inline double scaled_norm3(double a0, double a1, double a2) {  // gfortran NORM2
+  const double a[3] = {a0, a1, a2};
+  double scale = 1.0, res = 0.0;
+  for (int i = 0; i < 3; ++i)
+    if (a[i] != 0.0) {
+      const double ax = fabs(a[i]);
+      if (ax > scale) {
+        const double q = scale / ax;
+        res = 1.0 + res * q * q;
+        scale = ax;
+      } else {
+        const double q = ax / scale;
+        res += q * q;
+      }
+    }
+  return scale * sqrt(res);
+}
+
+// the subface's normal oriented out of sub-cell se, and its area
+__device__ inline double oriented(const DevMesh& m, int sf, int se, double* n) {
+  const double4 s = m.sfn[sf];
+  const double sg = m.sf_se[sf].x == se ? 1.0 : -1.0;
+  n[0] = sg == 1.0 ? s.x : -s.x;
+  n[1] = sg == 1.0 ? s.y : -s.y;
+  n[2] = sg == 1.0 ? s.z : -s.z;
+  return s.w;
+}
+__device__ inline int n_sub_faces(const int4 q) { return (q.x >= 0) + (q.y >= 0) + (q.z >= 0) + (q.w >= 0); }
+__device__ inline int sf_of(const int4 q, int p) { return p == 0 ? q.x : p == 1 ? q.y : p == 2 ? q.z : q.w; }
+
+// Warp-parallel dgetrf + dgetri of the n x n column-major matrix a (inv_lapack,
+// linear_solver_module.F90:629-641).
+__device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane) {
+  for (int j = 0; j < n; ++j) {
+    double big = -1.0;
+    int bi = n;
+    for (int i = j + lane; i < n; i += 32) {
+      const double x = fabs(a[i + n * j]);
+      if (x > big) {
+        big = x;
+        bi = i;
+      }
+    }
+    for (int o = 16; o > 0; o >>= 1) {  // largest |x|, the first index among equals
+      const double ob = __shfl_xor_sync(0xffffffffu, big, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > big || (ob == big && oi < bi)) {
+        big = ob;
+        bi = oi;
+      }
+    }
+    const int p = bi < n ? bi : j;
+    if (lane == 0) ipiv[j] = p;
+    const bool nz = a[p + n * j] != 0.0;
+    __syncwarp();
+    if (nz) {
+      if (p != j)
+        for (int k = lane; k < n; k += 32) {
+          const double t = a[j + n * k];
+          a[j + n * k] = a[p + n * k];
+          a[p + n * k] = t;
+        }
+      __syncwarp();
+      const double piv = a[j + n * j];
+      if (fabs(piv) >= 2.2250738585072014e-308) {
+        const double r = 1.0 / piv;
+        for (int i = j + 1 + lane; i < n; i += 32) a[i + n * j] = r * a[i + n * j];
+      } else {
+        for (int i = j + 1 + lane; i < n; i += 32) a[i + n * j] = a[i + n * j] / piv;
+      }
+    }
+    __syncwarp();
+    const int w = n - j - 1;
+    for (int e = lane; e < w * w; e += 32) {
+      const int i = j + 1 + e % w, k = j + 1 + e / w;
+      a[i + n * k] = a[i + n * k] - a[i + n * j] * a[j + n * k];
+    }
+    __syncwarp();
+  }
+  // dtrti2 ('Upper', 'Non-unit')
+  for (int j = 0; j < n; ++j) {
+    if (lane == 0) a[j + n * j] = 1.0 / a[j + n * j];
+    __syncwarp();
+    const double ajj = -a[j + n * j];
+    double* x = a + n * j;
+    for (int jj = 0; jj < j; ++jj) {  // dtrmv on x(0:j-1)
+      const double temp = x[jj];
+      __syncwarp();
+      if (temp != 0.0) {
+        for (int i = lane; i < jj; i += 32) x[i] = x[i] + temp * a[i + n * jj];
+        if (lane == 0) x[jj] = x[jj] * a[jj + n * jj];
+      }
+      __syncwarp();
+    }
+    for (int i = lane; i < j; i += 32) x[i] = ajj * x[i];
+    __syncwarp();
+  }
+  // inv(A) L = inv(U), column by column from the last (the unblocked dgetri sweep)
+  for (int j = n - 1; j >= 0; --j) {
+    for (int i = j + 1 + lane; i < n; i += 32) {
+      work[i] = a[i + n * j];
+      a[i + n * j] = 0.0;
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+      double acc = a[i + n * j];
+      for (int jj = j + 1; jj < n; ++jj) acc = acc + (-work[jj]) * a[i + n * jj];
+      a[i + n * j] = acc;
+    }
+    __syncwarp();
+  }
+  for (int i = lane; i < n; i += 32)
+    for (int j = n - 2; j >= 0; --j) {
+      const int p = ipiv[j];
+      if (p != j) {
+        const double t = a[i + n * j];
+        a[i + n * j] = a[i + n * p];
+        a[i + n * p] = t;
+      }
+    }
+  __syncwarp();
+}
+
+// C(m x p) = A(m x k) B(k x p), netlib dgemm order
+__device__ inline void warp_gemm(int m, int p, int k, const double* A, const double* B, double* C, int lane) {
+  for (int e = lane; e < m * p; e += 32) {
+    const int i = e % m, j = e / m;
+    double s = 0.0;
+    for (int l = 0; l < k; ++l) s = s + B[l + k * j] * A[i + m * l];
+    C[i + m * j] = s;
+  }
+  __syncwarp();
+}
+// y(m) = A(m x n) x, netlib dgemv order
+__device__ inline void warp_gemv(int m, int n, const double* A, const double* x, double* y, int lane) {
+  for (int i = lane; i < m; i += 32) {
+    double s = 0.0;
+    for (int j = 0; j < n; ++j) s = s + x[j] * A[i + m * j];
+    y[i] = s;
+  }
+  __syncwarp();
+}
+
+struct DiffSmem {  // offsets (doubles) of one vertex's work arrays, for the mesh's largest vertex
+  int N, S, St, T1, SNS, B, Vf, tmp, work, Ve, SB, SNSVe, blc3, theta, P, b1, ipiv, total;
+};
+__host__ __device__ inline DiffSmem diff_layout(int max_vsf, int max_vse) {
+  const int F = 3 * max_vsf, E = 3 * max_vse;
+  DiffSmem L{};
+  int o = 0;
+  L.N = o, o += F * F;
+  L.S = o, o += F * E;
+  L.St = o, o += E * F;
+  L.T1 = o, o += E * F;
+  L.SNS = o, o += E * E;
+  L.B = o, o += F;
+  L.Vf = o, o += F;
+  L.tmp = o, o += F;
+  L.work = o, o += F;
+  L.Ve = o, o += E;
+  L.SB = o, o += E;
+  L.SNSVe = o, o += E;
+  L.blc3 = o, o += 3 * E;
+  L.theta = o, o += E;
+  L.P = o, o += 5 * E;
+  L.b1 = o, o += E;
+  L.ipiv = o, o += F;  // ints stored in double slots
+  L.total = o;
+  return L;
+}
+
+__global__ void k_diff_mu0c(DevMesh m, DiffParams D, const double* __restrict__ U, double* mu0c, int init) {
+  if (init) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) *mu0c = D.sutherland ? 1e12 : D.mu_p;
+    return;
+  }
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne || !D.sutherland) return;
+  double u[5];
+  load_u(U, c, u);
+  atomic_min_pos(mu0c, mu_of(D, u));
+}
+
+// The momentum blc_3 (ns_vectorial_diffusion_module.F90:85-91) and the Neumann face's
+// N / S block (:149-152), row-major b[i][j]
+__device__ inline void mom_block(double al, double ap, double vol, double mu, double mu0c, const double* nl,
+                                 const double* np, double b[3][3]) {
+  const double s = al * ap * (1.0 / vol);
+  const double d = nl[0] * np[0] + nl[1] * np[1] + nl[2] * np[2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double e = i == j ? 1.0 : 0.0;
+      const double tp = np[i] * nl[j], tpt = np[j] * nl[i];
+      b[i][j] = s * ((mu * d * e + (mu - mu0c) * tp) + (mu0c - (2.0 / 3.0) * mu) * tpt);
+    }
+}
+__device__ inline void neumann_block(double al, double ap, double vol, const double* nl, const double* np,
+                                     double b[3][3]) {
+  const double s = al * ap * (1.0 / vol);
+  const double d = nl[0] * np[0] + nl[1] * np[1] + nl[2] * np[2];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double e = i == j ? 1.0 : 0.0;
+      b[i][j] = s * (d * e + (np[j] * nl[i]) / 3.0);
+    }
+}
+
+__global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, const double* __restrict__ U,
+                                                     double* __restrict__ dterm, const double* __restrict__ mu0c_p) {
+  extern __shared__ double sm[];
+  const DiffSmem L = diff_layout(m.max_vsf, m.max_vse);
+  const int lane = threadIdx.x;
+  double *N = sm + L.N, *S = sm + L.S, *St = sm + L.St, *T1 = sm + L.T1, *SNS = sm + L.SNS, *B = sm + L.B;
+  double *Vf = sm + L.Vf, *tmp = sm + L.tmp, *work = sm + L.work, *Ve = sm + L.Ve, *SB = sm + L.SB;
+  double *SNSVe = sm + L.SNSVe, *blc3 = sm + L.blc3, *theta = sm + L.theta, *P = sm + L.P, *b1 = sm + L.b1;
+  int* ipiv = reinterpret_cast<int*>(sm + L.ipiv);
+  const double mu0c = *mu0c_p;
+  for (int v = blockIdx.x; v < m.nv; v += gridDim.x) {
+    const int f0 = m.vsf_off[v], nf = m.vsf_off[v + 1] - f0;
+    const int s0 = m.vse_off[v], ne = m.vse_off[v + 1] - s0;
+    const int F = 3 * nf, E = 3 * ne;
+    // ---- momentum: build_momentum_diff_nodal_system (:7-193)
+    for (int e = lane; e < F * F; e += 32) N[e] = 0.0;
+    for (int e = lane; e < F * E; e += 32) S[e] = St[e] = 0.0;
+    for (int e = lane; e < F; e += 32) B[e] = 0.0;
+    __syncwarp();
+    for (int l = lane; l < nf; l += 32) {  // lane l owns row block l of N and S, column block l of St
+      const int sf = m.vsf[f0 + l];
+      const int ifl0 = 3 * m.sf_loc[sf];
+      const int2 lr = m.flr[m.sf_face[sf]];
+      const int2 se2 = m.sf_se[sf];
+      const double4 sn = m.sfn[sf];
+      const double al = sn.w;
+      int kind = 0;  // 0 interior, 1 neumann (the default wall, and a tag's "" or "neumann"), 2 dirichlet
+      int tag = 0;
+      if (lr.y == -1) {
+        kind = 1;
+      } else if (lr.y < -1) {
+        tag = -(lr.y + 1) - 1;
+        kind = D.bcV[tag] == 2 ? 2 : 1;
+      }
+      auto side = [&](int se, int elem, const double* nl, int mode) {
+        double u[5];
+        load_u(U, elem, u);
+        const double mue = mu_of(D, u);
+        const int ise0 = 3 * m.se_loc[se];
+        const int4 q4 = m.se_sf[se];
+        const double vol = m.vol_se[se];
+        const int nsf = n_sub_faces(q4);
+        for (int p = 0; p < nsf; ++p) {
+          const int sfp = sf_of(q4, p);
+          const int ifp0 = 3 * m.sf_loc[sfp];
+          double np[3];
+          const double ap = oriented(m, sfp, se, np);
+          double blc[3][3], bn[3][3];
+          mom_block(al, ap, vol, mue, mu0c, nl, np, blc);
+          if (mode == 1) neumann_block(al, ap, vol, nl, np, bn);
+          for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+              St[(ise0 + i) + E * (ifl0 + j)] += blc[j][i];
+              if (mode != 2) {
+                const double x = mode == 1 ? bn[i][j] : blc[i][j];
+                N[(ifl0 + i) + F * (ifp0 + j)] += x;
+                S[(ifl0 + i) + F * (ise0 + j)] += x;
+              }
+            }
+        }
+      };
+      const double nl[3] = {sn.x, sn.y, sn.z}, nr[3] = {-sn.x, -sn.y, -sn.z};
+      if (kind == 0) {
+        side(se2.x, lr.x, nl, 0);
+        side(se2.y, lr.y, nr, 0);
+      } else if (kind == 1) {
+        side(se2.x, lr.x, nl, 1);
+      } else {
+        side(se2.x, lr.x, nl, 2);
+        for (int k = 0; k < 3; ++k) B[ifl0 + k] = al * D.valV[tag][k];
+        for (int i = 0; i < 3; ++i) {
+          for (int c = 0; c < E; ++c) S[(ifl0 + i) + F * c] = 0.0;
+          for (int c = 0; c < F; ++c) N[(ifl0 + i) + F * c] = 0.0;
+          for (int j = 0; j < 3; ++j) N[(ifl0 + i) + F * (ifl0 + j)] = al * (i == j ? 1.0 : 0.0);
+        }
+      }
+    }
+    __syncwarp();
+    // ---- build_momentum_diff_mat_into_global_mat_diag (:233-318)
+    for (int l = lane; l < ne; l += 32) {
+      double u[5];
+      load_u(U, m.se_elem[m.vse[s0 + l]], u);
+      for (int k = 0; k < 3; ++k) Ve[3 * l + k] = u[1 + k] / u[0];
+      double Spc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int c = 0; c < nf; ++c)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) Spc[i][j] = Spc[i][j] + St[(3 * l + i) + E * (3 * c + j)];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) blc3[9 * l + i + 3 * j] = Spc[j][i] / u[0];
+    }
+    __syncwarp();
+    warp_gemv(F, E, S, Ve, Vf, lane);
+    for (int i = lane; i < F; i += 32) Vf[i] = Vf[i] + B[i];
+    __syncwarp();
+    warp_inverse(N, F, ipiv, work, lane);
+    warp_gemm(E, F, F, St, N, T1, lane);
+    warp_gemm(E, E, F, T1, S, SNS, lane);
+    warp_gemv(F, F, N, B, tmp, lane);
+    warp_gemv(E, F, St, tmp, SB, lane);
+    warp_gemv(F, F, N, Vf, B, lane);  // B = N^-1 (S Ve + B): the face velocities
+    warp_gemv(E, E, SNS, Ve, SNSVe, lane);
+    for (int l = lane; l < ne; l += 32) {
+      const int se = m.vse[s0 + l];
+      double u[5];
+      load_u(U, m.se_elem[se], u);
+      double* t = dterm + (size_t)D.kd * se;
+      for (int i = 0; i < 3; ++i) {
+        double mv = 0.0;
+        for (int k = 0; k < 3; ++k) mv = mv + SNS[(3 * l + i) + E * (3 * l + k)] * Ve[3 * l + k];
+        t[3 * i] = SNSVe[3 * l + i];
+        t[3 * i + 1] = mv;
+        t[3 * i + 2] = SB[3 * l + i];
+      }
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+          t[9 + 2 * (i + 3 * j)] = SNS[(3 * l + i) + E * (3 * l + j)] / u[0];
+          t[10 + 2 * (i + 3 * j)] = blc3[9 * l + i + 3 * j];
+        }
+      // viscous work (:285-313)
+      const int4 q4 = m.se_sf[se];
+      const int nsf = n_sub_faces(q4);
+      double Spc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int k = 0; k < nsf; ++k) {
+        const int sf = sf_of(q4, k);
+        double nl[3];
+        const double a = oriented(m, sf, se, nl);
+        const int q = 3 * m.sf_loc[sf];
+        double vm[3];
+        for (int d = 0; d < 3; ++d) vm[d] = B[q + d] - Ve[3 * l + d];
+        const double dd = vm[0] * nl[0] + vm[1] * nl[1] + vm[2] * nl[2];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            const double e = i == j ? 1.0 : 0.0;
+            Spc[i][j] = Spc[i][j] + a * ((vm[i] * nl[j] + vm[j] * nl[i]) - (2.0 / 3.0) * dd * e);
+          }
+      }
+      const double mue = mu_of(D, u), vse = m.vol_se[se];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Spc[i][j] = Spc[i][j] * mue / vse;
+      for (int k = 0; k < 4; ++k) t[27 + k] = 0.0;
+      for (int k = 0; k < nsf; ++k) {
+        const int sf = sf_of(q4, k);
+        double nl[3];
+        const double a = oriented(m, sf, se, nl);
+        const int q = 3 * m.sf_loc[sf];
+        double sv[3];
+        for (int i = 0; i < 3; ++i) {
+          double s = 0.0;
+          for (int c = 0; c < 3; ++c) s = s + Spc[i][c] * B[q + c];
+          sv[i] = s;
+        }
+        t[27 + k] = a * (sv[0] * nl[0] + sv[1] * nl[1] + sv[2] * nl[2]);
+      }
+    }
+    __syncwarp();
+    // ---- heat: build_diff_nodal_system (ns_diffusion_module.F90:7-110)
+    for (int e = lane; e < nf * nf; e += 32) N[e] = 0.0;
+    for (int e = lane; e < nf * ne; e += 32) S[e] = St[e] = 0.0;
+    for (int e = lane; e < nf; e += 32) B[e] = 0.0;
+    __syncwarp();
+    for (int l = lane; l < nf; l += 32) {
+      const int sf = m.vsf[f0 + l];
+      const int il = m.sf_loc[sf];
+      const int2 lr = m.flr[m.sf_face[sf]];
+      const int2 se2 = m.sf_se[sf];
+      const double4 sn = m.sfn[sf];
+      const double al = sn.w;
+      auto side = [&](int se, int elem, const double* nl) {
+        double u[5];
+        load_u(U, elem, u);
+        const double kap = mu_of(D, u) * D.Cv_p * kGamma / kPrandtl;
+        const int ie = m.se_loc[se];
+        const int4 q4 = m.se_sf[se];
+        const double vol = m.vol_se[se];
+        const int nsf = n_sub_faces(q4);
+        for (int p = 0; p < nsf; ++p) {
+          const int sfp = sf_of(q4, p);
+          const int ip = m.sf_loc[sfp];
+          double np[3];
+          const double ap = oriented(m, sfp, se, np);
+          const double b = kap * al * ap * (1.0 / vol) * (np[0] * nl[0] + np[1] * nl[1] + np[2] * nl[2]);
+          N[il + nf * ip] += b;
+          S[il + nf * ie] += b;
+          St[ie + ne * il] += b;
+        }
+      };
+      const double nl[3] = {sn.x, sn.y, sn.z}, nr[3] = {-sn.x, -sn.y, -sn.z};
+      side(se2.x, lr.x, nl);
+      if (se2.y >= 0) {
+        side(se2.y, lr.y, nr);
+      } else if (lr.y < -1 && D.bcT[-(lr.y + 1) - 1] == 2) {
+        B[il] = al * D.valT[-(lr.y + 1) - 1];
+        for (int c = 0; c < ne; ++c) S[il + nf * c] = 0.0;
+        for (int c = 0; c < nf; ++c) N[il + nf * c] = 0.0;
+        N[il + nf * il] = al;
+      }
+    }
+    __syncwarp();
+    warp_inverse(N, nf, ipiv, work, lane);
+    warp_gemm(ne, nf, nf, St, N, T1, lane);
+    warp_gemm(ne, ne, nf, T1, S, SNS, lane);
+    warp_gemv(nf, nf, N, B, tmp, lane);
+    warp_gemv(ne, nf, St, tmp, SB, lane);
+    for (int l = lane; l < ne; l += 32) {
+      double u[5];
+      load_u(U, m.se_elem[m.vse[s0 + l]], u);
+      theta[l] = temp_u(u, D.Cv_p);
+      const double nn = scaled_norm3(u[1] / u[0], u[2] / u[0], u[3] / u[0]);
+      P[5 * l] = (nn * nn - u[4] / u[0]) / (u[0] * D.Cv_p);
+      for (int k = 1; k < 4; ++k) P[5 * l + k] = -u[k] / ((u[0] * u[0]) * D.Cv_p);
+      P[5 * l + 4] = 1.0 / (u[0] * D.Cv_p);
+      double s = 0.0;
+      for (int c = 0; c < nf; ++c) s = s + St[l + ne * c];
+      b1[l] = s;
+    }
+    __syncwarp();
+    for (int l = lane; l < ne; l += 32) {
+      const int se = m.vse[s0 + l];
+      double u[5];
+      load_u(U, m.se_elem[se], u);
+      double* t = dterm + (size_t)D.kd * se;
+      for (int p = 0; p < ne; ++p) t[kDiffHead + p] = SNS[l + ne * p] * theta[p];
+      const double snl = SNS[l + ne * l], cc = b1[l] - snl;
+      for (int k = 0; k < 5; ++k) t[31 + k] = cc * P[5 * l + k];
+      double pu = 0.0;
+      for (int k = 0; k < 5; ++k) pu = pu + P[5 * l + k] * u[k];
+      t[36] = snl * pu;
+      t[37] = cc * pu;
+      t[38] = b1[l] * theta[l];
+      t[39] = SB[l];
+    }
+    __syncwarp();
+  }
+}
+
+__global__ void k_ns_diffusion_apply(DevMesh m, const double* __restrict__ dterm, int kd, double* __restrict__ rhs1,
+                                     double* __restrict__ diag) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  double* r1 = rhs1 + kRhs * (size_t)c;
+  double r[5], Dm[25];
+  for (int k = 0; k < 5; ++k) r[k] = r1[k];
+  for (int k = 0; k < 25; ++k) Dm[k] = 0.0;
+  apply_diffusion_terms(m, c, dterm, kd, r, Dm);
+  for (int k = 0; k < 5; ++k) r1[k] = r[k];
+  if (diag)
+    for (int k = 0; k < 25; ++k) diag[25 * (size_t)c + k] = Dm[k];
+}
+
+}  // namespace
+
+DiffParams diff_params_from(const subfv_ns_cfg& c, const DevMesh& m) {
+  DiffParams D{};
+  D.sutherland = c.use_sutherland;
+  D.mu_p = c.mu_p;
+  D.mu0 = c.mu0;
+  D.T0 = c.T0;
+  D.Cv_p = c.Cv_p;
+  for (int i = 0; i < 16; ++i) {
+    D.bcV[i] = c.bc_type_V[i];
+    D.bcT[i] = c.bc_type_T[i];
+    D.valT[i] = c.bc_val_T[i];
+    for (int k = 0; k < 3; ++k) D.valV[i][k] = c.bc_val_V[i][k];
+  }
+  D.kd = kDiffHead + std::max(1, m.max_vse);
+  return D;
+}
+
+size_t diffusion_smem_bytes(const DevMesh& m) {
+  return sizeof(double) * (size_t)diff_layout(m.max_vsf, m.max_vse).total;
+}
+
+int diffusion_prepare(size_t smem) {
+  SUBFV_CUDA(cudaFuncSetAttribute(k_ns_diffusion, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return 0;
+}
+
+void launch_ns_diffusion(const DevMesh& m, const DiffParams& D, const double* U, double* dterm, double* mu0c) {
+  k_diff_mu0c<<<1, 1, 0, m.stream>>>(m, D, U, mu0c, 1);
+  if (D.sutherland) k_diff_mu0c<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, D, U, mu0c, 0);
+  const size_t smem = diffusion_smem_bytes(m);
+  const int grid = std::max(1, std::min(m.nv, 148 * 8));
+  k_ns_diffusion<<<grid, 32, smem, m.stream>>>(m, D, U, dterm, mu0c);
+}
+
+void launch_ns_diffusion_apply(const DevMesh& m, const double* dterm, int kd, double* rhs1, double* diag) {
+  k_ns_diffusion_apply<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, dterm, kd, rhs1, diag);
+}
+
+}  // namespace subfv

@@ -31,7 +31,13 @@ class NsCfgC(C.Structure):
                 ("bc_style", C.c_int32), ("boundary_2d", C.c_int32), ("exclude_bound_vert", C.c_int32),
                 ("local_time_step", C.c_int32), ("n_bc", C.c_int32), ("bc_type", C.c_int32 * 16),
                 ("bc_val", (C.c_double * 5) * 16), ("cfl", C.c_double), ("tmax", C.c_double),
-                ("precision", C.c_int32)]
+                ("precision", C.c_int32), ("activate_diffusion", C.c_int32), ("use_sutherland", C.c_int32),
+                ("mu_p", C.c_double), ("mu0", C.c_double), ("T0", C.c_double), ("Cv_p", C.c_double),
+                ("bc_type_V", C.c_int32 * 16), ("bc_val_V", (C.c_double * 3) * 16), ("bc_type_T", C.c_int32 * 16),
+                ("bc_val_T", C.c_double * 16)]
+
+# bc_type_V / bc_type_T per tag (ns_global_data_module.F90:49-52; 0 is the namelist's "")
+BC_DIFF_NEUMANN, BC_DIFF_DIRICHLET = 1, 2
 
 
 class ImplicitStats(C.Structure):
@@ -56,6 +62,17 @@ class NsConfig:
     bc_type: list = field(default_factory=list)  # per tag
     bc_val: list = field(default_factory=list)   # per tag, primitive (rho, u, v, w, p)
     precision: int = 0  # 0 plain FP64, 1 FP32 wave-speed bounds, 2 also FP32 flux / reconstruction / limiters
+    # diffusion (activate_diffusion; the namelist's defaults)
+    activate_diffusion: bool = False
+    use_sutherland: bool = False
+    mu_p: float = 1.329e-5
+    mu0: float = 1.716e-5
+    T0: float = 273.15
+    Cv_p: float = 720.19471
+    bc_type_V: list = field(default_factory=list)  # per tag
+    bc_val_V: list = field(default_factory=list)   # per tag (u, v, w)
+    bc_type_T: list = field(default_factory=list)  # per tag
+    bc_val_T: list = field(default_factory=list)   # per tag (temperature)
 
     def to_c(self) -> NsCfgC:
         c = NsCfgC()
@@ -68,6 +85,14 @@ class NsConfig:
             for k in range(5):
                 c.bc_val[i][k] = float(self.bc_val[i][k]) if i < len(self.bc_val) else 0.0
         c.cfl, c.tmax, c.precision = float(self.cfl), float(self.tmax), int(self.precision)
+        c.activate_diffusion, c.use_sutherland = int(self.activate_diffusion), int(self.use_sutherland)
+        c.mu_p, c.mu0, c.T0, c.Cv_p = float(self.mu_p), float(self.mu0), float(self.T0), float(self.Cv_p)
+        for i in range(16):
+            c.bc_type_V[i] = int(self.bc_type_V[i]) if i < len(self.bc_type_V) else 0
+            c.bc_type_T[i] = int(self.bc_type_T[i]) if i < len(self.bc_type_T) else 0
+            c.bc_val_T[i] = float(self.bc_val_T[i]) if i < len(self.bc_val_T) else 0.0
+            for k in range(3):
+                c.bc_val_V[i][k] = float(self.bc_val_V[i][k]) if i < len(self.bc_val_V) else 0.0
         return c
 
     def oracle_dict(self) -> dict:
@@ -77,6 +102,15 @@ class NsConfig:
         if self.bc_type:
             d["bc_type"] = np.array(self.bc_type, np.int32)
             d["bc_val"] = np.array(self.bc_val, np.float64)
+        if self.activate_diffusion:
+            nb = max(1, len(self.bc_type))
+            pad = lambda a, shape: np.concatenate([np.asarray(a, np.float64).reshape((-1,) + shape[1:]),
+                                                   np.zeros((shape[0] - len(a),) + shape[1:])])
+            d.update(activate_diffusion=1, use_sutherland=int(self.use_sutherland),
+                     diff_dc=[self.mu_p, self.mu0, self.T0, self.Cv_p],
+                     bc_type_V=pad(self.bc_type_V, (nb,)).astype(np.int32),
+                     bc_val_V=pad(self.bc_val_V, (nb, 3)), bc_type_T=pad(self.bc_type_T, (nb,)).astype(np.int32),
+                     bc_val_T=pad(self.bc_val_T, (nb,)))
         return d
 
 
@@ -121,6 +155,19 @@ def compute_rhs_ns(mesh: Mesh, cfg: NsConfig, sol):
     st = check(_lib.load().subfv_compute_rhs_ns(mesh._h, C.byref(c), pd(sol), pd(rhs), pd(sl), pd(vp), pd(grad)),
                "subfv_compute_rhs_ns")
     return st, rhs, sl, vp, grad
+
+
+def compute_rhs_ns_diag(mesh: Mesh, cfg: NsConfig, sol):
+    """compute_rhs_ns with the diffusion blocks: (status, rhs, sum_lambda, mat_diag (n, 5, 5)),
+    mat_diag[c].T the reference's mat_diag(:, :, c)."""
+    sol = f64(sol)
+    rhs = np.empty((mesh.n_elems, 5))
+    sl = np.empty(mesh.n_elems)
+    diag = np.empty((mesh.n_elems, 5, 5))
+    c = cfg.to_c()
+    st = check(_lib.load().subfv_compute_rhs_ns_ex(mesh._h, C.byref(c), pd(sol), pd(rhs), pd(sl), None, None,
+                                                    pd(diag)), "subfv_compute_rhs_ns_ex")
+    return st, rhs, sl, diag
 
 
 class NsState:

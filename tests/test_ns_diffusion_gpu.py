@@ -1,0 +1,123 @@
+"""Navier-Stokes diffusion (activate_diffusion) on the GPU against the oracle restatement
+of src/ns/ns_vectorial_diffusion_module.F90 (momentum, viscous work) and
+src/ns/ns_diffusion_module.F90 (heat), with the point-implicit 5x5 solve of
+add_timedisc_and_solve (src/ns/ns_euler_module.F90:521-609). With a constant viscosity
+the residual, the diffusion blocks of mat_diag and the time loop are bit-identical to the
+oracle; Sutherland's law evaluates pow, whose last bits differ between CUDA and the host C
+library, so it is compared at 1e-12 of the scale. Unsupported uses are rejected."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NX, NY = 8, 6
+TAGS = {"xlo": 1, "xhi": 2, "ylo": 3, "yhi": 4}
+
+
+def _raws():
+    from subfv_b200 import meshgen
+    return {
+        "hex": meshgen.tag_slab_sides(meshgen.hex_slab(NX, NY, jitter=0.1, seed=3), NX, NY, TAGS),
+        "prism": meshgen.tag_slab_sides(
+            meshgen.prism_slab(NX, NY, -0.5, 0.5, -0.5, 0.5, -0.5, 0.5, jitter=0.05, seed=4), NX, NY, TAGS),
+        "box": meshgen.hex_box(4, jitter=0.05, seed=5, periodic=False),
+    }
+
+
+def _pair(raw):
+    from oracle.oracle import OracleMesh
+    from subfv_b200.mesh import Mesh
+    return Mesh.from_raw(raw), OracleMesh(raw)
+
+
+def _state(n, seed=5):
+    rng = np.random.default_rng(seed)
+    w = np.column_stack([rng.uniform(1.1, 1.3, n), rng.uniform(-0.1, 0.1, (n, 3)), rng.uniform(0.9, 1.1, n)])
+    return np.ascontiguousarray(np.column_stack([w[:, 0], w[:, 1:4] * w[:, :1],
+                                                 w[:, 4] / 0.4 + 0.5 * w[:, 0] * (w[:, 1:4] ** 2).sum(1)]))
+
+
+DIFF = {
+    "neumann": dict(),
+    "dirichlet": dict(bc_type_V=[1, 2, 2, 2], bc_val_V=[[0, 0, 0], [0, 0, 0], [0, 0, 0], [0.1, 0, 0]],
+                      bc_type_T=[2, 0, 1, 2], bc_val_T=[0.5, 0, 0, 0.35]),
+}
+
+
+def _cfg(mesh_name, diff_name, **kw):
+    from subfv_b200.ns import NsConfig
+    base = dict(scheme=1, second_order=True, method=4, bc_style=2, boundary_2d=mesh_name != "box", cfl=0.3,
+                activate_diffusion=True, mu_p=0.02, Cv_p=2.5)
+    if mesh_name != "box":
+        base.update(bc_type=[1, 1, 1, 1], bc_val=[[0] * 5] * 4, **DIFF[diff_name])
+    base.update(kw)
+    return NsConfig(**base)
+
+
+@pytest.mark.parametrize("mesh_name", ["hex", "prism", "box"])
+@pytest.mark.parametrize("diff_name", ["neumann", "dirichlet"])
+@pytest.mark.parametrize("scheme,order", [(1, True), (4, False)])
+def test_rhs_and_diag_bit_exact(native, oracle_lib, cuda_ok, mesh_name, diff_name, scheme, order):
+    from subfv_b200.ns import compute_rhs_ns_diag
+    if mesh_name == "box" and diff_name == "dirichlet":
+        pytest.skip("the box has only the default (Neumann) walls")
+    m, o = _pair(_raws()[mesh_name])
+    cfg = _cfg(mesh_name, diff_name, scheme=scheme, second_order=order)
+    sol = _state(m.n_elems)
+    st, rhs, sl, diag = compute_rhs_ns_diag(m, cfg, sol)
+    st_o, rhs_o, sl_o, diag_o = o.ns_rhs_diag(cfg.oracle_dict(), sol)
+    assert st == st_o == 0
+    assert np.abs(diag_o).max() > 0.0
+    np.testing.assert_array_equal(sl, sl_o)
+    np.testing.assert_array_equal(diag, diag_o)
+    np.testing.assert_array_equal(rhs, rhs_o)
+
+
+@pytest.mark.parametrize("mesh_name,diff_name", [("hex", "dirichlet"), ("prism", "neumann"), ("box", "neumann")])
+def test_time_loop_bit_exact(native, oracle_lib, cuda_ok, mesh_name, diff_name):
+    from subfv_b200.ns import NsState
+    m, o = _pair(_raws()[mesh_name])
+    cfg = _cfg(mesh_name, diff_name)
+    sol = _state(m.n_elems, seed=9)
+    s = NsState(m, cfg, sol)
+    st, n, t = s.advance(6)
+    sol_o = sol.copy()
+    st_o, it, t_o, res_o, rv_o, _ = o.ns_run(cfg.oracle_dict(), sol_o, 5)
+    assert st == st_o == 0 and n == it == 6 and t == t_o
+    np.testing.assert_array_equal(s.sol(), sol_o)
+    res, rv, _ = s.residuals()
+    assert res == pytest.approx(res_o, rel=1e-13)
+    np.testing.assert_allclose(rv, rv_o, rtol=1e-13)
+    s.close()
+
+
+def test_sutherland_close(native, oracle_lib, cuda_ok):
+    from subfv_b200.ns import compute_rhs_ns_diag
+    m, o = _pair(_raws()["hex"])
+    cfg = _cfg("hex", "dirichlet", use_sutherland=True, mu0=0.02, T0=0.4)
+    sol = _state(m.n_elems)
+    st, rhs, sl, diag = compute_rhs_ns_diag(m, cfg, sol)
+    st_o, rhs_o, sl_o, diag_o = o.ns_rhs_diag(cfg.oracle_dict(), sol)
+    assert st == st_o == 0
+    np.testing.assert_array_equal(sl, sl_o)
+    for k in range(5):
+        assert np.abs(rhs[:, k] - rhs_o[:, k]).max() <= 1e-12 * np.abs(rhs_o).max(), k
+    assert np.abs(diag - diag_o).max() <= 1e-12 * np.abs(diag_o).max()
+
+
+def test_unsupported_uses_rejected(native, cuda_ok):
+    from subfv_b200 import meshgen
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsBatch, NsState
+    per = Mesh.from_raw(meshgen.hex_box(4, periodic=True))
+    with pytest.raises(Exception):
+        NsState(per, _cfg("box", "neumann"), _state(per.n_elems))
+    with pytest.raises(Exception):
+        NsBatch(_cfg("hex", "neumann"), capacity=2, budget_bytes=1 << 30)
+    m = Mesh.from_raw(_raws()["hex"])
+    s = NsState(m, _cfg("hex", "neumann", scheme=4, second_order=False, method=0), _state(m.n_elems))
+    with pytest.raises(Exception):
+        s.be_jacobian(0.01)
+    with pytest.raises(Exception):
+        NsState(m, _cfg("hex", "neumann", bc_type_V=[3, 0, 0, 0]), _state(m.n_elems))
+    s.close()
