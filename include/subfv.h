@@ -52,6 +52,30 @@ int subfv_topology_array_get(const subfv_topology* t, const char* name, int32_t*
 int subfv_topology_coords(const subfv_topology* t, double* coords_out);
 void subfv_topology_destroy(subfv_topology* t);
 
+/* ---- mesh and solution files (host) ----
+   read_mesh_msh (mesh_reading_module.F90:154-205) for one process: gmsh ASCII MSH 2 or 4,
+   volumes of types 4-7 (tet, hex, prism, pyramid) and boundary faces of types 2-3 whose
+   tag is the 1-based index of the bc_names entry naming their physical group (0 when
+   none). MSH 2 takes node ids as the nodes' order; MSH 4 keeps the nodes the volumes use,
+   numbered in their order in $Nodes (:771-900). The arrays feed subfv_topology_build. */
+typedef struct subfv_msh subfv_msh;
+int subfv_msh_read(const char* path, int n_bc, const char* const* bc_names, subfv_msh** out);
+/* sizes: n_vert, n_elems, len(elem_vert), n_boundary_faces, len(bface_vert) */
+int subfv_msh_sizes(const subfv_msh* m, int64_t* sizes);
+int subfv_msh_get(const subfv_msh* m, double* coords, int32_t* elem_kind, int32_t* elem_vert_off,
+                  int32_t* elem_vert, int32_t* bface_off, int32_t* bface_vert, int32_t* bface_tag);
+void subfv_msh_destroy(subfv_msh* m);
+/* write_sol_vtu (ns_io_module.F90:403-884): ASCII VTU, polyhedral cells with their faces,
+   Nodal_Velocity (vp, may be NULL) and the cell fields Centroid (elem_coord, may be NULL),
+   Tag, MPI_Color, Density, Momentum, Energy, Velocity, Pressure, Internal_energy, H, Mach,
+   Temperature (Cv_p), mu (when mu >= 0) and Residual (norm2 of delta, may be NULL);
+   sol (5, n_elems) conservative */
+int subfv_write_sol_vtu(const char* path, const subfv_topology* t, const double* sol, const double* delta,
+                        const double* vp, const double* elem_coord, double Cv_p, double mu);
+/* restart_from_vtu_file (ns_io_module.F90:1333-1382): Density, Momentum and Energy (per
+   unit mass) of a VTU written above, into sol (5, n_elems) */
+int subfv_restart_from_vtu(const char* path, int64_t n_elems, double* sol);
+
 /* ---------------------------------------------------------------------------------
  * Device mesh. subfv_mesh_desc flattens mesh_type (src/mesh/mesh_module.F90:76-89);
  * the Fortran shim fills it from its mesh after build_mesh. */

@@ -32,6 +32,12 @@ SIGNATURES = {
     "subfv_topology_array_get": (c_int, [P, c_char_p, PI32]),
     "subfv_topology_coords": (c_int, [P, PD]),
     "subfv_topology_destroy": (None, [P]),
+    "subfv_msh_read": (c_int, [c_char_p, c_int, C.POINTER(c_char_p), C.POINTER(P)]),
+    "subfv_msh_sizes": (c_int, [P, C.POINTER(c_i64)]),
+    "subfv_msh_get": (c_int, [P, PD, PI32, PI32, PI32, PI32, PI32, PI32]),
+    "subfv_msh_destroy": (None, [P]),
+    "subfv_write_sol_vtu": (c_int, [c_char_p, P, PD, PD, PD, PD, c_dbl, c_dbl]),
+    "subfv_restart_from_vtu": (c_int, [c_char_p, c_i64, PD]),
     "subfv_mesh_create": (c_int, [P, C.POINTER(P)]),
     "subfv_mesh_create_from_topology": (c_int, [P, c_int, C.POINTER(P)]),
     "subfv_mesh_destroy": (c_int, [P]),
