@@ -1449,6 +1449,7 @@ __device__ __noinline__ void diffusion_cell_solve(const DevMesh& m, int c, const
   for (int k = 0; k < 5; ++k) d5[k] = x[k] - u[k];
 }
 
+template <bool DIFF = false>
 __device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U_rhs,
                                  const double* __restrict__ rhs1, const double* __restrict__ rhs2,
                                  const double* __restrict__ U_td, double* __restrict__ delta,
@@ -1480,7 +1481,7 @@ __device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const doub
     double u[5], d5[5], ad[5];
     ld5(U_td, c, u);
     const double s = a1 * (V / dt + 0.0);  // sum_lambda is zeroed once dt is known
-    if (dterm) {
+    if (DIFF) {
       diffusion_cell_solve(m, c, dterm, P.diff_kd, r, rv, u, s, d5);
       for (int k = 0; k < 5; ++k) ad[k] = a2 * d5[k];
     } else {
@@ -1534,6 +1535,7 @@ __device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const doub
   }
 }
 
+template <bool DIFF>
 __global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P, const double* __restrict__ U_rhs,
                                                           const double* __restrict__ rhs1,
                                                           const double* __restrict__ rhs2,
@@ -1541,7 +1543,7 @@ __global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P,
                                                           double* __restrict__ delta, double* __restrict__ partial,
                                                           NsScalars* sc, double a1, double a2,
                                                           const double* __restrict__ dterm) {
-  ns_timedisc_body(m, P, U_rhs, rhs1, rhs2, U_td, delta, partial, sc, a1, a2, blockIdx.x, dterm);
+  ns_timedisc_body<DIFF>(m, P, U_rhs, rhs1, rhs2, U_td, delta, partial, sc, a1, a2, blockIdx.x, dterm);
 }
 
 // scalar tail of add_timedisc_and_solve (:582-608); last_stage also advances t
@@ -2164,8 +2166,12 @@ void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs
                         const double* rhs2, const double* U_td, double* U_out, double* delta, double* partial,
                         NsScalars* sc, double a1, double a2, int last_stage, const double* dterm) {
   const int nb = ns_partial_blocks(m);
-  k_ns_timedisc<<<nb, kTdBlock, 0, m.stream>>>(m, P, U_rhs, rhs1, P.second_order ? rhs2 : nullptr, U_td, delta,
-                                               partial, sc, a1, a2, P.diff ? dterm : nullptr);
+  if (P.diff && dterm)
+    k_ns_timedisc<true><<<nb, kTdBlock, 0, m.stream>>>(m, P, U_rhs, rhs1, P.second_order ? rhs2 : nullptr, U_td,
+                                                       delta, partial, sc, a1, a2, dterm);
+  else
+    k_ns_timedisc<false><<<nb, kTdBlock, 0, m.stream>>>(m, P, U_rhs, rhs1, P.second_order ? rhs2 : nullptr, U_td,
+                                                        delta, partial, sc, a1, a2, nullptr);
   k_ns_finalize<<<1, 1, 0, m.stream>>>(sc, P, partial, nb, m.status, last_stage);
   k_ns_apply<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, U_td, delta, U_out, sc, a2);
   k_ns_reset_omega<<<1, 1, 0, m.stream>>>(sc);
