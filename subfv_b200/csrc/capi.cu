@@ -37,6 +37,8 @@ struct subfv_lag_state {
   int scheme = 0, method = 0;  // 0 "classic"; 1 "sidil" with method_length
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
+  cudaStream_t side = nullptr;  // the host-buffer step's copy back, beside move and geometry
+  cudaEvent_t updated = nullptr;
 };
 
 namespace subfv {
@@ -439,6 +441,8 @@ int subfv_lag_state_create(subfv_mesh* m, const double* sol, const double* mass,
 int subfv_lag_state_destroy(subfv_lag_state* s) {
   if (!s) return 0;
   if (s->graph) cudaGraphExecDestroy(s->graph);
+  if (s->updated) cudaEventDestroy(s->updated);
+  if (s->side) cudaStreamDestroy(s->side);
   cudaFree(s->sol6);
   cudaFree(s->rhs6);
   cudaFree(s->sc);
@@ -548,12 +552,27 @@ int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout) {
   cudaGetLastError();  // a pageable pointer is not an error here
   double* hbuf = pinned ? sol_inout : s->host_stage;
   if (!pinned) std::memcpy(s->host_stage, sol_inout, bytes);
+  if (!s->side) {
+    SUBFV_CUDA(cudaStreamCreateWithFlags(&s->side, cudaStreamNonBlocking));
+    SUBFV_CUDA(cudaEventCreateWithFlags(&s->updated, cudaEventDisableTiming));
+  }
   SUBFV_CUDA(cudaMemcpyAsync(s->dev_stage, hbuf, bytes, cudaMemcpyHostToDevice, d.stream));
   launch_pack6(d, d.ne, s->dev_stage, nullptr, s->sol6);
-  enqueue_lag_step(d, s->sol6, s->rhs6, s->sc, s->precision, s->scheme, s->method);
+  // the state is final once updated: its copy back runs on the side stream while the
+  // main stream moves the mesh and recomputes the geometry (which read neither sol6 nor
+  // the staging buffer)
+  enqueue_lag_step_head(d, s->sol6, s->rhs6, s->sc, s->precision, s->scheme, s->method);
+  launch_lag_update(d, s->sol6, s->rhs6, s->sc);
+  SUBFV_CUDA(cudaEventRecord(s->updated, d.stream));
+  SUBFV_CUDA(cudaStreamWaitEvent(s->side, s->updated, 0));
+  DevMesh ds = d;
+  ds.stream = s->side;
+  launch_unpack6(ds, d.ne, kRec, s->sol6, s->dev_stage);
+  SUBFV_CUDA(cudaMemcpyAsync(hbuf, s->dev_stage, bytes, cudaMemcpyDeviceToHost, s->side));
+  launch_lag_move(d, s->sc, 0.0);
+  launch_geometry(d, 0, nullptr, nullptr, s->sc);
   d.geom_partial = 1;
-  launch_unpack6(d, d.ne, kRec, s->sol6, s->dev_stage);
-  SUBFV_CUDA(cudaMemcpyAsync(hbuf, s->dev_stage, bytes, cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(s->side));
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
   if (!pinned) std::memcpy(sol_inout, s->host_stage, bytes);
   return check_status(d);

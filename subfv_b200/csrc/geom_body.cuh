@@ -99,6 +99,21 @@ constexpr int kGeoMaxV = 8, kGeoMaxF = 8, kGeoBlock = 64;
 
 // c: this thread's cell; every thread of a kGeoBlock-thread block calls (the caches are
 // indexed by threadIdx.x); dt: the step's time step for the update (with sol6)
+// lagrange_main.F90:110: new_sol = sol + dt*rhs, and the cell's pressure record
+__device__ inline void state_update(const DevMesh& m, double* sol6, const double* rhs6, const double dt,
+                                    const int c) {
+  double* u = sol6 + kRec * (size_t)c;
+  const double* r = rhs6 + kRhs * (size_t)c;
+  bool fin = true;
+  for (int k = 0; k < 5; ++k) {
+    u[k] = u[k] + dt * r[k];
+    fin = fin && isfinite(u[k]);
+  }
+  u[6] = lag_pressure(u[0], u[1], u[2], u[3], u[4]);
+  if (!fin) atomicOr(m.status, kErrNonFinite);
+  if (!(u[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
+}
+
 __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const double* rhs6, const double dt,
                                       const int c) {
   __shared__ double sX[kGeoMaxV][3][kGeoBlock];
@@ -232,18 +247,7 @@ __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const doub
   ok = ok && (fnorm2_3(nt.x, nt.y, nt.z) < 1e-14);
   ok = ok && (fnorm2_3(ns.x, ns.y, ns.z) < 1e-14);
   if (!ok) atomicOr(m.status, kErrMeshCheck);
-  if (sol6) {  // lagrange_main.F90:110: new_sol = sol + dt*rhs
-    double* u = sol6 + kRec * (size_t)c;
-    const double* r = rhs6 + kRhs * (size_t)c;
-    bool fin = true;
-    for (int k = 0; k < 5; ++k) {
-      u[k] = u[k] + dt * r[k];
-      fin = fin && isfinite(u[k]);
-    }
-    u[6] = lag_pressure(u[0], u[1], u[2], u[3], u[4]);
-    if (!fin) atomicOr(m.status, kErrNonFinite);
-    if (!(u[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
-  }
+  if (sol6) state_update(m, sol6, rhs6, dt, c);
 }
 
 }  // namespace geo

@@ -705,8 +705,8 @@ void launch_lag_batch_step(const LagTable& t, int precision, cudaStream_t s) {
 
 // One full time step of lagrange_main.F90:89-127 (graph-capturable: no host sync);
 // scheme 0 "classic", 1 "sidil" (FP64, method_length `method`).
-void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision, int scheme,
-                      int method) {
+void enqueue_lag_step_head(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision, int scheme,
+                           int method) {
   if (scheme == 1) {
     launch_lag_sidil_node(m, sol6, sc, method);
     launch_lag_cell(m, sol6, rhs6, sc, &sc->dtmin, 0, 7);
@@ -715,6 +715,11 @@ void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* 
     launch_lag_cell(m, sol6, rhs6, sc, &sc->dtmin, precision, 3);
   }
   launch_lag_finalize(m, sc);
+}
+
+void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision, int scheme,
+                      int method) {
+  enqueue_lag_step_head(m, sol6, rhs6, sc, precision, scheme, method);
   launch_lag_move(m, sc, 0.0);
   launch_geometry(m, 0, sol6, rhs6, sc);
 }

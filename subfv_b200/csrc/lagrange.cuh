@@ -24,6 +24,10 @@ void launch_set_scalar(const DevMesh& m, double* p, double v);
 // fills m.centry (allocated by the caller, ncsf records) from the cell CSR
 void launch_build_cell_entries(const DevMesh& m);
 // scheme 0 "classic", 1 "sidil" (method_length `method`, FP64)
+// the step up to lagrange_finalize (nodal solve, fluxes, dt); the rest is move_mesh and
+// the geometry, with the update fused in (enqueue_lag_step) or launched on its own
+void enqueue_lag_step_head(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision,
+                           int scheme = 0, int method = 0);
 void enqueue_lag_step(const DevMesh& m, double* sol6, double* rhs6, LagScalars* sc, int precision, int scheme = 0,
                       int method = 0);
 // scheme "sidil": vertex volumes of the current mesh, then vp = (velocity, nodal pressure)

@@ -329,6 +329,12 @@ __global__ void __launch_bounds__(geo::kGeoBlock) k_geom_step(DevMesh m, double*
   geo::geom_step_body(m, sol6, rhs6, sol6 ? sc->dt : 0.0, blockIdx.x * geo::kGeoBlock + threadIdx.x);
 }
 
+__global__ void k_lag_update(DevMesh m, double* sol6, const double* rhs6, const LagScalars* sc) {
+  if (sc->skip) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < m.ne) geo::state_update(m, sol6, rhs6, sc->dt, c);
+}
+
 // compute_vert_volume (:273-288)
 __global__ void k_vert_volume(DevMesh m) {
   int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -364,6 +370,9 @@ void launch_geometry(const DevMesh& m, int full, double* sol6, const double* rhs
     k_face_geom<0><<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, sc);
     k_geom_step<<<grid_for(m.ne, geo::kGeoBlock), geo::kGeoBlock, 0, m.stream>>>(m, sol6, rhs6, sc);
   }
+}
+void launch_lag_update(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc) {
+  k_lag_update<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, sol6, rhs6, sc);
 }
 void launch_vert_volume(const DevMesh& m) { k_vert_volume<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }
 void launch_vert_is_bound(const DevMesh& m) { k_vert_is_bound<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }

@@ -100,6 +100,8 @@ void devmesh_free(DevMesh* m);
 // update sol += dt*rhs fused in)
 void launch_geometry(const DevMesh& m, int full, double* sol6 = nullptr, const double* rhs6 = nullptr,
                      const LagScalars* sc = nullptr);
+// sol += dt*rhs alone (the update launch_geometry otherwise fuses in)
+void launch_lag_update(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc);
 void launch_vert_volume(const DevMesh& m);
 void launch_vert_is_bound(const DevMesh& m);
 

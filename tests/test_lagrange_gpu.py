@@ -205,12 +205,13 @@ def test_sidil_run_bit_exact(native, oracle_lib, cuda_ok, case):
 
 def test_step_host_pinned_and_pageable_agree(native, cuda_ok):
     """subfv_lag_step_host copies a page-locked caller buffer directly and a pageable one
-    through its staging buffer: both give the device loop's state, bit for bit."""
+    through its staging buffer, the copy back overlapping the mesh motion and geometry:
+    both give the device loop's state and mesh, bit for bit."""
     import torch
     from subfv_b200.lagrange import LagrangeState
     from subfv_b200.mesh import Mesh
     raw = lagrange_cases()["prism_jit"]
-    outs = []
+    outs, coords = [], []
     for kind in ("pageable", "pinned", "device"):
         m = Mesh.from_raw(raw)
         sol = _random_state(m.n_elems, 7)
@@ -219,6 +220,7 @@ def test_step_host_pinned_and_pageable_agree(native, cuda_ok):
         if kind == "device":
             s.advance(4)
             outs.append(s.sol())
+            coords.append(m.coords())
             continue
         if kind == "pinned":
             t = torch.empty(sol.shape, dtype=torch.float64, pin_memory=True)
@@ -229,5 +231,8 @@ def test_step_host_pinned_and_pageable_agree(native, cuda_ok):
         for _ in range(4):
             assert s.step_host(buf) == 0
         outs.append(buf.copy())
+        coords.append(m.coords())
     np.testing.assert_array_equal(outs[0], outs[2])
     np.testing.assert_array_equal(outs[1], outs[2])
+    np.testing.assert_array_equal(coords[0], coords[2])
+    np.testing.assert_array_equal(coords[1], coords[2])
