@@ -508,7 +508,12 @@ size_t diffusion_smem_bytes(const DevMesh& m) {
 }
 
 int diffusion_prepare(size_t smem) {
-  SUBFV_CUDA(cudaFuncSetAttribute(k_ns_diffusion, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  // the attribute is per kernel: only ever raised, so every live state's launch fits
+  static size_t granted = 0;
+  if (smem > granted) {
+    SUBFV_CUDA(cudaFuncSetAttribute(k_ns_diffusion, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    granted = smem;
+  }
   return 0;
 }
 
