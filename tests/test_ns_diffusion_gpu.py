@@ -121,3 +121,24 @@ def test_unsupported_uses_rejected(native, cuda_ok):
     with pytest.raises(Exception):
         NsState(m, _cfg("hex", "neumann", bc_type_V=[3, 0, 0, 0]), _state(m.n_elems))
     s.close()
+
+
+def test_states_of_different_meshes_coexist(native, oracle_lib, cuda_ok):
+    """A state on a mesh with larger vertex systems keeps running after one on a smaller
+    mesh is created (the kernel's shared-memory allowance only grows)."""
+    from subfv_b200.ns import NsState
+    raws = _raws()
+    mb, ob = _pair(raws["box"])
+    ms = _pair(raws["hex"])[0]
+    cfg = _cfg("box", "neumann")
+    sol = _state(mb.n_elems, seed=4)
+    big = NsState(mb, cfg, sol)
+    small = NsState(ms, _cfg("hex", "neumann"), _state(ms.n_elems))
+    assert small.advance(2)[0] == 0
+    st, n, _ = big.advance(3)
+    sol_o = sol.copy()
+    st_o, it, _, _, _, _ = ob.ns_run(cfg.oracle_dict(), sol_o, 2)
+    assert st == st_o == 0 and n == it
+    np.testing.assert_array_equal(big.sol(), sol_o)
+    big.close()
+    small.close()
