@@ -169,6 +169,9 @@ int subfv_lag_state_destroy(subfv_lag_state* s);
 int subfv_lag_state_set_scheme(subfv_lag_state* s, int scheme, int method_length);
 /* run n_steps (stops early once t >= t_max); returns status bits */
 int subfv_lag_advance(subfv_lag_state* s, int n_steps, int* steps_done, double* t);
+/* captures the graph the time loop replays (done by the first advance otherwise); the
+   state does not move */
+int subfv_lag_prepare(subfv_lag_state* s);
 int subfv_lag_advance_async(subfv_lag_state* s, int n_steps);
 int subfv_lag_sync(subfv_lag_state* s, int* steps_done, double* t);
 int subfv_lag_get_sol(subfv_lag_state* s, double* sol);
@@ -238,6 +241,9 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
                           subfv_ns_state** out);
 int subfv_ns_state_destroy(subfv_ns_state* s);
 /* n_steps iterations of ns_main.F90:83-107 (stops once t >= tmax); status bits */
+/* captures the graph the time loop replays (done by the first advance otherwise): set-up
+   that a caller may take out of its timed region; the state does not move */
+int subfv_ns_prepare(subfv_ns_state* s);
 int subfv_ns_advance(subfv_ns_state* s, int n_steps, int* steps_done, double* t);
 int subfv_ns_advance_async(subfv_ns_state* s, int n_steps);
 int subfv_ns_sync(subfv_ns_state* s, int* steps_done, double* t);

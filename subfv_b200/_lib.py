@@ -36,6 +36,8 @@ SIGNATURES = {
     "subfv_msh_sizes": (c_int, [P, C.POINTER(c_i64)]),
     "subfv_msh_get": (c_int, [P, PD, PI32, PI32, PI32, PI32, PI32, PI32]),
     "subfv_msh_destroy": (None, [P]),
+    "subfv_lag_prepare": (c_int, [P]),
+    "subfv_ns_prepare": (c_int, [P]),
     "subfv_write_sol_vtu": (c_int, [c_char_p, P, PD, PD, PD, PD, c_dbl, c_dbl]),
     "subfv_restart_from_vtu": (c_int, [c_char_p, c_i64, PD]),
     "subfv_mesh_create": (c_int, [P, C.POINTER(P)]),

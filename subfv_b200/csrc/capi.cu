@@ -476,10 +476,17 @@ int lag_graph(subfv_lag_state* s, int steps) {
 }
 }  // namespace
 
+constexpr int kLagGraphSteps = 16;  // steps per captured graph
+
+int subfv_lag_prepare(subfv_lag_state* s) {
+  if (!s) return -2;
+  return lag_graph(s, kLagGraphSteps) ? -1 : 0;
+}
+
 int subfv_lag_advance_async(subfv_lag_state* s, int n_steps) {
   DevMesh& d = s->m->d;
   if (n_steps > 0) d.geom_partial = 1;
-  const int chunk = 16;
+  const int chunk = kLagGraphSteps;
   if (n_steps >= chunk) {
     if (lag_graph(s, chunk)) return -1;
     for (int i = 0; i + chunk <= n_steps; i += chunk) SUBFV_CUDA(cudaGraphLaunch(s->graph, d.stream));

@@ -261,9 +261,16 @@ int subfv_ns_state_destroy(subfv_ns_state* s) {
   return 0;
 }
 
+constexpr int kNsGraphSteps = 8;  // steps per captured graph
+
+int subfv_ns_prepare(subfv_ns_state* s) {
+  if (!s) return -2;
+  return ns_graph(s, kNsGraphSteps) ? -1 : 0;
+}
+
 int subfv_ns_advance_async(subfv_ns_state* s, int n_steps) {
   DevMesh& d = s->m->d;
-  const int chunk = 8;
+  const int chunk = kNsGraphSteps;
   if (n_steps >= chunk) {
     if (ns_graph(s, chunk)) return -1;
     for (int i = 0; i + chunk <= n_steps; i += chunk) SUBFV_CUDA(cudaGraphLaunch(s->graph, d.stream));

@@ -190,6 +190,10 @@ class NsState:
     def advance_async(self, n_steps: int):
         check(_lib.load().subfv_ns_advance_async(self._h, int(n_steps)), "subfv_ns_advance_async")
 
+    def prepare(self):
+        """Capture the replayed step graph now (set-up; the state does not move)."""
+        check(_lib.load().subfv_ns_prepare(self._h), "subfv_ns_prepare")
+
     def sync(self):
         steps, t = C.c_int(), C.c_double()
         st = check(_lib.load().subfv_ns_sync(self._h, C.byref(steps), C.byref(t)), "subfv_ns_sync")

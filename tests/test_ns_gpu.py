@@ -153,3 +153,33 @@ def test_ns_3d_box_walls_bit_exact(native, oracle_lib, cuda_ok):
     st_o, it, t_o, _, _, _ = o.ns_run(cfg.oracle_dict(), sol_o, 4)
     assert st == st_o == 0 and t == t_o
     np.testing.assert_array_equal(s.sol(), sol_o)
+
+
+def test_prepare_leaves_state_and_results_unchanged(native, cuda_ok):
+    """Capturing the step graph ahead (prepare) neither moves the state nor changes the run."""
+    from subfv_b200 import meshgen
+    from subfv_b200.lagrange import LagrangeState
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsConfig, NsState, init_gresho
+    raw = meshgen.hex_slab(12, 10, jitter=0.1, seed=31)
+    outs = []
+    for prep in (False, True):
+        m = Mesh.from_raw(raw)
+        s = NsState(m, NsConfig(cfl=0.4), init_gresho(m, 0.1))
+        if prep:
+            s.prepare()
+            assert s.sync()[1] == 0
+        outs.append((s.advance(19), s.sol()))
+        s.close()
+    assert outs[0][0] == outs[1][0]
+    np.testing.assert_array_equal(outs[0][1], outs[1][1])
+    lag = []
+    for prep in (False, True):
+        m = Mesh.from_raw(raw)
+        sol = init_gresho(m, 0.1)
+        st = LagrangeState(m, sol, m.geometry("elem_volume") / sol[:, 0], cfl=0.5, t_max=1.0)
+        if prep:
+            st.prepare()
+        lag.append((st.advance(21), st.sol()))
+    assert lag[0][0] == lag[1][0]
+    np.testing.assert_array_equal(lag[0][1], lag[1][1])
