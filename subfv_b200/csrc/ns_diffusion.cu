@@ -521,7 +521,8 @@ void launch_ns_diffusion(const DevMesh& m, const DiffParams& D, const double* U,
   k_diff_mu0c<<<1, 1, 0, m.stream>>>(m, D, U, mu0c, 1);
   if (D.sutherland) k_diff_mu0c<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, D, U, mu0c, 0);
   const size_t smem = diffusion_smem_bytes(m);
-  const int grid = std::max(1, std::min(m.nv, 148 * 8));
+  // a warp per vertex: as many warps as shared memory lets reside (up to 32 per SM)
+  const int grid = std::max(1, std::min(m.nv, 148 * 32));
   k_ns_diffusion<<<grid, 32, smem, m.stream>>>(m, D, U, dterm, mu0c);
 }
 
