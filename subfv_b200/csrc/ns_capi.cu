@@ -193,7 +193,7 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
     // the reference's diffusion indexes the periodic extension of a vertex's lists by the
     // subfaces' original local ids, which collide; only meshes without periodic faces
     const size_t smem = diffusion_smem_bytes(d);
-    if (!d.vsf_identity || smem > 200 * 1024) {
+    if (!d.vsf_identity || smem > 200 * 1024 || d.max_vsf > 32) {
       set_error(!d.vsf_identity ? "subfv_ns: diffusion on a mesh with periodic faces is not supported"
                                 : "subfv_ns: a vertex's diffusion system exceeds shared memory");
       subfv_ns_state_destroy(s);

@@ -107,22 +107,40 @@ __device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane
     }
     __syncwarp();
   }
-  // dtrti2 ('Upper', 'Non-unit')
+  // dtrti2 ('Upper', 'Non-unit'). Column j's dtrmv keeps x(0:j-1) in registers, row i in
+  // lane i % 32 (n <= 96 here: three rows a lane). At step jj, x(jj) has not been touched
+  // yet (only later steps add to it), so its owner broadcasts the column's own entry; the
+  // owner then scales it by the diagonal, as dtrmv does.
   for (int j = 0; j < n; ++j) {
     if (lane == 0) a[j + n * j] = 1.0 / a[j + n * j];
     __syncwarp();
     const double ajj = -a[j + n * j];
     double* x = a + n * j;
-    for (int jj = 0; jj < j; ++jj) {  // dtrmv on x(0:j-1)
-      const double temp = x[jj];
-      __syncwarp();
-      if (temp != 0.0) {
-        for (int i = lane; i < jj; i += 32) x[i] = x[i] + temp * a[i + n * jj];
-        if (lane == 0) x[jj] = x[jj] * a[jj + n * jj];
-      }
-      __syncwarp();
+    double xr[3];
+    for (int r = 0; r < 3; ++r) {
+      const int i = lane + 32 * r;
+      xr[r] = i < j ? x[i] : 0.0;
     }
-    for (int i = lane; i < j; i += 32) x[i] = ajj * x[i];
+    for (int jj = 0; jj < j; ++jj) {
+      const int owner = jj & 31, slot = jj >> 5;
+      const double mine = slot == 0 ? xr[0] : slot == 1 ? xr[1] : xr[2];
+      const double temp = __shfl_sync(0xffffffffu, mine, owner);
+      if (temp != 0.0) {
+        for (int r = 0; r < 3; ++r) {
+          const int i = lane + 32 * r;
+          if (i < jj) xr[r] = xr[r] + temp * a[i + n * jj];
+        }
+        if (lane == owner) {
+          if (slot == 0) xr[0] = xr[0] * a[jj + n * jj];
+          else if (slot == 1) xr[1] = xr[1] * a[jj + n * jj];
+          else xr[2] = xr[2] * a[jj + n * jj];
+        }
+      }
+    }
+    for (int r = 0; r < 3; ++r) {
+      const int i = lane + 32 * r;
+      if (i < j) x[i] = ajj * xr[r];
+    }
     __syncwarp();
   }
   // inv(A) L = inv(U), column by column from the last (the unblocked dgetri sweep)
@@ -172,7 +190,7 @@ __device__ inline void warp_gemv(int m, int n, const double* A, const double* x,
 }
 
 struct DiffSmem {  // offsets (doubles) of one vertex's work arrays, for the mesh's largest vertex
-  int N, S, St, T1, SNS, B, Vf, tmp, work, Ve, SB, SNSVe, blc3, theta, P, b1, ipiv, total;
+  int N, S, St, T1, B, Vf, tmp, work, Ve, SB, SNSVe, blc3, theta, P, b1, ipiv, total;
 };
 __host__ __device__ inline DiffSmem diff_layout(int max_vsf, int max_vse) {
   const int F = 3 * max_vsf, E = 3 * max_vse;
@@ -181,8 +199,7 @@ __host__ __device__ inline DiffSmem diff_layout(int max_vsf, int max_vse) {
   L.N = o, o += F * F;
   L.S = o, o += F * E;
   L.St = o, o += E * F;
-  L.T1 = o, o += E * F;
-  L.SNS = o, o += E * E;
+  L.T1 = o, o += E * F;  // SNS (E x E, E <= F) takes N's storage once N is no longer read
   L.B = o, o += F;
   L.Vf = o, o += F;
   L.tmp = o, o += F;
@@ -240,7 +257,7 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
   extern __shared__ double sm[];
   const DiffSmem L = diff_layout(m.max_vsf, m.max_vse);
   const int lane = threadIdx.x;
-  double *N = sm + L.N, *S = sm + L.S, *St = sm + L.St, *T1 = sm + L.T1, *SNS = sm + L.SNS, *B = sm + L.B;
+  double *N = sm + L.N, *S = sm + L.S, *St = sm + L.St, *T1 = sm + L.T1, *B = sm + L.B;
   double *Vf = sm + L.Vf, *tmp = sm + L.tmp, *work = sm + L.work, *Ve = sm + L.Ve, *SB = sm + L.SB;
   double *SNSVe = sm + L.SNSVe, *blc3 = sm + L.blc3, *theta = sm + L.theta, *P = sm + L.P, *b1 = sm + L.b1;
   int* ipiv = reinterpret_cast<int*>(sm + L.ipiv);
@@ -330,12 +347,15 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     for (int i = lane; i < F; i += 32) Vf[i] = Vf[i] + B[i];
     __syncwarp();
     warp_inverse(N, F, ipiv, work, lane);
-    warp_gemm(E, F, F, St, N, T1, lane);
-    warp_gemm(E, E, F, T1, S, SNS, lane);
+    // the products of the reference in an order that frees N before SNS is formed, so
+    // SNS takes N's storage (each product's own arithmetic is unchanged)
     warp_gemv(F, F, N, B, tmp, lane);
+    warp_gemv(F, F, N, Vf, work, lane);  // N^-1 (S Ve + B): the face velocities
+    warp_gemm(E, F, F, St, N, T1, lane);
+    double* SNSm = N;
+    warp_gemm(E, E, F, T1, S, SNSm, lane);
     warp_gemv(E, F, St, tmp, SB, lane);
-    warp_gemv(F, F, N, Vf, B, lane);  // B = N^-1 (S Ve + B): the face velocities
-    warp_gemv(E, E, SNS, Ve, SNSVe, lane);
+    warp_gemv(E, E, SNSm, Ve, SNSVe, lane);
     for (int l = lane; l < ne; l += 32) {
       const int se = m.vse[s0 + l];
       double u[5];
@@ -343,14 +363,14 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
       double* t = dterm + (size_t)D.kd * se;
       for (int i = 0; i < 3; ++i) {
         double mv = 0.0;
-        for (int k = 0; k < 3; ++k) mv = mv + SNS[(3 * l + i) + E * (3 * l + k)] * Ve[3 * l + k];
+        for (int k = 0; k < 3; ++k) mv = mv + SNSm[(3 * l + i) + E * (3 * l + k)] * Ve[3 * l + k];
         t[3 * i] = SNSVe[3 * l + i];
         t[3 * i + 1] = mv;
         t[3 * i + 2] = SB[3 * l + i];
       }
       for (int j = 0; j < 3; ++j)
         for (int i = 0; i < 3; ++i) {
-          t[9 + 2 * (i + 3 * j)] = SNS[(3 * l + i) + E * (3 * l + j)] / u[0];
+          t[9 + 2 * (i + 3 * j)] = SNSm[(3 * l + i) + E * (3 * l + j)] / u[0];
           t[10 + 2 * (i + 3 * j)] = blc3[9 * l + i + 3 * j];
         }
       // viscous work (:285-313)
@@ -363,7 +383,7 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
         const double a = oriented(m, sf, se, nl);
         const int q = 3 * m.sf_loc[sf];
         double vm[3];
-        for (int d = 0; d < 3; ++d) vm[d] = B[q + d] - Ve[3 * l + d];
+        for (int d = 0; d < 3; ++d) vm[d] = work[q + d] - Ve[3 * l + d];
         const double dd = vm[0] * nl[0] + vm[1] * nl[1] + vm[2] * nl[2];
         for (int i = 0; i < 3; ++i)
           for (int j = 0; j < 3; ++j) {
@@ -383,7 +403,7 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
         double sv[3];
         for (int i = 0; i < 3; ++i) {
           double s = 0.0;
-          for (int c = 0; c < 3; ++c) s = s + Spc[i][c] * B[q + c];
+          for (int c = 0; c < 3; ++c) s = s + Spc[i][c] * work[q + c];
           sv[i] = s;
         }
         t[27 + k] = a * (sv[0] * nl[0] + sv[1] * nl[1] + sv[2] * nl[2]);
@@ -434,9 +454,9 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     }
     __syncwarp();
     warp_inverse(N, nf, ipiv, work, lane);
-    warp_gemm(ne, nf, nf, St, N, T1, lane);
-    warp_gemm(ne, ne, nf, T1, S, SNS, lane);
     warp_gemv(nf, nf, N, B, tmp, lane);
+    warp_gemm(ne, nf, nf, St, N, T1, lane);
+    warp_gemm(ne, ne, nf, T1, S, SNSm, lane);
     warp_gemv(ne, nf, St, tmp, SB, lane);
     for (int l = lane; l < ne; l += 32) {
       double u[5];
@@ -456,8 +476,8 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
       double u[5];
       load_u(U, m.se_elem[se], u);
       double* t = dterm + (size_t)D.kd * se;
-      for (int p = 0; p < ne; ++p) t[kDiffHead + p] = SNS[l + ne * p] * theta[p];
-      const double snl = SNS[l + ne * l], cc = b1[l] - snl;
+      for (int p = 0; p < ne; ++p) t[kDiffHead + p] = SNSm[l + ne * p] * theta[p];
+      const double snl = SNSm[l + ne * l], cc = b1[l] - snl;
       for (int k = 0; k < 5; ++k) t[31 + k] = cc * P[5 * l + k];
       double pu = 0.0;
       for (int k = 0; k < 5; ++k) pu = pu + P[5 * l + k] * u[k];
