@@ -61,6 +61,8 @@ def load():
         lib.or_ns_flux.argtypes = [C.c_int, PD, PD, PD, PD, PD]
         lib.or_lu3.argtypes = [PD, PD, PD]
         lib.or_potential_flow.argtypes = [PD, C.c_int, PD]
+        lib.or_lapack_inverse.argtypes = [C.c_int, PD]
+        lib.or_lapack_solve.argtypes = [C.c_int, PD, PD]
         lib.or_ns_set_diffusion.argtypes = [C.c_int, C.c_int, PD, C.c_int, PI, PD, PI, PD]
         lib.or_bcsr_matmul.argtypes = [C.c_int, C.c_int, C.c_int, PI, PI, PD, PD, PD]
         lib.or_bcsr_diag.argtypes = [C.c_int, C.c_int, PI, PI, PD, PD, PD]

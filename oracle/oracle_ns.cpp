@@ -1676,6 +1676,14 @@ void or_ns_set_diffusion(int active, int use_sutherland, const double* dc4, int 
     for (int k = 0; k < 3; ++k) g_diff.valV[i][k] = valV[3 * i + k];
   }
 }
+// inv_lapack (dgetrf + dgetri) of the n x n column-major a, in place
+void or_lapack_inverse(int n, double* a) { lapack_inverse(n, a); }
+// lu_solve_inplace_lapack: a (n x n column-major) overwritten by its factors, b by x
+void or_lapack_solve(int n, double* a, double* b) {
+  std::vector<int> ipiv(n);
+  lapack_getrf(n, a, ipiv.data());
+  lapack_getrs(n, a, ipiv.data(), b);
+}
 // sol_potential_flow_2d / _3d at x (primitive w)
 void or_potential_flow(const double* x, int three_d, double* w) { potential_flow(x, three_d != 0, w); }
 

@@ -89,3 +89,30 @@ def test_diffusion_changes_the_inviscid_result(oracle_lib):
     assert o.ns_run(_cfg(use_sutherland=1, diff_dc=[0.05, 0.05, 0.4, CV]), c, 3)[0] == 0
     assert np.isfinite(a).all() and np.isfinite(c).all()
     assert np.abs(a - b).max() > 1e-4 and np.abs(c - a).max() > 1e-6
+
+
+def test_linear_temperature_is_steady_on_an_orthogonal_slab(oracle_lib):
+    """Fluid at rest at uniform pressure with a temperature linear in x between two
+    Dirichlet walls at the matching temperatures (adiabatic elsewhere): the heat flux is
+    uniform, so nothing changes — to round-off on an orthogonal slab, where the sub-cell
+    flux reconstruction is exact for linear fields."""
+    from oracle.oracle import OracleMesh
+    from subfv_b200 import meshgen
+    raw = meshgen.tag_slab_sides(meshgen.hex_slab(NX, NY, jitter=0.0, seed=3), NX, NY,
+                                 {"xlo": 1, "xhi": 2, "ylo": 3, "yhi": 4})
+    o = OracleMesh(raw)
+    x = o.geom("elem_coord")[:, 0]
+    T = 0.4 + 0.1 * (x + 0.5)
+    e = CV * T
+    rho = 1.0 / (0.4 * e)
+    sol = np.ascontiguousarray(np.column_stack([rho, np.zeros((o.n_elems, 3)), rho * e]))
+    s = sol.copy()
+    kw = dict(bc_type_T=np.array([2, 2, 1, 1], np.int32), bc_val_T=np.array([0.4, 0.5, 0, 0]))
+    st, _, _, _, _, _ = o.ns_run(_cfg(**kw), s, 4)
+    assert st == 0
+    np.testing.assert_allclose(s, sol, rtol=0, atol=1e-14)
+    # the same field with a colder right wall does change
+    s2 = sol.copy()
+    kw["bc_val_T"] = np.array([0.4, 0.45, 0, 0])
+    assert o.ns_run(_cfg(**kw), s2, 4)[0] == 0
+    assert np.abs(s2 - sol).max() > 1e-6
