@@ -72,6 +72,12 @@ void subfv_msh_destroy(subfv_msh* m);
    sol (5, n_elems) conservative */
 int subfv_write_sol_vtu(const char* path, const subfv_topology* t, const double* sol, const double* delta,
                         const double* vp, const double* elem_coord, double Cv_p, double mu);
+/* write_sol_vtu_lag (lagrange_io_module.F90:26-289): the same mesh part, point data Vp
+   (3, n_vert) and Pp (nodal pressure, may be NULL), cell data Centroid / Rxy / R
+   (elem_coord, may be NULL), Tag, MPI_Color, Density (1 / tau), Velocity, Pressure and
+   Internal_energy of the Lagrangian state sol (tau, u, v, w, E) */
+int subfv_write_sol_vtu_lag(const char* path, const subfv_topology* t, const double* sol, const double* vp,
+                            const double* pp, const double* elem_coord);
 /* restart_from_vtu_file (ns_io_module.F90:1333-1382): Density, Momentum and Energy (per
    unit mass) of a VTU written above, into sol (5, n_elems) */
 int subfv_restart_from_vtu(const char* path, int64_t n_elems, double* sol);

@@ -40,6 +40,7 @@ SIGNATURES = {
     "subfv_ns_prepare": (c_int, [P]),
     "subfv_write_sol_vtu": (c_int, [c_char_p, P, PD, PD, PD, PD, c_dbl, c_dbl]),
     "subfv_restart_from_vtu": (c_int, [c_char_p, c_i64, PD]),
+    "subfv_write_sol_vtu_lag": (c_int, [c_char_p, P, PD, PD, PD, PD]),
     "subfv_mesh_create": (c_int, [P, C.POINTER(P)]),
     "subfv_mesh_create_from_topology": (c_int, [P, c_int, C.POINTER(P)]),
     "subfv_mesh_destroy": (c_int, [P]),

@@ -1,6 +1,7 @@
 // Mesh and solution files on the host: the gmsh MSH2 / MSH4 (ASCII) readers of
-// src/mesh/mesh_reading_module.F90:154-1324 (one process), the VTU solution writer of
-// src/ns/ns_io_module.F90:403-884 (its cell fields) and the VTU restart reader of
+// src/mesh/mesh_reading_module.F90:154-1324 (one process), the VTU solution writers of
+// src/ns/ns_io_module.F90:403-884 (its cell fields) and
+// src/lagrange/lagrange_io_module.F90:26-289, and the VTU restart reader of
 // src/ns/ns_io_module.F90:1333-1382.
 #include <algorithm>
 #include <cmath>
@@ -288,6 +289,80 @@ std::vector<int32_t> topo_array(const subfv_topology* t, const char* name) {
 
 }  // namespace
 
+// The VTU's mesh part shared by the Euler and Lagrangian writers: header, points,
+// polyhedral cells with their faces (the reference writes cell type 42); leaves the file
+// open before the point data. Returns the number of cells (0 on error).
+static int64_t write_vtu_mesh(std::FILE* f, const subfv_topology* t, std::vector<int32_t>& etag, int64_t& nv) {
+  const auto ev_off = topo_array(t, "elem_vert_off"), ev = topo_array(t, "elem_vert");
+  const auto ef_off = topo_array(t, "elem_face_off"), ef = topo_array(t, "elem_face");
+  const auto fv_off = topo_array(t, "face_vert_off"), fv = topo_array(t, "face_vert");
+  etag = topo_array(t, "elem_tag");
+  const int64_t ne = (int64_t)ev_off.size() - 1;
+  nv = subfv_topology_array_len(t, "vert_is_bound");
+  if (ne < 1 || nv < 1) return 0;
+  std::vector<double> x(3 * nv);
+  subfv_topology_coords(t, x.data());
+  double dmin = 1e100, dmax = -1e100;
+  for (double c : x) dmin = std::min(dmin, c), dmax = std::max(dmax, c);
+  std::fprintf(f, " <VTKFile type='UnstructuredGrid' version='1.0' byte_order='LittleEndian' header_type='UInt64'>\n");
+  std::fprintf(f, " <UnstructuredGrid>\n <Piece NumberOfPoints='%lld' NumberOfCells='%lld'>\n", (long long)nv,
+               (long long)ne);
+  std::fprintf(f, " <Points>\n <DataArray type='Float64' Name='Points' NumberOfComponents='3' format='ascii' "
+                  "RangeMin='%.17g' RangeMax='%.17g'>\n", dmin, dmax);
+  for (int64_t i = 0; i < nv; ++i) {
+    for (int d = 0; d < 3; ++d) put(f, x[3 * i + d]);
+    std::fputc('\n', f);
+  }
+  std::fprintf(f, " </DataArray>\n </Points>\n <Cells>\n");
+  std::fprintf(f, " <DataArray type='Int64' Name='connectivity' format='ascii' RangeMin='0' RangeMax='%lld'>\n",
+               (long long)(nv - 1));
+  for (int64_t c = 0; c < ne; ++c) {
+    for (int q = ev_off[c]; q < ev_off[c + 1]; ++q) std::fprintf(f, " %d", ev[q] - 1);
+    std::fputc('\n', f);
+  }
+  std::fprintf(f, " </DataArray>\n <DataArray type='Int64' Name='offsets' format='ascii' RangeMin='0' "
+                  "RangeMax='%d'>\n", ev_off[ne]);
+  for (int64_t c = 0; c < ne; ++c) std::fprintf(f, " %d\n", ev_off[c + 1]);
+  std::fprintf(f, " </DataArray>\n <DataArray type='UInt8' Name='types' format='ascii' RangeMin='42' "
+                  "RangeMax='42'>\n");
+  for (int64_t c = 0; c < ne; ++c) std::fprintf(f, " 42\n");  // polyhedra, faces below
+  std::fprintf(f, " </DataArray>\n <DataArray type='Int64' Name='faces' format='ascii' RangeMin='0' "
+                  "RangeMax='%lld'>\n", (long long)(nv - 1));
+  std::vector<int64_t> foff(ne);
+  int64_t s = 0;
+  for (int64_t c = 0; c < ne; ++c) {
+    const int nfc = ef_off[c + 1] - ef_off[c];
+    std::fprintf(f, " %d\n", nfc);
+    s += 1;
+    for (int q = ef_off[c]; q < ef_off[c + 1]; ++q) {
+      const int fc = ef[q] - 1;
+      std::fprintf(f, " %d", fv_off[fc + 1] - fv_off[fc]);
+      for (int k = fv_off[fc]; k < fv_off[fc + 1]; ++k) std::fprintf(f, " %d", fv[k] - 1);
+      std::fputc('\n', f);
+      s += 1 + fv_off[fc + 1] - fv_off[fc];
+    }
+    foff[c] = s;
+  }
+  std::fprintf(f, " </DataArray>\n <DataArray type='Int64' Name='faceoffsets' format='ascii' RangeMin='0' "
+                  "RangeMax='%lld'>\n", (long long)s);
+  for (int64_t c = 0; c < ne; ++c) std::fprintf(f, " %lld\n", (long long)foff[c]);
+  std::fprintf(f, " </DataArray>\n </Cells>\n");
+  return ne;
+}
+
+struct VtuFields {  // writes one DataArray per call, one line per entity
+  std::FILE* f;
+  template <class Fn>
+  void operator()(const char* type, const char* name, int nc, int64_t n, Fn&& fn) {
+    std::fprintf(f, " <DataArray type='%s' Name='%s' format='ascii' NumberOfComponents='%d'>\n", type, name, nc);
+    for (int64_t i = 0; i < n; ++i) {
+      fn(i);
+      std::fputc('\n', f);
+    }
+    std::fprintf(f, " </DataArray>\n");
+  }
+};
+
 extern "C" {
 
 int subfv_msh_read(const char* path, int n_bc, const char* const* bc_names, subfv_msh** out) {
@@ -373,76 +448,26 @@ int subfv_write_sol_vtu(const char* path, const subfv_topology* t, const double*
     return -2;
   }
   const double G = 1.4;  // ns_global_data_module.F90:9
-  const auto ev_off = topo_array(t, "elem_vert_off"), ev = topo_array(t, "elem_vert");
-  const auto ef_off = topo_array(t, "elem_face_off"), ef = topo_array(t, "elem_face");
-  const auto fv_off = topo_array(t, "face_vert_off"), fv = topo_array(t, "face_vert");
-  const auto etag = topo_array(t, "elem_tag");
-  const int64_t ne = (int64_t)ev_off.size() - 1;
-  const int64_t nv = subfv_topology_array_len(t, "vert_is_bound");
-  if (ne < 1 || nv < 1) {
-    set_error("subfv_write_sol_vtu: empty topology");
-    return -2;
-  }
-  std::vector<double> x(3 * nv);
-  subfv_topology_coords(t, x.data());
   std::FILE* f = std::fopen(path, "w");
   if (!f) {
     set_error(std::string("subfv_write_sol_vtu: cannot open ") + path);
     return -2;
   }
-  double dmin = 1e100, dmax = -1e100;
-  for (double c : x) dmin = std::min(dmin, c), dmax = std::max(dmax, c);
-  std::fprintf(f, " <VTKFile type='UnstructuredGrid' version='1.0' byte_order='LittleEndian' header_type='UInt64'>\n");
-  std::fprintf(f, " <UnstructuredGrid>\n <Piece NumberOfPoints='%lld' NumberOfCells='%lld'>\n", (long long)nv,
-               (long long)ne);
-  std::fprintf(f, " <Points>\n <DataArray type='Float64' Name='Points' NumberOfComponents='3' format='ascii' "
-                  "RangeMin='%.17g' RangeMax='%.17g'>\n", dmin, dmax);
-  for (int64_t i = 0; i < nv; ++i) {
-    for (int d = 0; d < 3; ++d) put(f, x[3 * i + d]);
-    std::fputc('\n', f);
+  std::vector<int32_t> etag;
+  int64_t nv = 0;
+  const int64_t ne = write_vtu_mesh(f, t, etag, nv);
+  if (ne == 0) {
+    std::fclose(f);
+    set_error("subfv_write_sol_vtu: empty topology");
+    return -2;
   }
-  std::fprintf(f, " </DataArray>\n </Points>\n <Cells>\n");
-  std::fprintf(f, " <DataArray type='Int64' Name='connectivity' format='ascii' RangeMin='0' RangeMax='%lld'>\n",
-               (long long)(nv - 1));
-  for (int64_t c = 0; c < ne; ++c) {
-    for (int q = ev_off[c]; q < ev_off[c + 1]; ++q) std::fprintf(f, " %d", ev[q] - 1);
-    std::fputc('\n', f);
-  }
-  std::fprintf(f, " </DataArray>\n <DataArray type='Int64' Name='offsets' format='ascii' RangeMin='0' "
-                  "RangeMax='%d'>\n", ev_off[ne]);
-  for (int64_t c = 0; c < ne; ++c) std::fprintf(f, " %d\n", ev_off[c + 1]);
-  std::fprintf(f, " </DataArray>\n <DataArray type='UInt8' Name='types' format='ascii' RangeMin='42' "
-                  "RangeMax='42'>\n");
-  for (int64_t c = 0; c < ne; ++c) std::fprintf(f, " 42\n");  // polyhedra, faces below
-  std::fprintf(f, " </DataArray>\n <DataArray type='Int64' Name='faces' format='ascii' RangeMin='0' "
-                  "RangeMax='%lld'>\n", (long long)(nv - 1));
-  std::vector<int64_t> foff(ne);
-  int64_t s = 0;
-  for (int64_t c = 0; c < ne; ++c) {
-    const int nfc = ef_off[c + 1] - ef_off[c];
-    std::fprintf(f, " %d\n", nfc);
-    s += 1;
-    for (int q = ef_off[c]; q < ef_off[c + 1]; ++q) {
-      const int fc = ef[q] - 1;
-      std::fprintf(f, " %d", fv_off[fc + 1] - fv_off[fc]);
-      for (int k = fv_off[fc]; k < fv_off[fc + 1]; ++k) std::fprintf(f, " %d", fv[k] - 1);
-      std::fputc('\n', f);
-      s += 1 + fv_off[fc + 1] - fv_off[fc];
-    }
-    foff[c] = s;
-  }
-  std::fprintf(f, " </DataArray>\n <DataArray type='Int64' Name='faceoffsets' format='ascii' RangeMin='0' "
-                  "RangeMax='%lld'>\n", (long long)s);
-  for (int64_t c = 0; c < ne; ++c) std::fprintf(f, " %lld\n", (long long)foff[c]);
-  std::fprintf(f, " </DataArray>\n </Cells>\n");
+  VtuFields fw{f};
   if (vp) {
-    std::fprintf(f, " <PointData>\n <DataArray type='Float64' Name='Nodal_Velocity' format='ascii' "
-                    "NumberOfComponents='3'>\n");
-    for (int64_t i = 0; i < nv; ++i) {
+    std::fprintf(f, " <PointData>\n");
+    fw("Float64", "Nodal_Velocity", 3, nv, [&](int64_t i) {
       for (int d = 0; d < 3; ++d) put(f, vp[3 * i + d]);
-      std::fputc('\n', f);
-    }
-    std::fprintf(f, " </DataArray>\n </PointData>\n");
+    });
+    std::fprintf(f, " </PointData>\n");
   }
   std::fprintf(f, " <CellData>\n");
   auto field = [&](const char* type, const char* name, int nc, auto&& fn) {
@@ -498,6 +523,64 @@ int subfv_write_sol_vtu(const char* path, const subfv_topology* t, const double*
   std::fclose(f);
   if (!ok) {
     set_error("subfv_write_sol_vtu: write failed");
+    return -1;
+  }
+  return 0;
+}
+
+int subfv_write_sol_vtu_lag(const char* path, const subfv_topology* t, const double* sol, const double* vp,
+                            const double* pp, const double* elem_coord) {
+  if (!path || !t || !sol || !vp) {
+    set_error("subfv_write_sol_vtu_lag: bad argument");
+    return -2;
+  }
+  const double G = 1.4;  // the Lagrangian module's gamma
+  std::FILE* f = std::fopen(path, "w");
+  if (!f) {
+    set_error(std::string("subfv_write_sol_vtu_lag: cannot open ") + path);
+    return -2;
+  }
+  std::vector<int32_t> etag;
+  int64_t nv = 0;
+  const int64_t ne = write_vtu_mesh(f, t, etag, nv);
+  if (ne == 0) {
+    std::fclose(f);
+    set_error("subfv_write_sol_vtu_lag: empty topology");
+    return -2;
+  }
+  VtuFields fw{f};
+  auto u = [&](int64_t c) { return sol + 5 * c; };
+  auto pressure = [&](int64_t c) {  // lagrange_module.F90:429-436
+    const double* q = u(c);
+    const double n = norm2(q + 1, 3);
+    return (G - 1.0) / q[0] * (q[4] - 0.5 * (n * n));
+  };
+  std::fprintf(f, " <PointData>\n");
+  fw("Float64", "Vp", 3, nv, [&](int64_t i) {
+    for (int d = 0; d < 3; ++d) put(f, vp[3 * i + d]);
+  });
+  if (pp) fw("Float64", "Pp", 1, nv, [&](int64_t i) { put(f, pp[i]); });
+  std::fprintf(f, " </PointData>\n <CellData>\n");
+  if (elem_coord) {
+    fw("Float64", "Centroid", 3, ne, [&](int64_t c) {
+      for (int d = 0; d < 3; ++d) put(f, elem_coord[3 * c + d]);
+    });
+    fw("Float64", "Rxy", 1, ne, [&](int64_t c) { put(f, norm2(elem_coord + 3 * c, 2)); });
+    fw("Float64", "R", 1, ne, [&](int64_t c) { put(f, norm2(elem_coord + 3 * c, 3)); });
+  }
+  fw("Int32", "Tag", 1, ne, [&](int64_t c) { std::fprintf(f, " %d", etag.empty() ? -1 : etag[c]); });
+  fw("Int32", "MPI_Color", 1, ne, [&](int64_t) { std::fprintf(f, " 0"); });
+  fw("Float64", "Density", 1, ne, [&](int64_t c) { put(f, 1.0 / u(c)[0]); });
+  fw("Float64", "Velocity", 3, ne, [&](int64_t c) {
+    for (int d = 1; d < 4; ++d) put(f, u(c)[d]);
+  });
+  fw("Float64", "Pressure", 1, ne, [&](int64_t c) { put(f, pressure(c)); });
+  fw("Float64", "Internal_energy", 1, ne, [&](int64_t c) { put(f, pressure(c) * u(c)[0] / (G - 1.0)); });
+  std::fprintf(f, " </CellData>\n </Piece>\n </UnstructuredGrid>\n </VTKFile>\n");
+  const bool ok = std::ferror(f) == 0;
+  std::fclose(f);
+  if (!ok) {
+    set_error("subfv_write_sol_vtu_lag: write failed");
     return -1;
   }
   return 0;

@@ -48,6 +48,14 @@ def write_sol_vtu(path: str, topology, sol, delta=None, vp=None, elem_coord=None
           "subfv_write_sol_vtu")
 
 
+def write_sol_vtu_lag(path: str, topology, sol, vp, pp=None, elem_coord=None) -> None:
+    """The Lagrangian solver's solution file for states sol (n, 5) = (tau, u, v, w, E),
+    nodal velocities vp (n_vert, 3) and optional nodal pressures pp."""
+    arrs = [None if a is None else f64(a) for a in (sol, vp, pp, elem_coord)]
+    ptr = [None if a is None else pd(a) for a in arrs]
+    check(_lib.load().subfv_write_sol_vtu_lag(str(path).encode(), topology._h, *ptr), "subfv_write_sol_vtu_lag")
+
+
 def restart_from_vtu(path: str, n_elems: int) -> np.ndarray:
     """Cell states (n_elems, 5) from a solution VTU (Density, Momentum, Energy per unit mass)."""
     sol = np.empty((n_elems, 5))

@@ -242,3 +242,31 @@ def test_msh_mesh_runs_on_gpu_like_oracle(native, oracle_lib, cuda_ok, tmp_path)
     assert st == st_o == 0
     np.testing.assert_array_equal(rhs, rhs_o)
     np.testing.assert_array_equal(sl, sl_o)
+
+
+def test_lagrangian_vtu(native, tmp_path):
+    """write_sol_vtu_lag's fields from a Lagrangian state (tau, u, v, w, E)."""
+    from subfv_b200.io import write_sol_vtu_lag
+    from subfv_b200.mesh import Topology
+    raw = _mesh("prism")
+    topo = Topology(raw)
+    rng = np.random.default_rng(4)
+    n = raw.n_elems
+    tau = rng.uniform(0.5, 2, n)
+    u = rng.uniform(-1, 1, (n, 3))
+    p = rng.uniform(0.5, 2, n)
+    E = p * tau / 0.4 + 0.5 * (u ** 2).sum(1)
+    sol = np.column_stack([tau, u, E])
+    vp = rng.normal(size=(raw.n_vert, 3))
+    cc = rng.normal(size=(n, 3))
+    path = tmp_path / "lag.vtu"
+    write_sol_vtu_lag(path, topo, sol, vp, pp=np.ones(raw.n_vert), elem_coord=cc)
+    root = ET.parse(path).getroot()
+    arrays = {a.get("Name"): np.array(a.text.split(), float) for a in root.iter("DataArray")}
+    np.testing.assert_allclose(arrays["Density"], 1 / tau, rtol=1e-15)
+    np.testing.assert_allclose(arrays["Pressure"], p, rtol=1e-13)
+    np.testing.assert_allclose(arrays["Internal_energy"], p * tau / 0.4, rtol=1e-13)
+    np.testing.assert_allclose(arrays["Rxy"], np.hypot(cc[:, 0], cc[:, 1]), rtol=1e-14)
+    np.testing.assert_allclose(arrays["Vp"].reshape(-1, 3), vp, rtol=1e-15)
+    assert arrays["Pp"].size == raw.n_vert and arrays["Tag"].size == n
+    topo.close()
