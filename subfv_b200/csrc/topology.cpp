@@ -374,21 +374,24 @@ int build_topology(const RawMeshView& in, Topology& T, std::string* err) {
   sesfo.assign(nse + 1, 0);
   sesf.clear();
   sesf.reserve(3 * (size_t)nse);
-  for (int e = 1; e <= ne; ++e)
+  std::vector<int32_t> lv;  // the cell's subfaces' vertices, gathered once per cell
+  for (int e = 1; e <= ne; ++e) {
+    const int q0 = esfo[e - 1], q1 = esfo[e];
+    lv.resize(q1 - q0);
+    for (int q = q0; q < q1; ++q) lv[q - q0] = sfv[esf[q] - 1];
     for (int j = ev_off[e - 1]; j < ev_off[e]; ++j) {
       int id = j + 1;
       ese[j] = id;
       see[j] = e;
       sev[j] = 0;
-      for (int q = esfo[e - 1]; q < esfo[e]; ++q) {
-        int sf = esf[q];
-        if (sfv[sf - 1] == ev[j]) {
-          sev[j] = sfv[sf - 1];
-          sesf.push_back(sf);
+      for (int q = q0; q < q1; ++q)
+        if (lv[q - q0] == ev[j]) {
+          sev[j] = lv[q - q0];
+          sesf.push_back(esf[q]);
         }
-      }
       sesfo[id] = (int32_t)sesf.size();
     }
+  }
   // (:454-473)
   V& sfls = T.arr["sub_face_left_sub_elem"];
   V& sfrs = T.arr["sub_face_right_sub_elem"];
