@@ -270,3 +270,27 @@ def test_lagrangian_vtu(native, tmp_path):
     np.testing.assert_allclose(arrays["Vp"].reshape(-1, 3), vp, rtol=1e-15)
     assert arrays["Pp"].size == raw.n_vert and arrays["Tag"].size == n
     topo.close()
+
+
+def test_msh_mesh_runs_in_the_oracle(native, oracle_lib, tmp_path):
+    """A named-boundary MSH mesh drives the oracle's explicit loop: freestream entering
+    through one side leaves through the supersonic-outflow side."""
+    from oracle.oracle import OracleMesh
+    from subfv_b200.io import read_msh
+    raw = _mesh("hex")
+    p = tmp_path / "m2.msh"
+    _write_msh2(p, raw)
+    got = read_msh(p, ["xlo", "xhi", "ylo", "yhi"])
+    o = OracleMesh(got)
+    n = o.n_elems
+    w = np.tile([1.0, 0.0, 0.0, 0.0, 1.0], (n, 1))
+    sol = np.ascontiguousarray(np.column_stack([w[:, 0], w[:, 1:4] * w[:, :1], w[:, 4] / 0.4]))
+    inflow = [1.2, 0.5, 0.0, 0.0, 1.3]
+    cfg = dict(scheme=1, second_order=1, method=4, bc_style=2, b2d=1, exclude_bound_vert=0, local_time_step=0,
+               cfl=0.3, tmax=1e30, n_bc=4, bc_type=np.array([3, 4, 1, 1], np.int32),
+               bc_val=np.array([inflow, [0] * 5, [0] * 5, [0] * 5], float))
+    st, it, t, _, _, _ = o.ns_run(cfg, sol, 29)
+    assert st == 0 and it == 30 and np.isfinite(sol).all()
+    x = o.geom("elem_coord")[:, 0]
+    left = sol[x < x.min() + 0.2]
+    assert left[:, 0].mean() > 1.05 and left[:, 1].mean() > 0.1  # the inflow has come in
