@@ -87,6 +87,61 @@ def hex_slab(nx, ny, x0=-0.5, x1=0.5, y0=-0.5, y1=0.5, z0=-0.5, z1=0.5, jitter=0
                    ev.astype(np.int32).ravel(), b2d=True)
 
 
+def _norm2(a):
+    """gfortran's NORM2 (scaled sum of squares) over the last axis."""
+    a = np.abs(np.asarray(a, np.float64))
+    scale = np.ones(a.shape[:-1])
+    res = np.zeros(a.shape[:-1])
+    for i in range(a.shape[-1]):
+        x = a[..., i]
+        nz = x != 0.0
+        big = nz & (x > scale)
+        q = np.where(big, scale / np.where(big, x, 1.0), 0.0)
+        res = np.where(big, 1.0 + res * q * q, res)
+        scale = np.where(big, x, scale)
+        small = nz & ~big
+        q2 = np.where(small, x / scale, 0.0)
+        res = np.where(small, res + q2 * q2, res)
+    return scale * np.sqrt(res)
+
+
+def map_cylinder(raw: RawMesh, dimen: int) -> RawMesh:
+    """A copy with the vertices moved by cylinder_mapping (mesh_geometry_module.F90:413-518),
+    the radial stretching the reference applies to its half-cylinder meshes before
+    build_mesh (dimen 2: unit cylinder about z, 21: radius 0.5, 3: unit sphere)."""
+    c = np.asarray(raw.coords, np.float64)
+    x, y = c[:, 0], c[:, 1]
+    if dimen == 2 or dimen == 21:
+        s = 2.0 if dimen == 21 else 1.0
+        r = _norm2(np.column_stack([s * x, s * y]))
+        th = np.arctan2(s * y, -s * x)
+    elif dimen == 3:
+        r = _norm2(c)
+        th = np.arctan2(_norm2(c[:, 1:]), -x)
+    else:
+        raise ValueError("dimen must be 2, 21 or 3")
+    r1, r2 = 1.0, 1.3851721918740656
+    t2 = th * th
+    t4 = t2 * t2
+    new_r2 = (r2 + 0.22082080765324227 * t2 + 0.07247276314520341 * t4 - 0.01622444200319442 * (t4 * t2)
+              + 0.00780545523147566 * (t4 * t4))
+    new_r = (r - r1) * (new_r2 - r1) / (r2 - r1) + r1
+    out = c.copy()
+    if dimen == 3:
+        out = c + (new_r - r)[:, None] * c
+    else:
+        out[:, 0] = -new_r * np.cos(th) / s
+        out[:, 1] = new_r * np.sin(th) / s
+    return RawMesh(out, raw.elem_kind, raw.elem_vert_off, raw.elem_vert, raw.bface_off, raw.bface_vert,
+                   raw.bface_tag, b2d=raw.b2d, periodic=raw.periodic)
+
+
+def rescale_mesh(raw: RawMesh, sf: float) -> RawMesh:
+    """A copy with every coordinate scaled by sf (mesh_reading_module.F90:1366-1377)."""
+    return RawMesh(sf * np.asarray(raw.coords, np.float64), raw.elem_kind, raw.elem_vert_off, raw.elem_vert,
+                   raw.bface_off, raw.bface_vert, raw.bface_tag, b2d=raw.b2d, periodic=raw.periodic)
+
+
 def tag_slab_sides(raw: RawMesh, nx: int, ny: int, tags: dict) -> RawMesh:
     """A copy of a hex_slab / prism_slab mesh of nx*ny columns with its side boundaries
     tagged (the MSH2 boundary elements the reference reads): tags maps "xlo", "xhi",
