@@ -103,3 +103,23 @@ def init_double_mach(elem_coord: np.ndarray):
     post = primit_to_conserv([8.0, 7.145, -4.125, 0.0, 116.5])
     below = x[:, 1] < 1.732 * (x[:, 0] - 0.1667)
     return np.ascontiguousarray(np.where(below[:, None], pre, post)), 0.2
+
+
+def _norm2_rows(a: np.ndarray) -> np.ndarray:
+    """gfortran's NORM2 row by row (scaled sum of squares)."""
+    from .meshgen import _norm2
+    return _norm2(a)
+
+
+def init_sedov(elem_coord: np.ndarray, elem_volume: np.ndarray, boundary_2d: bool = True) -> np.ndarray:
+    """init_sedov (ns_euler_module.F90:64-112): rho = 1 at rest with E = 1e-16 / (gamma - 1),
+    and the blast energy (0.984042 in 2-D, 0.851072 in 3-D) over the volume of the first
+    cell of smallest centroid radius (in the x-y plane for boundary_2d)."""
+    x = np.asarray(elem_coord, np.float64)
+    r = _norm2_rows(x[:, :2] if boundary_2d else x)
+    imin = int(np.argmin(r))  # the first index of the smallest radius, as the strict < scan keeps
+    sol = np.zeros((x.shape[0], 5))
+    sol[:, 0] = 1.0
+    sol[:, 4] = 1e-16 / (GAMMA - 1.0)
+    sol[imin, 4] = (0.984042 if boundary_2d else 0.851072) / float(elem_volume[imin])
+    return np.ascontiguousarray(sol)

@@ -53,3 +53,14 @@ def test_piecewise_states():
     assert tk == pytest.approx(80.0) and np.all(np.abs(kh[:, 0] - 1.4) <= 1e-2 + 1e-15)
     u = init_uniform(4, [1.0, 0.1, 0.2, 0.3, 2.0])
     assert u.shape == (4, 5) and np.all(u == u[0])
+
+
+def test_sedov_energy_in_the_central_cell():
+    from subfv_b200.ns_init import init_sedov
+    x = np.array([[0.3, 0.1, 0.0], [0.05, -0.02, 0.4], [-0.05, 0.02, 0.0], [1.0, 1.0, 1.0]])
+    vol = np.array([0.1, 0.2, 0.3, 0.4])
+    s = init_sedov(x, vol, boundary_2d=True)
+    assert s[1, 4] == pytest.approx(0.984042 / 0.2)  # first of the two cells at the smallest radius
+    assert np.all(s[[0, 2, 3], 4] == 1e-16 / (1.4 - 1.0)) and np.all(s[:, 0] == 1.0)
+    s3 = init_sedov(x, vol, boundary_2d=False)
+    assert s3[2, 4] == pytest.approx(0.851072 / 0.3)
