@@ -156,9 +156,13 @@ int subfv_compute_dt(subfv_mesh* m, const double* sol, double cfl, const double*
  * are device buffers the caller owns; nothing is allocated or freed. Scratch is a
  * static 128 KiB device array (one minimum per 256 cells), so meshes above 4,194,304
  * cells are rejected (-4). The first call on a device looks up that array's device
- * address: make it before any stream capture. Calls share the array: do not let two
- * calls overlap on the GPU. Runs on the mesh's stream and returns after it finishes;
- * the result equals subfv_compute_dt's. */
+ * address (and, under lazy module loading, loads the module that holds it): make it at
+ * start-up, before device memory is reserved and before any stream capture. Calls
+ * share the array: do not let two calls overlap on the GPU. Runs on the mesh's stream,
+ * on the mesh's device whichever device is current, and returns after it finishes; the
+ * mesh's stream does not wait for the caller's, so d_sol and d_vp must be complete
+ * before the call. The result and the status (SUBFV_ERR_NONFINITE on a negative or NaN
+ * CFL term) equal subfv_compute_dt's. */
 int subfv_compute_dt_noalloc(subfv_mesh* m, const double* d_sol, const double* d_vp, double cfl, double* d_dt);
 /* move_mesh(mesh, vp, dt) — lagrange_module.F90:772-784 */
 int subfv_move_mesh(subfv_mesh* m, const double* vp, double dt);

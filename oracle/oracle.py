@@ -58,6 +58,7 @@ def load():
         lib.or_ns_run.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_int, C.c_double, PD, PI, PD, PD, PD]
         lib.or_ns_gresho.argtypes = [C.c_void_p, C.c_double, PD]
         lib.or_pinv3.argtypes = [PD]
+        lib.or_set_lapack.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.or_ns_flux.argtypes = [C.c_int, PD, PD, PD, PD, PD]
         lib.or_lu3.argtypes = [PD, PD, PD]
         lib.or_potential_flow.argtypes = [PD, C.c_int, PD]
@@ -75,6 +76,28 @@ def load():
         lib.or_be_jacobian.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_double, PI, PI, PD, C.c_long]
         _lib = lib
     return _lib
+
+
+def _capsule_ptr(name):
+    """The C function pointer behind scipy.linalg.cython_lapack's exported routine."""
+    from scipy.linalg import cython_lapack
+    cap = cython_lapack.__pyx_capi__[name]
+    get_name = C.pythonapi.PyCapsule_GetName
+    get_name.restype, get_name.argtypes = C.c_char_p, [C.py_object]
+    get_ptr = C.pythonapi.PyCapsule_GetPointer
+    get_ptr.restype, get_ptr.argtypes = C.c_void_p, [C.py_object, C.c_char_p]
+    return get_ptr(cap, get_name(cap))
+
+
+def use_lapack(on: bool):
+    """Route the oracle's 3x3 pseudo-inverse and LU solve through scipy's bundled LAPACK
+    (dgesvd, dgetrf, dgetrs), called as the reference calls system LAPACK
+    (linear_solver_module.F90:643-715); off restores the restated algorithms that the
+    GPU kernels follow."""
+    if on:
+        load().or_set_lapack(_capsule_ptr("dgesvd"), _capsule_ptr("dgetrf"), _capsule_ptr("dgetrs"))
+    else:
+        load().or_set_lapack(None, None, None)
 
 
 def _pd(a):

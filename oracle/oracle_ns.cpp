@@ -110,9 +110,57 @@ static bool inv3_if_regular(double A[3][3]) {
   return true;
 }
 
+// Optional real LAPACK (Fortran calling convention, no hidden string lengths): when set
+// by or_set_lapack, pinv3 and lu_solve3 call it exactly as pseudo_inverse_inplace_lapack
+// and lu_solve_inplace_lapack do (linear_solver_module.F90:643-657, 683-715), in place
+// of the restated algorithms above and below. Test infrastructure only: it measures how
+// far the restatement's results drift from the reference's LAPACK calls.
+typedef void (*dgesvd_fn)(char*, char*, int*, int*, double*, int*, double*, double*, int*, double*, int*, double*,
+                          int*, int*);
+typedef void (*dgetrf_fn)(int*, int*, double*, int*, int*, int*);
+typedef void (*dgetrs_fn)(char*, int*, int*, double*, int*, int*, double*, int*, int*);
+static dgesvd_fn g_dgesvd = nullptr;
+static dgetrf_fn g_dgetrf = nullptr;
+static dgetrs_fn g_dgetrs = nullptr;
+
+// pseudo_inverse_inplace_lapack(3, mat), linear_solver_module.F90:683-715: dgesvd('A', 'O')
+// with LWORK = 5 n (the reference passes 5*n, not the queried size), VT written over A,
+// cut n 1e-12 max(Sigma), then A = matmul(transpose(A), matmul(Sigma_plus, transpose(U)))
+// with gfortran's matmul summing k ascending.
+static void pinv3_lapack(double A[3][3]) {
+  double a[9], U[9], S[3], work[15];
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) a[c * 3 + r] = A[r][c];
+  int n = 3, lda = 3, ldu = 3, ldvt = 3, lwork = 15, info = 0;
+  char ju = 'A', jvt = 'O';
+  g_dgesvd(&ju, &jvt, &n, &n, a, &lda, S, U, &ldu, a, &ldvt, work, &lwork, &info);
+  double smax = S[0];
+  for (int i = 1; i < 3; ++i) smax = std::fmax(smax, S[i]);
+  const double tol = 3 * 1e-12 * smax;
+  double Sp[3][3] = {};
+  for (int i = 0; i < 3; ++i) Sp[i][i] = S[i] > tol ? 1.0 / S[i] : 0.0;
+  double T[3][3];  // matmul(Sigma_plus, transpose(U)): T(i,j) = sum_k Sp(i,k) U(j,k)
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = s + Sp[i][k] * U[k * 3 + j];
+      T[i][j] = s;
+    }
+  for (int i = 0; i < 3; ++i)  // matmul(transpose(VT), T): sum_k VT(k,i) T(k,j)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0.0;
+      for (int k = 0; k < 3; ++k) s = s + a[i * 3 + k] * T[k][j];
+      A[i][j] = s;
+    }
+}
+
 // A[r][c] = mat(r+1, c+1). The inverse when the cut cannot bite, else one-sided Jacobi
 // on the columns: A V = U S.
 void pinv3(double A[3][3]) {
+  if (g_dgesvd) {
+    pinv3_lapack(A);
+    return;
+  }
   if (inv3_if_regular(A)) return;
   double U[3][3], V[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   std::memcpy(U, A, sizeof(U));
@@ -161,6 +209,17 @@ void pinv3(double A[3][3]) {
 
 // dgetrf2 + dgetrs ('N') on a 3x3 system; A is overwritten.
 void lu_solve3(double A[3][3], double* x, const double* b) {
+  if (g_dgetrf && g_dgetrs) {  // lu_solve_inplace_lapack, linear_solver_module.F90:643-657
+    double a[9], bc[3] = {b[0], b[1], b[2]};
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) a[c * 3 + r] = A[r][c];
+    int n = 3, one = 1, ipiv[3], info = 0;
+    char tr = 'N';
+    g_dgetrf(&n, &n, a, &n, ipiv, &info);
+    g_dgetrs(&tr, &n, &one, a, &n, ipiv, bc, &n, &info);
+    for (int k = 0; k < 3; ++k) x[k] = bc[k];
+    return;
+  }
   const double sfmin = 2.2250738585072014e-308;
   int ipiv[3];
   for (int j = 0; j < 3; ++j) {
@@ -1634,6 +1693,11 @@ int or_ns_run(void* h, const int* ic, const double* dc, const int* bc_type, cons
 }
 void or_ns_gresho(void* h, double mach, double* sol) { init_gresho(handle_mesh(h), mach, sol); }
 void or_pinv3(double* a9) { oracle_pinv3(a9); }
+void or_set_lapack(void* dgesvd, void* dgetrf, void* dgetrs) {
+  g_dgesvd = reinterpret_cast<dgesvd_fn>(dgesvd);
+  g_dgetrf = reinterpret_cast<dgetrf_fn>(dgetrf);
+  g_dgetrs = reinterpret_cast<dgetrs_fn>(dgetrs);
+}
 // one subface flux: scheme 3 three_wave, 5 modified_three_wave, else two_wave; lr (5, 2)
 void or_ns_flux(int scheme, const double* wl, const double* wr, const double* n, double* lr10, double* slsr) {
   double lr[2][5];

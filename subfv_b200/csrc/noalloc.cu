@@ -17,8 +17,14 @@
 // work overlaps on the GPU (different streams, or one device used from two threads)
 // race on it and must not be issued concurrently.
 //
-// The arithmetic is that of k_lag_cell's CFL terms (lagrange_module.F90:240-283), so the
-// result equals subfv_compute_dt's bit for bit.
+// The kernels run on the mesh's stream, which does not wait for the caller's streams:
+// d_sol and d_vp must be complete (the stream that wrote them synchronised) before the
+// call. The scratch address is looked up on the device that holds the mesh, whichever
+// device is current, and the caller's current device is restored afterwards.
+//
+// The arithmetic is that of k_lag_cell's CFL terms (lagrange_module.F90:240-283),
+// including the non-finite check that sets the mesh's status word, so the result and
+// the status equal subfv_compute_dt's bit for bit.
 #include <mutex>
 
 #include "../../include/subfv.h"
@@ -53,6 +59,8 @@ __global__ void __launch_bounds__(kNoAllocBlock) k_dt_partial(DevMesh m, const d
     const double* u = sol5 + 5 * (size_t)c;
     double pme = lag_pressure(u[0], u[1], u[2], u[3], u[4]);
     double csnd = sqrt(kGamma * pme * u[0]);
+    const double vse_c = m.vol_se[c < m.nse ? c : 0];  // sub_elem(i) with i the cell (reference quirk)
+    bool bad = false;
     for (int q = m.csf_off[c]; q < m.csf_off[c + 1]; ++q) {
       int e = m.csf[q];
       int p = e >> 1, side = e & 1;
@@ -65,14 +73,17 @@ __global__ void __launch_bounds__(kNoAllocBlock) k_dt_partial(DevMesh m, const d
       int sub = side == 0 ? se.x : se.y;
       double sg = side == 0 ? 1.0 : -1.0;
       const double* vps = vp3 + 3 * (size_t)sv;
-      double t1 = m.vol_se[c] / (area * csnd);
+      double t1 = vse_c / (area * csnd);
       if (t1 < dtloc) dtloc = t1;
+      bad = bad || !(t1 >= 0.0);
       if (sub >= 0) {
         double vn = dot3(vps[0], vps[1], vps[2], sg * fn.x, sg * fn.y, sg * fn.z);
         double t2 = 0.8 * m.vol_se[sub] / (1e-8 + fabs(vn) * fn.w);
         if (t2 < dtloc) dtloc = t2;
+        bad = bad || !(t2 >= 0.0);
       }
     }
+    if (bad) atomicOr(m.status, kErrNonFinite);
   }
   __shared__ double wmin[kNoAllocBlock / 32];
   double x = warp_min_na(dtloc);
@@ -123,12 +134,23 @@ extern "C" int subfv_compute_dt_noalloc(subfv_mesh* mesh, const double* d_sol, c
               "block minima of 256 cells); use subfv_compute_dt");
     return -4;
   }
-  int dev = 0;
-  SUBFV_CUDA(cudaGetDevice(&dev));
+  // the device that holds the mesh (its status word lives there)
+  cudaPointerAttributes attr{};
+  SUBFV_CUDA(cudaPointerGetAttributes(&attr, m.status));
+  const int dev = attr.device;
   if (dev < 0 || dev >= kMaxDevices) {
     set_error("subfv_compute_dt_noalloc: device index out of range");
     return -2;
   }
+  int cur = 0;
+  SUBFV_CUDA(cudaGetDevice(&cur));
+  if (cur != dev) SUBFV_CUDA(cudaSetDevice(dev));
+  struct Restore {
+    int cur, dev;
+    ~Restore() {
+      if (cur != dev) cudaSetDevice(cur);
+    }
+  } restore{cur, dev};
   double* partial = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -139,9 +161,12 @@ extern "C" int subfv_compute_dt_noalloc(subfv_mesh* mesh, const double* d_sol, c
     }
     partial = g_addr[dev];
   }
+  SUBFV_CUDA(cudaMemsetAsync(m.status, 0, sizeof(unsigned), m.stream));
   k_dt_partial<<<nblocks, kNoAllocBlock, 0, m.stream>>>(m, d_sol, d_vp, partial);
   k_dt_final<<<1, kNoAllocBlock, 0, m.stream>>>(partial, nblocks, cfl, d_dt);
   SUBFV_CUDA(cudaGetLastError());
+  unsigned st = 0;
+  SUBFV_CUDA(cudaMemcpyAsync(&st, m.status, sizeof(unsigned), cudaMemcpyDeviceToHost, m.stream));
   SUBFV_CUDA(cudaStreamSynchronize(m.stream));
-  return 0;
+  return (int)st;
 }
