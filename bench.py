@@ -13,6 +13,17 @@ through the C-ABI with host buffers: every step uploads the state from host memo
 downloads the result. The working set of a step (about 1 GB) is larger than the 126 MB
 L2, so no flush is needed between steps.
 
+`parity`: the same 4 steps run by the oracle (the CPU restatement, also the
+`cpu_baseline` sample) and by the GPU from the same initial state, compared bit for bit.
+
+`north_star` (one GPU, default run): the batched mixed-precision measurement
+(`batched_mixed`: 256 shock tubes, N uniform in [200, 20000], about 10.6 M cells, K
+steps at precision levels 0/1/2 against the plain FP64 path run one problem at a time,
+and per-field L1 / Linf / drift of 16 problems run to their end time) and a serving
+stream (`serve`: 32 Gresho or Sedov requests of up to 32,768 cells on a Poisson stream,
+p50/p99 latency and aggregate cell-updates/s against the requests solved one by one).
+`--workload shocktubes` / `serve` run those at their full sizes.
+
 Multi-GPU: independent replicas of the problem, one per rank (weak scaling, no
 data-path collective). `--impl reference` times the CPU restatement of the reference
 (oracle/) on the host cores instead.
@@ -58,6 +69,12 @@ def _args():
     p.add_argument("--rate", type=float, default=20.0)
     p.add_argument("--max-cells", type=int, default=1 << 18)
     p.add_argument("--time-scale", type=float, default=0.05)
+    p.add_argument("--no-north-star", action="store_true",
+                   help="skip the batched-mixed and serving measurements of the default run")
+    p.add_argument("--ns-problems", type=int, default=256, help="shock tubes in the default run's batch")
+    p.add_argument("--ns-steps", type=int, default=10)
+    p.add_argument("--serve-requests", type=int, default=32)
+    p.add_argument("--serve-max-cells", type=int, default=1 << 15)
     return p.parse_args()
 
 
@@ -189,8 +206,19 @@ def cpu_baseline(n_steps=4):
     n, _, _, _ = o.lag_run(sol, mass, CFL, 1.0, n_steps)
     el = time.perf_counter() - t0
     return {"value": n * o.n_elems / el, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+            "nproc": os.cpu_count(), "cpu_model": _cpu_model(),
             "sample": f"{n} time steps of the same 512x512 Sedov mesh, serial C++ restatement (oracle/), "
-                      f"{el:.1f} s"}
+                      f"{el:.1f} s"}, sol
+
+
+def _cpu_model():
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def run_reference(args, rank, world):
@@ -244,6 +272,11 @@ def run_reference(args, rank, world):
     print(json.dumps(out), flush=True)
 
 
+KERNEL_NAMES = {"face": "k_lag_face<0>", "node": "k_lag_node<0>", "cell": "k_lag_cell<0>",
+                "finalize": "k_lag_finalize", "move": "k_lag_move", "face_geom": "k_face_geom<0>",
+                "cell_geom": "k_geom_step"}
+
+
 def _time_device(stream, fn):
     import torch
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -286,9 +319,10 @@ def run_gresho(args, rank, world, local):
         st, steps, t = s2.sync()
         out[prec_name] = {"ms": ms, "steps": steps, "status": st, "sol": s2.sol(), "t": t}
     a = out["fp64"]["sol"]
-    scale = np.abs(a).sum(0)
-    l1 = {name: {k: float(np.abs(a[:, i] - out[name]["sol"][:, i]).sum() / max(scale[i], 1e-6 * scale[1:4].max()))
-                 for i, k in enumerate(["rho", "rho_u", "rho_v", "rho_w", "E"])} for name in ("mixed", "mixed_flux")}
+    l1 = {}
+    for name in ("mixed", "mixed_flux"):
+        e1, ei = field_errors(a, out[name]["sol"])
+        l1[name] = {"l1_rel": dict(zip(FIELDS, e1)), "linf_rel": dict(zip(FIELDS, ei))}
     cells = mesh.n_elems
     cpu = None
     if not args.no_cpu_baseline:
@@ -306,7 +340,7 @@ def run_gresho(args, rank, world, local):
            "mixed_flux_value": cells * 200 / (out["mixed_flux"]["ms"] / 1e3),
            "diffusion_value": cells * 200 / (out["fp64_diffusion"]["ms"] / 1e3),
            "ms_per_iteration": out["fp64"]["ms"] / 200, "cells": cells, "iterations": 200,
-           "mixed_l1_rel_vs_fp64": l1, "status": [out[k]["status"] for k in ("fp64", "mixed", "mixed_flux", "fp64_diffusion")],
+           "mixed_errors_vs_fp64": l1, "status": [out[k]["status"] for k in ("fp64", "mixed", "mixed_flux", "fp64_diffusion")],
            "sim_time_after_200": out["fp64"]["t"],
            "roofline": _ns_roofline(mesh_sizes, 2, out["fp64"]["ms"] / 200),
            "dtype": "f64", "cpu_baseline": cpu}
@@ -396,26 +430,35 @@ def _build_meshes(raws, local, threads=None):
         return list(ex.map(one, raws))
 
 
-def _l1_rel(a, b):
-    """Per-field L1 relative difference; near-zero fields (transverse momenta) are
-    scaled by the largest momentum component's L1 norm."""
-    scale = np.abs(a).sum(0)
-    mom = scale[1:4].max()
-    return [float(np.abs(a[:, i] - b[:, i]).sum() / max(scale[i], 1e-3 * mom, 1e-300)) for i in range(5)]
+FIELDS = ["rho", "rho_u", "rho_v", "rho_w", "E"]
 
 
-def run_shocktubes(args, rank, world, local):
-    """Batched shock tubes: `--problems` (1024) independent Riemann problems on N x 4 quad
-    strips, N uniform in [200, 20000] (seed 1), states as in subfv_b200.shocktube, first
-    order multi_point nodal solver, CFL 0.4, walls all round. Timed: K steps of the whole
-    batch in shared launches (graph-replayed), FP32 flux arithmetic with FP64 nodal
-    solver and accumulation ("mixed"), autotuned and fixed launch shapes, plus the plain
-    FP64 batch; the baseline is the plain FP64 path run one problem at a time
-    (subfv_ns_state, graph-replayed) over a sample of the problems."""
+def field_errors(a, b):
+    """Per-field relative errors of b against a (n, 5): L1 = sum |b - a| / sum |a| and
+    Linf = max |b - a| / max |a|. The three momentum components share one scale, that of
+    the momentum vector (the largest component norm), so a transverse momentum that is
+    zero up to round-off is measured against the flow's momentum, not against itself."""
+    l1s, lis = np.abs(a).sum(0), np.abs(a).max(0)
+    l1s[1:4], lis[1:4] = l1s[1:4].max(), lis[1:4].max()
+    d = np.abs(b - a)
+    return ([float(d[:, i].sum() / max(l1s[i], 1e-300)) for i in range(5)],
+            [float(d[:, i].max() / max(lis[i], 1e-300)) for i in range(5)])
+
+
+def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=16, tune=True):
+    """Batched shock tubes: `problems` independent Riemann problems on N x 4 quad strips,
+    N uniform in [200, nmax] (seed 1), states as in subfv_b200.shocktube, first order
+    multi_point nodal solver, CFL 0.4, walls all round. Timed: K steps of the whole batch
+    in shared launches (graph-replayed) at three precision levels (0 plain FP64, 1 FP32
+    wave-speed bounds, 2 also FP32 reconstruction and flux), autotuned and fixed launch
+    shapes; the baseline is the plain FP64 path run one problem at a time (subfv_ns_state,
+    graph-replayed) over a sample of the problems. Accuracy: `acc_problems` problems of
+    N <= 2000 run to their end time at each level, against plain FP64 (per-field L1 and
+    Linf, mass and energy drift)."""
     import torch
     from subfv_b200 import autotune, shocktube
     from subfv_b200.ns import NsBatch, NsConfig, NsState
-    rng_tubes = shocktube.sample(args.problems, seed=SEED, n_max=args.nmax)
+    rng_tubes = shocktube.sample(problems, seed=SEED, n_max=nmax)
     t0 = time.perf_counter()
     meshes = _build_meshes([(lambda t=t: shocktube.raw_mesh(t)) for t in rng_tubes], local)
     setup_s = time.perf_counter() - t0
@@ -425,39 +468,38 @@ def run_shocktubes(args, rank, world, local):
                       nse=sum(m.n_sub_elems for m in meshes))
     base = dict(scheme=1, second_order=False, method=4, bc_style=2, boundary_2d=True, cfl=0.4)
     budget = int(150e9)
-    res = {"metric": "cell-updates/s", "workload": f"shocktubes_{args.problems}_strips_Nx4",
-           "problems": args.problems, "cells": cells, "mesh_setup_s": setup_s,
-           "mesh_bytes": sum(m.device_bytes for m in meshes)}
-    K = args.steps
-    for name, prec in (("mixed", 1), ("mixed_flux", 2), ("fp64", 0)):
-        b = NsBatch(NsConfig(**base, precision=prec), capacity=args.problems, budget_bytes=budget)
+    res = {"workload": f"shocktubes_{problems}_strips_Nx4_N200-{nmax}", "problems": problems, "cells": cells,
+           "steps": K, "mesh_setup_s": setup_s, "mesh_bytes": sum(m.device_bytes for m in meshes)}
+    for name, prec in (("level1", 1), ("level2", 2), ("fp64", 0)):
+        b = NsBatch(NsConfig(**base, precision=prec), capacity=problems, budget_bytes=budget)
         slots = [b.add(m, s, t.t_end) for m, s, t in zip(meshes, sols, rng_tubes)]
         assert None not in slots
         log = []
-        best, _ = autotune.tune_ns_batch(b, log=log)
-        for _ in range(args.warmup):
+        best = autotune.DEFAULT
+        if tune:
+            best, _ = autotune.tune_ns_batch(b, log=log)
+        for _ in range(warmup):
             b.time_steps(1)
         sampler = ClockSampler(local)
         sampler.start()
         ms_tuned = b.time_steps(K)
         clocks = sampler.stop()
-        autotune.apply(b, autotune.DEFAULT)
-        b.time_steps(1)
-        ms_fixed = b.time_steps(K)
+        r = {"value": cells * K / (ms_tuned / 1e3), "ms_per_step": ms_tuned / K,
+             "roofline": _ns_roofline(tube_sizes, 1, ms_tuned / K),
+             "tuned_shape": {"node_lanes": best[0], "block_v": best[1], "grid_v": best[2], "grid_c": best[3]},
+             "autotune_trials": len(log), "clocks": clocks, "state_bytes": sum(b.state_bytes(m) for m in meshes)}
+        if tune:
+            autotune.apply(b, autotune.DEFAULT)
+            b.time_steps(1)
+            ms_fixed = b.time_steps(K)
+            r.update(fixed_value=cells * K / (ms_fixed / 1e3), fixed_ms_per_step=ms_fixed / K)
         b.sync()
-        st = max(b.info(k)[3] for k in slots)
-        res[name] = {"value": cells * K / (ms_tuned / 1e3), "ms_per_step": ms_tuned / K,
-                     "roofline": _ns_roofline(tube_sizes, 1, ms_tuned / K),
-                     "fixed_value": cells * K / (ms_fixed / 1e3), "fixed_ms_per_step": ms_fixed / K,
-                     "tuned_shape": {"node_lanes": best[0], "block_v": best[1], "grid_v": best[2],
-                                     "grid_c": best[3]},
-                     "autotune_trials": log, "status": st, "clocks": clocks,
-                     "state_bytes": sum(b.state_bytes(m) for m in meshes)}
+        r["status"] = max(b.info(k)[3] for k in slots)
+        res[name] = r
         b.close()
         torch.cuda.synchronize()
     # plain FP64, one problem at a time, over a sample of the problems
-    idx = np.random.default_rng(SEED + 1).choice(args.problems, size=min(args.solo_sample, args.problems),
-                                                 replace=False)
+    idx = np.random.default_rng(SEED + 1).choice(problems, size=min(solo_sample, problems), replace=False)
     solo_ms, solo_cells = 0.0, 0
     for i in idx:
         m, s, t = meshes[i], sols[i], rng_tubes[i]
@@ -468,13 +510,16 @@ def run_shocktubes(args, rank, world, local):
         solo_ms += _time_device(stream, lambda: st_.advance_async(K))
         solo_cells += m.n_elems * K
         st_.close()
-    res["solo_fp64"] = {"value": solo_cells / (solo_ms / 1e3), "problems": len(idx),
+    solo = solo_cells / (solo_ms / 1e3)
+    res["solo_fp64"] = {"value": solo, "problems": len(idx),
                         "note": "plain FP64 path, one problem at a time, K steps each"}
-    # accuracy of the mixed path: a sample of small problems run to their end time
-    acc_idx = [i for i in range(args.problems) if rng_tubes[i].n <= 2000][:16]
+    for name in ("fp64", "level1", "level2"):
+        res[name]["x_solo_fp64"] = res[name]["value"] / solo
+    # accuracy: small problems run to their end time at each level
+    acc_idx = [i for i in range(problems) if rng_tubes[i].n <= 2000][:acc_problems]
     if acc_idx:
         outs = {}
-        for name, prec in (("fp64", 0), ("mixed", 1), ("mixed_flux", 2)):
+        for name, prec in (("fp64", 0), ("level1", 1), ("level2", 2)):
             b = NsBatch(NsConfig(**base, precision=prec), capacity=len(acc_idx), budget_bytes=budget)
             sl = [b.add(meshes[i], sols[i], rng_tubes[i].t_end) for i in acc_idx]
             while True:
@@ -484,45 +529,48 @@ def run_shocktubes(args, rank, world, local):
                     break
             outs[name] = [b.sol(k, meshes[i].n_elems) for k, i in zip(sl, acc_idx)]
             b.close()
-        res["mixed_accuracy"] = {}
-        for name in ("mixed", "mixed_flux"):
-            l1 = np.array([_l1_rel(a, c) for a, c in zip(outs["fp64"], outs[name])])
-            drift = []
+
+        def drift(name):
+            out = []
             for i, u in zip(acc_idx, outs[name]):
                 vol = meshes[i].geometry("elem_volume")
                 t0_, t1_ = (sols[i] * vol[:, None]).sum(0), (u * vol[:, None]).sum(0)
-                drift.append([float(abs(t1_[k] - t0_[k]) / abs(t0_[k])) for k in (0, 4)])
-            res["mixed_accuracy"][name] = {"problems": len(acc_idx), "l1_rel_max_per_field": l1.max(0).tolist(),
-                                           "l1_rel_mean_per_field": l1.mean(0).tolist(),
-                                           "mass_energy_drift_max": np.array(drift).max(0).tolist()}
-        drift = []
-        for i, u in zip(acc_idx, outs["fp64"]):
-            vol = meshes[i].geometry("elem_volume")
-            t0_, t1_ = (sols[i] * vol[:, None]).sum(0), (u * vol[:, None]).sum(0)
-            drift.append([float(abs(t1_[k] - t0_[k]) / abs(t0_[k])) for k in (0, 4)])
-        res["fp64_mass_energy_drift_max"] = np.array(drift).max(0).tolist()
-        res["accuracy_note"] = "run to each problem's end time; fields rho, rho u, rho v, rho w, E"
-    res["value"] = res["mixed"]["value"]
-    res["unit"] = "cell-updates/s"
+                out.append([float(abs(t1_[k] - t0_[k]) / abs(t0_[k])) for k in (0, 4)])
+            return np.array(out).max(0).tolist()
+
+        acc = {"problems": len(acc_idx), "fields": FIELDS, "fp64_mass_energy_drift_max": drift("fp64"),
+               "note": "each problem run to its end time; errors against the plain FP64 run (bit-identical to "
+                       "the oracle); momentum components scaled by the momentum vector"}
+        for name in ("level1", "level2"):
+            e = np.array([field_errors(a, c) for a, c in zip(outs["fp64"], outs[name])])  # (p, 2, 5)
+            acc[name] = {"l1_rel_max": e[:, 0].max(0).tolist(), "linf_rel_max": e[:, 1].max(0).tolist(),
+                         "mass_energy_drift_max": drift(name),
+                         "meets_l1_1e-6": bool(e[:, 0].max() <= 1e-6)}
+        res["accuracy"] = acc
+    return res
+
+
+def run_shocktubes(args, rank, world, local):
+    """The batched shock-tube workload at full size (`--problems`, `--nmax`)."""
+    res = shocktube_block(args.problems, args.nmax, args.steps, args.warmup, args.solo_sample, local)
+    res.update(metric="cell-updates/s", value=res["level1"]["value"], unit="cell-updates/s")
     print(json.dumps(res), flush=True)
 
 
-def run_serve(args, rank, world, local):
-    """Serving: `--requests` solve requests (Gresho vortex or 2-D Sedov, triangles or
-    quadrilaterals, cells log-uniform in [4096, --max-cells], end time uniform in
-    [0.1, 1] x nominal x --time-scale) on a seeded Poisson stream of `--rate` requests per
-    second, served by subfv_b200.serve.Server under a 150 GB budget, in plain FP64 and in
-    mixed precision. Latency = arrival to result on the host. Baseline: a sample of the
-    same requests solved one at a time on the plain FP64 solo path."""
+def serve_block(n_requests, rate, max_cells, time_scale, solo_sample, local):
+    """Serving: solve requests (Gresho vortex or 2-D Sedov, triangles or quadrilaterals,
+    cells log-uniform in [4096, max_cells], end time uniform in [0.1, 1] x nominal x
+    time_scale) on a seeded Poisson stream of `rate` requests per second, served by
+    subfv_b200.serve.Server under a 150 GB budget, in plain FP64 and at precision level
+    1. Latency = arrival to result on the host. Baseline: a sample of the same requests
+    solved one at a time on the plain FP64 solo path."""
     import torch
     from subfv_b200 import serve
-    reqs = serve.make_requests(args.requests, rate=args.rate, seed=SEED, cells_max=args.max_cells,
-                               time_scale=args.time_scale)
-    res = {"metric": "cell-updates/s", "workload": f"serve_{args.requests}_requests", "requests": args.requests,
-           "rate_per_s": args.rate, "cells_max": args.max_cells, "time_scale": args.time_scale,
-           "budget_bytes": int(150e9)}
-    for name, prec in (("fp64", 0), ("mixed", 1)):
-        srv = serve.Server(budget_bytes=int(150e9), capacity=max(64, args.requests), precision=prec, chunk=8,
+    reqs = serve.make_requests(n_requests, rate=rate, seed=SEED, cells_max=max_cells, time_scale=time_scale)
+    res = {"workload": f"serve_{n_requests}_requests", "requests": n_requests, "rate_per_s": rate,
+           "cells_max": max_cells, "time_scale": time_scale, "budget_bytes": int(150e9)}
+    for name, prec in (("fp64", 0), ("level1", 1)):
+        srv = serve.Server(budget_bytes=int(150e9), capacity=max(64, n_requests), precision=prec, chunk=8,
                            build_threads=max(1, min(16, (os.cpu_count() or 2) - 2)), keep_solutions=False)
         sampler = ClockSampler(local)
         sampler.start()
@@ -536,7 +584,7 @@ def run_serve(args, rank, world, local):
                      "latency": serve.latency_stats(results), "clocks": clocks,
                      "steps_mean": float(np.mean([r.steps for r in results])) if results else 0.0}
     # one request at a time on the plain FP64 path, over a sample of the stream
-    idx = np.random.default_rng(SEED + 2).choice(len(reqs), size=min(args.solo_sample, len(reqs)), replace=False)
+    idx = np.random.default_rng(SEED + 2).choice(len(reqs), size=min(solo_sample, len(reqs)), replace=False)
     t0 = time.perf_counter()
     cu = 0
     for i in idx:
@@ -545,8 +593,14 @@ def run_serve(args, rank, world, local):
     el = time.perf_counter() - t0
     res["one_by_one_fp64"] = {"value": cu / el, "requests": len(idx), "seconds": el,
                               "note": "each request built and solved alone on the solo path, sequentially"}
-    res["value"] = res["mixed"]["value"]
-    res["unit"] = "cell-updates/s"
+    for name in ("fp64", "level1"):
+        res[name]["x_one_by_one_fp64"] = res[name]["value"] / res["one_by_one_fp64"]["value"]
+    return res
+
+
+def run_serve(args, rank, world, local):
+    res = serve_block(args.requests, args.rate, args.max_cells, args.time_scale, args.solo_sample, local)
+    res.update(metric="cell-updates/s", value=res["level1"]["value"], unit="cell-updates/s")
     print(json.dumps(res), flush=True)
 
 
@@ -621,7 +675,7 @@ def main():
     # per-kernel device times of eager steps (events between kernels, same stream)
     prof_steps = 10
     kms = state.profile_steps(prof_steps)
-    names = ["face", "node", "cell", "finalize", "move", "geom"]
+    names = ["face", "node", "cell", "finalize", "move", "face_geom", "cell_geom"]
     per = {k: v / prof_steps for k, v in zip(names, kms)}
     dom = max(per, key=per.get)
     sizes = _mesh_sizes(topo)
@@ -653,8 +707,28 @@ def main():
            "steps": k_e2e, "api": "subfv_lag_step_host", "host_buffer": "page-locked"}
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline()
+        cpu, sol_oracle = cpu_baseline()
+        # the same 4 steps on the GPU from the same initial state, compared bit for bit
+        mesh.set_coords(coords0)
+        mesh.compute_geometry_mesh()
+        st_par = LagrangeState(mesh, sol0, mass, cfl=CFL, t_max=1.0, precision=prec)
+        st_par.advance(4)
+        got = st_par.sol()
+        same = bool(np.array_equal(got, sol_oracle))
+        parity = {"against": "oracle (serial C++ restatement of lagrange_module.F90)", "steps": 4,
+                  "cells": cells, "bit_exact": same, "max_abs_diff": float(np.abs(got - sol_oracle).max())}
+        if prec != PLAIN_FP64:
+            e1, ei = field_errors(sol_oracle, got)
+            parity.update(l1_rel=dict(zip(FIELDS, e1)), linf_rel=dict(zip(FIELDS, ei)))
+        st_par.close()
+
+    north = None
+    if rank == 0 and world == 1 and not args.no_north_star:
+        north = {"batched_mixed": shocktube_block(args.ns_problems, args.nmax, args.ns_steps, 3, 32, local),
+                 "serve": serve_block(args.serve_requests, args.rate, args.serve_max_cells, args.time_scale, 8,
+                                      local)}
 
     if rank == 0:
         out = {
@@ -671,13 +745,15 @@ def main():
             "gpu_launches": 6 * args.steps,
             "clocks": clocks,
             "e2e": e2e,
-            "roofline": {"bound": "hbm", "kernel": ("k_face_geom<0>+k_geom_step" if dom == "geom" else f"k_lag_{dom}"), "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": KERNEL_NAMES[dom], "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": _traffic(dom), "algorithmic_bytes": kb[dom],
                          "kernel_ms": per[dom], "step_achieved_gbs": step_achieved},
             "kernel_ms": per,
             "fp64": _fp64_peak(),
             "cpu_baseline": cpu,
+            "parity": parity,
+            "north_star": north,
         }
         print(json.dumps(out), flush=True)
     if world > 1:

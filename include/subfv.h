@@ -34,6 +34,11 @@ int subfv_version(void);
  * achieved TFLOP/s (2 flops per FMA), the denominator of the FP64 fraction reported
  * for FP64-bound kernels. iters in [1, 2^20]; ~4096 takes a few milliseconds. */
 int subfv_probe_fp64_fma(int iters, double* tflops, double* ms);
+/* Check of the geometry kernels' exact division by 3 and by 6 (a reciprocal multiply
+ * with one FMA remainder correction; no counterpart in the reference): counts, over the
+ * n host doubles x, the quotients x/3 and x/6 that differ in any bit from CUDA's
+ * division. */
+int subfv_probe_div_const(const double* x, int64_t n, int64_t* mismatches);
 
 /* ---------------------------------------------------------------------------------
  * Topology: build_mesh (src/mesh/mesh_connectivity_module.F90:12-59) on the host,
@@ -169,7 +174,10 @@ int subfv_move_mesh(subfv_mesh* m, const double* vp, double dt);
 
 /* Device-resident time loop of lagrange_main.F90:89-127: state, mass and mesh stay in
  * HBM; each step = rhs, CFL reduction, mesh motion, geometry, update. The step loop
- * is replayed from a captured CUDA graph. */
+ * is replayed from a captured CUDA graph. precision 0: plain FP64 (bit-identical to the
+ * reference's arithmetic); 1: the per-face wave speeds in FP32, the nodal 3x3 solve,
+ * star pressures, fluxes, positions, volumes and sums in FP64 (totals conserved to
+ * FP64 rounding). */
 typedef struct subfv_lag_state subfv_lag_state;
 int subfv_lag_state_create(subfv_mesh* m, const double* sol, const double* mass, double cfl,
                            double t0, double t_max, int precision, subfv_lag_state** out);
@@ -191,8 +199,9 @@ int subfv_lag_last_dt(subfv_lag_state* s, double* dt);
 /* one step through host buffers: uploads sol, advances one step, downloads sol */
 int subfv_lag_step_host(subfv_lag_state* s, double* sol_inout);
 /* Runs n_steps steps launched one kernel at a time with CUDA events between kernels on
- * the mesh's stream; kernel_ms[k] receives the summed milliseconds of kernel k in step
- * order: node, cell, finalize, move, face geometry, cell geometry + update. */
+ * the mesh's stream; kernel_ms[0..6] receives the summed milliseconds of each kernel in
+ * step order: face wave speeds, node, cell, finalize, move, face geometry, cell
+ * geometry + update. */
 int subfv_lag_profile_steps(subfv_lag_state* s, int n_steps, double* kernel_ms);
 
 /* The CUDA stream (cudaStream_t) all work of this mesh is launched on. */
@@ -223,7 +232,9 @@ typedef struct subfv_ns_cfg {
   double cfl, tmax;
   int32_t precision;          /* 0 plain FP64; 1 FP32 wave-speed bounds of the nodal solver;
                                  2 also FP32 flux, reconstruction and limiter arithmetic
-                                 (nodal 3x3 systems and all sums FP64 in both) */
+                                 (nodal 3x3 systems, the flux's pressure-jump term and all
+                                 sums FP64 in both, so totals are conserved to FP64
+                                 rounding) */
   /* Navier-Stokes diffusion (namelist entries of ns_global_data_module.F90:10-46, 111):
      momentum and heat assembled point-implicitly into the cells' 5x5 blocks, always FP64.
      Explicit time loop and residual entry point only, on meshes without periodic faces. */

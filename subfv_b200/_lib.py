@@ -26,6 +26,7 @@ SIGNATURES = {
     "subfv_last_error": (c_char_p, []),
     "subfv_version": (c_int, []),
     "subfv_probe_fp64_fma": (c_int, [c_int, PD, PD]),
+    "subfv_probe_div_const": (c_int, [PD, c_i64, C.POINTER(c_i64)]),
     "subfv_topology_build": (c_int, [c_int, PD, c_int, PI32, PI32, PI32, c_int, PI32, PI32, PI32, c_int, c_int,
                                      C.POINTER(P)]),
     "subfv_topology_array_len": (c_i64, [P, c_char_p]),

@@ -90,9 +90,12 @@ int ensure_lag_arrays(DevMesh& d) {
   SUBFV_CUDA(cudaMallocAsync((void**)&d.frec, 6 * (size_t)d.nf * sizeof(double), d.stream));
   SUBFV_CUDA(cudaMallocAsync((void**)&d.centry, std::max<size_t>(d.ncsf, 1) * sizeof(int4), d.stream));
   SUBFV_CUDA(cudaMallocAsync((void**)&d.fS, (size_t)d.nf * sizeof(double4), d.stream));
+  SUBFV_CUDA(cudaMallocAsync((void**)&d.gface, 8 * (size_t)d.ne * sizeof(uint16_t), d.stream));
+  SUBFV_CUDA(cudaMallocAsync((void**)&d.gsub, (size_t)d.nse * sizeof(uint32_t), d.stream));
   d.bytes += 6 * (size_t)d.nf * sizeof(double) + std::max<size_t>(d.ncsf, 1) * sizeof(int4) +
-             (size_t)d.nf * sizeof(double4);
+             (size_t)d.nf * sizeof(double4) + 8 * (size_t)d.ne * sizeof(uint16_t) + (size_t)d.nse * sizeof(uint32_t);
   launch_build_cell_entries(d);
+  launch_build_geom_codes(d);
   SUBFV_CUDA(cudaGetLastError());
   return 0;
 }
@@ -593,7 +596,7 @@ void* subfv_mesh_stream(subfv_mesh* m) { return (void*)m->d.stream; }
 
 int subfv_lag_profile_steps(subfv_lag_state* s, int n_steps, double* kernel_ms) {
   DevMesh& d = s->m->d;
-  const int K = 6;
+  const int K = 7;
   cudaEvent_t ev[K + 1];
   for (int k = 0; k <= K; ++k) SUBFV_CUDA(cudaEventCreate(&ev[k]));
   for (int k = 0; k < K; ++k) kernel_ms[k] = 0.0;
@@ -609,9 +612,11 @@ int subfv_lag_profile_steps(subfv_lag_state* s, int n_steps, double* kernel_ms) 
     SUBFV_CUDA(cudaEventRecord(ev[4], d.stream));
     launch_lag_move(d, s->sc, 0.0);
     SUBFV_CUDA(cudaEventRecord(ev[5], d.stream));
-    launch_geometry(d, 0, s->sol6, s->rhs6, s->sc);
+    launch_face_geometry_step(d, s->sc);
     SUBFV_CUDA(cudaEventRecord(ev[6], d.stream));
-    SUBFV_CUDA(cudaEventSynchronize(ev[6]));
+    launch_cell_geometry_step(d, s->sol6, s->rhs6, s->sc);
+    SUBFV_CUDA(cudaEventRecord(ev[7], d.stream));
+    SUBFV_CUDA(cudaEventSynchronize(ev[7]));
     for (int k = 0; k < K; ++k) {
       float ms = 0.f;
       SUBFV_CUDA(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));

@@ -23,6 +23,31 @@ enum StatusBits : unsigned {
   kErrIndex = 1u << 5,       // an index outside its array (checked builds)
 };
 
+// x / D for D = 3 or 6, bit-identical to the IEEE quotient (round to nearest), by a
+// multiply with the rounded reciprocal R = RN(1/D) and one remainder correction
+// (Markstein's correction step for division with a fused multiply-add):
+//   q0 = RN(x R),  e = x - D q0 (exact, one FMA),  q = RN(q0 + e R) (one FMA).
+// Why it is exact for D = 3 * 2^k: R = (1/D)(1 - 2^-54), so x R is within half an ulp of
+// x/D and q0 within one ulp; then x - D q0 is a small multiple of ulp(q0), exactly
+// representable. q0 + e R = x/D - (e/D) 2^-54 differs from x/D by less than
+// ulp(x/D) 2^-54, while x/D is at least ulp(x/D)/6 away from every rounding midpoint
+// (x is a multiple of 2 or 4 ulp(x/D), and 2K - 3(2M + 1) is odd), so both round to the
+// same double. Zero (its sign), subnormal or huge x, infinities and NaN take the plain
+// division. The kernels that use it stay bit-identical to the CPU restatement, which
+// divides; subfv_probe_div_const checks it against CUDA's division.
+template <int D>
+__host__ __device__ inline double div_const(double x) {
+  static_assert(D == 3 || D == 6, "exact only for 3 * 2^k, checked for 3 and 6");
+  constexpr double R = 1.0 / D;
+  const double ax = fabs(x);
+  if (!(ax >= 0x1p-960 && ax <= 0x1p960)) return x / D;
+  const double q0 = x * R;
+  const double e = fma(-q0, (double)D, x);
+  return fma(e, R, q0);
+}
+__host__ __device__ inline double div3(double x) { return div_const<3>(x); }
+__host__ __device__ inline double div6(double x) { return div_const<6>(x); }
+
 // gfortran's inline NORM2 of a 3-vector: scaled sum of squares, scale starting at 1.
 __host__ __device__ inline double fnorm2_3(double a0, double a1, double a2) {
   // With every |a_i| <= 1 the scale stays 1, each a_i / scale is a_i exactly and a zero

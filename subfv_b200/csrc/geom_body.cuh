@@ -24,6 +24,15 @@ __device__ inline V3 half_sum(V3 a, V3 b) { return {0.5 * (a.x + b.x), 0.5 * (a.
 
 __device__ inline V3 pick4(const V3 (&P)[4], int i) { return i == 0 ? P[0] : i == 1 ? P[1] : i == 2 ? P[2] : P[3]; }
 
+// s / nvc, the vertex average of compute_elem_centroid: exact shortcuts for the usual
+// vertex counts (a power of two scales exactly; div6 is exact), the division otherwise
+__device__ inline V3 vertex_mean(V3 s, int nvc) {
+  if (nvc == 8) return {s.x * 0.125, s.y * 0.125, s.z * 0.125};
+  if (nvc == 4) return {s.x * 0.25, s.y * 0.25, s.z * 0.25};
+  if (nvc == 6) return {div6(s.x), div6(s.y), div6(s.z)};
+  return {s.x / nvc, s.y / nvc, s.z / nvc};
+}
+
 // compute_face_centroid + compute_subface_norm + compute_face_norm (:177-271), one thread
 // per face. Also fS[f] = sum over the face's subfaces (in face%sub_face order) of
 // area * unit normal, which the Lagrangian step's cell kernel uses for check_mesh's
@@ -42,7 +51,7 @@ __device__ inline void face_geom_body(const DevMesh& m, const int f) {
 #pragma unroll
   for (int k = 0; k < 4; ++k)
     if (k < n) cg = {cg.x + P[k].x, cg.y + P[k].y, cg.z + P[k].z};
-  cg = n == 4 ? V3{cg.x * 0.25, cg.y * 0.25, cg.z * 0.25} : V3{cg.x / 3, cg.y / 3, cg.z / 3};
+  cg = n == 4 ? V3{cg.x * 0.25, cg.y * 0.25, cg.z * 0.25} : V3{div3(cg.x), div3(cg.y), div3(cg.z)};
   V3 c = {0.0, 0.0, 0.0};
   double sum_area = 0.0;
 #pragma unroll
@@ -51,23 +60,22 @@ __device__ inline void face_geom_body(const DevMesh& m, const int f) {
       const V3 pj = P[j], pp = pick4(P, j + 1 == n ? 0 : j + 1);
       const V3 x = cross(sub(pj, cg), sub(pp, cg));
       const double area = 0.5 * fnorm2_3(x.x, x.y, x.z);
-      c.x = c.x + area * (pj.x + pp.x + cg.x) / 3.0;
-      c.y = c.y + area * (pj.y + pp.y + cg.y) / 3.0;
-      c.z = c.z + area * (pj.z + pp.z + cg.z) / 3.0;
+      c.x = c.x + div3(area * (pj.x + pp.x + cg.x));
+      c.y = c.y + div3(area * (pj.y + pp.y + cg.y));
+      c.z = c.z + div3(area * (pj.z + pp.z + cg.z));
       sum_area = sum_area + area;
     }
   c = {c.x / sum_area, c.y / sum_area, c.z / sum_area};
   m.fc[f] = make_double4(c.x, c.y, c.z, 0.0);
   const int4 fs = m.fsf[f];
   const int sfi[4] = {fs.x, fs.y, fs.z, fs.w};
+  const unsigned fp = m.fpos[f];
   V3 fnrm = {0.0, 0.0, 0.0}, S = {0.0, 0.0, 0.0};
 #pragma unroll
   for (int k = 0; k < 4; ++k)
     if (k < n) {
       const int sf = sfi[k];
-      const int vert = m.sf_vert[sf];
-      int j = 0;
-      while (j < n - 1 && vid[j] != vert) ++j;
+      const int j = (fp >> (2 * k)) & 3;  // the subface's vertex slot in the face
       const V3 cp = pick4(P, j);
       const V3 cpm = half_sum(pick4(P, j == 0 ? n - 1 : j - 1), cp), cpp = half_sum(pick4(P, j + 1 == n ? 0 : j + 1), cp);
       const V3 a = cross(sub(cpm, c), sub(cp, c));
@@ -88,14 +96,84 @@ __device__ inline void face_geom_body(const DevMesh& m, const int f) {
 // The cell part of compute_geometry_mesh for the Lagrangian step, one cell per thread,
 // after k_face_geom<0>: compute_elem_centroid (:59-110), compute_subelem_volume
 // (:112-160), compute_elem_volume (:162-175) and check_mesh (:374-411), then
-// sol += dt * rhs (lagrange_main.F90:110). The cell's vertex coordinates, face centroids
-// and face vertex positions are cached in shared memory (one column per thread), so each
-// is loaded once per cell. check_mesh_subface_closed adds each face's subface sum S as a
-// whole: the same total as the subface-by-subface sum up to rounding, and the test is a
-// 1e-14 threshold on its norm. Every face vertex must be a vertex of the cell (no
-// periodic faces); otherwise the cell reports SUBFV_ERR_INDEX.
+// sol += dt * rhs (lagrange_main.F90:110). The cell's vertex coordinates and face
+// centroids are cached in shared memory (one column per thread), so each is loaded once
+// per cell. The local topology comes from the static codes gface / gsub (built once by
+// build_geom_codes below): no id is searched and no face or subface index array is read
+// per step. check_mesh_subface_closed adds each face's subface sum S as a whole: the same
+// total as the subface-by-subface sum up to rounding, and the test is a 1e-14 threshold
+// on its norm. Every face vertex must be a vertex of the cell (no periodic faces);
+// otherwise the cell reports SUBFV_ERR_INDEX.
 constexpr int kGeoMaxV = 8, kGeoMaxF = 8, kGeoBlock = 64;
 
+// gface[8 c + j], face slot j of cell c (ef8 order): bits 3k..3k+2 the local index (in
+// the cell's vertex order) of the face's k-th vertex, bit 12 quadrilateral, bit 13 the
+// cell is the face's left neighbour, bit 14 valid (every face vertex found among the
+// cell's vertices). gsub[s], subcell s = (cell, local vertex k): bits 0..2 the number of
+// its subfaces, then per subface (sub_elem order) 5 bits: the face slot j (3 bits) and
+// the position kk of the vertex in that face's vertex order (2 bits).
+constexpr unsigned kGfQuad = 1u << 12, kGfLeft = 1u << 13, kGfValid = 1u << 14;
+
+// The codes of cell c, by the same searches the per-step kernel used to run: a face
+// vertex's local index is its first match among the cell's vertices; a subface's face
+// slot is the first slot holding its face (else the last slot) and its vertex position
+// the first match in that face (else the last position).
+__device__ inline void build_geom_codes(const DevMesh& m, const int c) {
+  if (c >= m.ne) return;
+  const int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
+  if (nvc > kGeoMaxV) {
+    for (int j = 0; j < kGeoMaxF; ++j) m.gface[8 * (size_t)c + j] = 0;
+    return;
+  }
+  int vid[kGeoMaxV], fid[kGeoMaxF];
+  unsigned code[kGeoMaxF];
+  for (int k = 0; k < nvc; ++k) vid[k] = m.ev[vb + k];
+  int nfc = 0;
+  for (int k = 0; k < kGeoMaxF; ++k) {
+    const int f = m.ef8[8 * (size_t)c + k];
+    if (f < 0) break;
+    fid[nfc++] = f;
+  }
+  for (int j = 0; j < kGeoMaxF; ++j) {
+    unsigned w = 0;
+    if (j < nfc) {
+      const int f = fid[j];
+      const int4 fv = m.fvert[f];
+      const int gid[4] = {fv.x, fv.y, fv.z, fv.w};
+      const int n = fv.w < 0 ? 3 : 4;
+      bool ok = true;
+      for (int k = 0; k < n; ++k) {
+        int q = 0;
+        while (q < nvc - 1 && vid[q] != gid[k]) ++q;
+        if (vid[q] != gid[k]) ok = false;
+        w |= (unsigned)q << (3 * k);
+      }
+      if (n == 4) w |= kGfQuad;
+      if (m.flr[f].x == c) w |= kGfLeft;
+      if (ok) w |= kGfValid;
+    }
+    code[j] = w;
+    m.gface[8 * (size_t)c + j] = (uint16_t)w;
+  }
+  for (int k = 0; k < nvc; ++k) {
+    const int4 q4 = m.se_sf[vb + k];
+    const int q[4] = {q4.x, q4.y, q4.z, q4.w};
+    unsigned g = 0;
+    int cnt = 0;
+    for (int jj = 0; jj < 4; ++jj) {
+      if (q[jj] < 0) break;
+      const int f = m.sf_face[q[jj]], vert = m.sf_vert[q[jj]];
+      int j = 0;
+      while (j < nfc - 1 && fid[j] != f) ++j;
+      const int n = 3 + ((code[j] & kGfQuad) ? 1 : 0);
+      int kk = 0;
+      while (kk < n - 1 && vid[(code[j] >> (3 * kk)) & 7] != vert) ++kk;
+      g |= (unsigned)(j | (kk << 3)) << (3 + 5 * jj);
+      ++cnt;
+    }
+    m.gsub[vb + k] = g | (unsigned)cnt;
+  }
+}
 
 // c: this thread's cell; every thread of a kGeoBlock-thread block calls (the caches are
 // indexed by threadIdx.x); dt: the step's time step for the update (with sol6)
@@ -114,13 +192,16 @@ __device__ inline void state_update(const DevMesh& m, double* sol6, const double
   if (!(u[0] > 0.0)) atomicOr(m.status, kErrNegDensity);
 }
 
+// the 16-bit code of face slot j (0..7) from the cell's four code words
+__device__ inline unsigned gface_code(const unsigned (&gw)[4], const int j) {
+  const unsigned w = (j >> 1) == 0 ? gw[0] : (j >> 1) == 1 ? gw[1] : (j >> 1) == 2 ? gw[2] : gw[3];
+  return (w >> (16 * (j & 1))) & 0xffffu;
+}
+
 __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const double* rhs6, const double dt,
                                       const int c) {
   __shared__ double sX[kGeoMaxV][3][kGeoBlock];
   __shared__ double sCF[kGeoMaxF][3][kGeoBlock];
-  __shared__ int sV[kGeoMaxV][kGeoBlock];
-  __shared__ int sF[kGeoMaxF][kGeoBlock];
-  __shared__ int8_t sLV[kGeoMaxF][4][kGeoBlock];
   const int t = threadIdx.x;
   if (c >= m.ne) return;
   const int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
@@ -128,99 +209,103 @@ __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const doub
     atomicOr(m.status, kErrIndex);
     return;
   }
+  const uint4 g4 = reinterpret_cast<const uint4*>(m.gface)[c];
+  const unsigned gw[4] = {g4.x, g4.y, g4.z, g4.w};
+  const int4 e0 = reinterpret_cast<const int4*>(m.ef8)[2 * (size_t)c];
+  const int4 e1 = reinterpret_cast<const int4*>(m.ef8)[2 * (size_t)c + 1];
+  const int fid[kGeoMaxF] = {e0.x, e0.y, e0.z, e0.w, e1.x, e1.y, e1.z, e1.w};
+  int nfc = 0;
+#pragma unroll
+  for (int j = 0; j < kGeoMaxF; ++j)
+    if (fid[j] >= 0 && nfc == j) nfc = j + 1;
+  // Every global load of the cell first: vertex coordinates, then per face its
+  // centroid, normal and subface sum (the check terms are formed as they arrive, in face
+  // order), then the subcells' codes. What follows reads shared memory and registers.
   V3 ce = {0.0, 0.0, 0.0};
   for (int k = 0; k < nvc; ++k) {
-    const int v = m.ev[vb + k];
-    const V3 x = ld3(m.x, v);
-    sV[k][t] = v;
+    const V3 x = ld3(m.x, m.ev[vb + k]);
     sX[k][0][t] = x.x;
     sX[k][1][t] = x.y;
     sX[k][2][t] = x.z;
     ce = {ce.x + x.x, ce.y + x.y, ce.z + x.z};
   }
-  ce = {ce.x / nvc, ce.y / nvc, ce.z / nvc};
-  int nfc = 0;
-  for (int k = 0; k < kGeoMaxF; ++k) {
-    const int f = m.ef8[8 * (size_t)c + k];
-    if (f < 0) break;
-    sF[nfc++][t] = f;
-  }
-  unsigned leftm = 0, quadm = 0;
-  V3 cen = {0.0, 0.0, 0.0};
-  double sum_vol = 0.0, vdiv = 0.0;
+  double vdiv = 0.0;
   V3 nt = {0.0, 0.0, 0.0}, ns = {0.0, 0.0, 0.0};
-  bool ok = true;
+  bool valid = true;
+#pragma unroll
+  for (int j = 0; j < kGeoMaxF; ++j)
+    if (j < nfc) {
+      const int f = fid[j];
+      const unsigned code = gface_code(gw, j);
+      valid = valid && (code & kGfValid);
+      const V3 cf = ld3(m.fc, f);
+      const double4 fn = m.fn[f];
+      const double4 S = m.fS[f];
+      sCF[j][0][t] = cf.x;
+      sCF[j][1][t] = cf.y;
+      sCF[j][2][t] = cf.z;
+      // check_mesh_elem_volume / _closed / _subface_closed terms of this face (the
+      // subface closure sums the face's own subface sum S, formed in face%sub_face order)
+      const double sg = (code & kGfLeft) ? 1.0 : -1.0;
+      const V3 nn = {sg * fn.x, sg * fn.y, sg * fn.z};
+      const V3 an = {fn.w * nn.x, fn.w * nn.y, fn.w * nn.z};
+      vdiv = vdiv + dot(cf, an);
+      nt = {nt.x + an.x, nt.y + an.y, nt.z + an.z};
+      ns = {ns.x + sg * S.x, ns.y + sg * S.y, ns.z + sg * S.z};
+    }
+  unsigned gs[kGeoMaxV];
+#pragma unroll
+  for (int k = 0; k < kGeoMaxV; ++k) gs[k] = k < nvc ? m.gsub[vb + k] : 0u;
+  if (!valid) {
+    atomicOr(m.status, kErrIndex);
+    return;
+  }
+  ce = vertex_mean(ce, nvc);
+  // compute_elem_centroid: tetrahedra (edge, face centroid, vertex centroid)
+  V3 cen = {0.0, 0.0, 0.0};
+  double sum_vol = 0.0;
   for (int j = 0; j < nfc; ++j) {
-    const int f = sF[j][t];
-    const int4 fv = m.fvert[f];
-    const int gid[4] = {fv.x, fv.y, fv.z, fv.w};
-    const int n = fv.w < 0 ? 3 : 4;
-    const bool left = m.flr[f].x == c;
-    if (left) leftm |= 1u << j;
-    if (n == 4) quadm |= 1u << j;
-    V3 P[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      P[k] = {0.0, 0.0, 0.0};
-      if (k < n) {
-        int q = 0;
-        while (q < nvc - 1 && sV[q][t] != gid[k]) ++q;
-        if (sV[q][t] != gid[k]) ok = false, q = 0;
-        sLV[j][k][t] = (int8_t)q;
-        P[k] = {sX[q][0][t], sX[q][1][t], sX[q][2][t]};
-      }
-    }
-    if (!ok) {
-      atomicOr(m.status, kErrIndex);
-      return;
-    }
-    // the face's geometry from k_face_geom
-    const V3 cf = ld3(m.fc, f);
-    sCF[j][0][t] = cf.x;
-    sCF[j][1][t] = cf.y;
-    sCF[j][2][t] = cf.z;
-    const double4 fn = m.fn[f];
-    const double4 S = m.fS[f];
-    const double sg = left ? 1.0 : -1.0;
-    // check_mesh_elem_volume / _closed / _subface_closed terms of this face (the subface
-    // closure sums the face's own subface sum S, formed in face%sub_face order)
-    const V3 nn = {sg * fn.x, sg * fn.y, sg * fn.z};
-    const V3 an = {fn.w * nn.x, fn.w * nn.y, fn.w * nn.z};
-    vdiv = vdiv + dot(cf, an);
-    nt = {nt.x + an.x, nt.y + an.y, nt.z + an.z};
-    ns = {ns.x + sg * S.x, ns.y + sg * S.y, ns.z + sg * S.z};
-    // compute_elem_centroid: tetrahedra (edge, face centroid, vertex centroid)
+    const unsigned code = gface_code(gw, j);
+    const int n = (code & kGfQuad) ? 4 : 3;
+    const bool left = (code & kGfLeft) != 0;
+    const V3 cf = {sCF[j][0][t], sCF[j][1][t], sCF[j][2][t]};
     const V3 fe = sub(cf, ce);
-#pragma unroll
-    for (int k = 0; k < 4; ++k)
-      if (k < n) {
-        const V3 cp = P[k], cpp = pick4(P, k + 1 == n ? 0 : k + 1);
-        const V3 x = left ? cross(sub(cp, cf), sub(cpp, cf)) : cross(sub(cpp, cf), sub(cp, cf));
-        const double vol = dot(x, fe) / 6.0;
-        cen.x = cen.x + vol * (cp.x + cpp.x + cf.x + ce.x) * 0.25;
-        cen.y = cen.y + vol * (cp.y + cpp.y + cf.y + ce.y) * 0.25;
-        cen.z = cen.z + vol * (cp.z + cpp.z + cf.z + ce.z) * 0.25;
-        sum_vol = sum_vol + vol;
+    int q = code & 7;
+    V3 cp = {sX[q][0][t], sX[q][1][t], sX[q][2][t]};
+    const V3 c0 = cp;
+    for (int k = 0; k < n; ++k) {
+      V3 cpp = c0;
+      if (k + 1 < n) {
+        q = (code >> (3 * (k + 1))) & 7;
+        cpp = {sX[q][0][t], sX[q][1][t], sX[q][2][t]};
       }
+      const V3 x = left ? cross(sub(cp, cf), sub(cpp, cf)) : cross(sub(cpp, cf), sub(cp, cf));
+      const double vol = div6(dot(x, fe));
+      cen.x = cen.x + vol * (cp.x + cpp.x + cf.x + ce.x) * 0.25;
+      cen.y = cen.y + vol * (cp.y + cpp.y + cf.y + ce.y) * 0.25;
+      cen.z = cen.z + vol * (cp.z + cpp.z + cf.z + ce.z) * 0.25;
+      sum_vol = sum_vol + vol;
+      cp = cpp;
+    }
   }
   cen = {cen.x / sum_vol, cen.y / sum_vol, cen.z / sum_vol};
   // compute_subelem_volume: subcell k is (cell, vertex k); its subfaces in sub_elem order
+  bool ok = true;
   double vcell = 0.0;
-  for (int k = 0; k < nvc; ++k) {
-    const int s = vb + k;
-    const int4 q4 = m.se_sf[s];
-    const int q[4] = {q4.x, q4.y, q4.z, q4.w};
-    double vol = 0.0;
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) {
-      if (q[jj] < 0) break;
-      const int f = m.sf_face[q[jj]], vert = m.sf_vert[q[jj]];
-      int j = 0;
-      while (j < nfc - 1 && sF[j][t] != f) ++j;
-      const int n = 3 + ((quadm >> j) & 1u);
-      int kk = 0;
-      while (kk < n - 1 && sV[sLV[j][kk][t]][t] != vert) ++kk;
-      const int lc = sLV[j][kk][t], lm = sLV[j][kk == 0 ? n - 1 : kk - 1][t], lp = sLV[j][kk + 1 == n ? 0 : kk + 1][t];
+  for (int k = 0; k < kGeoMaxV; ++k) {
+    if (k >= nvc) break;
+    const unsigned g = gs[k];
+    const int cnt = g & 7;
+    double vol = 0.0;
+    for (int jj = 0; jj < cnt; ++jj) {
+      const unsigned slot = (g >> (3 + 5 * jj)) & 31u;
+      const int j = slot & 7, kk = slot >> 3;
+      const unsigned code = gface_code(gw, j);
+      const int n = (code & kGfQuad) ? 4 : 3;
+      const int lc = (code >> (3 * kk)) & 7;
+      const int lm = (code >> (3 * (kk == 0 ? n - 1 : kk - 1))) & 7;
+      const int lp = (code >> (3 * (kk + 1 == n ? 0 : kk + 1))) & 7;
       const V3 cp = {sX[lc][0][t], sX[lc][1][t], sX[lc][2][t]};
       const V3 cpm = half_sum({sX[lm][0][t], sX[lm][1][t], sX[lm][2][t]}, cp);
       const V3 cpp = half_sum({sX[lp][0][t], sX[lp][1][t], sX[lp][2][t]}, cp);
@@ -228,21 +313,21 @@ __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const doub
       const V3 fe = sub(cf, cen);
       const V3 a = sub(cpm, cf), b = sub(cp, cf), cc3 = sub(cpp, cf);
       V3 x1, x2;
-      if ((leftm >> j) & 1u) {
+      if (code & kGfLeft) {
         x1 = cross(a, b);
         x2 = cross(b, cc3);
       } else {
         x1 = cross(cc3, b);
         x2 = cross(b, a);
       }
-      vol = vol + dot(x1, fe) / 6.0 + dot(x2, fe) / 6.0;
+      vol = vol + div6(dot(x1, fe)) + div6(dot(x2, fe));
     }
-    m.vol_se[s] = vol;
+    m.vol_se[vb + k] = vol;
     ok = ok && (vol > 0.0);
     vcell = vcell + vol;
   }
   m.vol[c] = vcell;
-  vdiv = vdiv / 3.0;
+  vdiv = div3(vdiv);
   ok = ok && (fabs(vcell - vdiv) < 1e-14);
   ok = ok && (fnorm2_3(nt.x, nt.y, nt.z) < 1e-14);
   ok = ok && (fnorm2_3(ns.x, ns.y, ns.z) < 1e-14);

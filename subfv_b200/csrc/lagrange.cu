@@ -17,8 +17,10 @@
 //
 // precision 0 (plain FP64) evaluates every expression in the reference's order and is
 // compiled without FMA contraction: bit-identical to the CPU restatement.
-// precision 1 (mixed) evaluates the per-face wave speeds and the subface fluxes in
-// FP32 and keeps the nodal 3x3 solve, positions, volumes and the residual sums in FP64.
+// precision 1 (mixed) evaluates the per-face wave speeds (the acoustic and shock bounds
+// of :68-73, square roots and divisions) in FP32 and keeps the nodal 3x3 solve, the star
+// pressures and fluxes, positions, volumes and the residual sums in FP64, so the totals
+// are conserved to FP64 rounding.
 #include <vector>
 
 #include "../../include/subfv.h"
@@ -336,7 +338,6 @@ __device__ inline double warp_min(double x) {
 template <int P>
 __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict__ sol6, double* __restrict__ rhs6,
                                      double* dt_slot, const int mode, const int c) {
-  using T = typename Flt<P>::T;
   double dtloc = 1e6;
   if (c < m.ne) {
     U5 me = ld_u(sol6, c);
@@ -400,40 +401,26 @@ __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict_
           double v_et = dot3(vpn.x, vpn.y, vpn.z, fn.x, fn.y, fn.z);
           double am = area / mass;
           const double2 ll = llc[u], vv = vvc[u];
+          // The star pressures and the flux in FP64 at every precision: at precision 1
+          // lambda is the FP32 wave speed (stored as a double), the same value the nodal
+          // solve used, so sum over a node of A (p*_L - p*_R) n = R - M v* closes to FP64
+          // rounding and the totals stay conserved.
           if (side == 0) {  // this cell is the face's left neighbour: lambda of its side, v.n
             double lam = ll.x, vme = vv.x;
-            if (P == 0) {
-              double ps = pme - lam * (v_et - vme);
-              r0 = r0 - am * (-v_et);
-              r1 = r1 - am * (ps * fn.x);
-              r2 = r2 - am * (ps * fn.y);
-              r3 = r3 - am * (ps * fn.z);
-              r4 = r4 - am * (ps * v_et);
-            } else {
-              T ps = (T)pme - (T)lam * ((T)v_et - (T)vme);
-              r0 = r0 - am * (double)(-(T)v_et);
-              r1 = r1 - am * (double)(ps * (T)fn.x);
-              r2 = r2 - am * (double)(ps * (T)fn.y);
-              r3 = r3 - am * (double)(ps * (T)fn.z);
-              r4 = r4 - am * (double)(ps * (T)v_et);
-            }
+            double ps = pme - lam * (v_et - vme);
+            r0 = r0 - am * (-v_et);
+            r1 = r1 - am * (ps * fn.x);
+            r2 = r2 - am * (ps * fn.y);
+            r3 = r3 - am * (ps * fn.z);
+            r4 = r4 - am * (ps * v_et);
           } else {  // right neighbour
             double lam = ll.y, vme = vv.y;
-            if (P == 0) {
-              double ps = pme + lam * (v_et - vme);
-              r0 = r0 + am * (-v_et);
-              r1 = r1 + am * (ps * fn.x);
-              r2 = r2 + am * (ps * fn.y);
-              r3 = r3 + am * (ps * fn.z);
-              r4 = r4 + am * (ps * v_et);
-            } else {
-              T ps = (T)pme + (T)lam * ((T)v_et - (T)vme);
-              r0 = r0 + am * (double)(-(T)v_et);
-              r1 = r1 + am * (double)(ps * (T)fn.x);
-              r2 = r2 + am * (double)(ps * (T)fn.y);
-              r3 = r3 + am * (double)(ps * (T)fn.z);
-              r4 = r4 + am * (double)(ps * (T)v_et);
-            }
+            double ps = pme + lam * (v_et - vme);
+            r0 = r0 + am * (-v_et);
+            r1 = r1 + am * (ps * fn.x);
+            r2 = r2 + am * (ps * fn.y);
+            r3 = r3 + am * (ps * fn.z);
+            r4 = r4 + am * (ps * v_et);
           }
         }
         if (mode & 2) {  // compute_dt terms for (cell, subface)

@@ -79,6 +79,23 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
     sf_se[i] = make_int2(d->sub_face_left_sub_elem[i] - 1, d->sub_face_right_sub_elem[i] - 1);
     sf_loc[i] = d->sub_face_loc ? d->sub_face_loc[i] - 1 : 0;
   }
+  // fpos: the vertex slot, in the face's vertex order, of each of the face's subfaces
+  // (face%sub_face order), 2 bits each; the first slot holding the subface's vertex (the
+  // last slot when none does), as the search of compute_subface_norm finds it
+  std::vector<uint8_t> fpos(nf, 0);
+  for (int f = 0; f < nf; ++f) {
+    const int v[4] = {fvert[f].x, fvert[f].y, fvert[f].z, fvert[f].w};
+    const int sfi[4] = {fsf[f].x, fsf[f].y, fsf[f].z, fsf[f].w};
+    const int n = v[3] < 0 ? 3 : 4;
+    unsigned code = 0;
+    for (int k = 0; k < n; ++k) {
+      const int vert = sfi[k] >= 0 && sfi[k] < nsf ? sf_vert[sfi[k]] : -1;
+      int j = 0;
+      while (j < n - 1 && v[j] != vert) ++j;
+      code |= (unsigned)j << (2 * k);
+    }
+    fpos[f] = (uint8_t)code;
+  }
   std::vector<int> se_elem(nse), se_vert(nse), se_loc(nse);
   std::vector<int4> se_sf(nse);
   for (int i = 0; i < nse; ++i) {
@@ -180,7 +197,7 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
       upload(&m->ekind, ekind, B, s) || alloc(&m->cc, ne, B, s) || alloc(&m->vol, ne, B, s) ||
       upload(&m->vsf_off, vsf_off, B, s) || upload(&m->vsf, vsf, B, s) || upload(&m->p_node, p_node, B, s) ||
       upload(&m->vse_off, vse_off, B, s) || upload(&m->vse, vse, B, s) || upload(&m->csf_off, csf_off, B, s) ||
-      upload(&m->csf, csf, B, s) || alloc(&m->status, 4, B, s))
+      upload(&m->csf, csf, B, s) || alloc(&m->status, 4, B, s) || upload(&m->fpos, fpos, B, s))
     return -1;
   SUBFV_CUDA(cudaStreamSynchronize(s));
   return 0;
@@ -191,7 +208,7 @@ void devmesh_free(DevMesh* m) {
                   m->sf_face, m->sf_vert, m->sf_se, m->sf_loc, m->sfn, m->sfa, m->se_elem, m->se_vert, m->se_loc,
                   m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
                   m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
-                  m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS};
+                  m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS, m->fpos, m->gface, m->gsub};
   // stream-ordered frees: they wait for the mesh stream's work but not for other
   // streams (a caller that used the mesh elsewhere orders that work first)
   for (void* p : ptrs)
@@ -318,7 +335,7 @@ __global__ void k_cell_geometry(DevMesh m) {
 }
 
 template <int FULL>
-__global__ void k_face_geom(DevMesh m, const LagScalars* sc) {
+__global__ void __launch_bounds__(128) k_face_geom(DevMesh m, const LagScalars* sc) {
   if (sc && sc->skip) return;
   geo::face_geom_body<FULL>(m, blockIdx.x * blockDim.x + threadIdx.x);
 }
@@ -328,6 +345,8 @@ __global__ void __launch_bounds__(geo::kGeoBlock) k_geom_step(DevMesh m, double*
   if (sc && sc->skip) return;
   geo::geom_step_body(m, sol6, rhs6, sol6 ? sc->dt : 0.0, blockIdx.x * geo::kGeoBlock + threadIdx.x);
 }
+
+__global__ void k_build_geom_codes(DevMesh m) { geo::build_geom_codes(m, blockIdx.x * blockDim.x + threadIdx.x); }
 
 __global__ void k_lag_update(DevMesh m, double* sol6, const double* rhs6, const LagScalars* sc) {
   if (sc->skip) return;
@@ -367,12 +386,21 @@ void launch_geometry(const DevMesh& m, int full, double* sol6, const double* rhs
     k_face_geom<1><<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, nullptr);
     k_cell_geometry<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m);
   } else {
-    k_face_geom<0><<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, sc);
-    k_geom_step<<<grid_for(m.ne, geo::kGeoBlock), geo::kGeoBlock, 0, m.stream>>>(m, sol6, rhs6, sc);
+    launch_face_geometry_step(m, sc);
+    launch_cell_geometry_step(m, sol6, rhs6, sc);
   }
+}
+void launch_face_geometry_step(const DevMesh& m, const LagScalars* sc) {
+  k_face_geom<0><<<grid_for(m.nf, 128), 128, 0, m.stream>>>(m, sc);
+}
+void launch_cell_geometry_step(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc) {
+  k_geom_step<<<grid_for(m.ne, geo::kGeoBlock), geo::kGeoBlock, 0, m.stream>>>(m, sol6, rhs6, sc);
 }
 void launch_lag_update(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc) {
   k_lag_update<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, sol6, rhs6, sc);
+}
+void launch_build_geom_codes(const DevMesh& m) {
+  k_build_geom_codes<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m);
 }
 void launch_vert_volume(const DevMesh& m) { k_vert_volume<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }
 void launch_vert_is_bound(const DevMesh& m) { k_vert_is_bound<<<grid_for(m.nv, 256), 256, 0, m.stream>>>(m); }

@@ -55,6 +55,13 @@ struct DevMesh {
   int4* centry = nullptr;
   // per face: sum of area * unit normal over its subfaces (Lagrangian step's mesh check)
   double4* fS = nullptr;
+  // Static local topology for the geometry kernels (the topology never changes, so the
+  // per-step kernels need no id searches; layouts in geom_body.cuh). fpos: per face,
+  // built at creation; gface (8 per cell, face slot order of ef8) and gsub (per subcell):
+  // built on first Lagrangian use.
+  uint8_t* fpos = nullptr;
+  uint16_t* gface = nullptr;
+  uint32_t* gsub = nullptr;
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;
@@ -100,9 +107,15 @@ void devmesh_free(DevMesh* m);
 // update sol += dt*rhs fused in)
 void launch_geometry(const DevMesh& m, int full, double* sol6 = nullptr, const double* rhs6 = nullptr,
                      const LagScalars* sc = nullptr);
+// the two halves of launch_geometry(m, 0, ...): the face kernel, then the cell kernel
+void launch_face_geometry_step(const DevMesh& m, const LagScalars* sc);
+void launch_cell_geometry_step(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc);
 // sol += dt*rhs alone (the update launch_geometry otherwise fuses in)
 void launch_lag_update(const DevMesh& m, double* sol6, const double* rhs6, const LagScalars* sc);
 void launch_vert_volume(const DevMesh& m);
+// the static local-topology codes of the Lagrangian geometry kernel (gface, gsub must be
+// allocated: 8 per cell, one per subcell)
+void launch_build_geom_codes(const DevMesh& m);
 void launch_vert_is_bound(const DevMesh& m);
 
 }  // namespace subfv

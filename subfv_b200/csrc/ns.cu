@@ -670,13 +670,22 @@ __device__ bool multi_point(const double* wl64, const double* wr64, const double
   bool ok = !(rhol_et < (T)0 || rhor_et < (T)0);
   T sl = vnl - lam_l / rhol;
   T sr = vnr + lam_r / rhor;
-  const T e[5] = {(T)0, n[0], n[1], n[2], v_et};
+  // The pressure-jump term 0.5 (p*_r - p*_l) (0, n, v*) in FP64 whatever T is:
+  // p*_r - p*_l = (lambda_l + lambda_r)(v* - vbar), so its sum over the node's subfaces
+  // is M v* - R, which the FP64 nodal solve closes; with the same normal velocities and
+  // pressures as vbar (the T-precision ones) the node's momentum and energy balance
+  // then holds to FP64 rounding and the totals stay conserved. For T = double these
+  // are the reference's expressions (:264-285) unchanged.
+  const double vet64 = vn_nodal;
+  const double plb64 = (double)pl - lam_l64 * (vet64 - (double)vnl);
+  const double prb64 = (double)pr + lam_r64 * (vet64 - (double)vnr);
+  const double e64[5] = {0.0, n64[0], n64[1], n64[2], vet64};
   for (int k = 0; k < 5; ++k) {
     T base = (T)0.5 * (fl[k] + fr[k]) -
              (T)0.5 * (fabs(sl) * (sle[k] - ul[k]) + fabs(v_et) * (sre[k] - sle[k]) + fabs(sr) * (ur[k] - sre[k]));
-    T jump = (T)0.5 * (pr_bar - pl_bar) * e[k];
-    lr[0][k] = (double)(base - jump);
-    lr[1][k] = (double)(-(base + jump));
+    const double jump = 0.5 * (prb64 - plb64) * e64[k];
+    lr[0][k] = (double)base - jump;
+    lr[1][k] = -((double)base + jump);
   }
   *sl_o = (double)sl;
   *sr_o = (double)sr;

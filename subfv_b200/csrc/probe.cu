@@ -74,3 +74,55 @@ extern "C" int subfv_probe_fp64_fma(int iters, double* tflops, double* ms) {
   if (out) cudaFree(out);
   return rc;
 }
+
+// Checks div3 / div6 (common.cuh) against CUDA's double division on n inputs: counts
+// the inputs whose quotients differ in any bit. No counterpart in the reference.
+namespace {
+__global__ void k_div_const(const double* __restrict__ x, int n, unsigned long long* __restrict__ bad) {
+  unsigned long long nb = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double v = x[i];
+    if (__double_as_longlong(div3(v)) != __double_as_longlong(v / 3.0)) ++nb;
+    if (__double_as_longlong(div6(v)) != __double_as_longlong(v / 6.0)) ++nb;
+  }
+  if (nb) atomicAdd(bad, nb);
+}
+}  // namespace
+
+extern "C" int subfv_probe_div_const(const double* x, int64_t n, int64_t* mismatches) {
+  if (!x || n < 0 || !mismatches) {
+    set_error("subfv_probe_div_const: bad argument");
+    return -2;
+  }
+  const int64_t chunk = 1 << 24;
+  double* d = nullptr;
+  unsigned long long* bad = nullptr;
+  int rc = 0;
+  if (cudaMalloc(&d, chunk * sizeof(double)) != cudaSuccess || cudaMalloc(&bad, sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMemset(bad, 0, sizeof(unsigned long long)) != cudaSuccess) {
+    set_error("subfv_probe_div_const: CUDA setup failed");
+    rc = -1;
+  }
+  for (int64_t o = 0; rc == 0 && o < n; o += chunk) {
+    const int m = (int)(n - o < chunk ? n - o : chunk);
+    if (cudaMemcpy(d, x + o, m * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("subfv_probe_div_const: copy failed");
+      rc = -1;
+      break;
+    }
+    k_div_const<<<592, 256>>>(d, m, bad);
+    if (cudaGetLastError() != cudaSuccess) {
+      set_error("subfv_probe_div_const: launch failed");
+      rc = -1;
+    }
+  }
+  unsigned long long h = 0;
+  if (rc == 0 && (cudaMemcpy(&h, bad, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)) {
+    set_error("subfv_probe_div_const: copy back failed");
+    rc = -1;
+  }
+  if (rc == 0) *mismatches = (int64_t)h;
+  if (d) cudaFree(d);
+  if (bad) cudaFree(bad);
+  return rc;
+}

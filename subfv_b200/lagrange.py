@@ -169,9 +169,9 @@ class LagrangeState:
         return int(_lib.load().subfv_mesh_stream(self.mesh._h))
 
     def profile_steps(self, n: int):
-        """Per-kernel device milliseconds summed over n eager steps (node, cell,
-        finalize, move, face geometry, cell geometry)."""
-        out = np.zeros(6)
+        """Per-kernel device milliseconds summed over n eager steps (face wave speeds,
+        node, cell, finalize, move, face geometry, cell geometry + update)."""
+        out = np.zeros(7)
         check(_lib.load().subfv_lag_profile_steps(self._h, int(n), pd(out)), "subfv_lag_profile_steps")
         return out
 

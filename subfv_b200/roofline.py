@@ -33,11 +33,14 @@ def lag_kernel_bytes(s: MeshSizes) -> dict:
                  + 8 * nsf + 8 * nse + 64 * ne + 48 * ne)
     b["finalize"] = 64
     b["move"] = 32 * nv * 3  # x read+write, vp read
-    # k_geom<0>: cell vertex lists, vertex records, cell faces, face vertex ids, L/R, face
-    # subface ids, subcell subface ids, subface->face/vertex; writes: face normal records,
-    # subface areas, subcell and cell volumes; update: cell records read+write, rhs read
-    b["geom"] = (4 * (ne + 1) + 4 * nse + 32 * nv + 32 * ne + 16 * nf + 8 * nf + 16 * nf + 16 * nse
-                 + 8 * nsf + 32 * nf + 8 * nsf + 8 * nse + 8 * ne + 64 * ne * 2 + 48 * ne)
+    # k_face_geom<0>: vertex records, face vertex and subface ids, the subfaces' vertex
+    # slots; writes: face centroids, normal records and subface sums, subface areas
+    b["face_geom"] = 32 * nv + 16 * nf + 16 * nf + nf + 32 * nf + 32 * nf + 32 * nf + 8 * nsf
+    # k_geom_step: cell vertex lists, vertex records, cell faces and their static codes,
+    # the face centroids, normal records and subface sums, the subcells' codes; writes:
+    # subcell and cell volumes; update: cell records read + write, rhs read
+    b["cell_geom"] = (4 * (ne + 1) + 4 * nse + 32 * nv + 32 * ne + 16 * ne + 96 * nf + 4 * nse
+                      + 8 * nse + 8 * ne + 64 * ne * 2 + 48 * ne)
     return b
 
 

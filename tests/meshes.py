@@ -18,3 +18,15 @@ def topology_cases():
         "hex_box_periodic": meshgen.hex_box(4, periodic=True),
         "strip": meshgen.strip(40),
     }
+
+
+def field_errors(a, b):
+    """Per-field relative errors of b against a, states (n, 5): L1 = sum |b - a| / sum |a|,
+    Linf = max |b - a| / max |a|. The three momentum (or velocity) components share the
+    scale of the largest one, so a component that is zero up to round-off (the transverse
+    momentum of a slab) is measured against the flow's momentum, not against itself."""
+    import numpy as np
+    l1s, lis = np.abs(a).sum(0), np.abs(a).max(0)
+    l1s[1:4], lis[1:4] = l1s[1:4].max(), lis[1:4].max()
+    d = np.abs(b - a)
+    return d.sum(0) / np.maximum(l1s, 1e-300), d.max(0) / np.maximum(lis, 1e-300)
