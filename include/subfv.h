@@ -253,6 +253,40 @@ typedef struct subfv_ns_cfg {
 int subfv_compute_rhs_ns(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs,
                          double* sum_lambda, double* vp, double* cell_grad);
 
+/* The procedures compute_rhs_ns and ns_main's loop call, one at a time, so a shim can
+ * keep ns_main.F90:83-107 as it is. Host arrays in the reference's layouts; each call
+ * uploads its inputs, runs on the mesh's stream and downloads its outputs.
+ *
+ * compute_euler_flux(mesh, sol, rhs, grad, sum_lambda, second_order, vp, h_p, mat_h_p) —
+ * ns_euler_module.F90:151-339 with the subface scheme of cfg (h_p and mat_h_p belong to
+ * the ZB schemes, which are not provided). sol (5, n_elems) and, when second_order, the
+ * cell gradients grad (3, 5, n_elems) in; rhs (5, n_elems), sum_lambda (n_elems, started
+ * at 1e-12) and vp (3, n_vert, the multi-point nodal velocities; may be NULL) out. */
+int subfv_compute_euler_flux(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs,
+                             const double* grad, double* sum_lambda, int second_order, double* vp);
+/* compute_cell_grad_from_nodal_grad(mesh, sol, grad, all_nodal_grad, method) —
+ * ns_euler_recon_module.F90:8-59, method = cfg->method (the nodal least-squares
+ * gradients, then the cell gradient of the method with the physical slope limiter and the
+ * relaxed maximum principle). sol (5, n_elems) in; grad (3, 5, n_elems) and nodal_grad
+ * (3, 5, n_vert; may be NULL) out. */
+int subfv_compute_cell_grad_from_nodal_grad(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol,
+                                            double* grad, double* nodal_grad);
+/* flux_limiting(mesh, sol, rhs, rhs_o2, sum_lambda, cfl) — ns_euler_recon_module.F90:560-601:
+ * rhs (5, n_elems) in and out, sol and rhs_o2 (5, n_elems) and sum_lambda (n_elems) in. */
+int subfv_flux_limiting(subfv_mesh* m, const double* sol, double* rhs, const double* rhs_o2,
+                        const double* sum_lambda, double cfl);
+/* add_timedisc_and_solve(mesh, sol, rhs, diag, sum_lambda, delta_sol, res, res_vect,
+ * num_procs, me, a1, a2, cfl, t, dt) — ns_euler_module.F90:521-609 on one process with
+ * the global time step (tmax, the namelist's, is an argument). In and out: sol (5,
+ * n_elems), rhs (5, n_elems; + a1 V/dt sol on return), diag (5, 5, n_elems column-major
+ * per cell; the LU factors of diag + a1 V/dt I on return, as dgetrf leaves them; NULL
+ * stands for zero blocks), sum_lambda (zeroed). Out: delta_sol (5, n_elems), *res (the
+ * sum of norm2(delta) in cell order), res_vect (5), *dt. Returns SUBFV_ERR_BAD_OMEGA,
+ * with sol not advanced, where the reference prints "BAD OMEGA" and stops. */
+int subfv_add_timedisc_and_solve(subfv_mesh* m, double* sol, double* rhs, double* diag, double* sum_lambda,
+                                 double* delta_sol, double* res, double* res_vect, double a1, double a2,
+                                 double cfl, double t, double tmax, double* dt);
+
 typedef struct subfv_ns_state subfv_ns_state;
 /* compute_rhs_ns with the diffusion blocks: mat_diag (5, 5, n_elems), column-major per
    cell, as ns_main.F90:130-179 leaves it for add_timedisc_and_solve (may be NULL) */

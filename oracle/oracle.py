@@ -58,6 +58,11 @@ def load():
         lib.or_ns_run.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, C.c_int, C.c_double, PD, PI, PD, PD, PD]
         lib.or_ns_gresho.argtypes = [C.c_void_p, C.c_double, PD]
         lib.or_pinv3.argtypes = [PD]
+        lib.or_euler_flux.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, PD, C.c_int, PD, PD, PD]
+        lib.or_cell_grads.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, PD, PD]
+        lib.or_flux_limiting.argtypes = [C.c_void_p, PD, PD, PD, PD, C.c_double]
+        lib.or_add_timedisc.argtypes = [C.c_void_p, PI, PD, PI, PD, PD, PD, PD, PD, PD, PD, PD, C.c_double,
+                                        C.c_double, C.c_double, PD]
         lib.or_set_lapack.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         lib.or_ns_flux.argtypes = [C.c_int, PD, PD, PD, PD, PD]
         lib.or_lu3.argtypes = [PD, PD, PD]
@@ -276,6 +281,52 @@ class OracleMesh:
         st = load().or_ns_rhs_diag(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), _pd(rhs), _pd(sl),
                                    _pd(diag))
         return st, rhs, sl, diag
+
+    # --- the procedures one at a time (grad arrays (n, 5, 3) = the reference's (3, 5, n))
+    @staticmethod
+    def _g_to_oracle(g):
+        return np.ascontiguousarray(np.asarray(g, np.float64).transpose(0, 2, 1).reshape(-1, 15))
+
+    @staticmethod
+    def _g_from_oracle(g):
+        return np.ascontiguousarray(g.reshape(-1, 3, 5).transpose(0, 2, 1))
+
+    def euler_flux(self, cfg, sol, grad, second_order):
+        """compute_euler_flux: (status, rhs (n, 5), sum_lambda (n,), vp (nv, 3))."""
+        ic, dc, bt, bv = self._ns_args(cfg)
+        sol = np.ascontiguousarray(sol, np.float64)
+        g = self._g_to_oracle(grad) if grad is not None else np.zeros((self.n_elems, 15))
+        rhs, sl, vp = np.zeros((self.n_elems, 5)), np.zeros(self.n_elems), np.zeros((self.n_vert, 3))
+        st = load().or_euler_flux(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), _pd(g), int(second_order),
+                                  _pd(rhs), _pd(sl), _pd(vp))
+        return st, rhs, sl, vp
+
+    def cell_grads(self, cfg, sol):
+        """compute_cell_grad_from_nodal_grad: (grad (n, 5, 3), nodal_grad (nv, 5, 3))."""
+        ic, dc, bt, bv = self._ns_args(cfg)
+        sol = np.ascontiguousarray(sol, np.float64)
+        g, ng = np.zeros((self.n_elems, 15)), np.zeros((self.n_vert, 15))
+        load().or_cell_grads(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), _pd(g), _pd(ng))
+        return self._g_from_oracle(g), self._g_from_oracle(ng)
+
+    def flux_limiting(self, sol, rhs, rhs_o2, sum_lambda, cfl):
+        """flux_limiting on a copy of rhs; returns it."""
+        r = np.array(rhs, np.float64)
+        load().or_flux_limiting(self._h, _pd(np.ascontiguousarray(sol, np.float64)), _pd(r),
+                                _pd(np.ascontiguousarray(rhs_o2, np.float64)),
+                                _pd(np.ascontiguousarray(sum_lambda, np.float64)), float(cfl))
+        return r
+
+    def add_timedisc(self, cfg, sol, rhs, diag, sum_lambda, a1, a2, t):
+        """add_timedisc_and_solve in place on sol, rhs, diag (n, 5, 5) or None, sum_lambda;
+        returns (status, delta (n, 5), res, res_vect, dt)."""
+        ic, dc, bt, bv = self._ns_args(cfg)
+        delta, rv = np.zeros((self.n_elems, 5)), np.zeros(5)
+        res, dt = C.c_double(), C.c_double()
+        st = load().or_add_timedisc(self._h, _pi(ic), _pd(dc), _pi(bt), _pd(bv), _pd(sol), _pd(rhs),
+                                    _pd(diag) if diag is not None else None, _pd(sum_lambda), _pd(delta),
+                                    C.byref(res), _pd(rv), float(a1), float(a2), float(t), C.byref(dt))
+        return st, delta, res.value, rv, dt.value
 
     def ns_run(self, cfg, sol, n_max_iter, final_res=-1.0, t0=0.0):
         """The ns_main time loop in place on sol (n_max_iter + 1 steps unless stopped)."""

@@ -1339,6 +1339,10 @@ static int compute_rhs_ns(const Mesh& m, const NsCfg& cfg, const double* sol, Ns
   return st;
 }
 
+// the caller's diag goes through the 5x5 LU even without diffusion (the standalone
+// add_timedisc_and_solve entry, whose diag may hold any blocks)
+static bool g_force_lu = false;
+
 // ns_euler_module.F90:521-609 (no diffusion blocks: diag = a1*(V/dt + sum_lambda)*I)
 static int add_timedisc_and_solve(const Mesh& m, const NsCfg& cfg, double* sol, double* rhs, double* sum_lambda,
                                   double* delta, double* res, double* res_vect, double a1, double a2, double t,
@@ -1360,7 +1364,7 @@ static int add_timedisc_and_solve(const Mesh& m, const NsCfg& cfg, double* sol, 
     double s = a1 * (m.elem[i].volume / dt + sum_lambda[i - 1]);
     double nw[5], d5[5], ad[5];
     for (int k = 0; k < 5; ++k) r[k] = r[k] + s * u[k];
-    if (g_diff.active) {  // diag + s I, then lu_solve_inplace_lapack (dgetrf + dgetrs)
+    if (g_diff.active || g_force_lu) {  // diag + s I, then lu_solve_inplace_lapack (dgetrf + dgetrs)
       double* D = diag + 25 * (i - 1);
       for (int a = 0; a < 5; ++a)
         for (int b = 0; b < 5; ++b) D[a + 5 * b] = D[a + 5 * b] + s * (a == b ? 1.0 : 0.0);
@@ -1692,6 +1696,41 @@ int or_ns_run(void* h, const int* ic, const double* dc, const int* bc_type, cons
                 res_vect, vp);
 }
 void or_ns_gresho(void* h, double mach, double* sol) { init_gresho(handle_mesh(h), mach, sol); }
+// The procedures one at a time (grad and ngrad in the oracle's layout, 15 per entity,
+// g[5 d + var]).
+int or_euler_flux(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val,
+                  const double* sol, const double* grad, int second_order, double* rhs, double* sum_lambda,
+                  double* vp) {
+  const Mesh& m = handle_mesh(h);
+  std::vector<double> vpw(3 * m.n_vert, 0.0);
+  g_ns_time = 0.0;
+  int st = compute_euler_flux(m, make_cfg(ic, dc, bc_type, bc_val), sol, rhs, grad, sum_lambda, second_order != 0,
+                              vp ? vp : vpw.data());
+  return st;
+}
+void or_cell_grads(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val,
+                   const double* sol, double* grad, double* ngrad) {
+  const Mesh& m = handle_mesh(h);
+  for (int i = 0; i < 15 * m.n_elems; ++i) grad[i] = 0.0;
+  for (int i = 0; i < 15 * m.n_vert; ++i) ngrad[i] = 0.0;
+  compute_cell_grads(m, make_cfg(ic, dc, bc_type, bc_val), sol, grad, ngrad);
+}
+void or_flux_limiting(void* h, const double* sol, double* rhs, const double* rhs_o2, const double* sum_lambda,
+                      double cfl) {
+  flux_limiting(handle_mesh(h), sol, rhs, rhs_o2, sum_lambda, cfl);
+}
+int or_add_timedisc(void* h, const int* ic, const double* dc, const int* bc_type, const double* bc_val, double* sol,
+                    double* rhs, double* diag, double* sum_lambda, double* delta, double* res, double* res_vect,
+                    double a1, double a2, double t, double* dt) {
+  const Mesh& m = handle_mesh(h);
+  std::vector<double> zero;
+  if (!diag) zero.assign(25 * m.n_elems, 0.0);
+  g_force_lu = diag != nullptr;
+  int st = add_timedisc_and_solve(m, make_cfg(ic, dc, bc_type, bc_val), sol, rhs, sum_lambda, delta, res, res_vect,
+                                  a1, a2, t, dt, diag ? diag : zero.data());
+  g_force_lu = false;
+  return st;
+}
 void or_pinv3(double* a9) { oracle_pinv3(a9); }
 void or_set_lapack(void* dgesvd, void* dgetrf, void* dgetrs) {
   g_dgesvd = reinterpret_cast<dgesvd_fn>(dgesvd);

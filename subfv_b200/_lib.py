@@ -69,6 +69,11 @@ SIGNATURES = {
     "subfv_lag_profile_steps": (c_int, [P, c_int, PD]),
     "subfv_compute_rhs_ns": (c_int, [P, P, PD, PD, PD, PD, PD]),
     "subfv_compute_rhs_ns_ex": (c_int, [P, P, PD, PD, PD, PD, PD, PD]),
+    "subfv_compute_euler_flux": (c_int, [P, P, PD, PD, PD, PD, c_int, PD]),
+    "subfv_compute_cell_grad_from_nodal_grad": (c_int, [P, P, PD, PD, PD]),
+    "subfv_flux_limiting": (c_int, [P, PD, PD, PD, PD, c_dbl]),
+    "subfv_add_timedisc_and_solve": (c_int, [P, PD, PD, PD, PD, PD, PD, PD, c_dbl, c_dbl, c_dbl, c_dbl, c_dbl,
+                                             PD]),
     "subfv_ns_state_create": (c_int, [P, P, PD, c_dbl, C.POINTER(P)]),
     "subfv_ns_state_destroy": (c_int, [P]),
     "subfv_ns_state_set_node_kernel": (c_int, [P, c_int]),

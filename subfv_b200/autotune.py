@@ -47,6 +47,22 @@ def tune_ns_batch(batch, steps=2, log=None, layouts=(0, 1)):
         try_((best[0], bv, best[2], best[3]))
     for mult in (2, 4, 16, 32, 64):
         try_((best[0], best[1], SMS * mult, best[3]))
+    if best != DEFAULT:
+        # short trials are noisy: keep the pick only if it beats the default again over
+        # a longer run
+        confirm = 4 * steps
+        apply(batch, DEFAULT)
+        batch.time_steps(1)
+        t_def = batch.time_steps(confirm)
+        apply(batch, best)
+        batch.time_steps(1)
+        t_pick = batch.time_steps(confirm)
+        trials.append((DEFAULT, t_def * steps / confirm))
+        trials.append((best, t_pick * steps / confirm))
+        if t_pick >= t_def:
+            best, t_best = DEFAULT, t_def * steps / confirm
+        else:
+            t_best = t_pick * steps / confirm
     apply(batch, best)
     if log is not None:
         log.extend({"node_lanes": s[0], "block_v": s[1], "grid_v": s[2], "grid_c": s[3], "ms_per_step": t / steps}

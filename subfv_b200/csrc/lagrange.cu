@@ -563,7 +563,7 @@ __global__ void __launch_bounds__(kLagFaceBlock) kb_face_geom(const LagItem* __r
     const int p = lag_item_of(wf, n, w);
     const LagItem& I = it[p];
     if (I.sc->skip) continue;
-    geo::face_geom_body<0>(I.m, (w - wf[p]) * kLagFaceBlock + threadIdx.x);
+    geo::face_geom_body<0>(I.m, face_at(I.m, (w - wf[p]) * kLagFaceBlock + threadIdx.x));
   }
 }
 __global__ void __launch_bounds__(geo::kGeoBlock) kb_geom_step(const LagItem* __restrict__ it,

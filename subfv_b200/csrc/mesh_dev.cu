@@ -187,6 +187,23 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
 
   if (upload(&m->vel_off, vel_off, B, s) || upload(&m->vel, vel, B, s) || upload(&m->cse_sorted, cse_sorted, B, s))
     return -1;
+  // launch orders: stable sorts by a code-path key
+  std::vector<int> forder(nf), vorder(nv);
+  {
+    std::vector<int> key(nf);
+    for (int f = 0; f < nf; ++f) key[f] = (fvert[f].w < 0 ? 0 : 2) + (flr[f].y >= 0 ? 0 : 1);
+    for (int f = 0; f < nf; ++f) forder[f] = f;
+    std::stable_sort(forder.begin(), forder.end(), [&](int a, int b) { return key[a] < key[b]; });
+    std::vector<long> vkey(nv);
+    for (int v = 0; v < nv; ++v) {
+      int nb = 0;
+      for (int p = vsf_off[v]; p < vsf_off[v + 1]; ++p) nb += flr[sf_face[vsf[p]]].y < 0 ? 1 : 0;
+      vkey[v] = ((long)(vsf_off[v + 1] - vsf_off[v]) << 20) + ((long)(vse_off[v + 1] - vse_off[v]) << 10) + nb;
+    }
+    for (int v = 0; v < nv; ++v) vorder[v] = v;
+    std::stable_sort(vorder.begin(), vorder.end(), [&](int a, int b) { return vkey[a] < vkey[b]; });
+  }
+  if (upload(&m->forder, forder, B, s) || upload(&m->vorder, vorder, B, s)) return -1;
   if (upload(&m->x, x, B, s) || alloc(&m->vp, nv, B, s) || alloc(&m->vol_v, nv, B, s) || upload(&m->is_bound, isb, B, s) ||
       upload(&m->fvert, fvert, B, s) || upload(&m->flr, flr, B, s) || upload(&m->fsf, fsf, B, s) ||
       alloc(&m->fc, nf, B, s) || alloc(&m->fn, nf, B, s) || upload(&m->sf_face, sf_face, B, s) ||
@@ -208,7 +225,7 @@ void devmesh_free(DevMesh* m) {
                   m->sf_face, m->sf_vert, m->sf_se, m->sf_loc, m->sfn, m->sfa, m->se_elem, m->se_vert, m->se_loc,
                   m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
                   m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
-                  m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS, m->fpos, m->gface, m->gsub};
+                  m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS, m->fpos, m->gface, m->gsub, m->forder, m->vorder};
   // stream-ordered frees: they wait for the mesh stream's work but not for other
   // streams (a caller that used the mesh elsewhere orders that work first)
   for (void* p : ptrs)
@@ -337,7 +354,7 @@ __global__ void k_cell_geometry(DevMesh m) {
 template <int FULL>
 __global__ void __launch_bounds__(128) k_face_geom(DevMesh m, const LagScalars* sc) {
   if (sc && sc->skip) return;
-  geo::face_geom_body<FULL>(m, blockIdx.x * blockDim.x + threadIdx.x);
+  geo::face_geom_body<FULL>(m, face_at(m, blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 __global__ void __launch_bounds__(geo::kGeoBlock) k_geom_step(DevMesh m, double* sol6, const double* rhs6,

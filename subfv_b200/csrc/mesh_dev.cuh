@@ -62,6 +62,14 @@ struct DevMesh {
   uint8_t* fpos = nullptr;
   uint16_t* gface = nullptr;
   uint32_t* gsub = nullptr;
+  // Launch orders (built at creation): the faces grouped by vertex count and interior /
+  // boundary, the vertices by subface count, subcell count and boundary subfaces, each
+  // group in numbering order. The long per-entity kernels (face geometry, the explicit
+  // Euler node kernel and nodal gradient) map thread t to forder[t] / vorder[t], so the
+  // threads of a warp follow the same code path; no result depends on the order. The short
+  // gather-bound kernels keep the numbering order, which coalesces better.
+  int* forder = nullptr;
+  int* vorder = nullptr;
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;
@@ -96,6 +104,10 @@ struct DevMesh {
   cudaStream_t stream = nullptr;
   size_t bytes = 0;
 };
+
+// the face / vertex a per-entity kernel's thread t works on (t past the end stays past it)
+__device__ inline int face_at(const DevMesh& m, int t) { return t < m.nf ? m.forder[t] : t; }
+__device__ inline int vert_at(const DevMesh& m, int t) { return t < m.nv ? m.vorder[t] : t; }
 
 int devmesh_create(const struct subfv_mesh_desc* d, DevMesh* m);
 void devmesh_free(DevMesh* m);

@@ -1209,7 +1209,7 @@ __global__ void __launch_bounds__(kNodeGroupThreads, 2) k_ns_node_group(DevMesh 
   if (sc && sc->done) return;
   __shared__ NodeGroupSmem sm;
   const int g = threadIdx.x / NG;
-  const int v = blockIdx.x * (kNodeGroupThreads / NG) + g;
+  const int v = vert_at(m, blockIdx.x * (kNodeGroupThreads / NG) + g);
   ns_node_group<T, L, NG>(m, P, U, grad, fs, so, v, true, sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g], sc);
 }
 
@@ -1218,7 +1218,7 @@ __global__ void __launch_bounds__(kNodeThreads) k_ns_node(DevMesh m, NsParams P,
                                                           const double* __restrict__ grad, double* __restrict__ fs,
                                                           int so, const NsScalars* sc) {
   if (sc && sc->done) return;
-  ns_node_vertex<T, L, MS, EXT>(m, P, U, grad, fs, so, blockIdx.x * blockDim.x + threadIdx.x, sc);
+  ns_node_vertex<T, L, MS, EXT>(m, P, U, grad, fs, so, vert_at(m, blockIdx.x * blockDim.x + threadIdx.x), sc);
 }
 
 __device__ inline double warp_min(double x) {
@@ -1304,7 +1304,7 @@ __device__ void ns_nodal_grad_body(const DevMesh& m, const double* __restrict__ 
 
 __global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* __restrict__ U,
                                                        double* __restrict__ ngrad, const NsScalars* sc) {
-  ns_nodal_grad_body(m, U, ngrad, sc, blockIdx.x * blockDim.x + threadIdx.x);
+  ns_nodal_grad_body(m, U, ngrad, sc, vert_at(m, blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // compute_cell_grad_method_2..6 (:166-320) + physical_slope_limiter + relaxed_maximum_principle
@@ -1643,7 +1643,7 @@ __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restr
     const NsItem& I = it[p];
     if (I.sc->done) continue;
     ns_node_vertex<T, L, MS, EXT>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so,
-                                  (w - wv[p]) * blockDim.x + threadIdx.x, I.sc);
+                                  vert_at(I.m, (w - wv[p]) * blockDim.x + threadIdx.x), I.sc);
   }
 }
 // the group variant: a work block of block_v vertices is walked kNodeGroupThreads / NG
@@ -1662,7 +1662,7 @@ __global__ void __launch_bounds__(kNodeGroupThreads, 2) kb_ns_node_group(const N
     const NsItem& I = it[p];
     if (I.sc->done) continue;
     for (int c = 0; c < block_v; c += VPB)
-      ns_node_group<T, L, NG>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, (w - wv[p]) * block_v + c + g, true,
+      ns_node_group<T, L, NG>(I.m, P, which ? I.U1 : I.U0, I.grad, I.fs, so, vert_at(I.m, (w - wv[p]) * block_v + c + g), true,
                              sm.v + g * NG * kLaneVals, sm.f + g * NG, sm.s[g], I.sc);
   }
 }
@@ -1682,7 +1682,7 @@ __global__ void __launch_bounds__(256) kb_ns_nodal_grad(const NsItem* __restrict
   for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
     const int p = item_of(wv, n, w);
     const NsItem& I = it[p];
-    ns_nodal_grad_body(I.m, which ? I.U1 : I.U0, I.ngrad, I.sc, (w - wv[p]) * blockDim.x + threadIdx.x);
+    ns_nodal_grad_body(I.m, which ? I.U1 : I.U0, I.ngrad, I.sc, vert_at(I.m, (w - wv[p]) * blockDim.x + threadIdx.x));
   }
 }
 template <class T>
@@ -2184,6 +2184,169 @@ void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs
   k_ns_finalize<<<1, 1, 0, m.stream>>>(sc, P, partial, nb, m.status, last_stage);
   k_ns_apply<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, U_td, delta, U_out, sc, a2);
   k_ns_reset_omega<<<1, 1, 0, m.stream>>>(sc);
+}
+
+
+// ---------------------------------------------------------------------------------
+// The reference's module procedures one at a time, for the host-buffer C entries of
+// ns_procs.cu (ns_main's loop calls them in turn). Arrays in the reference's layouts:
+// sol5 / rhs5 / delta5 five doubles per cell, diag25 the column-major 5 x 5 block.
+
+// compute_euler_flux (ns_euler_module.F90:151-339) at state U with the cell gradients
+// grad (read when second_order): corner sums by the node kernel, then the cell gather;
+// rhs records hold the five residuals and sum_lambda (started at 1e-12)
+void launch_ns_euler_flux(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs,
+                          double* rhs, int second_order, NsScalars* sc) {
+  launch_node(m, P, U, grad, fs, second_order ? 1 : 0, sc);
+  k_ns_gather<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, fs, rhs, sc, 0);
+}
+
+// compute_cell_grad_from_nodal_grad (ns_euler_recon_module.F90:8-59)
+void launch_ns_cell_grads(const DevMesh& m, const NsParams& P, const double* U, double* ngrad, double* grad,
+                          NsScalars* sc) {
+  k_ns_nodal_grad<<<grid_for(m.nv, 128), 128, 0, m.stream>>>(m, U, ngrad, sc);
+  if (P.precision == 2)
+    k_ns_cell_grad<float><<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+  else
+    k_ns_cell_grad<double><<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+}
+
+namespace {
+
+// dt = min(1e10, min_i V_i / sum_lambda_i): the first loop of flux_limiting
+// (ns_euler_recon_module.F90:575-580) and add_timedisc_and_solve (ns_euler_module.F90:
+// 546-551), before the factor cfl; the minimum of non-negative doubles is exact in any
+// order (atomicMin on the bit pattern)
+__global__ void __launch_bounds__(128) k_proc_dtmin(DevMesh m, const double* __restrict__ sl, double* slot) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double x = 1e10;
+  if (c < m.ne) x = fmin2(x, m.vol[c] / sl[c]);
+  __shared__ double wm[4];
+  x = warp_min(x);
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = x;
+  __syncthreads();
+  if (threadIdx.x == 0) atomic_min_pos(slot, fmin(fmin(wm[0], wm[1]), fmin(wm[2], wm[3])));
+}
+
+// flux_limiting's cell loop (:582-590)
+__global__ void __launch_bounds__(128) k_proc_flux_limiting(DevMesh m, const double* __restrict__ sol5,
+                                                            double* __restrict__ rhs5,
+                                                            const double* __restrict__ rhso2_5,
+                                                            const double* __restrict__ sl, double dt) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= m.ne) return;
+  double* r = rhs5 + 5 * (size_t)c;
+  const double* r2 = rhso2_5 + 5 * (size_t)c;
+  const double* u = sol5 + 5 * (size_t)c;
+  const double den = m.vol[c] / dt + sl[c];
+  double Ub[5], dU[5];
+  for (int k = 0; k < 5; ++k) {
+    Ub[k] = u[k] + r[k] / den;
+    dU[k] = (r2[k] - r[k]) / den;
+  }
+  const double w = fmin2(1.0, max_omega_for_positivity(Ub, dU));
+  for (int k = 0; k < 5; ++k) r[k] = r[k] + w * (r2[k] - r[k]);
+}
+
+// add_timedisc_and_solve's cell loop (:559-574) with the global time step (sum_lambda
+// already zeroed): rsq = rhs^2 (for res_vect), diag += a1 V/dt I, rhs += a1 V/dt sol,
+// the 5 x 5 solve (dgetrf + dgetrs, factors left in diag; without diag the block is
+// a1 V/dt I and the solve a division), delta, the positivity limiter's omega (atomic
+// minimum) and norm2(delta) (gfortran's scaled sum of squares)
+__global__ void __launch_bounds__(128) k_proc_timedisc(DevMesh m, const double* __restrict__ sol5,
+                                                       double* __restrict__ rhs5, double* __restrict__ diag25,
+                                                       double* __restrict__ delta5, double* __restrict__ rn,
+                                                       double* __restrict__ rsq, double a1, double a2, double dt,
+                                                       double* omega_slot) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  double om = 1.0;
+  if (c < m.ne) {
+    const double* u = sol5 + 5 * (size_t)c;
+    double* r = rhs5 + 5 * (size_t)c;
+    double x[5], d5[5], ad[5];
+    for (int k = 0; k < 5; ++k) rsq[5 * (size_t)c + k] = r[k] * r[k];
+    const double s = a1 * (m.vol[c] / dt + 0.0);
+    for (int k = 0; k < 5; ++k) {
+      r[k] = r[k] + s * u[k];
+      x[k] = r[k];
+    }
+    if (diag25) {
+      double D[25];
+      double* dg = diag25 + 25 * (size_t)c;
+      for (int k = 0; k < 25; ++k) D[k] = dg[k];
+      for (int a = 0; a < 5; ++a)
+        for (int b = 0; b < 5; ++b) D[a + 5 * b] = D[a + 5 * b] + s * (a == b ? 1.0 : 0.0);
+      lu_solve5(D, x);
+      for (int k = 0; k < 25; ++k) dg[k] = D[k];
+    } else {
+      for (int k = 0; k < 5; ++k) x[k] = x[k] / s;
+    }
+    for (int k = 0; k < 5; ++k) {
+      d5[k] = x[k] - u[k];
+      delta5[5 * (size_t)c + k] = d5[k];
+      ad[k] = a2 * d5[k];
+    }
+    om = max_omega_for_positivity(u, ad);
+    double scale = 1.0, res = 0.0;
+    for (int k = 0; k < 5; ++k)
+      if (d5[k] != 0.0) {
+        const double ax = fabs(d5[k]);
+        if (ax > scale) {
+          const double q = scale / ax;
+          res = 1.0 + res * q * q;
+          scale = ax;
+        } else {
+          const double q = ax / scale;
+          res += q * q;
+        }
+      }
+    rn[c] = scale * sqrt(res);
+  }
+  __shared__ double wm[4];
+  om = warp_min(om);
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = om;
+  __syncthreads();
+  if (threadIdx.x == 0) atomic_min_pos(omega_slot, fmin(fmin(wm[0], wm[1]), fmin(wm[2], wm[3])));
+}
+
+// res = sum_i norm2(delta_i) and res_vect(k) = sum_i rhs(k, i)^2 in cell order, as the
+// reference's loop adds them (one thread: the order is the result)
+__global__ void k_proc_ordered_sums(int n, const double* __restrict__ rn, const double* __restrict__ rsq,
+                                    double* out6) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  double res = 0.0, rv[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int c = 0; c < n; ++c) {
+    res = res + rn[c];
+    for (int k = 0; k < 5; ++k) rv[k] = rv[k] + rsq[5 * (size_t)c + k];
+  }
+  out6[0] = res;
+  for (int k = 0; k < 5; ++k) out6[1 + k] = rv[k];
+}
+
+// sol = sol + a2 omega delta (:608), aw = a2 * omega
+__global__ void k_proc_apply(int n5, double* __restrict__ sol5, const double* __restrict__ delta5, double aw) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n5) sol5[i] = sol5[i] + aw * delta5[i];
+}
+
+}  // namespace
+
+void launch_proc_dtmin(const DevMesh& m, const double* sl, double* slot) {
+  k_proc_dtmin<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, sl, slot);
+}
+void launch_proc_flux_limiting(const DevMesh& m, const double* sol5, double* rhs5, const double* rhso2_5,
+                               const double* sl, double dt) {
+  k_proc_flux_limiting<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, sol5, rhs5, rhso2_5, sl, dt);
+}
+void launch_proc_timedisc(const DevMesh& m, const double* sol5, double* rhs5, double* diag25, double* delta5,
+                          double* rn, double* rsq, double a1, double a2, double dt, double* omega_slot,
+                          double* sums6) {
+  k_proc_timedisc<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, sol5, rhs5, diag25, delta5, rn, rsq, a1, a2, dt,
+                                                               omega_slot);
+  k_proc_ordered_sums<<<1, 32, 0, m.stream>>>(m.ne, rn, rsq, sums6);
+}
+void launch_proc_apply(const DevMesh& m, double* sol5, const double* delta5, double aw) {
+  k_proc_apply<<<grid_for(5 * m.ne, 256), 256, 0, m.stream>>>(5 * m.ne, sol5, delta5, aw);
 }
 
 }  // namespace subfv

@@ -82,4 +82,19 @@ void launch_be_pack_rhs(const DevMesh& m, const double* rhs, double* b);
 void launch_be_update(const DevMesh& m, double* U, const double* x);
 int ns_partial_blocks(const DevMesh& m);
 
+// The reference's module procedures one at a time (host-buffer entries of ns_procs.cu):
+// compute_euler_flux, compute_cell_grad_from_nodal_grad, and the kernels of
+// flux_limiting and add_timedisc_and_solve on arrays in the reference's layouts.
+void launch_ns_euler_flux(const DevMesh& m, const NsParams& P, const double* U, const double* grad, double* fs,
+                          double* rhs, int second_order, NsScalars* sc);
+void launch_ns_cell_grads(const DevMesh& m, const NsParams& P, const double* U, double* ngrad, double* grad,
+                          NsScalars* sc);
+void launch_proc_dtmin(const DevMesh& m, const double* sl, double* slot);
+void launch_proc_flux_limiting(const DevMesh& m, const double* sol5, double* rhs5, const double* rhso2_5,
+                               const double* sl, double dt);
+void launch_proc_timedisc(const DevMesh& m, const double* sol5, double* rhs5, double* diag25, double* delta5,
+                          double* rn, double* rsq, double a1, double a2, double dt, double* omega_slot,
+                          double* sums6);
+void launch_proc_apply(const DevMesh& m, double* sol5, const double* delta5, double aw);
+
 }  // namespace subfv

@@ -647,3 +647,213 @@ int subfv_compute_rhs_ns_ex(subfv_mesh* m, const subfv_ns_cfg* cfg, const double
 }
 
 }  // extern "C"
+
+// ---- the reference's module procedures one at a time, on host buffers in the
+// reference's layouts, for a shim that keeps ns_main's loop as it is (ns_main.F90:83-107
+// calls compute_rhs_ns, whose compute_euler_flux / compute_cell_grad_from_nodal_grad /
+// flux_limiting are below, and add_timedisc_and_solve). Each call uploads its inputs,
+// runs the kernels on the mesh's stream and downloads its outputs; FP64 (the precision
+// field of cfg applies to compute_euler_flux and the gradients as in the state loop).
+
+namespace {
+
+struct StateHold {
+  subfv_ns_state* s = nullptr;
+  ~StateHold() {
+    if (s) subfv_ns_state_destroy(s);
+  }
+};
+
+int reset_scalars(subfv_ns_state* s) {
+  DevMesh& d = s->m->d;
+  NsScalars h{};
+  h.dtred = 1e10;
+  h.omega = 1.0;
+  h.t = 0.0;
+  h.final_res = -1.0;
+  h.tmax = s->P.tmax;
+  SUBFV_CUDA(cudaMemcpyAsync(s->sc, &h, sizeof(h), cudaMemcpyHostToDevice, d.stream));
+  return handle_clear_status(d);
+}
+
+// grad(3, 5, n) of the reference <-> the kernels' 15 doubles per entity, g[5 d + var]
+void grad_from_ref(const double* f, double* g, size_t n) {
+  for (size_t c = 0; c < n; ++c)
+    for (int dd = 0; dd < 3; ++dd)
+      for (int k = 0; k < 5; ++k) g[15 * c + 5 * dd + k] = f[15 * c + dd + 3 * k];
+}
+void grad_to_ref(const double* g, double* f, size_t n) {
+  for (size_t c = 0; c < n; ++c)
+    for (int dd = 0; dd < 3; ++dd)
+      for (int k = 0; k < 5; ++k) f[15 * c + dd + 3 * k] = g[15 * c + 5 * dd + k];
+}
+
+// device scratch of one call, released on the mesh's stream
+struct Scratch {
+  cudaStream_t q;
+  std::vector<void*> ptrs;
+  explicit Scratch(cudaStream_t s) : q(s) {}
+  ~Scratch() {
+    for (void* p : ptrs) cudaFreeAsync(p, q);
+  }
+  template <class T>
+  T* get(size_t n) {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), q) != cudaSuccess) return nullptr;
+    ptrs.push_back(p);
+    return static_cast<T*>(p);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int subfv_compute_euler_flux(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* rhs,
+                             const double* grad, double* sum_lambda, int second_order, double* vp) {
+  if (!m || !sol || !rhs || !sum_lambda || (second_order && !grad)) {
+    set_error("subfv_compute_euler_flux: null argument");
+    return -2;
+  }
+  StateHold h;
+  int rc = subfv_ns_state_create(m, cfg, sol, 0.0, &h.s);
+  if (rc) return rc;
+  DevMesh& d = m->d;
+  if (reset_scalars(h.s)) return -1;
+  std::vector<double> g;
+  if (second_order) {
+    g.resize(15 * (size_t)d.ne);
+    grad_from_ref(grad, g.data(), d.ne);
+    SUBFV_CUDA(cudaMemcpyAsync(h.s->grad, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  }
+  launch_ns_euler_flux(d, h.s->P, h.s->U0, h.s->grad, h.s->fs, h.s->rhs1, second_order, h.s->sc);
+  std::vector<double> r(kRhs * (size_t)d.ne);
+  SUBFV_CUDA(cudaMemcpyAsync(r.data(), h.s->rhs1, r.size() * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  std::vector<double4> vph(vp ? d.nv : 0);
+  if (vp) SUBFV_CUDA(cudaMemcpyAsync(vph.data(), d.vp, vph.size() * sizeof(double4), cudaMemcpyDeviceToHost, d.stream));
+  const int st = handle_check_status(d);
+  SUBFV_CUDA(cudaGetLastError());
+  for (int c = 0; c < d.ne; ++c) {
+    for (int k = 0; k < 5; ++k) rhs[5 * (size_t)c + k] = r[kRhs * (size_t)c + k];
+    sum_lambda[c] = r[kRhs * (size_t)c + 5];
+  }
+  for (int v = 0; vp && v < d.nv; ++v) {
+    vp[3 * (size_t)v] = vph[v].x;
+    vp[3 * (size_t)v + 1] = vph[v].y;
+    vp[3 * (size_t)v + 2] = vph[v].z;
+  }
+  return st;
+}
+
+int subfv_compute_cell_grad_from_nodal_grad(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* sol, double* grad,
+                                            double* nodal_grad) {
+  if (!m || !sol || !grad) {
+    set_error("subfv_compute_cell_grad_from_nodal_grad: null argument");
+    return -2;
+  }
+  StateHold h;
+  int rc = subfv_ns_state_create(m, cfg, sol, 0.0, &h.s);
+  if (rc) return rc;
+  DevMesh& d = m->d;
+  if (reset_scalars(h.s)) return -1;
+  launch_ns_cell_grads(d, h.s->P, h.s->U0, h.s->ngrad, h.s->grad, h.s->sc);
+  std::vector<double> g(15 * (size_t)d.ne), ng(nodal_grad ? 15 * (size_t)d.nv : 0);
+  SUBFV_CUDA(cudaMemcpyAsync(g.data(), h.s->grad, g.size() * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  if (nodal_grad)
+    SUBFV_CUDA(cudaMemcpyAsync(ng.data(), h.s->ngrad, ng.size() * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  const int st = handle_check_status(d);
+  SUBFV_CUDA(cudaGetLastError());
+  grad_to_ref(g.data(), grad, d.ne);
+  if (nodal_grad) grad_to_ref(ng.data(), nodal_grad, d.nv);
+  return st;
+}
+
+int subfv_flux_limiting(subfv_mesh* m, const double* sol, double* rhs, const double* rhs_o2, const double* sum_lambda,
+                        double cfl) {
+  if (!m || !sol || !rhs || !rhs_o2 || !sum_lambda) {
+    set_error("subfv_flux_limiting: null argument");
+    return -2;
+  }
+  DevMesh& d = m->d;
+  if (handle_ensure_full_geometry(d)) return -1;
+  const size_t n = d.ne;
+  Scratch w(d.stream);
+  double *u = w.get<double>(5 * n), *r = w.get<double>(5 * n), *r2 = w.get<double>(5 * n), *sl = w.get<double>(n),
+         *slot = w.get<double>(1);
+  if (!u || !r || !r2 || !sl || !slot) {
+    set_error("subfv_flux_limiting: device allocation failed");
+    return -1;
+  }
+  const double big = 1e10;
+  SUBFV_CUDA(cudaMemcpyAsync(u, sol, 5 * n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(r, rhs, 5 * n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(r2, rhs_o2, 5 * n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(sl, sum_lambda, n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(slot, &big, sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  launch_proc_dtmin(d, sl, slot);
+  double dtmin = 0.0;
+  SUBFV_CUDA(cudaMemcpyAsync(&dtmin, slot, sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  launch_proc_flux_limiting(d, u, r, r2, sl, cfl * dtmin);
+  SUBFV_CUDA(cudaMemcpyAsync(rhs, r, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  SUBFV_CUDA(cudaGetLastError());
+  return 0;
+}
+
+int subfv_add_timedisc_and_solve(subfv_mesh* m, double* sol, double* rhs, double* diag, double* sum_lambda,
+                                 double* delta_sol, double* res, double* res_vect, double a1, double a2, double cfl,
+                                 double t, double tmax, double* dt) {
+  if (!m || !sol || !rhs || !sum_lambda || !delta_sol || !res || !res_vect || !dt) {
+    set_error("subfv_add_timedisc_and_solve: null argument");
+    return -2;
+  }
+  DevMesh& d = m->d;
+  if (handle_ensure_full_geometry(d)) return -1;
+  const size_t n = d.ne;
+  Scratch w(d.stream);
+  double *u = w.get<double>(5 * n), *r = w.get<double>(5 * n), *dl = w.get<double>(5 * n),
+         *rsq = w.get<double>(5 * n), *rn = w.get<double>(n), *sl = w.get<double>(n), *slots = w.get<double>(8);
+  double* dg = diag ? w.get<double>(25 * n) : nullptr;
+  if (!u || !r || !dl || !rsq || !rn || !sl || !slots || (diag && !dg)) {
+    set_error("subfv_add_timedisc_and_solve: device allocation failed");
+    return -1;
+  }
+  // slots: [0] min V / sum_lambda, [1] omega, [2..7] res and the five sums of squares
+  const double init[2] = {1e10, 1.0};
+  SUBFV_CUDA(cudaMemcpyAsync(u, sol, 5 * n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(r, rhs, 5 * n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(sl, sum_lambda, n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  if (diag) SUBFV_CUDA(cudaMemcpyAsync(dg, diag, 25 * n * sizeof(double), cudaMemcpyHostToDevice, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(slots, init, sizeof(init), cudaMemcpyHostToDevice, d.stream));
+  launch_proc_dtmin(d, sl, slots);
+  double dtmin = 0.0;
+  SUBFV_CUDA(cudaMemcpyAsync(&dtmin, slots, sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  // dt = cfl min(...); global time step: dt = min(tmax - t + 1e-12, dt), sum_lambda = 0
+  double dtv = cfl * dtmin;
+  const double cap = tmax - t + 1e-12;
+  dtv = dtv < cap ? dtv : cap;
+  launch_proc_timedisc(d, u, r, dg, dl, rn, rsq, a1, a2, dtv, slots + 1, slots + 2);
+  double hs[7];
+  SUBFV_CUDA(cudaMemcpyAsync(hs, slots + 1, sizeof(hs), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  const double omega = hs[0];
+  int st = 0;
+  if (omega <= 1e-6) st |= SUBFV_ERR_BAD_OMEGA;  // the reference prints BAD OMEGA and stops
+  if (omega < 1.0) dtv = (1.0 - omega) * dtv;
+  if (!st) launch_proc_apply(d, u, dl, a2 * omega);
+  SUBFV_CUDA(cudaMemcpyAsync(sol, u, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(rhs, r, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaMemcpyAsync(delta_sol, dl, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  if (diag) SUBFV_CUDA(cudaMemcpyAsync(diag, dg, 25 * n * sizeof(double), cudaMemcpyDeviceToHost, d.stream));
+  SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  SUBFV_CUDA(cudaGetLastError());
+  for (size_t c = 0; c < n; ++c) sum_lambda[c] = 0.0;
+  *res = hs[1];
+  for (int k = 0; k < 5; ++k) res_vect[k] = std::sqrt(hs[2 + k]);
+  *dt = dtv;
+  return st;
+}
+
+}  // extern "C"

@@ -170,6 +170,73 @@ def compute_rhs_ns_diag(mesh: Mesh, cfg: NsConfig, sol):
     return st, rhs, sl, diag
 
 
+def compute_euler_flux(mesh: Mesh, cfg: NsConfig, sol, rhs, grad, sum_lambda, second_order: bool, vp=None,
+                       h_p=None, mat_h_p=None):
+    """compute_euler_flux (ns_euler_module.F90:151-339): fills rhs (n_elems, 5),
+    sum_lambda (n_elems) and vp (n_vert, 3) in place; grad (n_elems, 5, 3), the
+    reference's grad(3, 5, n), is read when second_order. h_p and mat_h_p belong to the
+    ZB schemes and are ignored. Returns the status bits."""
+    sol = f64(sol)
+    g = f64(grad) if second_order else None
+    for a, shape in ((rhs, (mesh.n_elems, 5)), (sum_lambda, (mesh.n_elems,))):
+        assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"] and a.shape == shape
+    if vp is not None:
+        assert vp.dtype == np.float64 and vp.flags["C_CONTIGUOUS"] and vp.shape == (mesh.n_vert, 3)
+    c = cfg.to_c()
+    return check(_lib.load().subfv_compute_euler_flux(mesh._h, C.byref(c), pd(sol), pd(rhs), pd(g) if g is not None
+                                                      else None, pd(sum_lambda), int(bool(second_order)),
+                                                      pd(vp) if vp is not None else None),
+                 "subfv_compute_euler_flux")
+
+
+def compute_cell_grad_from_nodal_grad(mesh: Mesh, sol, grad, all_nodal_grad, method: int, cfg: NsConfig | None = None):
+    """compute_cell_grad_from_nodal_grad (ns_euler_recon_module.F90:8-59): fills grad
+    (n_elems, 5, 3) and all_nodal_grad (n_vert, 5, 3), the reference's (3, 5, n), in
+    place. cfg supplies the boundary kinds the limiters read (method overrides its
+    method)."""
+    from dataclasses import replace
+    cfg = replace(cfg or NsConfig(), method=int(method))
+    sol = f64(sol)
+    assert grad.dtype == np.float64 and grad.flags["C_CONTIGUOUS"] and grad.shape == (mesh.n_elems, 5, 3)
+    assert all_nodal_grad.dtype == np.float64 and all_nodal_grad.flags["C_CONTIGUOUS"] and \
+        all_nodal_grad.shape == (mesh.n_vert, 5, 3)
+    c = cfg.to_c()
+    return check(_lib.load().subfv_compute_cell_grad_from_nodal_grad(mesh._h, C.byref(c), pd(sol), pd(grad),
+                                                                     pd(all_nodal_grad)),
+                 "subfv_compute_cell_grad_from_nodal_grad")
+
+
+def flux_limiting(mesh: Mesh, sol, rhs, rhs_o2, sum_lambda, cfl: float):
+    """flux_limiting (ns_euler_recon_module.F90:560-601): rhs (n_elems, 5) in place."""
+    sol, rhs_o2, sum_lambda = f64(sol), f64(rhs_o2), f64(sum_lambda)
+    assert rhs.dtype == np.float64 and rhs.flags["C_CONTIGUOUS"] and rhs.shape == (mesh.n_elems, 5)
+    return check(_lib.load().subfv_flux_limiting(mesh._h, pd(sol), pd(rhs), pd(rhs_o2), pd(sum_lambda), float(cfl)),
+                 "subfv_flux_limiting")
+
+
+def add_timedisc_and_solve(mesh: Mesh, sol, rhs, diag, sum_lambda, delta_sol, num_procs, me, a1, a2, cfl, t,
+                           tmax=1e30):
+    """add_timedisc_and_solve (ns_euler_module.F90:521-609), one process, global time
+    step. sol, rhs, diag (n_elems, 5, 5) with diag[c].T the reference's diag(:, :, c), or
+    None for zero blocks), sum_lambda and delta_sol are updated in place; returns
+    (status bits, res, res_vect (5,), dt). Status SUBFV_ERR_BAD_OMEGA (8) leaves sol as it
+    was, where the reference stops."""
+    assert num_procs == 1, "one process: the MPI decomposition is not used"
+    for a, shape in ((sol, (mesh.n_elems, 5)), (rhs, (mesh.n_elems, 5)), (delta_sol, (mesh.n_elems, 5)),
+                     (sum_lambda, (mesh.n_elems,))):
+        assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"] and a.shape == shape
+    if diag is not None:
+        assert diag.dtype == np.float64 and diag.flags["C_CONTIGUOUS"] and diag.shape == (mesh.n_elems, 5, 5)
+    res, dt = C.c_double(), C.c_double()
+    rv = np.zeros(5)
+    st = check(_lib.load().subfv_add_timedisc_and_solve(mesh._h, pd(sol), pd(rhs), pd(diag) if diag is not None
+                                                        else None, pd(sum_lambda), pd(delta_sol), C.byref(res),
+                                                        pd(rv), float(a1), float(a2), float(cfl), float(t),
+                                                        float(tmax), C.byref(dt)),
+               "subfv_add_timedisc_and_solve")
+    return st, res.value, rv, dt.value
+
+
 class NsState:
     """Device-resident time loop of ns_main.F90:83-107 (graph-replayed iterations)."""
 
