@@ -350,11 +350,13 @@ def run_gresho(args, rank, world, local):
 def run_implicit(args, rank, world, local):
     """3-D periodic box [-0.5,0.5]^3 (the reference's stitching frame), 96^3 hexahedra
     (884,736 cells), interior vertices jittered +-5% of h (seed 1); uniform flow at Mach
-    0.3 plus 8 seeded Fourier velocity modes (5%); one backward-Euler step: first-order
-    two-wave residual, its exact frozen-speed Jacobian (5x5 BCSR, 7-point face stencil),
+    0.3 plus 8 seeded Fourier velocity modes (5%); Navier-Stokes at Re = 1000 (rho = 1,
+    |u| = 1, L = 1: mu = 1e-3) and Pr = 0.72; one backward-Euler step: first-order
+    two-wave residual with the viscous and heat terms, the exact frozen-speed Euler
+    Jacobian (5x5 BCSR, 7-point face stencil) plus the point-implicit diffusion blocks,
     block-Jacobi GMRES(30) to 1e-8 relative, CFL 10. FP64 GMRES and FP32-matrix GMRES
     inside FP64 iterative refinement; FP64 GMRES with the coloured LU-SGS preconditioner
-    beside them."""
+    and the inviscid step beside them."""
     import torch
     from subfv_b200 import meshgen
     from subfv_b200.mesh import Mesh
@@ -365,10 +367,13 @@ def run_implicit(args, rank, world, local):
     mesh = Mesh.from_raw(raw)
     setup_s = time.perf_counter() - t0
     sol0 = init_fourier_flow(mesh, seed=SEED)
-    cfg = NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5)
-    res = {"metric": "cell-updates/s", "workload": f"periodic_box_{n}^3_backward_euler", "cells": mesh.n_elems,
-           "mesh_setup_s": setup_s}
-    for name, refine, pc in (("fp64", False, 1), ("fp32_refine", True, 1), ("fp64_lusgs", False, 2)):
+    inviscid = NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5)
+    viscous = NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5,
+                       activate_diffusion=True, mu_p=1e-3, prandtl=0.72)
+    res = {"metric": "cell-updates/s", "workload": f"periodic_box_{n}^3_backward_euler_navier_stokes",
+           "cells": mesh.n_elems, "mesh_setup_s": setup_s, "reynolds": 1000, "prandtl": 0.72}
+    for name, refine, pc, cfg in (("fp64", False, 1, viscous), ("fp32_refine", True, 1, viscous),
+                                  ("fp64_lusgs", False, 2, viscous), ("fp64_inviscid", False, 1, inviscid)):
         s = NsState(mesh, cfg, sol0)
         s.implicit_step(cfl_implicit=10.0, refine_fp32=refine, precond=pc)  # warm-up (pattern, workspace)
         s2 = NsState(mesh, cfg, sol0)

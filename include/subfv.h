@@ -245,6 +245,8 @@ typedef struct subfv_ns_cfg {
   double bc_val_V[16][3];
   int32_t bc_type_T[16];      /* per tag: 0 or 1 neumann, 2 dirichlet (temperature bc_val_T) */
   double bc_val_T[16];
+  double prandtl;             /* kappa = mu Cv_p gamma / prandtl; 0 stands for the reference's
+                                 parameter Prandtl = 0.71 (ns_global_data_module.F90:10) */
 } subfv_ns_cfg;
 
 /* compute_rhs_ns (ns_main.F90:130-179, no diffusion): one residual evaluation.
@@ -303,10 +305,10 @@ int subfv_ns_advance(subfv_ns_state* s, int n_steps, int* steps_done, double* t)
 int subfv_ns_advance_async(subfv_ns_state* s, int n_steps);
 int subfv_ns_sync(subfv_ns_state* s, int* steps_done, double* t);
 int subfv_ns_get_sol(subfv_ns_state* s, double* sol);
-/* Node kernel layout: 0 one thread per vertex (default), 1 a group of lanes per vertex
- * (8, 16 or 32 as the mesh needs, one per subface) with the per-vertex sums formed in
- * shared memory; 8, 16 or 32: a group of at least that many lanes. Results are
- * bit-identical in every layout. */
+/* Node kernel layout: 0 one thread per vertex (the default from 32,768 vertices up), 1 a
+ * group of lanes per vertex (8, 16 or 32 as the mesh needs, one per subface) with the
+ * per-vertex sums formed in shared memory (the default on smaller meshes); 8, 16 or 32:
+ * a group of at least that many lanes. Results are bit-identical in every layout. */
 int subfv_ns_state_set_node_kernel(subfv_ns_state* s, int lanes);
 /* res = sum of |delta|_2 and res_vect(5) of the last add_timedisc_and_solve call */
 int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double* dt);
@@ -314,7 +316,11 @@ int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double*
  * Euler step U += dU with (V/dt I - d rhs/dU) dU = rhs(U): rhs the first-order two-wave
  * residual, its Jacobian assembled exactly with the wave speeds frozen, solved by
  * block-Jacobi GMRES(krylov) to |r| < rel_tol |rhs| (or FP64 iterative refinement around
- * an FP32-matrix GMRES when refine_fp32); dt = cfl_implicit * min V / sum_lambda. */
+ * an FP32-matrix GMRES when refine_fp32); dt = cfl_implicit * min V / sum_lambda. With
+ * activate_diffusion the viscous and heat terms join the residual and their
+ * point-implicit blocks mat_diag (the reference's add_timedisc_and_solve solves
+ * (mat_diag + V/dt I) U^{n+1} = rhs + V/dt U^n) join the diagonal blocks, the right-hand
+ * side being rhs - mat_diag U. */
 typedef struct subfv_implicit_stats {
   double dt, b_norm, res_norm;
   int32_t conv, restarts, outer;

@@ -226,7 +226,9 @@ class OracleMesh:
     @staticmethod
     def _ns_args(cfg):
         nb = max(1, int(cfg.get("n_bc", 0)))
-        dif = [np.ascontiguousarray(cfg.get("diff_dc", [1.329e-5, 1.716e-5, 273.15, 720.19471]), np.float64),
+        dc = list(cfg.get("diff_dc", [1.329e-5, 1.716e-5, 273.15, 720.19471]))
+        dc = dc + [0.71] * (5 - len(dc))
+        dif = [np.ascontiguousarray(dc, np.float64),
                np.ascontiguousarray(cfg.get("bc_type_V", np.zeros(nb)), np.int32),
                np.ascontiguousarray(cfg.get("bc_val_V", np.zeros((nb, 3))), np.float64).reshape(-1),
                np.ascontiguousarray(cfg.get("bc_type_T", np.zeros(nb)), np.int32),

@@ -14,8 +14,10 @@
 // PARITY UNPINNED (no Fortran compiler or LAPACK build of the reference here).
 #include "oracle.h"
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <vector>
 
 namespace oracle {
@@ -968,11 +970,12 @@ struct NsWork {
 struct DiffCfg {
   int active = 0, use_sutherland = 0;
   double mu_p = 1.329e-5, mu0 = 1.716e-5, T0 = 273.15, Cv_p = 720.19471;
+  double prandtl = 0.71;             // ns_global_data_module.F90:10 (a parameter there)
   int bcV[16] = {0}, bcT[16] = {0};  // 0 or 1 neumann, 2 dirichlet
   double valV[16][3] = {{0}}, valT[16] = {0};
 };
 static DiffCfg g_diff;
-static const double kPrandtl = 0.71, kC0 = 110.4;  // ns_global_data_module.F90:10,20
+static const double kC0 = 110.4;  // ns_global_data_module.F90:20
 
 // column-major n x n, A(i,j) = a[i + n*j]
 static void lapack_getrf(int n, double* a, int* ipiv) {
@@ -1105,18 +1108,100 @@ static void neumann_block(double al, double ap, double vol, const double* nl, co
     }
 }
 
+// The stencil of a vertex's diffusion systems. Not the reference's: at a periodic node
+// its extended lists (build_periodic_stencil, mesh_connectivity_module.F90:1075-1328)
+// index the images' subfaces and subcells by their own id_loc_around_node, which
+// collide, and at periodic edges and corners they name subcells the list does not hold.
+// Here every image of a periodic node (vertices joined through the subface lists) gets
+// the union over the images, in ascending vertex order: each image's subfaces in list
+// order, the second copy of a periodic face dropped (key: its two cells, unordered; a
+// boundary face: its cell, boundary and face), then each image's own subcells (mesh_vert
+// the image) in list order. Rows and columns are positions in these lists, and an image
+// applies the terms of its own subcells only. Without periodic faces the stencil is the
+// vertex's own lists, and the positions are its id_loc_around_node.
+struct DiffStencil {
+  std::vector<int> sf, se;              // 1-based ids
+  std::vector<int> lse, rse, lpos, rpos;  // per stencil subface: its cells' subcells (0 none), positions (-1)
+  std::vector<std::array<int, 4>> fpos;  // per stencil subcell: its subfaces' positions (-1 pad)
+};
+
+static std::vector<DiffStencil> diffusion_stencils(const Mesh& m) {
+  const int nv = m.n_vert;
+  std::vector<int> up(nv + 1);
+  for (int v = 1; v <= nv; ++v) up[v] = v;
+  auto root = [&](int x) {
+    while (up[x] != x) x = up[x];
+    return x;
+  };
+  for (int v = 1; v <= nv; ++v)
+    for (int k = 1; k <= m.vert[v].n_sub_faces_neigh; ++k) {
+      const int a = root(v), b = root(m.sub_face[m.vert[v].sub_face_neigh[k]].mesh_vert);
+      if (a < b) up[b] = a;
+      else if (b < a) up[a] = b;
+    }
+  std::map<int, std::vector<int>> images;
+  for (int v = 1; v <= nv; ++v) images[root(v)].push_back(v);
+  auto fkey = [&](int s) {
+    const int f = m.sub_face[s].mesh_face, l = m.face[f].left_neigh, r = m.face[f].right_neigh;
+    if (r > 0) return std::array<int, 3>{std::min(l, r), std::max(l, r), 0};
+    return std::array<int, 3>{l, r, f};
+  };
+  std::vector<DiffStencil> out(nv + 1);
+  for (auto& kv : images) {
+    DiffStencil st;
+    std::map<std::array<int, 3>, int> where;
+    std::map<int, int> cellpos;
+    for (int v : kv.second)
+      for (int k = 1; k <= m.vert[v].n_sub_faces_neigh; ++k) {
+        const int s = m.vert[v].sub_face_neigh[k];
+        if (where.find(fkey(s)) == where.end()) {
+          where[fkey(s)] = (int)st.sf.size();
+          st.sf.push_back(s);
+        }
+      }
+    for (int v : kv.second)
+      for (int k = 1; k <= m.vert[v].n_sub_elems_neigh; ++k) {
+        const int e = m.vert[v].sub_elem_neigh[k];
+        if (m.sub_elem[e].mesh_vert != v) continue;
+        cellpos[m.sub_elem[e].mesh_elem] = (int)st.se.size();
+        st.se.push_back(e);
+      }
+    for (int s : st.sf) {
+      const Face& f = m.face[m.sub_face[s].mesh_face];
+      int lp = -1, rp = -1;
+      if (cellpos.count(f.left_neigh)) lp = cellpos[f.left_neigh];
+      if (f.right_neigh > 0 && cellpos.count(f.right_neigh)) rp = cellpos[f.right_neigh];
+      st.lpos.push_back(lp);
+      st.rpos.push_back(rp);
+      st.lse.push_back(lp >= 0 ? st.se[lp] : 0);
+      st.rse.push_back(rp >= 0 ? st.se[rp] : 0);
+    }
+    for (int e : st.se) {
+      std::array<int, 4> q = {-1, -1, -1, -1};
+      for (int p = 1; p <= m.sub_elem[e].n_sub_faces && p <= 4; ++p) {
+        auto it = where.find(fkey(m.sub_elem[e].sub_face[p]));
+        q[p - 1] = it == where.end() ? -1 : it->second;
+      }
+      st.fpos.push_back(q);
+    }
+    for (int v : kv.second) out[v] = st;
+  }
+  return out;
+}
+
 // build_momentum_diff_mat_into_global_mat_diag (:195-318), all vertices
 static void momentum_diffusion(const Mesh& m, const double* sol, const double* mu, double mu0c, double* diag,
                                double* rhs) {
+  const std::vector<DiffStencil> stencils = diffusion_stencils(m);
   for (int v = 1; v <= m.n_vert; ++v) {
-    const Vert& V = m.vert[v];
-    const int nf = V.n_sub_faces_neigh, ne = V.n_sub_elems_neigh, F = 3 * nf, E = 3 * ne;
+    const DiffStencil& Z = stencils[v];
+    const int nf = (int)Z.sf.size(), ne = (int)Z.se.size(), F = 3 * nf, E = 3 * ne;
     std::vector<double> N(F * F, 0.0), S(F * E, 0.0), St(E * F, 0.0), B(F, 0.0);
     // build_momentum_diff_nodal_system (:7-193)
     for (int l = 0; l < nf; ++l) {
-      const int isfl = V.sub_face_neigh[l + 1];
+      const int isfl = Z.sf[l];
       const SubFace& sl = m.sub_face[isfl];
-      const int ifl0 = 3 * (sl.id_loc_around_node - 1);
+      const int ifl0 = 3 * l;
       const int re = sl.right_elem_neigh;
       bool neu = false, dir = false;
       if (re < 0) {  // bc_V_id: "" and "neumann" are Neumann (ns_global_data_module.F90:229-236)
@@ -1125,15 +1210,15 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
       } else if (re == 0) {
         neu = true;
       }
-      auto side = [&](int se, int elem, const double* nl, int mode) {
+      auto side = [&](int se, int elem, const double* nl, int mode, int sp) {
         // mode 0: N, S, St with the full block; 1: Neumann (N, S the plain block, St the
         // full one); 2: Dirichlet (St only)
         const SubElem& E0 = m.sub_elem[se];
-        const int ise0 = 3 * (E0.id_loc_around_node - 1);
+        const int ise0 = 3 * sp;
         const double mue = mu[elem - 1];
         for (int p = 0; p < E0.n_sub_faces; ++p) {
           const int isfp = E0.sub_face[p + 1];
-          const int ifp0 = 3 * (m.sub_face[isfp].id_loc_around_node - 1);
+          const int ifp0 = 3 * Z.fpos[sp][p];
           double np[3];
           const double ap = se_sign_norm(m, isfp, se, np);
           double blc[3][3], bn[3][3];
@@ -1152,13 +1237,14 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
       };
       const double nl[3] = {sl.norm[1], sl.norm[2], sl.norm[3]};
       const double nr[3] = {-sl.norm[1], -sl.norm[2], -sl.norm[3]};
+      const Face& fl = m.face[sl.mesh_face];
       if (!neu && !dir) {
-        side(sl.left_sub_elem_neigh, sl.left_elem_neigh, nl, 0);
-        side(sl.right_sub_elem_neigh, sl.right_elem_neigh, nr, 0);
+        side(Z.lse[l], fl.left_neigh, nl, 0, Z.lpos[l]);
+        side(Z.rse[l], fl.right_neigh, nr, 0, Z.rpos[l]);
       } else if (neu) {
-        side(sl.left_sub_elem_neigh, sl.left_elem_neigh, nl, 1);
+        side(Z.lse[l], fl.left_neigh, nl, 1, Z.lpos[l]);
       } else {
-        side(sl.left_sub_elem_neigh, sl.left_elem_neigh, nl, 2);
+        side(Z.lse[l], fl.left_neigh, nl, 2, Z.lpos[l]);
         for (int k = 0; k < 3; ++k) B[ifl0 + k] = sl.area * g_diff.valV[-re - 1][k];
         for (int i = 0; i < 3; ++i) {
           for (int c = 0; c < E; ++c) S[(ifl0 + i) + F * c] = 0.0;
@@ -1169,11 +1255,11 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
     }
     std::vector<double> Ve(E), Vf(F), SB(E), SNS(E * E), T1(E * F), tmp(F), SNSVe(E), blc3(9 * ne);
     for (int l = 0; l < ne; ++l) {
-      const double* u = sol + 5 * (m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem - 1);
+      const double* u = sol + 5 * (m.sub_elem[Z.se[l]].mesh_elem - 1);
       for (int k = 0; k < 3; ++k) Ve[3 * l + k] = u[1 + k] / u[0];
     }
     for (int p = 0; p < ne; ++p) {
-      const double* u = sol + 5 * (m.sub_elem[V.sub_elem_neigh[p + 1]].mesh_elem - 1);
+      const double* u = sol + 5 * (m.sub_elem[Z.se[p]].mesh_elem - 1);
       double Spc[3][3] = {{0}};
       for (int l = 0; l < nf; ++l)
         for (int i = 0; i < 3; ++i)
@@ -1192,7 +1278,8 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
     Vf = B;
     blas_gemv(E, E, SNS.data(), Ve.data(), SNSVe.data());
     for (int l = 0; l < ne; ++l) {
-      const int iel = m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem;
+      if (m.sub_elem[Z.se[l]].mesh_vert != v) continue;  // a periodic image's subcell
+      const int iel = m.sub_elem[Z.se[l]].mesh_elem;
       const double* u = sol + 5 * (iel - 1);
       double* D = diag + 25 * (iel - 1);
       double* r = rhs + 5 * (iel - 1);
@@ -1207,7 +1294,8 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
       }
     }
     for (int p = 0; p < ne; ++p) {  // viscous work
-      const int isep = V.sub_elem_neigh[p + 1];
+      const int isep = Z.se[p];
+      if (m.sub_elem[isep].mesh_vert != v) continue;
       const SubElem& Ep = m.sub_elem[isep];
       const int iep = Ep.mesh_elem;
       double Spc[3][3] = {{0}};
@@ -1215,7 +1303,7 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
         const int isfl = Ep.sub_face[l + 1];
         double nl[3];
         const double a = se_sign_norm(m, isfl, isep, nl);
-        const int q = 3 * (m.sub_face[isfl].id_loc_around_node - 1);
+        const int q = 3 * Z.fpos[p][l];
         double vm[3];
         for (int k = 0; k < 3; ++k) vm[k] = Vf[q + k] - Ve[3 * p + k];
         const double dd = vm[0] * nl[0] + vm[1] * nl[1] + vm[2] * nl[2];
@@ -1231,7 +1319,7 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
         const int isfl = Ep.sub_face[l + 1];
         double nl[3];
         const double a = se_sign_norm(m, isfl, isep, nl);
-        const int q = 3 * (m.sub_face[isfl].id_loc_around_node - 1);
+        const int q = 3 * Z.fpos[p][l];
         double sv[3];
         for (int i = 0; i < 3; ++i) {
           double s = 0.0;
@@ -1246,22 +1334,23 @@ static void momentum_diffusion(const Mesh& m, const double* sol, const double* m
 
 // build_diff_mat_into_global_mat_diag (ns_diffusion_module.F90:112-184), all vertices
 static void heat_diffusion(const Mesh& m, const double* sol, const double* mu, double* diag, double* rhs) {
+  const std::vector<DiffStencil> stencils = diffusion_stencils(m);
   for (int v = 1; v <= m.n_vert; ++v) {
-    const Vert& V = m.vert[v];
-    const int nf = V.n_sub_faces_neigh, ne = V.n_sub_elems_neigh;
+    const DiffStencil& Z = stencils[v];
+    const int nf = (int)Z.sf.size(), ne = (int)Z.se.size();
     std::vector<double> N(nf * nf, 0.0), S(nf * ne, 0.0), St(ne * nf, 0.0), B(nf, 0.0);
     for (int l = 0; l < nf; ++l) {  // build_diff_nodal_system (:7-110)
-      const int isfl = V.sub_face_neigh[l + 1];
+      const int isfl = Z.sf[l];
       const SubFace& sl = m.sub_face[isfl];
-      const int il = sl.id_loc_around_node - 1;
+      const int il = l;
       const Face& fl = m.face[sl.mesh_face];
-      auto side = [&](int se, int elem, const double* nl) {
+      auto side = [&](int se, int elem, const double* nl, int sp) {
         const SubElem& E0 = m.sub_elem[se];
-        const int ie = E0.id_loc_around_node - 1;
-        const double kap = mu[elem - 1] * g_diff.Cv_p * G / kPrandtl;
+        const int ie = sp;
+        const double kap = mu[elem - 1] * g_diff.Cv_p * G / g_diff.prandtl;
         for (int p = 0; p < E0.n_sub_faces; ++p) {
           const int isfp = E0.sub_face[p + 1];
-          const int ip = m.sub_face[isfp].id_loc_around_node - 1;
+          const int ip = Z.fpos[sp][p];
           double np[3];
           const double ap = se_sign_norm(m, isfp, se, np);
           const double b = kap * sl.area * ap * (1.0 / E0.volume) * (np[0] * nl[0] + np[1] * nl[1] + np[2] * nl[2]);
@@ -1272,9 +1361,9 @@ static void heat_diffusion(const Mesh& m, const double* sol, const double* mu, d
       };
       const double nl[3] = {sl.norm[1], sl.norm[2], sl.norm[3]};
       const double nr[3] = {-sl.norm[1], -sl.norm[2], -sl.norm[3]};
-      side(sl.left_sub_elem_neigh, fl.left_neigh, nl);
-      if (sl.right_sub_elem_neigh > 0) {
-        side(sl.right_sub_elem_neigh, fl.right_neigh, nr);
+      side(Z.lse[l], fl.left_neigh, nl, Z.lpos[l]);
+      if (Z.rse[l] > 0) {
+        side(Z.rse[l], fl.right_neigh, nr, Z.rpos[l]);
       } else if (fl.right_neigh < 0 && g_diff.bcT[-fl.right_neigh - 1] == 2) {
         B[il] = sl.area * g_diff.valT[-fl.right_neigh - 1];
         for (int c = 0; c < ne; ++c) S[il + nf * c] = 0.0;
@@ -1289,7 +1378,7 @@ static void heat_diffusion(const Mesh& m, const double* sol, const double* mu, d
     blas_gemv(nf, nf, N.data(), B.data(), tmp.data());
     blas_gemv(ne, nf, St.data(), tmp.data(), SB.data());
     for (int l = 0; l < ne; ++l) {
-      const double* u = sol + 5 * (m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem - 1);
+      const double* u = sol + 5 * (m.sub_elem[Z.se[l]].mesh_elem - 1);
       theta[l] = temp_u(u);
       const double uv[3] = {u[1] / u[0], u[2] / u[0], u[3] / u[0]};
       const double nn = fnorm2(uv, 3);
@@ -1301,7 +1390,8 @@ static void heat_diffusion(const Mesh& m, const double* sol, const double* mu, d
       b1[l] = s;
     }
     for (int l = 0; l < ne; ++l) {
-      const int iel = m.sub_elem[V.sub_elem_neigh[l + 1]].mesh_elem;
+      if (m.sub_elem[Z.se[l]].mesh_vert != v) continue;
+      const int iel = m.sub_elem[Z.se[l]].mesh_elem;
       const double* u = sol + 5 * (iel - 1);
       double* D = diag + 25 * (iel - 1);
       double& r5 = rhs[5 * (iel - 1) + 4];
@@ -1772,6 +1862,7 @@ void or_ns_set_diffusion(int active, int use_sutherland, const double* dc4, int 
   g_diff.mu0 = dc4[1];
   g_diff.T0 = dc4[2];
   g_diff.Cv_p = dc4[3];
+  g_diff.prandtl = dc4[4] > 0.0 ? dc4[4] : 0.71;
   for (int i = 0; i < n_bc && i < 16; ++i) {
     g_diff.bcV[i] = bcV[i];
     g_diff.bcT[i] = bcT[i];

@@ -2,6 +2,9 @@
 // (src/mesh/mesh_geometry_module.F90:16-57). One thread per face / cell / vertex;
 // each recomputes what it needs from the vertex coordinates in the reference's order.
 #include <algorithm>
+#include <array>
+#include <functional>
+#include <map>
 #include <vector>
 
 #include "../../include/subfv.h"
@@ -27,6 +30,113 @@ int alloc(T** dst, size_t n, size_t* bytes, cudaStream_t s) {
   SUBFV_CUDA(cudaMallocAsync((void**)dst, n * sizeof(T), s));
   SUBFV_CUDA(cudaMemsetAsync(*dst, 0, n * sizeof(T), s));
   *bytes += n * sizeof(T);
+  return 0;
+}
+
+// Diffusion stencils of DevMesh (layout in mesh_dev.cuh). Periodic images are the
+// vertices whose subface lists hold each other's subfaces (build_periodic_stencil,
+// mesh_connectivity_module.F90:1075-1328); a node's images are taken in ascending order.
+struct DiffStencil {
+  std::vector<int> sf_off, sf, se_off, se;
+  std::vector<int2> sf_se, sf_seloc;
+  std::vector<int4> se_sfloc;
+  int max_sf = 0, max_se = 0;
+  bool complete = true;
+};
+
+int build_diffusion_stencil(int nv, const std::vector<int>& vsf_off, const std::vector<int>& vsf,
+                            const std::vector<int>& vse_off, const std::vector<int>& vse,
+                            const std::vector<int>& sf_face, const std::vector<int>& sf_vert,
+                            const std::vector<int2>& flr, const std::vector<int>& se_elem,
+                            const std::vector<int>& se_vert, const std::vector<int4>& se_sf, DiffStencil* out) {
+  std::vector<int> parent(nv);
+  for (int v = 0; v < nv; ++v) parent[v] = v;
+  std::function<int(int)> find = [&](int x) {
+    while (parent[x] != x) x = parent[x] = parent[parent[x]];
+    return x;
+  };
+  for (int v = 0; v < nv; ++v)
+    for (int p = vsf_off[v]; p < vsf_off[v + 1]; ++p) {
+      const int a = find(v), b = find(sf_vert[vsf[p]]);
+      if (a != b) parent[std::max(a, b)] = std::min(a, b);
+    }
+  std::vector<std::vector<int>> members(nv);
+  for (int v = 0; v < nv; ++v) members[find(v)].push_back(v);  // ascending within a class
+  // a subface's key: its cells, unordered, for an interior face (the two copies of a
+  // periodic face share it); its cell, boundary and face for a boundary face
+  auto key = [&](int s) {
+    const int f = sf_face[s];
+    const int2 lr = flr[f];
+    if (lr.y >= 0) return std::array<long, 3>{std::min(lr.x, lr.y), std::max(lr.x, lr.y), -1};
+    return std::array<long, 3>{lr.x, lr.y, f};
+  };
+  struct Cls {
+    std::vector<int> sf, se;
+    std::vector<int2> sf_se, sf_seloc;
+    std::vector<int4> se_sfloc;
+  };
+  std::vector<int> cls_of(nv, -1);
+  std::vector<Cls> classes;
+  for (int r = 0; r < nv; ++r) {
+    if (members[r].empty()) continue;
+    Cls c;
+    std::map<std::array<long, 3>, int> fpos;
+    std::map<int, int> epos;  // cell -> position in the subcell list
+    for (int v : members[r])
+      for (int p = vsf_off[v]; p < vsf_off[v + 1]; ++p) {
+        const int sfi = vsf[p];
+        if (fpos.emplace(key(sfi), (int)c.sf.size()).second) c.sf.push_back(sfi);
+      }
+    for (int v : members[r])
+      for (int q = vse_off[v]; q < vse_off[v + 1]; ++q) {
+        const int e = vse[q];
+        if (se_vert[e] != v) continue;
+        if (!epos.emplace(se_elem[e], (int)c.se.size()).second) {
+          set_error("subfv_mesh_create: a cell touches one periodic node twice");
+          return -2;
+        }
+        c.se.push_back(e);
+      }
+    for (int sfi : c.sf) {
+      const int2 lr = flr[sf_face[sfi]];
+      int2 pos = make_int2(-1, -1), ids = make_int2(-1, -1);
+      auto it = epos.find(lr.x);
+      if (it != epos.end()) pos.x = it->second, ids.x = c.se[it->second];
+      if (lr.y >= 0 && (it = epos.find(lr.y)) != epos.end()) pos.y = it->second, ids.y = c.se[it->second];
+      if (pos.x < 0 || (lr.y >= 0 && pos.y < 0)) out->complete = false;
+      c.sf_se.push_back(ids);
+      c.sf_seloc.push_back(pos);
+    }
+    for (int e : c.se) {
+      const int4 q4 = se_sf[e];
+      const int q[4] = {q4.x, q4.y, q4.z, q4.w};
+      int loc[4] = {-1, -1, -1, -1};
+      for (int k = 0; k < 4; ++k)
+        if (q[k] >= 0) {
+          auto jt = fpos.find(key(q[k]));
+          loc[k] = jt == fpos.end() ? -1 : jt->second;
+          if (loc[k] < 0) out->complete = false;
+        }
+      c.se_sfloc.push_back(make_int4(loc[0], loc[1], loc[2], loc[3]));
+    }
+    for (int v : members[r]) cls_of[v] = (int)classes.size();
+    classes.push_back(std::move(c));
+  }
+  DiffStencil& D = *out;
+  D.sf_off.assign(nv + 1, 0);
+  D.se_off.assign(nv + 1, 0);
+  for (int v = 0; v < nv; ++v) {
+    const Cls& c = classes[cls_of[v]];
+    D.sf_off[v + 1] = D.sf_off[v] + (int)c.sf.size();
+    D.se_off[v + 1] = D.se_off[v] + (int)c.se.size();
+    D.max_sf = std::max(D.max_sf, (int)c.sf.size());
+    D.max_se = std::max(D.max_se, (int)c.se.size());
+    D.sf.insert(D.sf.end(), c.sf.begin(), c.sf.end());
+    D.sf_se.insert(D.sf_se.end(), c.sf_se.begin(), c.sf_se.end());
+    D.sf_seloc.insert(D.sf_seloc.end(), c.sf_seloc.begin(), c.sf_seloc.end());
+    D.se.insert(D.se.end(), c.se.begin(), c.se.end());
+    D.se_sfloc.insert(D.se_sfloc.end(), c.se_sfloc.begin(), c.se_sfloc.end());
+  }
   return 0;
 }
 
@@ -204,6 +314,19 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
     std::stable_sort(vorder.begin(), vorder.end(), [&](int a, int b) { return vkey[a] < vkey[b]; });
   }
   if (upload(&m->forder, forder, B, s) || upload(&m->vorder, vorder, B, s)) return -1;
+  {
+    DiffStencil D;
+    if (int rc = build_diffusion_stencil(nv, vsf_off, vsf, vse_off, vse, sf_face, sf_vert, flr, se_elem, se_vert,
+                                         se_sf, &D))
+      return rc;
+    m->max_dsf = D.max_sf;
+    m->max_dse = D.max_se;
+    m->dstencil_ok = D.complete ? 1 : 0;
+    if (upload(&m->dsf_off, D.sf_off, B, s) || upload(&m->dsf, D.sf, B, s) || upload(&m->dsf_se, D.sf_se, B, s) ||
+        upload(&m->dsf_seloc, D.sf_seloc, B, s) || upload(&m->dse_off, D.se_off, B, s) ||
+        upload(&m->dse, D.se, B, s) || upload(&m->dse_sfloc, D.se_sfloc, B, s))
+      return -1;
+  }
   if (upload(&m->x, x, B, s) || alloc(&m->vp, nv, B, s) || alloc(&m->vol_v, nv, B, s) || upload(&m->is_bound, isb, B, s) ||
       upload(&m->fvert, fvert, B, s) || upload(&m->flr, flr, B, s) || upload(&m->fsf, fsf, B, s) ||
       alloc(&m->fc, nf, B, s) || alloc(&m->fn, nf, B, s) || upload(&m->sf_face, sf_face, B, s) ||
@@ -225,7 +348,8 @@ void devmesh_free(DevMesh* m) {
                   m->sf_face, m->sf_vert, m->sf_se, m->sf_loc, m->sfn, m->sfa, m->se_elem, m->se_vert, m->se_loc,
                   m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
                   m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
-                  m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS, m->fpos, m->gface, m->gsub, m->forder, m->vorder};
+                  m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS, m->fpos, m->gface, m->gsub, m->forder, m->vorder,
+                  m->dsf_off, m->dsf, m->dsf_se, m->dsf_seloc, m->dse_off, m->dse, m->dse_sfloc};
   // stream-ordered frees: they wait for the mesh stream's work but not for other
   // streams (a caller that used the mesh elsewhere orders that work first)
   for (void* p : ptrs)

@@ -70,6 +70,24 @@ struct DevMesh {
   // gather-bound kernels keep the numbering order, which coalesces better.
   int* forder = nullptr;
   int* vorder = nullptr;
+  // Diffusion stencils (built at creation). A vertex's diffusion system runs over the
+  // subfaces dsf[dsf_off[v]..] and subcells dse[dse_off[v]..]; rows and columns are the
+  // positions in these lists. Without periodic faces they are the vertex's own lists
+  // (positions = the reference's id_loc_around_node). At a periodic node every image
+  // vertex gets the same stencil: the union over the images of their subfaces (the two
+  // copies of a periodic face merged, keyed by their cells) and their own subcells.
+  // dsf_se: a stencil subface's left / right subcells (-1 none), dsf_seloc their
+  // positions in the subcell list; dse_sfloc: a stencil subcell's subfaces' positions in
+  // the subface list (-1 pad).
+  int* dsf_off = nullptr;
+  int* dsf = nullptr;
+  int2* dsf_se = nullptr;
+  int2* dsf_seloc = nullptr;
+  int* dse_off = nullptr;
+  int* dse = nullptr;
+  int4* dse_sfloc = nullptr;
+  int max_dsf = 0, max_dse = 0;
+  int dstencil_ok = 1;  // every stencil subface's subcells and subcell's subfaces found
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;

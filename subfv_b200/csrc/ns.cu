@@ -2109,6 +2109,28 @@ void launch_be_assemble(const DevMesh& m, const NsParams& P, const double* U, co
 void launch_be_pack_rhs(const DevMesh& m, const double* rhs, double* b) {
   k_be_pack_rhs<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m.ne, rhs, b);
 }
+// The diffusion terms in the backward-Euler system: the reference's point-implicit
+// blocks (add_timedisc_and_solve solves (mat_diag + a1 V/dt I) U^{n+1} = rhs + a1 V/dt U^n,
+// ns_euler_module.F90:565-576) go onto the diagonal blocks, and the right-hand side
+// becomes rhs - mat_diag U (the same system written for the increment).
+__global__ void k_be_add_diffusion(int ne, const int* __restrict__ dblk, const double* __restrict__ diag25,
+                                   const double* __restrict__ U, double* __restrict__ v, double* __restrict__ b) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ne) return;
+  const double* D = diag25 + 25 * (size_t)c;
+  double* blk = v + 25 * (size_t)dblk[c];
+  for (int e = 0; e < 25; ++e) blk[e] = blk[e] + D[e];
+  const double* u = U + kRec * (size_t)c;
+  for (int a = 0; a < 5; ++a) {
+    double s = 0.0;
+    for (int k = 0; k < 5; ++k) s = s + D[a + 5 * k] * u[k];
+    b[5 * (size_t)c + a] = b[5 * (size_t)c + a] - s;
+  }
+}
+void launch_be_add_diffusion(const DevMesh& m, const int* dblk, const double* diag25, const double* U, double* v,
+                             double* b) {
+  k_be_add_diffusion<<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m.ne, dblk, diag25, U, v, b);
+}
 void launch_be_update(const DevMesh& m, double* U, const double* x) {
   k_be_update<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, U, x);
 }

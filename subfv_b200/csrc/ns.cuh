@@ -80,6 +80,10 @@ void launch_be_assemble(const DevMesh& m, const NsParams& P, const double* U, co
                         const NsScalars* sc);
 void launch_be_pack_rhs(const DevMesh& m, const double* rhs, double* b);
 void launch_be_update(const DevMesh& m, double* U, const double* x);
+// the diffusion blocks diag25 (column-major 5 x 5 per cell) onto the diagonal blocks
+// (dblk) of the Jacobian values v, and b -= diag25 U
+void launch_be_add_diffusion(const DevMesh& m, const int* dblk, const double* diag25, const double* U, double* v,
+                             double* b);
 int ns_partial_blocks(const DevMesh& m);
 
 // The reference's module procedures one at a time (host-buffer entries of ns_procs.cu):

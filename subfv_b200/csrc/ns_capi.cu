@@ -19,6 +19,7 @@ struct ImplicitCtx {
   GmresWork W;
   int *jq_off = nullptr, *jq = nullptr, *jblk = nullptr, *row_off = nullptr, *dblk = nullptr;
   double *b = nullptr, *x = nullptr;
+  double* ddiag = nullptr;      // the diffusion blocks (25 per cell) when the state has diffusion
   std::vector<int> row1, col1;  // 1-based pattern (bcsr_matrix_type)
   int krylov = 0;
 };
@@ -38,6 +39,8 @@ struct subfv_ns_state {
 
 namespace {
 
+constexpr int kSmallMeshVertices = 32768;
+
 int check_cfg(const subfv_ns_cfg* c) {
   if (!c || (c->scheme < 1 || c->scheme > 8 || c->scheme == 7) || (c->method < 0 || c->method > 6) ||
       c->local_time_step != 0 || c->n_bc < 0 || c->n_bc > 16 || (c->precision < 0 || c->precision > 2)) {
@@ -56,7 +59,8 @@ int check_cfg(const subfv_ns_cfg* c) {
         set_error("subfv_ns: diffusion boundary kind not recognized (0/1 neumann, 2 dirichlet)");
         return -2;
       }
-    if (!(c->Cv_p > 0.0) || !(c->mu_p >= 0.0) || (c->use_sutherland && !(c->mu0 > 0.0 && c->T0 > 0.0))) {
+    if (!(c->Cv_p > 0.0) || !(c->mu_p >= 0.0) || (c->use_sutherland && !(c->mu0 > 0.0 && c->T0 > 0.0)) ||
+        !(c->prandtl >= 0.0)) {
       set_error("subfv_ns: diffusion parameters out of range");
       return -2;
     }
@@ -179,6 +183,10 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
   auto* s = new subfv_ns_state();
   s->m = m;
   s->P = ns_params_from(*cfg);
+  // a small mesh leaves most of the GPU idle with one thread per vertex: a group of lanes
+  // per vertex (one per subface) shortens each vertex's serial chain (Gresho 64x64: 0.39
+  // against 0.48 ms per iteration); subfv_ns_state_set_node_kernel overrides it
+  if (d.nv < kSmallMeshVertices) s->P.node_group = 1;
   const size_t ne = d.ne, nv = d.nv, nse = d.nse;
   cudaStream_t q = d.stream;
   if (dalloc(&s->U0, kRec * ne, q) || dalloc(&s->U1, kRec * ne, q) || dalloc(&s->fs, kNsFs * nse, q) ||
@@ -190,12 +198,11 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
     return -1;
   }
   if (s->P.diff) {
-    // the reference's diffusion indexes the periodic extension of a vertex's lists by the
-    // subfaces' original local ids, which collide; only meshes without periodic faces
+    // periodic nodes use the union stencil of their images (mesh_dev.cuh)
     const size_t smem = diffusion_smem_bytes(d);
-    if (!d.vsf_identity || smem > 200 * 1024 || d.max_vsf > 32) {
-      set_error(!d.vsf_identity ? "subfv_ns: diffusion on a mesh with periodic faces is not supported"
-                                : "subfv_ns: a vertex's diffusion system exceeds shared memory");
+    if (!d.dstencil_ok || smem > 200 * 1024 || d.max_dsf > 32) {
+      set_error(!d.dstencil_ok ? "subfv_ns: a periodic node's diffusion stencil is incomplete"
+                               : "subfv_ns: a vertex's diffusion system exceeds shared memory");
       subfv_ns_state_destroy(s);
       return -2;
     }
@@ -246,6 +253,7 @@ int subfv_ns_state_destroy(subfv_ns_state* s) {
     int* ip[] = {c->jq_off, c->jq, c->jblk, c->row_off, c->dblk};
     for (int* p : ip) cudaFree(p);
     cudaFree(c->b);
+    cudaFree(c->ddiag);
     cudaFree(c->x);
     gmres_work_free(&c->W);
     bcsr_free(&c->A);
@@ -443,6 +451,7 @@ int implicit_setup(subfv_ns_state* s, int krylov) {
       return -1;
     SUBFV_CUDA(cudaMalloc(&c->b, 5 * (size_t)ne * sizeof(double)));
     SUBFV_CUDA(cudaMalloc(&c->x, 5 * (size_t)ne * sizeof(double)));
+    if (s->P.diff) SUBFV_CUDA(cudaMalloc(&c->ddiag, 25 * (size_t)ne * sizeof(double)));
   }
   ImplicitCtx* c = s->imp;
   gmres_work_free(&c->W);
@@ -477,7 +486,12 @@ int implicit_assemble(subfv_ns_state* s, double cfl_implicit, double dt_force, d
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
   const double dt = dt_force > 0.0 ? dt_force : cfl_implicit * dtred;
   launch_be_assemble(d, Q, s->U0, c->jq_off, c->jq, c->jblk, c->row_off, c->dblk, c->A.v, dt, s->sc);
+  if (s->P.diff) {  // the viscous and heat terms at U0, with their point-implicit blocks
+    launch_ns_diffusion(d, s->D, s->U0, s->dterm, s->mu0c);
+    launch_ns_diffusion_apply(d, s->dterm, s->D.kd, s->rhs1, c->ddiag);
+  }
   launch_be_pack_rhs(d, s->rhs1, c->b);
+  if (s->P.diff) launch_be_add_diffusion(d, c->dblk, c->ddiag, s->U0, c->A.v, c->b);
   if (bcsr_set_values(&c->A, c->A.v, true)) return -1;
   *dt_out = dt;
   return 0;
@@ -494,8 +508,8 @@ int subfv_ns_implicit_step(subfv_ns_state* s, double cfl_implicit, int krylov, d
 
 int subfv_ns_implicit_step_ex(subfv_ns_state* s, double cfl_implicit, int krylov, double rel_tol, int refine_fp32,
                               int precond, subfv_implicit_stats* out) {
-  if (!s || krylov < 1 || krylov > 200 || !(rel_tol > 0.0) || (precond != 1 && precond != 2) || s->P.diff) {
-    set_error("subfv_ns_implicit_step: bad argument (the backward-Euler step has no diffusion blocks)");
+  if (!s || krylov < 1 || krylov > 200 || !(rel_tol > 0.0) || (precond != 1 && precond != 2)) {
+    set_error("subfv_ns_implicit_step: bad argument");
     return -2;
   }
   DevMesh& d = s->m->d;
@@ -553,10 +567,6 @@ int subfv_ns_implicit_step_ex(subfv_ns_state* s, double cfl_implicit, int krylov
 }
 
 int subfv_ns_be_jacobian(subfv_ns_state* s, double dt, int32_t* row, int32_t* col, double* v, int64_t cap) {
-  if (s && s->P.diff) {
-    set_error("subfv_ns_be_jacobian: the backward-Euler Jacobian has no diffusion blocks");
-    return -2;
-  }
   if (implicit_setup(s, 4)) return -1;
   ImplicitCtx* c = s->imp;
   if ((int64_t)c->col1.size() > cap) {

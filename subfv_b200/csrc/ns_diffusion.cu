@@ -12,7 +12,7 @@ namespace subfv {
 
 namespace {
 
-constexpr double kGamma = 1.4, kPrandtl = 0.71, kC0 = 110.4;  // ns_global_data_module.F90:9,10,20
+constexpr double kGamma = 1.4, kC0 = 110.4;  // ns_global_data_module.F90:9,20
 
 __device__ inline double temp_u(const double* u, double cv) {  // ns_euler_primitives_module.F90:52-63
   const double tau = 1.0 / u[0];
@@ -255,7 +255,7 @@ __device__ inline void neumann_block(double al, double ap, double vol, const dou
 __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, const double* __restrict__ U,
                                                      double* __restrict__ dterm, const double* __restrict__ mu0c_p) {
   extern __shared__ double sm[];
-  const DiffSmem L = diff_layout(m.max_vsf, m.max_vse);
+  const DiffSmem L = diff_layout(m.max_dsf, m.max_dse);
   const int lane = threadIdx.x;
   double *N = sm + L.N, *S = sm + L.S, *St = sm + L.St, *T1 = sm + L.T1, *B = sm + L.B;
   double *Vf = sm + L.Vf, *tmp = sm + L.tmp, *work = sm + L.work, *Ve = sm + L.Ve, *SB = sm + L.SB;
@@ -263,8 +263,8 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
   int* ipiv = reinterpret_cast<int*>(sm + L.ipiv);
   const double mu0c = *mu0c_p;
   for (int v = blockIdx.x; v < m.nv; v += gridDim.x) {
-    const int f0 = m.vsf_off[v], nf = m.vsf_off[v + 1] - f0;
-    const int s0 = m.vse_off[v], ne = m.vse_off[v + 1] - s0;
+    const int f0 = m.dsf_off[v], nf = m.dsf_off[v + 1] - f0;
+    const int s0 = m.dse_off[v], ne = m.dse_off[v + 1] - s0;
     const int F = 3 * nf, E = 3 * ne;
     // ---- momentum: build_momentum_diff_nodal_system (:7-193)
     for (int e = lane; e < F * F; e += 32) N[e] = 0.0;
@@ -272,10 +272,10 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     for (int e = lane; e < F; e += 32) B[e] = 0.0;
     __syncwarp();
     for (int l = lane; l < nf; l += 32) {  // lane l owns row block l of N and S, column block l of St
-      const int sf = m.vsf[f0 + l];
-      const int ifl0 = 3 * m.sf_loc[sf];
+      const int sf = m.dsf[f0 + l];
+      const int ifl0 = 3 * l;
       const int2 lr = m.flr[m.sf_face[sf]];
-      const int2 se2 = m.sf_se[sf];
+      const int2 se2 = m.dsf_se[f0 + l], sep = m.dsf_seloc[f0 + l];
       const double4 sn = m.sfn[sf];
       const double al = sn.w;
       int kind = 0;  // 0 interior, 1 neumann (the default wall, and a tag's "" or "neumann"), 2 dirichlet
@@ -286,17 +286,17 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
         tag = -(lr.y + 1) - 1;
         kind = D.bcV[tag] == 2 ? 2 : 1;
       }
-      auto side = [&](int se, int elem, const double* nl, int mode) {
+      auto side = [&](int se, int elem, const double* nl, int mode, int sp) {
         double u[5];
         load_u(U, elem, u);
         const double mue = mu_of(D, u);
-        const int ise0 = 3 * m.se_loc[se];
-        const int4 q4 = m.se_sf[se];
+        const int ise0 = 3 * sp;
+        const int4 q4 = m.se_sf[se], ql = m.dse_sfloc[s0 + sp];
         const double vol = m.vol_se[se];
         const int nsf = n_sub_faces(q4);
         for (int p = 0; p < nsf; ++p) {
           const int sfp = sf_of(q4, p);
-          const int ifp0 = 3 * m.sf_loc[sfp];
+          const int ifp0 = 3 * sf_of(ql, p);
           double np[3];
           const double ap = oriented(m, sfp, se, np);
           double blc[3][3], bn[3][3];
@@ -315,12 +315,12 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
       };
       const double nl[3] = {sn.x, sn.y, sn.z}, nr[3] = {-sn.x, -sn.y, -sn.z};
       if (kind == 0) {
-        side(se2.x, lr.x, nl, 0);
-        side(se2.y, lr.y, nr, 0);
+        side(se2.x, lr.x, nl, 0, sep.x);
+        side(se2.y, lr.y, nr, 0, sep.y);
       } else if (kind == 1) {
-        side(se2.x, lr.x, nl, 1);
+        side(se2.x, lr.x, nl, 1, sep.x);
       } else {
-        side(se2.x, lr.x, nl, 2);
+        side(se2.x, lr.x, nl, 2, sep.x);
         for (int k = 0; k < 3; ++k) B[ifl0 + k] = al * D.valV[tag][k];
         for (int i = 0; i < 3; ++i) {
           for (int c = 0; c < E; ++c) S[(ifl0 + i) + F * c] = 0.0;
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     // ---- build_momentum_diff_mat_into_global_mat_diag (:233-318)
     for (int l = lane; l < ne; l += 32) {
       double u[5];
-      load_u(U, m.se_elem[m.vse[s0 + l]], u);
+      load_u(U, m.se_elem[m.dse[s0 + l]], u);
       for (int k = 0; k < 3; ++k) Ve[3 * l + k] = u[1 + k] / u[0];
       double Spc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
       for (int c = 0; c < nf; ++c)
@@ -357,10 +357,12 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     warp_gemv(E, F, St, tmp, SB, lane);
     warp_gemv(E, E, SNSm, Ve, SNSVe, lane);
     for (int l = lane; l < ne; l += 32) {
-      const int se = m.vse[s0 + l];
+      const int se = m.dse[s0 + l];
+      if (m.se_vert[se] != v) continue;  // a periodic image's subcell: its own vertex writes it
       double u[5];
       load_u(U, m.se_elem[se], u);
       double* t = dterm + (size_t)D.kd * se;
+      const int4 ql = m.dse_sfloc[s0 + l];
       for (int i = 0; i < 3; ++i) {
         double mv = 0.0;
         for (int k = 0; k < 3; ++k) mv = mv + SNSm[(3 * l + i) + E * (3 * l + k)] * Ve[3 * l + k];
@@ -381,7 +383,7 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
         const int sf = sf_of(q4, k);
         double nl[3];
         const double a = oriented(m, sf, se, nl);
-        const int q = 3 * m.sf_loc[sf];
+        const int q = 3 * sf_of(ql, k);
         double vm[3];
         for (int d = 0; d < 3; ++d) vm[d] = work[q + d] - Ve[3 * l + d];
         const double dd = vm[0] * nl[0] + vm[1] * nl[1] + vm[2] * nl[2];
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
         const int sf = sf_of(q4, k);
         double nl[3];
         const double a = oriented(m, sf, se, nl);
-        const int q = 3 * m.sf_loc[sf];
+        const int q = 3 * sf_of(ql, k);
         double sv[3];
         for (int i = 0; i < 3; ++i) {
           double s = 0.0;
@@ -416,23 +418,23 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     for (int e = lane; e < nf; e += 32) B[e] = 0.0;
     __syncwarp();
     for (int l = lane; l < nf; l += 32) {
-      const int sf = m.vsf[f0 + l];
-      const int il = m.sf_loc[sf];
+      const int sf = m.dsf[f0 + l];
+      const int il = l;
       const int2 lr = m.flr[m.sf_face[sf]];
-      const int2 se2 = m.sf_se[sf];
+      const int2 se2 = m.dsf_se[f0 + l], sep = m.dsf_seloc[f0 + l];
       const double4 sn = m.sfn[sf];
       const double al = sn.w;
-      auto side = [&](int se, int elem, const double* nl) {
+      auto side = [&](int se, int elem, const double* nl, int sp) {
         double u[5];
         load_u(U, elem, u);
-        const double kap = mu_of(D, u) * D.Cv_p * kGamma / kPrandtl;
-        const int ie = m.se_loc[se];
-        const int4 q4 = m.se_sf[se];
+        const double kap = mu_of(D, u) * D.Cv_p * kGamma / D.prandtl;
+        const int ie = sp;
+        const int4 q4 = m.se_sf[se], ql = m.dse_sfloc[s0 + sp];
         const double vol = m.vol_se[se];
         const int nsf = n_sub_faces(q4);
         for (int p = 0; p < nsf; ++p) {
           const int sfp = sf_of(q4, p);
-          const int ip = m.sf_loc[sfp];
+          const int ip = sf_of(ql, p);
           double np[3];
           const double ap = oriented(m, sfp, se, np);
           const double b = kap * al * ap * (1.0 / vol) * (np[0] * nl[0] + np[1] * nl[1] + np[2] * nl[2]);
@@ -442,9 +444,9 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
         }
       };
       const double nl[3] = {sn.x, sn.y, sn.z}, nr[3] = {-sn.x, -sn.y, -sn.z};
-      side(se2.x, lr.x, nl);
+      side(se2.x, lr.x, nl, sep.x);
       if (se2.y >= 0) {
-        side(se2.y, lr.y, nr);
+        side(se2.y, lr.y, nr, sep.y);
       } else if (lr.y < -1 && D.bcT[-(lr.y + 1) - 1] == 2) {
         B[il] = al * D.valT[-(lr.y + 1) - 1];
         for (int c = 0; c < ne; ++c) S[il + nf * c] = 0.0;
@@ -460,7 +462,7 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     warp_gemv(ne, nf, St, tmp, SB, lane);
     for (int l = lane; l < ne; l += 32) {
       double u[5];
-      load_u(U, m.se_elem[m.vse[s0 + l]], u);
+      load_u(U, m.se_elem[m.dse[s0 + l]], u);
       theta[l] = temp_u(u, D.Cv_p);
       const double nn = scaled_norm3(u[1] / u[0], u[2] / u[0], u[3] / u[0]);
       P[5 * l] = (nn * nn - u[4] / u[0]) / (u[0] * D.Cv_p);
@@ -472,7 +474,8 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     }
     __syncwarp();
     for (int l = lane; l < ne; l += 32) {
-      const int se = m.vse[s0 + l];
+      const int se = m.dse[s0 + l];
+      if (m.se_vert[se] != v) continue;
       double u[5];
       load_u(U, m.se_elem[se], u);
       double* t = dterm + (size_t)D.kd * se;
@@ -513,18 +516,19 @@ DiffParams diff_params_from(const subfv_ns_cfg& c, const DevMesh& m) {
   D.mu0 = c.mu0;
   D.T0 = c.T0;
   D.Cv_p = c.Cv_p;
+  D.prandtl = c.prandtl > 0.0 ? c.prandtl : 0.71;  // ns_global_data_module.F90:10
   for (int i = 0; i < 16; ++i) {
     D.bcV[i] = c.bc_type_V[i];
     D.bcT[i] = c.bc_type_T[i];
     D.valT[i] = c.bc_val_T[i];
     for (int k = 0; k < 3; ++k) D.valV[i][k] = c.bc_val_V[i][k];
   }
-  D.kd = kDiffHead + std::max(1, m.max_vse);
+  D.kd = kDiffHead + std::max(1, m.max_dse);
   return D;
 }
 
 size_t diffusion_smem_bytes(const DevMesh& m) {
-  return sizeof(double) * (size_t)diff_layout(m.max_vsf, m.max_vse).total;
+  return sizeof(double) * (size_t)diff_layout(m.max_dsf, m.max_dse).total;
 }
 
 int diffusion_prepare(size_t smem) {

@@ -30,6 +30,7 @@ struct DiffParams {
   double mu_p, mu0, T0, Cv_p;
   int bcV[16], bcT[16];  // 0 or 1 neumann, 2 dirichlet
   double valV[16][3], valT[16];
+  double prandtl;
   int kd;  // doubles per corner record
 };
 
@@ -66,7 +67,7 @@ __device__ inline void apply_diffusion_terms(const DevMesh& m, int c, const doub
     const int se = m.cse_sorted[q];
     const double* t = dterm + (size_t)kd * se;
     const int v = m.se_vert[se];
-    const int nsen = m.vse_off[v + 1] - m.vse_off[v];
+    const int nsen = m.dse_off[v + 1] - m.dse_off[v];  // the length of the writing vertex's stencil
     for (int p = 0; p < nsen; ++p) r[4] = r[4] + t[kDiffHead + p];
     for (int k = 0; k < 5; ++k) D[4 + 5 * k] = D[4 + 5 * k] + t[31 + k];
     r[4] = (((r[4] - t[36]) + t[37]) - t[38]) + t[39];

@@ -49,6 +49,7 @@ module subfv_c
     real(c_double)     :: bc_val_V(3, 16)
     integer(c_int32_t) :: bc_type_T(16)
     real(c_double)     :: bc_val_T(16)
+    real(c_double)     :: prandtl           ! 0: the reference's Prandtl = 0.71
   end type subfv_ns_cfg
 
   interface

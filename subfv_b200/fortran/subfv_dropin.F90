@@ -347,7 +347,7 @@ contains
   function dropin_ns_cfg() result(c)
     use ns_global_data_module, only: scheme_id, second_order, method, bc_style, boundary_2d, &
       exclude_bound_vert, local_time_step, n_bc, bc_euler_id, bc_val, cfl, tmax, activate_diffusion, &
-      use_sutherland, mu_p, mu0, T0, Cv_p, bc_V_id, bc_val_V, bc_T_id, bc_val_T
+      use_sutherland, mu_p, mu0, T0, Cv_p, bc_V_id, bc_val_V, bc_T_id, bc_val_T, Prandtl
     type(subfv_ns_cfg) :: c
     integer :: i
     c%scheme = scheme_id
@@ -381,6 +381,7 @@ contains
     c%mu0 = mu0
     c%T0 = T0
     c%Cv_p = Cv_p
+    c%prandtl = Prandtl
   end function dropin_ns_cfg
 
   ! compute_euler_flux (ns_euler_module.F90:151-339); h_p and mat_h_p belong to the ZB

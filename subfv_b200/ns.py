@@ -34,7 +34,7 @@ class NsCfgC(C.Structure):
                 ("precision", C.c_int32), ("activate_diffusion", C.c_int32), ("use_sutherland", C.c_int32),
                 ("mu_p", C.c_double), ("mu0", C.c_double), ("T0", C.c_double), ("Cv_p", C.c_double),
                 ("bc_type_V", C.c_int32 * 16), ("bc_val_V", (C.c_double * 3) * 16), ("bc_type_T", C.c_int32 * 16),
-                ("bc_val_T", C.c_double * 16)]
+                ("bc_val_T", C.c_double * 16), ("prandtl", C.c_double)]
 
 # bc_type_V / bc_type_T per tag (ns_global_data_module.F90:49-52; 0 is the namelist's "")
 BC_DIFF_NEUMANN, BC_DIFF_DIRICHLET = 1, 2
@@ -69,6 +69,7 @@ class NsConfig:
     mu0: float = 1.716e-5
     T0: float = 273.15
     Cv_p: float = 720.19471
+    prandtl: float = 0.71  # the reference's parameter (ns_global_data_module.F90:10)
     bc_type_V: list = field(default_factory=list)  # per tag
     bc_val_V: list = field(default_factory=list)   # per tag (u, v, w)
     bc_type_T: list = field(default_factory=list)  # per tag
@@ -87,6 +88,7 @@ class NsConfig:
         c.cfl, c.tmax, c.precision = float(self.cfl), float(self.tmax), int(self.precision)
         c.activate_diffusion, c.use_sutherland = int(self.activate_diffusion), int(self.use_sutherland)
         c.mu_p, c.mu0, c.T0, c.Cv_p = float(self.mu_p), float(self.mu0), float(self.T0), float(self.Cv_p)
+        c.prandtl = float(self.prandtl)
         for i in range(16):
             c.bc_type_V[i] = int(self.bc_type_V[i]) if i < len(self.bc_type_V) else 0
             c.bc_type_T[i] = int(self.bc_type_T[i]) if i < len(self.bc_type_T) else 0
@@ -107,7 +109,7 @@ class NsConfig:
             pad = lambda a, shape: np.concatenate([np.asarray(a, np.float64).reshape((-1,) + shape[1:]),
                                                    np.zeros((shape[0] - len(a),) + shape[1:])])
             d.update(activate_diffusion=1, use_sutherland=int(self.use_sutherland),
-                     diff_dc=[self.mu_p, self.mu0, self.T0, self.Cv_p],
+                     diff_dc=[self.mu_p, self.mu0, self.T0, self.Cv_p, self.prandtl],
                      bc_type_V=pad(self.bc_type_V, (nb,)).astype(np.int32),
                      bc_val_V=pad(self.bc_val_V, (nb, 3)), bc_type_T=pad(self.bc_type_T, (nb,)).astype(np.int32),
                      bc_val_T=pad(self.bc_val_T, (nb,)))

@@ -76,3 +76,23 @@ def gather_lists(local: list) -> list:
     out = [None] * dist.get_world_size()
     dist.all_gather_object(out, list(local))
     return [x for part in out for x in part]
+
+
+def run_partitioned(sizes: list[int], solve):
+    """Independent problems over the ranks: partition_by_cells on their sizes, each rank
+    solves its share with solve(indices) -> (one result per index, units processed,
+    seconds), then every rank receives all results in problem order. Returns (results,
+    whole-job units per second, the slowest rank's seconds). With one process it is
+    solve(all problems)."""
+    dist = _dist()
+    world = dist.get_world_size() if dist else 1
+    rank = dist.get_rank() if dist else 0
+    mine = partition_by_cells(list(sizes), world)[rank]
+    results, units, seconds = solve(mine)
+    if len(results) != len(mine):
+        raise ValueError("solve must return one result per problem index")
+    rate, slowest = aggregate_throughput(float(units), float(seconds))
+    out = [None] * len(sizes)
+    for i, r in gather_lists(list(zip(mine, results))):
+        out[i] = r
+    return out, rate, slowest

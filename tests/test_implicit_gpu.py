@@ -114,3 +114,60 @@ def test_implicit_step_lusgs_matches_oracle(native, oracle_lib, cuda_ok):
     s2 = NsState(m, _cfg(), sol)
     _, stats_bj = s2.implicit_step(cfl_implicit=cfl, krylov=30, rel_tol=1e-8, precond=1)
     assert stats["restarts"] <= stats_bj["restarts"]
+
+
+def _diff_cfg():
+    from subfv_b200.ns import NsConfig
+    return NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5,
+                    activate_diffusion=True, mu_p=2e-3, Cv_p=2.5, prandtl=0.72)
+
+
+def test_be_jacobian_with_diffusion_bit_exact(native, oracle_lib, cuda_ok):
+    """With diffusion the assembled matrix is the frozen-speed Euler Jacobian plus the
+    reference's point-implicit diffusion blocks on the diagonal, on a periodic box."""
+    from oracle.oracle import OracleMesh
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsState, init_fourier_flow
+    raw = _meshes()["box_periodic"]
+    m, o = Mesh.from_raw(raw), OracleMesh(raw)
+    sol = init_fourier_flow(m, seed=3)
+    s = NsState(m, _diff_cfg(), sol)
+    row, col, v = s.be_jacobian(0.013)
+    ro, co, vo = o.be_jacobian(_diff_cfg().oracle_dict(), sol, 0.013)
+    _, _, _, diag = o.ns_rhs_diag(_diff_cfg().oracle_dict(), sol)
+    for c in range(o.n_elems):
+        j = ro[c] - 1 + int(np.searchsorted(co[ro[c] - 1:ro[c + 1] - 1], c + 1))
+        vo[j] = vo[j] + diag[c]
+    np.testing.assert_array_equal(row, ro)
+    np.testing.assert_array_equal(col, co)
+    np.testing.assert_array_equal(v, vo)
+
+
+def test_implicit_step_with_diffusion_matches_oracle(native, oracle_lib, cuda_ok):
+    """One backward-Euler step with viscous and heat terms on a periodic box equals the
+    oracle's matrix and right-hand side (rhs - mat_diag U) solved by bcsr_gmres_diag, to
+    GMRES round-off."""
+    from oracle.oracle import OracleBcsr, OracleMesh
+    from subfv_b200.bcsr import BcsrMatrix
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsState, init_fourier_flow
+    raw = _meshes()["box_periodic"]
+    m, o = Mesh.from_raw(raw), OracleMesh(raw)
+    cfg = _diff_cfg()
+    sol = init_fourier_flow(m, seed=4)
+    cfl = 10.0
+    s = NsState(m, cfg, sol)
+    st, stats = s.implicit_step(cfl_implicit=cfl, krylov=30, rel_tol=1e-8)
+    assert st == 0 and stats["conv"] == 1
+    _, rhs_o, sl_o, diag = o.ns_rhs_diag(cfg.oracle_dict(), sol)
+    dt = cfl * min(1e10, float(np.min(o.geom("elem_volume") / sl_o)))
+    assert stats["dt"] == dt
+    row, col, v = o.be_jacobian(cfg.oracle_dict(), sol, dt)
+    for c in range(o.n_elems):
+        j = row[c] - 1 + int(np.searchsorted(col[row[c] - 1:row[c + 1] - 1], c + 1))
+        v[j] = v[j] + diag[c]
+    b = (rhs_o - np.einsum('nij,nj->ni', diag.transpose(0, 2, 1), sol)).reshape(-1)
+    x, conv, it, _, _ = OracleBcsr(BcsrMatrix(o.n_elems, 5, row, col, v)).gmres(b, 1e-8 * np.linalg.norm(b), 30,
+                                                                                precond=True)
+    assert conv
+    assert np.abs(s.sol() - (sol + x.reshape(-1, 5))).max() <= 1e-8 * np.abs(x).max()

@@ -116,3 +116,45 @@ def test_linear_temperature_is_steady_on_an_orthogonal_slab(oracle_lib):
     kw["bc_val_T"] = np.array([0.4, 0.45, 0, 0])
     assert o.ns_run(_cfg(**kw), s2, 4)[0] == 0
     assert np.abs(s2 - sol).max() > 1e-6
+
+
+def _periodic_pair(n):
+    from oracle.oracle import OracleMesh
+    from subfv_b200 import meshgen
+    return OracleMesh(meshgen.hex_box(n, jitter=0.0, seed=0, periodic=True))
+
+
+def _prim_to_cons(w):
+    return np.ascontiguousarray(np.column_stack([w[:, 0], w[:, 1:4] * w[:, :1],
+                                                 w[:, 4] / 0.4 + 0.5 * w[:, 0] * (w[:, 1:4] ** 2).sum(1)]))
+
+
+def _viscous_term(o, sol, mu):
+    """The full diffusion term of each cell, rhs_visc - mat_diag U (the reference's
+    point-implicit split: add_timedisc_and_solve solves (mat_diag + s I) U_new = rhs + s U)."""
+    from subfv_b200.ns import NsConfig
+    base = dict(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5)
+    _, r_d, _, diag = o.ns_rhs_diag(NsConfig(**base, activate_diffusion=True, mu_p=mu).oracle_dict(), sol)
+    _, r_e, _, _, _ = o.ns_rhs(NsConfig(**base).oracle_dict(), sol)
+    return (r_d - r_e) - np.einsum('nij,nj->ni', diag.transpose(0, 2, 1), sol)
+
+
+def test_periodic_box_diffusion_is_consistent(oracle_lib):
+    """Diffusion on a periodic box (each periodic node's system over the union of its
+    images' subfaces and subcells): a uniform flow has no viscous or heat term, and the
+    x-momentum term of a shear wave u = A sin(2 pi y) converges to mu u'' at second order."""
+    mu, A = 1e-2, 0.01
+    errs = []
+    for n in (8, 16):
+        o = _periodic_pair(n)
+        cc, vol = o.geom("elem_coord"), o.geom("elem_volume")
+        ones = np.ones(len(cc))
+        uni = _prim_to_cons(np.column_stack([ones, 0.3 * ones, 0.1 * ones, -0.2 * ones, ones]))
+        assert np.abs(_viscous_term(o, uni, mu)).max() <= 1e-13 * mu * 0.3
+        ux = A * np.sin(2 * np.pi * cc[:, 1])
+        shear = _prim_to_cons(np.column_stack([ones, ux, 0 * ux, 0 * ux, ones]))
+        visc = _viscous_term(o, shear, mu)
+        exact = -mu * (2 * np.pi) ** 2 * ux * vol
+        errs.append(np.abs(visc[:, 1] - exact).max() / np.abs(exact).max())
+    print("shear-wave viscous term, max relative error at 8^3 and 16^3:", errs)
+    assert errs[1] < 0.02 and errs[0] / errs[1] > 3.5

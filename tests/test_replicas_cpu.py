@@ -1,6 +1,8 @@
 """Host logic of the multi-GPU runs (one process per GPU, independent work per rank),
 exercised with two gloo ranks on the CPU: max-over-ranks timing, whole-job throughput,
-the cell-count partition of independent problems, and gathering per-rank results."""
+the cell-count partition of independent problems, gathering per-rank results, and the
+partition -> per-rank solve -> gather flow of the batched shock tubes on tiny problems
+(solved on each rank by the CPU restatement, which stands in for the GPU batch here)."""
 import os
 
 import pytest
@@ -54,3 +56,66 @@ def test_partition_balances_and_is_deterministic():
     assert sorted(i for p in parts for i in p) == list(range(10))
     assert all(p == sorted(p) for p in parts)
     assert partition_by_cells(cells, 1) == [list(range(10))]
+
+
+def _tubes():
+    from subfv_b200 import shocktube
+    return shocktube.sample(6, seed=3, n_min=8, n_max=24)
+
+
+def _solve_tubes(indices):
+    """Each problem to its end time on this rank (first-order multi_point, CFL 0.4)."""
+    import time
+    import numpy as np
+    from oracle.oracle import OracleMesh
+    from subfv_b200 import shocktube
+    from subfv_b200.ns import NsConfig
+    tubes = _tubes()
+    out, units, t0 = [], 0, time.perf_counter()
+    for i in indices:
+        raw = shocktube.raw_mesh(tubes[i])
+        o = OracleMesh(raw)
+
+        class _M:  # what initial_state reads of a mesh
+            n_elems = o.n_elems
+
+            def geometry(self, name, o=o):
+                return o.geom(name)
+        sol = np.ascontiguousarray(shocktube.initial_state(_M(), tubes[i]))
+        cfg = NsConfig(scheme=1, second_order=False, method=4, bc_style=2, boundary_2d=True, cfl=0.4,
+                       tmax=tubes[i].t_end)
+        st, it, t, _, _, _ = o.ns_run(cfg.oracle_dict(), sol, 10 ** 6)
+        out.append((st, it, sol.tobytes()))
+        units += o.n_elems * it
+    return out, units, time.perf_counter() - t0
+
+
+def _worker_partitioned(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from subfv_b200 import replicas
+        sizes = [t.n_cells for t in _tubes()]
+        res, rate, sec = replicas.run_partitioned(sizes, _solve_tubes)
+        q.put((rank, res, rate, sec))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_partitioned_shock_tubes_two_gloo_ranks():
+    world, port = 2, 30617 + os.getpid() % 1000
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    ps = [ctx.Process(target=_worker_partitioned, args=(r, world, port, q)) for r in range(world)]
+    for p in ps:
+        p.start()
+    res = sorted((q.get(timeout=120) for _ in ps), key=lambda x: x[0])
+    for p in ps:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    alone, _, _ = _solve_tubes(list(range(len(_tubes()))))
+    for rank, got, rate, sec in res:
+        assert got == alone  # every problem, in problem order, as solved on one rank
+        assert rate > 0 and sec > 0
+    assert res[0][2] == res[1][2]  # the same whole-job figure on every rank
