@@ -450,7 +450,7 @@ def field_errors(a, b):
             [float(d[:, i].max() / max(lis[i], 1e-300)) for i in range(5)])
 
 
-def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=16, tune=True):
+def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=16, tune=True, rank=0, world=1):
     """Batched shock tubes: `problems` independent Riemann problems on N x 4 quad strips,
     N uniform in [200, nmax] (seed 1), states as in subfv_b200.shocktube, first order
     multi_point nodal solver, CFL 0.4, walls all round. Timed: K steps of the whole batch
@@ -459,11 +459,18 @@ def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=
     shapes; the baseline is the plain FP64 path run one problem at a time (subfv_ns_state,
     graph-replayed) over a sample of the problems. Accuracy: `acc_problems` problems of
     N <= 2000 run to their end time at each level, against plain FP64 (per-field L1 and
-    Linf, mass and energy drift)."""
+    Linf, mass and energy drift).
+
+    With several ranks (one per GPU) the problems are split by cell count
+    (replicas.partition_by_cells, the same on every rank), each rank runs its share, and
+    the figures are whole-job: all ranks' cell-updates over the slowest rank's time; no
+    device collective."""
     import torch
-    from subfv_b200 import autotune, shocktube
+    from subfv_b200 import autotune, replicas, shocktube
     from subfv_b200.ns import NsBatch, NsConfig, NsState
-    rng_tubes = shocktube.sample(problems, seed=SEED, n_max=nmax)
+    all_tubes = shocktube.sample(problems, seed=SEED, n_max=nmax)
+    mine = replicas.partition_by_cells([t.n_cells for t in all_tubes], world)[rank]
+    rng_tubes = [all_tubes[i] for i in mine]
     t0 = time.perf_counter()
     meshes = _build_meshes([(lambda t=t: shocktube.raw_mesh(t)) for t in rng_tubes], local)
     setup_s = time.perf_counter() - t0
@@ -473,10 +480,12 @@ def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=
                       nse=sum(m.n_sub_elems for m in meshes))
     base = dict(scheme=1, second_order=False, method=4, bc_style=2, boundary_2d=True, cfl=0.4)
     budget = int(150e9)
-    res = {"workload": f"shocktubes_{problems}_strips_Nx4_N200-{nmax}", "problems": problems, "cells": cells,
-           "steps": K, "mesh_setup_s": setup_s, "mesh_bytes": sum(m.device_bytes for m in meshes)}
+    res = {"workload": f"shocktubes_{problems}_strips_Nx4_N200-{nmax}", "problems": problems,
+           "cells": int(sum(replicas.gather_lists([cells]))), "steps": K, "ranks": world,
+           "mesh_setup_s": replicas.max_over_ranks(setup_s),
+           "mesh_bytes_per_rank_max": int(replicas.max_over_ranks(sum(m.device_bytes for m in meshes)))}
     for name, prec in (("level1", 1), ("level2", 2), ("fp64", 0)):
-        b = NsBatch(NsConfig(**base, precision=prec), capacity=problems, budget_bytes=budget)
+        b = NsBatch(NsConfig(**base, precision=prec), capacity=max(1, len(meshes)), budget_bytes=budget)
         slots = [b.add(m, s, t.t_end) for m, s, t in zip(meshes, sols, rng_tubes)]
         assert None not in slots
         log = []
@@ -489,7 +498,8 @@ def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=
         sampler.start()
         ms_tuned = b.time_steps(K)
         clocks = sampler.stop()
-        r = {"value": cells * K / (ms_tuned / 1e3), "ms_per_step": ms_tuned / K,
+        v_tuned, s_tuned = replicas.aggregate_throughput(cells * K, ms_tuned / 1e3)
+        r = {"value": v_tuned, "ms_per_step": 1e3 * s_tuned / K,
              "roofline": _ns_roofline(tube_sizes, 1, ms_tuned / K),
              "tuned_shape": {"node_lanes": best[0], "block_v": best[1], "grid_v": best[2], "grid_c": best[3]},
              "autotune_trials": len(log), "clocks": clocks, "state_bytes": sum(b.state_bytes(m) for m in meshes)}
@@ -497,14 +507,16 @@ def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=
             autotune.apply(b, autotune.DEFAULT)
             b.time_steps(1)
             ms_fixed = b.time_steps(K)
-            r.update(fixed_value=cells * K / (ms_fixed / 1e3), fixed_ms_per_step=ms_fixed / K)
+            v_fixed, s_fixed = replicas.aggregate_throughput(cells * K, ms_fixed / 1e3)
+            r.update(fixed_value=v_fixed, fixed_ms_per_step=1e3 * s_fixed / K)
         b.sync()
-        r["status"] = max(b.info(k)[3] for k in slots)
+        r["status"] = int(replicas.max_over_ranks(max([b.info(k)[3] for k in slots], default=0)))
         res[name] = r
         b.close()
         torch.cuda.synchronize()
     # plain FP64, one problem at a time, over a sample of the problems
-    idx = np.random.default_rng(SEED + 1).choice(problems, size=min(solo_sample, problems), replace=False)
+    idx = np.random.default_rng(SEED + 1 + rank).choice(len(meshes), size=min(solo_sample, len(meshes)),
+                                                        replace=False)
     solo_ms, solo_cells = 0.0, 0
     for i in idx:
         m, s, t = meshes[i], sols[i], rng_tubes[i]
@@ -515,16 +527,20 @@ def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=
         solo_ms += _time_device(stream, lambda: st_.advance_async(K))
         solo_cells += m.n_elems * K
         st_.close()
-    solo = solo_cells / (solo_ms / 1e3)
-    res["solo_fp64"] = {"value": solo, "problems": len(idx),
+    solo, _ = replicas.aggregate_throughput(solo_cells, solo_ms / 1e3)
+    res["solo_fp64"] = {"value": solo, "problems": int(sum(replicas.gather_lists([len(idx)]))),
                         "note": "plain FP64 path, one problem at a time, K steps each"}
     for name in ("fp64", "level1", "level2"):
         res[name]["x_solo_fp64"] = res[name]["value"] / solo
     # accuracy: small problems run to their end time at each level
-    acc_idx = [i for i in range(problems) if rng_tubes[i].n <= 2000][:acc_problems]
-    if acc_idx:
+    acc_idx = [i for i in range(len(meshes)) if rng_tubes[i].n <= 2000][:max(1, acc_problems // world)]
+    # every rank takes part in the gathers below, with or without small problems of its own
+    if True:
         outs = {}
         for name, prec in (("fp64", 0), ("level1", 1), ("level2", 2)):
+            if not acc_idx:
+                outs[name] = []
+                continue
             b = NsBatch(NsConfig(**base, precision=prec), capacity=len(acc_idx), budget_bytes=budget)
             sl = [b.add(meshes[i], sols[i], rng_tubes[i].t_end) for i in acc_idx]
             while True:
@@ -541,62 +557,82 @@ def shocktube_block(problems, nmax, K, warmup, solo_sample, local, acc_problems=
                 vol = meshes[i].geometry("elem_volume")
                 t0_, t1_ = (sols[i] * vol[:, None]).sum(0), (u * vol[:, None]).sum(0)
                 out.append([float(abs(t1_[k] - t0_[k]) / abs(t0_[k])) for k in (0, 4)])
-            return np.array(out).max(0).tolist()
+            return out
 
-        acc = {"problems": len(acc_idx), "fields": FIELDS, "fp64_mass_energy_drift_max": drift("fp64"),
+        def gmax(rows):  # the largest of every rank's rows, per column
+            rows = replicas.gather_lists([list(map(float, r)) for r in rows])
+            return np.array(rows).max(0).tolist() if rows else None
+
+        acc = {"problems": int(sum(replicas.gather_lists([len(acc_idx)]))), "fields": FIELDS,
+               "fp64_mass_energy_drift_max": gmax(drift("fp64")),
                "note": "each problem run to its end time; errors against the plain FP64 run (bit-identical to "
                        "the oracle); momentum components scaled by the momentum vector"}
         for name in ("level1", "level2"):
-            e = np.array([field_errors(a, c) for a, c in zip(outs["fp64"], outs[name])])  # (p, 2, 5)
-            acc[name] = {"l1_rel_max": e[:, 0].max(0).tolist(), "linf_rel_max": e[:, 1].max(0).tolist(),
-                         "mass_energy_drift_max": drift(name),
-                         "meets_l1_1e-6": bool(e[:, 0].max() <= 1e-6)}
+            e = [field_errors(a, c) for a, c in zip(outs["fp64"], outs[name])]
+            l1 = gmax([x[0] for x in e])
+            acc[name] = {"l1_rel_max": l1, "linf_rel_max": gmax([x[1] for x in e]),
+                         "mass_energy_drift_max": gmax(drift(name)),
+                         "meets_l1_1e-6": bool(l1 is not None and max(l1) <= 1e-6)}
         res["accuracy"] = acc
     return res
 
 
 def run_shocktubes(args, rank, world, local):
-    """The batched shock-tube workload at full size (`--problems`, `--nmax`)."""
-    res = shocktube_block(args.problems, args.nmax, args.steps, args.warmup, args.solo_sample, local)
-    res.update(metric="cell-updates/s", value=res["level1"]["value"], unit="cell-updates/s")
-    print(json.dumps(res), flush=True)
+    """The batched shock-tube workload at full size (`--problems`, `--nmax`), the
+    problems split over the ranks."""
+    res = shocktube_block(args.problems, args.nmax, args.steps, args.warmup, args.solo_sample, local,
+                          rank=rank, world=world)
+    res.update(metric="cell-updates/s", value=res["level1"]["value"], unit="cell-updates/s", n_gpus=world,
+               scaling="strong")
+    if rank == 0:
+        print(json.dumps(res), flush=True)
 
 
-def serve_block(n_requests, rate, max_cells, time_scale, solo_sample, local):
+def serve_block(n_requests, rate, max_cells, time_scale, solo_sample, local, rank=0, world=1):
     """Serving: solve requests (Gresho vortex or 2-D Sedov, triangles or quadrilaterals,
     cells log-uniform in [4096, max_cells], end time uniform in [0.1, 1] x nominal x
     time_scale) on a seeded Poisson stream of `rate` requests per second, served by
     subfv_b200.serve.Server under a 150 GB budget, in plain FP64 and at precision level
     1. Latency = arrival to result on the host. Baseline: a sample of the same requests
-    solved one at a time on the plain FP64 solo path."""
+    solved one at a time on the plain FP64 solo path.
+
+    With several ranks (one per GPU) the stream is split by cell count
+    (replicas.partition_by_cells), each rank serves its requests at their arrival times,
+    and the figures are whole-job: latencies of all requests, all ranks' cell-updates over
+    the longest makespan; no device collective."""
     import torch
-    from subfv_b200 import serve
-    reqs = serve.make_requests(n_requests, rate=rate, seed=SEED, cells_max=max_cells, time_scale=time_scale)
+    from subfv_b200 import replicas, serve
+    all_reqs = serve.make_requests(n_requests, rate=rate, seed=SEED, cells_max=max_cells, time_scale=time_scale)
+    mine = replicas.partition_by_cells([r.n_cells for r in all_reqs], world)[rank]
+    reqs = [all_reqs[i] for i in mine]
     res = {"workload": f"serve_{n_requests}_requests", "requests": n_requests, "rate_per_s": rate,
-           "cells_max": max_cells, "time_scale": time_scale, "budget_bytes": int(150e9)}
+           "cells_max": max_cells, "time_scale": time_scale, "budget_bytes_per_gpu": int(150e9), "ranks": world}
     for name, prec in (("fp64", 0), ("level1", 1)):
         srv = serve.Server(budget_bytes=int(150e9), capacity=max(64, n_requests), precision=prec, chunk=8,
                            build_threads=max(1, min(16, (os.cpu_count() or 2) - 2)), keep_solutions=False)
         sampler = ClockSampler(local)
         sampler.start()
-        results, makespan = srv.run(reqs)
+        results, makespan = srv.run(reqs) if reqs else ([], 1e-9)
         clocks = sampler.stop()
         srv.close()
         torch.cuda.synchronize()
         cu = sum(r.n_cells * r.steps for r in results)
-        res[name] = {"value": cu / makespan, "makespan_s": makespan, "cell_updates": cu,
-                     "completed": len(results), "failed": sum(1 for r in results if r.status),
-                     "latency": serve.latency_stats(results), "clocks": clocks,
-                     "steps_mean": float(np.mean([r.steps for r in results])) if results else 0.0}
+        value, slowest = replicas.aggregate_throughput(cu, makespan)
+        everything = replicas.gather_lists(results)
+        res[name] = {"value": value, "makespan_s": slowest, "cell_updates": int(sum(r.n_cells * r.steps for r in everything)),
+                     "completed": len(everything), "failed": sum(1 for r in everything if r.status),
+                     "latency": serve.latency_stats(everything), "clocks": clocks,
+                     "steps_mean": float(np.mean([r.steps for r in everything])) if everything else 0.0}
     # one request at a time on the plain FP64 path, over a sample of the stream
-    idx = np.random.default_rng(SEED + 2).choice(len(reqs), size=min(solo_sample, len(reqs)), replace=False)
+    idx = np.random.default_rng(SEED + 2 + rank).choice(len(reqs), size=min(solo_sample, len(reqs)), replace=False)
     t0 = time.perf_counter()
     cu = 0
     for i in idx:
         steps, t, st, _ = serve.solve_alone(reqs[i], precision=0)
         cu += reqs[i].n_cells * steps
-    el = time.perf_counter() - t0
-    res["one_by_one_fp64"] = {"value": cu / el, "requests": len(idx), "seconds": el,
+    el = max(time.perf_counter() - t0, 1e-9)
+    one, el = replicas.aggregate_throughput(cu, el)
+    res["one_by_one_fp64"] = {"value": one, "requests": int(sum(replicas.gather_lists([len(idx)]))), "seconds": el,
                               "note": "each request built and solved alone on the solo path, sequentially"}
     for name in ("fp64", "level1"):
         res[name]["x_one_by_one_fp64"] = res[name]["value"] / res["one_by_one_fp64"]["value"]
@@ -604,9 +640,11 @@ def serve_block(n_requests, rate, max_cells, time_scale, solo_sample, local):
 
 
 def run_serve(args, rank, world, local):
-    res = serve_block(args.requests, args.rate, args.max_cells, args.time_scale, args.solo_sample, local)
-    res.update(metric="cell-updates/s", value=res["level1"]["value"], unit="cell-updates/s")
-    print(json.dumps(res), flush=True)
+    res = serve_block(args.requests, args.rate, args.max_cells, args.time_scale, args.solo_sample, local, rank, world)
+    res.update(metric="cell-updates/s", value=res["level1"]["value"], unit="cell-updates/s", n_gpus=world,
+               scaling="weak")
+    if rank == 0:
+        print(json.dumps(res), flush=True)
 
 
 def _libmod():
@@ -619,9 +657,18 @@ def main():
     rank, world, local = _dist()
     if args.workload != "lagrange":
         import torch
+        import torch.distributed as dist
+        from datetime import timedelta
         torch.cuda.set_device(local)
-        {"gresho": run_gresho, "implicit": run_implicit, "shocktubes": run_shocktubes,
-         "serve": run_serve}[args.workload](args, rank, world, local)
+        sharded = world > 1 and args.workload in ("shocktubes", "serve")
+        if sharded:  # independent problems split over the ranks; only host reductions
+            dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        if sharded or rank == 0:  # the single-mesh workloads run once, on rank 0
+            {"gresho": run_gresho, "implicit": run_implicit, "shocktubes": run_shocktubes,
+             "serve": run_serve}[args.workload](args, rank, world, local)
+        if sharded:
+            dist.barrier()
+            dist.destroy_process_group()
         return
     import torch
     import torch.distributed as dist
