@@ -59,9 +59,164 @@ __device__ inline int n_sub_faces(const int4 q) { return (q.x >= 0) + (q.y >= 0)
 __device__ inline int sf_of(const int4 q, int p) { return p == 0 ? q.x : p == 1 ? q.y : p == 2 ? q.z : q.w; }
 
 // Warp-parallel dgetrf + dgetri of the n x n column-major matrix a (inv_lapack,
-// linear_solver_module.F90:629-641).
+// linear_solver_module.F90:629-641), n <= 96. Each row-parallel phase gives lane r the
+// rows r, r + 32, r + 64 (only the groups that still hold live rows), keeps their
+// running values in registers and issues each group of four loads before using them,
+// so no phase divides indices or waits on a shuffle chain; every element still
+// receives the same operations in the same order as in the serial algorithm.
+
+// dgetf2's rank-1 update of the trailing block after column j (dger with alpha = -1:
+// a(i,k) - l(i) u(k)), rows j + 1 + lane + 32 g
+template <int G>
+__device__ __forceinline__ void lu_update(double* a, int n, int j, int lane) {
+  double l[G];
+  double* row[G];
+  bool ok[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    const int i = j + 1 + lane + 32 * g;
+    ok[g] = i < n;
+    const int ic = ok[g] ? i : j + 1;  // a dead lane reads a live row and stores nothing
+    l[g] = a[ic + n * j];
+    row[g] = a + ic;
+  }
+  const double* pr = a + j;  // the pivot row, a broadcast
+  int k = j + 1;
+  for (; k + 3 < n; k += 4) {
+    double u[4];
+#pragma unroll
+    for (int t = 0; t < 4; ++t) u[t] = pr[n * (k + t)];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      double x[4];
+#pragma unroll
+      for (int t = 0; t < 4; ++t) x[t] = row[g][n * (k + t)];
+      if (ok[g]) {
+#pragma unroll
+        for (int t = 0; t < 4; ++t) row[g][n * (k + t)] = x[t] - l[g] * u[t];
+      }
+    }
+  }
+  for (; k < n; ++k) {
+    const double u = pr[n * k];
+#pragma unroll
+    for (int g = 0; g < G; ++g)
+      if (ok[g]) row[g][n * k] = row[g][n * k] - l[g] * u;
+  }
+}
+
+// Column j > 0 of dtrti2 ('Upper', 'Non-unit'): x := T x with T the already inverted
+// leading block (dtrmv, upper, no transpose), then x := -x / U(j,j) (dscal). In dtrmv,
+// step jj reads x(jj) before any step has changed it (later steps only add to rows
+// above them), and when it is non-zero scales x(jj) by T(jj,jj) and adds x(jj) T(i,jj)
+// to each row i < jj. So a row's result is its own value scaled by the diagonal, then
+// the original x(jj) T(i,jj) added in increasing jj, each skipped when x(jj) is zero:
+// every lane reads the original column and accumulates its rows i < j (G groups).
+template <int G>
+__device__ __forceinline__ void trti_col(double* a, int n, int j, int lane) {
+  const double ajj = -a[j + n * j];
+  double* x = a + n * j;
+  double acc[G];
+  int ii[G];
+#pragma unroll
+  for (int g = 0; g < G; ++g) {
+    const int i = lane + 32 * g;
+    ii[g] = i < j ? i : j;  // a dead lane never adds (ii >= every jj) and is never stored
+    const int ic = i < j ? i : 0;
+    const double x0 = x[ic], d = a[ic + n * ic];
+    acc[g] = x0 != 0.0 ? x0 * d : x0;  // dtrmv's step jj = i
+  }
+  int jj = 1;
+  for (; jj + 3 < j; jj += 4) {
+    double t[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) t[u] = x[jj + u];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int ic = ii[g] < j ? ii[g] : 0;
+      double av[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) av[u] = a[ic + n * (jj + u)];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (t[u] != 0.0 && ii[g] < jj + u) acc[g] = acc[g] + t[u] * av[u];
+    }
+  }
+  for (; jj < j; ++jj) {
+    const double t = x[jj];
+#pragma unroll
+    for (int g = 0; g < G; ++g) {
+      const int ic = ii[g] < j ? ii[g] : 0;
+      const double av = a[ic + n * jj];
+      if (t != 0.0 && ii[g] < jj) acc[g] = acc[g] + t * av;
+    }
+  }
+  __syncwarp();  // every lane has read the column before it is overwritten
+#pragma unroll
+  for (int g = 0; g < G; ++g)
+    if (ii[g] < j) x[ii[g]] = ajj * acc[g];
+  __syncwarp();
+}
+
+// dgetri's unblocked sweep, inv(A) L = inv(U) column by column from the last: column j
+// becomes (its upper part, zero below the diagonal) - sum over jj > j, in increasing jj,
+// of L(jj,j) times column jj; then the column interchanges of ipiv from the last. Rows
+// are independent: lane r keeps rows r + 32 g, and each column's L entries are copied
+// to work (2 n doubles, alternate halves per column) before any row overwrites them.
+template <int NQ>
+__device__ __forceinline__ void getri_sweep(double* a, int n, const int* ipiv, double* work, int lane) {
+  int ic[NQ];
+#pragma unroll
+  for (int g = 0; g < NQ; ++g) ic[g] = lane + 32 * g < n ? lane + 32 * g : 0;
+  for (int j = n - 1; j >= 0; --j) {
+    double* w = work + (j & 1) * n;
+    for (int i = j + 1 + lane; i < n; i += 32) w[i] = a[i + n * j];
+    __syncwarp();
+    double acc[NQ];
+#pragma unroll
+    for (int g = 0; g < NQ; ++g) acc[g] = lane + 32 * g <= j ? a[ic[g] + n * j] : 0.0;
+    int jj = j + 1;
+    for (; jj + 3 < n; jj += 4) {
+      double wv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) wv[u] = -w[jj + u];
+#pragma unroll
+      for (int g = 0; g < NQ; ++g) {
+        double av[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) av[u] = a[ic[g] + n * (jj + u)];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[g] = acc[g] + wv[u] * av[u];
+      }
+    }
+    for (; jj < n; ++jj) {
+      const double wv = -w[jj];
+#pragma unroll
+      for (int g = 0; g < NQ; ++g) acc[g] = acc[g] + wv * a[ic[g] + n * jj];
+    }
+#pragma unroll
+    for (int g = 0; g < NQ; ++g)
+      if (lane + 32 * g < n) a[lane + 32 * g + n * j] = acc[g];
+  }
+#pragma unroll
+  for (int g = 0; g < NQ; ++g) {
+    const int i = lane + 32 * g;
+    if (i < n)
+      for (int j = n - 2; j >= 0; --j) {
+        const int p = ipiv[j];
+        if (p != j) {
+          const double t = a[i + n * j];
+          a[i + n * j] = a[i + n * p];
+          a[i + n * p] = t;
+        }
+      }
+  }
+  __syncwarp();
+}
+
+// work: 2 n doubles
 __device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane) {
-  for (int j = 0; j < n; ++j) {
+  for (int j = 0; j < n; ++j) {  // dgetf2
     double big = -1.0;
     int bi = n;
     for (int i = j + lane; i < n; i += 32) {
@@ -84,13 +239,14 @@ __device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane
     const bool nz = a[p + n * j] != 0.0;
     __syncwarp();
     if (nz) {
-      if (p != j)
+      if (p != j) {
         for (int k = lane; k < n; k += 32) {
           const double t = a[j + n * k];
           a[j + n * k] = a[p + n * k];
           a[p + n * k] = t;
         }
-      __syncwarp();
+        __syncwarp();
+      }
       const double piv = a[j + n * j];
       if (fabs(piv) >= 2.2250738585072014e-308) {
         const double r = 1.0 / piv;
@@ -101,83 +257,82 @@ __device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane
     }
     __syncwarp();
     const int w = n - j - 1;
-    for (int e = lane; e < w * w; e += 32) {
-      const int i = j + 1 + e % w, k = j + 1 + e / w;
-      a[i + n * k] = a[i + n * k] - a[i + n * j] * a[j + n * k];
-    }
+    if (w > 64) lu_update<3>(a, n, j, lane);
+    else if (w > 32) lu_update<2>(a, n, j, lane);
+    else if (w > 0) lu_update<1>(a, n, j, lane);
     __syncwarp();
   }
-  // dtrti2 ('Upper', 'Non-unit'). Column j's dtrmv keeps x(0:j-1) in registers, row i in
-  // lane i % 32 (n <= 96 here: three rows a lane). At step jj, x(jj) has not been touched
-  // yet (only later steps add to it), so its owner broadcasts the column's own entry; the
-  // owner then scales it by the diagonal, as dtrmv does.
-  for (int j = 0; j < n; ++j) {
+  for (int j = 0; j < n; ++j) {  // dtrti2
     if (lane == 0) a[j + n * j] = 1.0 / a[j + n * j];
     __syncwarp();
-    const double ajj = -a[j + n * j];
-    double* x = a + n * j;
-    double xr[3];
-    for (int r = 0; r < 3; ++r) {
-      const int i = lane + 32 * r;
-      xr[r] = i < j ? x[i] : 0.0;
-    }
-    for (int jj = 0; jj < j; ++jj) {
-      const int owner = jj & 31, slot = jj >> 5;
-      const double mine = slot == 0 ? xr[0] : slot == 1 ? xr[1] : xr[2];
-      const double temp = __shfl_sync(0xffffffffu, mine, owner);
-      if (temp != 0.0) {
-        for (int r = 0; r < 3; ++r) {
-          const int i = lane + 32 * r;
-          if (i < jj) xr[r] = xr[r] + temp * a[i + n * jj];
-        }
-        if (lane == owner) {
-          if (slot == 0) xr[0] = xr[0] * a[jj + n * jj];
-          else if (slot == 1) xr[1] = xr[1] * a[jj + n * jj];
-          else xr[2] = xr[2] * a[jj + n * jj];
-        }
-      }
-    }
-    for (int r = 0; r < 3; ++r) {
-      const int i = lane + 32 * r;
-      if (i < j) x[i] = ajj * xr[r];
-    }
-    __syncwarp();
+    if (j > 64) trti_col<3>(a, n, j, lane);
+    else if (j > 32) trti_col<2>(a, n, j, lane);
+    else if (j > 0) trti_col<1>(a, n, j, lane);
   }
-  // inv(A) L = inv(U), column by column from the last (the unblocked dgetri sweep)
-  for (int j = n - 1; j >= 0; --j) {
-    for (int i = j + 1 + lane; i < n; i += 32) {
-      work[i] = a[i + n * j];
-      a[i + n * j] = 0.0;
-    }
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-      double acc = a[i + n * j];
-      for (int jj = j + 1; jj < n; ++jj) acc = acc + (-work[jj]) * a[i + n * jj];
-      a[i + n * j] = acc;
-    }
-    __syncwarp();
-  }
-  for (int i = lane; i < n; i += 32)
-    for (int j = n - 2; j >= 0; --j) {
-      const int p = ipiv[j];
-      if (p != j) {
-        const double t = a[i + n * j];
-        a[i + n * j] = a[i + n * p];
-        a[i + n * p] = t;
-      }
-    }
-  __syncwarp();
+  if (n > 64) getri_sweep<3>(a, n, ipiv, work, lane);
+  else if (n > 32) getri_sweep<2>(a, n, ipiv, work, lane);
+  else getri_sweep<1>(a, n, ipiv, work, lane);
 }
 
-// C(m x p) = A(m x k) B(k x p), netlib dgemm order
-__device__ inline void warp_gemm(int m, int p, int k, const double* A, const double* B, double* C, int lane) {
-  for (int e = lane; e < m * p; e += 32) {
-    const int i = e % m, j = e / m;
-    double s = 0.0;
-    for (int l = 0; l < k; ++l) s = s + B[l + k * j] * A[i + m * l];
-    C[i + m * j] = s;
+// C(m x p) = A(m x k) B(k x p), netlib dgemm order: C(i,j) = sum over l, in order, of
+// B(l,j) A(i,l). C is written over B's storage with leading dimension m <= k: column j of
+// C needs only column j of B, so each block of columns is summed into registers and
+// stored once the whole warp has read that block of B (the stored block ends at
+// m (j0 + JB) <= k (j0 + JB), below the columns still to be read). A lane owns rows
+// lane + 32 g, so one load of A(i,l) serves JB sums and B(l,j) is a broadcast.
+template <int NQ, int JB>
+__device__ __forceinline__ void gemm_block(int m, int k, const double* A, double* BC, int j0, int lane) {
+  double s[NQ][JB];
+#pragma unroll
+  for (int g = 0; g < NQ; ++g)
+#pragma unroll
+    for (int jj = 0; jj < JB; ++jj) s[g][jj] = 0.0;
+  const double* b = BC + (size_t)k * j0;
+  int ic[NQ];
+#pragma unroll
+  for (int g = 0; g < NQ; ++g) ic[g] = lane + 32 * g < m ? lane + 32 * g : 0;
+  int l = 0;
+  for (; l + 1 < k; l += 2) {
+    double bv[2][JB];
+#pragma unroll
+    for (int u = 0; u < 2; ++u)
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) bv[u][jj] = b[l + u + k * jj];
+#pragma unroll
+    for (int g = 0; g < NQ; ++g) {
+      const double a0 = A[ic[g] + m * l], a1 = A[ic[g] + m * (l + 1)];
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) s[g][jj] = s[g][jj] + bv[0][jj] * a0;
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) s[g][jj] = s[g][jj] + bv[1][jj] * a1;
+    }
+  }
+  if (l < k) {
+#pragma unroll
+    for (int g = 0; g < NQ; ++g) {
+      const double a0 = A[ic[g] + m * l];
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) s[g][jj] = s[g][jj] + b[l + k * jj] * a0;
+    }
   }
   __syncwarp();
+#pragma unroll
+  for (int g = 0; g < NQ; ++g)
+    if (lane + 32 * g < m)
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) BC[lane + 32 * g + m * (j0 + jj)] = s[g][jj];
+}
+template <int NQ>
+__device__ void gemm_over_b_rows(int m, int p, int k, const double* A, double* BC, int lane) {
+  int j0 = 0;
+  for (; j0 + 4 <= p; j0 += 4) gemm_block<NQ, 4>(m, k, A, BC, j0, lane);
+  for (; j0 < p; ++j0) gemm_block<NQ, 1>(m, k, A, BC, j0, lane);
+  __syncwarp();
+}
+__device__ inline void warp_gemm_over_b(int m, int p, int k, const double* A, double* BC, int lane) {
+  if (m <= 32) gemm_over_b_rows<1>(m, p, k, A, BC, lane);
+  else if (m <= 64) gemm_over_b_rows<2>(m, p, k, A, BC, lane);
+  else gemm_over_b_rows<3>(m, p, k, A, BC, lane);
 }
 // y(m) = A(m x n) x, netlib dgemv order
 __device__ inline void warp_gemv(int m, int n, const double* A, const double* x, double* y, int lane) {
@@ -188,9 +343,28 @@ __device__ inline void warp_gemv(int m, int n, const double* A, const double* x,
   }
   __syncwarp();
 }
+// y1 = A x1 and y2 = A x2 in one pass over A, each in netlib dgemv order
+__device__ inline void warp_gemv2(int m, int n, const double* A, const double* x1, const double* x2, double* y1,
+                                  double* y2, int lane) {
+  for (int i = lane; i < m; i += 32) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < n; ++j) {
+      const double av = A[i + m * j];
+      s1 = s1 + x1[j] * av;
+      s2 = s2 + x2[j] * av;
+    }
+    y1[i] = s1;
+    y2[i] = s2;
+  }
+  __syncwarp();
+}
 
-struct DiffSmem {  // offsets (doubles) of one vertex's work arrays, for the mesh's largest vertex
-  int N, S, St, T1, B, Vf, tmp, work, Ve, SB, SNSVe, blc3, theta, P, b1, ipiv, total;
+// Offsets (doubles) of one vertex's work arrays, for the mesh's largest vertex. N holds
+// the nodal matrix, then its inverse, then St N^-1; S holds S, then SNS = St N^-1 S. The
+// heat system reuses the same arrays at its smaller sizes, with its per-subcell theta,
+// P and b1 placed in St past the heat St's ne x nf entries.
+struct DiffSmem {
+  int N, S, St, B, Vf, tmp, work, Ve, SB, SNSVe, blc3, ipiv, total;
 };
 __host__ __device__ inline DiffSmem diff_layout(int max_vsf, int max_vse) {
   const int F = 3 * max_vsf, E = 3 * max_vse;
@@ -199,18 +373,14 @@ __host__ __device__ inline DiffSmem diff_layout(int max_vsf, int max_vse) {
   L.N = o, o += F * F;
   L.S = o, o += F * E;
   L.St = o, o += E * F;
-  L.T1 = o, o += E * F;  // SNS (E x E, E <= F) takes N's storage once N is no longer read
   L.B = o, o += F;
   L.Vf = o, o += F;
   L.tmp = o, o += F;
-  L.work = o, o += F;
+  L.work = o, o += F;  // tmp and work together are the inverse's 2 F scratch
   L.Ve = o, o += E;
   L.SB = o, o += E;
   L.SNSVe = o, o += E;
   L.blc3 = o, o += 3 * E;
-  L.theta = o, o += E;
-  L.P = o, o += 5 * E;
-  L.b1 = o, o += E;
   L.ipiv = o, o += F;  // ints stored in double slots
   L.total = o;
   return L;
@@ -257,9 +427,9 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
   extern __shared__ double sm[];
   const DiffSmem L = diff_layout(m.max_dsf, m.max_dse);
   const int lane = threadIdx.x;
-  double *N = sm + L.N, *S = sm + L.S, *St = sm + L.St, *T1 = sm + L.T1, *B = sm + L.B;
+  double *N = sm + L.N, *S = sm + L.S, *St = sm + L.St, *B = sm + L.B;
   double *Vf = sm + L.Vf, *tmp = sm + L.tmp, *work = sm + L.work, *Ve = sm + L.Ve, *SB = sm + L.SB;
-  double *SNSVe = sm + L.SNSVe, *blc3 = sm + L.blc3, *theta = sm + L.theta, *P = sm + L.P, *b1 = sm + L.b1;
+  double *SNSVe = sm + L.SNSVe, *blc3 = sm + L.blc3;
   int* ipiv = reinterpret_cast<int*>(sm + L.ipiv);
   const double mu0c = *mu0c_p;
   for (int v = blockIdx.x; v < m.nv; v += gridDim.x) {
@@ -346,14 +516,14 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     warp_gemv(F, E, S, Ve, Vf, lane);
     for (int i = lane; i < F; i += 32) Vf[i] = Vf[i] + B[i];
     __syncwarp();
-    warp_inverse(N, F, ipiv, work, lane);
-    // the products of the reference in an order that frees N before SNS is formed, so
-    // SNS takes N's storage (each product's own arithmetic is unchanged)
-    warp_gemv(F, F, N, B, tmp, lane);
-    warp_gemv(F, F, N, Vf, work, lane);  // N^-1 (S Ve + B): the face velocities
-    warp_gemm(E, F, F, St, N, T1, lane);
-    double* SNSm = N;
-    warp_gemm(E, E, F, T1, S, SNSm, lane);
+    warp_inverse(N, F, ipiv, tmp, lane);  // tmp and work (adjacent, 2 F) as its scratch
+    // the products of the reference, the two with N^-1 as a vector first, then
+    // T1 = St N^-1 over N and SNS = T1 S over S (each product's own arithmetic unchanged)
+    warp_gemv2(F, F, N, B, Vf, tmp, work, lane);  // N^-1 B, and N^-1 (S Ve + B): the face velocities
+    warp_gemm_over_b(E, F, F, St, N, lane);
+    const double* T1 = N;
+    warp_gemm_over_b(E, E, F, T1, S, lane);
+    const double* SNSm = S;
     warp_gemv(E, F, St, tmp, SB, lane);
     warp_gemv(E, E, SNSm, Ve, SNSVe, lane);
     for (int l = lane; l < ne; l += 32) {
@@ -455,11 +625,14 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
       }
     }
     __syncwarp();
-    warp_inverse(N, nf, ipiv, work, lane);
+    warp_inverse(N, nf, ipiv, tmp, lane);
     warp_gemv(nf, nf, N, B, tmp, lane);
-    warp_gemm(ne, nf, nf, St, N, T1, lane);
-    warp_gemm(ne, ne, nf, T1, S, SNSm, lane);
+    warp_gemm_over_b(ne, nf, nf, St, N, lane);
+    warp_gemm_over_b(ne, ne, nf, T1, S, lane);
     warp_gemv(ne, nf, St, tmp, SB, lane);
+    double* theta = St + ne * nf;  // past the heat St, which the loops below still read
+    double* P = theta + ne;
+    double* b1 = P + 5 * ne;
     for (int l = lane; l < ne; l += 32) {
       double u[5];
       load_u(U, m.se_elem[m.dse[s0 + l]], u);
