@@ -59,6 +59,8 @@ def _args():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     p.add_argument("--n", type=int, default=N_SIDE)
+    p.add_argument("--renumber", default="bfs", choices=["bfs", "hilbert"],
+                   help="vertex order of the Lagrangian mesh: the reference's breadth-first order or a Hilbert curve")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="lagrange",
                    choices=["lagrange", "gresho", "implicit", "shocktubes", "serve"])
@@ -192,13 +194,13 @@ def _traffic(kernel):
     return d.get("per_launch_dram_bytes", {}).get(kernel)
 
 
-def cpu_baseline(n_steps=4):
-    """The oracle (serial CPU restatement) on the same 512x512 mesh, a bounded number of
-    steps, on one host core."""
+def cpu_baseline(n_steps=4, renumber="bfs"):
+    """The oracle (serial CPU restatement) on the same 512x512 mesh, in the same vertex
+    order, a bounded number of steps, on one host core."""
     from oracle.oracle import OracleMesh
     from subfv_b200 import meshgen
     raw = _raw(N_SIDE)
-    o = OracleMesh(raw)
+    o = OracleMesh(raw, renumber=renumber)
     mask = meshgen.sedov_origin_mask(o.topo("elem_vert_off"), o.topo("elem_vert"), o.geom("vert_coord"))
     sol = o.sedov_init(e_total=E_SEDOV, mask=mask)
     mass = o.geom("elem_volume") / sol[:, 0]
@@ -364,14 +366,15 @@ def run_implicit(args, rank, world, local):
     n = 96 if args.n == N_SIDE else args.n
     t0 = time.perf_counter()
     raw = meshgen.hex_box(n, jitter=0.05, seed=SEED, periodic=True)
-    mesh = Mesh.from_raw(raw)
+    mesh = Mesh.from_raw(raw, renumber=args.renumber)
     setup_s = time.perf_counter() - t0
     sol0 = init_fourier_flow(mesh, seed=SEED)
     inviscid = NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5)
     viscous = NsConfig(scheme=4, second_order=False, method=0, bc_style=2, boundary_2d=False, cfl=0.5,
                        activate_diffusion=True, mu_p=1e-3, prandtl=0.72)
     res = {"metric": "cell-updates/s", "workload": f"periodic_box_{n}^3_backward_euler_navier_stokes",
-           "cells": mesh.n_elems, "mesh_setup_s": setup_s, "reynolds": 1000, "prandtl": 0.72}
+           "cells": mesh.n_elems, "mesh_setup_s": setup_s, "reynolds": 1000, "prandtl": 0.72,
+           "vertex_order": args.renumber}
     for name, refine, pc, cfg in (("fp64", False, 1, viscous), ("fp32_refine", True, 1, viscous),
                                   ("fp64_lusgs", False, 2, viscous), ("fp64_inviscid", False, 1, inviscid)):
         s = NsState(mesh, cfg, sol0)
@@ -692,7 +695,7 @@ def main():
 
     prec = MIXED if args.precision == "mixed" else PLAIN_FP64
     raw = _raw(args.n)
-    mesh = Mesh.from_raw(raw)
+    mesh = Mesh.from_raw(raw, renumber=args.renumber)
     topo = mesh.topo
     mask = meshgen.sedov_origin_mask(topo.array("elem_vert_off"), topo.array("elem_vert"), topo.coords())
     sol0 = init_sol_sedov(mesh, e_total=E_SEDOV, mask=mask)
@@ -761,7 +764,7 @@ def main():
     cpu = None
     parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu, sol_oracle = cpu_baseline()
+        cpu, sol_oracle = cpu_baseline(renumber=args.renumber)
         # the same 4 steps on the GPU from the same initial state, compared bit for bit
         mesh.set_coords(coords0)
         mesh.compute_geometry_mesh()
@@ -791,6 +794,7 @@ def main():
             "data": "synthetic (seeded jittered mesh, Sedov initial state)",
             "config": {"workload": WORKLOAD, "cells": cells, "vertices": mesh.n_vert,
                        "sub_faces": mesh.n_sub_faces, "precision": args.precision, "cfl": CFL,
+                       "vertex_order": args.renumber,
                        "l2": "working set ~1 GB per step > 126 MB L2 (no flush needed)",
                        "parallelism": f"replicas x{world}"},
             "status_bits": st, "sim_time": t_now,

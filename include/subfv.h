@@ -52,6 +52,15 @@ int subfv_topology_build(int n_vert, const double* coords, int n_elems, const in
                          const int32_t* elem_vert_off, const int32_t* elem_vert, int n_bfaces,
                          const int32_t* bface_off, const int32_t* bface_vert, const int32_t* bface_tag,
                          int b2d, int periodic, subfv_topology** out);
+/* The same with a choice of vertex order: renumber 0 is the reference's breadth-first
+ * order (subfv_topology_build); 1 orders the vertices along a Hilbert curve (the 2-D
+ * curve of (x, y) for slabs, b2d, else the 3-D curve; ties by input id), and cells,
+ * faces and subfaces then follow the reference's rules over that order. Results on a
+ * renumbered mesh differ from the breadth-first mesh's only in the order of sums. */
+int subfv_topology_build_ex(int n_vert, const double* coords, int n_elems, const int32_t* elem_kind,
+                            const int32_t* elem_vert_off, const int32_t* elem_vert, int n_bfaces,
+                            const int32_t* bface_off, const int32_t* bface_vert, const int32_t* bface_tag,
+                            int b2d, int periodic, int renumber, subfv_topology** out);
 int64_t subfv_topology_array_len(const subfv_topology* t, const char* name);
 int subfv_topology_array_get(const subfv_topology* t, const char* name, int32_t* out);
 int subfv_topology_coords(const subfv_topology* t, double* coords_out);

@@ -85,7 +85,8 @@ void read_raw(Mesh& m, int n_vert, const double* coords, int n_elems, const int*
               const int* ev_off, const int* ev, int n_bf, const int* bf_off, const int* bf_vert,
               const int* bf_tag);
 // mesh_connectivity_module.F90:12-59 (num_procs = 1).
-void build_mesh(Mesh& m, bool use_sub_entities, bool b2d, bool periodic);
+// renumber 0: the reference's BFS vertex order; 1: vertices along a Hilbert curve
+void build_mesh(Mesh& m, bool use_sub_entities, bool b2d, bool periodic, int renumber = 0);
 // mesh_geometry_module.F90:16-57.
 void compute_geometry_mesh(Mesh& m, bool b2d);
 void find_if_vert_is_bound(Mesh& m, bool b2d);

@@ -33,6 +33,9 @@ def load():
         lib = C.CDLL(str(LIB_PATH))
         lib.or_mesh_new.restype = C.c_void_p
         lib.or_mesh_new.argtypes = [C.c_int, PD, C.c_int, PI, PI, PI, C.c_int, PI, PI, PI, C.c_int, C.c_int]
+        lib.or_mesh_new_ex.restype = C.c_void_p
+        lib.or_mesh_new_ex.argtypes = [C.c_int, PD, C.c_int, PI, PI, PI, C.c_int, PI, PI, PI, C.c_int, C.c_int,
+                                       C.c_int]
         lib.or_mesh_free.argtypes = [C.c_void_p]
         lib.or_topo_len.argtypes = [C.c_void_p, C.c_char_p]
         lib.or_topo_get.argtypes = [C.c_void_p, C.c_char_p, PI]
@@ -118,7 +121,7 @@ def _pi(a):
 class OracleMesh:
     """build_mesh + compute_geometry_mesh on the CPU, as the reference does them."""
 
-    def __init__(self, raw):
+    def __init__(self, raw, renumber="bfs"):
         lib = load()
         self._keep = [np.ascontiguousarray(raw.coords.reshape(-1), np.float64),
                       np.ascontiguousarray(raw.elem_kind, np.int32),
@@ -129,8 +132,9 @@ class OracleMesh:
                       np.ascontiguousarray(raw.bface_tag, np.int32)]
         c, k, o, v, bo, bv, bt = self._keep
         self.b2d = bool(raw.b2d)
-        self._h = lib.or_mesh_new(raw.n_vert, _pd(c), raw.n_elems, _pi(k), _pi(o), _pi(v), int(bo.size - 1),
-                                  _pi(bo), _pi(bv), _pi(bt), int(raw.b2d), int(raw.periodic))
+        self._h = lib.or_mesh_new_ex(raw.n_vert, _pd(c), raw.n_elems, _pi(k), _pi(o), _pi(v), int(bo.size - 1),
+                                     _pi(bo), _pi(bv), _pi(bt), int(raw.b2d), int(raw.periodic),
+                                     {"bfs": 0, "hilbert": 1}[renumber])
         if not self._h:
             raise RuntimeError("oracle build_mesh failed")
         s = self.topo("sizes")

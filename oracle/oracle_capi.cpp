@@ -30,13 +30,13 @@ Mesh& handle_mesh(void* h) { return ((OHandle*)h)->m; }
 
 extern "C" {
 
-void* or_mesh_new(int n_vert, const double* coords, int n_elems, const int* kind, const int* ev_off,
-                  const int* ev, int n_bf, const int* bf_off, const int* bf_vert, const int* bf_tag,
-                  int b2d, int periodic) {
+void* or_mesh_new_ex(int n_vert, const double* coords, int n_elems, const int* kind, const int* ev_off,
+                     const int* ev, int n_bf, const int* bf_off, const int* bf_vert, const int* bf_tag,
+                     int b2d, int periodic, int renumber) {
   OHandle* h = new OHandle();
   try {
     read_raw(h->m, n_vert, coords, n_elems, kind, ev_off, ev, n_bf, bf_off, bf_vert, bf_tag);
-    build_mesh(h->m, true, b2d != 0, periodic != 0);
+    build_mesh(h->m, true, b2d != 0, periodic != 0, renumber);
     h->topo = export_topology(h->m);
     compute_geometry_mesh(h->m, b2d != 0);
   } catch (...) {
@@ -44,6 +44,11 @@ void* or_mesh_new(int n_vert, const double* coords, int n_elems, const int* kind
     return nullptr;
   }
   return h;
+}
+
+void* or_mesh_new(int n_vert, const double* coords, int n_elems, const int* kind, const int* ev_off, const int* ev,
+                  int n_bf, const int* bf_off, const int* bf_vert, const int* bf_tag, int b2d, int periodic) {
+  return or_mesh_new_ex(n_vert, coords, n_elems, kind, ev_off, ev, n_bf, bf_off, bf_vert, bf_tag, b2d, periodic, 0);
 }
 
 void or_mesh_free(void* p) { delete (OHandle*)p; }

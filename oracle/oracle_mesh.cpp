@@ -1,6 +1,7 @@
 // Test infrastructure only (oracle). Restatement of the subfv mesh pipeline:
 // MSH2 element->face tables, build_mesh topology, compute_geometry_mesh.
 // PARITY UNPINNED (no Fortran compiler here; the reference tests hold no golden data).
+#include <algorithm>
 #include "oracle.h"
 #include <cmath>
 #include <cstdio>
@@ -148,6 +149,81 @@ static void renumber_vert_mesh(Mesh& m) {
   for (int i = 1; i <= m.n_boundary_faces; ++i)
     for (int j = 1; j <= m.boundary_face[i].n_vert; ++j)
       m.boundary_face[i].vert[j] = otn[m.boundary_face[i].vert[j]];
+}
+
+// Not in the reference: the vertices along a Hilbert curve instead of the BFS order, for
+// checking the library's optional renumbering. J. Skilling, "Programming the Hilbert
+// curve", AIP Conf. Proc. 707, 381 (2004): the grid point's coordinates are turned into
+// the transposed Hilbert index (inverse undo, then Gray encode) and its bits read most
+// significant first across the axes. Slabs use (x, y) with 31 bits, else (x, y, z) with
+// 21 bits, on a cube of the largest extent; equal keys keep the input order.
+static unsigned long long skilling_key(unsigned int x[3], int n, int b) {
+  unsigned int m = 1u << (b - 1);
+  for (unsigned int q = m; q > 1; q >>= 1) {
+    unsigned int p = q - 1;
+    for (int i = 0; i < n; ++i) {
+      if (x[i] & q) {
+        x[0] ^= p;
+      } else {
+        unsigned int t = (x[0] ^ x[i]) & p;
+        x[0] ^= t;
+        x[i] ^= t;
+      }
+    }
+  }
+  for (int i = 1; i < n; ++i) x[i] ^= x[i - 1];
+  unsigned int t = 0;
+  for (unsigned int q = m; q > 1; q >>= 1)
+    if (x[n - 1] & q) t ^= q - 1;
+  for (int i = 0; i < n; ++i) x[i] ^= t;
+  unsigned long long key = 0;
+  for (int bit = b - 1; bit >= 0; --bit)
+    for (int i = 0; i < n; ++i) key = (key << 1) | ((x[i] >> bit) & 1u);
+  return key;
+}
+
+static void apply_vert_order(Mesh& m, const std::vector<int>& otn) {
+  std::vector<Vert> tmp = m.vert;
+  for (int i = 1; i <= m.n_vert; ++i) m.vert[otn[i]] = tmp[i];
+  for (int i = 1; i <= m.n_elems; ++i)
+    for (int j = 1; j <= m.elem[i].n_vert; ++j) m.elem[i].vert[j] = otn[m.elem[i].vert[j]];
+  for (int i = 1; i <= m.n_faces; ++i)
+    for (int j = 1; j <= m.minimal_face[i].n_vert; ++j)
+      m.minimal_face[i].vert[j] = otn[m.minimal_face[i].vert[j]];
+  for (int i = 1; i <= m.n_boundary_faces; ++i)
+    for (int j = 1; j <= m.boundary_face[i].n_vert; ++j)
+      m.boundary_face[i].vert[j] = otn[m.boundary_face[i].vert[j]];
+}
+
+static void renumber_vert_hilbert(Mesh& m, bool b2d) {
+  int nv = m.n_vert, n = b2d ? 2 : 3, bits = b2d ? 31 : 21;
+  double lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) lo[d] = hi[d] = m.vert[1].coord[d + 1];
+  for (int i = 2; i <= nv; ++i)
+    for (int d = 0; d < 3; ++d) {
+      if (m.vert[i].coord[d + 1] < lo[d]) lo[d] = m.vert[i].coord[d + 1];
+      if (m.vert[i].coord[d + 1] > hi[d]) hi[d] = m.vert[i].coord[d + 1];
+    }
+  double ext = 0.0;
+  for (int d = 0; d < n; ++d)
+    if (hi[d] - lo[d] > ext) ext = hi[d] - lo[d];
+  double top = (double)((1u << bits) - 1u);
+  double scale = ext > 0.0 ? top / ext : 0.0;
+  std::vector<std::pair<unsigned long long, int>> order(nv);
+  for (int i = 1; i <= nv; ++i) {
+    unsigned int x[3] = {0, 0, 0};
+    for (int d = 0; d < n; ++d) {
+      double q = (m.vert[i].coord[d + 1] - lo[d]) * scale;
+      if (q < 0.0) q = 0.0;
+      if (q > top) q = top;
+      x[d] = (unsigned int)q;
+    }
+    order[i - 1] = std::make_pair(skilling_key(x, n, bits), i);
+  }
+  std::sort(order.begin(), order.end());
+  std::vector<int> otn(nv + 1, -1);
+  for (int k = 0; k < nv; ++k) otn[order[k].second] = k + 1;
+  apply_vert_order(m, otn);
 }
 
 // mesh_connectivity_module.F90:752-849 (num_procs = 1: first touch over vertices)
@@ -610,9 +686,12 @@ static void build_periodic_stencil(Mesh& m) {
 }
 
 // mesh_connectivity_module.F90:12-59 (single rank)
-void build_mesh(Mesh& m, bool use_sub_entities, bool b2d, bool periodic) {
+void build_mesh(Mesh& m, bool use_sub_entities, bool b2d, bool periodic, int renumber) {
   build_node_elem_neigh(m);
-  renumber_vert_mesh(m);
+  if (renumber == 1)
+    renumber_vert_hilbert(m, b2d);
+  else
+    renumber_vert_mesh(m);
   renumber_elem_mesh(m);
   build_faces(m);
   build_node_face_connectivity(m);

@@ -29,6 +29,8 @@ SIGNATURES = {
     "subfv_probe_div_const": (c_int, [PD, c_i64, C.POINTER(c_i64)]),
     "subfv_topology_build": (c_int, [c_int, PD, c_int, PI32, PI32, PI32, c_int, PI32, PI32, PI32, c_int, c_int,
                                      C.POINTER(P)]),
+    "subfv_topology_build_ex": (c_int, [c_int, PD, c_int, PI32, PI32, PI32, c_int, PI32, PI32, PI32, c_int, c_int,
+                                        c_int, C.POINTER(P)]),
     "subfv_topology_array_len": (c_i64, [P, c_char_p]),
     "subfv_topology_array_get": (c_int, [P, c_char_p, PI32]),
     "subfv_topology_coords": (c_int, [P, PD]),

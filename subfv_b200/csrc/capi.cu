@@ -132,12 +132,23 @@ int subfv_topology_build(int n_vert, const double* coords, int n_elems, const in
                          const int32_t* elem_vert_off, const int32_t* elem_vert, int n_bfaces,
                          const int32_t* bface_off, const int32_t* bface_vert, const int32_t* bface_tag,
                          int b2d, int periodic, subfv_topology** out) {
+  return subfv_topology_build_ex(n_vert, coords, n_elems, elem_kind, elem_vert_off, elem_vert, n_bfaces, bface_off,
+                                 bface_vert, bface_tag, b2d, periodic, 0, out);
+}
+int subfv_topology_build_ex(int n_vert, const double* coords, int n_elems, const int32_t* elem_kind,
+                            const int32_t* elem_vert_off, const int32_t* elem_vert, int n_bfaces,
+                            const int32_t* bface_off, const int32_t* bface_vert, const int32_t* bface_tag,
+                            int b2d, int periodic, int renumber, subfv_topology** out) {
   if (!out || !coords || !elem_kind || !elem_vert_off || !elem_vert) {
     set_error("subfv_topology_build: null argument");
     return -2;
   }
+  if (renumber != 0 && renumber != 1) {
+    set_error("subfv_topology_build_ex: renumber must be 0 (breadth-first) or 1 (Hilbert curve)");
+    return -2;
+  }
   RawMeshView in{n_vert, coords, n_elems, elem_kind, elem_vert_off, elem_vert,
-                 n_bfaces, bface_off, bface_vert, bface_tag, b2d, periodic};
+                 n_bfaces, bface_off, bface_vert, bface_tag, b2d, periodic, renumber};
   auto* t = new subfv_topology();
   std::string err;
   int rc = build_topology(in, t->t, &err);

@@ -57,7 +57,68 @@ FaceKey make_key(const int32_t* v, int n) {
 
 bool near(double a, double b) { return a < b + 1e-12 && a > b - 1e-12; }
 
+// Index of the grid point X (n coordinates of b bits) along the n-dimensional Hilbert
+// curve, by Skilling's transpose method (J. Skilling, "Programming the Hilbert curve",
+// AIP Conf. Proc. 707, 381 (2004)): undo the excess rotations level by level, Gray-code
+// the transposed index, then read its bits most significant first across the axes.
+uint64_t hilbert_index(uint32_t* X, int n, int b) {
+  const uint32_t M = 1u << (b - 1);
+  for (uint32_t Q = M; Q > 1; Q >>= 1) {
+    const uint32_t P = Q - 1;
+    for (int i = 0; i < n; ++i) {
+      if (X[i] & Q) {
+        X[0] ^= P;
+      } else {
+        const uint32_t t = (X[0] ^ X[i]) & P;
+        X[0] ^= t;
+        X[i] ^= t;
+      }
+    }
+  }
+  for (int i = 1; i < n; ++i) X[i] ^= X[i - 1];
+  uint32_t t = 0;
+  for (uint32_t Q = M; Q > 1; Q >>= 1)
+    if (X[n - 1] & Q) t ^= Q - 1;
+  for (int i = 0; i < n; ++i) X[i] ^= t;
+  uint64_t key = 0;
+  for (int bit = b - 1; bit >= 0; --bit)
+    for (int i = 0; i < n; ++i) key = (key << 1) | ((X[i] >> bit) & 1u);
+  return key;
+}
+
 }  // namespace
+
+void hilbert_vertex_order(int nv, const double* c, int b2d, std::vector<int32_t>& otn, std::vector<int32_t>& nto) {
+  const int dims = b2d ? 2 : 3, bits = b2d ? 31 : 21;
+  double lo[3], hi[3];
+  for (int d = 0; d < 3; ++d) lo[d] = hi[d] = c[d];
+  for (int i = 1; i < nv; ++i)
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = std::min(lo[d], c[3 * i + d]);
+      hi[d] = std::max(hi[d], c[3 * i + d]);
+    }
+  double ext = 0.0;
+  for (int d = 0; d < dims; ++d) ext = std::max(ext, hi[d] - lo[d]);
+  const double top = (double)((1u << bits) - 1u);
+  const double scale = ext > 0.0 ? top / ext : 0.0;
+  std::vector<std::pair<uint64_t, int32_t>> key(nv);
+  for (int i = 0; i < nv; ++i) {
+    uint32_t X[3] = {0, 0, 0};
+    for (int d = 0; d < dims; ++d) {
+      double q = (c[3 * i + d] - lo[d]) * scale;
+      q = q < 0.0 ? 0.0 : (q > top ? top : q);
+      X[d] = (uint32_t)q;
+    }
+    key[i] = {hilbert_index(X, dims, bits), i + 1};
+  }
+  std::sort(key.begin(), key.end());
+  otn.assign(nv + 1, -1);
+  nto.assign(nv + 1, -1);
+  for (int k = 0; k < nv; ++k) {
+    nto[k + 1] = key[k].second;
+    otn[key[k].second] = k + 1;
+  }
+}
 
 int build_topology(const RawMeshView& in, Topology& T, std::string* err) {
   const int nv = in.n_vert, ne = in.n_elems;
@@ -81,9 +142,12 @@ int build_topology(const RawMeshView& in, Topology& T, std::string* err) {
   });
 
   // -- BFS vertex renumbering (:851-926): a FIFO over the new numbering, restarted at
-  // the lowest unnumbered vertex when a component is exhausted.
+  // the lowest unnumbered vertex when a component is exhausted. Or, as an option, the
+  // vertices along a Hilbert curve; everything below follows whichever order is chosen.
   V otn_v(nv + 1, -1), nto_v(nv + 1, -1);
-  {
+  if (in.renumber == 1) {
+    hilbert_vertex_order(nv, in.coords, in.b2d, otn_v, nto_v);
+  } else {
     int iloc = 1, head = 1, scan = 1;
     otn_v[1] = 1;
     nto_v[1] = 1;

@@ -25,6 +25,7 @@ struct RawMeshView {
   const int32_t* bface_tag;   // boundary-condition index (0 = none / wall)
   int b2d;
   int periodic;
+  int renumber = 0;  // 0: the reference's BFS vertex order; 1: along a Hilbert curve
 };
 
 // All ids are 1-based like the reference's; face_right: >0 cell, 0 wall, <0 -tag.
@@ -38,5 +39,12 @@ struct Topology {
 
 // Returns 0 on success, a positive code on malformed input.
 int build_topology(const RawMeshView& in, Topology& out, std::string* err);
+
+// Position of each vertex along a Hilbert curve: new id (1-based) of input vertex i at
+// otn[i], input id of new vertex k at nto[k] (both 1-based, entry 0 unused). Slabs
+// (b2d) follow the 2-D curve of (x, y), so a column's vertices share a key; 3-D meshes
+// the 3-D curve of (x, y, z); both on a cube around the mesh, ties by input id.
+void hilbert_vertex_order(int n_vert, const double* coords, int b2d, std::vector<int32_t>& otn,
+                          std::vector<int32_t>& nto);
 
 }  // namespace subfv

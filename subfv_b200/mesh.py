@@ -21,20 +21,29 @@ SUBFV_ERR_BAD_OMEGA = 8
 SUBFV_ERR_GMRES = 16
 
 
-class Topology:
-    """build_mesh output: the reference's numbering, arrays fetched by mesh_type name."""
+RENUMBER = {"bfs": 0, "hilbert": 1}
 
-    def __init__(self, raw: RawMesh):
+
+class Topology:
+    """build_mesh output, arrays fetched by mesh_type name. renumber "bfs" is the
+    reference's numbering; "hilbert" orders the vertices along a Hilbert curve (cells,
+    faces and subfaces then follow the reference's rules over that order)."""
+
+    def __init__(self, raw: RawMesh, renumber: str = "bfs"):
         lib = _lib.load()
+        if renumber not in RENUMBER:
+            raise ValueError(f"renumber must be one of {sorted(RENUMBER)}")
+        self.renumber = renumber
         self.raw = raw
         h = C.c_void_p()
         coords = f64(raw.coords.reshape(-1))
         kind, off, ev = i32(raw.elem_kind), i32(raw.elem_vert_off), i32(raw.elem_vert)
         bo, bv, bt = i32(raw.bface_off), i32(raw.bface_vert), i32(raw.bface_tag)
         nbf = int(bo.size - 1)
-        check(lib.subfv_topology_build(raw.n_vert, pd(coords), raw.n_elems, pi(kind), pi(off), pi(ev), nbf,
-                                       pi(bo), pi(bv), pi(bt), int(raw.b2d), int(raw.periodic), C.byref(h)),
-              "subfv_topology_build")
+        check(lib.subfv_topology_build_ex(raw.n_vert, pd(coords), raw.n_elems, pi(kind), pi(off), pi(ev), nbf,
+                                          pi(bo), pi(bv), pi(bt), int(raw.b2d), int(raw.periodic),
+                                          RENUMBER[renumber], C.byref(h)),
+              "subfv_topology_build_ex")
         self._h = h
         s = self.array("sizes")
         self.n_vert, self.n_elems, self.n_faces, self.n_sub_faces, self.n_sub_elems, self.n_max_sub_faces_around_node = map(int, s)
@@ -80,8 +89,8 @@ class Mesh:
         self.geometry_status = self.compute_geometry_mesh() if geometry else 0
 
     @classmethod
-    def from_raw(cls, raw: RawMesh, geometry: bool = True) -> "Mesh":
-        return cls(Topology(raw), b2d=raw.b2d, geometry=geometry)
+    def from_raw(cls, raw: RawMesh, geometry: bool = True, renumber: str = "bfs") -> "Mesh":
+        return cls(Topology(raw, renumber), b2d=raw.b2d, geometry=geometry)
 
     def compute_geometry_mesh(self) -> int:
         """Returns SUBFV_ERR_MESH_CHECK where the reference error-stops on check_mesh."""
