@@ -127,19 +127,20 @@ __device__ inline void lag_node_body(const DevMesh& m, const int v) {
   double R0 = 0, R1 = 0, R2 = 0, B0 = 0, B1 = 0, B2 = 0;
   const int p0 = m.vsf_off[v], p1 = m.vsf_off[v + 1];
   // entries in chunks of kNodeChunk: the chunk's loads are issued together, then the
-  // sums run in entry order
+  // sums run in entry order; the next chunk's subface ids and areas are loaded while
+  // they run
+  int fc[kNodeChunk];
+  double arc[kNodeChunk];
+#pragma unroll
+  for (int u = 0; u < kNodeChunk; ++u)
+    if (p0 + u < p1) {
+      const int sf = m.vsf_identity ? p0 + u : m.vsf[p0 + u];
+      fc[u] = m.sf_face[sf];
+      arc[u] = m.sfa[sf];
+    }
   for (int p = p0; p < p1; p += kNodeChunk) {
     double4 fnc[kNodeChunk];
     double2 llc[kNodeChunk], xkc[kNodeChunk];
-    double arc[kNodeChunk];
-    int fc[kNodeChunk];
-#pragma unroll
-    for (int u = 0; u < kNodeChunk; ++u)
-      if (p + u < p1) {
-        const int sf = m.vsf_identity ? p + u : m.vsf[p + u];
-        fc[u] = m.sf_face[sf];
-        arc[u] = m.sfa[sf];
-      }
 #pragma unroll
     for (int u = 0; u < kNodeChunk; ++u)
       if (p + u < p1) {
@@ -147,6 +148,15 @@ __device__ inline void lag_node_body(const DevMesh& m, const int v) {
         const double2* fr = reinterpret_cast<const double2*>(m.frec + kFrec * (size_t)fc[u]);
         llc[u] = fr[0];
         xkc[u] = fr[2];
+      }
+    int fn_next[kNodeChunk];
+    double ar_next[kNodeChunk];
+#pragma unroll
+    for (int u = 0; u < kNodeChunk; ++u)
+      if (p + kNodeChunk + u < p1) {
+        const int sf = m.vsf_identity ? p + kNodeChunk + u : m.vsf[p + kNodeChunk + u];
+        fn_next[u] = m.sf_face[sf];
+        ar_next[u] = m.sfa[sf];
       }
 #pragma unroll
     for (int u = 0; u < kNodeChunk; ++u) {
@@ -176,6 +186,11 @@ __device__ inline void lag_node_body(const DevMesh& m, const int v) {
       M00 = M00 + w * (n0 * n0); M01 = M01 + w * (n0 * n1); M02 = M02 + w * (n0 * n2);
       M10 = M10 + w * (n1 * n0); M11 = M11 + w * (n1 * n1); M12 = M12 + w * (n1 * n2);
       M20 = M20 + w * (n2 * n0); M21 = M21 + w * (n2 * n1); M22 = M22 + w * (n2 * n2);
+    }
+#pragma unroll
+    for (int u = 0; u < kNodeChunk; ++u) {
+      fc[u] = fn_next[u];
+      arc[u] = ar_next[u];
     }
   }
   // inverse_3_by_3 (linear_solver_module.F90:134-172): adjugate of the transpose
@@ -349,12 +364,13 @@ __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict_
     const double vse_c = m.vol_se[c < m.nse ? c : 0];  // sub_elem(i) with i the cell (reference quirk)
     const int q1 = m.csf_off[c + 1];
     // entries in chunks of kCellChunk: the chunk's loads are issued together, then the
-    // sums run in entry order
-    for (int q = m.csf_off[c]; q < q1; q += kCellChunk) {
-      int4 Ec[kCellChunk];
+    // sums run in entry order; the next chunk's entries are loaded while they run
+    int q = m.csf_off[c];
+    int4 Ec[kCellChunk];
 #pragma unroll
-      for (int u = 0; u < kCellChunk; ++u)
-        if (q + u < q1) Ec[u] = m.centry[q + u];
+    for (int u = 0; u < kCellChunk; ++u)
+      if (q + u < q1) Ec[u] = m.centry[q + u];
+    for (; q < q1; q += kCellChunk) {
       double4 fnc[kCellChunk], vpc[kCellChunk];
       double2 llc[kCellChunk], vvc[kCellChunk];
       double arc[kCellChunk], vsub[kCellChunk];
@@ -373,6 +389,10 @@ __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict_
           }
           if (mode & 2) vsub[u] = E.w >= 0 ? m.vol_se[E.w] : 0.0;
         }
+      int4 En[kCellChunk];
+#pragma unroll
+      for (int u = 0; u < kCellChunk; ++u)
+        if (q + kCellChunk + u < q1) En[u] = m.centry[q + kCellChunk + u];
 #pragma unroll
       for (int u = 0; u < kCellChunk; ++u) {
         if (q + u >= q1) break;
@@ -435,6 +455,8 @@ __device__ inline void lag_cell_body(const DevMesh& m, const double* __restrict_
           bad = bad || !(t1 >= 0.0) || !(t2 >= 0.0);
         }
       }
+#pragma unroll
+      for (int u = 0; u < kCellChunk; ++u) Ec[u] = En[u];
     }
     if (mode & 1) {
       double2* r = reinterpret_cast<double2*>(rhs6 + kRhs * (size_t)c);
