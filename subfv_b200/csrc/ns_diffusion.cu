@@ -67,8 +67,9 @@ __device__ inline int sf_of(const int4 q, int p) { return p == 0 ? q.x : p == 1 
 
 // dgetf2's rank-1 update of the trailing block after column j (dger with alpha = -1:
 // a(i,k) - l(i) u(k)), rows j + 1 + lane + 32 g
-template <int G>
-__device__ __forceinline__ void lu_update(double* a, int n, int j, int lane) {
+template <int G, int NC>
+__device__ __forceinline__ void lu_update(double* a, int n_rt, int j, int lane) {
+  const int n = NC > 0 ? NC : n_rt;
   double l[G];
   double* row[G];
   bool ok[G];
@@ -112,8 +113,9 @@ __device__ __forceinline__ void lu_update(double* a, int n, int j, int lane) {
 // to each row i < jj. So a row's result is its own value scaled by the diagonal, then
 // the original x(jj) T(i,jj) added in increasing jj, each skipped when x(jj) is zero:
 // every lane reads the original column and accumulates its rows i < j (G groups).
-template <int G>
-__device__ __forceinline__ void trti_col(double* a, int n, int j, int lane) {
+template <int G, int NC>
+__device__ __forceinline__ void trti_col(double* a, int n_rt, int j, int lane) {
+  const int n = NC > 0 ? NC : n_rt;
   const double ajj = -a[j + n * j];
   double* x = a + n * j;
   double acc[G];
@@ -163,8 +165,9 @@ __device__ __forceinline__ void trti_col(double* a, int n, int j, int lane) {
 // of L(jj,j) times column jj; then the column interchanges of ipiv from the last. Rows
 // are independent: lane r keeps rows r + 32 g, and each column's L entries are copied
 // to work (2 n doubles, alternate halves per column) before any row overwrites them.
-template <int NQ>
-__device__ __forceinline__ void getri_sweep(double* a, int n, const int* ipiv, double* work, int lane) {
+template <int NQ, int NC>
+__device__ __forceinline__ void getri_sweep(double* a, int n_rt, const int* ipiv, double* work, int lane) {
+  const int n = NC > 0 ? NC : n_rt;
   int ic[NQ];
 #pragma unroll
   for (int g = 0; g < NQ; ++g) ic[g] = lane + 32 * g < n ? lane + 32 * g : 0;
@@ -214,8 +217,10 @@ __device__ __forceinline__ void getri_sweep(double* a, int n, const int* ipiv, d
   __syncwarp();
 }
 
-// work: 2 n doubles
-__device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane) {
+// work: 2 n doubles. NC > 0 fixes n at compile time (every index product a constant).
+template <int NC>
+__device__ void warp_inverse_n(double* a, int n_rt, int* ipiv, double* work, int lane) {
+  const int n = NC > 0 ? NC : n_rt;
   for (int j = 0; j < n; ++j) {  // dgetf2
     double big = -1.0;
     int bi = n;
@@ -257,21 +262,33 @@ __device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane
     }
     __syncwarp();
     const int w = n - j - 1;
-    if (w > 64) lu_update<3>(a, n, j, lane);
-    else if (w > 32) lu_update<2>(a, n, j, lane);
-    else if (w > 0) lu_update<1>(a, n, j, lane);
+    if (w > 64) lu_update<3, NC>(a, n, j, lane);
+    else if (w > 32) lu_update<2, NC>(a, n, j, lane);
+    else if (w > 0) lu_update<1, NC>(a, n, j, lane);
     __syncwarp();
   }
   for (int j = 0; j < n; ++j) {  // dtrti2
     if (lane == 0) a[j + n * j] = 1.0 / a[j + n * j];
     __syncwarp();
-    if (j > 64) trti_col<3>(a, n, j, lane);
-    else if (j > 32) trti_col<2>(a, n, j, lane);
-    else if (j > 0) trti_col<1>(a, n, j, lane);
+    if (j > 64) trti_col<3, NC>(a, n, j, lane);
+    else if (j > 32) trti_col<2, NC>(a, n, j, lane);
+    else if (j > 0) trti_col<1, NC>(a, n, j, lane);
   }
-  if (n > 64) getri_sweep<3>(a, n, ipiv, work, lane);
-  else if (n > 32) getri_sweep<2>(a, n, ipiv, work, lane);
-  else getri_sweep<1>(a, n, ipiv, work, lane);
+  if (n > 64) getri_sweep<3, NC>(a, n, ipiv, work, lane);
+  else if (n > 32) getri_sweep<2, NC>(a, n, ipiv, work, lane);
+  else getri_sweep<1, NC>(a, n, ipiv, work, lane);
+}
+
+// The sizes of hexahedral meshes (momentum 36, heat 12 per vertex) and of one-layer slabs
+// of hexahedra (24, 8) with their index arithmetic fixed; others at run time.
+__device__ inline void warp_inverse(double* a, int n, int* ipiv, double* work, int lane) {
+  switch (n) {
+    case 36: warp_inverse_n<36>(a, n, ipiv, work, lane); break;
+    case 24: warp_inverse_n<24>(a, n, ipiv, work, lane); break;
+    case 12: warp_inverse_n<12>(a, n, ipiv, work, lane); break;
+    case 8: warp_inverse_n<8>(a, n, ipiv, work, lane); break;
+    default: warp_inverse_n<0>(a, n, ipiv, work, lane);
+  }
 }
 
 // C(m x p) = A(m x k) B(k x p), netlib dgemm order: C(i,j) = sum over l, in order, of
@@ -280,8 +297,9 @@ __device__ void warp_inverse(double* a, int n, int* ipiv, double* work, int lane
 // stored once the whole warp has read that block of B (the stored block ends at
 // m (j0 + JB) <= k (j0 + JB), below the columns still to be read). A lane owns rows
 // lane + 32 g, so one load of A(i,l) serves JB sums and B(l,j) is a broadcast.
-template <int NQ, int JB>
-__device__ __forceinline__ void gemm_block(int m, int k, const double* A, double* BC, int j0, int lane) {
+template <int NQ, int JB, int MC, int KC>
+__device__ __forceinline__ void gemm_block(int m_rt, int k_rt, const double* A, double* BC, int j0, int lane) {
+  const int m = MC > 0 ? MC : m_rt, k = KC > 0 ? KC : k_rt;
   double s[NQ][JB];
 #pragma unroll
   for (int g = 0; g < NQ; ++g)
@@ -322,15 +340,20 @@ __device__ __forceinline__ void gemm_block(int m, int k, const double* A, double
 #pragma unroll
       for (int jj = 0; jj < JB; ++jj) BC[lane + 32 * g + m * (j0 + jj)] = s[g][jj];
 }
-template <int NQ>
+template <int NQ, int MC = 0, int KC = 0>
 __device__ void gemm_over_b_rows(int m, int p, int k, const double* A, double* BC, int lane) {
   int j0 = 0;
-  for (; j0 + 4 <= p; j0 += 4) gemm_block<NQ, 4>(m, k, A, BC, j0, lane);
-  for (; j0 < p; ++j0) gemm_block<NQ, 1>(m, k, A, BC, j0, lane);
+  for (; j0 + 4 <= p; j0 += 4) gemm_block<NQ, 4, MC, KC>(m, k, A, BC, j0, lane);
+  for (; j0 < p; ++j0) gemm_block<NQ, 1, MC, KC>(m, k, A, BC, j0, lane);
   __syncwarp();
 }
+// (m, k) of the hexahedral and one-layer-slab vertices fixed at compile time, as above
 __device__ inline void warp_gemm_over_b(int m, int p, int k, const double* A, double* BC, int lane) {
-  if (m <= 32) gemm_over_b_rows<1>(m, p, k, A, BC, lane);
+  if (m == 24 && k == 36) gemm_over_b_rows<1, 24, 36>(m, p, k, A, BC, lane);
+  else if (m == 8 && k == 12) gemm_over_b_rows<1, 8, 12>(m, p, k, A, BC, lane);
+  else if (m == 12 && k == 24) gemm_over_b_rows<1, 12, 24>(m, p, k, A, BC, lane);
+  else if (m == 4 && k == 8) gemm_over_b_rows<1, 4, 8>(m, p, k, A, BC, lane);
+  else if (m <= 32) gemm_over_b_rows<1>(m, p, k, A, BC, lane);
   else if (m <= 64) gemm_over_b_rows<2>(m, p, k, A, BC, lane);
   else gemm_over_b_rows<3>(m, p, k, A, BC, lane);
 }
