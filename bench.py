@@ -16,7 +16,7 @@ L2, so no flush is needed between steps.
 `parity`: the same 4 steps run by the oracle (the CPU restatement, also the
 `cpu_baseline` sample) and by the GPU from the same initial state, compared bit for bit.
 
-`north_star` (one GPU, default run): the batched mixed-precision measurement
+`batched_and_served` (one GPU, default run): the batched mixed-precision measurement
 (`batched_mixed`: 256 shock tubes, N uniform in [200, 20000], about 10.6 M cells, K
 steps at precision levels 0/1/2 against the plain FP64 path run one problem at a time,
 and per-field L1 / Linf / drift of 16 problems run to their end time) and a serving
@@ -71,7 +71,7 @@ def _args():
     p.add_argument("--rate", type=float, default=20.0)
     p.add_argument("--max-cells", type=int, default=1 << 18)
     p.add_argument("--time-scale", type=float, default=0.05)
-    p.add_argument("--no-north-star", action="store_true",
+    p.add_argument("--no-batch-serve", action="store_true",
                    help="skip the batched-mixed and serving measurements of the default run")
     p.add_argument("--ns-problems", type=int, default=256, help="shock tubes in the default run's batch")
     p.add_argument("--ns-steps", type=int, default=10)
@@ -779,9 +779,9 @@ def main():
             parity.update(l1_rel=dict(zip(FIELDS, e1)), linf_rel=dict(zip(FIELDS, ei)))
         st_par.close()
 
-    north = None
-    if rank == 0 and world == 1 and not args.no_north_star:
-        north = {"batched_mixed": shocktube_block(args.ns_problems, args.nmax, args.ns_steps, 3, 32, local),
+    batch_serve = None
+    if rank == 0 and world == 1 and not args.no_batch_serve:
+        batch_serve = {"batched_mixed": shocktube_block(args.ns_problems, args.nmax, args.ns_steps, 3, 32, local),
                  "serve": serve_block(args.serve_requests, args.rate, args.serve_max_cells, args.time_scale, 8,
                                       local)}
 
@@ -809,7 +809,7 @@ def main():
             "fp64": _fp64_peak(),
             "cpu_baseline": cpu,
             "parity": parity,
-            "north_star": north,
+            "batched_and_served": batch_serve,
         }
         print(json.dumps(out), flush=True)
     if world > 1:
