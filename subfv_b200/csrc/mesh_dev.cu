@@ -314,19 +314,6 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
     std::stable_sort(vorder.begin(), vorder.end(), [&](int a, int b) { return vkey[a] < vkey[b]; });
   }
   if (upload(&m->forder, forder, B, s) || upload(&m->vorder, vorder, B, s)) return -1;
-  {
-    DiffStencil D;
-    if (int rc = build_diffusion_stencil(nv, vsf_off, vsf, vse_off, vse, sf_face, sf_vert, flr, se_elem, se_vert,
-                                         se_sf, &D))
-      return rc;
-    m->max_dsf = D.max_sf;
-    m->max_dse = D.max_se;
-    m->dstencil_ok = D.complete ? 1 : 0;
-    if (upload(&m->dsf_off, D.sf_off, B, s) || upload(&m->dsf, D.sf, B, s) || upload(&m->dsf_se, D.sf_se, B, s) ||
-        upload(&m->dsf_seloc, D.sf_seloc, B, s) || upload(&m->dse_off, D.se_off, B, s) ||
-        upload(&m->dse, D.se, B, s) || upload(&m->dse_sfloc, D.se_sfloc, B, s))
-      return -1;
-  }
   if (upload(&m->x, x, B, s) || alloc(&m->vp, nv, B, s) || alloc(&m->vol_v, nv, B, s) || upload(&m->is_bound, isb, B, s) ||
       upload(&m->fvert, fvert, B, s) || upload(&m->flr, flr, B, s) || upload(&m->fsf, fsf, B, s) ||
       alloc(&m->fc, nf, B, s) || alloc(&m->fn, nf, B, s) || upload(&m->sf_face, sf_face, B, s) ||
@@ -340,6 +327,49 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
       upload(&m->csf, csf, B, s) || alloc(&m->status, 4, B, s) || upload(&m->fpos, fpos, B, s))
     return -1;
   SUBFV_CUDA(cudaStreamSynchronize(s));
+  return 0;
+}
+
+namespace {
+template <class T>
+int fetch(std::vector<T>& h, const T* d, size_t n, cudaStream_t s) {
+  h.resize(n);
+  if (n) SUBFV_CUDA(cudaMemcpyAsync(h.data(), d, n * sizeof(T), cudaMemcpyDeviceToHost, s));
+  return 0;
+}
+}  // namespace
+
+// The diffusion stencil is only read by the Navier-Stokes diffusion terms: it is built the
+// first time a state asks for them, from the node lists already on the device (a mesh
+// that never runs diffusion holds none of its arrays).
+int ensure_diffusion_stencil(DevMesh* m) {
+  if (m->dstencil_built) return 0;
+  cudaStream_t s = m->stream;
+  std::vector<int> vsf_off, vsf, vse_off, vse, sf_face, sf_vert, se_elem, se_vert;
+  std::vector<int2> flr;
+  std::vector<int4> se_sf;
+  if (fetch(vsf_off, m->vsf_off, (size_t)m->nv + 1, s) || fetch(vse_off, m->vse_off, (size_t)m->nv + 1, s) ||
+      fetch(sf_face, m->sf_face, (size_t)m->nsf, s) || fetch(sf_vert, m->sf_vert, (size_t)m->nsf, s) ||
+      fetch(flr, m->flr, (size_t)m->nf, s) || fetch(se_elem, m->se_elem, (size_t)m->nse, s) ||
+      fetch(se_vert, m->se_vert, (size_t)m->nse, s) || fetch(se_sf, m->se_sf, (size_t)m->nse, s))
+    return -1;
+  SUBFV_CUDA(cudaStreamSynchronize(s));
+  if (fetch(vsf, m->vsf, (size_t)vsf_off[m->nv], s) || fetch(vse, m->vse, (size_t)vse_off[m->nv], s)) return -1;
+  SUBFV_CUDA(cudaStreamSynchronize(s));
+  DiffStencil D;
+  if (int rc = build_diffusion_stencil(m->nv, vsf_off, vsf, vse_off, vse, sf_face, sf_vert, flr, se_elem, se_vert,
+                                       se_sf, &D))
+    return rc;
+  size_t* B = &m->bytes;
+  if (upload(&m->dsf_off, D.sf_off, B, s) || upload(&m->dsf, D.sf, B, s) || upload(&m->dsf_se, D.sf_se, B, s) ||
+      upload(&m->dsf_seloc, D.sf_seloc, B, s) || upload(&m->dse_off, D.se_off, B, s) ||
+      upload(&m->dse, D.se, B, s) || upload(&m->dse_sfloc, D.se_sfloc, B, s))
+    return -1;
+  SUBFV_CUDA(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  m->max_dsf = D.max_sf;
+  m->max_dse = D.max_se;
+  m->dstencil_ok = D.complete ? 1 : 0;
+  m->dstencil_built = 1;
   return 0;
 }
 

@@ -87,7 +87,8 @@ struct DevMesh {
   int* dse = nullptr;
   int4* dse_sfloc = nullptr;
   int max_dsf = 0, max_dse = 0;
-  int dstencil_ok = 1;  // every stencil subface's subcells and subcell's subfaces found
+  int dstencil_ok = 1;     // every stencil subface's subcells and subcell's subfaces found
+  int dstencil_built = 0;  // the d* arrays exist (ensure_diffusion_stencil)
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;
@@ -129,6 +130,9 @@ __device__ inline int vert_at(const DevMesh& m, int t) { return t < m.nv ? m.vor
 
 int devmesh_create(const struct subfv_mesh_desc* d, DevMesh* m);
 void devmesh_free(DevMesh* m);
+// Builds the Navier-Stokes diffusion stencil (dsf*, dse*, max_dsf, max_dse, dstencil_ok)
+// on first use; later calls return at once.
+int ensure_diffusion_stencil(DevMesh* m);
 
 // Geometry kernels (mesh_geometry_module.F90:16-57), launched on m.stream.
 // sc (optional): a step whose skip flag is set leaves everything untouched; with sol6

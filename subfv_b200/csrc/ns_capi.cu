@@ -199,6 +199,10 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
   }
   if (s->P.diff) {
     // periodic nodes use the union stencil of their images (mesh_dev.cuh)
+    if (ensure_diffusion_stencil(&d)) {
+      subfv_ns_state_destroy(s);
+      return -1;
+    }
     const size_t smem = diffusion_smem_bytes(d);
     if (!d.dstencil_ok || smem > 200 * 1024 || d.max_dsf > 32) {
       set_error(!d.dstencil_ok ? "subfv_ns: a periodic node's diffusion stencil is incomplete"

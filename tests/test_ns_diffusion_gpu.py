@@ -142,3 +142,26 @@ def test_states_of_different_meshes_coexist(native, oracle_lib, cuda_ok):
     np.testing.assert_array_equal(big.sol(), sol_o)
     big.close()
     small.close()
+
+
+def test_stencil_built_on_first_diffusion_state(native, oracle_lib, cuda_ok):
+    """A mesh holds no diffusion stencil until a state with the diffusion terms asks for
+    it; a second such state reuses it, and the residual is the oracle's either way."""
+    from subfv_b200.ns import NsState, compute_rhs_ns_diag
+    raw = _raws()["box_periodic"]
+    m, o = _pair(raw)
+    before = m.device_bytes
+    NsState(m, _cfg("box_periodic", "neumann", activate_diffusion=False), _state(m.n_elems)).close()
+    assert m.device_bytes == before  # an inviscid state builds nothing on the mesh
+    cfg = _cfg("box_periodic", "neumann")
+    sol = _state(m.n_elems)
+    st, rhs, sl, diag = compute_rhs_ns_diag(m, cfg, sol)
+    grown = m.device_bytes
+    assert grown > before
+    st2, rhs2, _, diag2 = compute_rhs_ns_diag(m, cfg, sol)
+    assert m.device_bytes == grown
+    np.testing.assert_array_equal(rhs, rhs2)
+    np.testing.assert_array_equal(diag, diag2)
+    st_o, rhs_o, sl_o, diag_o = o.ns_rhs_diag(cfg.oracle_dict(), sol)
+    assert st == st_o == 0
+    np.testing.assert_array_equal(rhs, rhs_o)
