@@ -698,7 +698,9 @@ int gmres_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, dou
   double rho = device_norm2(A, W, W.r, n);
   if (rho < 0.0) return -1;
   int it = 0;
-  if (rho < tol) {
+  // A zero residual is solved by x = 0 whatever tol is; the reference, given tol = 0 (a
+  // relative tolerance on b = 0), would divide the residual by its zero norm
+  if (rho < tol || rho == 0.0) {
     st->conv = 1;
     st->rho = rho;
     st->restarts = 0;
@@ -787,7 +789,7 @@ int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double*
   double rn = bnorm;
   int outer = 0;
   for (outer = 1; outer <= max_outer; ++outer) {
-    if (rn < rel_tol * bnorm) {
+    if (rn < rel_tol * bnorm || rn == 0.0) {
       st->conv = 1;
       break;
     }
@@ -800,7 +802,7 @@ int gmres_refine_device(const DevBcsr& A, GmresWork& W, double* x, const double*
     rn = device_norm2(A, W, W.rr, n);
     if (rn < 0.0) return -1;
   }
-  if (!st->conv && rn < rel_tol * bnorm) st->conv = 1;
+  if (!st->conv && (rn < rel_tol * bnorm || rn == 0.0)) st->conv = 1;
   st->outer = outer - (st->conv ? 1 : 0);
   st->rho = rn;
   SUBFV_CUDA(cudaGetLastError());
@@ -845,7 +847,8 @@ int pcg_device(const DevBcsr& A, GmresWork& W, double* x, const double* b, doubl
   launch_pivot_diag(A, r, mr, flag);
   double rdr = device_dot(A, W, mr, r, n);
   st->res = std::sqrt(rdr);
-  const bool done0 = std::sqrt(rdr) < tol;
+  // a zero residual is already solved (the recurrence would divide 0 by 0 with tol = 0)
+  const bool done0 = std::sqrt(rdr) < tol || (rdr == 0.0 && device_norm2(A, W, r, n) == 0.0);
   if (!done0) SUBFV_CUDA(cudaMemcpyAsync(p, mr, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
   for (long k = 1; k <= n && !done0; ++k) {
     st->iters = (int)k;

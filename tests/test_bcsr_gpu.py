@@ -166,3 +166,26 @@ def test_pcgm_matches_oracle(native, oracle_lib, cuda_ok, bs):
     assert st == sto == 0 and it == ito
     assert np.abs(x - xo).max() <= 1e-9 * np.abs(xo).max()
     assert np.linalg.norm(b - _dense(A) @ x) <= 1.01 * tol
+
+
+def test_zero_right_hand_side_is_solved_by_zero(native, cuda_ok):
+    """b = 0: every Krylov entry returns x = 0, converged, without an Arnoldi cycle, also
+    at tol = 0 (a relative tolerance on b = 0), where the reference's recurrences would
+    divide the zero residual by its zero norm; PCG from x0 = 0 likewise."""
+    from subfv_b200.bcsr import DeviceBcsr, greedy_colors, grid_matrix
+    A = grid_matrix(4, 4, 3, bs=5, stencil=27, seed=13)
+    d = DeviceBcsr(A)
+    d.set_colors(*greedy_colors(A))
+    b = np.zeros(d.n)
+    for tol in (0.0, 1e-10):
+        for pc in (True, False):
+            x, conv, it, rho = d.gmres(b, tol, 30, precond=pc)
+            assert conv and it == 0 and rho == 0.0 and not x.any(), (tol, pc)
+        x, conv, it, rho = d.gmres_lusgs(b, tol)
+        assert conv and it == 0 and not x.any()
+    x, conv, outer, rho = d.gmres_refine(b, rel_tol=1e-8)
+    assert conv and not x.any() and np.isfinite(rho)
+    S = DeviceBcsr(_spd(3, 3, 2, 5, 41))
+    for tol in (0.0, 1e-10):
+        x, it, st, res = S.pcgm(np.zeros(S.n), tol)
+        assert st == 0 and it == 0 and res == 0.0 and not x.any()
