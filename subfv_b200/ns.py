@@ -123,6 +123,38 @@ def init_gresho(mesh: Mesh, mach: float) -> np.ndarray:
     return sol
 
 
+GRESHO_MACHS = (1.0e-1, 1.0e-2, 1.0e-3, 1.0e-4)
+
+
+def gresho_convergence(mesh: Mesh, cfg: "NsConfig", machs=GRESHO_MACHS, tmax: float = 1e-2, cfl: float = 0.9,
+                       n_max_iter: int = 100000, chunk: int = 256):
+    """The loop of subfvgreshoconv (src/ns/ns_gresho_convergence_main.F90:42-127): for
+    each Mach number, the Gresho vortex of sol_gresho_mach at the cell centroids, run
+    with the configuration's scheme (global time step, CFL `cfl`) until t reaches `tmax`
+    (or `n_max_iter` iterations), then the density fluctuation
+    L2_rho = sqrt(sum_c V_c (rho_c - 1)^2). The iterations run on the device-resident
+    loop (NsState). Returns the rows of the reference's convergence.dat: a list of
+    (mach, L2_rho, t_final, n_iter, status)."""
+    from dataclasses import replace
+    c = replace(cfg, cfl=float(cfl), tmax=float(tmax), local_time_step=False)
+    vol = mesh.geometry("elem_volume")
+    rows = []
+    for mach in machs:
+        sol0 = init_gresho(mesh, float(mach))
+        s = NsState(mesh, c, sol0)
+        n, t, st = 0, 0.0, 0
+        while n < n_max_iter:
+            st, n_now, t = s.advance(min(chunk, n_max_iter - n))
+            if st or n_now == n:
+                break
+            n = n_now
+        sol = s.sol()
+        s.close()
+        l2 = float(np.sqrt(np.sum(vol * (sol[:, 0] - 1.0) ** 2)))
+        rows.append((float(mach), l2, float(t), int(n), int(st)))
+    return rows
+
+
 def init_fourier_flow(mesh: Mesh, mach=0.3, n_modes=8, amp=0.05, seed=0, gamma=1.4) -> np.ndarray:
     """Uniform flow along x at Mach `mach` (rho = 1, |u| = 1) plus `n_modes` seeded
     divergence-free Fourier modes of velocity with relative amplitude `amp`, periodic on

@@ -228,3 +228,27 @@ def test_node_group_kernel_bitwise(native, cuda_ok, cfg_name):
     for other in res[1:]:
         for a, c in zip(res[0], other):
             np.testing.assert_array_equal(a, c)
+
+
+def test_empty_batch_advances_and_then_admits(native, cuda_ok):
+    """An empty batch (none admitted yet, or all removed) advances without error and
+    without touching anything; a problem admitted afterwards still gets its solo result."""
+    from subfv_b200.ns import NsBatch, NsConfig
+    cfg = NsConfig(**CFGS["mp_o1_fp32"], boundary_2d=True, cfl=0.4)
+    m, sol, tmax = _setup()[0]
+    b = NsBatch(cfg, capacity=2, budget_bytes=1 << 34)
+    b.advance(7)
+    b.sync()
+    k = b.add(m, sol, tmax)
+    assert k is not None
+    b.advance(9)
+    b.sync()
+    t, steps, done, st = b.info(k)
+    got = b.sol(k, m.n_elems)
+    b.remove(k)
+    b.advance(5)  # empty again
+    b.sync()
+    st0, steps0, t0, ref = _solo(m, cfg, sol, tmax, 9)
+    assert st == st0 == 0 and steps == steps0 == 9 and t == t0
+    np.testing.assert_array_equal(got, ref)
+    b.close()

@@ -103,3 +103,28 @@ def test_lag_batch_join_leave_and_grid(native, cuda_ok):
         np.testing.assert_array_equal(got, ref)
         np.testing.assert_array_equal(x, xref)
     b.close()
+
+
+def test_empty_lag_batch_advances_and_then_admits(native, cuda_ok):
+    """An empty Lagrangian batch advances without error; a problem admitted afterwards
+    ends with its solo state, and the batch can be emptied and advanced again."""
+    from subfv_b200.lagrange import LagBatch
+    raw, cfl, t_max = _cases()[0]
+    b = LagBatch(capacity=2, budget_bytes=1 << 34)
+    b.advance(4)
+    b.sync()
+    m, sol = _problem(raw)
+    k = b.add(m, sol, t_max, cfl=cfl)
+    assert k is not None
+    b.advance(11)
+    b.sync()
+    t, steps, done, st = b.info(k)
+    got, x = b.sol(k, m.n_elems), m.coords()
+    b.remove(k)
+    b.advance(3)
+    b.sync()
+    st0, steps0, t0, ref, x0 = _solo(raw, cfl, t_max, 11, 0)
+    assert st == st0 == 0 and steps == steps0 and t == t0
+    np.testing.assert_array_equal(got, ref)
+    np.testing.assert_array_equal(x, x0)
+    b.close()
