@@ -105,6 +105,10 @@ __device__ inline void face_geom_body(const DevMesh& m, const int f) {
 // on its norm. Every face vertex must be a vertex of the cell (no periodic faces);
 // otherwise the cell reports SUBFV_ERR_INDEX.
 constexpr int kGeoMaxV = 8, kGeoMaxF = 8, kGeoBlock = 64;
+// faces of a cell the step kernel stages (hexahedra have 6, prisms and pyramids 5,
+// tetrahedra 4): with a face-centroid cache of 6 rather than 8 slots the kernel's shared
+// memory no longer limits it below the 9 blocks its registers allow
+constexpr int kGeoCellFaces = 6;
 
 // gface[8 c + j], face slot j of cell c (ef8 order): bits 3k..3k+2 the local index (in
 // the cell's vertex order) of the face's k-th vertex, bit 12 quadrilateral, bit 13 the
@@ -201,7 +205,7 @@ __device__ inline unsigned gface_code(const unsigned (&gw)[4], const int j) {
 __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const double* rhs6, const double dt,
                                       const int c) {
   __shared__ double sX[kGeoMaxV][3][kGeoBlock];
-  __shared__ double sCF[kGeoMaxF][3][kGeoBlock];
+  __shared__ double sCF[kGeoCellFaces][3][kGeoBlock];
   const int t = threadIdx.x;
   if (c >= m.ne) return;
   const int vb = m.ev_off[c], nvc = m.ev_off[c + 1] - vb;
@@ -218,6 +222,10 @@ __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const doub
 #pragma unroll
   for (int j = 0; j < kGeoMaxF; ++j)
     if (fid[j] >= 0 && nfc == j) nfc = j + 1;
+  if (nfc > kGeoCellFaces) {
+    atomicOr(m.status, kErrIndex);
+    return;
+  }
   // Every global load of the cell first: vertex coordinates, then per face its
   // centroid, normal and subface sum (the check terms are formed as they arrive, in face
   // order), then the subcells' codes. What follows reads shared memory and registers.
@@ -233,7 +241,7 @@ __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const doub
   V3 nt = {0.0, 0.0, 0.0}, ns = {0.0, 0.0, 0.0};
   bool valid = true;
 #pragma unroll
-  for (int j = 0; j < kGeoMaxF; ++j)
+  for (int j = 0; j < kGeoCellFaces; ++j)
     if (j < nfc) {
       const int f = fid[j];
       const unsigned code = gface_code(gw, j);
