@@ -379,7 +379,9 @@ void devmesh_free(DevMesh* m) {
                   m->se_sf, m->vol_se, m->ev_off, m->ev, m->ef8, m->ekind, m->cc, m->vol, m->vsf_off,
                   m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
                   m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS, m->fpos, m->gface, m->gsub, m->forder, m->vorder,
-                  m->dsf_off, m->dsf, m->dsf_se, m->dsf_seloc, m->dse_off, m->dse, m->dse_sfloc};
+                  m->dsf_off, m->dsf, m->dsf_se, m->dsf_seloc, m->dse_off, m->dse, m->dse_sfloc,
+                  m->dcache, m->dcache_off};
+  diffusion_cache_forget(m);
   // stream-ordered frees: they wait for the mesh stream's work but not for other
   // streams (a caller that used the mesh elsewhere orders that work first)
   for (void* p : ptrs)

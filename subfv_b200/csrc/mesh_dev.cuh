@@ -89,6 +89,13 @@ struct DevMesh {
   int max_dsf = 0, max_dse = 0;
   int dstencil_ok = 1;     // every stencil subface's subcells and subcell's subfaces found
   int dstencil_built = 0;  // the d* arrays exist (ensure_diffusion_stencil)
+  // With a constant viscosity the diffusion systems of a vertex depend on the mesh and
+  // the diffusion constants only: their inverse and products, computed once, are kept
+  // here (per vertex at dcache_off[v] doubles), for the constants in dcache_key (a host
+  // object; ns_diffusion.cu). Null when not built.
+  double* dcache = nullptr;
+  long long* dcache_off = nullptr;
+  void* dcache_key = nullptr;
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;
@@ -133,6 +140,8 @@ void devmesh_free(DevMesh* m);
 // Builds the Navier-Stokes diffusion stencil (dsf*, dse*, max_dsf, max_dse, dstencil_ok)
 // on first use; later calls return at once.
 int ensure_diffusion_stencil(DevMesh* m);
+// releases the host side of the diffusion cache (the device arrays go with the mesh's)
+void diffusion_cache_forget(DevMesh* m);
 
 // Geometry kernels (mesh_geometry_module.F90:16-57), launched on m.stream.
 // sc (optional): a step whose skip flag is set leaves everything untouched; with sol6

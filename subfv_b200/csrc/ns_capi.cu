@@ -229,6 +229,10 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
   launch_ns_pack(d, s->stage, s->U0);
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
   SUBFV_CUDA(cudaGetLastError());
+  if (s->P.diff && diffusion_cache_build(&d, s->D, s->U0, s->dterm, s->mu0c)) {
+    subfv_ns_state_destroy(s);
+    return -1;
+  }
   *out = s;
   return 0;
 }

@@ -4,6 +4,8 @@
 // a matrix product, solve or inverse is produced by one lane in the order the reference
 // (netlib LAPACK / BLAS) accumulates it, so the results are those of the serial code.
 #include <algorithm>
+#include <cstring>
+#include <vector>
 
 #include "ns.cuh"
 #include "ns_diffusion.cuh"
@@ -445,8 +447,37 @@ __device__ inline void neumann_block(double al, double ap, double vol, const dou
     }
 }
 
+// Where a vertex's invariant diffusion arrays sit in the cache (constant viscosity): S
+// (F x E), B (F), N^-1 (F x F), SNS (E x E), SB (E), the per-subcell sums of St (9 per
+// subcell, blc3's numerators), then the heat system's SNS (ne x ne), SB (ne) and b1 (ne).
+struct DiffCacheView {
+  double *S, *B, *Ninv, *SNS, *SB, *Spc, *SNSh, *SBh, *b1;
+};
+__host__ __device__ inline long long diff_cache_doubles(int nf, int ne) {
+  const long long F = 3 * nf, E = 3 * ne;
+  return F * E + F + F * F + E * E + E + 3 * E + (long long)ne * ne + 2LL * ne;
+}
+__device__ inline DiffCacheView diff_cache_view(double* c, int nf, int ne) {
+  const int F = 3 * nf, E = 3 * ne;
+  DiffCacheView w;
+  w.S = c;
+  w.B = w.S + (size_t)F * E;
+  w.Ninv = w.B + F;
+  w.SNS = w.Ninv + (size_t)F * F;
+  w.SB = w.SNS + (size_t)E * E;
+  w.Spc = w.SB + E;
+  w.SNSh = w.Spc + 3 * E;
+  w.SBh = w.SNSh + (size_t)ne * ne;
+  w.b1 = w.SBh + ne;
+  return w;
+}
+
+// FILL: the same computation, which also stores the state-independent arrays of each
+// vertex in the cache (only with a constant viscosity, where they do not depend on U)
+template <bool FILL>
 __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, const double* __restrict__ U,
-                                                     double* __restrict__ dterm, const double* __restrict__ mu0c_p) {
+                                                     double* __restrict__ dterm, const double* __restrict__ mu0c_p,
+                                                     double* __restrict__ cache, const long long* __restrict__ coff) {
   extern __shared__ double sm[];
   const DiffSmem L = diff_layout(m.max_dsf, m.max_dse);
   const int lane = threadIdx.x;
@@ -459,6 +490,8 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     const int f0 = m.dsf_off[v], nf = m.dsf_off[v + 1] - f0;
     const int s0 = m.dse_off[v], ne = m.dse_off[v + 1] - s0;
     const int F = 3 * nf, E = 3 * ne;
+    DiffCacheView cw{};
+    if (FILL) cw = diff_cache_view(cache + coff[v], nf, ne);
     // ---- momentum: build_momentum_diff_nodal_system (:7-193)
     for (int e = lane; e < F * F; e += 32) N[e] = 0.0;
     for (int e = lane; e < F * E; e += 32) S[e] = St[e] = 0.0;
@@ -534,12 +567,21 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
           for (int j = 0; j < 3; ++j) Spc[i][j] = Spc[i][j] + St[(3 * l + i) + E * (3 * c + j)];
       for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) blc3[9 * l + i + 3 * j] = Spc[j][i] / u[0];
+      if (FILL)
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) cw.Spc[9 * l + i + 3 * j] = Spc[j][i];
+    }
+    if (FILL) {
+      for (int e = lane; e < F * E; e += 32) cw.S[e] = S[e];
+      for (int e = lane; e < F; e += 32) cw.B[e] = B[e];
     }
     __syncwarp();
     warp_gemv(F, E, S, Ve, Vf, lane);
     for (int i = lane; i < F; i += 32) Vf[i] = Vf[i] + B[i];
     __syncwarp();
     warp_inverse(N, F, ipiv, tmp, lane);  // tmp and work (adjacent, 2 F) as its scratch
+    if (FILL)
+      for (int e = lane; e < F * F; e += 32) cw.Ninv[e] = N[e];
     // the products of the reference, the two with N^-1 as a vector first, then
     // T1 = St N^-1 over N and SNS = T1 S over S (each product's own arithmetic unchanged)
     warp_gemv2(F, F, N, B, Vf, tmp, work, lane);  // N^-1 B, and N^-1 (S Ve + B): the face velocities
@@ -549,6 +591,10 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
     const double* SNSm = S;
     warp_gemv(E, F, St, tmp, SB, lane);
     warp_gemv(E, E, SNSm, Ve, SNSVe, lane);
+    if (FILL) {
+      for (int e = lane; e < E * E; e += 32) cw.SNS[e] = SNSm[e];
+      for (int e = lane; e < E; e += 32) cw.SB[e] = SB[e];
+    }
     for (int l = lane; l < ne; l += 32) {
       const int se = m.dse[s0 + l];
       if (m.se_vert[se] != v) continue;  // a periodic image's subcell: its own vertex writes it
@@ -669,6 +715,13 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
       b1[l] = s;
     }
     __syncwarp();
+    if (FILL) {
+      for (int e = lane; e < ne * ne; e += 32) cw.SNSh[e] = SNSm[e];
+      for (int e = lane; e < ne; e += 32) {
+        cw.SBh[e] = SB[e];
+        cw.b1[e] = b1[e];
+      }
+    }
     for (int l = lane; l < ne; l += 32) {
       const int se = m.dse[s0 + l];
       if (m.se_vert[se] != v) continue;
@@ -684,6 +737,144 @@ __global__ void __launch_bounds__(32) k_ns_diffusion(DevMesh m, DiffParams D, co
       t[37] = cc * pu;
       t[38] = b1[l] * theta[l];
       t[39] = SB[l];
+    }
+    __syncwarp();
+  }
+}
+
+// The corner records from the cache (constant viscosity): the state-dependent part of
+// k_ns_diffusion only, with the same operations in the same order on the same stored
+// values, so the records are bit-identical to the full kernel's. A warp per vertex,
+// kDiffWarps per block; the matrices are read from the cache with the rows on the lanes.
+constexpr int kDiffWarps = 4;
+__global__ void __launch_bounds__(32 * kDiffWarps) k_ns_diffusion_cached(DevMesh m, DiffParams D,
+                                                                         const double* __restrict__ U,
+                                                                         double* __restrict__ dterm,
+                                                                         const double* __restrict__ cache,
+                                                                         const long long* __restrict__ coff) {
+  extern __shared__ double smc[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int MF = 3 * m.max_dsf, ME = 3 * m.max_dse;
+  double* base = smc + (size_t)wid * (2 * MF + 7 * ME);
+  double *Vf = base, *work = Vf + MF, *Ve = work + MF, *SNSVe = Ve + ME, *blc3 = SNSVe + ME;
+  double *theta = blc3 + 3 * ME, *P = theta + ME / 3;
+  for (int v = blockIdx.x * kDiffWarps + wid; v < m.nv; v += gridDim.x * kDiffWarps) {
+    const int f0 = m.dsf_off[v], nf = m.dsf_off[v + 1] - f0;
+    const int s0 = m.dse_off[v], ne = m.dse_off[v + 1] - s0;
+    const int F = 3 * nf, E = 3 * ne;
+    const DiffCacheView c = diff_cache_view(const_cast<double*>(cache) + coff[v], nf, ne);
+    (void)f0;
+    for (int l = lane; l < ne; l += 32) {
+      double u[5];
+      load_u(U, m.se_elem[m.dse[s0 + l]], u);
+      for (int k = 0; k < 3; ++k) Ve[3 * l + k] = u[1 + k] / u[0];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) blc3[9 * l + i + 3 * j] = c.Spc[9 * l + i + 3 * j] / u[0];
+    }
+    __syncwarp();
+    for (int i = lane; i < F; i += 32) {  // S Ve + B
+      double s = 0.0;
+      for (int j = 0; j < E; ++j) s = s + Ve[j] * c.S[i + F * j];
+      Vf[i] = s;
+    }
+    __syncwarp();
+    for (int i = lane; i < F; i += 32) Vf[i] = Vf[i] + c.B[i];
+    __syncwarp();
+    for (int i = lane; i < F; i += 32) {  // N^-1 (S Ve + B): the face velocities
+      double s = 0.0;
+      for (int j = 0; j < F; ++j) s = s + Vf[j] * c.Ninv[i + F * j];
+      work[i] = s;
+    }
+    for (int i = lane; i < E; i += 32) {  // SNS Ve
+      double s = 0.0;
+      for (int j = 0; j < E; ++j) s = s + Ve[j] * c.SNS[i + E * j];
+      SNSVe[i] = s;
+    }
+    __syncwarp();
+    const double* SNSm = c.SNS;
+    const double* SB = c.SB;
+    for (int l = lane; l < ne; l += 32) {
+      const int se = m.dse[s0 + l];
+      if (m.se_vert[se] != v) continue;  // a periodic image's subcell: its own vertex writes it
+      double u[5];
+      load_u(U, m.se_elem[se], u);
+      double* t = dterm + (size_t)D.kd * se;
+      const int4 ql = m.dse_sfloc[s0 + l];
+      for (int i = 0; i < 3; ++i) {
+        double mv = 0.0;
+        for (int k = 0; k < 3; ++k) mv = mv + SNSm[(3 * l + i) + E * (3 * l + k)] * Ve[3 * l + k];
+        t[3 * i] = SNSVe[3 * l + i];
+        t[3 * i + 1] = mv;
+        t[3 * i + 2] = SB[3 * l + i];
+      }
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+          t[9 + 2 * (i + 3 * j)] = SNSm[(3 * l + i) + E * (3 * l + j)] / u[0];
+          t[10 + 2 * (i + 3 * j)] = blc3[9 * l + i + 3 * j];
+        }
+      // viscous work (:285-313)
+      const int4 q4 = m.se_sf[se];
+      const int nsf = n_sub_faces(q4);
+      double Spc[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+      for (int k = 0; k < nsf; ++k) {
+        const int sf = sf_of(q4, k);
+        double nl[3];
+        const double a = oriented(m, sf, se, nl);
+        const int q = 3 * sf_of(ql, k);
+        double vm[3];
+        for (int d = 0; d < 3; ++d) vm[d] = work[q + d] - Ve[3 * l + d];
+        const double dd = vm[0] * nl[0] + vm[1] * nl[1] + vm[2] * nl[2];
+        for (int i = 0; i < 3; ++i)
+          for (int j = 0; j < 3; ++j) {
+            const double e = i == j ? 1.0 : 0.0;
+            Spc[i][j] = Spc[i][j] + a * ((vm[i] * nl[j] + vm[j] * nl[i]) - (2.0 / 3.0) * dd * e);
+          }
+      }
+      const double mue = mu_of(D, u), vse = m.vol_se[se];
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Spc[i][j] = Spc[i][j] * mue / vse;
+      for (int k = 0; k < 4; ++k) t[27 + k] = 0.0;
+      for (int k = 0; k < nsf; ++k) {
+        const int sf = sf_of(q4, k);
+        double nl[3];
+        const double a = oriented(m, sf, se, nl);
+        const int q = 3 * sf_of(ql, k);
+        double sv[3];
+        for (int i = 0; i < 3; ++i) {
+          double s = 0.0;
+          for (int cc = 0; cc < 3; ++cc) s = s + Spc[i][cc] * work[q + cc];
+          sv[i] = s;
+        }
+        t[27 + k] = a * (sv[0] * nl[0] + sv[1] * nl[1] + sv[2] * nl[2]);
+      }
+    }
+    __syncwarp();
+    // ---- heat
+    for (int l = lane; l < ne; l += 32) {
+      double u[5];
+      load_u(U, m.se_elem[m.dse[s0 + l]], u);
+      theta[l] = temp_u(u, D.Cv_p);
+      const double nn = scaled_norm3(u[1] / u[0], u[2] / u[0], u[3] / u[0]);
+      P[5 * l] = (nn * nn - u[4] / u[0]) / (u[0] * D.Cv_p);
+      for (int k = 1; k < 4; ++k) P[5 * l + k] = -u[k] / ((u[0] * u[0]) * D.Cv_p);
+      P[5 * l + 4] = 1.0 / (u[0] * D.Cv_p);
+    }
+    __syncwarp();
+    for (int l = lane; l < ne; l += 32) {
+      const int se = m.dse[s0 + l];
+      if (m.se_vert[se] != v) continue;
+      double u[5];
+      load_u(U, m.se_elem[se], u);
+      double* t = dterm + (size_t)D.kd * se;
+      for (int p = 0; p < ne; ++p) t[kDiffHead + p] = c.SNSh[l + ne * p] * theta[p];
+      const double snl = c.SNSh[l + ne * l], cc = c.b1[l] - snl;
+      for (int k = 0; k < 5; ++k) t[31 + k] = cc * P[5 * l + k];
+      double pu = 0.0;
+      for (int k = 0; k < 5; ++k) pu = pu + P[5 * l + k] * u[k];
+      t[36] = snl * pu;
+      t[37] = cc * pu;
+      t[38] = c.b1[l] * theta[l];
+      t[39] = c.SBh[l];
     }
     __syncwarp();
   }
@@ -731,19 +922,93 @@ int diffusion_prepare(size_t smem) {
   // the attribute is per kernel: only ever raised, so every live state's launch fits
   static size_t granted = 0;
   if (smem > granted) {
-    SUBFV_CUDA(cudaFuncSetAttribute(k_ns_diffusion, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SUBFV_CUDA(cudaFuncSetAttribute(k_ns_diffusion<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    SUBFV_CUDA(cudaFuncSetAttribute(k_ns_diffusion<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     granted = smem;
   }
+  return 0;
+}
+
+namespace {
+// The constants the cached arrays depend on (besides the mesh): zero-filled, so that
+// whole objects compare bytewise.
+struct DiffCacheKey {
+  int sutherland;
+  int bcV[16], bcT[16];
+  double mu_p, Cv_p, prandtl;
+  double valV[16][3], valT[16];
+};
+DiffCacheKey cache_key_of(const DiffParams& D) {
+  DiffCacheKey k;
+  std::memset(&k, 0, sizeof k);
+  k.sutherland = D.sutherland;
+  for (int i = 0; i < 16; ++i) {
+    k.bcV[i] = D.bcV[i];
+    k.bcT[i] = D.bcT[i];
+    k.valT[i] = D.valT[i];
+    for (int c = 0; c < 3; ++c) k.valV[i][c] = D.valV[i][c];
+  }
+  k.mu_p = D.mu_p;
+  k.Cv_p = D.Cv_p;
+  k.prandtl = D.prandtl;
+  return k;
+}
+bool cache_matches(const DevMesh& m, const DiffParams& D) {
+  if (!m.dcache || !m.dcache_key || D.sutherland) return false;
+  const DiffCacheKey k = cache_key_of(D);
+  return std::memcmp(&k, m.dcache_key, sizeof k) == 0;
+}
+int grid_full(const DevMesh& m) { return std::max(1, std::min(m.nv, 148 * 32)); }
+}  // namespace
+
+void diffusion_cache_forget(DevMesh* m) {
+  delete static_cast<DiffCacheKey*>(m->dcache_key);
+  m->dcache_key = nullptr;
+}
+
+// Built once per mesh and never rewritten: a state whose step graph reads the cache keeps
+// its constants; a later state with other constants takes the full kernel.
+int diffusion_cache_build(DevMesh* m, const DiffParams& D, const double* U, double* dterm, double* mu0c) {
+  if (D.sutherland || m->dcache) return 0;
+  cudaStream_t s = m->stream;
+  {
+    std::vector<int> fo(m->nv + 1), so(m->nv + 1);
+    SUBFV_CUDA(cudaMemcpyAsync(fo.data(), m->dsf_off, fo.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    SUBFV_CUDA(cudaMemcpyAsync(so.data(), m->dse_off, so.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
+    SUBFV_CUDA(cudaStreamSynchronize(s));
+    std::vector<long long> off(m->nv + 1, 0);
+    for (int v = 0; v < m->nv; ++v) off[v + 1] = off[v] + diff_cache_doubles(fo[v + 1] - fo[v], so[v + 1] - so[v]);
+    const size_t bytes = sizeof(double) * (size_t)off[m->nv] + sizeof(long long) * off.size();
+    size_t free_b = 0, total_b = 0;
+    SUBFV_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    if (bytes > free_b / 2) return 0;  // no room to spare: every step recomputes them
+    SUBFV_CUDA(cudaMallocAsync((void**)&m->dcache, sizeof(double) * (size_t)off[m->nv], s));
+    SUBFV_CUDA(cudaMallocAsync((void**)&m->dcache_off, sizeof(long long) * off.size(), s));
+    SUBFV_CUDA(cudaMemcpyAsync(m->dcache_off, off.data(), sizeof(long long) * off.size(), cudaMemcpyHostToDevice, s));
+    SUBFV_CUDA(cudaStreamSynchronize(s));  // off goes out of scope
+    m->bytes += bytes;
+  }
+  k_diff_mu0c<<<1, 1, 0, s>>>(*m, D, U, mu0c, 1);
+  k_ns_diffusion<true><<<grid_full(*m), 32, diffusion_smem_bytes(*m), s>>>(*m, D, U, dterm, mu0c, m->dcache,
+                                                                            m->dcache_off);
+  SUBFV_CUDA(cudaGetLastError());
+  SUBFV_CUDA(cudaStreamSynchronize(s));
+  m->dcache_key = new DiffCacheKey(cache_key_of(D));
   return 0;
 }
 
 void launch_ns_diffusion(const DevMesh& m, const DiffParams& D, const double* U, double* dterm, double* mu0c) {
   k_diff_mu0c<<<1, 1, 0, m.stream>>>(m, D, U, mu0c, 1);
   if (D.sutherland) k_diff_mu0c<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, D, U, mu0c, 0);
-  const size_t smem = diffusion_smem_bytes(m);
+  if (cache_matches(m, D)) {
+    const size_t smem = sizeof(double) * kDiffWarps * (size_t)(2 * 3 * m.max_dsf + 7 * 3 * m.max_dse);
+    const int grid = std::max(1, std::min((m.nv + kDiffWarps - 1) / kDiffWarps, 148 * 16));
+    k_ns_diffusion_cached<<<grid, 32 * kDiffWarps, smem, m.stream>>>(m, D, U, dterm, m.dcache, m.dcache_off);
+    return;
+  }
   // a warp per vertex: as many warps as shared memory lets reside (up to 32 per SM)
-  const int grid = std::max(1, std::min(m.nv, 148 * 32));
-  k_ns_diffusion<<<grid, 32, smem, m.stream>>>(m, D, U, dterm, mu0c);
+  k_ns_diffusion<false><<<grid_full(m), 32, diffusion_smem_bytes(m), m.stream>>>(m, D, U, dterm, mu0c, nullptr,
+                                                                                 nullptr);
 }
 
 void launch_ns_diffusion_apply(const DevMesh& m, const double* dterm, int kd, double* rhs1, double* diag) {

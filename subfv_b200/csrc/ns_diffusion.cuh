@@ -39,8 +39,14 @@ DiffParams diff_params_from(const subfv_ns_cfg& c, const DevMesh& m);
 size_t diffusion_smem_bytes(const DevMesh& m);
 // lets the vertex kernel use smem bytes of dynamic shared memory
 int diffusion_prepare(size_t smem);
-// mu0corr (into *mu0c) and the corner records of state U
+// mu0corr (into *mu0c) and the corner records of state U; from the mesh's cache when it
+// holds the arrays for D's constants
 void launch_ns_diffusion(const DevMesh& m, const DiffParams& D, const double* U, double* dterm, double* mu0c);
+// With a constant viscosity, computes each vertex's state-independent diffusion arrays
+// once into the mesh's cache (also writing the corner records of U into dterm), unless
+// the mesh has a cache already (for any constants) or it would take more than half the
+// free device memory; at state creation, outside any stream capture.
+int diffusion_cache_build(DevMesh* m, const DiffParams& D, const double* U, double* dterm, double* mu0c);
 // rhs1 (kRhs records) += the diffusion terms; diag (25 per cell, column-major) = the
 // diffusion blocks (the residual entry point; the time loop applies them in place)
 void launch_ns_diffusion_apply(const DevMesh& m, const double* dterm, int kd, double* rhs1, double* diag);
