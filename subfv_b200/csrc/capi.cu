@@ -258,6 +258,7 @@ int subfv_mesh_set_coords(subfv_mesh* m, const double* c) {
   for (int i = 0; i < d.nv; ++i) x[i] = make_double4(c[3 * i], c[3 * i + 1], c[3 * i + 2], 0.0);
   SUBFV_CUDA(cudaMemcpyAsync(d.x, x.data(), x.size() * sizeof(double4), cudaMemcpyHostToDevice, d.stream));
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+  ++d.geom_epoch;
   return 0;
 }
 int subfv_mesh_get_coords(subfv_mesh* m, double* c) {
@@ -314,6 +315,7 @@ int subfv_mesh_get_geometry(subfv_mesh* m, const char* name, double* out) {
 
 int subfv_compute_geometry_mesh(subfv_mesh* m) {
   DevMesh& d = m->d;
+  ++d.geom_epoch;
   if (clear_status(d)) return -1;
   launch_geometry(d, 1);
   launch_vert_is_bound(d);
@@ -409,6 +411,7 @@ int subfv_compute_dt(subfv_mesh* m, const double* sol, double cfl, const double*
 
 int subfv_move_mesh(subfv_mesh* m, const double* vp, double dt) {
   DevMesh& d = m->d;
+  ++d.geom_epoch;
   if (ensure_scratch(m)) return -1;
   SUBFV_CUDA(cudaMemcpyAsync(m->stage, vp, 3 * (size_t)d.nv * sizeof(double), cudaMemcpyHostToDevice, d.stream));
   launch_vp_in(d, m->stage);
@@ -426,6 +429,7 @@ int subfv_lag_state_create(subfv_mesh* m, const double* sol, const double* mass,
     return -2;
   }
   DevMesh& d = m->d;
+  d.moving = 1;
   if (ensure_scratch(m)) return -1;
   auto* s = new subfv_lag_state();
   s->m = m;

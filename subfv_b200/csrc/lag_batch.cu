@@ -279,6 +279,7 @@ int subfv_lag_batch_add(subfv_lag_batch* b, subfv_mesh* m, int take_mesh, const 
     return -2;
   }
   if (handle_ensure_full_geometry(m->d) || handle_ensure_lag_arrays(m->d)) return -1;
+  m->d.moving = 1;
   const DevMesh& d = m->d;
   const int64_t need = state_bytes(d) + (int64_t)d.bytes;
   int k = -1;

@@ -96,6 +96,11 @@ struct DevMesh {
   double* dcache = nullptr;
   long long* dcache_off = nullptr;
   void* dcache_key = nullptr;
+  // Geometry changes the cache must see: geom_epoch counts host calls that move the
+  // vertices or recompute the geometry; moving is set once a Lagrangian state or batch
+  // owns the mesh (it then moves every step, and the cache is not used).
+  unsigned long long geom_epoch = 0;
+  int moving = 0;
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;

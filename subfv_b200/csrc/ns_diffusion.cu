@@ -953,25 +953,35 @@ DiffCacheKey cache_key_of(const DiffParams& D) {
   k.prandtl = D.prandtl;
   return k;
 }
+// the constants and the geometry epoch the cache was filled for
+struct DiffCacheMeta {
+  DiffCacheKey key;
+  unsigned long long epoch;
+};
 bool cache_matches(const DevMesh& m, const DiffParams& D) {
-  if (!m.dcache || !m.dcache_key || D.sutherland) return false;
+  if (!m.dcache || !m.dcache_key || D.sutherland || m.moving) return false;
+  const auto* meta = static_cast<const DiffCacheMeta*>(m.dcache_key);
   const DiffCacheKey k = cache_key_of(D);
-  return std::memcmp(&k, m.dcache_key, sizeof k) == 0;
+  return meta->epoch == m.geom_epoch && std::memcmp(&k, &meta->key, sizeof k) == 0;
 }
 int grid_full(const DevMesh& m) { return std::max(1, std::min(m.nv, 148 * 32)); }
 }  // namespace
 
 void diffusion_cache_forget(DevMesh* m) {
-  delete static_cast<DiffCacheKey*>(m->dcache_key);
+  delete static_cast<DiffCacheMeta*>(m->dcache_key);
   m->dcache_key = nullptr;
 }
 
-// Built once per mesh and never rewritten: a state whose step graph reads the cache keeps
-// its constants; a later state with other constants takes the full kernel.
+// Built once per mesh geometry and never rewritten for other constants: a state whose
+// step graph reads the cache keeps its constants, and a later state with other constants
+// takes the full kernel. After the geometry changed (a new epoch) the arrays are refilled
+// in place for the next state; a mesh that a Lagrangian state or batch moves has none.
 int diffusion_cache_build(DevMesh* m, const DiffParams& D, const double* U, double* dterm, double* mu0c) {
-  if (D.sutherland || m->dcache) return 0;
+  if (D.sutherland || m->moving) return 0;
+  if (m->dcache && m->dcache_key && static_cast<const DiffCacheMeta*>(m->dcache_key)->epoch == m->geom_epoch)
+    return 0;
   cudaStream_t s = m->stream;
-  {
+  if (!m->dcache) {
     std::vector<int> fo(m->nv + 1), so(m->nv + 1);
     SUBFV_CUDA(cudaMemcpyAsync(fo.data(), m->dsf_off, fo.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
     SUBFV_CUDA(cudaMemcpyAsync(so.data(), m->dse_off, so.size() * sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -988,12 +998,13 @@ int diffusion_cache_build(DevMesh* m, const DiffParams& D, const double* U, doub
     SUBFV_CUDA(cudaStreamSynchronize(s));  // off goes out of scope
     m->bytes += bytes;
   }
+  diffusion_cache_forget(m);  // invalid until refilled
   k_diff_mu0c<<<1, 1, 0, s>>>(*m, D, U, mu0c, 1);
   k_ns_diffusion<true><<<grid_full(*m), 32, diffusion_smem_bytes(*m), s>>>(*m, D, U, dterm, mu0c, m->dcache,
                                                                             m->dcache_off);
   SUBFV_CUDA(cudaGetLastError());
   SUBFV_CUDA(cudaStreamSynchronize(s));
-  m->dcache_key = new DiffCacheKey(cache_key_of(D));
+  m->dcache_key = new DiffCacheMeta{cache_key_of(D), m->geom_epoch};
   return 0;
 }
 

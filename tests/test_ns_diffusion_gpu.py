@@ -186,3 +186,38 @@ def test_cached_and_recomputed_paths_agree(native, oracle_lib, cuda_ok):
             np.testing.assert_array_equal(diag, diag_o, err_msg=f"{mesh_name} mu {mu}")
             sizes.append(m.device_bytes)
         assert sizes[0] == sizes[1] == sizes[2]  # one cache, built once
+
+
+def test_cache_follows_geometry_changes(native, oracle_lib, cuda_ok):
+    """The cached diffusion arrays belong to one geometry: after the vertices move
+    (subfv_mesh_set_coords, then subfv_compute_geometry_mesh) a new state refills them,
+    and its residual is the oracle's on the moved mesh."""
+    from dataclasses import replace as dc_replace
+    from oracle.oracle import OracleMesh
+    from subfv_b200.ns import compute_rhs_ns_diag
+    raw = _raws()["hex"]
+    m, o = _pair(raw)
+    cfg = _cfg("hex", "dirichlet")
+    sol = _state(m.n_elems)
+    st, rhs, _, diag = compute_rhs_ns_diag(m, cfg, sol)
+    st_o, rhs_o, _, diag_o = o.ns_rhs_diag(cfg.oracle_dict(), sol)
+    np.testing.assert_array_equal(rhs, rhs_o)
+    # move the interior vertices a little (the walls and the two z layers stay flat)
+    c = raw.coords.copy()
+    lo, hi = c.min(0), c.max(0)
+    inner = (c[:, 0] > lo[0] + 1e-9) & (c[:, 0] < hi[0] - 1e-9) & (c[:, 1] > lo[1] + 1e-9) & (c[:, 1] < hi[1] - 1e-9)
+    rng = np.random.default_rng(11)
+    shift = rng.uniform(-0.02, 0.02, (len(c), 2)) / NX
+    key = np.round(c[:, :2], 9)
+    _, col = np.unique(key, axis=0, return_inverse=True)  # the same shift on both layers of a column
+    c[inner, :2] += shift[col.ravel()][inner]
+    raw2 = dc_replace(raw, coords=c)
+    o2 = OracleMesh(raw2)
+    m.set_coords(o2.geom("vert_coord"))
+    assert m.compute_geometry_mesh() == 0
+    st2, rhs2, _, diag2 = compute_rhs_ns_diag(m, cfg, sol)
+    st2_o, rhs2_o, _, diag2_o = o2.ns_rhs_diag(cfg.oracle_dict(), sol)
+    assert st2 == st2_o == 0
+    assert not np.array_equal(rhs2_o, rhs_o)
+    np.testing.assert_array_equal(rhs2, rhs2_o)
+    np.testing.assert_array_equal(diag2, diag2_o)
