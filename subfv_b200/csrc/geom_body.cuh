@@ -82,10 +82,16 @@ __device__ inline void face_geom_body(const DevMesh& m, const int f) {
       const V3 b = cross(sub(cp, c), sub(cpp, c));
       const V3 nr = {0.5 * (a.x + b.x), 0.5 * (a.y + b.y), 0.5 * (a.z + b.z)};
       const double area = fnorm2_3(nr.x, nr.y, nr.z);
-      const V3 un = {nr.x / area, nr.y / area, nr.z / area};
-      if (FULL) m.sfn[sf] = make_double4(un.x, un.y, un.z, area);
+      if (FULL) {
+        const V3 un = {nr.x / area, nr.y / area, nr.z / area};
+        m.sfn[sf] = make_double4(un.x, un.y, un.z, area);
+        S = {S.x + area * un.x, S.y + area * un.y, S.z + area * un.z};
+      } else {
+        // the step keeps no unit normals: the closure sum takes the area vector itself
+        // (A n of the check, up to rounding), which only feeds check_mesh's threshold
+        S = {S.x + nr.x, S.y + nr.y, S.z + nr.z};
+      }
       m.sfa[sf] = area;
-      S = {S.x + area * un.x, S.y + area * un.y, S.z + area * un.z};
       fnrm = {fnrm.x + nr.x, fnrm.y + nr.y, fnrm.z + nr.z};
     }
   const double fa = fnorm2_3(fnrm.x, fnrm.y, fnrm.z);
