@@ -317,7 +317,9 @@ int subfv_ns_get_sol(subfv_ns_state* s, double* sol);
 /* Node kernel layout: 0 one thread per vertex (the default from 32,768 vertices up), 1 a
  * group of lanes per vertex (8, 16 or 32 as the mesh needs, one per subface) with the
  * per-vertex sums formed in shared memory (the default on smaller meshes); 8, 16 or 32:
- * a group of at least that many lanes. Results are bit-identical in every layout. */
+ * a group of at least that many lanes. With a group layout the second-order cell
+ * gradient also runs a group of 8 lanes per cell (one per vertex) when no cell has more
+ * than 8 vertices. Results are bit-identical in every layout. */
 int subfv_ns_state_set_node_kernel(subfv_ns_state* s, int lanes);
 /* res = sum of |delta|_2 and res_vect(5) of the last add_timedisc_and_solve call */
 int subfv_ns_residuals(subfv_ns_state* s, double* res, double* res_vect, double* dt);

@@ -223,6 +223,8 @@ int devmesh_create(const subfv_mesh_desc* d, DevMesh* m) {
   }
   std::vector<int> ev_off(ne + 1), ev(d->elem_vert_off[ne]), ef8(8 * (size_t)ne, -1), ekind(ne);
   for (int c = 0; c <= ne; ++c) ev_off[c] = d->elem_vert_off[c];
+  m->max_evc = 0;
+  for (int c = 0; c < ne; ++c) m->max_evc = std::max(m->max_evc, ev_off[c + 1] - ev_off[c]);
   for (int c = 0; c < ne; ++c) {
     ekind[c] = d->elem_kind ? d->elem_kind[c] : 0;
     for (int k = ev_off[c]; k < ev_off[c + 1]; ++k) {

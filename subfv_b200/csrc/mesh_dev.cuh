@@ -29,6 +29,7 @@ struct DevMesh {
   int b2d = 1;
   int vsf_identity = 0;  // vsf[p] == p for every p (no periodic extension)
   int max_vsf = 0, max_vse = 0;  // the most subfaces / subcells around one vertex
+  int max_evc = 0;               // the most vertices of one cell
   // vertices
   double4* x = nullptr;
   double4* vp = nullptr;

@@ -16,6 +16,8 @@
 //   k_ns_nodal_grad  one thread per vertex: least-squares gradient, 3x3 pseudo-inverse
 //   k_ns_cell_grad   one thread per cell: method-4 weighting, physical slope limiter,
 //                    relaxed maximum principle
+//   (on small meshes the node kernel and both gradients run a group of lanes per
+//   vertex or cell instead: k_ns_node_group, k_ns_nodal_grad_group, k_ns_cell_grad_group)
 // then per stage k_ns_timedisc (flux limiting blend, diagonal solve, positivity limiter,
 // residual partial sums), k_ns_finalize (one thread) and k_ns_apply.
 //
@@ -1307,6 +1309,80 @@ __global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* 
   ns_nodal_grad_body(m, U, ngrad, sc, vert_at(m, blockIdx.x * blockDim.x + threadIdx.x));
 }
 
+// The same nodal gradient with a group of NG lanes per vertex, lane p holding the
+// vertex's p-th subface (both cells' primitives, the 15 gradient and 9 matrix terms): the
+// sums run in subface order by shuffles, each lane forming the same totals and the same
+// pseudo-inverse, and the lanes share the stores. Every lane of the warp reaches every
+// shuffle.
+template <int NG>
+__device__ void ns_nodal_grad_group(const DevMesh& m, const double* __restrict__ U, double* __restrict__ ngrad,
+                                    const NsScalars* sc, const int t, const int lane) {
+  if (sc && sc->done) return;
+  constexpr unsigned kAll = 0xffffffffu;
+  const bool live = t < m.nv;
+  const int v = vert_at(m, t);
+  const int pb = live ? m.vsf_off[v] : 0, np = live ? m.vsf_off[v + 1] - pb : 0;
+  const int nmax = __reduce_max_sync(kAll, np);
+  double tg[15], tm[9];
+  for (int i = 0; i < 15; ++i) tg[i] = 0.0;
+  for (int i = 0; i < 9; ++i) tm[i] = 0.0;
+  int in = 0;
+  if (lane < np) {
+    const int sf = m.vsf[pb + lane];
+    const int2 lr = m.flr[m.sf_face[sf]];
+    if (lr.y >= 0) {
+      in = 1;
+      double ul[5], ur[5], wl[5], wr[5];
+      ld5(U, lr.x, ul);
+      ld5(U, lr.y, ur);
+      c2p(ul, wl);
+      c2p(ur, wr);
+      const double4 sn = m.sfn[sf];
+      const double n[3] = {sn.x, sn.y, sn.z};
+      const double4 cl = m.cc[lr.x], cr = m.cc[lr.y];
+      const double dxc[3] = {cr.x - cl.x, cr.y - cl.y, cr.z - cl.z};
+      for (int d = 0; d < 3; ++d)
+        for (int k = 0; k < 5; ++k) tg[5 * d + k] = sn.w * (n[d] * (wr[k] - wl[k]));
+      for (int d = 0; d < 3; ++d)
+        for (int e = 0; e < 3; ++e) tm[3 * d + e] = sn.w * (n[d] * dxc[e]);
+    }
+  }
+  double g[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
+  double mat[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  for (int j = 0; j < nmax; ++j) {
+    const bool add = __shfl_sync(kAll, in, j, NG) != 0;
+#pragma unroll
+    for (int i = 0; i < 15; ++i) {
+      const double x = __shfl_sync(kAll, tg[i], j, NG);
+      if (add) g[i / 5][i % 5] = g[i / 5][i % 5] + x;
+    }
+#pragma unroll
+    for (int i = 0; i < 9; ++i) {
+      const double x = __shfl_sync(kAll, tm[i], j, NG);
+      if (add) mat[i / 3][i % 3] = mat[i / 3][i % 3] + x;
+    }
+  }
+  if (!live) return;
+  pinv3(mat);
+  const bool bnd = m.is_bound[v] != 0;
+  double* o = ngrad + 15 * (size_t)v;
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+#pragma unroll
+    for (int k = 0; k < 5; ++k)
+      if ((5 * d + k) % NG == lane) {
+        double s = 0.0;
+        for (int e = 0; e < 3; ++e) s = s + mat[d][e] * g[e][k];
+        o[5 * d + k] = bnd ? 0.0 : s;
+      }
+}
+
+template <int NG>
+__global__ void __launch_bounds__(128) k_ns_nodal_grad_group(DevMesh m, const double* __restrict__ U,
+                                                             double* __restrict__ ngrad, const NsScalars* sc) {
+  ns_nodal_grad_group<NG>(m, U, ngrad, sc, blockIdx.x * (128 / NG) + threadIdx.x / NG, threadIdx.x % NG);
+}
+
 // compute_cell_grad_method_2..6 (:166-320) + physical_slope_limiter + relaxed_maximum_principle
 template <class T>
 __device__ void ns_cell_grad_body(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
@@ -1432,6 +1508,201 @@ __global__ void __launch_bounds__(128) k_ns_cell_grad(DevMesh m, NsParams P, con
                                                       const double* __restrict__ ngrad, double* __restrict__ grad,
                                                       const NsScalars* sc) {
   ns_cell_grad_body<T>(m, P, U, ngrad, grad, sc, blockIdx.x * blockDim.x + threadIdx.x);
+}
+
+// The same cell gradient with a group of kCellLanes lanes per cell, lane j holding the
+// cell's j-th vertex, for small meshes where a thread per cell leaves most SMs idle and
+// each cell's chain sets the kernel's length. Per-vertex terms (weights, their products,
+// the limiters' candidates, the neighbour states' primitives) are formed in parallel;
+// every sum is taken in vertex order by shuffles, each lane forming the same totals from
+// the same operands, so the sums have the thread-per-cell kernel's bits. The min / max
+// folds (tmin2, tmax2) run over each lane's own list from the initial value, then over
+// the lanes' results in vertex order: a fold keeps the first occurrence of its extreme
+// among the values strictly past the initial one and never takes a NaN, so the two-level
+// fold returns the single fold's bits. Every lane of the warp reaches every shuffle.
+template <class T>
+__device__ void ns_cell_grad_group(const DevMesh& m, const NsParams& P, const double* __restrict__ U,
+                                   const double* __restrict__ ngrad, double* __restrict__ grad,
+                                   const NsScalars* sc, const int c, const int lane) {
+  if (sc && sc->done) return;
+  const bool live = c < m.ne;
+  if (P.method == 0 || P.method == 1) {
+    if (live)
+      for (int i = lane; i < 15; i += kCellLanes) grad[15 * (size_t)c + i] = 0.0;
+    return;
+  }
+  constexpr unsigned kAll = 0xffffffffu;
+  const T eps = (T)1e-3, tol = (T)1e-8;
+  const int vb = live ? m.ev_off[c] : 0, nvc = live ? m.ev_off[c + 1] - vb : 0;
+  const int nmax = __reduce_max_sync(kAll, nvc);
+  const bool own = lane < nvc;
+  const int v = own ? m.ev[vb + lane] : 0;
+  T ng[15], vol = 0;
+  for (int i = 0; i < 15; ++i) ng[i] = 0;
+  if (own) {
+    const double* src = ngrad + 15 * (size_t)v;
+    for (int i = 0; i < 15; ++i) ng[i] = (T)src[i];
+    vol = (T)m.vol_v[v];
+  }
+  T g[15], ws[5] = {0, 0, 0, 0, 0};
+  for (int i = 0; i < 15; ++i) g[i] = 0;
+  if (P.method == 2) {  // dual-volume average
+    T t[15], dvs = 0;
+    for (int i = 0; i < 15; ++i) t[i] = vol * ng[i];
+    for (int j = 0; j < nmax; ++j) {
+      const bool in = j < nvc;
+      for (int i = 0; i < 15; ++i) {
+        const T x = __shfl_sync(kAll, t[i], j, kCellLanes);
+        if (in) g[i] = g[i] + x;
+      }
+      const T x = __shfl_sync(kAll, vol, j, kCellLanes);
+      if (in) dvs = dvs + x;
+    }
+    for (int i = 0; i < 15; ++i) g[i] = g[i] / dvs;
+  } else if (P.method == 3) {  // the vertex gradient of smallest norm, per variable
+    for (int k = 0; k < 5; ++k) {
+      const T o = oi3<T>(ng[k], ng[5 + k], ng[10 + k]);
+      T best = __shfl_sync(kAll, o, 0, kCellLanes);
+      int sel = 0;
+      for (int j = 1; j < nmax; ++j) {
+        const T x = __shfl_sync(kAll, o, j, kCellLanes);
+        if (j < nvc && x < best) {
+          best = x;
+          sel = j;
+        }
+      }
+      for (int d = 0; d < 3; ++d) g[5 * d + k] = __shfl_sync(kAll, ng[5 * d + k], sel, kCellLanes);
+    }
+  } else {  // 4: V / (eps + |g|); 5, 6: V / (eps + |g|)^2 (6 adds the central average)
+    T w[5], t[15];
+    for (int k = 0; k < 5; ++k) {
+      const T q = eps + oi3<T>(ng[k], ng[5 + k], ng[10 + k]);
+      w[k] = P.method == 4 ? vol / q : vol / (q * q);
+      for (int d = 0; d < 3; ++d) t[5 * d + k] = w[k] * ng[5 * d + k];
+    }
+    for (int j = 0; j < nmax; ++j) {
+      const bool in = j < nvc;
+      for (int i = 0; i < 15; ++i) {
+        const T x = __shfl_sync(kAll, t[i], j, kCellLanes);
+        if (in) g[i] = g[i] + x;
+      }
+      for (int k = 0; k < 5; ++k) {
+        const T x = __shfl_sync(kAll, w[k], j, kCellLanes);
+        if (in) ws[k] = ws[k] + x;
+      }
+    }
+    if (P.method == 6) {  // OI of the (3, 5) central gradient: the norm of its first column
+      T cg[15], cws = 0;
+      for (int i = 0; i < 15; ++i) {
+        cg[i] = 0;
+        t[i] = vol * ng[i];
+      }
+      for (int j = 0; j < nmax; ++j) {
+        const bool in = j < nvc;
+        for (int i = 0; i < 15; ++i) {
+          const T x = __shfl_sync(kAll, t[i], j, kCellLanes);
+          if (in) cg[i] = cg[i] + x;
+        }
+        const T x = __shfl_sync(kAll, vol, j, kCellLanes);
+        if (in) cws = cws + x;
+      }
+      for (int i = 0; i < 15; ++i) cg[i] = cg[i] / cws;
+      const T q = eps + oi3<T>(cg[0], cg[5], cg[10]);
+      const T wc = cws / (q * q);
+      for (int i = 0; i < 15; ++i) g[i] = g[i] + wc * cg[i];
+      for (int k = 0; k < 5; ++k) ws[k] = ws[k] + wc;
+    }
+    for (int k = 0; k < 5; ++k)
+      for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
+  }
+  T w0[5] = {0, 0, 0, 0, 0}, dx[3] = {0, 0, 0};
+  if (live) {
+    double u0[5];
+    ld5(U, c, u0);
+    T uu[5];
+    for (int k = 0; k < 5; ++k) uu[k] = (T)u0[k];
+    c2p(uu, w0);
+  }
+  if (own) {
+    const double4 ce = m.cc[c], xv = m.x[v];
+    dx[0] = (T)(xv.x - ce.x);
+    dx[1] = (T)(xv.y - ce.y);
+    dx[2] = (T)(xv.z - ce.z);
+  }
+  T om = 1;  // physical_slope_limiter: this lane's vertex
+  {
+    T dw0 = 0, dw4 = 0;
+    for (int d = 0; d < 3; ++d) dw0 = dw0 + g[5 * d] * dx[d];
+    for (int d = 0; d < 3; ++d) dw4 = dw4 + g[5 * d + 4] * dx[d];
+    if (dw0 < (T)0) om = tmin2(om, tmax2((T)0, w0[0] / (tol - dw0)));
+    if (dw4 < (T)0) om = tmin2(om, tmax2((T)0, w0[4] / (tol - dw4)));
+  }
+  T omega = 1;
+  for (int j = 0; j < nmax; ++j) {
+    const T x = __shfl_sync(kAll, om, j, kCellLanes);
+    if (j < nvc) omega = tmin2(omega, x);
+  }
+  for (int i = 0; i < 15; ++i) g[i] = omega * g[i];
+  T rmin = (T)1e100, rmax = 0, pmin = (T)1e100, pmax = 0;  // relaxed_maximum_principle
+  if (sizeof(T) == 4) rmin = pmin = (T)3.0e38f;
+  T lrmin = rmin, lrmax = rmax, lpmin = pmin, lpmax = pmax;
+  if (own)
+    for (int q = m.vel_off[v]; q < m.vel_off[v + 1]; ++q) {
+      double un[5];
+      ld5(U, m.vel[q], un);
+      T ut[5], w[5];
+      for (int k = 0; k < 5; ++k) ut[k] = (T)un[k];
+      c2p(ut, w);
+      lpmin = tmin2(lpmin, w[4]);
+      lpmax = tmax2(lpmax, w[4]);
+      lrmin = tmin2(lrmin, w[0]);
+      lrmax = tmax2(lrmax, w[0]);
+    }
+  for (int j = 0; j < nmax; ++j) {
+    const T a = __shfl_sync(kAll, lpmin, j, kCellLanes), b = __shfl_sync(kAll, lpmax, j, kCellLanes);
+    const T e = __shfl_sync(kAll, lrmin, j, kCellLanes), f = __shfl_sync(kAll, lrmax, j, kCellLanes);
+    if (j < nvc) {
+      pmin = tmin2(pmin, a);
+      pmax = tmax2(pmax, b);
+      rmin = tmin2(rmin, e);
+      rmax = tmax2(rmax, f);
+    }
+  }
+  pmin = ((T)1.0 - (T)1e-2) * pmin;
+  rmin = ((T)1.0 - (T)1e-2) * rmin;
+  pmax = ((T)1.0 + (T)1e-2) * pmax;
+  rmax = ((T)1.0 + (T)1e-2) * rmax;
+  om = 1;
+  {
+    T dw0 = 0, dw4 = 0;
+    for (int d = 0; d < 3; ++d) dw0 = dw0 + g[5 * d] * dx[d];
+    for (int d = 0; d < 3; ++d) dw4 = dw4 + g[5 * d + 4] * dx[d];
+    if (dw0 < (T)0)
+      om = tmin2(om, tmax2((T)0, (w0[0] - rmin) / (tol - dw0)));
+    else
+      om = tmin2(om, tmax2((T)0, -(w0[0] - rmax) / (tol + dw0)));
+    if (dw4 < (T)0)
+      om = tmin2(om, tmax2((T)0, (w0[4] - pmin) / (tol - dw4)));
+    else
+      om = tmin2(om, tmax2((T)0, -(w0[4] - pmax) / (tol + dw4)));
+  }
+  omega = 1;
+  for (int j = 0; j < nmax; ++j) {
+    const T x = __shfl_sync(kAll, om, j, kCellLanes);
+    if (j < nvc) omega = tmin2(omega, x);
+  }
+  if (live)
+#pragma unroll
+    for (int i = 0; i < 15; ++i)
+      if (i % kCellLanes == lane) grad[15 * (size_t)c + i] = (double)(omega * g[i]);
+}
+
+template <class T>
+__global__ void __launch_bounds__(128) k_ns_cell_grad_group(DevMesh m, NsParams P, const double* __restrict__ U,
+                                                            const double* __restrict__ ngrad,
+                                                            double* __restrict__ grad, const NsScalars* sc) {
+  const int c = blockIdx.x * (blockDim.x / kCellLanes) + threadIdx.x / kCellLanes;
+  ns_cell_grad_group<T>(m, P, U, ngrad, grad, sc, c, threadIdx.x % kCellLanes);
 }
 
 constexpr int kTdBlock = 128;
@@ -2177,17 +2448,48 @@ void launch_node(const DevMesh& m, const NsParams& P, const double* U, const dou
   else launch_node_tl<double, double>(m, P, U, grad, fs, so, sc);
 }
 
+// The nodal gradient: a group of 8, 16 or 32 lanes per vertex (the fewest that hold
+// every vertex's subfaces) along with the grouped node kernel, else a thread per vertex.
+void launch_nodal_grad(const DevMesh& m, const NsParams& P, const double* U, double* ngrad, const NsScalars* sc) {
+  const int k = m.max_vsf, ng = k <= 8 ? 8 : k <= 16 ? 16 : k <= 32 ? 32 : 0;
+  if (P.node_group && ng) {
+    const int g = grid_for(m.nv, 128 / ng);
+    if (ng == 8) k_ns_nodal_grad_group<8><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
+    else if (ng == 16) k_ns_nodal_grad_group<16><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
+    else k_ns_nodal_grad_group<32><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
+    return;
+  }
+  k_ns_nodal_grad<<<grid_for(m.nv, 128), 128, 0, m.stream>>>(m, U, ngrad, sc);
+}
+
+// The cell gradient: a group of kCellLanes lanes per cell along with the grouped node
+// kernel when every cell has at most kCellLanes vertices, else a thread per cell (same
+// results either way).
+void launch_cell_grad(const DevMesh& m, const NsParams& P, const double* U, const double* ngrad, double* grad,
+                      const NsScalars* sc) {
+  if (P.node_group && m.max_evc > 0 && m.max_evc <= kCellLanes) {
+    const int g = grid_for(m.ne, 128 / kCellLanes);
+    if (P.precision == 2)
+      k_ns_cell_grad_group<float><<<g, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+    else
+      k_ns_cell_grad_group<double><<<g, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+    return;
+  }
+  const int g = grid_for(m.ne, 128);
+  if (P.precision == 2)
+    k_ns_cell_grad<float><<<g, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+  else
+    k_ns_cell_grad<double><<<g, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+}
+
 void launch_ns_rhs(const DevMesh& m, const NsParams& P, const double* U, double* fs, double* rhs1, double* rhs2,
                    double* ngrad, double* grad, NsScalars* sc) {
-  const int gv = grid_for(m.nv, 128), gc = grid_for(m.ne, 128);
+  const int gc = grid_for(m.ne, 128);
   launch_node(m, P, U, grad, fs, 0, sc);
   k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs1, sc, sc ? 1 : 0);
   if (P.second_order) {
-    k_ns_nodal_grad<<<gv, 128, 0, m.stream>>>(m, U, ngrad, sc);
-    if (P.precision == 2)
-      k_ns_cell_grad<float><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
-    else
-      k_ns_cell_grad<double><<<gc, 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+    launch_nodal_grad(m, P, U, ngrad, sc);
+    launch_cell_grad(m, P, U, ngrad, grad, sc);
     launch_node(m, P, U, grad, fs, 1, sc);
     k_ns_gather<<<gc, 128, 0, m.stream>>>(m, fs, rhs2, sc, 0);
   }
@@ -2226,11 +2528,8 @@ void launch_ns_euler_flux(const DevMesh& m, const NsParams& P, const double* U, 
 // compute_cell_grad_from_nodal_grad (ns_euler_recon_module.F90:8-59)
 void launch_ns_cell_grads(const DevMesh& m, const NsParams& P, const double* U, double* ngrad, double* grad,
                           NsScalars* sc) {
-  k_ns_nodal_grad<<<grid_for(m.nv, 128), 128, 0, m.stream>>>(m, U, ngrad, sc);
-  if (P.precision == 2)
-    k_ns_cell_grad<float><<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
-  else
-    k_ns_cell_grad<double><<<grid_for(m.ne, 128), 128, 0, m.stream>>>(m, P, U, ngrad, grad, sc);
+  launch_nodal_grad(m, P, U, ngrad, sc);
+  launch_cell_grad(m, P, U, ngrad, grad, sc);
 }
 
 namespace {

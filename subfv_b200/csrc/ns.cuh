@@ -8,6 +8,7 @@ namespace subfv {
 
 constexpr int kNsMaxSf = 32;  // subfaces around a vertex (a 3-D hex vertex has 12)
 constexpr int kNsFs = 6;      // per-subcell record: five corner flux sums and the wave-speed sum
+constexpr int kCellLanes = 8;  // lanes per cell of the grouped cell gradient (cells of up to 8 vertices)
 
 struct NsParams {
   int scheme, second_order, method, bc_style, b2d, excl, lts, n_bc;
@@ -16,6 +17,8 @@ struct NsParams {
   double cfl, tmax;
   int precision;
   int node_group;  // 0: one thread per vertex; else a group of lanes per vertex, at least node_group
+                  // (and, on meshes whose cells have at most kCellLanes vertices, a group of
+                  // kCellLanes lanes per cell in the solo cell gradient)
   int diff, diff_kd;  // diffusion terms to apply in the time discretisation, doubles per corner record
 };
 

@@ -307,7 +307,9 @@ class NsState:
 
     def set_node_kernel(self, lanes: int):
         """0: one thread per vertex; 1: a group of lanes per vertex (8/16/32 as the mesh
-        needs); 8, 16, 32: a group of at least that many lanes. Same results in all."""
+        needs); 8, 16, 32: a group of at least that many lanes. A group layout also runs
+        the cell gradient with 8 lanes per cell (cells of up to 8 vertices). Same results
+        in all."""
         check(_lib.load().subfv_ns_state_set_node_kernel(self._h, int(lanes)), "subfv_ns_state_set_node_kernel")
 
     def residuals(self):

@@ -73,6 +73,34 @@ def test_compute_rhs_ns_bit_exact(native, oracle_lib, cuda_ok, mesh_name, cfg_na
     np.testing.assert_array_equal(grad.transpose(0, 2, 1).reshape(-1, 15), grad_o)
 
 
+@pytest.mark.parametrize("method", [2, 3, 4, 5, 6])
+def test_grouped_gradients_bitwise(native, cuda_ok, method):
+    """The cell gradient with a group of 8 lanes per cell (each vertex's terms on its own
+    lane, the sums in vertex order by shuffles, the min / max folds per lane and then over
+    the lanes in vertex order) and the nodal gradient with a group of 8 or 16 lanes per
+    vertex (a subface per lane, sums in subface order) give the thread kernels' states bit
+    for bit: FP64 and the FP32 level, hexahedral and prism slabs and a periodic hexahedral
+    box. set_node_kernel(0) selects a thread per vertex and per cell, 1 the lane groups."""
+    from subfv_b200 import meshgen
+    from subfv_b200.mesh import Mesh
+    from subfv_b200.ns import NsConfig, NsState, init_fourier_flow
+    cases = [(Mesh.from_raw(raw), True) for raw in _meshes().values()]
+    cases.append((Mesh.from_raw(meshgen.hex_box(5, jitter=0.05, seed=3, periodic=True)), False))
+    for m, b2d in cases:
+        sol = _perturbed_gresho(m, 9) if b2d else init_fourier_flow(m, seed=4)
+        for prec in (0, 2):
+            cfg = NsConfig(scheme=1, second_order=True, method=method, bc_style=2, boundary_2d=b2d, cfl=0.4,
+                           precision=prec, tmax=1e30)
+            out = []
+            for lanes in (0, 1):
+                s = NsState(m, cfg, sol)
+                s.set_node_kernel(lanes)
+                out.append((s.advance(6), s.sol()))
+                s.close()
+            assert out[0][0] == out[1][0] and out[0][0][0] == 0
+            np.testing.assert_array_equal(out[0][1], out[1][1])
+
+
 def test_gresho_init_matches_oracle(native, oracle_lib, cuda_ok):
     from subfv_b200.ns import init_gresho
     m, o = _pair(_meshes()["hex_slab"])
