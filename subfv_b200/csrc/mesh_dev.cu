@@ -382,7 +382,7 @@ void devmesh_free(DevMesh* m) {
                   m->vsf, m->p_node, m->vse_off, m->vse, m->csf_off, m->csf, m->status,
                   m->vel_off, m->vel, m->cse_sorted, m->frec, m->centry, m->fS, m->fpos, m->gface, m->gsub, m->forder, m->vorder,
                   m->dsf_off, m->dsf, m->dsf_se, m->dsf_seloc, m->dse_off, m->dse, m->dse_sfloc,
-                  m->dcache, m->dcache_off};
+                  m->dcache, m->dcache_off, m->npinv};
   diffusion_cache_forget(m);
   // stream-ordered frees: they wait for the mesh stream's work but not for other
   // streams (a caller that used the mesh elsewhere orders that work first)

@@ -102,6 +102,10 @@ struct DevMesh {
   // owns the mesh (it then moves every step, and the cache is not used).
   unsigned long long geom_epoch = 0;
   int moving = 0;
+  // The pseudo-inverse of each vertex's nodal-gradient matrix (9 doubles per vertex, row
+  // major), valid while npinv_epoch == geom_epoch (ensure_nodal_pinv in ns.cuh).
+  double* npinv = nullptr;
+  unsigned long long npinv_epoch = 0;
   // set when a Lagrangian step refreshed only the arrays the next step reads (face
   // normals and areas, subface areas, volumes); the rest is recomputed on demand
   int geom_partial = 0;

@@ -1268,7 +1268,41 @@ __global__ void __launch_bounds__(128) k_ns_gather(DevMesh m, const double* __re
   ns_gather_body(m, fs, rhs, sc, reduce, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-// compute_nodal_grad (ns_euler_recon_module.F90:453-490); ng[15] = g[5*d + var]
+// The matrix of compute_nodal_grad (ns_euler_recon_module.F90:453-490) at vertex v,
+// sum over its interior subfaces of A n (x_r - x_l)^T in subface order: it depends on
+// the geometry alone.
+__device__ inline void nodal_grad_matrix(const DevMesh& m, const int v, double mat[3][3]) {
+  for (int d = 0; d < 3; ++d)
+    for (int e = 0; e < 3; ++e) mat[d][e] = 0.0;
+  for (int p = m.vsf_off[v]; p < m.vsf_off[v + 1]; ++p) {
+    const int sf = m.vsf[p];
+    const int2 lr = m.flr[m.sf_face[sf]];
+    if (lr.y < 0) continue;
+    const double4 sn = m.sfn[sf];
+    const double n[3] = {sn.x, sn.y, sn.z};
+    const double4 cl = m.cc[lr.x], cr = m.cc[lr.y];
+    const double dxc[3] = {cr.x - cl.x, cr.y - cl.y, cr.z - cl.z};
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + sn.w * (n[d] * dxc[e]);
+  }
+}
+
+// The pseudo-inverse of every vertex's matrix, npinv[9 v + 3 d + e], for a mesh whose
+// geometry stays put between the steps that read it: the same sums and the same pinv3
+// as the per-step kernels, so a gradient formed from it has their bits.
+__global__ void __launch_bounds__(128) k_ns_nodal_pinv(DevMesh m, double* __restrict__ npinv) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m.nv) return;
+  double mat[3][3];
+  nodal_grad_matrix(m, v, mat);
+  pinv3(mat);
+  for (int d = 0; d < 3; ++d)
+    for (int e = 0; e < 3; ++e) npinv[9 * (size_t)v + 3 * d + e] = mat[d][e];
+}
+
+// compute_nodal_grad (ns_euler_recon_module.F90:453-490); ng[15] = g[5*d + var]. CACHED:
+// the pseudo-inverse comes from m.npinv (k_ns_nodal_pinv) instead of being formed here.
+template <bool CACHED>
 __device__ void ns_nodal_grad_body(const DevMesh& m, const double* __restrict__ U, double* __restrict__ ngrad,
                                    const NsScalars* sc, const int v) {
   if (sc && sc->done) return;
@@ -1286,14 +1320,21 @@ __device__ void ns_nodal_grad_body(const DevMesh& m, const double* __restrict__ 
     c2p(ur, wr);
     const double4 sn = m.sfn[sf];
     const double n[3] = {sn.x, sn.y, sn.z};
-    const double4 cl = m.cc[lr.x], cr = m.cc[lr.y];
-    const double dxc[3] = {cr.x - cl.x, cr.y - cl.y, cr.z - cl.z};
     for (int d = 0; d < 3; ++d)
       for (int k = 0; k < 5; ++k) g[d][k] = g[d][k] + sn.w * (n[d] * (wr[k] - wl[k]));
-    for (int d = 0; d < 3; ++d)
-      for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + sn.w * (n[d] * dxc[e]);
+    if (!CACHED) {
+      const double4 cl = m.cc[lr.x], cr = m.cc[lr.y];
+      const double dxc[3] = {cr.x - cl.x, cr.y - cl.y, cr.z - cl.z};
+      for (int d = 0; d < 3; ++d)
+        for (int e = 0; e < 3; ++e) mat[d][e] = mat[d][e] + sn.w * (n[d] * dxc[e]);
+    }
   }
-  pinv3(mat);
+  if (CACHED) {
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e) mat[d][e] = m.npinv[9 * (size_t)v + 3 * d + e];
+  } else {
+    pinv3(mat);
+  }
   const bool bnd = m.is_bound[v] != 0;
   double* o = ngrad + 15 * (size_t)v;
   for (int d = 0; d < 3; ++d)
@@ -1304,17 +1345,18 @@ __device__ void ns_nodal_grad_body(const DevMesh& m, const double* __restrict__ 
     }
 }
 
+template <bool CACHED>
 __global__ void __launch_bounds__(128) k_ns_nodal_grad(DevMesh m, const double* __restrict__ U,
                                                        double* __restrict__ ngrad, const NsScalars* sc) {
-  ns_nodal_grad_body(m, U, ngrad, sc, vert_at(m, blockIdx.x * blockDim.x + threadIdx.x));
+  ns_nodal_grad_body<CACHED>(m, U, ngrad, sc, vert_at(m, blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 // The same nodal gradient with a group of NG lanes per vertex, lane p holding the
 // vertex's p-th subface (both cells' primitives, the 15 gradient and 9 matrix terms): the
 // sums run in subface order by shuffles, each lane forming the same totals and the same
 // pseudo-inverse, and the lanes share the stores. Every lane of the warp reaches every
-// shuffle.
-template <int NG>
+// shuffle. CACHED: the pseudo-inverse comes from m.npinv and no matrix terms are formed.
+template <int NG, bool CACHED>
 __device__ void ns_nodal_grad_group(const DevMesh& m, const double* __restrict__ U, double* __restrict__ ngrad,
                                     const NsScalars* sc, const int t, const int lane) {
   if (sc && sc->done) return;
@@ -1339,12 +1381,14 @@ __device__ void ns_nodal_grad_group(const DevMesh& m, const double* __restrict__
       c2p(ur, wr);
       const double4 sn = m.sfn[sf];
       const double n[3] = {sn.x, sn.y, sn.z};
-      const double4 cl = m.cc[lr.x], cr = m.cc[lr.y];
-      const double dxc[3] = {cr.x - cl.x, cr.y - cl.y, cr.z - cl.z};
       for (int d = 0; d < 3; ++d)
         for (int k = 0; k < 5; ++k) tg[5 * d + k] = sn.w * (n[d] * (wr[k] - wl[k]));
-      for (int d = 0; d < 3; ++d)
-        for (int e = 0; e < 3; ++e) tm[3 * d + e] = sn.w * (n[d] * dxc[e]);
+      if (!CACHED) {
+        const double4 cl = m.cc[lr.x], cr = m.cc[lr.y];
+        const double dxc[3] = {cr.x - cl.x, cr.y - cl.y, cr.z - cl.z};
+        for (int d = 0; d < 3; ++d)
+          for (int e = 0; e < 3; ++e) tm[3 * d + e] = sn.w * (n[d] * dxc[e]);
+      }
     }
   }
   double g[3][5] = {{0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}, {0, 0, 0, 0, 0}};
@@ -1356,14 +1400,20 @@ __device__ void ns_nodal_grad_group(const DevMesh& m, const double* __restrict__
       const double x = __shfl_sync(kAll, tg[i], j, NG);
       if (add) g[i / 5][i % 5] = g[i / 5][i % 5] + x;
     }
+    if (!CACHED)
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      const double x = __shfl_sync(kAll, tm[i], j, NG);
-      if (add) mat[i / 3][i % 3] = mat[i / 3][i % 3] + x;
-    }
+      for (int i = 0; i < 9; ++i) {
+        const double x = __shfl_sync(kAll, tm[i], j, NG);
+        if (add) mat[i / 3][i % 3] = mat[i / 3][i % 3] + x;
+      }
   }
   if (!live) return;
-  pinv3(mat);
+  if (CACHED) {
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e) mat[d][e] = m.npinv[9 * (size_t)v + 3 * d + e];
+  } else {
+    pinv3(mat);
+  }
   const bool bnd = m.is_bound[v] != 0;
   double* o = ngrad + 15 * (size_t)v;
 #pragma unroll
@@ -1377,10 +1427,11 @@ __device__ void ns_nodal_grad_group(const DevMesh& m, const double* __restrict__
       }
 }
 
-template <int NG>
+template <int NG, bool CACHED>
 __global__ void __launch_bounds__(128) k_ns_nodal_grad_group(DevMesh m, const double* __restrict__ U,
                                                              double* __restrict__ ngrad, const NsScalars* sc) {
-  ns_nodal_grad_group<NG>(m, U, ngrad, sc, blockIdx.x * (128 / NG) + threadIdx.x / NG, threadIdx.x % NG);
+  ns_nodal_grad_group<NG, CACHED>(m, U, ngrad, sc, blockIdx.x * (128 / NG) + threadIdx.x / NG,
+                                  threadIdx.x % NG);
 }
 
 // compute_cell_grad_method_2..6 (:166-320) + physical_slope_limiter + relaxed_maximum_principle
@@ -1835,10 +1886,23 @@ __device__ void ns_finalize_body(NsScalars* sc, const NsParams& P, const double*
   }
   double dt = P.cfl * sc->dtred;
   if (!P.lts) dt = fmin2(sc->tmax - sc->t + 1e-12, dt);
+  // the partial sums in block order, the loads of eight blocks issued before their adds
   double res = 0.0, rv[5] = {0, 0, 0, 0, 0};
-  for (int b = 0; b < nblocks; ++b) {
-    res = res + partial[6 * (size_t)b];
-    for (int k = 0; k < 5; ++k) rv[k] = rv[k] + partial[6 * (size_t)b + 1 + k];
+  constexpr int kAhead = 8;
+  for (int b0 = 0; b0 < nblocks; b0 += kAhead) {
+    double buf[kAhead][6];
+#pragma unroll
+    for (int i = 0; i < kAhead; ++i)
+      if (b0 + i < nblocks)
+#pragma unroll
+        for (int k = 0; k < 6; ++k) buf[i][k] = partial[6 * (size_t)(b0 + i) + k];
+#pragma unroll
+    for (int i = 0; i < kAhead; ++i)
+      if (b0 + i < nblocks) {
+        res = res + buf[i][0];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) rv[k] = rv[k] + buf[i][1 + k];
+      }
   }
   const double omega = sc->omega;
   if (omega <= 1e-6) atomicOr(status, kErrBadOmega);
@@ -1953,7 +2017,7 @@ __global__ void __launch_bounds__(256) kb_ns_nodal_grad(const NsItem* __restrict
   for (int w = blockIdx.x; w < wv[n]; w += gridDim.x) {
     const int p = item_of(wv, n, w);
     const NsItem& I = it[p];
-    ns_nodal_grad_body(I.m, which ? I.U1 : I.U0, I.ngrad, I.sc, vert_at(I.m, (w - wv[p]) * blockDim.x + threadIdx.x));
+    ns_nodal_grad_body<false>(I.m, which ? I.U1 : I.U0, I.ngrad, I.sc, vert_at(I.m, (w - wv[p]) * blockDim.x + threadIdx.x));
   }
 }
 template <class T>
@@ -2450,16 +2514,35 @@ void launch_node(const DevMesh& m, const NsParams& P, const double* U, const dou
 
 // The nodal gradient: a group of 8, 16 or 32 lanes per vertex (the fewest that hold
 // every vertex's subfaces) along with the grouped node kernel, else a thread per vertex.
-void launch_nodal_grad(const DevMesh& m, const NsParams& P, const double* U, double* ngrad, const NsScalars* sc) {
+template <bool CACHED>
+void launch_nodal_grad_t(const DevMesh& m, const NsParams& P, const double* U, double* ngrad, const NsScalars* sc) {
   const int k = m.max_vsf, ng = k <= 8 ? 8 : k <= 16 ? 16 : k <= 32 ? 32 : 0;
   if (P.node_group && ng) {
     const int g = grid_for(m.nv, 128 / ng);
-    if (ng == 8) k_ns_nodal_grad_group<8><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
-    else if (ng == 16) k_ns_nodal_grad_group<16><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
-    else k_ns_nodal_grad_group<32><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
+    if (ng == 8) k_ns_nodal_grad_group<8, CACHED><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
+    else if (ng == 16) k_ns_nodal_grad_group<16, CACHED><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
+    else k_ns_nodal_grad_group<32, CACHED><<<g, 128, 0, m.stream>>>(m, U, ngrad, sc);
     return;
   }
-  k_ns_nodal_grad<<<grid_for(m.nv, 128), 128, 0, m.stream>>>(m, U, ngrad, sc);
+  k_ns_nodal_grad<CACHED><<<grid_for(m.nv, 128), 128, 0, m.stream>>>(m, U, ngrad, sc);
+}
+// with the mesh's cached pseudo-inverses when they belong to its current geometry
+void launch_nodal_grad(const DevMesh& m, const NsParams& P, const double* U, double* ngrad, const NsScalars* sc) {
+  if (m.npinv && m.npinv_epoch == m.geom_epoch) launch_nodal_grad_t<true>(m, P, U, ngrad, sc);
+  else launch_nodal_grad_t<false>(m, P, U, ngrad, sc);
+}
+
+int ensure_nodal_pinv(DevMesh* m) {
+  if (m->moving || m->nv == 0) return 0;
+  if (m->npinv && m->npinv_epoch == m->geom_epoch) return 0;
+  if (!m->npinv) {
+    SUBFV_CUDA(cudaMallocAsync((void**)&m->npinv, 9 * (size_t)m->nv * sizeof(double), m->stream));
+    m->bytes += 9 * (size_t)m->nv * sizeof(double);
+  }
+  k_ns_nodal_pinv<<<grid_for(m->nv, 128), 128, 0, m->stream>>>(*m, m->npinv);
+  SUBFV_CUDA(cudaGetLastError());
+  m->npinv_epoch = m->geom_epoch;
+  return 0;
 }
 
 // The cell gradient: a group of kCellLanes lanes per cell along with the grouped node

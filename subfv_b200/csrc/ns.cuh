@@ -45,6 +45,10 @@ struct NsItem {
 // Per-vertex array bound of the node kernel for a mesh: the smallest of 8, 16, 32 that
 // holds every vertex's subfaces and subcells (0: a vertex has more than 32).
 int ns_node_lanes(const DevMesh& m);
+// Fills (or refills after the geometry changed) the mesh's per-vertex pseudo-inverses of
+// the nodal-gradient matrices (DevMesh::npinv), on the mesh stream; nothing for a moving
+// mesh. The solo gradient launches read them while they match the current geometry.
+int ensure_nodal_pinv(DevMesh* m);
 // Table of in-flight problems on the device: items, work-block prefixes over their
 // vertices (wv, block_v vertices per work block) and cells (wc, 128 cells per work
 // block), and hdr[0] = the number of problems. Up to cap problems; the grids are

@@ -35,6 +35,8 @@ struct subfv_ns_state {
   ImplicitCtx* imp = nullptr;
   DiffParams D{};                                // diffusion parameters (P.diff)
   double *dterm = nullptr, *mu0c = nullptr;      // corner records, mu0corr
+  unsigned long long seen_epoch = 0;             // the mesh geometry the state last ran on
+  int geom_seen = 0;
 };
 
 namespace {
@@ -99,7 +101,28 @@ void enqueue_ns_step(subfv_ns_state* s) {
   }
 }
 
+// The caches that belong to the mesh geometry (the nodal-gradient pseudo-inverses, the
+// diffusion arrays) are filled for the state's first steps and refilled once the mesh's
+// geometry has changed since the state last ran; the captured step loop, which holds the
+// kernels chosen for the old caches, is then dropped.
+int ns_sync_geometry(subfv_ns_state* s) {
+  DevMesh& d = s->m->d;
+  if (s->geom_seen && s->seen_epoch == d.geom_epoch) return 0;
+  if (s->P.second_order && ensure_nodal_pinv(&d)) return -1;
+  if (s->geom_seen && s->P.diff && diffusion_cache_build(&d, s->D, s->U0, s->dterm, s->mu0c)) return -1;
+  if (s->graph) {
+    SUBFV_CUDA(cudaStreamSynchronize(d.stream));
+    cudaGraphExecDestroy(s->graph);
+    s->graph = nullptr;
+    s->graph_steps = 0;
+  }
+  s->seen_epoch = d.geom_epoch;
+  s->geom_seen = 1;
+  return 0;
+}
+
 int ns_graph(subfv_ns_state* s, int steps) {
+  if (ns_sync_geometry(s)) return -1;
   if (s->graph && s->graph_steps == steps) return 0;
   if (s->graph) {
     cudaGraphExecDestroy(s->graph);
@@ -229,7 +252,7 @@ int subfv_ns_state_create(subfv_mesh* m, const subfv_ns_cfg* cfg, const double* 
   launch_ns_pack(d, s->stage, s->U0);
   SUBFV_CUDA(cudaStreamSynchronize(d.stream));
   SUBFV_CUDA(cudaGetLastError());
-  if (s->P.diff && diffusion_cache_build(&d, s->D, s->U0, s->dterm, s->mu0c)) {
+  if ((s->P.diff && diffusion_cache_build(&d, s->D, s->U0, s->dterm, s->mu0c)) || ns_sync_geometry(s)) {
     subfv_ns_state_destroy(s);
     return -1;
   }
@@ -286,6 +309,7 @@ int subfv_ns_prepare(subfv_ns_state* s) {
 
 int subfv_ns_advance_async(subfv_ns_state* s, int n_steps) {
   DevMesh& d = s->m->d;
+  if (ns_sync_geometry(s)) return -1;
   const int chunk = kNsGraphSteps;
   if (n_steps >= chunk) {
     if (ns_graph(s, chunk)) return -1;

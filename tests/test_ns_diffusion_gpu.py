@@ -146,13 +146,15 @@ def test_states_of_different_meshes_coexist(native, oracle_lib, cuda_ok):
 
 def test_stencil_built_on_first_diffusion_state(native, oracle_lib, cuda_ok):
     """A mesh holds no diffusion stencil until a state with the diffusion terms asks for
-    it; a second such state reuses it, and the residual is the oracle's either way."""
+    it (a second-order inviscid state adds only the nodal-gradient pseudo-inverses, 72
+    bytes per vertex); a second such state reuses it, and the residual is the oracle's
+    either way."""
     from subfv_b200.ns import NsState, compute_rhs_ns_diag
     raw = _raws()["box_periodic"]
     m, o = _pair(raw)
     before = m.device_bytes
     NsState(m, _cfg("box_periodic", "neumann", activate_diffusion=False), _state(m.n_elems)).close()
-    assert m.device_bytes == before  # an inviscid state builds nothing on the mesh
+    assert m.device_bytes == before + 72 * m.n_vert  # no diffusion arrays
     cfg = _cfg("box_periodic", "neumann")
     sol = _state(m.n_elems)
     st, rhs, sl, diag = compute_rhs_ns_diag(m, cfg, sol)
@@ -221,3 +223,40 @@ def test_cache_follows_geometry_changes(native, oracle_lib, cuda_ok):
     assert not np.array_equal(rhs2_o, rhs_o)
     np.testing.assert_array_equal(rhs2, rhs2_o)
     np.testing.assert_array_equal(diag2, diag2_o)
+
+
+def test_running_state_follows_geometry_changes(native, oracle_lib, cuda_ok):
+    """A viscous state that keeps running after its mesh's vertices move drops its
+    captured step loop and refills the cached diffusion arrays and nodal-gradient
+    pseudo-inverses: eight steps on the first geometry and eight on the moved one equal
+    the oracle's, bit for bit."""
+    from dataclasses import replace as dc_replace
+    from oracle.oracle import OracleMesh
+    from subfv_b200.ns import NsState
+    raw = _raws()["hex"]
+    m, o = _pair(raw)
+    cfg = _cfg("hex", "dirichlet")
+    sol = _state(m.n_elems)
+    s = NsState(m, cfg, sol)
+    st, n, _ = s.advance(8)  # one captured graph of eight steps
+    assert st == 0 and n == 8
+    c = raw.coords.copy()
+    lo, hi = c.min(0), c.max(0)
+    inner = (c[:, 0] > lo[0] + 1e-9) & (c[:, 0] < hi[0] - 1e-9) & (c[:, 1] > lo[1] + 1e-9) & (c[:, 1] < hi[1] - 1e-9)
+    rng = np.random.default_rng(13)
+    shift = rng.uniform(-0.02, 0.02, (len(c), 2)) / NX
+    _, col = np.unique(np.round(c[:, :2], 9), axis=0, return_inverse=True)  # one shift per column
+    c[inner, :2] += shift[col.ravel()][inner]
+    o2 = OracleMesh(dc_replace(raw, coords=c))
+    m.set_coords(o2.geom("vert_coord"))
+    assert m.compute_geometry_mesh() == 0
+    st, n, t = s.advance(8)
+    assert st == 0 and n == 16
+    sol_o = sol.copy()
+    st_o, it, t_o, _, _, _ = o.ns_run(cfg.oracle_dict(), sol_o, 7)
+    assert st_o == 0 and it == 8
+    st_o, it, t_o, _, _, _ = o2.ns_run(cfg.oracle_dict(), sol_o, 7, t0=t_o)
+    assert st_o == 0 and it == 8
+    assert t == t_o
+    np.testing.assert_array_equal(s.sol(), sol_o)
+    s.close()

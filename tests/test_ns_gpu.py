@@ -101,6 +101,45 @@ def test_grouped_gradients_bitwise(native, cuda_ok, method):
             np.testing.assert_array_equal(out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("lanes", [0, 1])
+def test_state_follows_geometry_changes(native, oracle_lib, cuda_ok, lanes):
+    """A state that keeps running after its mesh's vertices move (subfv_mesh_set_coords,
+    then subfv_compute_geometry_mesh) drops its captured step loop and refills the mesh's
+    geometry caches (the nodal-gradient pseudo-inverses): its states are the oracle's, run
+    eight steps on the first geometry and eight on the moved one. Both node layouts."""
+    from dataclasses import replace as dc_replace
+    from oracle.oracle import OracleMesh
+    from subfv_b200.ns import NsConfig, NsState, init_gresho
+    raw = _meshes()["hex_slab"]
+    m, o = _pair(raw)
+    cfg = NsConfig(**CFGS["mp_o2_m5"], boundary_2d=True, cfl=0.4)
+    sol = _perturbed_gresho(m, 3)
+    s = NsState(m, cfg, sol)
+    s.set_node_kernel(lanes)
+    st, n, t = s.advance(8)  # one captured graph of eight steps
+    assert st == 0 and n == 8
+    c = raw.coords.copy()
+    lo, hi = c.min(0), c.max(0)
+    inner = (c[:, 0] > lo[0] + 1e-9) & (c[:, 0] < hi[0] - 1e-9) & (c[:, 1] > lo[1] + 1e-9) & (c[:, 1] < hi[1] - 1e-9)
+    rng = np.random.default_rng(12)
+    shift = rng.uniform(-0.02, 0.02, (len(c), 2)) / 12
+    _, col = np.unique(np.round(c[:, :2], 9), axis=0, return_inverse=True)  # one shift per column
+    c[inner, :2] += shift[col.ravel()][inner]
+    o2 = OracleMesh(dc_replace(raw, coords=c))
+    m.set_coords(o2.geom("vert_coord"))
+    assert m.compute_geometry_mesh() == 0
+    st, n, t = s.advance(8)
+    assert st == 0 and n == 16
+    sol_o = sol.copy()
+    st_o, it, t_o, _, _, _ = o.ns_run(cfg.oracle_dict(), sol_o, 7)
+    assert st_o == 0 and it == 8
+    st_o, it, t_o, _, _, _ = o2.ns_run(cfg.oracle_dict(), sol_o, 7, t0=t_o)
+    assert st_o == 0 and it == 8
+    assert t == t_o
+    np.testing.assert_array_equal(s.sol(), sol_o)
+    s.close()
+
+
 def test_gresho_init_matches_oracle(native, oracle_lib, cuda_ok):
     from subfv_b200.ns import init_gresho
     m, o = _pair(_meshes()["hex_slab"])
