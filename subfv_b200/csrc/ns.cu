@@ -156,8 +156,17 @@ __device__ bool inv3_if_regular(double A[3][3]) {
 // linear_solver_module.F90:683-715): the inverse when the cut cannot bite, else a
 // one-sided Jacobi SVD of six sweeps.
 __device__ __noinline__ void pinv3_jacobi(double A[3][3]);
+// the Jacobi case works on a copy: an array whose address reaches an out-of-line call
+// lives in local memory on every path, so the caller's matrix keeps no escaping address
 __device__ inline void pinv3(double A[3][3]) {
-  if (!inv3_if_regular(A)) pinv3_jacobi(A);
+  if (!inv3_if_regular(A)) {
+    double B[3][3];
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e) B[d][e] = A[d][e];
+    pinv3_jacobi(B);
+    for (int d = 0; d < 3; ++d)
+      for (int e = 0; e < 3; ++e) A[d][e] = B[d][e];
+  }
 }
 // the rank-deficient case, out of line (rare; keeps the callers' registers low)
 __device__ __noinline__ void pinv3_jacobi(double A[3][3]) {
@@ -321,15 +330,19 @@ __device__ __noinline__ void potential_flow(const double4 x4, bool three_d, T* w
 // compute_right_state (:331-409): the ghost state by boundary kind (1 wall, 2 adherence
 // wall, 3 freestream, 4 supersonic outflow, 5 pondered inflow, 6 double-Mach inflow /
 // outflow, 7 double-Mach bottom, 8 and 9 the potential flows in 2-D and 3-D); sol_l /
-// sol_r conservative, n the subface normal. The kinds that read the face centroid or the
-// time do so out of line; sc->t is the time of the step being evaluated (null: 0).
+// sol_r conservative, n the subface normal. The kinds that read the face centroid fx or
+// the time t (of the step being evaluated) are out of line. Their arguments are values
+// only: a reference to the kernel's mesh or parameter block would make every thread of
+// the calling kernel copy that block into local memory.
+struct BcVals {
+  double v[5];
+};
 template <class T>
-__device__ __noinline__ void right_state_ext(const DevMesh& m, const NsParams& P, int kind, int y, int sf,
-                                             const T* n, const T* sol_l, T* sol_r, const NsScalars* sc) {
-  const double* bv = P.bc_val[-(y + 1) - 1];
+__device__ __noinline__ void right_state_ext(int kind, const BcVals bv, const double4 fx, const double t, const T* n,
+                                             const T* sol_l, T* sol_r) {
   if (kind == 2) {
     for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
-    for (int k = 1; k < 4; ++k) sol_r[k] = (T)2.0 * sol_l[0] * (T)bv[k] - sol_l[k];
+    for (int k = 1; k < 4; ++k) sol_r[k] = (T)2.0 * sol_l[0] * (T)bv.v[k] - sol_l[k];
     const T nl = oi3<T>(sol_l[1] / sol_l[0], sol_l[2] / sol_l[0], sol_l[3] / sol_l[0]);
     const T nr = oi3<T>(sol_r[1] / sol_r[0], sol_r[2] / sol_r[0], sol_r[3] / sol_r[0]);
     sol_r[4] = sol_l[4] - (T)0.5 * sol_l[0] * (nl * nl) + (T)0.5 * sol_l[0] * (nr * nr);
@@ -337,13 +350,12 @@ __device__ __noinline__ void right_state_ext(const DevMesh& m, const NsParams& P
   }
   if (kind == 5) {
     T w[5];
-    for (int k = 0; k < 5; ++k) w[k] = (T)bv[k];
+    for (int k = 0; k < 5; ++k) w[k] = (T)bv.v[k];
     p2c(w, sol_r);
     if (dotT(sol_r + 1, n) > (T)0)
       for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
     return;
   }
-  const double4 fx = m.fc[m.sf_face[sf]];
   if (kind == 8 || kind == 9) {
     T w[5];
     potential_flow<T>(fx, kind == 9, w);
@@ -352,8 +364,7 @@ __device__ __noinline__ void right_state_ext(const DevMesh& m, const NsParams& P
   }
   const T post[5] = {(T)8.0, (T)7.145, (T)-4.125, (T)0.0, (T)116.5}, pre[5] = {(T)1.4, 0, 0, 0, (T)1.0};
   if (kind == 6) {
-    const T t = sc ? (T)sc->t : (T)0;
-    p2c((T)fx.y > (T)1.732 * ((T)fx.x - (T)0.1667 - (T)10.0 * t) ? post : pre, sol_r);
+    p2c((T)fx.y > (T)1.732 * ((T)fx.x - (T)0.1667 - (T)10.0 * (T)t) ? post : pre, sol_r);
   } else if ((T)fx.x < (T)0.1667) {  // kind 7
     p2c(post, sol_r);
   } else {
@@ -378,7 +389,11 @@ __device__ void right_state(const DevMesh& m, const NsParams& P, int y, int sf, 
   } else if (kind == 4) {
     for (int k = 0; k < 5; ++k) sol_r[k] = sol_l[k];
   } else {
-    right_state_ext<T>(m, P, kind, y, sf, n, sol_l, sol_r, sc);
+    BcVals bv;
+    for (int k = 0; k < 5; ++k) bv.v[k] = P.bc_val[-(y + 1) - 1][k];
+    const double4 fx = kind >= 6 ? m.fc[m.sf_face[sf]] : make_double4(0.0, 0.0, 0.0, 0.0);
+    const double t = (kind == 6 && sc) ? sc->t : 0.0;
+    right_state_ext<T>(kind, bv, fx, t, n, sol_l, sol_r);
   }
 }
 
@@ -633,6 +648,52 @@ __device__ __noinline__ void blend_three_wave(const double* w10, const double* n
     for (int k = 0; k < 5; ++k) lr[q][k] = wa * lr[q][k] + (1.0 - wa) * lr3[q][k];
 }
 
+// The out-of-line fluxes called on private copies of the node kernels' arrays (the
+// subface's states, its normal and area, the flux pair and wave speeds), so that those
+// arrays keep no escaping address and stay in registers on the multi_point and two_wave
+// paths; the called routines see the same values.
+struct FluxCopy {
+  double w[10], n[4], lr[2][5], sl, sr;
+  __device__ void load(const double* w10, const double* n4) {
+    for (int k = 0; k < 10; ++k) w[k] = w10[k];
+    for (int d = 0; d < 4; ++d) n[d] = n4[d];
+  }
+  __device__ void store(double o[2][5], double* sl_o, double* sr_o) const {
+    for (int q = 0; q < 2; ++q)
+      for (int k = 0; k < 5; ++k) o[q][k] = lr[q][k];
+    *sl_o = sl;
+    *sr_o = sr;
+  }
+};
+template <class T>
+__device__ inline void three_wave_c(const double* w10, const double* n4, double lr[2][5], double* sl, double* sr,
+                                    bool modified) {
+  FluxCopy c;
+  c.load(w10, n4);
+  three_wave<T>(c.w, c.w + 5, c.n, c.lr, &c.sl, &c.sr, modified);
+  c.store(lr, sl, sr);
+}
+template <class T>
+__device__ inline void multi_point_pressure_c(const double* w10, const double* n4, double lr[2][5], double p_nodal,
+                                              double lam_l, double lam_r, double* sl, double* sr, bool ph) {
+  FluxCopy c;
+  c.load(w10, n4);
+  multi_point_pressure<T>(c.w, c.w + 5, c.n, c.lr, p_nodal, lam_l, lam_r, &c.sl, &c.sr, ph);
+  c.store(lr, sl, sr);
+}
+template <class T>
+__device__ inline void blend_three_wave_c(const double* w10, const double* n4, double amin, double lr[2][5],
+                                          double* sl, double* sr) {
+  FluxCopy c;
+  c.load(w10, n4);
+  for (int q = 0; q < 2; ++q)
+    for (int k = 0; k < 5; ++k) c.lr[q][k] = lr[q][k];
+  c.sl = *sl;
+  c.sr = *sr;
+  blend_three_wave<T>(c.w, c.n, amin, c.lr, &c.sl, &c.sr);
+  c.store(lr, sl, sr);
+}
+
 // multi_point (ns_euler_rs_module.F90:200-286); false on a negative star density
 template <class T>
 __device__ bool multi_point(const double* wl64, const double* wr64, const double* n64, double lr[2][5],
@@ -757,21 +818,22 @@ __device__ inline double vbar_of(double lam_l, double lam_r, double vnl, double 
 
 // compute_lambdas_and_solve_nodal_pressure for one vertex (thread-per-vertex layout):
 // ten iterations of p_node = s1 / s2, the bounds kept in L between iterations. Out of
-// line, so the other schemes' register allocation does not carry it.
+// line, so the other schemes' register allocation does not carry it; it takes the
+// subface normals' array and the walls of bc_style 1 (bit j: subface j) by value, since
+// a reference to the kernel's mesh or parameter block would make every thread copy it.
 template <class T, class L, int MS>
-__device__ __noinline__ double nodal_pressure_vertex(const DevMesh& m, const NsParams& P, int nsfn, const int* sfj,
-                                                     const int* yj, const T (*wlr)[10], L (*lam)[2]) {
+__device__ __noinline__ double nodal_pressure_vertex(const double4* __restrict__ sfn, unsigned wall1, int nsfn,
+                                                     const int* sfj, const T (*wlr)[10], L (*lam)[2]) {
   double p_node = 0.0;
   for (int iter = 1; iter <= 10; ++iter) {
     double s1 = 0.0, s2 = 0.0;
     for (int j = 0; j < nsfn; ++j) {
-      const double4 sn4 = m.sfn[sfj[j]];
+      const double4 sn4 = sfn[sfj[j]];
       const double n[3] = {sn4.x, sn4.y, sn4.z};
       double w10[10];
       for (int k = 0; k < 10; ++k) w10[k] = (double)wlr[j][k];
       double ll = (double)lam[j][0], lr = (double)lam[j][1], t1, t2;
-      nodal_pressure_terms(iter, P.bc_style == 1 && is_wall(P, yj[j]), w10, w10 + 5, n, sn4.w, p_node, ll, lr, t1,
-                           t2);
+      nodal_pressure_terms(iter, ((wall1 >> j) & 1u) != 0, w10, w10 + 5, n, sn4.w, p_node, ll, lr, t1, t2);
       s1 = s1 + t1;
       s2 = s2 + t2;
       lam[j][0] = (L)ll;
@@ -800,12 +862,16 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
   T wlr[MS][10];
   L lam[MS][2];  // lambda_l, lambda_r
   int sfj[MS], yj[MS];
+  // bit j: subface j is a slip wall (is_wall), looked up once: the kind table is indexed
+  // by each subface's own tag, and inside the loops below the lookups would serialise
+  unsigned wallm = 0u;
   double amin = 0.0;  // minval of the subface areas (warea of multi_point_iso, ns_euler_module.F90:386-397)
   for (int j = 0; j < nsfn; ++j) {
     const int sf = m.vsf[p0 + j];
     const int2 lr = m.flr[m.sf_face[sf]];
     sfj[j] = sf;
     yj[j] = lr.y;
+    if (is_wall(P, lr.y)) wallm |= 1u << j;
     if (EXT && P.scheme == 2) amin = j == 0 ? m.sfn[sf].w : fmin2(amin, m.sfn[sf].w);
     double w10[10];
     reconstruct<T>(m, P, U, grad, v, sf, lr.x, lr.y, so != 0, w10, w10 + 5, sc);
@@ -825,8 +891,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
         const double n[4] = {sn4.x, sn4.y, sn4.z, sn4.w};
         snd[j][0] = sqrt((L)G * (L)wlr[j][4] / (L)wlr[j][0]);
         snd[j][1] = sqrt((L)G * (L)wlr[j][9] / (L)wlr[j][5]);
-        const int y = yj[j];
-        if (y < 0 && !(P.b2d && fabs(n[2]) > 1e-12) && (y == -1 || P.bc_type[-(y + 1) - 1] == 1))
+        if (((wallm >> j) & 1u) && !(P.b2d && fabs(n[2]) > 1e-12))
           for (int d = 0; d < 3; ++d) Bp[d] = Bp[d] + n[3] * n[d];
       }
       for (int iter = 1; iter <= 4; ++iter) {
@@ -849,7 +914,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
           const T ntT[3] = {(T)n[0], (T)n[1], (T)n[2]};
           const double vnl_f = (double)dotT(wlr[j] + 1, ntT), vnr_f = (double)dotT(wlr[j] + 6, ntT);
           const double pl_f = (double)wlr[j][4], pr_f = (double)wlr[j][9];
-          const bool wall = is_wall(P, yj[j]);
+          const bool wall = (wallm >> j) & 1u;
           const L c1 = (L)1, c15 = (L)1.5, c0 = (L)0;
           if (iter == 1) {
             lam_l = tmax2(tmax2(tmax2(lam_l, al * rhol), sqrt(rhol * tmax2(c0, pr - pl))), -rhol * (vnr - vnl));
@@ -896,7 +961,9 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     m.vp[v] = make_double4(vn3[0], vn3[1], vn3[2], 0.0);
   }
   const double p_node =
-      (EXT && (P.scheme == 6 || P.scheme == 8)) ? nodal_pressure_vertex<T, L, MS>(m, P, nsfn, sfj, yj, wlr, lam) : 0.0;
+      (EXT && (P.scheme == 6 || P.scheme == 8))
+          ? nodal_pressure_vertex<T, L, MS>(m.sfn, P.bc_style == 1 ? wallm : 0u, nsfn, sfj, wlr, lam)
+          : 0.0;
   double fsv[MS][6];  // five flux sums and the wave-speed sum per subcell
   for (int j = 0; j < nsen; ++j)
     for (int k = 0; k < 6; ++k) fsv[j][k] = 0.0;
@@ -911,17 +978,16 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
     for (int k = 0; k < 10; ++k) w10[k] = (double)wlr[j][k];
     double lr[2][5], sl, sr;
     if ((P.scheme == 1 || iso) && !excl) {
-      const double vn = is_wall(P, yj[j]) ? 0.0 : dotT(vn3, n);
+      const double vn = ((wallm >> j) & 1u) ? 0.0 : dotT(vn3, n);
       if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam[j][0], (double)lam[j][1], &sl, &sr)) bad = true;
     } else if (EXT && (P.scheme == 3 || P.scheme == 5)) {
-      three_wave<T>(w10, w10 + 5, n, lr, &sl, &sr, P.scheme == 5);
+      three_wave_c<T>(w10, n, lr, &sl, &sr, P.scheme == 5);
     } else if (EXT && (P.scheme == 6 || P.scheme == 8)) {
-      multi_point_pressure<T>(w10, w10 + 5, n, lr, p_node, (double)lam[j][0], (double)lam[j][1], &sl, &sr,
-                              P.scheme == 8);
+      multi_point_pressure_c<T>(w10, n, lr, p_node, (double)lam[j][0], (double)lam[j][1], &sl, &sr, P.scheme == 8);
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
-    if (iso) blend_three_wave<T>(w10, n, amin, lr, &sl, &sr);
+    if (iso) blend_three_wave_c<T>(w10, n, amin, lr, &sl, &sr);
     if (m.se_vert[se.x] == v && lse_loc < nsen) {
       const double area = n[3];
       fsv[lse_loc][5] = fsv[lse_loc][5] + area * fmax2(0.0, -sl);
@@ -953,6 +1019,7 @@ __device__ void ns_node_vertex(const DevMesh& m, const NsParams& P, const double
 // on the same sums. NG is 8, 16 or 32; a block of kNodeGroupThreads lanes holds
 // kNodeGroupThreads / NG vertices.
 constexpr int kNodeGroupThreads = 256;
+constexpr int kNodeGroupMinBlocks = 2;
 constexpr int kLaneVals = 12;  // per-lane scratch doubles: 9 solver terms or 12 subcell terms
 
 template <int NG>
@@ -1142,14 +1209,13 @@ __device__ void ns_node_group(const DevMesh& m, const NsParams& P, const double*
       if (!multi_point<T>(w10, w10 + 5, n, lr, vn, (double)lam_l, (double)lam_r, &sl, &sr))
         atomicOr(m.status, kErrNegDensity);
     } else if (P.scheme == 3 || P.scheme == 5) {
-      three_wave<T>(w10, w10 + 5, n, lr, &sl, &sr, P.scheme == 5);
+      three_wave_c<T>(w10, n, lr, &sl, &sr, P.scheme == 5);
     } else if (P.scheme == 6 || P.scheme == 8) {
-      multi_point_pressure<T>(w10, w10 + 5, n, lr, p_node, (double)lam_l, (double)lam_r, &sl, &sr,
-                              P.scheme == 8);
+      multi_point_pressure_c<T>(w10, n, lr, p_node, (double)lam_l, (double)lam_r, &sl, &sr, P.scheme == 8);
     } else {
       two_wave<T>(w10, w10 + 5, n, lr, &sl, &sr);
     }
-    if (iso) blend_three_wave<T>(w10, n, amin, lr, &sl, &sr);
+    if (iso) blend_three_wave_c<T>(w10, n, amin, lr, &sl, &sr);
     if (m.se_vert[se.x] == v && lse_loc < nsen) {
       const double area = n[3];
       double* c = gv + j * kLaneVals;
@@ -1203,7 +1269,7 @@ struct NodeGroupSmem {
 };
 
 template <class T, class L, int NG>
-__global__ void __launch_bounds__(kNodeGroupThreads, 2) k_ns_node_group(DevMesh m, NsParams P,
+__global__ void __launch_bounds__(kNodeGroupThreads, kNodeGroupMinBlocks) k_ns_node_group(DevMesh m, NsParams P,
                                                                      const double* __restrict__ U,
                                                                      const double* __restrict__ grad,
                                                                      double* __restrict__ fs, int so,
@@ -1765,9 +1831,16 @@ constexpr int kTdBlock = 128;
 // called by every thread of a kTdBlock-thread block; blk is the block's index within
 // its problem (it selects the slot of the residual partial sums)
 // With diffusion the cell's terms go onto the limited residual and into its 5x5 block,
-// and the cell solves (block + s I) x = rhs + s U by LU (out of line: rare).
-__device__ __noinline__ void diffusion_cell_solve(const DevMesh& m, int c, const double* __restrict__ dterm, int kd,
-                                                  double* r, double* rv, const double* u, double s, double* d5) {
+// and the cell solves (block + s I) x = rhs + s U by LU (out of line: rare). The
+// out-of-line solve takes the five mesh arrays it reads by value: a reference to the
+// kernel's mesh would make every thread copy the whole mesh block into local memory.
+struct DiffCellView {
+  const int *ev_off, *cse_sorted, *se_vert, *dse_off;
+  const int4* se_sf;
+};
+__device__ __noinline__ void diffusion_cell_solve(const DiffCellView m, int c, const double* __restrict__ dterm,
+                                                  int kd, double* r, double* rv, const double* u, double s,
+                                                  double* d5) {
   double D[25];
   for (int k = 0; k < 25; ++k) D[k] = 0.0;
   apply_diffusion_terms(m, c, dterm, kd, r, D);
@@ -1813,7 +1886,8 @@ __device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const doub
     ld5(U_td, c, u);
     const double s = a1 * (V / dt + 0.0);  // sum_lambda is zeroed once dt is known
     if (DIFF) {
-      diffusion_cell_solve(m, c, dterm, P.diff_kd, r, rv, u, s, d5);
+      diffusion_cell_solve({m.ev_off, m.cse_sorted, m.se_vert, m.dse_off, m.se_sf}, c, dterm, P.diff_kd, r, rv, u, s,
+                           d5);
       for (int k = 0; k < 5; ++k) ad[k] = a2 * d5[k];
     } else {
       for (int k = 0; k < 5; ++k) rv[k] = r[k] * r[k];
@@ -1984,7 +2058,7 @@ __global__ void __launch_bounds__(kNodeThreads) kb_ns_node(const NsItem* __restr
 // the group variant: a work block of block_v vertices is walked kNodeGroupThreads / NG
 // vertices at a time
 template <class T, class L, int NG>
-__global__ void __launch_bounds__(kNodeGroupThreads, 2) kb_ns_node_group(const NsItem* __restrict__ it,
+__global__ void __launch_bounds__(kNodeGroupThreads, kNodeGroupMinBlocks) kb_ns_node_group(const NsItem* __restrict__ it,
                                                                       const int* __restrict__ wv,
                                                                       const int* __restrict__ hdr, NsParams P,
                                                                       int which, int so, int block_v) {
@@ -2159,15 +2233,16 @@ __device__ inline double euler_jac_entry(const EulerJacScalars& e, const double*
 // domain: I; adherence wall: the derivative of its reflection about the wall velocity;
 // imposed states: 0). fx0 is the face centroid's x. Out of line: rare, and it holds
 // three full matrices.
-__device__ __noinline__ void ghost_block(const NsParams& P, int y, const double* wl, const double* wr,
+// kind: the boundary kind of the face, bc its values (by value: a reference to the
+// kernel's parameter block would make every thread copy it into local memory)
+__device__ __noinline__ void ghost_block(int kind, const BcVals bc, const double* wl, const double* wr,
                                          const double* n, double area, double fx0, double* g) {
   double JL[5][5], JR[5][5];
   two_wave_jac(wl, wr, n, JL, JR);
-  const int kind = y == -1 ? 1 : P.bc_type[-(y + 1) - 1];
   double M[5][5];
   for (int a = 0; a < 5; ++a)
     for (int b = 0; b < 5; ++b) M[a][b] = 0.0;
-  const double* bv = y == -1 ? nullptr : P.bc_val[-(y + 1) - 1];
+  const double* bv = bc.v;
   if (kind == 1 || (kind == 7 && !(fx0 < 0.1667))) {
     M[0][0] = M[4][4] = 1.0;
     for (int a = 0; a < 3; ++a)
@@ -2252,7 +2327,11 @@ __global__ void __launch_bounds__(64) k_be_assemble(DevMesh m, NsParams P, const
     reconstruct<double>(m, P, U, nullptr, m.sf_vert[sf], sf, lr.x, lr.y, false, wl, wr, sc);
     if (side == 0 && lr.y < 0) {
       double g[25];
-      ghost_block(P, lr.y, wl, wr, n, area, m.fc[m.sf_face[sf]].x, g);
+      const int kind = lr.y == -1 ? 1 : P.bc_type[-(lr.y + 1) - 1];
+      BcVals bc{{0.0, 0.0, 0.0, 0.0, 0.0}};
+      if (lr.y != -1)
+        for (int k = 0; k < 5; ++k) bc.v[k] = P.bc_val[-(lr.y + 1) - 1][k];
+      ghost_block(kind, bc, wl, wr, n, area, m.fc[m.sf_face[sf]].x, g);
 #pragma unroll
       for (int e = 0; e < 25; ++e) D[e] = D[e] + g[e];
       continue;

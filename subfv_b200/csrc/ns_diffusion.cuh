@@ -53,7 +53,9 @@ void launch_ns_diffusion_apply(const DevMesh& m, const double* dterm, int kd, do
 
 // The cell's diffusion terms onto its residual r (after flux limiting) and its block D
 // (column-major, zero on entry).
-__device__ inline void apply_diffusion_terms(const DevMesh& m, int c, const double* __restrict__ dterm, int kd,
+// M: DevMesh or any view with its ev_off, cse_sorted, se_sf, se_vert and dse_off arrays
+template <class M>
+__device__ inline void apply_diffusion_terms(const M& m, int c, const double* __restrict__ dterm, int kd,
                                              double* r, double* D) {
   const int e0 = m.ev_off[c], e1 = m.ev_off[c + 1];
   for (int q = e0; q < e1; ++q) {
