@@ -1307,10 +1307,27 @@ __device__ void ns_gather_body(const DevMesh& m, const double* __restrict__ fs, 
   double dmin = 1e10;
   if (c < m.ne) {
     double r[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, sl = 1e-12;
-    for (int q = m.ev_off[c]; q < m.ev_off[c + 1]; ++q) {
-      const double* f = fs + kNsFs * (size_t)m.cse_sorted[q];
-      for (int k = 0; k < 5; ++k) r[k] = r[k] - f[k];
-      sl = sl + f[5];
+    // the corner records of four subcells at a time loaded before their sums, which run
+    // in the list's order
+    constexpr int kAhead = 4;
+    const int q1 = m.ev_off[c + 1];
+    for (int q0 = m.ev_off[c]; q0 < q1; q0 += kAhead) {
+      int id[kAhead];
+#pragma unroll
+      for (int i = 0; i < kAhead; ++i) id[i] = q0 + i < q1 ? m.cse_sorted[q0 + i] : 0;
+      double f[kAhead][6];
+#pragma unroll
+      for (int i = 0; i < kAhead; ++i)
+        if (q0 + i < q1)
+#pragma unroll
+          for (int k = 0; k < 6; ++k) f[i][k] = fs[kNsFs * (size_t)id[i] + k];
+#pragma unroll
+      for (int i = 0; i < kAhead; ++i)
+        if (q0 + i < q1) {
+#pragma unroll
+          for (int k = 0; k < 5; ++k) r[k] = r[k] - f[i][k];
+          sl = sl + f[i][5];
+        }
     }
     double* o = rhs + kRhs * (size_t)c;
     for (int k = 0; k < 5; ++k) o[k] = r[k];
@@ -1661,6 +1678,35 @@ __device__ void ns_cell_grad_group(const DevMesh& m, const NsParams& P, const do
     for (int i = 0; i < 15; ++i) ng[i] = (T)src[i];
     vol = (T)m.vol_v[v];
   }
+  // relaxed_maximum_principle, this lane's part: the states of the cells around its
+  // vertex do not depend on the gradient, so their folds run first, their loads issued
+  // four cells at a time (the folds in the list's order)
+  T lrmin = (T)1e100, lrmax = 0, lpmin = (T)1e100, lpmax = 0;
+  if (sizeof(T) == 4) lrmin = lpmin = (T)3.0e38f;
+  if (own) {
+    constexpr int kAhead = 4;
+    const int qb = m.vel_off[v + 1];
+    for (int q0 = m.vel_off[v]; q0 < qb; q0 += kAhead) {
+      int id[kAhead];
+#pragma unroll
+      for (int i = 0; i < kAhead; ++i) id[i] = q0 + i < qb ? m.vel[q0 + i] : 0;
+      double un[kAhead][5];
+#pragma unroll
+      for (int i = 0; i < kAhead; ++i)
+        if (q0 + i < qb) ld5(U, id[i], un[i]);
+#pragma unroll
+      for (int i = 0; i < kAhead; ++i)
+        if (q0 + i < qb) {
+          T ut[5], w[5];
+          for (int k = 0; k < 5; ++k) ut[k] = (T)un[i][k];
+          c2p(ut, w);
+          lpmin = tmin2(lpmin, w[4]);
+          lpmax = tmax2(lpmax, w[4]);
+          lrmin = tmin2(lrmin, w[0]);
+          lrmax = tmax2(lrmax, w[0]);
+        }
+    }
+  }
   T g[15], ws[5] = {0, 0, 0, 0, 0};
   for (int i = 0; i < 15; ++i) g[i] = 0;
   if (P.method == 2) {  // dual-volume average
@@ -1762,19 +1808,6 @@ __device__ void ns_cell_grad_group(const DevMesh& m, const NsParams& P, const do
   for (int i = 0; i < 15; ++i) g[i] = omega * g[i];
   T rmin = (T)1e100, rmax = 0, pmin = (T)1e100, pmax = 0;  // relaxed_maximum_principle
   if (sizeof(T) == 4) rmin = pmin = (T)3.0e38f;
-  T lrmin = rmin, lrmax = rmax, lpmin = pmin, lpmax = pmax;
-  if (own)
-    for (int q = m.vel_off[v]; q < m.vel_off[v + 1]; ++q) {
-      double un[5];
-      ld5(U, m.vel[q], un);
-      T ut[5], w[5];
-      for (int k = 0; k < 5; ++k) ut[k] = (T)un[k];
-      c2p(ut, w);
-      lpmin = tmin2(lpmin, w[4]);
-      lpmax = tmax2(lpmax, w[4]);
-      lrmin = tmin2(lrmin, w[0]);
-      lrmax = tmax2(lrmax, w[0]);
-    }
   for (int j = 0; j < nmax; ++j) {
     const T a = __shfl_sync(kAll, lpmin, j, kCellLanes), b = __shfl_sync(kAll, lpmax, j, kCellLanes);
     const T e = __shfl_sync(kAll, lrmin, j, kCellLanes), f = __shfl_sync(kAll, lrmax, j, kCellLanes);
