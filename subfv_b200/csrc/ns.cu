@@ -19,7 +19,8 @@
 //   (on small meshes the node kernel and both gradients run a group of lanes per
 //   vertex or cell instead: k_ns_node_group, k_ns_nodal_grad_group, k_ns_cell_grad_group)
 // then per stage k_ns_timedisc (flux limiting blend, diagonal solve, positivity limiter,
-// residual partial sums), k_ns_finalize (one thread) and k_ns_apply.
+// residual partial sums; its last block to finish runs the stage's scalar tail) and
+// k_ns_apply (batched problems: kb_ns_timedisc, kb_ns_finalize, kb_ns_apply).
 //
 // Plain FP64 (precision 0) follows the reference's evaluation order and is compiled
 // without FMA contraction, so it reproduces the CPU restatement bit for bit, except the
@@ -1973,16 +1974,6 @@ __device__ void ns_timedisc_body(const DevMesh& m, const NsParams& P, const doub
   }
 }
 
-template <bool DIFF>
-__global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P, const double* __restrict__ U_rhs,
-                                                          const double* __restrict__ rhs1,
-                                                          const double* __restrict__ rhs2,
-                                                          const double* __restrict__ U_td,
-                                                          double* __restrict__ delta, double* __restrict__ partial,
-                                                          NsScalars* sc, double a1, double a2,
-                                                          const double* __restrict__ dterm) {
-  ns_timedisc_body<DIFF>(m, P, U_rhs, rhs1, rhs2, U_td, delta, partial, sc, a1, a2, blockIdx.x, dterm);
-}
 
 // scalar tail of add_timedisc_and_solve (:582-608); last_stage also advances t
 __device__ void ns_finalize_body(NsScalars* sc, const NsParams& P, const double* __restrict__ partial, int nblocks,
@@ -2002,7 +1993,7 @@ __device__ void ns_finalize_body(NsScalars* sc, const NsParams& P, const double*
     for (int i = 0; i < kAhead; ++i)
       if (b0 + i < nblocks)
 #pragma unroll
-        for (int k = 0; k < 6; ++k) buf[i][k] = partial[6 * (size_t)(b0 + i) + k];
+        for (int k = 0; k < 6; ++k) buf[i][k] = __ldcg(partial + 6 * (size_t)(b0 + i) + k);
 #pragma unroll
     for (int i = 0; i < kAhead; ++i)
       if (b0 + i < nblocks) {
@@ -2011,7 +2002,9 @@ __device__ void ns_finalize_body(NsScalars* sc, const NsParams& P, const double*
         for (int k = 0; k < 5; ++k) rv[k] = rv[k] + buf[i][1 + k];
       }
   }
-  const double omega = sc->omega;
+  const double omega = __ldcg(&sc->omega);
+  sc->omega_step = omega;  // for the update; the next stage's limiter starts afresh
+  sc->omega = 1.0;
   if (omega <= 1e-6) atomicOr(status, kErrBadOmega);
   if (!P.lts && omega < 1.0) dt = (1.0 - omega) * dt;
   sc->res = res;
@@ -2026,9 +2019,32 @@ __device__ void ns_finalize_body(NsScalars* sc, const NsParams& P, const double*
   }
 }
 
-__global__ void k_ns_finalize(NsScalars* sc, NsParams P, const double* __restrict__ partial, int nblocks,
-                              unsigned* status, int last_stage) {
-  ns_finalize_body(sc, P, partial, nblocks, status, last_stage);
+// The time discretisation of one problem with the stage's scalar tail folded in: each
+// block publishes its partial sums and limiter minimum, then counts itself in, and the
+// block that arrives last runs ns_finalize_body over all the blocks' partial sums (in
+// block order, whichever block that is, reading them from L2) and clears the count. No
+// block waits for another.
+template <bool DIFF>
+__global__ void __launch_bounds__(kTdBlock) k_ns_timedisc(DevMesh m, NsParams P, const double* __restrict__ U_rhs,
+                                                          const double* __restrict__ rhs1,
+                                                          const double* __restrict__ rhs2,
+                                                          const double* __restrict__ U_td,
+                                                          double* __restrict__ delta, double* __restrict__ partial,
+                                                          NsScalars* sc, double a1, double a2,
+                                                          const double* __restrict__ dterm, int last_stage) {
+  ns_timedisc_body<DIFF>(m, P, U_rhs, rhs1, rhs2, U_td, delta, partial, sc, a1, a2, blockIdx.x, dterm);
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();  // this block's partial sums and limiter minimum before its arrival
+    last = atomicAdd(&sc->arrive, 1u) == gridDim.x - 1 ? 1 : 0;
+  }
+  __syncthreads();
+  if (last && threadIdx.x == 0) {
+    __threadfence();
+    ns_finalize_body(sc, P, partial, gridDim.x, m.status, last_stage);
+    sc->arrive = 0u;
+  }
 }
 
 // sol = sol + a2*omega*delta (:608); U_out may be U_td
@@ -2036,7 +2052,7 @@ __device__ void ns_apply_body(const DevMesh& m, const double* __restrict__ U_td,
                               double* __restrict__ U_out, NsScalars* sc, double a2, const int c) {
   if (sc->skip) return;
   if (c >= m.ne) return;
-  const double omega = sc->omega;
+  const double omega = sc->omega_step;
   const double* u = U_td + kRec * (size_t)c;
   double* o = U_out + kRec * (size_t)c;
   const double* d = delta + 5 * (size_t)c;
@@ -2054,7 +2070,6 @@ __global__ void k_ns_apply(DevMesh m, const double* __restrict__ U_td, const dou
   ns_apply_body(m, U_td, delta, U_out, sc, a2, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
-__global__ void k_ns_reset_omega(NsScalars* sc) { sc->omega = 1.0; }
 
 // ---------------------------------------------------------------------------------
 // Batched launches over a table of problems. A persistent grid walks the work blocks of
@@ -2167,10 +2182,6 @@ __global__ void __launch_bounds__(128) kb_ns_apply(const NsItem* __restrict__ it
     const NsItem& I = it[p];
     ns_apply_body(I.m, I.U0, I.delta, stage == 0 ? I.U1 : I.U0, I.sc, a2, (w - wc[p]) * 128 + threadIdx.x);
   }
-}
-__global__ void kb_ns_reset_omega(const NsItem* __restrict__ it, const int* __restrict__ hdr) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < hdr[0]) it[p].sc->omega = 1.0;
 }
 
 // ---------------------------------------------------------------------------------
@@ -2530,7 +2541,6 @@ void launch_ns_batch_step(const NsTable& t, const NsParams& P, cudaStream_t s) {
     kb_ns_timedisc<<<gc, kTdBlock, 0, s>>>(t.items, t.wc, t.hdr, P, st, a1, a2);
     kb_ns_finalize<<<gp, 128, 0, s>>>(t.items, t.hdr, P, last);
     kb_ns_apply<<<gc, 128, 0, s>>>(t.items, t.wc, t.hdr, st, a2);
-    kb_ns_reset_omega<<<gp, 128, 0, s>>>(t.items, t.hdr);
   };
   if (P.second_order) {
     rhs(0);
@@ -2696,13 +2706,11 @@ void launch_ns_timedisc(const DevMesh& m, const NsParams& P, const double* U_rhs
   const int nb = ns_partial_blocks(m);
   if (P.diff && dterm)
     k_ns_timedisc<true><<<nb, kTdBlock, 0, m.stream>>>(m, P, U_rhs, rhs1, P.second_order ? rhs2 : nullptr, U_td,
-                                                       delta, partial, sc, a1, a2, dterm);
+                                                       delta, partial, sc, a1, a2, dterm, last_stage);
   else
     k_ns_timedisc<false><<<nb, kTdBlock, 0, m.stream>>>(m, P, U_rhs, rhs1, P.second_order ? rhs2 : nullptr, U_td,
-                                                        delta, partial, sc, a1, a2, nullptr);
-  k_ns_finalize<<<1, 1, 0, m.stream>>>(sc, P, partial, nb, m.status, last_stage);
+                                                        delta, partial, sc, a1, a2, nullptr, last_stage);
   k_ns_apply<<<grid_for(m.ne, 256), 256, 0, m.stream>>>(m, U_td, delta, U_out, sc, a2);
-  k_ns_reset_omega<<<1, 1, 0, m.stream>>>(sc);
 }
 
 

@@ -24,7 +24,9 @@ struct NsParams {
 
 struct NsScalars {
   double dtred;    // running min of V / sum_lambda of the current stage (starts at 1e10)
-  double omega;    // running min of the positivity limiter (starts at 1)
+  double omega;    // running min of the positivity limiter (starts at 1; reset by the finalize)
+  double omega_step;  // the limiter of the last finalized stage, which the update applies
+  unsigned arrive;    // blocks of the current stage's time discretisation that finished
   double dt;       // time step of the last stage (after the omega correction)
   double t, final_res;
   double res, resv[5];
