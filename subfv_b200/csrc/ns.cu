@@ -1708,6 +1708,21 @@ __device__ void ns_cell_grad_group(const DevMesh& m, const NsParams& P, const do
         }
     }
   }
+  // the cell's primitive state and this lane's vertex offset, for both limiters
+  T w0[5] = {0, 0, 0, 0, 0}, dx[3] = {0, 0, 0};
+  if (live) {
+    double u0[5];
+    ld5(U, c, u0);
+    T uu[5];
+    for (int k = 0; k < 5; ++k) uu[k] = (T)u0[k];
+    c2p(uu, w0);
+  }
+  if (own) {
+    const double4 ce = m.cc[c], xv = m.x[v];
+    dx[0] = (T)(xv.x - ce.x);
+    dx[1] = (T)(xv.y - ce.y);
+    dx[2] = (T)(xv.z - ce.z);
+  }
   T g[15], ws[5] = {0, 0, 0, 0, 0};
   for (int i = 0; i < 15; ++i) g[i] = 0;
   if (P.method == 2) {  // dual-volume average
@@ -1778,20 +1793,6 @@ __device__ void ns_cell_grad_group(const DevMesh& m, const NsParams& P, const do
     }
     for (int k = 0; k < 5; ++k)
       for (int d = 0; d < 3; ++d) g[5 * d + k] = g[5 * d + k] / ws[k];
-  }
-  T w0[5] = {0, 0, 0, 0, 0}, dx[3] = {0, 0, 0};
-  if (live) {
-    double u0[5];
-    ld5(U, c, u0);
-    T uu[5];
-    for (int k = 0; k < 5; ++k) uu[k] = (T)u0[k];
-    c2p(uu, w0);
-  }
-  if (own) {
-    const double4 ce = m.cc[c], xv = m.x[v];
-    dx[0] = (T)(xv.x - ce.x);
-    dx[1] = (T)(xv.y - ce.y);
-    dx[2] = (T)(xv.z - ce.z);
   }
   T om = 1;  // physical_slope_limiter: this lane's vertex
   {
