@@ -124,6 +124,17 @@ constexpr int kGeoCellFaces = 6;
 // the position kk of the vertex in that face's vertex order (2 bits).
 constexpr unsigned kGfQuad = 1u << 12, kGfLeft = 1u << 13, kGfValid = 1u << 14;
 
+// check_mesh's closure tests (mesh_geometry_module.F90:374-411) compare a norm2 with
+// 1e-14. With every component at most 1 in magnitude gfortran's NORM2 is the correctly
+// rounded sqrt(a*a + b*b + c*c), and rounding sqrt to nearest is monotone, so the test
+// holds exactly when the sum is below the smallest double whose rounded square root
+// reaches 1e-14; a component above 1 (or a NaN) fails both forms. The step's cell kernel
+// takes this form and skips the two square roots.
+constexpr double kClosedSumSq = 0x1.fb0f6be506018p-94;  // 9.999999999999999e-29
+__device__ inline bool norm2_below_1em14(double a0, double a1, double a2) {
+  return fabs(a0) <= 1.0 && fabs(a1) <= 1.0 && fabs(a2) <= 1.0 && (a0 * a0 + a1 * a1 + a2 * a2) < kClosedSumSq;
+}
+
 // The codes of cell c, by the same searches the per-step kernel used to run: a face
 // vertex's local index is its first match among the cell's vertices; a subface's face
 // slot is the first slot holding its face (else the last slot) and its vertex position
@@ -343,8 +354,8 @@ __device__ inline void geom_step_body(const DevMesh& m, double* sol6, const doub
   m.vol[c] = vcell;
   vdiv = div3(vdiv);
   ok = ok && (fabs(vcell - vdiv) < 1e-14);
-  ok = ok && (fnorm2_3(nt.x, nt.y, nt.z) < 1e-14);
-  ok = ok && (fnorm2_3(ns.x, ns.y, ns.z) < 1e-14);
+  ok = ok && norm2_below_1em14(nt.x, nt.y, nt.z);
+  ok = ok && norm2_below_1em14(ns.x, ns.y, ns.z);
   if (!ok) atomicOr(m.status, kErrMeshCheck);
   if (sol6) state_update(m, sol6, rhs6, dt, c);
 }
